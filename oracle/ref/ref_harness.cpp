@@ -1,0 +1,308 @@
+/*
+ * Test-only harness around the UNMODIFIED MSGseqTK v1.2.3 sources (compiled in
+ * place from the reference tree by oracle/ref/Makefile). It exposes a small
+ * extern "C" surface so that Python tests can run the reference's own
+ * read-mapping path as the checker for the CUDA path, and so the bench can time
+ * the reference's OpenMP CPU path. Nothing in the product links this file.
+ *
+ * The reference keeps SMEM bi-interval fields private and its
+ * SMEM::getFwdStart() getter recurses forever (SMEM.h:84-90), so this
+ * translation unit alone reads SMEM members through a private->public define.
+ */
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <string>
+#include <algorithm>
+#include <cmath>
+#include <chrono>
+#include <array>
+#include <set>
+#include <map>
+#include <unordered_map>
+#include <unordered_set>
+#include <iostream>
+#include <sstream>
+#include <regex>
+#include <limits>
+#include <stdexcept>
+#include <utility>
+#include <stack>
+#include <numeric>
+#include <cassert>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define private public
+#define protected public
+#include "SMEM.h"
+#include "SeedChain.h"
+#include "Alignment.h"
+#undef private
+#undef protected
+
+using namespace EGriceLab::MSGseqTK;
+
+namespace {
+
+struct RefDB {
+    MetaGenome mtg;
+    FMDIndex fmd;
+};
+
+/* Decode 2-bit-free ASCII (ACGTN...) into a reference PrimarySeq. */
+PrimarySeq make_read(const uint8_t* nt16, int64_t L, const uint8_t* qual, const char* name) {
+    DNAseq seq(nt16, nt16 + L);
+    QualStr q;
+    if (qual) q.assign(qual, qual + L);
+    else q.assign(L, 30);
+    return PrimarySeq(seq, name ? std::string(name) : std::string("r"), std::string(""), q);
+}
+
+}  // namespace
+
+extern "C" {
+
+/* Build a MetaGenome of n genomes with one chromosome each (chromosome k has
+ * nt16 codes seqs[offs[k]..offs[k+1]) ), then the FMD-index the same way
+ * msgseqtk-build does for a DB below the block size (msgseqtk-build.cpp:435-438):
+ * FMDIndex(mtg.getBDSeq(), true, 32). */
+void* ref_db_build(int64_t n_chrom, const uint8_t* seqs, const int64_t* offs) {
+    RefDB* db = new RefDB();
+    for (int64_t k = 0; k < n_chrom; ++k) {
+        Genome g("g" + std::to_string(k), "genome" + std::to_string(k));
+        DNAseq s(seqs + offs[k], seqs + offs[k + 1]);
+        g.addChrom("chr" + std::to_string(k), s);
+        db->mtg.addGenome(g);
+    }
+    db->mtg.updateIndex();
+    db->fmd = FMDIndex(db->mtg.getBDSeq(), true, FMDIndex::SA_SAMPLE_RATE);
+    return db;
+}
+
+void ref_db_free(void* h) { delete (RefDB*)h; }
+
+int64_t ref_db_length(void* h) { return ((RefDB*)h)->fmd.length(); }
+
+int64_t ref_db_num_chroms(void* h) { return ((RefDB*)h)->mtg.numChroms(); }
+
+/* B[256] and C[256] of the FMD-index. */
+void ref_db_counts(void* h, int64_t* B, int64_t* C) {
+    RefDB* db = (RefDB*)h;
+    for (int i = 0; i < 256; ++i) { B[i] = db->fmd.B[i]; C[i] = db->fmd.C[i]; }
+}
+
+/* The BWT as nt16 codes (FMDIndex::getBWT, FMDIndex.cpp:195). */
+void ref_db_bwt(void* h, uint8_t* out) {
+    DNAseq b = ((RefDB*)h)->fmd.getBWT();
+    std::memcpy(out, b.data(), b.size());
+}
+
+/* The BD text (MetaGenome::getBDSeq, MetaGenome.h:333). */
+void ref_db_bdseq(void* h, uint8_t* out) {
+    DNAseq s = ((RefDB*)h)->mtg.getBDSeq();
+    std::memcpy(out, s.data(), s.size());
+}
+
+int64_t ref_db_access_sa(void* h, int64_t i) { return ((RefDB*)h)->fmd.accessSA(i); }
+
+int64_t ref_db_rank(void* h, int64_t b, int64_t i) { return (int64_t)((RefDB*)h)->fmd.bwtRRR.rank(b, i); }
+
+/* The reference's own SA sample set: rows flagged in SAidx and their values. */
+int64_t ref_db_sa_samples(void* h, int64_t* rows, int64_t* vals, int64_t cap) {
+    RefDB* db = (RefDB*)h;
+    const int64_t n = db->fmd.length();
+    int64_t k = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (db->fmd.SAidx.access(i)) {
+            if (k < cap) { rows[k] = i; vals[k] = db->fmd.SAsampled[db->fmd.SAidx.rank1(i) - 1]; }
+            ++k;
+        }
+    }
+    return k;
+}
+
+/* Chromosome table: BD start/end and forward length per tid. */
+void ref_db_chroms(void* h, int64_t* bd_start, int64_t* bd_end, int64_t* chr_len) {
+    RefDB* db = (RefDB*)h;
+    for (size_t t = 0; t < db->mtg.numChroms(); ++t) {
+        bd_start[t] = db->mtg.getChromBDStart(t);
+        bd_end[t] = db->mtg.getChromBDEnd(t);
+        chr_len[t] = db->mtg.getChromLength(t);
+    }
+}
+
+/* FMDIndex::backExt on an arbitrary bi-interval; returns the new size. */
+int64_t ref_back_ext(void* h, int64_t* p, int64_t* q, int64_t* s, int b) {
+    return ((RefDB*)h)->fmd.backExt(*p, *q, *s, (nt16_t)b);
+}
+
+int64_t ref_fwd_ext(void* h, int64_t* p, int64_t* q, int64_t* s, int b) {
+    return ((RefDB*)h)->fmd.fwdExt(*p, *q, *s, (nt16_t)b);
+}
+
+double ref_loglik(void* h, int b) { return ((RefDB*)h)->fmd.loglik((nt16_t)b); }
+
+/* SMEM_LIST::findAllSMEMS (SMEM.cpp:186) in emission order.
+ * out rows of 6: from, to, fwdStart, revStart, size, logP(bits). */
+int64_t ref_find_smems(void* h, const uint8_t* read, int64_t L, int64_t min_len, double max_evalue,
+                       int64_t* out, int64_t cap) {
+    RefDB* db = (RefDB*)h;
+    PrimarySeq r = make_read(read, L, nullptr, "r");
+    SMEM_LIST smems = SMEM_LIST::findAllSMEMS(&r, &db->mtg, &db->fmd, min_len, max_evalue);
+    int64_t k = 0;
+    for (const SMEM& m : smems) {
+        if (k < cap) {
+            int64_t* o = out + 6 * k;
+            o[0] = m.from; o[1] = m.to; o[2] = m.fwdStart; o[3] = m.revStart; o[4] = m.size;
+            std::memcpy(&o[5], &m.logP, 8);
+        }
+        ++k;
+    }
+    return k;
+}
+
+/* SMEM_LIST::findSeeds (SMEM.cpp:271): rows of 6: from, to, start, end, tid, strand. */
+int64_t ref_find_seeds(void* h, const uint8_t* read, int64_t L, int64_t min_len, double max_evalue,
+                       int64_t max_nseed, int64_t* out, int64_t cap) {
+    RefDB* db = (RefDB*)h;
+    PrimarySeq r = make_read(read, L, nullptr, "r");
+    SeedList seeds = SMEM_LIST::findSeeds(&r, &db->mtg, &db->fmd, min_len, max_evalue, max_nseed);
+    int64_t k = 0;
+    for (const SeedPair& s : seeds) {
+        if (k < cap) {
+            int64_t* o = out + 6 * k;
+            o[0] = s.getFrom(); o[1] = s.getTo(); o[2] = s.getStart(); o[3] = s.getEnd();
+            o[4] = s.getTid(); o[5] = (int64_t)s.getStrand();
+        }
+        ++k;
+    }
+    return k;
+}
+
+/* SeedChain::getChains (SeedChain.cpp:40) on given seeds (rows of 6 as above).
+ * out_idx receives, per chain, the indices of its seeds; out_off the chain
+ * offsets (n_chain + 1 entries). Returns the number of chains. */
+int64_t ref_get_chains(const int64_t* seeds, int64_t n, int64_t max_mismatch, int64_t max_indel,
+                       int64_t* out_off, int64_t* out_idx, int64_t cap_chain, int64_t cap_idx) {
+    SeedList list;
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t* s = seeds + 6 * i;
+        list.push_back(SeedPair(s[0], s[2], s[1] - s[0], s[4], (GLoc::STRAND)s[5], 0.0));
+    }
+    ChainList chains = SeedChain::getChains(list, max_mismatch, max_indel);
+    int64_t nc = 0, ni = 0;
+    if (cap_chain > 0) out_off[0] = 0;
+    for (const SeedChain& c : chains) {
+        for (const SeedPair& s : c) {
+            int64_t idx = -1;
+            for (int64_t i = 0; i < n; ++i) if (list[i] == s) { idx = i; break; }
+            if (ni < cap_idx) out_idx[ni] = idx;
+            ++ni;
+        }
+        ++nc;
+        if (nc < cap_chain + 1 && cap_chain > 0 && nc <= cap_chain) out_off[nc] = ni;
+    }
+    return nc;
+}
+
+/* One alignment record as the reference builds it per chain
+ * (Alignment::buildAlignments, Alignment.cpp:420), before filtering. */
+struct RefAln {
+    int64_t tid, strand, t_start, t_end, aln_from, aln_to, aln_start, aln_end;
+    double aln_score;
+    int64_t n_cigar;
+    int64_t cigar_off;
+    int64_t md_off;
+    int64_t md_len;
+};
+
+/* Per-read SE mapping through chain DP: seeds -> chains -> alignments.
+ * cigar words and MD text are appended into the given buffers. Returns the
+ * number of alignments (unfiltered, chain order). */
+int64_t ref_align_read(void* h, const uint8_t* read, int64_t L, int64_t min_len, double max_evalue,
+                       int64_t max_nseed, int mode, RefAln* out, int64_t cap,
+                       uint32_t* cigar_buf, int64_t cigar_cap, int64_t* cigar_used,
+                       char* md_buf, int64_t md_cap, int64_t* md_used) {
+    RefDB* db = (RefDB*)h;
+    /* const, as in msgseqtk-align.cpp:603-604: the non-const revcom()
+     * overload would reverse-complement the read in place */
+    const PrimarySeq r = make_read(read, L, nullptr, "r");
+    const PrimarySeq rc = r.revcom();
+    SeedList seeds = SMEM_LIST::findSeeds(&r, &db->mtg, &db->fmd, min_len, max_evalue, max_nseed);
+    if (seeds.empty()) return 0;
+    const int64_t maxMismatch = std::ceil(L * Alignment::MAX_MISMATCH_RATE);
+    const int64_t maxIndel = std::ceil(L * Alignment::MAX_INDEL_RATE);
+    ChainList chains = SeedChain::getChains(seeds, maxMismatch, maxIndel);
+    ALIGN_LIST alns = Alignment::buildAlignments(&r, &rc, db->mtg, chains,
+                                                 mode == 0 ? Alignment::GLOBAL : Alignment::LOCAL);
+    int64_t k = 0;
+    for (const Alignment& a : alns) {
+        if (k < cap) {
+            RefAln& o = out[k];
+            o.tid = a.tid; o.strand = a.qStrand; o.t_start = a.tStart; o.t_end = a.tEnd;
+            o.aln_from = a.alnFrom; o.aln_to = a.alnTo; o.aln_start = a.alnStart; o.aln_end = a.alnEnd;
+            o.aln_score = a.alnScore;
+            BAM::cigar_str cg = a.getAlnCigar();
+            std::string md = a.getAlnMDTag();
+            o.n_cigar = cg.size();
+            o.cigar_off = *cigar_used;
+            for (uint32_t w : cg) { if (*cigar_used < cigar_cap) cigar_buf[*cigar_used] = w; ++*cigar_used; }
+            o.md_off = *md_used;
+            o.md_len = md.size();
+            for (char ch : md) { if (*md_used < md_cap) md_buf[*md_used] = ch; ++*md_used; }
+        }
+        ++k;
+    }
+    return k;
+}
+
+/* The reference's SE mapping task body (msgseqtk-align.cpp:610-648) over a
+ * batch of reads with OpenMP, for timing: findSeeds -> getChains ->
+ * buildAlignments -> filter -> evaluate -> calcMapQ -> sort. reads are nt16
+ * codes at offs[i]..offs[i+1]; quals likewise. Returns the number of reads
+ * with at least one alignment kept; *seconds gets the steady_clock time. */
+int64_t ref_map_batch(void* h, int64_t n_reads, const uint8_t* reads, const uint8_t* quals,
+                      const int64_t* offs, int64_t min_len, double max_evalue, int64_t max_nseed,
+                      double min_score_rate, int n_threads, double* seconds, int64_t* n_aln_out) {
+    RefDB* db = (RefDB*)h;
+#ifdef _OPENMP
+    if (n_threads > 0) omp_set_num_threads(n_threads);
+#endif
+    int64_t mapped = 0, n_aln = 0;
+    auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : mapped, n_aln)
+    for (int64_t i = 0; i < n_reads; ++i) {
+        const int64_t L = offs[i + 1] - offs[i];
+        const PrimarySeq r = make_read(reads + offs[i], L, quals ? quals + offs[i] : nullptr, "r");
+        const PrimarySeq rc = r.revcom();
+        SeedList seeds = SMEM_LIST::findSeeds(&r, &db->mtg, &db->fmd, min_len, max_evalue, max_nseed);
+        if (seeds.empty()) continue;
+        const int64_t maxMismatch = std::ceil(L * Alignment::MAX_MISMATCH_RATE);
+        const int64_t maxIndel = std::ceil(L * Alignment::MAX_INDEL_RATE);
+        ChainList chains = SeedChain::getChains(seeds, maxMismatch, maxIndel);
+        ALIGN_LIST alns = Alignment::buildAlignments(&r, &rc, db->mtg, chains, Alignment::GLOBAL);
+        Alignment::filter(alns, min_score_rate);
+        if (alns.empty()) continue;
+        Alignment::evaluate(alns);
+        Alignment::calcMapQ(alns);
+        Alignment::sort(alns);
+        mapped += 1;
+        n_aln += (int64_t)alns.size();
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    *seconds = std::chrono::duration<double>(t1 - t0).count();
+    *n_aln_out = n_aln;
+    return mapped;
+}
+
+int ref_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"
