@@ -1,0 +1,191 @@
+/*
+ * msg_b200.h -- C ABI of the B200 (sm_100a) read-mapping library that stands
+ * in for MSGseqTK's seeding -> locate -> chaining -> DP path.
+ *
+ * The reference has no FFI; its "operator API" is a set of C++ classes called
+ * from the per-read task bodies of msgseqtk-align (src/msgseqtk-align.cpp:610-628
+ * for single-end, :680-705 for each mate of a pair). Each entry point below
+ * names the reference interface it replaces. Plain pointers and sizes only;
+ * all host buffers belong to the caller; no exceptions cross the ABI; every
+ * function returns an msg_status.
+ *
+ * Threading: one host thread per msg_ctx (calls on one context are not
+ * re-entrant); contexts are independent. Each context owns one CUDA stream.
+ */
+#ifndef MSG_B200_H
+#define MSG_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum msg_status {
+    MSG_OK = 0,
+    MSG_EINVAL = 1,        /* bad argument (null pointer, inconsistent sizes) */
+    MSG_ENOMEM = 2,        /* device or host allocation failed */
+    MSG_EUNSUPPORTED = 3,  /* input the CUDA path does not implement (see msg_strerror) */
+    MSG_ETIMEOUT = 4,      /* a bounded device wait ran out */
+    MSG_ECUDA = 5,         /* CUDA runtime error */
+    MSG_ESTATE = 6,        /* call out of order (e.g. mapping before an index is loaded) */
+    MSG_EINTERNAL = 7      /* a device-side consistency check failed */
+} msg_status;
+
+/* Human-readable text for a status code (static storage). */
+const char* msg_strerror(int status);
+
+typedef struct msg_ctx msg_ctx;
+
+/* Detail of the last failure on this context (valid until the next call). */
+const char* msg_last_error(const msg_ctx* ctx);
+
+/* Create a context on CUDA device `device`. */
+int msg_ctx_create(int device, msg_ctx** out);
+void msg_ctx_destroy(msg_ctx* ctx);
+
+/* Decoded FMD-index, as FMDIndex holds it (src/FMDIndex.h:337-343):
+ * the BWT as nt16 codes (getBWT, FMDIndex.cpp:195), base counts B[0..15]
+ * (C[] is derived exactly as buildCounts does, FMDIndex.cpp:118-129), and the
+ * SA sample set -- rows flagged in SAidx (i % 32 == 0 or BWT[i] == 0,
+ * FMDIndex.cpp:465-480) with their SAsampled values, rows ascending. */
+typedef struct msg_fmd_view {
+    int64_t n;
+    const uint8_t* bwt;
+    const int64_t* base_count;   /* 16 entries */
+    int64_t n_samples;
+    const int64_t* sample_rows;
+    const int64_t* sample_vals;
+} msg_fmd_view;
+
+/* MetaGenome coordinate table and target sequences (src/MetaGenome.h:147-167,
+ * 237-261, 319-321): per chromosome (tid order) its BD start/end, its length
+ * WITHOUT the terminator, and the forward nt16 sequences concatenated at
+ * chr_off[t] .. chr_off[t+1]. */
+typedef struct msg_mtg_view {
+    int64_t n_chrom;
+    const int64_t* bd_start;
+    const int64_t* bd_end;
+    const int64_t* chr_len;
+    const uint8_t* chr_seq;
+    const int64_t* chr_off;      /* n_chrom + 1 entries */
+} msg_mtg_view;
+
+/* Load an index into device memory (replaces FMDIndex::load + MetaGenome::load
+ * for the mapping path, src/msgseqtk-align.cpp:444-508). Builds the device
+ * image: 2-bit BWT with occurrence buckets, the full suffix array (recovered
+ * on the device from the SA samples), and the chromosome table. */
+int msg_index_load(msg_ctx* ctx, const msg_fmd_view* fmd, const msg_mtg_view* mtg);
+
+/* Device bytes held by the loaded index. */
+int msg_index_bytes(const msg_ctx* ctx, int64_t* bytes);
+
+/* Mapping parameters (src/msgseqtk-align.cpp:183-397 defaults). */
+typedef struct msg_map_params {
+    int64_t min_len;        /* --min-seed, SMEM::MIN_LENGTH = 17 */
+    double max_evalue;      /* --max-evalue, SMEM::MAX_EVALUE = 0.01; +inf for no limit */
+    int64_t max_nseed;      /* --max-nseed, SMEM::MAX_NSEED = 500 */
+    int32_t mode;           /* 0 = GLOBAL (NW, default), 1 = LOCAL (SW) */
+    /* ScoreScheme (src/ScoreScheme.cpp:14-18); integral values only */
+    double match, mismatch, gap_open, gap_ext;
+} msg_map_params;
+
+/* Fill defaults. */
+void msg_map_params_default(msg_map_params* p);
+
+/* A batch of reads: nt16 codes concatenated, read i at seq[off[i] .. off[i+1]). */
+typedef struct msg_read_batch {
+    int64_t n_reads;
+    const uint8_t* seq;
+    const int64_t* off;     /* n_reads + 1 entries */
+} msg_read_batch;
+
+/* One alignment per seed chain, in the order Alignment::buildAlignments
+ * produces them (src/Alignment.cpp:420-427), before Alignment::filter.
+ * Coordinates follow Alignment's fields (src/Alignment.h:357-372). */
+typedef struct msg_aln {
+    int64_t read;           /* index of the read in the batch */
+    int32_t tid;
+    int32_t strand;         /* GLoc::STRAND: 1 = FWD, 2 = REV */
+    int64_t t_start, t_end; /* DP window on the chromosome */
+    int64_t aln_from, aln_to, aln_start, aln_end;
+    int32_t aln_score;      /* integral; the reference stores it as a double */
+    int32_t flags;          /* bit0: last row held no finite score; bit1: traceback left the matrix */
+    int64_t cigar_off;      /* CIGAR words (SAM encoding len<<4|op) in the output's cigar array */
+    int32_t n_cigar;
+    int32_t pad;
+} msg_aln;
+
+/* Output buffers owned by the caller. The library fills at most *_cap entries
+ * and always reports the counts it needed in n_aln / n_cigar; when a count
+ * exceeds its capacity the call returns MSG_EINVAL with nothing else valid. */
+typedef struct msg_aln_out {
+    int64_t aln_cap;
+    msg_aln* aln;
+    int64_t cigar_cap;
+    uint32_t* cigar;
+    int64_t n_aln;          /* out */
+    int64_t n_cigar;        /* out */
+    int64_t* read_aln_off;  /* optional, n_reads + 1: alignments of read i are aln[off[i] .. off[i+1]) */
+} msg_aln_out;
+
+/* Optional per-stage dumps for parity checks (any pointer may be NULL). */
+typedef struct msg_stage_dump {
+    /* SMEMs in SMEM_LIST::findAllSMEMS emission order (src/SMEM.cpp:186-215),
+     * rows of 6 int64: from, to, fwdStart, revStart, size, logP bit pattern */
+    int64_t smem_cap;
+    int64_t* smem;
+    int64_t* smem_off;      /* n_reads + 1 */
+    /* seeds after SeedPair::removeRedundant (src/SeedPair.cpp:71-88), rows of
+     * 6 int64: from, to, start, end, tid, strand */
+    int64_t seed_cap;
+    int64_t* seed;
+    int64_t* seed_off;      /* n_reads + 1 */
+    int64_t n_smem, n_seed; /* out */
+} msg_stage_dump;
+
+/* Statistics of the last mapping call. */
+typedef struct msg_map_stats {
+    int64_t n_reads, n_smem, n_seed, n_chain, n_aln;
+    int64_t n_ext;          /* bi-interval extensions that reached the occurrence lookup */
+    int64_t n_sa;           /* suffix-array rows located */
+    int64_t dp_cells;       /* cells of the reference DP cell set (rectangles + seed diagonals) */
+    int64_t host_sorted;    /* reads whose SMEM order needed the host std::sort */
+    double ms_total, ms_smem, ms_locate, ms_chain, ms_dp;
+} msg_map_stats;
+
+/* Map a batch of reads held in HOST memory: the per-read SE task body
+ * findSeeds -> getChains -> buildAlignments (src/msgseqtk-align.cpp:612-625;
+ * SMEM_LIST::findSeeds src/SMEM.cpp:271, SeedChain::getChains
+ * src/SeedChain.cpp:40, Alignment::buildAlignments src/Alignment.cpp:420).
+ * For paired-end data call it on both mates (findSeedsPE, src/SMEM.h:383-389,
+ * is two independent findSeeds calls). `dump` may be NULL. */
+int msg_map_batch(msg_ctx* ctx, const msg_read_batch* reads, const msg_map_params* params,
+                  msg_aln_out* out, msg_stage_dump* dump);
+
+/* Same as msg_map_batch with the reads already in device memory (seq and off
+ * are device pointers); results still land in the caller's host buffers. */
+int msg_map_batch_device(msg_ctx* ctx, const msg_read_batch* dev_reads, const msg_map_params* params,
+                         msg_aln_out* out, msg_stage_dump* dump);
+
+int msg_last_stats(const msg_ctx* ctx, msg_map_stats* stats);
+
+/* ---- Single-operation entry points (parity checks of the index layer) ---- */
+
+/* WaveletTreeRRR::rank (src/libsds/src/WaveletTreeRRR.cpp:101-125) through
+ * FMDIndex: occurrences of nt16 symbol b[k] in BWT[0 .. i[k]] (or -1 when
+ * i[k] >= n) for k < count. Host arrays. */
+int msg_occ_query(msg_ctx* ctx, int64_t count, const uint8_t* b, const int64_t* i, int64_t* out);
+
+/* FMDIndex::backExt (src/FMDIndex.cpp:577-610) when dir == 0, fwdExt
+ * (src/FMDIndex.h:226-228) when dir == 1, on count bi-intervals in place;
+ * ret[k] receives the returned size. Host arrays. */
+int msg_bi_ext_query(msg_ctx* ctx, int64_t count, int dir, const uint8_t* b, int64_t* p, int64_t* q,
+                     int64_t* s, int64_t* ret);
+
+/* FMDIndex::accessSA (src/FMDIndex.cpp:520-527) for count rows. Host arrays. */
+int msg_sa_query(msg_ctx* ctx, int64_t count, const int64_t* rows, int64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,54 @@
+// Context lifetime and status strings of the C ABI.
+#include <cstdio>
+
+#include "msg_ctx.cuh"
+
+extern "C" const char* msg_strerror(int status) {
+    switch (status) {
+        case MSG_OK: return "ok";
+        case MSG_EINVAL: return "invalid argument";
+        case MSG_ENOMEM: return "out of memory";
+        case MSG_EUNSUPPORTED: return "unsupported input for the CUDA path";
+        case MSG_ETIMEOUT: return "bounded device wait ran out";
+        case MSG_ECUDA: return "CUDA runtime error";
+        case MSG_ESTATE: return "call out of order";
+        case MSG_EINTERNAL: return "device consistency check failed";
+        default: return "unknown status";
+    }
+}
+
+extern "C" int msg_ctx_create(int device, msg_ctx** out) {
+    if (!out) return MSG_EINVAL;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return MSG_ECUDA;
+    if (device < 0 || device >= n) return MSG_EINVAL;
+    if (cudaSetDevice(device) != cudaSuccess) return MSG_ECUDA;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return MSG_ECUDA;
+    if (prop.major < 10) return MSG_EUNSUPPORTED;  // built for sm_100a only
+    msg_ctx* c = new (std::nothrow) msg_ctx();
+    if (!c) return MSG_ENOMEM;
+    c->device = device;
+    c->num_sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return MSG_ECUDA; }
+    for (auto& e : c->ev) cudaEventCreate(&e);
+    *out = c;
+    return MSG_OK;
+}
+
+extern "C" void msg_ctx_destroy(msg_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    c->index_free();
+    for (msg::DevBuf* b : {&c->reads, &c->offs, &c->smem, &c->smem_cnt, &c->prev, &c->sel, &c->seedoff, &c->seeds,
+                           &c->seeds2, &c->rcount, &c->chains, &c->chainidx, &c->dpinfo, &c->scratch, &c->path,
+                           &c->alnbuf, &c->cigbuf, &c->misc, &c->status})
+        b->release();
+    for (auto& e : c->ev) cudaEventDestroy(e);
+    cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+extern "C" const char* msg_last_error(const msg_ctx* c) { return c ? c->last_error.c_str() : ""; }

@@ -1,0 +1,534 @@
+// Read-mapping pipeline on sm_100a: SMEM seeding -> seed selection -> locate ->
+// redundant-seed removal -> DFS chaining -> seed-guided affine DP + traceback.
+//
+// Every stage reproduces the reference's results exactly (integer/byte work;
+// the double-precision SMEM log-likelihood sums are made in the reference's
+// order with round-to-nearest adds). Kernel-to-reference mapping:
+//   k_smem      SMEM_LIST::findAllSMEMS / findFwdBackSMEMS / findBackFwdSMEMS (SMEM.cpp:64-215)
+//   k_select    SMEM_LIST::findSeeds sort + maxNSeed cut (SMEM.cpp:271-300)
+//   k_locate    SMEM::getSeeds (SMEM.cpp:244-269) with FMDIndex::accessSA and MetaGenome::getTid/getLoc/getStrand
+//   k_dedup     SeedPair::removeRedundant (SeedPair.cpp:71-88)
+//   k_chain     SeedChain::getChains / dfsSeeds (SeedChain.cpp:40-73)
+//   k_dp        Alignment ctor window, calculateScores(chain), backTraceNW/SW (Alignment.cpp:46-276)
+//   k_cigar     Alignment::getAlnCigar (Alignment.cpp:278-303)
+#include "map_kernels.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#include <cub/cub.cuh>
+
+#include "msg_ctx.cuh"
+
+using namespace msg;
+
+namespace {
+
+int64_t nblk(int64_t n, int t) { return (n + t - 1) / t; }
+
+// Largest double ll with n * exp(ll) <= max_e (the e-value test of
+// SMEM::evalue, SMEM.h:102-110, made with the host's own exp exactly as the
+// reference makes it). The predicate is monotone in ll, so SMEM stages compare
+// the log-likelihood sum against this threshold instead of calling exp.
+uint64_t dkey(double d) {
+    uint64_t u;
+    std::memcpy(&u, &d, 8);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+double dval(uint64_t k) {
+    uint64_t u = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    double d;
+    std::memcpy(&d, &u, 8);
+    return d;
+}
+bool evalue_ok(int64_t n, double ll, double max_e) { return (double)n * std::exp(ll) <= max_e; }
+
+int evalue_threshold(int64_t n, double max_e, double* thr, int* all) {
+    if (std::isnan(max_e) || max_e < 0) return MSG_EINVAL;
+    if (std::isinf(max_e)) { *all = 1; *thr = std::numeric_limits<double>::infinity(); return MSG_OK; }
+    *all = 0;
+    uint64_t lo = dkey(-std::numeric_limits<double>::infinity());
+    uint64_t hi = dkey(std::numeric_limits<double>::infinity());
+    if (!evalue_ok(n, dval(lo), max_e)) { *thr = -std::numeric_limits<double>::infinity(); return MSG_OK; }
+    while (hi - lo > 1) {  // invariant: ok(lo), !ok(hi)
+        const uint64_t mid = lo + (hi - lo) / 2;
+        if (evalue_ok(n, dval(mid), max_e)) lo = mid; else hi = mid;
+    }
+    // monotonicity check around the threshold
+    for (uint64_t d = 1; d <= 4096; d <<= 1) {
+        if (lo >= d && !evalue_ok(n, dval(lo - d), max_e)) return MSG_EINTERNAL;
+        if (!evalue_ok(n, dval(lo + d), max_e) == false) return MSG_EINTERNAL;
+    }
+    *thr = dval(lo);
+    return MSG_OK;
+}
+
+template <typename T>
+cudaError_t scan_excl(msg_ctx* ctx, const T* in, T* out, int64_t n, DevBuf& tmpb) {
+    size_t tb = 0;
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, n, ctx->stream);
+    if (e != cudaSuccess) return e;
+    e = tmpb.ensure(tb);
+    if (e != cudaSuccess) return e;
+    return cub::DeviceScan::ExclusiveSum(tmpb.p, tb, in, out, n, ctx->stream);
+}
+
+// exclusive scan of n values into n+1 offsets; returns the total
+template <typename T>
+cudaError_t offsets(msg_ctx* ctx, T* cnt_with_room, int64_t n, T* off, DevBuf& tmpb, T* total) {
+    cudaError_t e = cudaMemsetAsync(cnt_with_room + n, 0, sizeof(T), ctx->stream);
+    if (e != cudaSuccess) return e;
+    e = scan_excl(ctx, cnt_with_room, off, n + 1, tmpb);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(total, off + n, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(ctx->stream);
+}
+
+__global__ void k_i32_to_i64(const int32_t* __restrict__ a, int64_t* __restrict__ b, int64_t n) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i];
+}
+
+__global__ void k_read_len(const int64_t* __restrict__ off, int64_t n, int64_t* __restrict__ len,
+                           unsigned long long* __restrict__ mx) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t l = off[i + 1] - off[i];
+    len[i] = l;
+    atomicMax(mx, (unsigned long long)(l < 0 ? 0 : l));
+}
+
+__global__ void k_smem_read(const int64_t* __restrict__ smem_off, int64_t n_reads, int32_t* __restrict__ smem_read) {
+    const int64_t r = blockIdx.x;
+    if (r >= n_reads) return;
+    for (int64_t k = smem_off[r] + threadIdx.x; k < smem_off[r + 1]; k += blockDim.x) smem_read[k] = (int32_t)r;
+}
+
+__global__ void k_gather_off(const int64_t* __restrict__ smem_off, const int64_t* __restrict__ smem_seed_off,
+                             int64_t n_reads, int64_t* __restrict__ read_seed_off) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r > n_reads) return;
+    read_seed_off[r] = smem_seed_off[smem_off[r]];
+}
+
+__global__ void k_aln_cig(msg_aln* __restrict__ aln, const int64_t* __restrict__ cig_off, int64_t n) {
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    aln[c].cigar_off = cig_off[c];
+    aln[c].n_cigar = (int32_t)(cig_off[c + 1] - cig_off[c]);
+    aln[c].pad = 0;
+}
+
+struct Timer {
+    msg_ctx* ctx;
+    int k = 0;
+    void mark() { cudaEventRecord(ctx->ev[k++], ctx->stream); }
+    float ms(int a, int b) {
+        float t = 0;
+        cudaEventElapsedTime(&t, ctx->ev[a], ctx->ev[b]);
+        return t;
+    }
+};
+
+int check_params(const msg_map_params* p, DpParams* dp) {
+    if (!p) return MSG_EINVAL;
+    if (p->min_len < 1 || p->max_nseed < 1 || (p->mode != 0 && p->mode != 1)) return MSG_EINVAL;
+    if (std::isnan(p->max_evalue) || p->max_evalue < 0) return MSG_EINVAL;
+    const double v[4] = {p->match, p->mismatch, p->gap_open, p->gap_ext};
+    int32_t iv[4];
+    for (int k = 0; k < 4; ++k) {
+        if (!(v[k] >= 0 && v[k] <= 1 << 20) || std::floor(v[k]) != v[k]) return MSG_EUNSUPPORTED;
+        iv[k] = (int32_t)v[k];
+    }
+    dp->match = iv[0]; dp->mismatch = iv[1]; dp->gap_o = iv[2]; dp->gap_e = iv[3]; dp->mode = p->mode;
+    return MSG_OK;
+}
+
+}  // namespace
+
+extern "C" void msg_map_params_default(msg_map_params* p) {
+    if (!p) return;
+    p->min_len = 17;
+    p->max_evalue = 0.01;
+    p->max_nseed = 500;
+    p->mode = 0;
+    p->match = 1;
+    p->mismatch = 3;
+    p->gap_open = 5;
+    p->gap_ext = 2;
+}
+
+static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, int64_t n_reads,
+                    const msg_map_params* params, msg_aln_out* out, msg_stage_dump* dump) {
+    DpParams dpp;
+    int rc = check_params(params, &dpp);
+    if (rc != MSG_OK) return ctx->fail(rc, rc == MSG_EUNSUPPORTED ? "score scheme must be non-negative integers" : "bad mapping parameters");
+    const IndexImage& im = ctx->idx;
+    const IndexDev& ix = im.dev;
+    double thr = 0;
+    int thr_all = 0;
+    rc = evalue_threshold(ix.n, params->max_evalue, &thr, &thr_all);
+    if (rc != MSG_OK) return ctx->fail(rc, "e-value threshold");
+    cudaStream_t st = ctx->stream;
+    msg_map_stats& S = ctx->stats;
+    std::memset(&S, 0, sizeof(S));
+    S.n_reads = n_reads;
+    Timer tm{ctx};
+    auto t_host0 = std::chrono::steady_clock::now();
+    tm.mark();  // 0
+#define CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return ctx->cuda_fail(e_); } while (0)
+    DevBuf& misc = ctx->misc;
+    CK(ctx->status.ensure(64));
+    uint32_t* d_status = ctx->status.as<uint32_t>();
+    unsigned long long* d_ctr = reinterpret_cast<unsigned long long*>(d_status + 4);
+    CK(cudaMemsetAsync(d_status, 0, 64, st));
+
+    // read lengths
+    CK(ctx->rcount.ensure((n_reads + 1) * sizeof(int64_t) * 8 + 64));
+    int64_t* d_rlen = ctx->rcount.as<int64_t>();
+    int64_t* d_cnt64 = d_rlen + (n_reads + 1);          // scratch counts (n+1)
+    int64_t* d_smem_off = d_cnt64 + (n_reads + 1);      // n+1
+    int64_t* d_read_seed_off = d_smem_off + (n_reads + 1);
+    int64_t* d_nchain = d_read_seed_off + (n_reads + 1);
+    int64_t* d_nidx = d_nchain + (n_reads + 1);
+    int64_t* d_chain_off = d_nidx + (n_reads + 1);
+    int64_t* d_idx_off = d_chain_off + (n_reads + 1);
+    unsigned long long h_maxlen = 0;
+    if (n_reads > 0) {
+        k_read_len<<<nblk(n_reads, 256), 256, 0, st>>>(d_off, n_reads, d_rlen, d_ctr + 2);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(&h_maxlen, d_ctr + 2, 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    const int64_t Lmax = (int64_t)h_maxlen;
+
+    // ---------------- SMEMs ----------------
+    const int threads = 256;
+    const int blocks = ctx->num_sms * 8;
+    const int64_t n_warps = (int64_t)blocks * threads / 32;
+    const int64_t pv_cap = Lmax + 2;
+    CK(ctx->prev.ensure(n_warps * pv_cap * (4 + 8 + 8 + 8 + 8) + 64));
+    int64_t cap = 16;
+    int64_t h_nsmem = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        CK(ctx->smem.ensure((size_t)std::max<int64_t>(1, n_reads) * cap * 48));
+        CK(ctx->smem_cnt.ensure((n_reads + 1) * sizeof(int32_t)));
+        SmemArgs sa{};
+        sa.seq = d_seq; sa.off = d_off; sa.n_reads = n_reads; sa.min_len = params->min_len;
+        sa.thr = thr; sa.thr_all = thr_all;
+        for (int b = 0; b < 16; ++b) sa.llk[b] = im.llk[b];
+        sa.out = ctx->smem.as<int64_t>(); sa.cap = cap; sa.count = ctx->smem_cnt.as<int32_t>();
+        char* pv = ctx->prev.as<char>();
+        sa.pv_p = reinterpret_cast<int64_t*>(pv);
+        sa.pv_q = sa.pv_p + n_warps * pv_cap;
+        sa.pv_s = sa.pv_q + n_warps * pv_cap;
+        sa.pv_lp = reinterpret_cast<double*>(sa.pv_s + n_warps * pv_cap);
+        sa.pv_pos = reinterpret_cast<int32_t*>(sa.pv_lp + n_warps * pv_cap);
+        sa.pv_cap = pv_cap;
+        sa.work = d_ctr;
+        sa.n_ext = d_ctr + 1;
+        sa.status = d_status;
+        CK(cudaMemsetAsync(d_ctr, 0, 16, st));
+        CK(cudaMemsetAsync(d_status, 0, 4, st));
+        if (n_reads > 0) {
+            k_smem<<<blocks, threads, 0, st>>>(sa, ix);
+            CK(cudaGetLastError());
+        }
+        uint32_t h_status = 0;
+        CK(cudaMemcpyAsync(&h_status, d_status, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (h_status & kErrInternal) return ctx->fail(MSG_EINTERNAL, "SMEM stage consistency check failed");
+        if (!(h_status & kErrOverflow)) break;
+        if (attempt == 1) return ctx->fail(MSG_EINTERNAL, "SMEM output overflow after resizing");
+        // rerun with the largest per-read count as capacity
+        std::vector<int32_t> cnt(n_reads);
+        CK(cudaMemcpy(cnt.data(), ctx->smem_cnt.p, n_reads * 4, cudaMemcpyDeviceToHost));
+        cap = *std::max_element(cnt.begin(), cnt.end());
+    }
+    {
+        unsigned long long e = 0;
+        CK(cudaMemcpyAsync(&e, d_ctr + 1, 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        S.n_ext = (int64_t)e;
+    }
+    if (n_reads > 0) k_i32_to_i64<<<nblk(n_reads, 256), 256, 0, st>>>(ctx->smem_cnt.as<int32_t>(), d_cnt64, n_reads);
+    CK(offsets(ctx, d_cnt64, n_reads, d_smem_off, misc, &h_nsmem));
+    S.n_smem = h_nsmem;
+    CK(ctx->sel.ensure((h_nsmem + 1) * (48 + 1 + 4 + 8 + 8 + 4) + 64));
+    int64_t* d_smem = ctx->sel.as<int64_t>();                              // dense SMEM rows
+    int64_t* d_smem_seed_cnt = d_smem + 6 * h_nsmem;                       // n_smem + 1
+    int64_t* d_smem_seed_off = d_smem_seed_cnt + (h_nsmem + 1);            // n_smem + 1
+    int32_t* d_smem_read = reinterpret_cast<int32_t*>(d_smem_seed_off + (h_nsmem + 1));
+    int32_t* d_fill = d_smem_read + (h_nsmem + 1);
+    uint8_t* d_sel = reinterpret_cast<uint8_t*>(d_fill + (h_nsmem + 1));
+    if (n_reads > 0) {
+        k_compact_smem<<<n_reads, 64, 0, st>>>(ctx->smem.as<int64_t>(), cap, ctx->smem_cnt.as<int32_t>(), d_smem_off,
+                                               n_reads, d_smem);
+        CK(cudaGetLastError());
+    }
+    tm.mark();  // 1
+
+    // ---------------- selection (maxNSeed) ----------------
+    int32_t* d_hflag = reinterpret_cast<int32_t*>(d_cnt64);  // reuse scratch (n int32)
+    if (n_reads > 0) {
+        k_select<<<nblk(n_reads, 256), 256, 0, st>>>(d_smem, d_smem_off, n_reads, params->max_nseed, d_sel, d_hflag);
+        CK(cudaGetLastError());
+        std::vector<int32_t> hflag(n_reads);
+        CK(cudaMemcpyAsync(hflag.data(), d_hflag, n_reads * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        std::vector<int64_t> flagged;
+        for (int64_t r = 0; r < n_reads; ++r) if (hflag[r]) flagged.push_back(r);
+        if (!flagged.empty()) {
+            // SMEM_LIST::findSeeds (SMEM.cpp:275-291): std::sort by loglik (not
+            // stable; same libstdc++ algorithm on the same emission order), then
+            // locate until at least maxNSeed seeds.
+            std::vector<int64_t> soff(n_reads + 1);
+            CK(cudaMemcpy(soff.data(), d_smem_off, (n_reads + 1) * 8, cudaMemcpyDeviceToHost));
+            struct HS { double lp; int64_t size; int64_t k; };
+            for (int64_t r : flagged) {
+                const int64_t a = soff[r], b = soff[r + 1];
+                std::vector<int64_t> rows((b - a) * 6);
+                CK(cudaMemcpy(rows.data(), d_smem + 6 * a, (b - a) * 48, cudaMemcpyDeviceToHost));
+                std::vector<HS> v;
+                for (int64_t k = 0; k < b - a; ++k) {
+                    HS h;
+                    std::memcpy(&h.lp, &rows[6 * k + 5], 8);
+                    h.size = rows[6 * k + 4];
+                    h.k = k;
+                    v.push_back(h);
+                }
+                std::sort(v.begin(), v.end(), [](const HS& x, const HS& y) -> bool { return x.lp < y.lp; });
+                std::vector<uint8_t> sel(b - a, 0);
+                int64_t got = 0;
+                for (const HS& h : v) {
+                    sel[h.k] = 1;
+                    got += h.size;
+                    if (got >= params->max_nseed) break;
+                }
+                CK(cudaMemcpy(d_sel + a, sel.data(), b - a, cudaMemcpyHostToDevice));
+            }
+            S.host_sorted = (int64_t)flagged.size();
+        }
+    }
+    if (h_nsmem > 0) {
+        k_seed_counts<<<nblk(h_nsmem, 256), 256, 0, st>>>(d_smem, d_sel, h_nsmem, d_smem_seed_cnt);
+        CK(cudaGetLastError());
+    }
+    int64_t h_nseed_raw = 0;
+    CK(offsets(ctx, d_smem_seed_cnt, h_nsmem, d_smem_seed_off, misc, &h_nseed_raw));
+    if (n_reads > 0) {
+        k_gather_off<<<nblk(n_reads + 1, 256), 256, 0, st>>>(d_smem_off, d_smem_seed_off, n_reads, d_read_seed_off);
+        k_smem_read<<<n_reads, 64, 0, st>>>(d_smem_off, n_reads, d_smem_read);
+        CK(cudaGetLastError());
+    }
+
+    // ---------------- locate ----------------
+    CK(ctx->seeds.ensure((h_nseed_raw + 1) * sizeof(Seed)));
+    CK(ctx->seeds2.ensure((h_nseed_raw + 1) * sizeof(Seed)));
+    Seed* d_seeds = ctx->seeds.as<Seed>();
+    Seed* d_seeds2 = ctx->seeds2.as<Seed>();
+    S.n_sa = 2 * h_nseed_raw;
+    if (h_nseed_raw > 0) {
+        CK(cudaMemsetAsync(d_fill, 0, (h_nsmem + 1) * 4, st));
+        const int64_t g = std::min<int64_t>(nblk(h_nseed_raw, 256), (int64_t)ctx->num_sms * 32);
+        k_locate<<<g, 256, 0, st>>>(ix, d_smem, d_smem_seed_off, d_smem_read, d_off, h_nsmem, h_nseed_raw, d_fill,
+                                    d_seeds, d_status);
+        CK(cudaGetLastError());
+    }
+    tm.mark();  // 2
+
+    // ---------------- redundant-seed removal ----------------
+    int32_t* d_ndedup = reinterpret_cast<int32_t*>(d_cnt64);  // n int32 (flags no longer needed)
+    if (n_reads > 0) {
+        k_dedup<<<nblk(n_reads * 32, 128), 128, 0, st>>>(d_read_seed_off, n_reads, d_seeds, d_seeds2, d_seeds, d_ndedup);
+        CK(cudaGetLastError());
+    }
+
+    // ---------------- chains ----------------
+    CK(ctx->chains.ensure((h_nseed_raw + 1) * (1 + 4 + 4) + 64));
+    uint8_t* d_vis = ctx->chains.as<uint8_t>();
+    int32_t* d_stki = reinterpret_cast<int32_t*>(d_vis + ((h_nseed_raw + 1 + 15) / 16) * 16);
+    int32_t* d_stkj = d_stki + (h_nseed_raw + 1);
+    int64_t h_nchain = 0, h_nidx = 0;
+    if (n_reads > 0) {
+        k_chain<<<nblk(n_reads, 128), 128, 0, st>>>(d_read_seed_off, d_ndedup, d_rlen, n_reads, d_seeds, d_vis, d_stki,
+                                                   d_stkj, 0, d_nchain, d_nidx, nullptr, nullptr, nullptr, nullptr,
+                                                   nullptr, nullptr);
+        CK(cudaGetLastError());
+    }
+    CK(offsets(ctx, d_nchain, n_reads, d_chain_off, misc, &h_nchain));
+    CK(offsets(ctx, d_nidx, n_reads, d_idx_off, misc, &h_nidx));
+    S.n_chain = h_nchain;
+    CK(ctx->chainidx.ensure((h_nchain + 1) * (8 + 4 + 4) + (h_nidx + 1) * 8 + 64));
+    int64_t* d_cidx_off = ctx->chainidx.as<int64_t>();
+    int64_t* d_cidx = d_cidx_off + (h_nchain + 1);
+    int32_t* d_clen = reinterpret_cast<int32_t*>(d_cidx + (h_nidx + 1));
+    int32_t* d_cread = d_clen + (h_nchain + 1);
+    if (n_reads > 0 && h_nchain > 0) {
+        k_chain<<<nblk(n_reads, 128), 128, 0, st>>>(d_read_seed_off, d_ndedup, d_rlen, n_reads, d_seeds, d_vis, d_stki,
+                                                   d_stkj, 1, nullptr, nullptr, d_chain_off, d_idx_off, d_cidx_off,
+                                                   d_clen, d_cread, d_cidx);
+        CK(cudaGetLastError());
+    }
+    tm.mark();  // 3
+
+    // ---------------- DP ----------------
+    CK(ctx->dpinfo.ensure((h_nchain + 1) * 8 * 8 + 64));
+    int64_t* d_ts = ctx->dpinfo.as<int64_t>();
+    int64_t* d_te = d_ts + (h_nchain + 1);
+    int64_t* d_cells = d_te + (h_nchain + 1);
+    int64_t* d_pcap = d_cells + (h_nchain + 1);
+    int64_t* d_rect_off = d_pcap + (h_nchain + 1);
+    int64_t* d_path_off = d_rect_off + (h_nchain + 1);
+    int64_t* d_dpcells = d_path_off + (h_nchain + 1);
+    int64_t* d_ncig = d_dpcells + (h_nchain + 1);
+    int64_t h_cells = 0, h_pathtot = 0;
+    if (h_nchain > 0) {
+        k_dp_prep<<<nblk(h_nchain, 256), 256, 0, st>>>(ix, d_seeds, d_cidx_off, d_clen, d_cread, d_cidx, d_off, h_nchain,
+                                                       d_ts, d_te, d_cells, d_pcap, d_dpcells);
+        CK(cudaGetLastError());
+        // total reference cells for the stats
+        size_t tb = 0;
+        CK(cub::DeviceReduce::Sum(nullptr, tb, d_dpcells, d_ncig, h_nchain, st));
+        CK(misc.ensure(tb));
+        CK(cub::DeviceReduce::Sum(misc.p, tb, d_dpcells, d_ncig, h_nchain, st));
+        CK(cudaMemcpyAsync(&S.dp_cells, d_ncig, 8, cudaMemcpyDeviceToHost, st));
+    }
+    CK(offsets(ctx, d_cells, h_nchain, d_rect_off, misc, &h_cells));
+    CK(offsets(ctx, d_pcap, h_nchain, d_path_off, misc, &h_pathtot));
+    CK(ctx->scratch.ensure((h_cells + 1) * 3 * sizeof(int32_t) + (h_nidx + 1) * 2 * sizeof(int32_t) + 64));
+    const int64_t P16 = ((h_pathtot + 1 + 15) / 16) * 16;
+    CK(ctx->path.ensure(2 * P16 + (h_nchain + 1) * 4 + 64));
+    CK(ctx->alnbuf.ensure((h_nchain + 1) * sizeof(msg_aln)));
+    int32_t* d_rect = ctx->scratch.as<int32_t>();
+    int32_t* d_aux = d_rect + (h_cells + 1) * 3;
+    uint8_t* d_path = ctx->path.as<uint8_t>();
+    uint8_t* d_qbuf = d_path + P16;
+    int32_t* d_plen = reinterpret_cast<int32_t*>(d_path + 2 * P16);
+    msg_aln* d_aln = ctx->alnbuf.as<msg_aln>();
+    if (h_nchain > 0) {
+        DpArgs da{};
+        da.ix = ix; da.seeds = d_seeds; da.chain_idx_off = d_cidx_off; da.chain_len = d_clen; da.chain_read = d_cread;
+        da.chain_idx = d_cidx; da.n_chain = h_nchain; da.rseq = d_seq; da.roff = d_off; da.t_start = d_ts;
+        da.t_end = d_te; da.rect_off = d_rect_off; da.rect = d_rect; da.aux = d_aux; da.qbuf = d_qbuf;
+        da.path_off = d_path_off; da.path = d_path; da.path_len = d_plen; da.aln = d_aln; da.pp = dpp;
+        da.status = d_status;
+        k_dp<<<nblk(h_nchain * 32, 128), 128, 0, st>>>(da);
+        CK(cudaGetLastError());
+    }
+    tm.mark();  // 4
+    int64_t h_ncig = 0;
+    if (h_nchain > 0) {
+        k_cigar<<<nblk(h_nchain, 256), 256, 0, st>>>(h_nchain, d_aln, d_off, d_path_off, d_plen, d_path, 0, d_ncig,
+                                                     nullptr, nullptr);
+        CK(cudaGetLastError());
+    }
+    int64_t* d_cig_off = d_cells;  // reuse: cells no longer needed after the scan
+    CK(offsets(ctx, d_ncig, h_nchain, d_cig_off, misc, &h_ncig));
+    CK(ctx->cigbuf.ensure((h_ncig + 1) * 4));
+    if (h_nchain > 0) {
+        k_cigar<<<nblk(h_nchain, 256), 256, 0, st>>>(h_nchain, d_aln, d_off, d_path_off, d_plen, d_path, 1, nullptr,
+                                                     d_cig_off, ctx->cigbuf.as<uint32_t>());
+        k_aln_cig<<<nblk(h_nchain, 256), 256, 0, st>>>(d_aln, d_cig_off, h_nchain);
+        CK(cudaGetLastError());
+    }
+    tm.mark();  // 5
+    uint32_t h_status = 0;
+    CK(cudaMemcpyAsync(&h_status, d_status, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (h_status & kErrInternal) return ctx->fail(MSG_EINTERNAL, "device consistency check failed");
+    S.n_aln = h_nchain;
+    S.ms_smem = tm.ms(0, 1);
+    S.ms_locate = tm.ms(1, 2);
+    S.ms_chain = tm.ms(2, 3);
+    S.ms_dp = tm.ms(3, 5);
+
+    // ---------------- results ----------------
+    out->n_aln = h_nchain;
+    out->n_cigar = h_ncig;
+    if (h_nchain > out->aln_cap || h_ncig > out->cigar_cap) return ctx->fail(MSG_EINVAL, "output capacity too small");
+    if (h_nchain > 0) {
+        CK(cudaMemcpyAsync(out->aln, d_aln, h_nchain * sizeof(msg_aln), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(out->cigar, ctx->cigbuf.p, h_ncig * 4, cudaMemcpyDeviceToHost, st));
+    }
+    if (out->read_aln_off) CK(cudaMemcpyAsync(out->read_aln_off, d_chain_off, (n_reads + 1) * 8, cudaMemcpyDeviceToHost, st));
+    if (dump) {
+        dump->n_smem = h_nsmem;
+        if (dump->smem && h_nsmem <= dump->smem_cap)
+            CK(cudaMemcpyAsync(dump->smem, d_smem, h_nsmem * 48, cudaMemcpyDeviceToHost, st));
+        if (dump->smem_off) CK(cudaMemcpyAsync(dump->smem_off, d_smem_off, (n_reads + 1) * 8, cudaMemcpyDeviceToHost, st));
+        // dense seeds per read after removeRedundant
+        std::vector<int64_t> rso(n_reads + 1);
+        std::vector<int32_t> nd(n_reads);
+        CK(cudaMemcpyAsync(rso.data(), d_read_seed_off, (n_reads + 1) * 8, cudaMemcpyDeviceToHost, st));
+        if (n_reads > 0) CK(cudaMemcpyAsync(nd.data(), d_ndedup, n_reads * 4, cudaMemcpyDeviceToHost, st));
+        std::vector<Seed> hs(h_nseed_raw);
+        if (h_nseed_raw > 0) CK(cudaMemcpyAsync(hs.data(), d_seeds, h_nseed_raw * sizeof(Seed), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        int64_t k = 0;
+        for (int64_t r = 0; r < n_reads; ++r) {
+            if (dump->seed_off) dump->seed_off[r] = k;
+            for (int32_t j = 0; j < nd[r]; ++j, ++k) {
+                if (dump->seed && k < dump->seed_cap) {
+                    const Seed& s = hs[rso[r] + j];
+                    int64_t* o = dump->seed + 6 * k;
+                    o[0] = s.from; o[1] = s.to; o[2] = s.start; o[3] = s.end; o[4] = s.tid; o[5] = s.strand;
+                }
+            }
+        }
+        if (dump->seed_off) dump->seed_off[n_reads] = k;
+        dump->n_seed = k;
+    }
+    CK(cudaStreamSynchronize(st));
+    S.n_seed = h_nseed_raw;
+    S.ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host0).count();
+#undef CK
+    return MSG_OK;
+}
+
+extern "C" int msg_map_batch_device(msg_ctx* ctx, const msg_read_batch* reads, const msg_map_params* params,
+                                    msg_aln_out* out, msg_stage_dump* dump) {
+    if (!ctx || !reads || !params || !out) return MSG_EINVAL;
+    if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
+    if (reads->n_reads < 0 || (reads->n_reads > 0 && (!reads->seq || !reads->off))) return MSG_EINVAL;
+    if (reads->n_reads > INT32_MAX) return MSG_EINVAL;
+    return map_impl(ctx, reads->seq, reads->off, reads->n_reads, params, out, dump);
+}
+
+extern "C" int msg_map_batch(msg_ctx* ctx, const msg_read_batch* reads, const msg_map_params* params,
+                             msg_aln_out* out, msg_stage_dump* dump) {
+    if (!ctx || !reads || !params || !out) return MSG_EINVAL;
+    if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
+    const int64_t n = reads->n_reads;
+    if (n < 0 || (n > 0 && (!reads->seq || !reads->off))) return MSG_EINVAL;
+    if (n > INT32_MAX) return MSG_EINVAL;
+    for (int64_t i = 0; i < n; ++i)
+        if (reads->off[i + 1] < reads->off[i]) return MSG_EINVAL;
+    const int64_t bytes = n > 0 ? reads->off[n] - reads->off[0] : 0;
+    cudaError_t e = ctx->reads.ensure(bytes + 16);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    e = ctx->offs.ensure((n + 1) * 8);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    std::vector<int64_t> off0(n + 1);
+    for (int64_t i = 0; i <= n; ++i) off0[i] = n > 0 ? reads->off[i] - reads->off[0] : 0;
+    if (bytes > 0) {
+        e = cudaMemcpyAsync(ctx->reads.p, reads->seq + reads->off[0], bytes, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return ctx->cuda_fail(e);
+    }
+    e = cudaMemcpyAsync(ctx->offs.p, off0.data(), (n + 1) * 8, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    return map_impl(ctx, ctx->reads.as<uint8_t>(), ctx->offs.as<int64_t>(), n, params, out, dump);
+}
+
+extern "C" int msg_last_stats(const msg_ctx* ctx, msg_map_stats* stats) {
+    if (!ctx || !stats) return MSG_EINVAL;
+    *stats = ctx->stats;
+    return MSG_OK;
+}

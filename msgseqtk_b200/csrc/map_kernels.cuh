@@ -1,0 +1,935 @@
+// Device kernels of the mapping pipeline (included by map.cu only).
+#pragma once
+#include <cstdint>
+
+#include "../../include/msg_b200.h"
+#include "msg_internal.cuh"
+
+namespace msg {
+
+constexpr int32_t NEG = -(1 << 30);  // the reference's -inf; absorbing under sat_add / add_s
+enum { FWD = 1, REV = 2 };
+enum { OP_M = 0, OP_I = 1, OP_D = 2, OP_S = 4 };
+
+struct Seed {
+    int32_t from, to, tid, strand;
+    int64_t start, end;
+};
+static_assert(sizeof(Seed) == 32, "seed layout");
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
+
+// ======================================================================
+// SMEM stage: one warp per read, lanes over the `prev` candidate list.
+// ======================================================================
+
+struct SmemArgs {
+    const uint8_t* seq;
+    const int64_t* off;
+    int64_t n_reads;
+    int64_t min_len;
+    double thr;        // largest log-likelihood whose e-value passes (host-computed)
+    int thr_all;       // 1 when max_evalue is +inf: every SMEM passes
+    double llk[16];
+    int64_t* out;      // 6 x int64 rows; read r's slot starts at row r * cap
+    int64_t cap;
+    int32_t* count;    // per read: SMEMs emitted (may exceed cap)
+    int32_t* pv_pos;   // per-warp prev lists, pv_cap entries each
+    int64_t* pv_p;
+    int64_t* pv_q;
+    int64_t* pv_s;
+    double* pv_lp;
+    int64_t pv_cap;
+    unsigned long long* work;
+    unsigned long long* n_ext;
+    uint32_t* status;
+};
+
+struct SmemState {
+    int64_t from, to, p, q, s;
+    double lp;
+};
+
+struct WarpSmem {
+    const SmemArgs* a;
+    const IndexDev* ix;
+    const uint8_t* rd;
+    int64_t L;
+    int64_t* out;
+    int32_t n_out;
+    int32_t* pv_pos;
+    int64_t *pv_p, *pv_q, *pv_s;
+    double* pv_lp;
+    unsigned long long ext;
+
+    __device__ int base(int64_t i) const { return (i >= 0 && i < L) ? (int)__ldg(rd + i) : 0; }
+
+    __device__ void emit(bool cand, int64_t from, int64_t to, int64_t p, int64_t q, int64_t s, double lp) {
+        const unsigned m = __ballot_sync(0xffffffffu, cand);
+        if (cand) {
+            const int64_t k = n_out + __popc(m & lanemask_lt());
+            if (k < a->cap) {
+                int64_t* o = out + 6 * k;
+                o[0] = from; o[1] = to; o[2] = p; o[3] = q; o[4] = s;
+                o[5] = __double_as_longlong(lp);
+            }
+        }
+        n_out += __popc(m);
+    }
+
+    __device__ void reverse_prev(int n) {
+        for (int k = lane_id(); k < n / 2; k += 32) {
+            const int o = n - 1 - k;
+            int32_t t0 = pv_pos[k]; pv_pos[k] = pv_pos[o]; pv_pos[o] = t0;
+            int64_t t1 = pv_p[k]; pv_p[k] = pv_p[o]; pv_p[o] = t1;
+            int64_t t2 = pv_q[k]; pv_q[k] = pv_q[o]; pv_q[o] = t2;
+            int64_t t3 = pv_s[k]; pv_s[k] = pv_s[o]; pv_s[o] = t3;
+            double t4 = pv_lp[k]; pv_lp[k] = pv_lp[o]; pv_lp[o] = t4;
+        }
+        __syncwarp();
+    }
+
+    // One lockstep extension of every prev entry. All entries share the outer
+    // end `fixed`; pv_pos holds each entry's other end. dir 0: backward
+    // extension by base b (findFwdBackSMEMS loop, SMEM.cpp:92-115); dir 1:
+    // forward extension (findBackFwdSMEMS loop, SMEM.cpp:147-170). Emits the
+    // SMEMs the reference pushes to `curr` and compacts the survivors.
+    __device__ int step_prev(int n_prev, int dir, int64_t fixed, int b, bool add_ll) {
+        int64_t carry_size = -1;
+        bool found_valid = false;
+        int n_keep = 0;
+        const double llb = a->llk[b & 15];
+        for (int base_k = 0; base_k < n_prev; base_k += 32) {
+            const int k = base_k + lane_id();
+            const bool act = k < n_prev;
+            int32_t pos = 0;
+            int64_t p = 0, q = 0, s = 0, p_old = 0, q_old = 0, s_old = 0;
+            double lp = 0, lp_old = 0;
+            if (act) {
+                pos = pv_pos[k]; p = pv_p[k]; q = pv_q[k]; s = pv_s[k]; lp = pv_lp[k];
+                p_old = p; q_old = q; s_old = s; lp_old = lp;
+                if (is_basic(b)) ext++;
+                if (dir == 0) back_ext(*ix, p, q, s, b); else fwd_ext(*ix, p, q, s, b);
+                if (add_ll) lp = __dadd_rn(lp, llb);
+            }
+            const int64_t up = __shfl_up_sync(0xffffffffu, s, 1);
+            const int64_t sp = lane_id() == 0 ? carry_size : up;
+            const bool valid = act && s >= 1 && (k == 0 || s != sp);
+            if (act && k > 0 && s >= 1 && s < sp) atomicOr(a->status, kErrInternal);  // sizes never decrease along prev
+            const unsigned vb = __ballot_sync(0xffffffffu, valid);
+            const int limit = vb ? __ffs(vb) - 1 : 31;
+            const int64_t e_from = dir == 0 ? fixed : (int64_t)pos;
+            const int64_t e_to = dir == 0 ? (int64_t)pos : fixed;
+            const bool sig = a->thr_all || lp_old <= a->thr;
+            const bool cand = act && !found_valid && lane_id() <= limit && s != s_old && s_old >= 1 &&
+                              (e_to - e_from) >= a->min_len && sig;
+            emit(cand, e_from, e_to, p_old, q_old, s_old, lp_old);
+            if (vb) found_valid = true;
+            __syncwarp();
+            if (valid) {
+                const int w = n_keep + __popc(vb & lanemask_lt());
+                pv_pos[w] = pos; pv_p[w] = p; pv_q[w] = q; pv_s[w] = s; pv_lp[w] = lp;
+            }
+            n_keep += __popc(vb);
+            const int last = min(31, n_prev - 1 - base_k);
+            carry_size = __shfl_sync(0xffffffffu, s, last);
+            __syncwarp();
+        }
+        return n_keep;
+    }
+
+    __device__ void push_prev(int& n, const SmemState& m, int32_t pos) {
+        if (n < a->pv_cap) {
+            pv_pos[n] = pos; pv_p[n] = m.p; pv_q[n] = m.q; pv_s[n] = m.s; pv_lp[n] = m.lp;
+        } else {
+            atomicOr(a->status, kErrInternal);
+        }
+        ++n;
+    }
+
+    __device__ SmemState init_at(int64_t from) const {
+        const int b = base(from);
+        SmemState m;
+        m.from = from; m.to = from + 1;
+        m.p = ix->C[b]; m.q = ix->C[comp16(b)]; m.s = ix->C[b + 1] - ix->C[b];
+        m.lp = __dadd_rn(0.0, a->llk[b]);  // SMEM::evaluate (SMEM.cpp:19-24)
+        return m;
+    }
+
+    // SMEM_LIST::findFwdBackSMEMS (SMEM.cpp:64-117). from/to are in/out.
+    __device__ void fwd_back(int64_t& from, int64_t& to) {
+        const int b = base(from);
+        to = from + 1;
+        if (!is_basic(b)) return;
+        int n_prev = 0;
+        int64_t end_to = 0;
+        if (lane_id() == 0) {
+            SmemState m = init_at(from), m0 = m;
+            while (m.s >= 1) {
+                const int nb = base(m.to);  // getBase(L) is the read's terminator, 0
+                if (is_basic(nb)) ext++;
+                fwd_ext(*ix, m.p, m.q, m.s, nb);
+                if (m.to < L) m.lp = __dadd_rn(m.lp, a->llk[nb]);
+                m.to++;
+                if (m.s != m0.s && m0.to >= a->min_len) {
+                    bool sig = a->thr_all != 0;
+                    if (!sig) {  // SMEM::loglik(0, to) (SMEM.cpp:26-40)
+                        double ll = __dadd_rn(0.0, m0.lp);
+                        for (int64_t i = 0; i < m0.from; ++i) ll = __dadd_rn(ll, a->llk[base(i)]);
+                        sig = ll <= a->thr;
+                    }
+                    if (sig) push_prev(n_prev, m0, (int32_t)m0.to);
+                }
+                m0 = m;
+            }
+            end_to = m.to;
+        }
+        n_prev = __shfl_sync(0xffffffffu, n_prev, 0);
+        to = __shfl_sync(0xffffffffu, end_to, 0);
+        __syncwarp();
+        if (n_prev > a->pv_cap) return;
+        if (n_prev == 0) { from--; return; }
+        reverse_prev(n_prev);
+        while (from >= 0 && n_prev > 0) {
+            const int b2 = from > 0 ? base(from - 1) : 0;
+            n_prev = step_prev(n_prev, 0, from, b2, from > 0);
+            from--;
+        }
+    }
+
+    // SMEM_LIST::findBackFwdSMEMS (SMEM.cpp:119-172). from/to are in/out.
+    __device__ void back_fwd(int64_t& from, int64_t& to) {
+        const int b = base(from);
+        to = from + 1;
+        if (!is_basic(b)) return;
+        int n_prev = 0;
+        int64_t end_from = 0;
+        if (lane_id() == 0) {
+            SmemState m = init_at(from), m0 = m;
+            while (m.s >= 1) {
+                const int nb = m.from > 0 ? base(m.from - 1) : 0;
+                if (is_basic(nb)) ext++;
+                back_ext(*ix, m.p, m.q, m.s, nb);
+                if (m.from > 0) m.lp = __dadd_rn(m.lp, a->llk[nb]);
+                m.from--;
+                if (m.s != m0.s && L - m0.from >= a->min_len) {
+                    bool sig = a->thr_all != 0;
+                    if (!sig) {  // SMEM::loglik(from, L)
+                        double ll = __dadd_rn(0.0, m0.lp);
+                        for (int64_t i = m0.to; i < L; ++i) ll = __dadd_rn(ll, a->llk[base(i)]);
+                        sig = ll <= a->thr;
+                    }
+                    if (sig) push_prev(n_prev, m0, (int32_t)m0.from);
+                }
+                m0 = m;
+            }
+            end_from = m.from;
+        }
+        n_prev = __shfl_sync(0xffffffffu, n_prev, 0);
+        from = __shfl_sync(0xffffffffu, end_from, 0);
+        __syncwarp();
+        if (n_prev > a->pv_cap) return;
+        if (n_prev == 0) { to++; return; }
+        reverse_prev(n_prev);
+        while (to <= L && n_prev > 0) {
+            const int b2 = base(to);
+            n_prev = step_prev(n_prev, 1, to, b2, to < L);
+            to++;
+        }
+    }
+
+    // SMEM_LIST::findAllSMEMS (SMEM.cpp:186-215)
+    __device__ void find_all() {
+        int64_t from = L / 2;
+        int64_t to = from + 1;
+        fwd_back(from, to);
+        while (from > 0 || to < L) {
+            int64_t from0 = to;
+            if (from0 < L) fwd_back(from0, to);
+            from -= 1;
+            int64_t to0 = from + 1;
+            if (from >= 0) back_fwd(from, to0);
+        }
+    }
+};
+
+__global__ void __launch_bounds__(256) k_smem(SmemArgs a, IndexDev ix) {
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    WarpSmem w;
+    w.a = &a;
+    w.ix = &ix;
+    w.pv_pos = a.pv_pos + warp * a.pv_cap;
+    w.pv_p = a.pv_p + warp * a.pv_cap;
+    w.pv_q = a.pv_q + warp * a.pv_cap;
+    w.pv_s = a.pv_s + warp * a.pv_cap;
+    w.pv_lp = a.pv_lp + warp * a.pv_cap;
+    w.ext = 0;
+    for (;;) {
+        unsigned long long r = 0;
+        if (lane_id() == 0) r = atomicAdd(a.work, 1ull);
+        r = __shfl_sync(0xffffffffu, r, 0);
+        if ((int64_t)r >= a.n_reads) break;
+        const int64_t o0 = a.off[r];
+        w.rd = a.seq + o0;
+        w.L = a.off[r + 1] - o0;
+        w.out = a.out + 6 * (int64_t)r * a.cap;
+        w.n_out = 0;
+        if (w.L > 0) w.find_all();
+        if (lane_id() == 0) {
+            a.count[r] = w.n_out;
+            if (w.n_out > a.cap) atomicOr(a.status, kErrOverflow);
+        }
+    }
+    // lanes count their own extensions
+    unsigned long long e = w.ext;
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+    if (lane_id() == 0 && e) atomicAdd(a.n_ext, e);
+}
+
+// Copy each read's SMEMs into a dense array (read r at smem_off[r]).
+__global__ void k_compact_smem(const int64_t* __restrict__ src, int64_t cap, const int32_t* __restrict__ count,
+                               const int64_t* __restrict__ smem_off, int64_t n_reads, int64_t* __restrict__ dst) {
+    const int64_t r = blockIdx.x;
+    if (r >= n_reads) return;
+    const int64_t n = min((int64_t)count[r], cap);
+    for (int64_t j = threadIdx.x; j < 6 * n; j += blockDim.x) dst[6 * smem_off[r] + j] = src[6 * r * cap + j];
+}
+
+// ======================================================================
+// Seed selection: SMEM_LIST::findSeeds locates SMEMs in ascending loglik
+// order and stops after the SMEM that brings the located count to maxNSeed
+// (SMEM.cpp:275-300). Every SMEM contributes exactly `size` seeds
+// (assert at SMEM.cpp:267), so when all but the smallest SMEM hold fewer than
+// maxNSeed seeds the order cannot matter and all are selected. Otherwise the
+// read is flagged for the host, which runs the same std::sort.
+// ======================================================================
+__global__ void k_select(const int64_t* __restrict__ smem, const int64_t* __restrict__ smem_off, int64_t n_reads,
+                         int64_t max_nseed, uint8_t* __restrict__ sel, int32_t* __restrict__ host_flag) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= n_reads) return;
+    const int64_t a = smem_off[r], b = smem_off[r + 1];
+    int64_t tot = 0, mn = INT64_MAX;
+    for (int64_t k = a; k < b; ++k) {
+        const int64_t s = smem[6 * k + 4];
+        tot += s;
+        mn = min(mn, s);
+    }
+    const bool all = (b == a) || (tot - mn < max_nseed);
+    for (int64_t k = a; k < b; ++k) sel[k] = all ? 1 : 0;
+    host_flag[r] = all ? 0 : 1;
+}
+
+__global__ void k_seed_counts(const int64_t* __restrict__ smem, const uint8_t* __restrict__ sel, int64_t n,
+                              int64_t* __restrict__ cnt) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    cnt[k] = sel[k] ? smem[6 * k + 4] : 0;
+}
+
+// ======================================================================
+// Locate: SMEM::getSeeds over the selected SMEMs. One thread per SA-row
+// pair (fwdStart + i, revStart + i); the full suffix array is resident, so
+// accessSA is a single gather. getTid's linear scan over disjoint chromosome
+// spans equals a binary search over their starts.
+// ======================================================================
+__device__ __forceinline__ int64_t chrom_of(const IndexDev& ix, int64_t pos) {
+    int64_t a = 0, b = ix.n_chrom;
+    while (b - a > 1) {
+        const int64_t m = (a + b) >> 1;
+        if (__ldg(ix.bd_start + m) <= pos) a = m; else b = m;
+    }
+    return a;
+}
+
+__global__ void k_locate(IndexDev ix, const int64_t* __restrict__ smem, const int64_t* __restrict__ smem_seed_off,
+                         const int32_t* __restrict__ smem_read, const int64_t* __restrict__ read_off, int64_t n_smem,
+                         int64_t total, int32_t* __restrict__ fill, Seed* __restrict__ seeds,
+                         uint32_t* __restrict__ status) {
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total; g += (int64_t)gridDim.x * blockDim.x) {
+        int64_t a = 0, b = n_smem;  // last k with smem_seed_off[k] <= g
+        while (b - a > 1) {
+            const int64_t m = (a + b) >> 1;
+            if (smem_seed_off[m] <= g) a = m; else b = m;
+        }
+        const int64_t k = a;
+        const int64_t i = g - smem_seed_off[k];
+        const int64_t* m = smem + 6 * k;
+        const int64_t from = m[0], to = m[1], len = to - from;
+        const int32_t r = smem_read[k];
+        const int64_t L = read_off[r + 1] - read_off[r];
+        for (int side = 0; side < 2; ++side) {
+            const int64_t row = (side == 0 ? m[2] : m[3]) + i;
+            const int64_t bd = (int64_t)__ldg(ix.sa + row);
+            const int64_t tid = chrom_of(ix, bd);
+            const int64_t st = ix.bd_start[tid], en = ix.bd_end[tid];
+            const bool fwd = st <= bd && bd < st + (en - st) / 2;
+            if (!fwd) continue;
+            const int64_t loc = bd - st;
+            const int32_t slot = atomicAdd(&fill[k], 1);
+            if (slot >= m[4]) { atomicOr(status, kErrInternal); continue; }
+            Seed s;
+            if (side == 0) { s.from = (int32_t)from; s.to = (int32_t)to; s.strand = FWD; }
+            else { s.from = (int32_t)(L - to); s.to = (int32_t)(L - to + len); s.strand = REV; }
+            s.tid = (int32_t)tid;
+            s.start = loc;
+            s.end = loc + len;
+            seeds[smem_seed_off[k] + slot] = s;
+        }
+    }
+}
+
+// ======================================================================
+// Redundant-seed removal, one warp per read: rank sort by SeedPair's
+// operator< (SeedPair.h:225-232), then a seed is dropped when any later seed
+// contains it or is contained by it (SeedPair::approxEqual, SeedPair.h:171-185).
+// ======================================================================
+__device__ __forceinline__ bool seed_less(const Seed& l, const Seed& r) {
+    if (l.from != r.from) return l.from < r.from;
+    if (l.to != r.to) return l.to < r.to;
+    if (l.tid != r.tid) return l.tid < r.tid;
+    if (l.strand != r.strand) return l.strand < r.strand;
+    if (l.start != r.start) return l.start < r.start;
+    return l.end < r.end;
+}
+__device__ __forceinline__ bool containing(const Seed& l, const Seed& r) {
+    return l.tid == r.tid && l.strand == r.strand && l.from <= r.from && l.to >= r.to && l.start <= r.start &&
+           l.end >= r.end;
+}
+
+__global__ void k_dedup(const int64_t* __restrict__ read_seed_off, int64_t n_reads, const Seed* __restrict__ in,
+                        Seed* __restrict__ tmp, Seed* __restrict__ out, int32_t* __restrict__ n_out) {
+    const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (r >= n_reads) return;
+    const int64_t a = read_seed_off[r];
+    const int64_t n = read_seed_off[r + 1] - a;
+    for (int64_t i = lane_id(); i < n; i += 32) {
+        const Seed si = in[a + i];
+        int64_t rank = 0;
+        for (int64_t j = 0; j < n; ++j) {
+            const Seed sj = in[a + j];
+            if (seed_less(sj, si) || (j < i && !seed_less(si, sj))) rank++;
+        }
+        tmp[a + rank] = si;
+    }
+    __syncwarp();
+    int64_t kept = 0;
+    for (int64_t base = 0; base < n; base += 32) {
+        const int64_t i = base + lane_id();
+        bool keep = false;
+        Seed si;
+        if (i < n) {
+            si = tmp[a + i];
+            keep = true;
+            for (int64_t j = i + 1; j < n; ++j) {
+                const Seed sj = tmp[a + j];
+                if (containing(si, sj) || containing(sj, si)) { keep = false; break; }
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) out[a + kept + __popc(m & lanemask_lt())] = si;
+        kept += __popc(m);
+    }
+    if (lane_id() == 0) n_out[r] = (int32_t)kept;
+}
+
+// ======================================================================
+// Chaining: SeedChain::getChains / dfsSeeds with the recursion on an explicit
+// stack; same visiting order. One thread per read, two passes (count, emit).
+// ======================================================================
+__device__ __forceinline__ int64_t loc_dist(int64_t ls, int64_t le, int64_t rs, int64_t re) {  // Loc.h:89-91
+    const bool ov = ls < re && le > rs;
+    return ov ? 0 : ls < rs ? rs - le + 1 : ls - re + 1;
+}
+
+__device__ __forceinline__ bool chain_ok(const Seed& l, const Seed& r, int64_t max_mm, int64_t max_indel) {
+    // SeedPair::isCompatitable / nMismatch / nIndel (SeedPair.h:136-158)
+    if (!(l.to <= r.from && l.end <= r.start && l.tid == r.tid && l.strand == r.strand)) return false;
+    const int64_t mm = min(loc_dist(l.from, l.to, r.from, r.to), loc_dist(l.start, l.end, r.start, r.end));
+    if (mm > max_mm) return false;
+    int64_t ind = (int64_t)(r.from - l.to) - (r.start - l.end);
+    if (ind < 0) ind = -ind;
+    return ind <= max_indel;
+}
+
+__global__ void k_chain(const int64_t* __restrict__ read_seed_off, const int32_t* __restrict__ n_seed,
+                        const int64_t* __restrict__ read_len, int64_t n_reads, const Seed* __restrict__ seeds,
+                        uint8_t* __restrict__ visited, int32_t* __restrict__ stk_i, int32_t* __restrict__ stk_j,
+                        int pass, int64_t* __restrict__ n_chain, int64_t* __restrict__ n_idx,
+                        const int64_t* __restrict__ chain_off, const int64_t* __restrict__ idx_off,
+                        int64_t* __restrict__ chain_idx_off, int32_t* __restrict__ chain_len,
+                        int32_t* __restrict__ chain_read, int64_t* __restrict__ chain_idx) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= n_reads) return;
+    const int64_t a = read_seed_off[r];
+    const int64_t N = n_seed[r];
+    const int64_t L = read_len[r];
+    // msgseqtk-align.cpp:619-620
+    const int64_t max_mm = (int64_t)ceil(__dmul_rn((double)L, 0.2));
+    const int64_t max_indel = (int64_t)ceil(__dmul_rn((double)L, 0.1));
+    uint8_t* vis = visited + a;
+    int32_t* si = stk_i + a;
+    int32_t* sj = stk_j + a;
+    for (int64_t i = 0; i < N; ++i) vis[i] = 0;
+    int64_t nc = 0, ni = 0;
+    int64_t c_base = pass ? chain_off[r] : 0;
+    int64_t i_base = pass ? idx_off[r] : 0;
+    for (int64_t root = 0; root < N; ++root) {
+        if (vis[root]) continue;
+        vis[root] = 1;
+        int depth = 0;
+        si[0] = (int32_t)root; sj[0] = (int32_t)(root + 1);
+        // leaf flag kept in the sign of stk_j: negative once a child was taken
+        while (depth >= 0) {
+            const int64_t i = si[depth];
+            int64_t j = sj[depth] < 0 ? -(int64_t)sj[depth] - 1 : sj[depth];
+            const bool had_child = sj[depth] < 0;
+            bool descended = false;
+            const Seed s_i = seeds[a + i];
+            while (j < N) {
+                const int64_t jj = j++;
+                if (!vis[jj] && chain_ok(s_i, seeds[a + jj], max_mm, max_indel)) {
+                    sj[depth] = (int32_t)(-(j) - 1);  // resume at j, child taken
+                    vis[jj] = 1;
+                    ++depth;
+                    si[depth] = (int32_t)jj;
+                    sj[depth] = (int32_t)(jj + 1);
+                    descended = true;
+                    break;
+                }
+            }
+            if (descended) continue;
+            if (!had_child) {  // leaf: emit the current stack as a chain
+                if (pass) {
+                    chain_idx_off[c_base + nc] = i_base + ni;
+                    chain_len[c_base + nc] = depth + 1;
+                    chain_read[c_base + nc] = (int32_t)r;
+                    for (int d = 0; d <= depth; ++d) chain_idx[i_base + ni + d] = a + si[d];
+                }
+                nc++;
+                ni += depth + 1;
+            }
+            --depth;
+        }
+    }
+    if (!pass) { n_chain[r] = nc; n_idx[r] = ni; }
+}
+
+// ======================================================================
+// DP. The reference fills three (L+1) x (tLen+1) double matrices with -inf and
+// writes them in a fixed order (Alignment.cpp:54-171): 5' rectangle, then per
+// seed [clear its block, diagonal, the cell past it, I.row(to+1) = M.row(to)+o,
+// D.col(end+1) = M.col(end)+o], the gap rectangle to the next seed, and the 3'
+// rectangle. Rectangles and seed blocks are disjoint, so the final value of
+// any cell is given by the last region in that order that writes it. Only the
+// rectangles are stored (M, I, D per cell); every other cell is derived on
+// demand by `Chain::M/I/D` below. A query made while computing region m only
+// looks at regions written before m, which is exactly the state the reference
+// saw at that point.
+// ======================================================================
+__device__ __forceinline__ int32_t sat_add(int32_t a, int32_t b) {  // a + b for b <= 0, -inf absorbing
+    return a == NEG ? NEG : max(a + b, NEG);
+}
+__device__ __forceinline__ int32_t add_s(int32_t a, int32_t s) { return a == NEG ? NEG : a + s; }
+
+struct DpParams {
+    int32_t match, mismatch, gap_o, gap_e;
+    int32_t mode;  // 0 NW, 1 SW
+};
+
+struct ChainCtx {
+    const Seed* seeds;          // global seeds
+    const int64_t* idx;         // chain's seed indices
+    int32_t n;                  // seeds in the chain
+    int64_t L, T;               // query length, window length
+    int64_t t_start;
+    const uint8_t* query;       // read (FWD) or reverse complement in scratch (REV)
+    const uint8_t* target;      // chromosome + t_start
+    int64_t target_avail;       // chromosome bases available from t_start (beyond: terminator 0)
+    int32_t* rect;              // rectangle storage: [M | I | D] blocks per rectangle
+    int32_t* aux;               // per seed: diag start, rectangle offset of the following gap
+    DpParams pp;
+    int32_t sc_match, sc_mis;
+
+    __device__ int64_t qf(int k) const { return seeds[idx[k]].from; }
+    __device__ int64_t qt(int k) const { return seeds[idx[k]].to; }
+    __device__ int64_t ts(int k) const { return seeds[idx[k]].start - t_start; }
+    __device__ int64_t te(int k) const { return seeds[idx[k]].end - t_start; }
+    __device__ int tb(int64_t t) const { return t < target_avail ? (int)__ldg(target + t) : 0; }
+    // ScoreScheme::getScore (ScoreScheme.cpp:20-24)
+    __device__ int32_t score(int qb, int tbb) const {
+        return ((qb & tbb) && qb != 15 && tbb != 15) ? sc_match : -sc_mis;
+    }
+
+    // row/column boundaries: b[0]=0, b[2k-1]=qf_k, b[2k]=qt_k, b[2n+1]=L
+    __device__ int64_t rb(int m) const {
+        if (m <= 0) return 0;
+        if (m >= 2 * n + 1) return L;
+        const int k = (m + 1) / 2 - 1;
+        return (m & 1) ? qf(k) : qt(k);
+    }
+    __device__ int64_t cb(int m) const {
+        if (m <= 0) return 0;
+        if (m >= 2 * n + 1) return T;
+        const int k = (m + 1) / 2 - 1;
+        return (m & 1) ? ts(k) : te(k);
+    }
+    // segment of matrix row i >= 1: smallest m with i <= b[m+1]
+    __device__ int row_seg(int64_t i) const {
+        int lo = 0, hi = 2 * n;
+        while (lo < hi) { const int mid = (lo + hi) >> 1; if (i <= rb(mid + 1)) hi = mid; else lo = mid + 1; }
+        return lo;
+    }
+    __device__ int col_seg(int64_t j) const {
+        int lo = 0, hi = 2 * n;
+        while (lo < hi) { const int mid = (lo + hi) >> 1; if (j <= cb(mid + 1)) hi = mid; else lo = mid + 1; }
+        return lo;
+    }
+    __device__ int64_t rect_off(int m) const {  // cell offset of rectangle m (even m)
+        return m == 0 ? 0 : (int64_t)aux[2 * (m / 2 - 1) + 1];
+    }
+    __device__ int32_t* rect_ptr(int m, int which, int64_t i, int64_t j) const {
+        const int64_t r0 = rb(m), c0 = cb(m);
+        const int64_t R = rb(m + 1) - r0, Cc = cb(m + 1) - c0;
+        const int64_t area = R * Cc;
+        return rect + rect_off(m) * 3 + which * area + (i - r0 - 1) * Cc + (j - c0 - 1);
+    }
+    __device__ int32_t diag_start(int k) const { return aux[2 * k]; }
+    // seed k (0-based) with qt == v, or -1
+    __device__ int seed_by_qt(int64_t v) const {
+        int lo = 0, hi = n - 1;
+        while (lo <= hi) { const int mid = (lo + hi) >> 1; const int64_t x = qt(mid); if (x == v) return mid; if (x < v) lo = mid + 1; else hi = mid - 1; }
+        return -1;
+    }
+    __device__ int seed_by_te(int64_t v) const {
+        int lo = 0, hi = n - 1;
+        while (lo <= hi) { const int mid = (lo + hi) >> 1; const int64_t x = te(mid); if (x == v) return mid; if (x < v) lo = mid + 1; else hi = mid - 1; }
+        return -1;
+    }
+
+    // Final value of M(i,j) as seen by region `stage` (regions < stage written).
+    __device__ int32_t M(int64_t i, int64_t j, int stage) const {
+        if (i >= 1 && j >= 1) {
+            const int mr = row_seg(i);
+            if (mr == col_seg(j) && mr < stage) {
+                if (!(mr & 1)) return *rect_ptr(mr, 0, i, j);
+                const int k = (mr + 1) / 2 - 1;
+                const int64_t d = i - qf(k) - 1;
+                if (i - qf(k) == j - ts(k)) return diag_start(k) + (int32_t)d * sc_match;
+                return NEG;
+            }
+            const int k = seed_by_qt(i - 1);  // the cell past seed k (Alignment.cpp:157-160)
+            if (k >= 0 && 2 * k + 1 < stage && te(k) + 1 == j) return diag_start(k) + (int32_t)(qt(k) - qf(k)) * sc_match;
+        }
+        if (pp.mode == 0) return i == 0 ? 0 : NEG;
+        return (i == 0 || j == 0) ? 0 : NEG;
+    }
+    __device__ int32_t I(int64_t i, int64_t j, int stage) const {
+        if (i >= 1 && j >= 1) {
+            const int mr = row_seg(i);
+            if (mr == col_seg(j) && mr < stage && !(mr & 1)) return *rect_ptr(mr, 1, i, j);
+        }
+        if (i >= 1) {
+            const int k = seed_by_qt(i - 1);  // I.row(to+1) = M.row(to) + o (Alignment.cpp:161-163)
+            if (k >= 0 && 2 * k + 1 < stage) return sat_add(M(i - 1, j, 2 * k + 2), -(pp.gap_o + pp.gap_e));
+        }
+        if (pp.mode == 0 && j == 0) return i == 0 ? 0 : -(pp.gap_o + pp.gap_e * (int32_t)i);  // initNW
+        return NEG;
+    }
+    __device__ int32_t D(int64_t i, int64_t j, int stage) const {
+        if (i >= 1 && j >= 1) {
+            const int mr = row_seg(i);
+            if (mr == col_seg(j) && mr < stage && !(mr & 1)) return *rect_ptr(mr, 2, i, j);
+        }
+        if (j >= 1) {
+            const int k = seed_by_te(j - 1);  // D.col(end+1) = M.col(end) + o (Alignment.cpp:165-169)
+            if (k >= 0 && 2 * k + 1 < stage) return sat_add(M(i, j - 1, 2 * k + 2), -(pp.gap_o + pp.gap_e));
+        }
+        return NEG;
+    }
+
+    // Warp-cooperative fill of rectangle m (Alignment::calculateScoresNW/SW,
+    // Alignment.cpp:72-133) by anti-diagonals.
+    __device__ void fill_rect(int m) {
+        const int64_t r0 = rb(m), c0 = cb(m);
+        const int64_t R = rb(m + 1) - r0, Cc = cb(m + 1) - c0;
+        if (R <= 0 || Cc <= 0) return;
+        const int32_t o = -(pp.gap_o + pp.gap_e), e = -pp.gap_e;
+        for (int64_t d = 0; d < R + Cc - 1; ++d) {
+            const int64_t rlo = max((int64_t)0, d - (Cc - 1)), rhi = min(R - 1, d);
+            for (int64_t rr = rlo + lane_id(); rr <= rhi; rr += 32) {
+                const int64_t cc = d - rr;
+                const int64_t i = r0 + 1 + rr, j = c0 + 1 + cc;
+                int32_t md, id, dd, mu, iu, ml, dl;
+                if (rr > 0 && cc > 0) { md = *rect_ptr(m, 0, i - 1, j - 1); id = *rect_ptr(m, 1, i - 1, j - 1); dd = *rect_ptr(m, 2, i - 1, j - 1); }
+                else { md = M(i - 1, j - 1, m); id = I(i - 1, j - 1, m); dd = D(i - 1, j - 1, m); }
+                if (rr > 0) { mu = *rect_ptr(m, 0, i - 1, j); iu = *rect_ptr(m, 1, i - 1, j); }
+                else { mu = M(i - 1, j, m); iu = I(i - 1, j, m); }
+                if (cc > 0) { ml = *rect_ptr(m, 0, i, j - 1); dl = *rect_ptr(m, 2, i, j - 1); }
+                else { ml = M(i, j - 1, m); dl = D(i, j - 1, m); }
+                const int s = score(query[i - 1], tb(j - 1));
+                int32_t mv = add_s(max(max(md, dd), id), s);
+                if (pp.mode == 1) mv = max(mv, 0);
+                *rect_ptr(m, 0, i, j) = mv;
+                *rect_ptr(m, 1, i, j) = max(sat_add(mu, o), sat_add(iu, e));
+                *rect_ptr(m, 2, i, j) = max(sat_add(ml, o), sat_add(dl, e));
+            }
+            __syncwarp();
+        }
+    }
+};
+
+struct DpArgs {
+    IndexDev ix;
+    const Seed* seeds;
+    const int64_t* chain_idx_off;
+    const int32_t* chain_len;
+    const int32_t* chain_read;
+    const int64_t* chain_idx;
+    int64_t n_chain;
+    const uint8_t* rseq;
+    const int64_t* roff;
+    const int64_t* t_start;
+    const int64_t* t_end;
+    const int64_t* rect_off;    // per chain, in cells (x3 int32)
+    int32_t* rect;
+    int32_t* aux;               // per chain at 2 * chain_idx_off
+    uint8_t* qbuf;              // reverse-complement query per chain at path_off
+    const int64_t* path_off;    // per chain, capacity L + tLen + 1
+    uint8_t* path;
+    int32_t* path_len;
+    msg_aln* aln;
+    DpParams pp;
+    uint32_t* status;
+};
+
+// Alignment ctor window (Alignment.cpp:46-52): tStart = max(0, (int64)(start - 1.1*from)),
+// tEnd = min(chrLen, (int64)(end + 1.1*(qTo - to))) with chrLen counting the
+// chromosome's terminator (MetaGenome.h:237 over MetaGenome.cpp:208).
+__global__ void k_dp_prep(IndexDev ix, const Seed* __restrict__ seeds, const int64_t* __restrict__ chain_idx_off,
+                          const int32_t* __restrict__ chain_len, const int32_t* __restrict__ chain_read,
+                          const int64_t* __restrict__ chain_idx, const int64_t* __restrict__ roff, int64_t n_chain,
+                          int64_t* __restrict__ t_start, int64_t* __restrict__ t_end, int64_t* __restrict__ cells,
+                          int64_t* __restrict__ pathcap, int64_t* __restrict__ dpcells) {
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= n_chain) return;
+    const int64_t* idx = chain_idx + chain_idx_off[c];
+    const int n = chain_len[c];
+    const Seed f = seeds[idx[0]], l = seeds[idx[n - 1]];
+    const int64_t r = chain_read[c];
+    const int64_t L = roff[r + 1] - roff[r];
+    const int64_t chr_len = ix.chr_len[f.tid] + 1;
+    const double k11 = 1.0 + 0.1;
+    const double ts = __dsub_rn((double)f.start, __dmul_rn(k11, (double)f.from));
+    const double te = __dadd_rn((double)l.end, __dmul_rn(k11, (double)(L - l.to)));
+    const int64_t tS = max((int64_t)0, (int64_t)ts);
+    const int64_t tE = min(chr_len, (int64_t)te);
+    t_start[c] = tS;
+    t_end[c] = tE;
+    const int64_t T = tE - tS;
+    int64_t area = 0, diag = 0;
+    {   // 5' rectangle, gaps, 3' rectangle (Alignment.cpp:54-70)
+        int64_t a0 = f.from, b0 = f.start - tS;
+        if (a0 > 0 && b0 > 0) area += a0 * b0;
+        for (int k = 0; k < n; ++k) {
+            const Seed s = seeds[idx[k]];
+            diag += s.to - s.from;
+            if (k + 1 < n) {
+                const Seed t = seeds[idx[k + 1]];
+                const int64_t R = t.from - s.to, C = t.start - s.end;
+                if (R > 0 && C > 0) area += R * C;
+            }
+        }
+        const int64_t R = L - l.to, C = tE - l.end;
+        if (R > 0 && C > 0) area += R * C;
+    }
+    cells[c] = area;
+    pathcap[c] = L + T + 1;
+    dpcells[c] = area + diag;
+}
+
+__device__ __forceinline__ int match_max(int32_t m, int32_t i, int32_t d) {  // Alignment.h:577-589
+    int32_t mx = m;
+    int s = OP_M;
+    if (i > mx) { mx = d; s = OP_I; }
+    if (d > mx) s = OP_D;
+    return s;
+}
+
+__global__ void __launch_bounds__(128) k_dp(DpArgs a) {
+    const int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (c >= a.n_chain) return;
+    ChainCtx x;
+    x.seeds = a.seeds;
+    x.idx = a.chain_idx + a.chain_idx_off[c];
+    x.n = a.chain_len[c];
+    const int64_t r = a.chain_read[c];
+    x.L = a.roff[r + 1] - a.roff[r];
+    x.t_start = a.t_start[c];
+    x.T = a.t_end[c] - x.t_start;
+    const Seed f = a.seeds[x.idx[0]];
+    const int64_t chr_len = a.ix.chr_len[f.tid];
+    x.target = a.ix.chr_seq + a.ix.chr_off[f.tid] + x.t_start;
+    x.target_avail = chr_len - x.t_start;
+    x.rect = a.rect + a.rect_off[c] * 3;
+    x.aux = a.aux + 2 * a.chain_idx_off[c];
+    x.pp = a.pp;
+    x.sc_match = a.pp.match;
+    x.sc_mis = a.pp.mismatch;
+    const uint8_t* rd = a.rseq + a.roff[r];
+    uint8_t* path = a.path + a.path_off[c];
+    if (f.strand == FWD) {
+        x.query = rd;
+    } else {  // PrimarySeq::revcom
+        uint8_t* qb = a.qbuf + a.path_off[c];
+        for (int64_t i = lane_id(); i < x.L; i += 32) qb[i] = (uint8_t)comp16(rd[x.L - 1 - i]);
+        __syncwarp();
+        x.query = qb;
+    }
+    // rectangle offsets of the gaps and the 3' end: aux[2k+1] = offset of
+    // rectangle 2(k+1) (gap after seed k, or the 3' rectangle for k = n-1)
+    if (lane_id() == 0) {
+        int64_t off = 0;
+        {
+            const int64_t R = x.rb(1) - x.rb(0), C = x.cb(1) - x.cb(0);
+            if (R > 0 && C > 0) off += R * C;
+        }
+        for (int k = 0; k < x.n; ++k) {
+            x.aux[2 * k + 1] = (int32_t)off;
+            const int m = 2 * (k + 1);
+            const int64_t R = x.rb(m + 1) - x.rb(m), C = x.cb(m + 1) - x.cb(m);
+            if (R > 0 && C > 0) off += R * C;
+        }
+    }
+    __syncwarp();
+    // region order: R0 (m=0), then per seed k: S_k (m=2k+1), G_k / R3 (m=2k+2)
+    x.fill_rect(0);
+    for (int k = 0; k < x.n; ++k) {
+        const int m = 2 * k + 1;
+        if (lane_id() == 0) {  // first diagonal cell (Alignment.cpp:146-153): max(M,D,I + s, 0)
+            const int64_t i = x.qf(k), j = x.ts(k);
+            const int32_t mx = max(max(x.M(i, j, m), x.D(i, j, m)), x.I(i, j, m));
+            x.aux[2 * k] = max(add_s(mx, x.sc_match), 0);
+        }
+        __syncwarp();
+        x.fill_rect(m + 1);
+    }
+    const int stage = 2 * x.n + 2;
+    // ---- traceback ----
+    int64_t aln_to = 0, aln_end = 0;
+    int32_t best = NEG;
+    int s0 = OP_M;
+    int32_t flags = 0;
+    if (a.pp.mode == 0) {  // backTraceNW: scan the last row, M before I, first strict max
+        int64_t bkey = INT64_MAX;
+        for (int64_t j = 1 + lane_id(); j <= x.T; j += 32) {
+            const int32_t vm = x.M(x.L, j, stage), vi = x.I(x.L, j, stage);
+            if (vm > best || (vm == best && vm != NEG && 2 * j < bkey)) { best = vm; bkey = 2 * j; }
+            if (vi > best || (vi == best && vi != NEG && 2 * j + 1 < bkey)) { best = vi; bkey = 2 * j + 1; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const int32_t ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int64_t ok = __shfl_xor_sync(0xffffffffu, bkey, o);
+            if (ob > best || (ob == best && ok < bkey)) { best = ob; bkey = ok; }
+        }
+        aln_to = x.L;
+        if (best == NEG) { aln_end = 0; s0 = OP_M; flags |= 1; }
+        else { aln_end = bkey >> 1; s0 = (bkey & 1) ? OP_I : OP_M; }
+    } else {  // backTraceSW: Eigen maxCoeff, first max in column-major order
+        int64_t bkey = 0;  // M(0,0) = 0
+        best = 0;
+        auto consider = [&](int64_t i, int64_t j, int32_t v) {
+            const int64_t key = j * (x.L + 1) + i;
+            if (v > best || (v == best && key < bkey)) { best = v; bkey = key; }
+        };
+        for (int m = 0; m <= 2 * x.n; m += 2) {
+            const int64_t r0 = x.rb(m), c0 = x.cb(m);
+            const int64_t R = x.rb(m + 1) - r0, C = x.cb(m + 1) - c0;
+            if (R <= 0 || C <= 0) continue;
+            for (int64_t t = lane_id(); t < R * C; t += 32) {
+                const int64_t i = r0 + 1 + t / C, j = c0 + 1 + t % C;
+                consider(i, j, *x.rect_ptr(m, 0, i, j));
+            }
+        }
+        for (int k = 0; k < x.n; ++k) {
+            const int64_t len = x.qt(k) - x.qf(k);
+            for (int64_t d = lane_id(); d < len; d += 32) {
+                const int64_t i = x.qf(k) + 1 + d, j = x.ts(k) + 1 + d;
+                consider(i, j, x.M(i, j, stage));
+            }
+            if (lane_id() == 0) {
+                const int64_t i = x.qt(k) + 1, j = x.te(k) + 1;
+                if (i <= x.L && j <= x.T) consider(i, j, x.M(i, j, stage));
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const int32_t ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int64_t ok = __shfl_xor_sync(0xffffffffu, bkey, o);
+            if (ob > best || (ob == best && ok < bkey)) { best = ob; bkey = ok; }
+        }
+        aln_to = bkey % (x.L + 1);
+        aln_end = bkey / (x.L + 1);
+        s0 = OP_M;
+    }
+    if (lane_id() == 0) {
+        const int32_t go = a.pp.gap_o, ge = a.pp.gap_e;
+        int64_t i = aln_to, j = aln_end;
+        int s = s0;
+        int64_t np = 0;
+        const int64_t cap = x.L + x.T + 1;
+        for (;;) {
+            if (a.pp.mode == 0) { if (!(i > 0)) break; }
+            else { if (!(s != OP_M || x.M(i, j, stage) > 0)) break; }
+            const bool ok = (s == OP_M) ? (i >= 1 && j >= 1) : (s == OP_I) ? (i >= 1) : (j >= 1);
+            if (!ok || np >= cap) { flags |= 2; break; }
+            path[np++] = (uint8_t)s;
+            if (s == OP_M) { s = match_max(x.M(i - 1, j - 1, stage), x.I(i - 1, j - 1, stage), x.D(i - 1, j - 1, stage)); i--; j--; }
+            else if (s == OP_I) { s = sat_add(x.M(i - 1, j, stage), -(go + ge)) > sat_add(x.I(i - 1, j, stage), -ge) ? OP_M : OP_I; i--; }
+            else { s = sat_add(x.M(i, j - 1, stage), -(go + ge)) > sat_add(x.D(i, j - 1, stage), -ge) ? OP_M : OP_D; j--; }
+        }
+        a.path_len[c] = (int32_t)np;
+        msg_aln& o = a.aln[c];
+        o.read = r;
+        o.tid = f.tid;
+        o.strand = f.strand;
+        o.t_start = x.t_start;
+        o.t_end = a.t_end[c];
+        o.aln_from = i;
+        o.aln_to = aln_to;
+        o.aln_start = x.t_start + j;
+        o.aln_end = x.t_start + aln_end;
+        o.aln_score = best == NEG ? INT32_MIN : best;
+        o.flags = flags;
+        if (flags & 2) atomicOr(a.status, kErrTrace);
+    }
+}
+
+// CIGAR runs (Alignment::getAlnCigar): 5' clip, the reversed path in runs, 3' clip.
+__global__ void k_cigar(int64_t n_chain, const msg_aln* __restrict__ aln, const int64_t* __restrict__ roff,
+                        const int64_t* __restrict__ path_off, const int32_t* __restrict__ path_len,
+                        const uint8_t* __restrict__ path, int pass, int64_t* __restrict__ n_cig,
+                        const int64_t* __restrict__ cig_off, uint32_t* __restrict__ cig) {
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= n_chain) return;
+    const msg_aln& a = aln[c];
+    const int64_t L = roff[a.read + 1] - roff[a.read];
+    const uint8_t* p = path + path_off[c];
+    const int64_t np = path_len[c];
+    int64_t k = 0;
+    uint32_t* out = pass ? cig + cig_off[c] : nullptr;
+    if (a.aln_from > 0) { if (pass) out[k] = (uint32_t)(a.aln_from << 4 | OP_S); ++k; }
+    if (np > 0) {
+        uint32_t op = p[np - 1], len = 1;
+        for (int64_t t = np - 2; t >= 0; --t) {
+            if (p[t] != op) { if (pass) out[k] = len << 4 | op; ++k; len = 1; }
+            else len++;
+            op = p[t];
+        }
+        if (pass) out[k] = len << 4 | op;
+        ++k;
+    }
+    if (L - a.aln_to > 0) { if (pass) out[k] = (uint32_t)((L - a.aln_to) << 4 | OP_S); ++k; }
+    if (!pass) n_cig[c] = k;
+}
+
+}  // namespace msg

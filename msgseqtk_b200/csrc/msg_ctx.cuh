@@ -1,0 +1,78 @@
+// Context object behind the C ABI: one CUDA stream, the device index image and
+// reusable per-batch device buffers.
+#pragma once
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/msg_b200.h"
+#include "msg_internal.cuh"
+
+namespace msg {
+
+struct IndexImage {
+    bool loaded = false;
+    Bucket* bkt = nullptr;
+    int64_t* dollar_rows = nullptr;
+    uint32_t* sa = nullptr;
+    int64_t* chr_tab = nullptr;
+    uint8_t* chr_seq = nullptr;
+    int64_t B[16] = {0};
+    double llk[16] = {0};
+    int64_t bytes = 0;
+    IndexDev dev{};
+};
+
+// A grow-only device buffer reused across batches.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes + bytes / 4 + 256;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+    void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+};
+
+}  // namespace msg
+
+struct msg_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    msg::IndexImage idx;
+    std::string last_error;
+    msg_map_stats stats{};
+    // batch buffers
+    msg::DevBuf reads, offs, smem, smem_cnt, prev, sel, seedoff, seeds, seeds2, rcount, chains, chainidx, dpinfo,
+        scratch, path, alnbuf, cigbuf, misc, status;
+    cudaEvent_t ev[8];
+
+    int fail(int code, const char* why) {
+        last_error = why;
+        return code;
+    }
+    int cuda_fail(cudaError_t e) {
+        last_error = cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? MSG_ENOMEM : MSG_ECUDA;
+    }
+    void index_free() {
+        if (idx.bkt) cudaFree(idx.bkt);
+        if (idx.dollar_rows) cudaFree(idx.dollar_rows);
+        if (idx.sa) cudaFree(idx.sa);
+        if (idx.chr_tab) cudaFree(idx.chr_tab);
+        if (idx.chr_seq) cudaFree(idx.chr_seq);
+        idx = msg::IndexImage();
+    }
+};

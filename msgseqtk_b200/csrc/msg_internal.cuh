@@ -1,0 +1,145 @@
+// Internal device-side layout and primitives of the sm_100a mapping library.
+//
+// Index image in HBM
+//   * occurrence buckets: 64 B each, 192 BWT symbols per bucket.
+//       word 0: count of '$' before the bucket (bit 31 set when the bucket holds a '$')
+//       words 1-3: counts of A, C, G before the bucket (T is derived)
+//       words 4-15: 192 symbols x 2 bits (A=0, C=1, G=2, T=3; '$' stored as A)
+//     one 64 B load (4 x 128-bit) gives all five counts at any row.
+//   * dollar rows: sorted rows whose BWT symbol is '$' (2 per chromosome).
+//   * full suffix array, uint32 per row (N < 2^32), so locating a row is one
+//     4-byte gather instead of an LF walk.
+//   * chromosome table and forward nt16 target sequences for the DP.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace msg {
+
+constexpr int kBucketSyms = 192;
+
+struct __align__(16) Bucket {
+    uint32_t cnt[4];
+    uint32_t bits[12];
+};
+static_assert(sizeof(Bucket) == 64, "bucket must be one 64 B line");
+
+// nt16 helpers (DNAalphabet.h:37-191)
+__host__ __device__ inline bool is_basic(int b) { return b == 1 || b == 2 || b == 4 || b == 8; }
+__host__ __device__ inline int to_int(int b) {  // $,A,C,G,T -> 0..4 (others 0)
+    return b == 1 ? 1 : b == 2 ? 2 : b == 4 ? 3 : b == 8 ? 4 : 0;
+}
+__host__ __device__ inline int comp16(int b) {
+    // reverse the 4 bits: A<->T, C<->G, IUPAC codes map accordingly, N->N, 0->0
+    return ((b & 1) << 3) | ((b & 2) << 1) | ((b & 4) >> 1) | ((b & 8) >> 3);
+}
+__host__ __device__ inline int encode_int(int j) { return j == 1 ? 1 : j == 2 ? 2 : j == 3 ? 4 : j == 4 ? 8 : 0; }
+
+struct IndexDev {
+    const Bucket* bkt;
+    const int64_t* dollar_rows;
+    int64_t n_dollar;
+    const uint32_t* sa;
+    int64_t n;
+    int64_t C[17];           // FMDIndex::C for nt16 codes 0..16
+    const int64_t* bd_start; // per chromosome
+    const int64_t* bd_end;
+    const int64_t* chr_len;
+    const int64_t* chr_off;
+    const uint8_t* chr_seq;
+    int64_t n_chrom;
+};
+
+struct Occ5 {
+    int64_t c[5];  // $, A, C, G, T in BWT[0 .. i]
+};
+
+// Count of '$' rows in [lo, hi) by binary search in the sorted dollar rows.
+__device__ inline int64_t dollar_between(const IndexDev& ix, int64_t lo, int64_t hi) {
+    int64_t a = 0, b = ix.n_dollar;
+    while (a < b) { int64_t m = (a + b) >> 1; if (ix.dollar_rows[m] < lo) a = m + 1; else b = m; }
+    int64_t s = a;
+    a = s; b = ix.n_dollar;
+    while (a < b) { int64_t m = (a + b) >> 1; if (ix.dollar_rows[m] < hi) a = m + 1; else b = m; }
+    return a - s;
+}
+
+// Occurrences of $,A,C,G,T in BWT[0 .. i] for -1 <= i < n.
+__device__ inline Occ5 occ5(const IndexDev& ix, int64_t i) {
+    Occ5 o;
+    const int64_t j = i + 1;               // exclusive end
+    const int64_t k = j / kBucketSyms;
+    const int r = (int)(j - k * kBucketSyms);
+    const uint4* p = reinterpret_cast<const uint4*>(ix.bkt + k);
+    const uint4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2), w3 = __ldg(p + 3);
+    const uint32_t words[12] = {w1.x, w1.y, w1.z, w1.w, w2.x, w2.y, w2.z, w2.w, w3.x, w3.y, w3.z, w3.w};
+    uint32_t nA = 0, nC = 0, nG = 0;
+#pragma unroll
+    for (int w = 0; w < 12; ++w) {
+        const int lo = w * 16;
+        uint32_t valid;
+        if (r >= lo + 16) valid = 0x55555555u;
+        else if (r <= lo) valid = 0u;
+        else valid = 0x55555555u & ((1u << (2 * (r - lo))) - 1u);
+        const uint32_t x = words[w];
+        const uint32_t hi = x >> 1, lo_ = x;
+        // code 0 (A): both bits clear; 1 (C): lo set hi clear; 2 (G): hi set lo clear
+        nA += __popc(~lo_ & ~hi & valid);
+        nC += __popc(lo_ & ~hi & valid);
+        nG += __popc(~lo_ & hi & valid);
+    }
+    const bool has_dollar = (w0.x >> 31) != 0;
+    int64_t d_in = 0;
+    if (has_dollar && r > 0) d_in = dollar_between(ix, k * kBucketSyms, j);
+    o.c[0] = (int64_t)(w0.x & 0x7fffffffu) + d_in;
+    o.c[1] = (int64_t)w0.y + (int64_t)nA - d_in;
+    o.c[2] = (int64_t)w0.z + nC;
+    o.c[3] = (int64_t)w0.w + nG;
+    o.c[4] = j - o.c[0] - o.c[1] - o.c[2] - o.c[3];
+    return o;
+}
+
+// BWT symbol (nt16) at row i, with its occurrence count in BWT[0 .. i].
+__device__ inline int bwt_at(const IndexDev& ix, int64_t i) {
+    const int64_t k = i / kBucketSyms;
+    const int r = (int)(i - k * kBucketSyms);
+    const uint32_t w = __ldg(&ix.bkt[k].bits[r >> 4]);
+    const int code = (w >> (2 * (r & 15))) & 3;
+    if (code == 0 && (__ldg(&ix.bkt[k].cnt[0]) >> 31) && dollar_between(ix, i, i + 1)) return 0;
+    return encode_int(code + 1);
+}
+
+// FMDIndex::backExt (FMDIndex.cpp:577-610). Returns the new size.
+// n_ext counts extensions that reached the occurrence lookup.
+__device__ inline int64_t back_ext(const IndexDev& ix, int64_t& p, int64_t& q, int64_t& s, int b) {
+    if (!is_basic(b)) return (s = 0);
+    const int c = to_int(b);
+    const Occ5 lo = occ5(ix, p - 1);
+    const Occ5 hi = occ5(ix, p + s - 1);
+    const int64_t O = lo.c[c];
+    int64_t sB[5];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) sB[j] = hi.c[j] - lo.c[j];
+    if (sB[c] <= 0) return (s = sB[c]);
+    if (sB[c] != s) {
+        int64_t qq = q + sB[0];  // qB[4]
+        for (int j = 4; j > c; --j) qq += sB[j];
+        q = qq;
+    }
+    p = ix.C[b] + O;
+    s = sB[c];
+    return s;
+}
+
+__device__ inline int64_t fwd_ext(const IndexDev& ix, int64_t& p, int64_t& q, int64_t& s, int b) {
+    return back_ext(ix, q, p, s, comp16(b));
+}
+
+// Error bits of the device status word.
+enum : uint32_t {
+    kErrInternal = 1u,     // consistency check failed
+    kErrOverflow = 2u,     // an output capacity was exceeded (host retries)
+    kErrTrace = 4u,        // traceback left the matrix (reference would read out of bounds)
+};
+
+}  // namespace msg

@@ -53,12 +53,12 @@ def suffix_array(text: np.ndarray, device: str | torch.device = "cpu") -> torch.
     n = int(text.shape[0])
     dev = torch.device(device)
     sym = torch.from_numpy(text.astype(np.int64)).to(dev)
-    code = torch.zeros(n + 21, dtype=torch.int64, device=dev)
     # 0 = past the end, 1 + distinct symbol index otherwise
     uniq = torch.unique(sym)
-    code[:n] = torch.searchsorted(uniq, sym) + 1
     bits = max(1, int(uniq.numel()).bit_length())
-    k = min(63 // bits, 64)
+    k = 63 // bits
+    code = torch.zeros(n + k, dtype=torch.int64, device=dev)
+    code[:n] = torch.searchsorted(uniq, sym) + 1
     key = torch.zeros(n, dtype=torch.int64, device=dev)
     for j in range(k):
         key = (key << bits) | code[j:j + n]

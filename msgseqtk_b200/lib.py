@@ -1,0 +1,278 @@
+"""ctypes binding of the C ABI in include/msg_b200.h (libmsg_b200.so).
+
+The shared library is built in-tree by msgseqtk_b200/csrc/Makefile; there is
+no CPU fallback -- loading fails loudly when the library or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmsg_b200.so")
+
+MSG_OK, MSG_EINVAL, MSG_ENOMEM, MSG_EUNSUPPORTED, MSG_ETIMEOUT, MSG_ECUDA, MSG_ESTATE, MSG_EINTERNAL = range(8)
+
+i64p = C.POINTER(C.c_int64)
+u8p = C.POINTER(C.c_uint8)
+
+ALN_DTYPE = np.dtype([("read", "<i8"), ("tid", "<i4"), ("strand", "<i4"), ("t_start", "<i8"), ("t_end", "<i8"),
+                      ("aln_from", "<i8"), ("aln_to", "<i8"), ("aln_start", "<i8"), ("aln_end", "<i8"),
+                      ("aln_score", "<i4"), ("flags", "<i4"), ("cigar_off", "<i8"), ("n_cigar", "<i4"),
+                      ("pad", "<i4")])
+assert ALN_DTYPE.itemsize == 88
+
+# symbols of the C ABI, in include/msg_b200.h order
+EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy", "msg_index_load", "msg_index_bytes",
+           "msg_map_params_default", "msg_map_batch", "msg_map_batch_device", "msg_last_stats", "msg_occ_query",
+           "msg_bi_ext_query", "msg_sa_query"]
+
+
+class FmdView(C.Structure):
+    _fields_ = [("n", C.c_int64), ("bwt", u8p), ("base_count", i64p), ("n_samples", C.c_int64),
+                ("sample_rows", i64p), ("sample_vals", i64p)]
+
+
+class MtgView(C.Structure):
+    _fields_ = [("n_chrom", C.c_int64), ("bd_start", i64p), ("bd_end", i64p), ("chr_len", i64p), ("chr_seq", u8p),
+                ("chr_off", i64p)]
+
+
+class MapParams(C.Structure):
+    _fields_ = [("min_len", C.c_int64), ("max_evalue", C.c_double), ("max_nseed", C.c_int64), ("mode", C.c_int32),
+                ("match", C.c_double), ("mismatch", C.c_double), ("gap_open", C.c_double), ("gap_ext", C.c_double)]
+
+
+class ReadBatch(C.Structure):
+    _fields_ = [("n_reads", C.c_int64), ("seq", u8p), ("off", i64p)]
+
+
+class AlnOut(C.Structure):
+    _fields_ = [("aln_cap", C.c_int64), ("aln", C.c_void_p), ("cigar_cap", C.c_int64), ("cigar", C.c_void_p),
+                ("n_aln", C.c_int64), ("n_cigar", C.c_int64), ("read_aln_off", i64p)]
+
+
+class StageDump(C.Structure):
+    _fields_ = [("smem_cap", C.c_int64), ("smem", i64p), ("smem_off", i64p), ("seed_cap", C.c_int64),
+                ("seed", i64p), ("seed_off", i64p), ("n_smem", C.c_int64), ("n_seed", C.c_int64)]
+
+
+class MapStats(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("n_reads", "n_smem", "n_seed", "n_chain", "n_aln", "n_ext", "n_sa",
+                                         "dp_cells", "host_sorted")] + \
+               [(n, C.c_double) for n in ("ms_total", "ms_smem", "ms_locate", "ms_chain", "ms_dp")]
+
+
+def build(force: bool = False) -> str:
+    """Compile the CUDA library for sm_100a in-tree (nvcc cross-compiles
+    without a GPU)."""
+    args = ["make", "-s", "-j4", "-C", os.path.join(HERE, "csrc")]
+    if force:
+        subprocess.run(args + ["clean"], check=True)
+    subprocess.run(args, check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"CUDA library {path} is missing; run msgseqtk_b200.lib.build()")
+    L = C.CDLL(path)
+    L.msg_strerror.restype = C.c_char_p
+    L.msg_strerror.argtypes = [C.c_int]
+    L.msg_last_error.restype = C.c_char_p
+    L.msg_last_error.argtypes = [C.c_void_p]
+    L.msg_ctx_create.argtypes = [C.c_int, C.POINTER(C.c_void_p)]
+    L.msg_ctx_destroy.argtypes = [C.c_void_p]
+    L.msg_index_load.argtypes = [C.c_void_p, C.POINTER(FmdView), C.POINTER(MtgView)]
+    L.msg_index_bytes.argtypes = [C.c_void_p, i64p]
+    L.msg_map_params_default.argtypes = [C.POINTER(MapParams)]
+    L.msg_map_params_default.restype = None
+    L.msg_map_batch.argtypes = [C.c_void_p, C.POINTER(ReadBatch), C.POINTER(MapParams), C.POINTER(AlnOut),
+                                C.POINTER(StageDump)]
+    L.msg_map_batch_device.argtypes = L.msg_map_batch.argtypes
+    L.msg_last_stats.argtypes = [C.c_void_p, C.POINTER(MapStats)]
+    L.msg_occ_query.argtypes = [C.c_void_p, C.c_int64, u8p, i64p, i64p]
+    L.msg_bi_ext_query.argtypes = [C.c_void_p, C.c_int64, C.c_int, u8p, i64p, i64p, i64p, i64p]
+    L.msg_sa_query.argtypes = [C.c_void_p, C.c_int64, i64p, i64p]
+    _lib = L
+    return L
+
+
+class MsgError(RuntimeError):
+    def __init__(self, code, detail=""):
+        self.code = code
+        lib = load_library()
+        super().__init__(f"{lib.msg_strerror(code).decode()} ({code}): {detail}")
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def default_params(**kw) -> MapParams:
+    p = MapParams()
+    load_library().msg_map_params_default(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class Context:
+    """One device context: a CUDA stream, a loaded index and batch buffers."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        rc = self.lib.msg_ctx_create(device, C.byref(h))
+        if rc != MSG_OK:
+            raise MsgError(rc, "msg_ctx_create")
+        self.h = h
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.msg_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != MSG_OK:
+            raise MsgError(rc, f"{what}: {self.lib.msg_last_error(self.h).decode()}")
+
+    def load_index(self, view):
+        k = [np.ascontiguousarray(x) for x in (view.bwt, view.B.astype(np.int64), view.sample_rows, view.sample_vals,
+                                               view.bd_start, view.bd_end, view.chr_len, view.chr_seq, view.chr_off)]
+        f = FmdView(view.n, _p(k[0], u8p), _p(k[1], i64p), len(k[2]), _p(k[2], i64p), _p(k[3], i64p))
+        m = MtgView(len(k[4]), _p(k[4], i64p), _p(k[5], i64p), _p(k[6], i64p), _p(k[7], u8p), _p(k[8], i64p))
+        self._check(self.lib.msg_index_load(self.h, C.byref(f), C.byref(m)), "msg_index_load")
+
+    def index_bytes(self) -> int:
+        b = C.c_int64(0)
+        self._check(self.lib.msg_index_bytes(self.h, C.byref(b)), "msg_index_bytes")
+        return b.value
+
+    def occ(self, b, i):
+        b = np.ascontiguousarray(b, dtype=np.uint8)
+        i = np.ascontiguousarray(i, dtype=np.int64)
+        out = np.zeros(len(i), dtype=np.int64)
+        self._check(self.lib.msg_occ_query(self.h, len(i), _p(b, u8p), _p(i, i64p), _p(out, i64p)), "msg_occ_query")
+        return out
+
+    def bi_ext(self, direction, b, p, q, s):
+        b = np.ascontiguousarray(b, dtype=np.uint8)
+        p, q, s = (np.array(x, dtype=np.int64) for x in (p, q, s))
+        ret = np.zeros(len(b), dtype=np.int64)
+        self._check(self.lib.msg_bi_ext_query(self.h, len(b), direction, _p(b, u8p), _p(p, i64p), _p(q, i64p),
+                                              _p(s, i64p), _p(ret, i64p)), "msg_bi_ext_query")
+        return ret, p, q, s
+
+    def sa(self, rows):
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        out = np.zeros(len(rows), dtype=np.int64)
+        self._check(self.lib.msg_sa_query(self.h, len(rows), _p(rows, i64p), _p(out, i64p)), "msg_sa_query")
+        return out
+
+    def map(self, seq, off, params: MapParams | None = None, dump: bool = False, device_ptrs=None,
+            aln_cap: int | None = None, cigar_cap: int | None = None):
+        """Map reads (nt16 codes `seq`, offsets `off`). Returns a dict with the
+        alignment records, CIGAR words and per-read alignment offsets; with
+        dump=True also the SMEM and seed lists."""
+        params = params or default_params()
+        n = len(off) - 1
+        if device_ptrs is None:
+            seq = np.ascontiguousarray(seq, dtype=np.uint8)
+            off = np.ascontiguousarray(off, dtype=np.int64)
+            batch = ReadBatch(n, _p(seq, u8p), _p(off, i64p))
+            fn = self.lib.msg_map_batch
+        else:
+            batch = ReadBatch(n, C.cast(C.c_void_p(device_ptrs[0]), u8p), C.cast(C.c_void_p(device_ptrs[1]), i64p))
+            fn = self.lib.msg_map_batch_device
+        aln_cap = aln_cap or max(16, 4 * n)
+        cigar_cap = cigar_cap or max(64, 16 * aln_cap)
+        while True:
+            aln = np.zeros(aln_cap, dtype=ALN_DTYPE)
+            cig = np.zeros(cigar_cap, dtype=np.uint32)
+            roff = np.zeros(n + 1, dtype=np.int64)
+            out = AlnOut(aln_cap, aln.ctypes.data, cigar_cap, cig.ctypes.data, 0, 0, _p(roff, i64p))
+            d = None
+            if dump:
+                smem_cap = 64 * n + 64
+                seed_cap = 64 * n + 64
+                sm = np.zeros((smem_cap, 6), dtype=np.int64)
+                so = np.zeros(n + 1, dtype=np.int64)
+                sd = np.zeros((seed_cap, 6), dtype=np.int64)
+                sdo = np.zeros(n + 1, dtype=np.int64)
+                d = StageDump(smem_cap, _p(sm, i64p), _p(so, i64p), seed_cap, _p(sd, i64p), _p(sdo, i64p), 0, 0)
+            rc = fn(self.h, C.byref(batch), C.byref(params), C.byref(out), C.byref(d) if d is not None else None)
+            if rc == MSG_EINVAL and (out.n_aln > aln_cap or out.n_cigar > cigar_cap):
+                aln_cap = max(aln_cap, out.n_aln) * 2
+                cigar_cap = max(cigar_cap, out.n_cigar) * 2
+                continue
+            self._check(rc, "msg_map_batch")
+            res = dict(aln=aln[:out.n_aln].copy(), cigar=cig[:out.n_cigar].copy(), read_aln_off=roff)
+            if dump:
+                if d.n_smem > smem_cap or d.n_seed > seed_cap:
+                    raise MsgError(MSG_EINVAL, "dump capacity")
+                res.update(smem=sm[:d.n_smem].copy(), smem_off=so, seed=sd[:d.n_seed].copy(), seed_off=sdo)
+            return res
+
+    def stats(self) -> dict:
+        s = MapStats()
+        self._check(self.lib.msg_last_stats(self.h, C.byref(s)), "msg_last_stats")
+        return {k: getattr(s, k) for k, _ in MapStats._fields_}
+
+
+_ASCII = np.frombuffer(b"$ACMGRSVTWYHKDBN", dtype=np.uint8)
+_COMP = np.array([0, 8, 4, 12, 2, 10, 6, 14, 1, 9, 5, 13, 3, 11, 7, 15], dtype=np.uint8)
+
+
+def md_tag(cigar_words, query: np.ndarray, target_at, aln_from: int, aln_start: int) -> str:
+    """Alignment::getAlnMDTag (Alignment.cpp:305-353) from CIGAR runs: '='/'X'
+    by (query & target) != 0, insertions written as '^' + query bases."""
+    md = []
+    prev = -1
+    ln = 0
+    i, j = aln_from, aln_start
+    for w in cigar_words:
+        op, n = int(w) & 15, int(w) >> 4
+        if op == 4:
+            continue
+        for _ in range(n):
+            if op == 0:
+                qb, tb = int(query[i]), int(target_at(j))
+                o = 7 if (qb & tb) else 8
+            else:
+                o = op
+            if o == 7:
+                i += 1; j += 1; ln += 1
+            elif o == 8:
+                md.append(str(ln)); ln = 0
+                md.append(chr(_ASCII[int(target_at(j))]))
+                i += 1; j += 1
+            elif o == 1:
+                if prev != 1:
+                    md.append(str(ln))
+                ln = 0
+                if o != prev:
+                    md.append("^")
+                md.append(chr(_ASCII[int(query[i])]))
+                i += 1
+            elif o == 2:
+                j += 1
+            prev = o
+    md.append(str(ln))
+    return "".join(md)

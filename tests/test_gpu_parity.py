@@ -1,0 +1,173 @@
+"""Parity of the CUDA path (through the C ABI) with the reference: committed
+fixtures from the reference's own code, and the CPU restatement (oracle) on
+freshly generated inputs. Integer/byte results must be bit-exact."""
+import numpy as np
+import pytest
+
+from msgseqtk_b200 import index_build, lib, synth
+from oracle.bind import Oracle
+
+pytestmark = pytest.mark.gpu
+
+COMP = [0, 8, 4, 12, 2, 10, 6, 14, 1, 9, 5, 13, 3, 11, 7, 15]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = lib.Context(0)
+    yield c
+    c.close()
+
+
+def aln_records(res, i):
+    aln, cig, roff = res["aln"], res["cigar"], res["read_aln_off"]
+    out = []
+    for g in aln[roff[i]:roff[i + 1]]:
+        fields = [int(g["tid"]), int(g["strand"]), int(g["t_start"]), int(g["t_end"]), int(g["aln_from"]),
+                  int(g["aln_to"]), int(g["aln_start"]), int(g["aln_end"]), int(g["aln_score"])]
+        words = [int(x) for x in cig[g["cigar_off"]:g["cigar_off"] + g["n_cigar"]]]
+        out.append((fields, words, int(g["flags"])))
+    return out
+
+
+def md_of(words, read, strand, chrom, aln_from, aln_start):
+    q = read if strand == 1 else synth.revcom(read)
+    return lib.md_tag(words, q, lambda j: chrom[j] if j < len(chrom) else 0, aln_from, aln_start)
+
+
+def compare_with_oracle(res, orc, reads_fn, n_reads, genomes, **ps):
+    for i in range(n_reads):
+        r = reads_fn(i)
+        exp = orc.align_read(r, **ps)
+        got = aln_records(res, i)
+        assert len(got) == len(exp), (i, len(got), len(exp))
+        for (fields, words, flags), e in zip(got, exp):
+            ef = [e["tid"], e["strand"], e["t_start"], e["t_end"], e["aln_from"], e["aln_to"], e["aln_start"],
+                  e["aln_end"], int(e["aln_score"]) if np.isfinite(e["aln_score"]) else -(2 ** 31)]
+            assert fields == ef, (i, fields, ef)
+            assert words == e["cigar"], (i, words, e["cigar"])
+            assert flags == e["flags"], (i, flags, e["flags"])
+            md = md_of(words, r, fields[1], genomes[fields[0]], fields[4], fields[6])
+            assert md == e["md"], (i, md, e["md"])
+
+
+@pytest.mark.parametrize("name", ["uniform", "repeats"])
+def test_occ_ext_sa_match_oracle(ctx, cases, oracle_built, name):
+    c = cases[name]
+    ctx.load_index(c.view)
+    orc = Oracle(c.view)
+    n = c.view.n
+    rng = np.random.default_rng(11)
+    b = rng.choice(np.array([0, 1, 2, 4, 8], dtype=np.uint8), size=4000)
+    i = rng.integers(-1, n + 2, size=4000)
+    got = ctx.occ(b, i)
+    exp = [orc.rank(int(x), int(y)) if 0 <= y < n else -1 for x, y in zip(b, i)]
+    assert np.array_equal(got, np.array(exp))
+    # bi-intervals reached by extending read substrings, then one more step
+    Cc = np.concatenate([[0], np.cumsum(c.view.B)])
+    for direction in (0, 1):
+        P, Q, S, Bs, E = [], [], [], [], []
+        for k in range(400):
+            r = c.read(k % (len(c.read_off) - 1))
+            pos = int(rng.integers(1, len(r) - 1))
+            base = int(r[pos])
+            p, q, s = int(Cc[base]), int(Cc[COMP[base]]), int(Cc[base + 1] - Cc[base])
+            steps = int(rng.integers(0, 25))
+            for t in range(steps + 1):
+                j = pos - 1 - t if direction == 0 else pos + 1 + t
+                nb = int(r[j]) if 0 <= j < len(r) else 0
+                if t == steps or s <= 0:
+                    if rng.random() < 0.2:
+                        nb = int(rng.choice([0, 1, 2, 4, 8, 15]))
+                    P.append(p); Q.append(q); S.append(s); Bs.append(nb)
+                    E.append((orc.back_ext if direction == 0 else orc.fwd_ext)(p, q, s, nb))
+                    break
+                _, p, q, s = (orc.back_ext if direction == 0 else orc.fwd_ext)(p, q, s, nb)
+        ret, p2, q2, s2 = ctx.bi_ext(direction, Bs, P, Q, S)
+        for k, e in enumerate(E):
+            assert (ret[k], p2[k], q2[k], s2[k]) == e, (direction, k, e)
+    # the full suffix array recovered on the device equals a host suffix sort
+    sa_ref = index_build.suffix_array(index_build.bd_text(c.genomes)).numpy()
+    assert np.array_equal(ctx.sa(np.arange(n)), sa_ref)
+
+
+@pytest.mark.parametrize("name", ["uniform", "repeats"])
+def test_mapping_matches_reference_fixtures(ctx, cases, name):
+    c = cases[name]
+    ctx.load_index(c.view)
+    n = len(c.read_off) - 1
+    for k in range(c.n_params):
+        ps = c.params(k)
+        ex = c.expected(k)
+        params = lib.default_params(min_len=ps["min_len"], max_evalue=ps["max_evalue"], max_nseed=ps["max_nseed"],
+                                    mode=ps["mode"])
+        res = ctx.map(c.reads, c.read_off, params, dump=True)
+        assert np.array_equal(res["smem_off"], ex["smem_off"])
+        assert np.array_equal(res["smem"], ex["smem"])
+        assert np.array_equal(res["seed_off"], ex["seed_off"])
+        assert np.array_equal(res["seed"], ex["seed"])
+        assert np.array_equal(res["read_aln_off"], ex["aln_off"])
+        for i in range(n):
+            got = aln_records(res, i)
+            rows = ex["aln"][ex["aln_off"][i]:ex["aln_off"][i + 1]]
+            for (fields, words, flags), row, j in zip(got, rows, range(ex["aln_off"][i], ex["aln_off"][i + 1])):
+                assert fields == [int(x) for x in row[:9]], (name, k, i)
+                assert words == [int(x) for x in ex["cigar"][row[9]:row[9] + row[10]]], (name, k, i)
+                md = md_of(words, c.read(i), fields[1], c.genomes[fields[0]], fields[4], fields[6])
+                assert md == ex["md"][j], (name, k, i)
+
+
+def test_mapping_matches_oracle_small_workload(ctx, oracle_built):
+    """4 genomes x 200 kbp, 2000 single-end 150 bp reads with the small
+    workload's error model, plus paired-end mates with 5% random pairs."""
+    g = synth.small_genomes(seed=21, n_genomes=4, length=200_000)
+    view = index_build.build_view(g)
+    ctx.load_index(view)
+    orc = Oracle(view)
+    rs = synth.sample_reads(g, 2000, seed=22)
+    res = ctx.map(rs.seqs, rs.offs)
+    compare_with_oracle(res, orc, rs.read, len(rs), g)
+    m1, m2 = synth.sample_pairs(g, 500, seed=23)
+    pe = synth.interleave(m1, m2)
+    res = ctx.map(pe.seqs, pe.offs)
+    compare_with_oracle(res, orc, pe.read, len(pe), g)
+
+
+def test_edge_cases_match_oracle(ctx, oracle_built):
+    """Empty and ragged reads, N bases, reads shorter than the seed length,
+    reads at chromosome ends (window reaching the terminator), random reads,
+    local mode, infinite e-value and a tight maxNSeed."""
+    g = synth.repeat_genomes(seed=31, n_genomes=3, length=12_000)
+    view = index_build.build_view(g)
+    ctx.load_index(view)
+    orc = Oracle(view)
+    rng = np.random.default_rng(32)
+    reads = [np.zeros(0, np.uint8), g[0][:150].copy(), g[1][-150:].copy(), synth.revcom(g[2][:120]),
+             synth.revcom(g[0][-90:]), g[1][500:510].copy(), synth._BASES[rng.integers(0, 4, 150)]]
+    r = g[2][1000:1150].copy(); r[[10, 75, 140]] = 15; reads.append(r)
+    r = g[0][3000:3200].copy(); r[100] = 15; reads.append(r)
+    reads += [g[k][s:s + int(L)].copy() for k, s, L in zip(rng.integers(0, 3, 40), rng.integers(0, 11_000, 40),
+                                                            rng.integers(1, 400, 40)) if s + L <= len(g[k])]
+    seq = np.concatenate(reads).astype(np.uint8)
+    off = np.concatenate([[0], np.cumsum([len(x) for x in reads])]).astype(np.int64)
+    for ps in (dict(min_len=17, max_evalue=0.01, max_nseed=500, mode=0),
+               dict(min_len=5, max_evalue=float("inf"), max_nseed=40, mode=0),
+               dict(min_len=9, max_evalue=0.5, max_nseed=500, mode=1)):
+        res = ctx.map(seq, off, lib.default_params(**ps))
+        compare_with_oracle(res, orc, lambda i: reads[i], len(reads), g, **ps)
+    res = ctx.map(np.zeros(0, np.uint8), np.zeros(1, np.int64))
+    assert len(res["aln"]) == 0
+
+
+def test_unsupported_inputs_fail_loudly(ctx):
+    g = synth.small_genomes(seed=41, n_genomes=1, length=5000)
+    view = index_build.build_view(g)
+    ctx.load_index(view)
+    with pytest.raises(lib.MsgError) as e:
+        ctx.map(g[0][:150], np.array([0, 150]), lib.default_params(match=1.5))
+    assert e.value.code == lib.MSG_EUNSUPPORTED
+    gn = [g[0].copy()]
+    gn[0][100] = 15
+    with pytest.raises(lib.MsgError) as e:
+        ctx.load_index(index_build.build_view(gn))
+    assert e.value.code == lib.MSG_EUNSUPPORTED
