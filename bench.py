@@ -1,0 +1,362 @@
+"""Benchmark of the B200 read-mapping path on the scale workload.
+
+Workload (one GPU): a synthetic metagenome of 200 genomes with log-normal
+lengths (median 3 Mbp, sigma 0.5, ~600 Mbp, per-genome GC uniform 30-70%),
+indexed as MSGseqTK's bidirectional FMD-index (~1.2 G BWT symbols), and 2 M
+read pairs (2 x 150 bp, fragment ~ Normal(400, 50), 1% substitutions, 0.1%
+indels of 1-3 bp, 5% random pairs). Mates are mapped as single reads, as the
+reference's findSeedsPE does. A step maps one batch of reads (default 250 k
+pairs = 500 k reads) end to end: SMEMs -> seed selection -> locate ->
+redundant-seed removal -> chains -> DP + traceback -> CIGAR. Default parameters
+(min seed 17, e-value 0.01, maxNSeed 500, GLOBAL NW, scores 1/3/5/2).
+
+Reported line (rank 0): `value` = reads/s over all ranks with the reads
+already resident in HBM and results left on the device; `e2e` = the same
+through msg_map_batch with pinned host reads in and host alignment records
+out, copies inside the timed region; `roofline` for the dominant kernel;
+`cpu_baseline` = the reference's own mapping path (compiled from its sources)
+on a bounded sample of the same reads with all host threads.
+
+`--impl reference` times that reference CPU path alone (rank 0; other ranks
+exit without work).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "mapped reads/sec/GPU (2x150bp) + DP GCUPS, learned-band vs plain GPU, bit-exact SAM"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+HBM_FALLBACK = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--pairs", type=int, default=2_000_000, help="read pairs per GPU")
+    ap.add_argument("--batch-pairs", type=int, default=250_000)
+    ap.add_argument("--genomes", type=int, default=200)
+    ap.add_argument("--median", type=float, default=3e6)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--validate", type=int, default=2000, help="reads checked against the oracle after timing")
+    return ap.parse_args()
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 9]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_workload(args, rank, device):
+    from msgseqtk_b200 import index_build, synth
+    t0 = time.time()
+    genomes = synth.scale_genomes(seed=args.seed, n_genomes=args.genomes, median=args.median)
+    t1 = time.time()
+    view = index_build.build_view(genomes, device=device)
+    t2 = time.time()
+    m1, m2 = synth.sample_pairs(genomes, args.pairs, seed=1000 + rank)
+    reads = synth.interleave(m1, m2)
+    t3 = time.time()
+    setup = {"genome_s": round(t1 - t0, 1), "index_s": round(t2 - t1, 1), "reads_s": round(t3 - t2, 1)}
+    return genomes, view, reads, setup
+
+
+def cpu_baseline(genomes, view, reads, target_s, impl_line=False):
+    """The reference's mapping path (oracle/_ref, compiled from its sources)
+    on a bounded sample of the reads, all host threads."""
+    from oracle.bind import REF_SO, Reference
+    if not os.path.exists(REF_SO):
+        return None
+    t0 = time.time()
+    ref = Reference(genomes, view=view)
+    build_s = time.time() - t0
+    threads = ref.lib.ref_max_threads()
+    n_cal = min(len(reads), 200 * threads)
+    _, _, sec = ref.map_batch(reads.seqs[:reads.offs[n_cal]], reads.quals[:reads.offs[n_cal]],
+                              reads.offs[:n_cal + 1], n_threads=threads)
+    rate = n_cal / max(sec, 1e-9)
+    n = int(min(len(reads), max(n_cal, rate * target_s)))
+    a, b = reads.offs[0], reads.offs[n]
+    mapped, n_aln, sec = ref.map_batch(reads.seqs[a:b], reads.quals[a:b], reads.offs[:n + 1] - a, n_threads=threads)
+    return {"value": n / sec, "unit": "reads/s", "cores": threads, "kind": "reference",
+            "sample": f"first {n} reads of the workload (of {len(reads)}), reference findSeeds->getChains->"
+                      f"buildAlignments->filter->evaluate->calcMapQ->sort per read, OpenMP {threads} threads",
+            "seconds": round(sec, 2), "mapped_reads": int(mapped), "index_build_s": round(build_s, 1)}, ref
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import torch
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    genomes, view, reads, setup = make_workload(args, rank, dev)
+    from oracle.bind import REF_SO, Reference
+    if not os.path.exists(REF_SO):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmsgref.so was not built"}))
+        return
+    ref = Reference(genomes, view=view)
+    threads = ref.lib.ref_max_threads()
+    n_cal = min(len(reads), 200 * threads)
+    _, _, sec = ref.map_batch(reads.seqs[:reads.offs[n_cal]], reads.quals[:reads.offs[n_cal]],
+                              reads.offs[:n_cal + 1], n_threads=threads)
+    rate = n_cal / max(sec, 1e-9)
+    per_step = int(min(len(reads) // max(1, args.steps + args.warmup), max(1000, rate * args.cpu_seconds / 2)))
+    times = []
+    for s in range(args.warmup + args.steps):
+        a_r = (s * per_step) % max(1, len(reads) - per_step)
+        a, b = reads.offs[a_r], reads.offs[a_r + per_step]
+        _, _, sec = ref.map_batch(reads.seqs[a:b], reads.quals[a:b], reads.offs[a_r:a_r + per_step + 1] - a,
+                                  n_threads=threads)
+        if s >= args.warmup:
+            times.append(sec)
+    total = sum(times)
+    value = per_step * len(times) / total
+    line = {"metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * total / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "scale: 200 genomes ~600 Mbp (log-normal, GC 30-70%), 2x150 bp pairs, "
+                                   "insert N(400,50), 1% sub, 0.1% indel, 5% random pairs",
+                       "reads_per_step": per_step, "bd_symbols": view.n, "parallelism": f"omp{threads}"},
+            "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads, "kind": "reference",
+                             "sample": f"{per_step} reads per step from the workload"},
+            "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "setup": setup}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+    import torch
+    import torch.distributed as dist
+    from msgseqtk_b200 import lib
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://")
+    genomes, view, reads, setup = make_workload(args, rank, f"cuda:{local}")
+    torch.cuda.empty_cache()
+    ctx = lib.Context(local)
+    t0 = time.time()
+    ctx.load_index(view)
+    setup["load_s"] = round(time.time() - t0, 1)
+    setup["index_gb"] = round(ctx.index_bytes() / 1e9, 2)
+    params = lib.default_params()
+
+    # batches: reads resident on the device, and pinned host copies for e2e
+    bp = 2 * args.batch_pairs
+    n_batches = max(1, len(reads) // bp)
+    d_seq = torch.from_numpy(reads.seqs).cuda()
+    offs_d = []
+    for k in range(n_batches):
+        o = reads.offs[k * bp:(k + 1) * bp + 1]
+        offs_d.append(torch.from_numpy(o - o[0]).cuda())
+    h_seq = torch.from_numpy(reads.seqs).pin_memory().numpy()
+    h_offs = [torch.from_numpy(reads.offs[k * bp:(k + 1) * bp + 1] - reads.offs[k * bp]).pin_memory().numpy()
+              for k in range(n_batches)]
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+
+    def run_device(k):
+        base = int(reads.offs[k * bp])
+        return ctx.map_device(d_seq.data_ptr() + base, offs_d[k].data_ptr(), len(offs_d[k]) - 1, params)
+
+    for s in range(args.warmup):
+        run_device(s % n_batches)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    agg = {"smem": 0.0, "locate": 0.0, "chain": 0.0, "dp": 0.0, "n_ext": 0, "dp_cells": 0, "n_reads": 0,
+           "n_launch": 0, "n_aln": 0, "host_sorted": 0, "n_sa": 0}
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for s in range(args.steps):
+        run_device((args.warmup + s) % n_batches)
+        st = ctx.stats()
+        agg["smem"] += st["ms_smem"]; agg["locate"] += st["ms_locate"]; agg["chain"] += st["ms_chain"]
+        agg["dp"] += st["ms_dp"]
+        for k in ("n_ext", "dp_cells", "n_reads", "n_launch", "n_aln", "host_sorted", "n_sa"):
+            agg[k] += st[k]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        n_tot = torch.tensor([agg["n_reads"]], device="cuda", dtype=torch.float64)
+        dist.all_reduce(n_tot)
+        total_reads = float(n_tot.item())
+    else:
+        total_reads = float(agg["n_reads"])
+    value = total_reads / (ms / 1000.0)
+
+    # end to end through the public API: pinned host reads in, host records out
+    aln_buf = np.zeros(8 * bp, dtype=lib.ALN_DTYPE)
+    cig_buf = np.zeros(64 * bp, dtype=np.uint32)
+    roff_buf = np.zeros(bp + 1, dtype=np.int64)
+    for s in range(min(args.warmup, 1)):
+        k = s % n_batches
+        ctx.map_into(h_seq[reads.offs[k * bp]:], h_offs[k], aln_buf, cig_buf, roff_buf, params)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    h2d = d2h = 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_reads = 0
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for s in range(args.steps):
+        k = (args.warmup + s) % n_batches
+        a = int(reads.offs[k * bp])
+        seq_view = h_seq[a:int(reads.offs[min(len(reads), (k + 1) * bp)])]
+        na, nc = ctx.map_into(seq_view, h_offs[k], aln_buf, cig_buf, roff_buf, params)
+        h2d += seq_view.nbytes + h_offs[k].nbytes
+        d2h += na * lib.ALN_DTYPE.itemsize + nc * 4 + roff_buf[:len(h_offs[k])].nbytes
+        e2e_reads += len(h_offs[k]) - 1
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+        n_tot = torch.tensor([e2e_reads], device="cuda", dtype=torch.float64)
+        dist.all_reduce(n_tot)
+        e2e_reads = float(n_tot.item())
+    e2e = {"value": e2e_reads / (ms_e2e / 1000.0), "unit": "reads/s", "h2d_bytes_per_step": int(h2d // args.steps),
+           "d2h_bytes_per_step": int(d2h // args.steps)}
+
+    # roofline of the dominant stage
+    peaks = json.load(open(PEAKS)) if os.path.exists(PEAKS) else {}
+    hbm = peaks.get("hbm_gbs")
+    peak_note = "measured" if hbm else "fallback"
+    hbm = hbm or HBM_FALLBACK
+    stage_ms = {k: agg[k] for k in ("smem", "locate", "chain", "dp")}
+    dom = max(stage_ms, key=stage_ms.get)
+    read_bytes = float(reads.offs[min(len(reads), n_batches * bp)]) / n_batches * args.steps
+    smem_bytes = 128.0 * agg["n_ext"] + read_bytes
+    achieved = smem_bytes / (agg["smem"] / 1000.0) / 1e9 if agg["smem"] > 0 else 0.0
+    roofline = {"kernel": "k_smem (SMEM bi-interval extension)", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm, "traffic": None, "peak_source": peak_note,
+                "alg_bytes_per_launch": smem_bytes / args.steps, "dominant_stage": dom,
+                "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()}}
+    gcups = agg["dp_cells"] / (agg["dp"] / 1000.0) / 1e9 if agg["dp"] > 0 else 0.0
+
+    # validation: a sample of the timed reads through the oracle
+    valid = None
+    if rank == 0 and args.validate > 0:
+        from oracle.bind import Oracle
+        orc = Oracle(view)
+        n = min(args.validate, len(reads))
+        res = ctx.map(reads.seqs[:reads.offs[n]], reads.offs[:n + 1], params)
+        bad = 0
+        for i in range(n):
+            exp = orc.align_read(reads.read(i))
+            got = res["aln"][res["read_aln_off"][i]:res["read_aln_off"][i + 1]]
+            if len(exp) != len(got):
+                bad += 1
+                continue
+            for g, e in zip(got, exp):
+                f = [int(g[x]) for x in ("tid", "strand", "t_start", "t_end", "aln_from", "aln_to", "aln_start",
+                                         "aln_end", "aln_score")]
+                ef = [e["tid"], e["strand"], e["t_start"], e["t_end"], e["aln_from"], e["aln_to"], e["aln_start"],
+                      e["aln_end"], int(e["aln_score"])]
+                w = [int(x) for x in res["cigar"][g["cigar_off"]:g["cigar_off"] + g["n_cigar"]]]
+                if f != ef or w != e["cigar"]:
+                    bad += 1
+                    break
+        valid = {"reads": n, "mismatching_reads": bad}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        r = cpu_baseline(genomes, view, reads, args.cpu_seconds)
+        cpu = r[0] if r else None
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+                "config": {"workload": "scale: 200 genomes ~600 Mbp (log-normal, GC 30-70%), 2x150 bp pairs, "
+                                       "insert N(400,50), 1% sub, 0.1% indel, 5% random pairs; mates mapped as "
+                                       "single reads (findSeedsPE)",
+                           "reads_per_step": bp, "pairs_per_gpu": args.pairs, "bd_symbols": view.n,
+                           "l2": "inputs larger than L2 (index %.1f GB, new reads every step)" % setup["index_gb"],
+                           "parallelism": f"dp{world}" if world > 1 else "single GPU"},
+                "gcups": gcups, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+                "gpu_launches": agg["n_launch"], "validation": valid, "setup": setup,
+                "stats": {k: agg[k] for k in ("n_ext", "n_sa", "n_aln", "dp_cells", "host_sorted")}}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -117,7 +117,10 @@ typedef struct msg_aln {
 
 /* Output buffers owned by the caller. The library fills at most *_cap entries
  * and always reports the counts it needed in n_aln / n_cigar; when a count
- * exceeds its capacity the call returns MSG_EINVAL with nothing else valid. */
+ * exceeds its capacity the call returns MSG_EINVAL with nothing else valid.
+ * When aln, cigar and read_aln_off are all NULL the results stay in the
+ * context's device buffers (see msg_result_device) and only the counts are
+ * returned. */
 typedef struct msg_aln_out {
     int64_t aln_cap;
     msg_aln* aln;
@@ -150,6 +153,7 @@ typedef struct msg_map_stats {
     int64_t n_sa;           /* suffix-array rows located */
     int64_t dp_cells;       /* cells of the reference DP cell set (rectangles + seed diagonals) */
     int64_t host_sorted;    /* reads whose SMEM order needed the host std::sort */
+    int64_t n_launch;       /* kernels of this library launched by the call */
     double ms_total, ms_smem, ms_locate, ms_chain, ms_dp;
 } msg_map_stats;
 
@@ -168,6 +172,14 @@ int msg_map_batch_device(msg_ctx* ctx, const msg_read_batch* dev_reads, const ms
                          msg_aln_out* out, msg_stage_dump* dump);
 
 int msg_last_stats(const msg_ctx* ctx, msg_map_stats* stats);
+
+/* Device pointers to the last call's results (valid until the next mapping
+ * call on this context): msg_aln records, CIGAR words, per-read offsets. */
+int msg_result_device(const msg_ctx* ctx, const msg_aln** aln, const uint32_t** cigar, const int64_t** read_aln_off);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or events against the library's. */
+int msg_ctx_stream(const msg_ctx* ctx, void** stream);
 
 /* ---- Single-operation entry points (parity checks of the index layer) ---- */
 

@@ -200,7 +200,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     int64_t* d_idx_off = d_chain_off + (n_reads + 1);
     unsigned long long h_maxlen = 0;
     if (n_reads > 0) {
-        k_read_len<<<nblk(n_reads, 256), 256, 0, st>>>(d_off, n_reads, d_rlen, d_ctr + 2);
+        S.n_launch++, k_read_len<<<nblk(n_reads, 256), 256, 0, st>>>(d_off, n_reads, d_rlen, d_ctr + 2);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(&h_maxlen, d_ctr + 2, 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -236,7 +236,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         CK(cudaMemsetAsync(d_ctr, 0, 16, st));
         CK(cudaMemsetAsync(d_status, 0, 4, st));
         if (n_reads > 0) {
-            k_smem<<<blocks, threads, 0, st>>>(sa, ix);
+            S.n_launch++, k_smem<<<blocks, threads, 0, st>>>(sa, ix);
             CK(cudaGetLastError());
         }
         uint32_t h_status = 0;
@@ -256,7 +256,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         CK(cudaStreamSynchronize(st));
         S.n_ext = (int64_t)e;
     }
-    if (n_reads > 0) k_i32_to_i64<<<nblk(n_reads, 256), 256, 0, st>>>(ctx->smem_cnt.as<int32_t>(), d_cnt64, n_reads);
+    if (n_reads > 0) S.n_launch++, k_i32_to_i64<<<nblk(n_reads, 256), 256, 0, st>>>(ctx->smem_cnt.as<int32_t>(), d_cnt64, n_reads);
     CK(offsets(ctx, d_cnt64, n_reads, d_smem_off, misc, &h_nsmem));
     S.n_smem = h_nsmem;
     CK(ctx->sel.ensure((h_nsmem + 1) * (48 + 1 + 4 + 8 + 8 + 4) + 64));
@@ -267,7 +267,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     int32_t* d_fill = d_smem_read + (h_nsmem + 1);
     uint8_t* d_sel = reinterpret_cast<uint8_t*>(d_fill + (h_nsmem + 1));
     if (n_reads > 0) {
-        k_compact_smem<<<n_reads, 64, 0, st>>>(ctx->smem.as<int64_t>(), cap, ctx->smem_cnt.as<int32_t>(), d_smem_off,
+        S.n_launch++, k_compact_smem<<<n_reads, 64, 0, st>>>(ctx->smem.as<int64_t>(), cap, ctx->smem_cnt.as<int32_t>(), d_smem_off,
                                                n_reads, d_smem);
         CK(cudaGetLastError());
     }
@@ -276,7 +276,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     // ---------------- selection (maxNSeed) ----------------
     int32_t* d_hflag = reinterpret_cast<int32_t*>(d_cnt64);  // reuse scratch (n int32)
     if (n_reads > 0) {
-        k_select<<<nblk(n_reads, 256), 256, 0, st>>>(d_smem, d_smem_off, n_reads, params->max_nseed, d_sel, d_hflag);
+        S.n_launch++, k_select<<<nblk(n_reads, 256), 256, 0, st>>>(d_smem, d_smem_off, n_reads, params->max_nseed, d_sel, d_hflag);
         CK(cudaGetLastError());
         std::vector<int32_t> hflag(n_reads);
         CK(cudaMemcpyAsync(hflag.data(), d_hflag, n_reads * 4, cudaMemcpyDeviceToHost, st));
@@ -316,14 +316,14 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         }
     }
     if (h_nsmem > 0) {
-        k_seed_counts<<<nblk(h_nsmem, 256), 256, 0, st>>>(d_smem, d_sel, h_nsmem, d_smem_seed_cnt);
+        S.n_launch++, k_seed_counts<<<nblk(h_nsmem, 256), 256, 0, st>>>(d_smem, d_sel, h_nsmem, d_smem_seed_cnt);
         CK(cudaGetLastError());
     }
     int64_t h_nseed_raw = 0;
     CK(offsets(ctx, d_smem_seed_cnt, h_nsmem, d_smem_seed_off, misc, &h_nseed_raw));
     if (n_reads > 0) {
-        k_gather_off<<<nblk(n_reads + 1, 256), 256, 0, st>>>(d_smem_off, d_smem_seed_off, n_reads, d_read_seed_off);
-        k_smem_read<<<n_reads, 64, 0, st>>>(d_smem_off, n_reads, d_smem_read);
+        S.n_launch++, k_gather_off<<<nblk(n_reads + 1, 256), 256, 0, st>>>(d_smem_off, d_smem_seed_off, n_reads, d_read_seed_off);
+        S.n_launch++, k_smem_read<<<n_reads, 64, 0, st>>>(d_smem_off, n_reads, d_smem_read);
         CK(cudaGetLastError());
     }
 
@@ -336,7 +336,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     if (h_nseed_raw > 0) {
         CK(cudaMemsetAsync(d_fill, 0, (h_nsmem + 1) * 4, st));
         const int64_t g = std::min<int64_t>(nblk(h_nseed_raw, 256), (int64_t)ctx->num_sms * 32);
-        k_locate<<<g, 256, 0, st>>>(ix, d_smem, d_smem_seed_off, d_smem_read, d_off, h_nsmem, h_nseed_raw, d_fill,
+        S.n_launch++, k_locate<<<g, 256, 0, st>>>(ix, d_smem, d_smem_seed_off, d_smem_read, d_off, h_nsmem, h_nseed_raw, d_fill,
                                     d_seeds, d_status);
         CK(cudaGetLastError());
     }
@@ -345,7 +345,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     // ---------------- redundant-seed removal ----------------
     int32_t* d_ndedup = reinterpret_cast<int32_t*>(d_cnt64);  // n int32 (flags no longer needed)
     if (n_reads > 0) {
-        k_dedup<<<nblk(n_reads * 32, 128), 128, 0, st>>>(d_read_seed_off, n_reads, d_seeds, d_seeds2, d_seeds, d_ndedup);
+        S.n_launch++, k_dedup<<<nblk(n_reads * 32, 128), 128, 0, st>>>(d_read_seed_off, n_reads, d_seeds, d_seeds2, d_seeds, d_ndedup);
         CK(cudaGetLastError());
     }
 
@@ -356,7 +356,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     int32_t* d_stkj = d_stki + (h_nseed_raw + 1);
     int64_t h_nchain = 0, h_nidx = 0;
     if (n_reads > 0) {
-        k_chain<<<nblk(n_reads, 128), 128, 0, st>>>(d_read_seed_off, d_ndedup, d_rlen, n_reads, d_seeds, d_vis, d_stki,
+        S.n_launch++, k_chain<<<nblk(n_reads, 128), 128, 0, st>>>(d_read_seed_off, d_ndedup, d_rlen, n_reads, d_seeds, d_vis, d_stki,
                                                    d_stkj, 0, d_nchain, d_nidx, nullptr, nullptr, nullptr, nullptr,
                                                    nullptr, nullptr);
         CK(cudaGetLastError());
@@ -370,7 +370,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     int32_t* d_clen = reinterpret_cast<int32_t*>(d_cidx + (h_nidx + 1));
     int32_t* d_cread = d_clen + (h_nchain + 1);
     if (n_reads > 0 && h_nchain > 0) {
-        k_chain<<<nblk(n_reads, 128), 128, 0, st>>>(d_read_seed_off, d_ndedup, d_rlen, n_reads, d_seeds, d_vis, d_stki,
+        S.n_launch++, k_chain<<<nblk(n_reads, 128), 128, 0, st>>>(d_read_seed_off, d_ndedup, d_rlen, n_reads, d_seeds, d_vis, d_stki,
                                                    d_stkj, 1, nullptr, nullptr, d_chain_off, d_idx_off, d_cidx_off,
                                                    d_clen, d_cread, d_cidx);
         CK(cudaGetLastError());
@@ -389,7 +389,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     int64_t* d_ncig = d_dpcells + (h_nchain + 1);
     int64_t h_cells = 0, h_pathtot = 0;
     if (h_nchain > 0) {
-        k_dp_prep<<<nblk(h_nchain, 256), 256, 0, st>>>(ix, d_seeds, d_cidx_off, d_clen, d_cread, d_cidx, d_off, h_nchain,
+        S.n_launch++, k_dp_prep<<<nblk(h_nchain, 256), 256, 0, st>>>(ix, d_seeds, d_cidx_off, d_clen, d_cread, d_cidx, d_off, h_nchain,
                                                        d_ts, d_te, d_cells, d_pcap, d_dpcells);
         CK(cudaGetLastError());
         // total reference cells for the stats
@@ -418,13 +418,13 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         da.t_end = d_te; da.rect_off = d_rect_off; da.rect = d_rect; da.aux = d_aux; da.qbuf = d_qbuf;
         da.path_off = d_path_off; da.path = d_path; da.path_len = d_plen; da.aln = d_aln; da.pp = dpp;
         da.status = d_status;
-        k_dp<<<nblk(h_nchain * 32, 128), 128, 0, st>>>(da);
+        S.n_launch++, k_dp<<<nblk(h_nchain * 32, 128), 128, 0, st>>>(da);
         CK(cudaGetLastError());
     }
     tm.mark();  // 4
     int64_t h_ncig = 0;
     if (h_nchain > 0) {
-        k_cigar<<<nblk(h_nchain, 256), 256, 0, st>>>(h_nchain, d_aln, d_off, d_path_off, d_plen, d_path, 0, d_ncig,
+        S.n_launch++, k_cigar<<<nblk(h_nchain, 256), 256, 0, st>>>(h_nchain, d_aln, d_off, d_path_off, d_plen, d_path, 0, d_ncig,
                                                      nullptr, nullptr);
         CK(cudaGetLastError());
     }
@@ -432,9 +432,9 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     CK(offsets(ctx, d_ncig, h_nchain, d_cig_off, misc, &h_ncig));
     CK(ctx->cigbuf.ensure((h_ncig + 1) * 4));
     if (h_nchain > 0) {
-        k_cigar<<<nblk(h_nchain, 256), 256, 0, st>>>(h_nchain, d_aln, d_off, d_path_off, d_plen, d_path, 1, nullptr,
+        S.n_launch++, k_cigar<<<nblk(h_nchain, 256), 256, 0, st>>>(h_nchain, d_aln, d_off, d_path_off, d_plen, d_path, 1, nullptr,
                                                      d_cig_off, ctx->cigbuf.as<uint32_t>());
-        k_aln_cig<<<nblk(h_nchain, 256), 256, 0, st>>>(d_aln, d_cig_off, h_nchain);
+        S.n_launch++, k_aln_cig<<<nblk(h_nchain, 256), 256, 0, st>>>(d_aln, d_cig_off, h_nchain);
         CK(cudaGetLastError());
     }
     tm.mark();  // 5
@@ -451,12 +451,20 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     // ---------------- results ----------------
     out->n_aln = h_nchain;
     out->n_cigar = h_ncig;
-    if (h_nchain > out->aln_cap || h_ncig > out->cigar_cap) return ctx->fail(MSG_EINVAL, "output capacity too small");
-    if (h_nchain > 0) {
-        CK(cudaMemcpyAsync(out->aln, d_aln, h_nchain * sizeof(msg_aln), cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(out->cigar, ctx->cigbuf.p, h_ncig * 4, cudaMemcpyDeviceToHost, st));
+    ctx->res_aln = d_aln;
+    ctx->res_cigar = ctx->cigbuf.as<uint32_t>();
+    ctx->res_off = d_chain_off;
+    const bool on_device = !out->aln && !out->cigar && !out->read_aln_off;
+    if (!on_device) {
+        if (h_nchain > out->aln_cap || h_ncig > out->cigar_cap) return ctx->fail(MSG_EINVAL, "output capacity too small");
+        if (h_nchain > 0) {
+            if (!out->aln || !out->cigar) return ctx->fail(MSG_EINVAL, "null output buffer");
+            CK(cudaMemcpyAsync(out->aln, d_aln, h_nchain * sizeof(msg_aln), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(out->cigar, ctx->cigbuf.p, h_ncig * 4, cudaMemcpyDeviceToHost, st));
+        }
+        if (out->read_aln_off)
+            CK(cudaMemcpyAsync(out->read_aln_off, d_chain_off, (n_reads + 1) * 8, cudaMemcpyDeviceToHost, st));
     }
-    if (out->read_aln_off) CK(cudaMemcpyAsync(out->read_aln_off, d_chain_off, (n_reads + 1) * 8, cudaMemcpyDeviceToHost, st));
     if (dump) {
         dump->n_smem = h_nsmem;
         if (dump->smem && h_nsmem <= dump->smem_cap)
@@ -525,6 +533,21 @@ extern "C" int msg_map_batch(msg_ctx* ctx, const msg_read_batch* reads, const ms
     e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return ctx->cuda_fail(e);
     return map_impl(ctx, ctx->reads.as<uint8_t>(), ctx->offs.as<int64_t>(), n, params, out, dump);
+}
+
+extern "C" int msg_result_device(const msg_ctx* ctx, const msg_aln** aln, const uint32_t** cigar,
+                                 const int64_t** read_aln_off) {
+    if (!ctx) return MSG_EINVAL;
+    if (aln) *aln = ctx->res_aln;
+    if (cigar) *cigar = ctx->res_cigar;
+    if (read_aln_off) *read_aln_off = ctx->res_off;
+    return MSG_OK;
+}
+
+extern "C" int msg_ctx_stream(const msg_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return MSG_EINVAL;
+    *stream = (void*)ctx->stream;
+    return MSG_OK;
 }
 
 extern "C" int msg_last_stats(const msg_ctx* ctx, msg_map_stats* stats) {

@@ -58,6 +58,9 @@ struct msg_ctx {
     msg::DevBuf reads, offs, smem, smem_cnt, prev, sel, seedoff, seeds, seeds2, rcount, chains, chainidx, dpinfo,
         scratch, path, alnbuf, cigbuf, misc, status;
     cudaEvent_t ev[8];
+    const msg_aln* res_aln = nullptr;
+    const uint32_t* res_cigar = nullptr;
+    const int64_t* res_off = nullptr;
 
     int fail(int code, const char* why) {
         last_error = why;

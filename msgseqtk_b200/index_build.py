@@ -36,6 +36,7 @@ class FmdView:
     chr_len: np.ndarray
     chr_seq: np.ndarray      # uint8 forward chromosome sequences, concatenated
     chr_off: np.ndarray      # int64, n_chrom + 1
+    gap_sa: np.ndarray | None = None  # SA values of the B[0] '$'-suffix rows (FMDIndex::gapSA)
 
 
 def bd_text(chroms) -> np.ndarray:
@@ -98,6 +99,7 @@ def build_view(chroms, device: str | torch.device = "cpu") -> FmdView:
     del prev
     rows_t = torch.nonzero((torch.arange(n, device=sa_t.device) % SA_SAMPLE_RATE == 0) | (bwt_t == 0)).flatten()
     vals_t = sa_t[rows_t]
+    gap_sa = sa_t[: 2 * len(chroms)].cpu().numpy().astype(np.int64)
     bwt = bwt_t.cpu().numpy()
     rows = rows_t.cpu().numpy().astype(np.int64)
     vals = vals_t.cpu().numpy().astype(np.int64)
@@ -110,4 +112,5 @@ def build_view(chroms, device: str | torch.device = "cpu") -> FmdView:
     chr_off = np.zeros(len(chroms) + 1, dtype=np.int64)
     np.cumsum(lens, out=chr_off[1:])
     chr_seq = np.concatenate(chroms).astype(np.uint8)
-    return FmdView(n, bwt, B, rows, vals, bd_start.astype(np.int64), bd_end.astype(np.int64), lens, chr_seq, chr_off)
+    return FmdView(n, bwt, B, rows, vals, bd_start.astype(np.int64), bd_end.astype(np.int64), lens, chr_seq, chr_off,
+                   gap_sa)

@@ -28,7 +28,7 @@ assert ALN_DTYPE.itemsize == 88
 # symbols of the C ABI, in include/msg_b200.h order
 EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy", "msg_index_load", "msg_index_bytes",
            "msg_map_params_default", "msg_map_batch", "msg_map_batch_device", "msg_last_stats", "msg_occ_query",
-           "msg_bi_ext_query", "msg_sa_query"]
+           "msg_result_device", "msg_ctx_stream", "msg_bi_ext_query", "msg_sa_query"]
 
 
 class FmdView(C.Structure):
@@ -62,7 +62,7 @@ class StageDump(C.Structure):
 
 class MapStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("n_reads", "n_smem", "n_seed", "n_chain", "n_aln", "n_ext", "n_sa",
-                                         "dp_cells", "host_sorted")] + \
+                                         "dp_cells", "host_sorted", "n_launch")] + \
                [(n, C.c_double) for n in ("ms_total", "ms_smem", "ms_locate", "ms_chain", "ms_dp")]
 
 
@@ -100,6 +100,8 @@ def load_library(path: str = LIB_PATH):
                                 C.POINTER(StageDump)]
     L.msg_map_batch_device.argtypes = L.msg_map_batch.argtypes
     L.msg_last_stats.argtypes = [C.c_void_p, C.POINTER(MapStats)]
+    L.msg_result_device.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+    L.msg_ctx_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     L.msg_occ_query.argtypes = [C.c_void_p, C.c_int64, u8p, i64p, i64p]
     L.msg_bi_ext_query.argtypes = [C.c_void_p, C.c_int64, C.c_int, u8p, i64p, i64p, i64p, i64p]
     L.msg_sa_query.argtypes = [C.c_void_p, C.c_int64, i64p, i64p]
@@ -229,6 +231,32 @@ class Context:
                     raise MsgError(MSG_EINVAL, "dump capacity")
                 res.update(smem=sm[:d.n_smem].copy(), smem_off=so, seed=sd[:d.n_seed].copy(), seed_off=sdo)
             return res
+
+    def stream_handle(self) -> int:
+        h = C.c_void_p()
+        self._check(self.lib.msg_ctx_stream(self.h, C.byref(h)), "msg_ctx_stream")
+        return h.value or 0
+
+    def map_device(self, seq_ptr: int, off_ptr: int, n_reads: int, params: MapParams | None = None):
+        """Map reads already in device memory; results stay on the device.
+        Returns (n_aln, n_cigar)."""
+        params = params or default_params()
+        batch = ReadBatch(n_reads, C.cast(C.c_void_p(seq_ptr), u8p), C.cast(C.c_void_p(off_ptr), i64p))
+        out = AlnOut(0, None, 0, None, 0, 0, None)
+        self._check(self.lib.msg_map_batch_device(self.h, C.byref(batch), C.byref(params), C.byref(out), None),
+                    "msg_map_batch_device")
+        return out.n_aln, out.n_cigar
+
+    def map_into(self, seq: np.ndarray, off: np.ndarray, aln: np.ndarray, cig: np.ndarray, roff: np.ndarray,
+                 params: MapParams | None = None):
+        """Map host reads into caller-owned (e.g. pinned) host buffers.
+        Returns (n_aln, n_cigar)."""
+        params = params or default_params()
+        batch = ReadBatch(len(off) - 1, _p(seq, u8p), _p(off, i64p))
+        out = AlnOut(len(aln), aln.ctypes.data, len(cig), cig.ctypes.data, 0, 0, _p(roff, i64p))
+        self._check(self.lib.msg_map_batch(self.h, C.byref(batch), C.byref(params), C.byref(out), None),
+                    "msg_map_batch")
+        return out.n_aln, out.n_cigar
 
     def stats(self) -> dict:
         s = MapStats()

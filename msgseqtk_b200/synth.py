@@ -58,43 +58,43 @@ def scale_genomes(seed: int = 2, n_genomes: int = 200, median: float = 3e6, sigm
     return [random_genome(rng, int(l), float(g)) for l, g in zip(lens, gcs)]
 
 
-def _mutate(rng, frag: np.ndarray, L: int, sub_rate: float, indel_rate: float) -> np.ndarray:
-    """Apply substitutions and indels (length U{1..3}) to a fragment, return L bases."""
-    out = []
-    i = 0
-    n = len(frag)
-    while len(out) < L and i < n:
-        u = rng.random()
-        if u < indel_rate:
-            k = int(rng.integers(1, 4))
-            if rng.random() < 0.5:  # insertion
-                out.extend(_BASES[rng.integers(0, 4, size=k)].tolist())
-            else:  # deletion
-                i += k
-            continue
-        b = int(frag[i])
-        if rng.random() < sub_rate:
-            choices = [x for x in (A, C, G, T) if x != b]
-            b = choices[int(rng.integers(0, 3))]
-        out.append(b)
-        i += 1
-    while len(out) < L:
-        out.append(int(_BASES[rng.integers(0, 4)]))
-    return np.array(out[:L], dtype=np.uint8)
+def _indel_read(rng, win: np.ndarray, L: int, n_ev: int) -> np.ndarray:
+    """Apply n_ev indels (insertion or deletion of U{1..3} bases, equally
+    likely) at uniform read positions to a substituted window; L bases out."""
+    pos = np.sort(rng.integers(0, L, size=n_ev))
+    parts = []
+    i = 0  # position in the window
+    o = 0  # bases emitted
+    for p in pos:
+        take = max(0, int(p) - o)
+        parts.append(win[i:i + take])
+        i += take
+        o += take
+        k = int(rng.integers(1, 4))
+        if rng.random() < 0.5:
+            parts.append(_BASES[rng.integers(0, 4, size=k)])
+            o += k
+        else:
+            i += k
+    parts.append(win[i:i + max(0, L - o)])
+    out = np.concatenate(parts)[:L]
+    if len(out) < L:
+        out = np.concatenate([out, _BASES[rng.integers(0, 4, size=L - len(out))]])
+    return out
 
 
 def _apply_errors(rng, windows: np.ndarray, L: int, sub_rate: float, indel_rate: float) -> np.ndarray:
-    """Vectorised substitutions on all reads; reads drawing an indel are redone
-    base by base with _mutate."""
-    n = windows.shape[0]
-    reads = windows[:, :L].copy()
-    sub = rng.random((n, L)) < sub_rate
-    shift = rng.integers(1, 4, size=(n, L))
-    idx = np.searchsorted(_BASES, reads)
-    reads = np.where(sub, _BASES[(idx + shift) % 4], reads)
-    has_indel = rng.random(n) < 1.0 - (1.0 - indel_rate) ** L
-    for r in np.nonzero(has_indel)[0]:
-        reads[r] = _mutate(rng, windows[r], L, sub_rate, indel_rate)
+    """Substitutions at sub_rate per base (vectorised over all reads), then
+    Binomial(L, indel_rate) indels per read."""
+    n, W = windows.shape
+    sub = rng.random((n, W)) < sub_rate
+    shift = rng.integers(1, 4, size=(n, W), dtype=np.int8)
+    idx = np.searchsorted(_BASES, windows).astype(np.int8)
+    win = np.where(sub, _BASES[(idx + shift) % 4], windows)
+    reads = win[:, :L].copy()
+    n_ev = rng.binomial(L, indel_rate, size=n)
+    for r in np.nonzero(n_ev)[0]:
+        reads[r] = _indel_read(rng, win[r], L, int(n_ev[r]))
     return reads
 
 

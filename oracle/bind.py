@@ -193,7 +193,10 @@ class Oracle:
 class Reference:
     """The reference's own code path (compiled from its sources)."""
 
-    def __init__(self, chroms, so: str = REF_SO):
+    def __init__(self, chroms, so: str = REF_SO, view=None):
+        """Build the reference DB for `chroms`: with the reference's own
+        FMDIndex constructor (divsufsort), or, when `view` is given, from that
+        decoded view through the reference's WaveletTreeRRR/BitSeqRRR."""
         self.lib = L = C.CDLL(so)
         L.ref_db_build.restype = C.c_void_p
         L.ref_db_build.argtypes = [C.c_int64, u8p, i64p]
@@ -233,7 +236,15 @@ class Reference:
         seqs = np.ascontiguousarray(np.concatenate(chroms).astype(np.uint8))
         offs = np.zeros(len(chroms) + 1, dtype=np.int64)
         np.cumsum([len(c) for c in chroms], out=offs[1:])
-        self.h = L.ref_db_build(len(chroms), _p(seqs, u8p), _p(offs, i64p))
+        L.ref_db_from_view.restype = C.c_void_p
+        L.ref_db_from_view.argtypes = [C.c_int64, u8p, i64p, C.c_int64, u8p, i64p, C.c_int64, i64p, i64p, i64p]
+        if view is None:
+            self.h = L.ref_db_build(len(chroms), _p(seqs, u8p), _p(offs, i64p))
+        else:
+            k = [np.ascontiguousarray(x) for x in (view.bwt, view.B.astype(np.int64), view.sample_rows,
+                                                   view.sample_vals, view.gap_sa)]
+            self.h = L.ref_db_from_view(len(chroms), _p(seqs, u8p), _p(offs, i64p), view.n, _p(k[0], u8p),
+                                        _p(k[1], i64p), len(k[2]), _p(k[2], i64p), _p(k[3], i64p), _p(k[4], i64p))
         self.n = L.ref_db_length(self.h)
 
     def __del__(self):

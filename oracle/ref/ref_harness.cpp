@@ -81,6 +81,43 @@ void* ref_db_build(int64_t n_chrom, const uint8_t* seqs, const int64_t* offs) {
     return db;
 }
 
+/* Same DB, with the FMD-index assembled from an already decoded view (BWT,
+ * base counts, SA samples) by the reference's own structures: the BWT goes
+ * into WaveletTreeRRR(bwt, 0, 15, 32) exactly as the FMDIndex constructor does
+ * (FMDIndex.cpp:66), SAidx into BitSeqRRR(bits, 32) (FMDIndex.cpp:477), and
+ * C[] is accumulated as buildCounts does (FMDIndex.cpp:124-129). Used for
+ * large synthetic DBs where divsufsort on the host would dominate the run;
+ * the view equals what the constructor builds (suffix arrays are unique). */
+void* ref_db_from_view(int64_t n_chrom, const uint8_t* seqs, const int64_t* offs, int64_t n, const uint8_t* bwt,
+                       const int64_t* B16, int64_t n_samples, const int64_t* rows, const int64_t* vals,
+                       const int64_t* gap_sa) {
+    RefDB* db = new RefDB();
+    for (int64_t k = 0; k < n_chrom; ++k) {
+        Genome g("g" + std::to_string(k), "genome" + std::to_string(k));
+        DNAseq s(seqs + offs[k], seqs + offs[k + 1]);
+        g.addChrom("chr" + std::to_string(k), s);
+        db->mtg.addGenome(g);
+    }
+    db->mtg.updateIndex();
+    FMDIndex& f = db->fmd;
+    for (int i = 0; i < 256; ++i) { f.B[i] = 0; f.C[i] = 0; }
+    for (int i = 0; i < 16; ++i) f.B[i] = B16[i];
+    int64_t S = 0;
+    for (int i = 0; i <= 16; ++i) { f.C[i] = S; S += f.B[i]; }
+    {
+        DNAseq b(bwt, bwt + n);
+        f.bwtRRR = WaveletTreeRRR(b, 0, DNAalphabet::NT16_MAX, FMDIndex::RRR_SAMPLE_RATE);
+    }
+    f.gapSA.assign(gap_sa, gap_sa + B16[0]);
+    {
+        BitStr32 bstr(n);
+        for (int64_t k = 0; k < n_samples; ++k) bstr.set(rows[k]);
+        f.SAidx = BitSeqRRR(bstr, FMDIndex::RRR_SAMPLE_RATE);
+    }
+    f.SAsampled.assign(vals, vals + n_samples);
+    return db;
+}
+
 void ref_db_free(void* h) { delete (RefDB*)h; }
 
 int64_t ref_db_length(void* h) { return ((RefDB*)h)->fmd.length(); }
