@@ -181,6 +181,30 @@ int msg_result_device(const msg_ctx* ctx, const msg_aln** aln, const uint32_t** 
  * own work or events against the library's. */
 int msg_ctx_stream(const msg_ctx* ctx, void** stream);
 
+/* ---- Seeding that allocates nothing ----
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc/cudaFree while mapping -- a host application whose GPU memory is
+ * all owned by its own allocator (a framework's caching pool, or a fixed
+ * reservation carved out at start-up), where an extra device allocation would
+ * fail or fragment that budget. It runs the same SMEM search as msg_map_batch
+ * (SMEM_LIST::findAllSMEMS per read, src/SMEM.cpp:186-215) with every input
+ * and output in caller-owned DEVICE memory: reads (d_seq, d_off as in
+ * msg_read_batch), SMEM rows (6 int64 each, as in msg_stage_dump) written to
+ * d_smem at row r * cap_per_read for read r, and per-read counts in d_count.
+ * Its working memory is one static device array of fixed size that every GPU
+ * loading this library holds until exit (about 14 MB with the limits below);
+ * reads longer than MSG_NOALLOC_MAX_READ_LEN are rejected with MSG_EINVAL.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) and caches it; make that first call before any
+ * stream capture on the device. All calls share the array: calls that overlap
+ * on the GPU (two contexts or threads at once) race and must be serialised by
+ * the caller. A count above cap_per_read returns MSG_EINVAL with the needed
+ * counts left in d_count. */
+#define MSG_NOALLOC_MAX_READ_LEN 320
+#define MSG_NOALLOC_WARPS 1184
+int msg_smem_batch_noalloc(msg_ctx* ctx, int64_t n_reads, const uint8_t* d_seq, const int64_t* d_off,
+                           const msg_map_params* params, int64_t* d_smem, int64_t cap_per_read, int32_t* d_count);
+
 /* ---- Single-operation entry points (parity checks of the index layer) ---- */
 
 /* WaveletTreeRRR::rank (src/libsds/src/WaveletTreeRRR.cpp:101-125) through

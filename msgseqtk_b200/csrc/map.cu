@@ -555,3 +555,99 @@ extern "C" int msg_last_stats(const msg_ctx* ctx, msg_map_stats* stats) {
     *stats = ctx->stats;
     return MSG_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Seeding without device allocation. The per-warp candidate lists and the
+// launch counters of k_smem live in one file-scope device array, so this entry
+// point needs no cudaMalloc/cudaFree (nor any allocating library routine).
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int64_t kStaticMaxReadLen = MSG_NOALLOC_MAX_READ_LEN;
+constexpr int64_t kStaticWarps = MSG_NOALLOC_WARPS;
+constexpr int64_t kStaticPvCap = kStaticMaxReadLen + 2;
+constexpr size_t kStaticHdr = 256;  // work counter, extension counter, max read length, status word
+constexpr size_t kStaticBytes = kStaticHdr + (size_t)kStaticWarps * kStaticPvCap * (8 + 8 + 8 + 8 + 4);
+
+__global__ void k_maxlen(const int64_t* __restrict__ off, int64_t n, unsigned long long* __restrict__ mx) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t l = off[i + 1] - off[i];
+    atomicMax(mx, (unsigned long long)(l < 0 ? 0 : l));
+}
+}  // namespace
+
+// Shared by every call on a device: contents persist between calls, so the
+// header is cleared at the start of each call; calls that overlap on the GPU
+// race on it.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kStaticBytes];
+
+// Device address of g_noalloc_scratch per device ordinal. In host code the
+// array's name is only a host-side stand-in, so the address is looked up with
+// cudaGetSymbolAddress on the first call on each device (with that device
+// current) and cached.
+static void* g_noalloc_addr[256] = {nullptr};
+
+extern "C" int msg_smem_batch_noalloc(msg_ctx* ctx, int64_t n_reads, const uint8_t* d_seq, const int64_t* d_off,
+                                      const msg_map_params* params, int64_t* d_smem, int64_t cap_per_read,
+                                      int32_t* d_count) {
+    if (!ctx || !params || n_reads < 0 || cap_per_read < 0) return MSG_EINVAL;
+    if (n_reads > 0 && (!d_seq || !d_off || !d_count || (cap_per_read > 0 && !d_smem))) return MSG_EINVAL;
+    if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
+    DpParams dpp;
+    int rc = check_params(params, &dpp);
+    if (rc != MSG_OK) return ctx->fail(rc, "bad mapping parameters");
+    double thr = 0;
+    int thr_all = 0;
+    rc = evalue_threshold(ctx->idx.dev.n, params->max_evalue, &thr, &thr_all);
+    if (rc != MSG_OK) return ctx->fail(rc, "e-value threshold");
+    if (ctx->device < 0 || ctx->device >= 256) return MSG_EINVAL;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    if (!g_noalloc_addr[ctx->device]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) return ctx->cuda_fail(e == cudaSuccess ? cudaErrorInvalidSymbol : e);
+        g_noalloc_addr[ctx->device] = p;
+    }
+    unsigned char* base = static_cast<unsigned char*>(g_noalloc_addr[ctx->device]);
+    unsigned long long* hdr = reinterpret_cast<unsigned long long*>(base);
+    uint32_t* status = reinterpret_cast<uint32_t*>(hdr + 3);
+    cudaStream_t st = ctx->stream;
+    if (n_reads == 0) return MSG_OK;
+    e = cudaMemsetAsync(base, 0, kStaticHdr, st);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    k_maxlen<<<nblk(n_reads, 256), 256, 0, st>>>(d_off, n_reads, hdr + 2);
+    unsigned long long maxlen = 0;
+    e = cudaMemcpyAsync(&maxlen, hdr + 2, sizeof(maxlen), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    if ((int64_t)maxlen > kStaticMaxReadLen)
+        return ctx->fail(MSG_EINVAL, "a read is longer than MSG_NOALLOC_MAX_READ_LEN");
+    SmemArgs sa{};
+    sa.seq = d_seq; sa.off = d_off; sa.n_reads = n_reads; sa.min_len = params->min_len;
+    sa.thr = thr; sa.thr_all = thr_all;
+    for (int b = 0; b < 16; ++b) sa.llk[b] = ctx->idx.llk[b];
+    sa.out = d_smem; sa.cap = cap_per_read; sa.count = d_count;
+    unsigned char* pv = base + kStaticHdr;
+    const int64_t slots = kStaticWarps * kStaticPvCap;
+    sa.pv_p = reinterpret_cast<int64_t*>(pv);
+    sa.pv_q = sa.pv_p + slots;
+    sa.pv_s = sa.pv_q + slots;
+    sa.pv_lp = reinterpret_cast<double*>(sa.pv_s + slots);
+    sa.pv_pos = reinterpret_cast<int32_t*>(sa.pv_lp + slots);
+    sa.pv_cap = kStaticPvCap;
+    sa.work = hdr;
+    sa.n_ext = hdr + 1;
+    sa.status = status;
+    const int blocks = (int)std::min<int64_t>(ctx->num_sms, kStaticWarps / 8);  // 8 warps per 256-thread block
+    k_smem<<<blocks, 256, 0, st>>>(sa, ctx->idx.dev);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    uint32_t h_status = 0;
+    e = cudaMemcpyAsync(&h_status, status, sizeof(h_status), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    if (h_status & kErrInternal) return ctx->fail(MSG_EINTERNAL, "SMEM stage consistency check failed");
+    if (h_status & kErrOverflow) return ctx->fail(MSG_EINVAL, "output capacity too small; d_count holds the needed counts");
+    return MSG_OK;
+}

@@ -28,7 +28,7 @@ assert ALN_DTYPE.itemsize == 88
 # symbols of the C ABI, in include/msg_b200.h order
 EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy", "msg_index_load", "msg_index_bytes",
            "msg_map_params_default", "msg_map_batch", "msg_map_batch_device", "msg_last_stats", "msg_occ_query",
-           "msg_result_device", "msg_ctx_stream", "msg_bi_ext_query", "msg_sa_query"]
+           "msg_result_device", "msg_ctx_stream", "msg_smem_batch_noalloc", "msg_bi_ext_query", "msg_sa_query"]
 
 
 class FmdView(C.Structure):
@@ -102,6 +102,8 @@ def load_library(path: str = LIB_PATH):
     L.msg_last_stats.argtypes = [C.c_void_p, C.POINTER(MapStats)]
     L.msg_result_device.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     L.msg_ctx_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    L.msg_smem_batch_noalloc.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(MapParams),
+                                         C.c_void_p, C.c_int64, C.c_void_p]
     L.msg_occ_query.argtypes = [C.c_void_p, C.c_int64, u8p, i64p, i64p]
     L.msg_bi_ext_query.argtypes = [C.c_void_p, C.c_int64, C.c_int, u8p, i64p, i64p, i64p, i64p]
     L.msg_sa_query.argtypes = [C.c_void_p, C.c_int64, i64p, i64p]
@@ -257,6 +259,14 @@ class Context:
         self._check(self.lib.msg_map_batch(self.h, C.byref(batch), C.byref(params), C.byref(out), None),
                     "msg_map_batch")
         return out.n_aln, out.n_cigar
+
+    def smem_noalloc(self, seq_ptr: int, off_ptr: int, n_reads: int, out_ptr: int, cap_per_read: int,
+                     count_ptr: int, params: MapParams | None = None) -> int:
+        """msg_smem_batch_noalloc on caller-owned device buffers; returns the
+        status code (MSG_EINVAL when a count exceeded cap_per_read)."""
+        params = params or default_params()
+        return self.lib.msg_smem_batch_noalloc(self.h, n_reads, seq_ptr, off_ptr, C.byref(params), out_ptr,
+                                               cap_per_read, count_ptr)
 
     def stats(self) -> dict:
         s = MapStats()
