@@ -12,6 +12,7 @@
 //   k_dp        Alignment ctor window, calculateScores(chain), backTraceNW/SW (Alignment.cpp:46-276)
 //   k_cigar     Alignment::getAlnCigar (Alignment.cpp:278-303)
 #include "map_kernels.cuh"
+#include "smem_thread.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -208,41 +209,66 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     const int64_t Lmax = (int64_t)h_maxlen;
 
     // ---------------- SMEMs ----------------
+    // Reads up to 254 bp: one thread per read (k_smem_thread); longer reads:
+    // one warp per read with lanes over the candidate list (k_smem).
+    const bool thread_path = Lmax + 2 <= 256;
     const int threads = 256;
     const int blocks = ctx->num_sms * 8;
     const int64_t n_warps = (int64_t)blocks * threads / 32;
     const int64_t pv_cap = Lmax + 2;
-    CK(ctx->prev.ensure(n_warps * pv_cap * (4 + 8 + 8 + 8 + 8) + 64));
+    int64_t n_thr = 0;
+    if (thread_path) {
+        int bps = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread, 128, 0));
+        n_thr = (int64_t)ctx->num_sms * std::max(1, bps) * 128;
+        CK(ctx->prev.ensure(n_thr * pv_cap * sizeof(PrevEntry) + 64));
+        CK(cudaMemcpyToSymbolAsync(c_llk, im.llk, sizeof(im.llk), 0, cudaMemcpyHostToDevice, st));
+    } else {
+        CK(ctx->prev.ensure(n_warps * pv_cap * (4 + 8 + 8 + 8 + 8) + 64));
+    }
     int64_t cap = 16;
     int64_t h_nsmem = 0;
     for (int attempt = 0; attempt < 2; ++attempt) {
         CK(ctx->smem.ensure((size_t)std::max<int64_t>(1, n_reads) * cap * 48));
         CK(ctx->smem_cnt.ensure((n_reads + 1) * sizeof(int32_t)));
-        SmemArgs sa{};
-        sa.seq = d_seq; sa.off = d_off; sa.n_reads = n_reads; sa.min_len = params->min_len;
-        sa.thr = thr; sa.thr_all = thr_all;
-        for (int b = 0; b < 16; ++b) sa.llk[b] = im.llk[b];
-        sa.out = ctx->smem.as<int64_t>(); sa.cap = cap; sa.count = ctx->smem_cnt.as<int32_t>();
-        char* pv = ctx->prev.as<char>();
-        sa.pv_p = reinterpret_cast<int64_t*>(pv);
-        sa.pv_q = sa.pv_p + n_warps * pv_cap;
-        sa.pv_s = sa.pv_q + n_warps * pv_cap;
-        sa.pv_lp = reinterpret_cast<double*>(sa.pv_s + n_warps * pv_cap);
-        sa.pv_pos = reinterpret_cast<int32_t*>(sa.pv_lp + n_warps * pv_cap);
-        sa.pv_cap = pv_cap;
-        sa.work = d_ctr;
-        sa.n_ext = d_ctr + 1;
-        sa.status = d_status;
         CK(cudaMemsetAsync(d_ctr, 0, 16, st));
         CK(cudaMemsetAsync(d_status, 0, 4, st));
-        if (n_reads > 0) {
-            S.n_launch++, k_smem<<<blocks, threads, 0, st>>>(sa, ix);
-            CK(cudaGetLastError());
+        if (thread_path) {
+            SmemThreadArgs ta{};
+            ta.seq = d_seq; ta.off = d_off; ta.n_reads = n_reads; ta.min_len = params->min_len;
+            ta.thr = thr; ta.thr_all = thr_all;
+            ta.out = ctx->smem.as<int64_t>(); ta.cap = cap; ta.count = ctx->smem_cnt.as<int32_t>();
+            ta.prev = ctx->prev.as<PrevEntry>(); ta.pv_cap = pv_cap;
+            ta.work = d_ctr; ta.n_ext = d_ctr + 1; ta.status = d_status;
+            if (n_reads > 0) {
+                S.n_launch++, k_smem_thread<<<n_thr / 128, 128, 0, st>>>(ta, ix);
+                CK(cudaGetLastError());
+            }
+        } else {
+            SmemArgs sa{};
+            sa.seq = d_seq; sa.off = d_off; sa.n_reads = n_reads; sa.min_len = params->min_len;
+            sa.thr = thr; sa.thr_all = thr_all;
+            for (int b = 0; b < 16; ++b) sa.llk[b] = im.llk[b];
+            sa.out = ctx->smem.as<int64_t>(); sa.cap = cap; sa.count = ctx->smem_cnt.as<int32_t>();
+            char* pv = ctx->prev.as<char>();
+            sa.pv_p = reinterpret_cast<int64_t*>(pv);
+            sa.pv_q = sa.pv_p + n_warps * pv_cap;
+            sa.pv_s = sa.pv_q + n_warps * pv_cap;
+            sa.pv_lp = reinterpret_cast<double*>(sa.pv_s + n_warps * pv_cap);
+            sa.pv_pos = reinterpret_cast<int32_t*>(sa.pv_lp + n_warps * pv_cap);
+            sa.pv_cap = pv_cap;
+            sa.work = d_ctr;
+            sa.n_ext = d_ctr + 1;
+            sa.status = d_status;
+            if (n_reads > 0) {
+                S.n_launch++, k_smem<<<blocks, threads, 0, st>>>(sa, ix);
+                CK(cudaGetLastError());
+            }
         }
         uint32_t h_status = 0;
         CK(cudaMemcpyAsync(&h_status, d_status, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        if (h_status & kErrInternal) return ctx->fail(MSG_EINTERNAL, "SMEM stage consistency check failed");
+        if (h_status & (kErrInternal | 0x100u)) return ctx->fail(MSG_EINTERNAL, "SMEM stage consistency check failed");
         if (!(h_status & kErrOverflow)) break;
         if (attempt == 1) return ctx->fail(MSG_EINTERNAL, "SMEM output overflow after resizing");
         // rerun with the largest per-read count as capacity
@@ -399,14 +425,16 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         CK(cub::DeviceReduce::Sum(misc.p, tb, d_dpcells, d_ncig, h_nchain, st));
         CK(cudaMemcpyAsync(&S.dp_cells, d_ncig, 8, cudaMemcpyDeviceToHost, st));
     }
-    CK(offsets(ctx, d_cells, h_nchain, d_rect_off, misc, &h_cells));
+    CK(offsets(ctx, d_cells, h_nchain, d_rect_off, misc, &h_cells));  // d_cells holds bytes per chain
     CK(offsets(ctx, d_pcap, h_nchain, d_path_off, misc, &h_pathtot));
-    CK(ctx->scratch.ensure((h_cells + 1) * 3 * sizeof(int32_t) + (h_nidx + 1) * 2 * sizeof(int32_t) + 64));
+    const int64_t aux_bytes = ((2 * (h_nidx + 1) + h_nchain + 1) * sizeof(int32_t) + 15) / 16 * 16;
+    CK(ctx->scratch.ensure(h_cells + 64 + aux_bytes + (h_nidx + 1) * sizeof(int4)));
     const int64_t P16 = ((h_pathtot + 1 + 15) / 16) * 16;
     CK(ctx->path.ensure(2 * P16 + (h_nchain + 1) * 4 + 64));
     CK(ctx->alnbuf.ensure((h_nchain + 1) * sizeof(msg_aln)));
-    int32_t* d_rect = ctx->scratch.as<int32_t>();
-    int32_t* d_aux = d_rect + (h_cells + 1) * 3;
+    uint8_t* d_scr = ctx->scratch.as<uint8_t>();
+    int32_t* d_aux = reinterpret_cast<int32_t*>(d_scr + (h_cells + 64) / 16 * 16);
+    int4* d_sdbuf = reinterpret_cast<int4*>(reinterpret_cast<uint8_t*>(d_aux) + aux_bytes);
     uint8_t* d_path = ctx->path.as<uint8_t>();
     uint8_t* d_qbuf = d_path + P16;
     int32_t* d_plen = reinterpret_cast<int32_t*>(d_path + 2 * P16);
@@ -415,10 +443,10 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         DpArgs da{};
         da.ix = ix; da.seeds = d_seeds; da.chain_idx_off = d_cidx_off; da.chain_len = d_clen; da.chain_read = d_cread;
         da.chain_idx = d_cidx; da.n_chain = h_nchain; da.rseq = d_seq; da.roff = d_off; da.t_start = d_ts;
-        da.t_end = d_te; da.rect_off = d_rect_off; da.rect = d_rect; da.aux = d_aux; da.qbuf = d_qbuf;
-        da.path_off = d_path_off; da.path = d_path; da.path_len = d_plen; da.aln = d_aln; da.pp = dpp;
-        da.status = d_status;
-        S.n_launch++, k_dp<<<nblk(h_nchain * 32, 128), 128, 0, st>>>(da);
+        da.t_end = d_te; da.scr_off = d_rect_off; da.scr = d_scr; da.aux = d_aux; da.sdbuf = d_sdbuf;
+        da.qbuf = d_qbuf; da.path_off = d_path_off; da.path = d_path; da.path_len = d_plen; da.aln = d_aln;
+        da.pp = dpp; da.status = d_status;
+        S.n_launch++, k_dp<<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
         CK(cudaGetLastError());
     }
     tm.mark();  // 4

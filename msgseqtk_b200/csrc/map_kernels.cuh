@@ -521,11 +521,15 @@ __global__ void k_chain(const int64_t* __restrict__ read_seed_off, const int32_t
 // seed [clear its block, diagonal, the cell past it, I.row(to+1) = M.row(to)+o,
 // D.col(end+1) = M.col(end)+o], the gap rectangle to the next seed, and the 3'
 // rectangle. Rectangles and seed blocks are disjoint, so the final value of
-// any cell is given by the last region in that order that writes it. Only the
-// rectangles are stored (M, I, D per cell); every other cell is derived on
-// demand by `Chain::M/I/D` below. A query made while computing region m only
-// looks at regions written before m, which is exactly the state the reference
-// saw at that point.
+// any cell is given by the last region in that order that writes it; a query
+// made while computing region m only looks at regions written before m, which
+// is the state the reference saw at that point. No rectangle's boundary lies
+// inside another rectangle, so rectangles are filled from derived values only.
+//
+// Per rectangle cell only a 1-byte traceback code is stored (the decisions the
+// reference's matchMax/insMax/delMax would take there, and M > 0 for local
+// mode); full M/I/D values are kept for the rectangle's last row and column,
+// the only rectangle cells a traceback can reach from outside.
 // ======================================================================
 __device__ __forceinline__ int32_t sat_add(int32_t a, int32_t b) {  // a + b for b <= 0, -inf absorbing
     return a == NEG ? NEG : max(a + b, NEG);
@@ -537,41 +541,65 @@ struct DpParams {
     int32_t mode;  // 0 NW, 1 SW
 };
 
+constexpr int kDpWarps = 4;       // warps per block in k_dp
+constexpr int kSmemSeeds = 64;    // chain seeds cached in shared memory per warp
+
+__device__ __forceinline__ int match_max(int32_t m, int32_t i, int32_t d) {  // Alignment.h:577-589
+    int32_t mx = m;
+    int s = OP_M;
+    if (i > mx) { mx = d; s = OP_I; }
+    if (d > mx) s = OP_D;
+    return s;
+}
+
+struct RectGeo {
+    int64_t r0, c0, R, C;
+    uint8_t* code;    // stripes x (C + 31) x 32 codes
+    int32_t* rowbuf;  // (C + 1) x 3: bottom row of the previous stripe
+    int32_t* lastrow; // C x 3
+    int32_t* lastcol; // R x 3
+};
+
+__device__ __forceinline__ int64_t rect_bytes(int64_t R, int64_t C) {
+    if (R <= 0 || C <= 0) return 0;
+    const int64_t stripes = (R + 31) / 32;
+    const int64_t code = ((stripes * (C + 31) * 32) + 15) / 16 * 16;
+    return code + ((C + 1) * 3 + C * 3 + R * 3) * 4 + 16;
+}
+
 struct ChainCtx {
-    const Seed* seeds;          // global seeds
-    const int64_t* idx;         // chain's seed indices
+    const int4* sd;             // per seed: qf, qt, ts, te (window-relative)
     int32_t n;                  // seeds in the chain
     int64_t L, T;               // query length, window length
-    int64_t t_start;
     const uint8_t* query;       // read (FWD) or reverse complement in scratch (REV)
     const uint8_t* target;      // chromosome + t_start
     int64_t target_avail;       // chromosome bases available from t_start (beyond: terminator 0)
-    int32_t* rect;              // rectangle storage: [M | I | D] blocks per rectangle
-    int32_t* aux;               // per seed: diag start, rectangle offset of the following gap
+    uint8_t* scratch;           // rectangle storage of this chain
+    int32_t* diag;              // per seed: first diagonal value
+    int32_t* roff;              // per rectangle index (0..n): byte offset in scratch
     DpParams pp;
-    int32_t sc_match, sc_mis;
+    uint32_t* status;
 
-    __device__ int64_t qf(int k) const { return seeds[idx[k]].from; }
-    __device__ int64_t qt(int k) const { return seeds[idx[k]].to; }
-    __device__ int64_t ts(int k) const { return seeds[idx[k]].start - t_start; }
-    __device__ int64_t te(int k) const { return seeds[idx[k]].end - t_start; }
+    __device__ int64_t qf(int k) const { return sd[k].x; }
+    __device__ int64_t qt(int k) const { return sd[k].y; }
+    __device__ int64_t ts(int k) const { return sd[k].z; }
+    __device__ int64_t te(int k) const { return sd[k].w; }
     __device__ int tb(int64_t t) const { return t < target_avail ? (int)__ldg(target + t) : 0; }
     // ScoreScheme::getScore (ScoreScheme.cpp:20-24)
     __device__ int32_t score(int qb, int tbb) const {
-        return ((qb & tbb) && qb != 15 && tbb != 15) ? sc_match : -sc_mis;
+        return ((qb & tbb) && qb != 15 && tbb != 15) ? pp.match : -pp.mismatch;
     }
-
-    // row/column boundaries: b[0]=0, b[2k-1]=qf_k, b[2k]=qt_k, b[2n+1]=L
+    // row/column boundaries: b[0]=0, b[2k+1]=qf_k, b[2k+2]=qt_k, b[2n+1]=L
     __device__ int64_t rb(int m) const {
         if (m <= 0) return 0;
         if (m >= 2 * n + 1) return L;
-        const int k = (m + 1) / 2 - 1;
+        const int k = (m - 1) >> 1;
         return (m & 1) ? qf(k) : qt(k);
     }
     __device__ int64_t cb(int m) const {
         if (m <= 0) return 0;
         if (m >= 2 * n + 1) return T;
-        const int k = (m + 1) / 2 - 1;
+        const int k = (m - 1) >> 1;
         return (m & 1) ? ts(k) : te(k);
     }
     // segment of matrix row i >= 1: smallest m with i <= b[m+1]
@@ -585,17 +613,32 @@ struct ChainCtx {
         while (lo < hi) { const int mid = (lo + hi) >> 1; if (j <= cb(mid + 1)) hi = mid; else lo = mid + 1; }
         return lo;
     }
-    __device__ int64_t rect_off(int m) const {  // cell offset of rectangle m (even m)
-        return m == 0 ? 0 : (int64_t)aux[2 * (m / 2 - 1) + 1];
+    __device__ RectGeo rect(int m) const {
+        RectGeo g;
+        g.r0 = rb(m); g.c0 = cb(m);
+        g.R = rb(m + 1) - g.r0; g.C = cb(m + 1) - g.c0;
+        uint8_t* base = scratch + roff[m >> 1];
+        const int64_t stripes = (g.R + 31) / 32;
+        g.code = base;
+        int32_t* ints = reinterpret_cast<int32_t*>(base + ((stripes * (g.C + 31) * 32) + 15) / 16 * 16);
+        g.rowbuf = ints;
+        g.lastrow = ints + (g.C + 1) * 3;
+        g.lastcol = g.lastrow + g.C * 3;
+        return g;
     }
-    __device__ int32_t* rect_ptr(int m, int which, int64_t i, int64_t j) const {
-        const int64_t r0 = rb(m), c0 = cb(m);
-        const int64_t R = rb(m + 1) - r0, Cc = cb(m + 1) - c0;
-        const int64_t area = R * Cc;
-        return rect + rect_off(m) * 3 + which * area + (i - r0 - 1) * Cc + (j - c0 - 1);
+    __device__ uint8_t code_at(const RectGeo& g, int64_t i, int64_t j) const {
+        const int64_t rr = i - g.r0 - 1, cc = j - g.c0 - 1;
+        const int64_t stripe = rr >> 5, lane = rr & 31;
+        return g.code[(stripe * (g.C + 31) + cc + lane) * 32 + lane];
     }
-    __device__ int32_t diag_start(int k) const { return aux[2 * k]; }
-    // seed k (0-based) with qt == v, or -1
+    // stored value of a rectangle cell (its last row or column)
+    __device__ int32_t rect_val(int m, int which, int64_t i, int64_t j) const {
+        const RectGeo g = rect(m);
+        if (i == g.r0 + g.R) return g.lastrow[(j - g.c0 - 1) * 3 + which];
+        if (j == g.c0 + g.C) return g.lastcol[(i - g.r0 - 1) * 3 + which];
+        atomicOr(status, kErrInternal);
+        return NEG;
+    }
     __device__ int seed_by_qt(int64_t v) const {
         int lo = 0, hi = n - 1;
         while (lo <= hi) { const int mid = (lo + hi) >> 1; const int64_t x = qt(mid); if (x == v) return mid; if (x < v) lo = mid + 1; else hi = mid - 1; }
@@ -606,20 +649,18 @@ struct ChainCtx {
         while (lo <= hi) { const int mid = (lo + hi) >> 1; const int64_t x = te(mid); if (x == v) return mid; if (x < v) lo = mid + 1; else hi = mid - 1; }
         return -1;
     }
-
     // Final value of M(i,j) as seen by region `stage` (regions < stage written).
     __device__ int32_t M(int64_t i, int64_t j, int stage) const {
         if (i >= 1 && j >= 1) {
             const int mr = row_seg(i);
             if (mr == col_seg(j) && mr < stage) {
-                if (!(mr & 1)) return *rect_ptr(mr, 0, i, j);
-                const int k = (mr + 1) / 2 - 1;
-                const int64_t d = i - qf(k) - 1;
-                if (i - qf(k) == j - ts(k)) return diag_start(k) + (int32_t)d * sc_match;
+                if (!(mr & 1)) return rect_val(mr, 0, i, j);
+                const int k = (mr - 1) >> 1;
+                if (i - qf(k) == j - ts(k)) return diag[k] + (int32_t)(i - qf(k) - 1) * pp.match;
                 return NEG;
             }
             const int k = seed_by_qt(i - 1);  // the cell past seed k (Alignment.cpp:157-160)
-            if (k >= 0 && 2 * k + 1 < stage && te(k) + 1 == j) return diag_start(k) + (int32_t)(qt(k) - qf(k)) * sc_match;
+            if (k >= 0 && 2 * k + 1 < stage && te(k) + 1 == j) return diag[k] + (int32_t)(qt(k) - qf(k)) * pp.match;
         }
         if (pp.mode == 0) return i == 0 ? 0 : NEG;
         return (i == 0 || j == 0) ? 0 : NEG;
@@ -627,7 +668,7 @@ struct ChainCtx {
     __device__ int32_t I(int64_t i, int64_t j, int stage) const {
         if (i >= 1 && j >= 1) {
             const int mr = row_seg(i);
-            if (mr == col_seg(j) && mr < stage && !(mr & 1)) return *rect_ptr(mr, 1, i, j);
+            if (mr == col_seg(j) && mr < stage && !(mr & 1)) return rect_val(mr, 1, i, j);
         }
         if (i >= 1) {
             const int k = seed_by_qt(i - 1);  // I.row(to+1) = M.row(to) + o (Alignment.cpp:161-163)
@@ -639,7 +680,7 @@ struct ChainCtx {
     __device__ int32_t D(int64_t i, int64_t j, int stage) const {
         if (i >= 1 && j >= 1) {
             const int mr = row_seg(i);
-            if (mr == col_seg(j) && mr < stage && !(mr & 1)) return *rect_ptr(mr, 2, i, j);
+            if (mr == col_seg(j) && mr < stage && !(mr & 1)) return rect_val(mr, 2, i, j);
         }
         if (j >= 1) {
             const int k = seed_by_te(j - 1);  // D.col(end+1) = M.col(end) + o (Alignment.cpp:165-169)
@@ -648,31 +689,72 @@ struct ChainCtx {
         return NEG;
     }
 
-    // Warp-cooperative fill of rectangle m (Alignment::calculateScoresNW/SW,
-    // Alignment.cpp:72-133) by anti-diagonals.
-    __device__ void fill_rect(int m) {
-        const int64_t r0 = rb(m), c0 = cb(m);
-        const int64_t R = rb(m + 1) - r0, Cc = cb(m + 1) - c0;
-        if (R <= 0 || Cc <= 0) return;
+    // Warp fill of rectangle m (Alignment::calculateScoresNW/SW,
+    // Alignment.cpp:72-133): stripes of 32 rows, lane = row, one column per
+    // step along the anti-diagonal wavefront; values travel by shuffles.
+    // Returns this lane's best (M, column-major key) for local mode.
+    __device__ void fill_rect(int m, int32_t& best, int64_t& bkey) {
+        const RectGeo g = rect(m);
+        if (g.R <= 0 || g.C <= 0) return;
+        const int lane = lane_id();
         const int32_t o = -(pp.gap_o + pp.gap_e), e = -pp.gap_e;
-        for (int64_t d = 0; d < R + Cc - 1; ++d) {
-            const int64_t rlo = max((int64_t)0, d - (Cc - 1)), rhi = min(R - 1, d);
-            for (int64_t rr = rlo + lane_id(); rr <= rhi; rr += 32) {
-                const int64_t cc = d - rr;
-                const int64_t i = r0 + 1 + rr, j = c0 + 1 + cc;
-                int32_t md, id, dd, mu, iu, ml, dl;
-                if (rr > 0 && cc > 0) { md = *rect_ptr(m, 0, i - 1, j - 1); id = *rect_ptr(m, 1, i - 1, j - 1); dd = *rect_ptr(m, 2, i - 1, j - 1); }
-                else { md = M(i - 1, j - 1, m); id = I(i - 1, j - 1, m); dd = D(i - 1, j - 1, m); }
-                if (rr > 0) { mu = *rect_ptr(m, 0, i - 1, j); iu = *rect_ptr(m, 1, i - 1, j); }
-                else { mu = M(i - 1, j, m); iu = I(i - 1, j, m); }
-                if (cc > 0) { ml = *rect_ptr(m, 0, i, j - 1); dl = *rect_ptr(m, 2, i, j - 1); }
-                else { ml = M(i, j - 1, m); dl = D(i, j - 1, m); }
-                const int s = score(query[i - 1], tb(j - 1));
-                int32_t mv = add_s(max(max(md, dd), id), s);
-                if (pp.mode == 1) mv = max(mv, 0);
-                *rect_ptr(m, 0, i, j) = mv;
-                *rect_ptr(m, 1, i, j) = max(sat_add(mu, o), sat_add(iu, e));
-                *rect_ptr(m, 2, i, j) = max(sat_add(ml, o), sat_add(dl, e));
+        const int64_t stripes = (g.R + 31) / 32;
+        for (int64_t sp = 0; sp < stripes; ++sp) {
+            const int64_t rr = sp * 32 + lane;
+            const bool row_ok = rr < g.R;
+            const int64_t i = g.r0 + 1 + rr;
+            // left boundary (column c0) of this row and of the row above
+            int32_t ml = NEG, dl = NEG, md0 = NEG, id0 = NEG, dd0 = NEG;
+            if (row_ok) {
+                ml = M(i, g.c0, m); dl = D(i, g.c0, m);
+                md0 = M(i - 1, g.c0, m); id0 = I(i - 1, g.c0, m); dd0 = D(i - 1, g.c0, m);
+            }
+            const int qb = row_ok ? (int)query[i - 1] : 0;
+            int32_t pm = NEG, pi = NEG, pd = NEG;       // this lane's output of the previous step
+            int32_t um = NEG, ui = NEG, ud = NEG;       // up neighbour (i-1, j) of the current step
+            int32_t dm = md0, di = id0, dd = dd0;       // diagonal neighbour (i-1, j-1)
+            uint8_t* code_base = g.code + sp * (g.C + 31) * 32;
+            for (int64_t t = 0; t < g.C + 31; ++t) {
+                const int64_t c = t - lane;
+                const int32_t sm_ = __shfl_up_sync(0xffffffffu, pm, 1);
+                const int32_t si_ = __shfl_up_sync(0xffffffffu, pi, 1);
+                const int32_t sd_ = __shfl_up_sync(0xffffffffu, pd, 1);
+                const bool act = row_ok && c >= 0 && c < g.C;
+                if (lane == 0) {
+                    if (act) {
+                        const int64_t j = g.c0 + 1 + c;
+                        if (sp == 0) { um = M(i - 1, j, m); ui = I(i - 1, j, m); ud = D(i - 1, j, m); }
+                        else { um = g.rowbuf[c * 3]; ui = g.rowbuf[c * 3 + 1]; ud = g.rowbuf[c * 3 + 2]; }
+                    }
+                } else {
+                    um = sm_; ui = si_; ud = sd_;
+                }
+                if (act) {
+                    const int64_t j = g.c0 + 1 + c;
+                    const int32_t lm = c == 0 ? ml : pm;
+                    const int32_t ld = c == 0 ? dl : pd;
+                    const int s = score(qb, tb(j - 1));
+                    const int32_t mx = max(max(dm, dd), di);
+                    int32_t mv = add_s(mx, s);
+                    if (pp.mode == 1) mv = max(mv, 0);
+                    const int32_t a1 = sat_add(um, o), a2 = sat_add(ui, e);
+                    const int32_t iv = max(a1, a2);
+                    const int32_t b1 = sat_add(lm, o), b2 = sat_add(ld, e);
+                    const int32_t dv = max(b1, b2);
+                    const uint8_t code = (uint8_t)(match_max(dm, di, dd) | ((a1 > a2) ? 4 : 0) |
+                                                   ((b1 > b2) ? 8 : 0) | (mv > 0 ? 16 : 0));
+                    code_base[(c + lane) * 32 + lane] = code;
+                    if (rr == g.R - 1) { g.lastrow[c * 3] = mv; g.lastrow[c * 3 + 1] = iv; g.lastrow[c * 3 + 2] = dv; }
+                    if (c == g.C - 1) { g.lastcol[rr * 3] = mv; g.lastcol[rr * 3 + 1] = iv; g.lastcol[rr * 3 + 2] = dv; }
+                    if (lane == 31) { g.rowbuf[c * 3] = mv; g.rowbuf[c * 3 + 1] = iv; g.rowbuf[c * 3 + 2] = dv; }
+                    if (pp.mode == 1) {
+                        const int64_t key = j * (L + 1) + i;
+                        if (mv > best || (mv == best && key < bkey)) { best = mv; bkey = key; }
+                    }
+                    pm = mv; pi = iv; pd = dv;
+                }
+                // the up neighbour of this step is the diagonal of the next
+                if (act) { dm = um; di = ui; dd = ud; }
             }
             __syncwarp();
         }
@@ -691,9 +773,10 @@ struct DpArgs {
     const int64_t* roff;
     const int64_t* t_start;
     const int64_t* t_end;
-    const int64_t* rect_off;    // per chain, in cells (x3 int32)
-    int32_t* rect;
-    int32_t* aux;               // per chain at 2 * chain_idx_off
+    const int64_t* scr_off;     // per chain, bytes of rectangle storage
+    uint8_t* scr;
+    int32_t* aux;               // per chain at 2 * chain_idx_off + chain index: diag (n) and rect offsets (n + 1)
+    int4* sdbuf;                // per chain seed geometry when n > kSmemSeeds (at chain_idx_off)
     uint8_t* qbuf;              // reverse-complement query per chain at path_off
     const int64_t* path_off;    // per chain, capacity L + tLen + 1
     uint8_t* path;
@@ -709,7 +792,7 @@ struct DpArgs {
 __global__ void k_dp_prep(IndexDev ix, const Seed* __restrict__ seeds, const int64_t* __restrict__ chain_idx_off,
                           const int32_t* __restrict__ chain_len, const int32_t* __restrict__ chain_read,
                           const int64_t* __restrict__ chain_idx, const int64_t* __restrict__ roff, int64_t n_chain,
-                          int64_t* __restrict__ t_start, int64_t* __restrict__ t_end, int64_t* __restrict__ cells,
+                          int64_t* __restrict__ t_start, int64_t* __restrict__ t_end, int64_t* __restrict__ bytes,
                           int64_t* __restrict__ pathcap, int64_t* __restrict__ dpcells) {
     const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (c >= n_chain) return;
@@ -727,10 +810,11 @@ __global__ void k_dp_prep(IndexDev ix, const Seed* __restrict__ seeds, const int
     t_start[c] = tS;
     t_end[c] = tE;
     const int64_t T = tE - tS;
-    int64_t area = 0, diag = 0;
+    int64_t area = 0, diag = 0, by = 0;
     {   // 5' rectangle, gaps, 3' rectangle (Alignment.cpp:54-70)
-        int64_t a0 = f.from, b0 = f.start - tS;
+        const int64_t a0 = f.from, b0 = f.start - tS;
         if (a0 > 0 && b0 > 0) area += a0 * b0;
+        by += rect_bytes(a0, b0);
         for (int k = 0; k < n; ++k) {
             const Seed s = seeds[idx[k]];
             diag += s.to - s.from;
@@ -738,44 +822,46 @@ __global__ void k_dp_prep(IndexDev ix, const Seed* __restrict__ seeds, const int
                 const Seed t = seeds[idx[k + 1]];
                 const int64_t R = t.from - s.to, C = t.start - s.end;
                 if (R > 0 && C > 0) area += R * C;
+                by += rect_bytes(R, C);
             }
         }
         const int64_t R = L - l.to, C = tE - l.end;
         if (R > 0 && C > 0) area += R * C;
+        by += rect_bytes(R, C);
     }
-    cells[c] = area;
+    bytes[c] = by;
     pathcap[c] = L + T + 1;
     dpcells[c] = area + diag;
 }
 
-__device__ __forceinline__ int match_max(int32_t m, int32_t i, int32_t d) {  // Alignment.h:577-589
-    int32_t mx = m;
-    int s = OP_M;
-    if (i > mx) { mx = d; s = OP_I; }
-    if (d > mx) s = OP_D;
-    return s;
-}
-
-__global__ void __launch_bounds__(128) k_dp(DpArgs a) {
+__global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
+    __shared__ int4 s_sd[kDpWarps][kSmemSeeds];
+    const int w = threadIdx.x >> 5;
     const int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (c >= a.n_chain) return;
     ChainCtx x;
-    x.seeds = a.seeds;
-    x.idx = a.chain_idx + a.chain_idx_off[c];
+    const int64_t* idx = a.chain_idx + a.chain_idx_off[c];
     x.n = a.chain_len[c];
     const int64_t r = a.chain_read[c];
     x.L = a.roff[r + 1] - a.roff[r];
-    x.t_start = a.t_start[c];
-    x.T = a.t_end[c] - x.t_start;
-    const Seed f = a.seeds[x.idx[0]];
+    const int64_t t_start = a.t_start[c];
+    x.T = a.t_end[c] - t_start;
+    const Seed f = a.seeds[idx[0]];
     const int64_t chr_len = a.ix.chr_len[f.tid];
-    x.target = a.ix.chr_seq + a.ix.chr_off[f.tid] + x.t_start;
-    x.target_avail = chr_len - x.t_start;
-    x.rect = a.rect + a.rect_off[c] * 3;
-    x.aux = a.aux + 2 * a.chain_idx_off[c];
+    x.target = a.ix.chr_seq + a.ix.chr_off[f.tid] + t_start;
+    x.target_avail = chr_len - t_start;
+    x.scratch = a.scr + a.scr_off[c];
+    int32_t* aux = a.aux + 2 * a.chain_idx_off[c] + c;
+    x.diag = aux;
+    x.roff = aux + x.n;
     x.pp = a.pp;
-    x.sc_match = a.pp.match;
-    x.sc_mis = a.pp.mismatch;
+    x.status = a.status;
+    int4* sd = x.n <= kSmemSeeds ? s_sd[w] : a.sdbuf + a.chain_idx_off[c];
+    for (int k = lane_id(); k < x.n; k += 32) {
+        const Seed s = a.seeds[idx[k]];
+        sd[k] = make_int4(s.from, s.to, (int)(s.start - t_start), (int)(s.end - t_start));
+    }
+    x.sd = sd;
     const uint8_t* rd = a.rseq + a.roff[r];
     uint8_t* path = a.path + a.path_off[c];
     if (f.strand == FWD) {
@@ -783,45 +869,40 @@ __global__ void __launch_bounds__(128) k_dp(DpArgs a) {
     } else {  // PrimarySeq::revcom
         uint8_t* qb = a.qbuf + a.path_off[c];
         for (int64_t i = lane_id(); i < x.L; i += 32) qb[i] = (uint8_t)comp16(rd[x.L - 1 - i]);
-        __syncwarp();
         x.query = qb;
     }
-    // rectangle offsets of the gaps and the 3' end: aux[2k+1] = offset of
-    // rectangle 2(k+1) (gap after seed k, or the 3' rectangle for k = n-1)
-    if (lane_id() == 0) {
+    __syncwarp();
+    if (lane_id() == 0) {  // byte offsets of rectangles 0..n in this chain's storage
         int64_t off = 0;
-        {
-            const int64_t R = x.rb(1) - x.rb(0), C = x.cb(1) - x.cb(0);
-            if (R > 0 && C > 0) off += R * C;
-        }
-        for (int k = 0; k < x.n; ++k) {
-            x.aux[2 * k + 1] = (int32_t)off;
-            const int m = 2 * (k + 1);
-            const int64_t R = x.rb(m + 1) - x.rb(m), C = x.cb(m + 1) - x.cb(m);
-            if (R > 0 && C > 0) off += R * C;
+        for (int q = 0; q <= x.n; ++q) {
+            const int m = 2 * q;
+            x.roff[q] = (int32_t)off;
+            off += rect_bytes(x.rb(m + 1) - x.rb(m), x.cb(m + 1) - x.cb(m));
         }
     }
     __syncwarp();
-    // region order: R0 (m=0), then per seed k: S_k (m=2k+1), G_k / R3 (m=2k+2)
-    x.fill_rect(0);
+    int32_t best = 0;       // local mode: M(0,0) = 0 is the first candidate
+    int64_t bkey = 0;
+    x.fill_rect(0, best, bkey);
     for (int k = 0; k < x.n; ++k) {
         const int m = 2 * k + 1;
         if (lane_id() == 0) {  // first diagonal cell (Alignment.cpp:146-153): max(M,D,I + s, 0)
             const int64_t i = x.qf(k), j = x.ts(k);
             const int32_t mx = max(max(x.M(i, j, m), x.D(i, j, m)), x.I(i, j, m));
-            x.aux[2 * k] = max(add_s(mx, x.sc_match), 0);
+            x.diag[k] = max(add_s(mx, a.pp.match), 0);
         }
         __syncwarp();
-        x.fill_rect(m + 1);
+        x.fill_rect(m + 1, best, bkey);
     }
+    __syncwarp();
     const int stage = 2 * x.n + 2;
     // ---- traceback ----
     int64_t aln_to = 0, aln_end = 0;
-    int32_t best = NEG;
     int s0 = OP_M;
     int32_t flags = 0;
     if (a.pp.mode == 0) {  // backTraceNW: scan the last row, M before I, first strict max
-        int64_t bkey = INT64_MAX;
+        best = NEG;
+        bkey = INT64_MAX;
         for (int64_t j = 1 + lane_id(); j <= x.T; j += 32) {
             const int32_t vm = x.M(x.L, j, stage), vi = x.I(x.L, j, stage);
             if (vm > best || (vm == best && vm != NEG && 2 * j < bkey)) { best = vm; bkey = 2 * j; }
@@ -836,21 +917,10 @@ __global__ void __launch_bounds__(128) k_dp(DpArgs a) {
         if (best == NEG) { aln_end = 0; s0 = OP_M; flags |= 1; }
         else { aln_end = bkey >> 1; s0 = (bkey & 1) ? OP_I : OP_M; }
     } else {  // backTraceSW: Eigen maxCoeff, first max in column-major order
-        int64_t bkey = 0;  // M(0,0) = 0
-        best = 0;
         auto consider = [&](int64_t i, int64_t j, int32_t v) {
             const int64_t key = j * (x.L + 1) + i;
             if (v > best || (v == best && key < bkey)) { best = v; bkey = key; }
         };
-        for (int m = 0; m <= 2 * x.n; m += 2) {
-            const int64_t r0 = x.rb(m), c0 = x.cb(m);
-            const int64_t R = x.rb(m + 1) - r0, C = x.cb(m + 1) - c0;
-            if (R <= 0 || C <= 0) continue;
-            for (int64_t t = lane_id(); t < R * C; t += 32) {
-                const int64_t i = r0 + 1 + t / C, j = c0 + 1 + t % C;
-                consider(i, j, *x.rect_ptr(m, 0, i, j));
-            }
-        }
         for (int k = 0; k < x.n; ++k) {
             const int64_t len = x.qt(k) - x.qf(k);
             for (int64_t d = lane_id(); d < len; d += 32) {
@@ -859,7 +929,10 @@ __global__ void __launch_bounds__(128) k_dp(DpArgs a) {
             }
             if (lane_id() == 0) {
                 const int64_t i = x.qt(k) + 1, j = x.te(k) + 1;
-                if (i <= x.L && j <= x.T) consider(i, j, x.M(i, j, stage));
+                if (i <= x.L && j <= x.T) {
+                    const int mr = x.row_seg(i);
+                    if (!(mr == x.col_seg(j) && !(mr & 1))) consider(i, j, x.M(i, j, stage));
+                }
             }
         }
         for (int o = 16; o > 0; o >>= 1) {
@@ -877,27 +950,53 @@ __global__ void __launch_bounds__(128) k_dp(DpArgs a) {
         int s = s0;
         int64_t np = 0;
         const int64_t cap = x.L + x.T + 1;
+        int cur_m = -1;  // rectangle holding (i, j), if any
+        RectGeo g{};
         for (;;) {
+            // locate (i, j): inside a rectangle -> traceback codes
+            bool in_rect = false;
+            if (i >= 1 && j >= 1) {
+                if (cur_m >= 0 && i > g.r0 && i <= g.r0 + g.R && j > g.c0 && j <= g.c0 + g.C) in_rect = true;
+                else {
+                    const int mr = x.row_seg(i);
+                    if (mr == x.col_seg(j) && !(mr & 1)) { cur_m = mr; g = x.rect(mr); in_rect = true; }
+                }
+            }
+            const uint8_t code = in_rect ? x.code_at(g, i, j) : 0;
             if (a.pp.mode == 0) { if (!(i > 0)) break; }
-            else { if (!(s != OP_M || x.M(i, j, stage) > 0)) break; }
+            else {
+                const bool mpos = in_rect ? ((code >> 4) & 1) : (x.M(i, j, stage) > 0);
+                if (!(s != OP_M || mpos)) break;
+            }
             const bool ok = (s == OP_M) ? (i >= 1 && j >= 1) : (s == OP_I) ? (i >= 1) : (j >= 1);
             if (!ok || np >= cap) { flags |= 2; break; }
             path[np++] = (uint8_t)s;
-            if (s == OP_M) { s = match_max(x.M(i - 1, j - 1, stage), x.I(i - 1, j - 1, stage), x.D(i - 1, j - 1, stage)); i--; j--; }
-            else if (s == OP_I) { s = sat_add(x.M(i - 1, j, stage), -(go + ge)) > sat_add(x.I(i - 1, j, stage), -ge) ? OP_M : OP_I; i--; }
-            else { s = sat_add(x.M(i, j - 1, stage), -(go + ge)) > sat_add(x.D(i, j - 1, stage), -ge) ? OP_M : OP_D; j--; }
+            if (s == OP_M) {
+                s = in_rect ? (code & 3) : match_max(x.M(i - 1, j - 1, stage), x.I(i - 1, j - 1, stage), x.D(i - 1, j - 1, stage));
+                i--; j--;
+            } else if (s == OP_I) {
+                const bool mm = in_rect ? ((code >> 2) & 1)
+                                        : sat_add(x.M(i - 1, j, stage), -(go + ge)) > sat_add(x.I(i - 1, j, stage), -ge);
+                s = mm ? OP_M : OP_I;
+                i--;
+            } else {
+                const bool mm = in_rect ? ((code >> 3) & 1)
+                                        : sat_add(x.M(i, j - 1, stage), -(go + ge)) > sat_add(x.D(i, j - 1, stage), -ge);
+                s = mm ? OP_M : OP_D;
+                j--;
+            }
         }
         a.path_len[c] = (int32_t)np;
         msg_aln& o = a.aln[c];
         o.read = r;
         o.tid = f.tid;
         o.strand = f.strand;
-        o.t_start = x.t_start;
+        o.t_start = t_start;
         o.t_end = a.t_end[c];
         o.aln_from = i;
         o.aln_to = aln_to;
-        o.aln_start = x.t_start + j;
-        o.aln_end = x.t_start + aln_end;
+        o.aln_start = t_start + j;
+        o.aln_end = t_start + aln_end;
         o.aln_score = best == NEG ? INT32_MIN : best;
         o.flags = flags;
         if (flags & 2) atomicOr(a.status, kErrTrace);

@@ -1,0 +1,318 @@
+// SMEM search with one thread per read (included by map.cu after
+// map_kernels.cuh). The reference's findAllSMEMS / findFwdBackSMEMS /
+// findBackFwdSMEMS control flow (SMEM.cpp:64-215) is unrolled into a state
+// machine whose every step performs exactly one bi-interval extension, so the
+// occurrence-bucket loads of all 32 reads of a warp issue together. Candidate
+// lists (`prev`) live in per-thread global scratch; their processing follows
+// the reference's sequential loop entry by entry (validity by the running
+// size s0, emission while nValid == 0, in-place compaction).
+#pragma once
+#include "map_kernels.cuh"
+
+namespace msg {
+
+struct PrevEntry {
+    int64_t p, q, s;
+    double lp;
+    int64_t pos;  // `to` (fwd-back) or `from` (back-fwd) of the entry
+};
+
+struct SmemThreadArgs {
+    const uint8_t* seq;
+    const int64_t* off;
+    int64_t n_reads;
+    int64_t min_len;
+    double thr;
+    int thr_all;
+    int64_t* out;
+    int64_t cap;
+    int32_t* count;
+    PrevEntry* prev;        // pv_cap entries per thread
+    int64_t pv_cap;
+    unsigned long long* work;
+    unsigned long long* n_ext;
+    uint32_t* status;
+};
+
+__constant__ double c_llk[16];
+
+enum SmemPhase : int {
+    PH_NEXT_READ = 0,
+    PH_OUTER_LOOP,      // while (from > 0 || to < L)
+    PH_OUTER_BACK,      // --from; back-fwd call
+    PH_FB_WALK,         // forward walk of findFwdBackSMEMS
+    PH_FB_ITER,         // start of one backward pass over prev
+    PH_FB_ENTRY,        // one prev entry of that pass
+    PH_BF_WALK,         // backward walk of findBackFwdSMEMS
+    PH_BF_ITER,
+    PH_BF_ENTRY,
+    PH_DONE
+};
+
+struct ThreadSmem {
+    const uint8_t* rd;
+    int64_t L;
+    int64_t* out;
+    int32_t n_out;
+    int64_t r;
+    // findAllSMEMS variables and the call in progress
+    int64_t from, to;
+    int site;               // 0: first FB(from,to)  1: FB(from0,to)  2: BF(from,to0)
+    int64_t cf, ct;         // the called function's from/to
+    // walk state
+    SmemState m, m0;
+    int n_prev;
+    // pass over prev
+    int k, n_keep;
+    int64_t s0, n_valid;
+    int b2;
+    PrevEntry e0;
+    int phase;
+    unsigned long long ext;
+
+    __device__ int base(int64_t i) const { return (i >= 0 && i < L) ? (int)__ldg(rd + i) : 0; }
+};
+
+__device__ __forceinline__ void smem_emit(ThreadSmem& t, const SmemThreadArgs& a, int64_t from, int64_t to,
+                                          const PrevEntry& e) {
+    if (t.n_out < a.cap) {
+        int64_t* o = t.out + 6 * (int64_t)t.n_out;
+        o[0] = from; o[1] = to; o[2] = e.p; o[3] = e.q; o[4] = e.s;
+        o[5] = __double_as_longlong(e.lp);
+    }
+    t.n_out++;
+}
+
+// Returns from the FB/BF call in progress to findAllSMEMS.
+__device__ __forceinline__ void smem_return(ThreadSmem& t) {
+    if (t.site == 0) { t.from = t.cf; t.to = t.ct; t.phase = PH_OUTER_LOOP; }
+    else if (t.site == 1) { t.to = t.ct; t.phase = PH_OUTER_BACK; }
+    else { t.from = t.cf; t.phase = PH_OUTER_LOOP; }
+}
+
+__device__ __forceinline__ SmemState smem_init_state(const ThreadSmem& t, int64_t from) {
+    const int b = t.base(from);
+    SmemState m;
+    m.from = from; m.to = from + 1;
+    m.p = 0; m.q = 0; m.s = 0;
+    m.lp = __dadd_rn(0.0, c_llk[b]);
+    return m;
+}
+
+// Enter FB(cf, ct) (SMEM.cpp:64-77).
+__device__ __forceinline__ void smem_call_fb(ThreadSmem& t, const IndexDev& ix, int site, int64_t cf) {
+    t.site = site;
+    t.cf = cf;
+    const int b = t.base(cf);
+    t.ct = cf + 1;
+    if (!is_basic(b)) { smem_return(t); return; }
+    t.m = smem_init_state(t, cf);
+    t.m.p = ix.C[b]; t.m.q = ix.C[comp16(b)]; t.m.s = ix.C[b + 1] - ix.C[b];
+    t.m0 = t.m;
+    t.n_prev = 0;
+    t.phase = PH_FB_WALK;
+}
+
+// Enter BF(cf, ct) (SMEM.cpp:119-132).
+__device__ __forceinline__ void smem_call_bf(ThreadSmem& t, const IndexDev& ix, int64_t cf) {
+    t.site = 2;
+    t.cf = cf;
+    const int b = t.base(cf);
+    t.ct = cf + 1;
+    if (!is_basic(b)) { smem_return(t); return; }
+    t.m = smem_init_state(t, cf);
+    t.m.p = ix.C[b]; t.m.q = ix.C[comp16(b)]; t.m.s = ix.C[b + 1] - ix.C[b];
+    t.m0 = t.m;
+    t.n_prev = 0;
+    t.phase = PH_BF_WALK;
+}
+
+__device__ __forceinline__ void reverse_entries(PrevEntry* pv, int n) {
+    for (int i = 0, j = n - 1; i < j; ++i, --j) { PrevEntry x = pv[i]; pv[i] = pv[j]; pv[j] = x; }
+}
+
+// Advance the state machine until an extension is needed. On return with
+// true, (P,Q,S,B) is a backward extension to perform (forward extensions are
+// expressed as backward ones on the swapped interval).
+__device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const IndexDev& ix, PrevEntry* pv,
+                             int64_t& P, int64_t& Q, int64_t& S, int& B) {
+    for (;;) {
+        switch (t.phase) {
+            case PH_OUTER_LOOP:
+                if (!(t.from > 0 || t.to < t.L)) { t.phase = PH_DONE; return false; }
+                if (t.to < t.L) { smem_call_fb(t, ix, 1, t.to); continue; }
+                t.phase = PH_OUTER_BACK;
+                continue;
+            case PH_OUTER_BACK:
+                t.from -= 1;
+                if (t.from >= 0) { smem_call_bf(t, ix, t.from); continue; }
+                t.phase = PH_OUTER_LOOP;
+                continue;
+            case PH_FB_WALK:
+                if (t.m.s >= 1) {  // fwdExt with the base at `to` (0 past the read end)
+                    const int nb = t.base(t.m.to);
+                    P = t.m.q; Q = t.m.p; S = t.m.s; B = comp16(nb);
+                    return true;
+                }
+                t.ct = t.m.to;
+                if (t.n_prev == 0) { t.cf--; smem_return(t); continue; }
+                reverse_entries(pv, t.n_prev);
+                t.phase = PH_FB_ITER;
+                continue;
+            case PH_FB_ITER:
+                if (!(t.cf >= 0 && t.n_prev > 0)) { smem_return(t); continue; }
+                t.k = 0; t.n_keep = 0; t.s0 = -1; t.n_valid = 0;
+                t.b2 = t.cf > 0 ? t.base(t.cf - 1) : 0;
+                t.phase = PH_FB_ENTRY;
+                continue;
+            case PH_FB_ENTRY:
+                if (t.k == t.n_prev) { t.n_prev = t.n_keep; t.cf--; t.phase = PH_FB_ITER; continue; }
+                t.e0 = pv[t.k];
+                P = t.e0.p; Q = t.e0.q; S = t.e0.s; B = t.b2;
+                return true;
+            case PH_BF_WALK:
+                if (t.m.s >= 1) {
+                    const int nb = t.m.from > 0 ? t.base(t.m.from - 1) : 0;
+                    P = t.m.p; Q = t.m.q; S = t.m.s; B = nb;
+                    return true;
+                }
+                t.cf = t.m.from;
+                if (t.n_prev == 0) { t.ct++; smem_return(t); continue; }
+                reverse_entries(pv, t.n_prev);
+                t.phase = PH_BF_ITER;
+                continue;
+            case PH_BF_ITER:
+                if (!(t.ct <= t.L && t.n_prev > 0)) { smem_return(t); continue; }
+                t.k = 0; t.n_keep = 0; t.s0 = -1; t.n_valid = 0;
+                t.b2 = t.base(t.ct);
+                t.phase = PH_BF_ENTRY;
+                continue;
+            case PH_BF_ENTRY:
+                if (t.k == t.n_prev) { t.n_prev = t.n_keep; t.ct++; t.phase = PH_BF_ITER; continue; }
+                t.e0 = pv[t.k];
+                P = t.e0.q; Q = t.e0.p; S = t.e0.s; B = comp16(t.b2);
+                return true;
+            default:
+                return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void smem_push(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, const SmemState& m,
+                                          int64_t pos) {
+    if (t.n_prev < a.pv_cap) {
+        PrevEntry e;
+        e.p = m.p; e.q = m.q; e.s = m.s; e.lp = m.lp; e.pos = pos;
+        pv[t.n_prev] = e;
+    } else {
+        atomicOr(a.status, kErrOverflow | 0x100u);  // prev capacity: the batch reruns on the warp kernel
+    }
+    t.n_prev++;
+}
+
+// Apply the result of the extension requested by smem_advance.
+__device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, int64_t P, int64_t Q,
+                                           int64_t S) {
+    switch (t.phase) {
+        case PH_FB_WALK: {  // SMEM.cpp:79-86
+            t.m.q = P; t.m.p = Q; t.m.s = S;
+            const int nb = t.base(t.m.to);
+            if (t.m.to < t.L) t.m.lp = __dadd_rn(t.m.lp, c_llk[nb]);
+            t.m.to++;
+            if (t.m.s != t.m0.s && t.m0.to >= a.min_len) {
+                bool sig = a.thr_all != 0;
+                if (!sig) {
+                    double ll = __dadd_rn(0.0, t.m0.lp);
+                    for (int64_t i = 0; i < t.m0.from; ++i) ll = __dadd_rn(ll, c_llk[t.base(i)]);
+                    sig = ll <= a.thr;
+                }
+                if (sig) smem_push(t, a, pv, t.m0, t.m0.to);
+            }
+            t.m0 = t.m;
+            break;
+        }
+        case PH_BF_WALK: {  // SMEM.cpp:134-141
+            t.m.p = P; t.m.q = Q; t.m.s = S;
+            if (t.m.from > 0) t.m.lp = __dadd_rn(t.m.lp, c_llk[t.base(t.m.from - 1)]);
+            t.m.from--;
+            if (t.m.s != t.m0.s && t.L - t.m0.from >= a.min_len) {
+                bool sig = a.thr_all != 0;
+                if (!sig) {
+                    double ll = __dadd_rn(0.0, t.m0.lp);
+                    for (int64_t i = t.m0.to; i < t.L; ++i) ll = __dadd_rn(ll, c_llk[t.base(i)]);
+                    sig = ll <= a.thr;
+                }
+                if (sig) smem_push(t, a, pv, t.m0, t.m0.from);
+            }
+            t.m0 = t.m;
+            break;
+        }
+        case PH_FB_ENTRY:
+        case PH_BF_ENTRY: {  // SMEM.cpp:97-112 / 152-167
+            const bool fb = t.phase == PH_FB_ENTRY;
+            PrevEntry e = t.e0;
+            if (fb) { e.p = P; e.q = Q; } else { e.q = P; e.p = Q; }
+            e.s = S;
+            const bool add = fb ? (t.cf > 0) : (t.ct < t.L);
+            if (add) e.lp = __dadd_rn(e.lp, c_llk[t.b2]);
+            const int64_t e_from = fb ? t.cf : t.e0.pos;
+            const int64_t e_to = fb ? t.e0.pos : t.ct;
+            if (e.s != t.e0.s && t.e0.s >= 1 && t.n_valid == 0 && e_to - e_from >= a.min_len &&
+                (a.thr_all || t.e0.lp <= a.thr))
+                smem_emit(t, a, e_from, e_to, t.e0);
+            if (e.s >= 1 && e.s != t.s0) {
+                t.s0 = e.s;
+                t.n_valid++;
+                pv[t.n_keep++] = e;
+            }
+            t.k++;
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_smem_thread(SmemThreadArgs a, IndexDev ix) {
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    PrevEntry* pv = a.prev + tid * a.pv_cap;
+    ThreadSmem t;
+    t.phase = PH_NEXT_READ;
+    t.ext = 0;
+    t.n_out = 0;
+    t.r = -1;
+    for (;;) {
+        int64_t P = 0, Q = 0, S = 0;
+        int B = 0;
+        bool have = false;
+        while (!have) {
+            if (t.phase == PH_NEXT_READ || t.phase == PH_DONE) {
+                if (t.phase == PH_DONE) {
+                    a.count[t.r] = t.n_out;
+                    if (t.n_out > a.cap) atomicOr(a.status, kErrOverflow);
+                }
+                const unsigned long long r = atomicAdd(a.work, 1ull);
+                if ((int64_t)r >= a.n_reads) { t.phase = -1; break; }
+                t.r = (int64_t)r;
+                const int64_t o0 = a.off[r];
+                t.rd = a.seq + o0;
+                t.L = a.off[r + 1] - o0;
+                t.out = a.out + 6 * (int64_t)r * a.cap;
+                t.n_out = 0;
+                if (t.L <= 0) { t.phase = PH_DONE; continue; }
+                t.from = t.L / 2;  // SMEM.cpp:189-191
+                t.to = t.from + 1;
+                smem_call_fb(t, ix, 0, t.from);
+                continue;
+            }
+            have = smem_advance(t, a, ix, pv, P, Q, S, B);
+        }
+        if (t.phase == -1) break;
+        if (is_basic(B)) t.ext++;
+        back_ext(ix, P, Q, S, B);
+        smem_apply(t, a, pv, P, Q, S);
+    }
+    if (t.ext) atomicAdd(a.n_ext, t.ext);
+}
+
+}  // namespace msg
