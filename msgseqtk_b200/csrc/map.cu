@@ -221,7 +221,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         int bps = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread, 128, 0));
         n_thr = (int64_t)ctx->num_sms * std::max(1, bps) * 128;
-        CK(ctx->prev.ensure(n_thr * pv_cap * sizeof(PrevEntry) + 64));
+        CK(ctx->prev.ensure(n_thr * pv_cap * (sizeof(PrevEntry) + 2 * sizeof(double)) + 64));
         CK(cudaMemcpyToSymbolAsync(c_llk, im.llk, sizeof(im.llk), 0, cudaMemcpyHostToDevice, st));
     } else {
         CK(ctx->prev.ensure(n_warps * pv_cap * (4 + 8 + 8 + 8 + 8) + 64));
@@ -239,6 +239,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             ta.thr = thr; ta.thr_all = thr_all;
             ta.out = ctx->smem.as<int64_t>(); ta.cap = cap; ta.count = ctx->smem_cnt.as<int32_t>();
             ta.prev = ctx->prev.as<PrevEntry>(); ta.pv_cap = pv_cap;
+            ta.llsum = reinterpret_cast<double*>(ta.prev + n_thr * pv_cap);
             ta.work = d_ctr; ta.n_ext = d_ctr + 1; ta.status = d_status;
             if (n_reads > 0) {
                 S.n_launch++, k_smem_thread<<<n_thr / 128, 128, 0, st>>>(ta, ix);

@@ -699,6 +699,14 @@ struct ChainCtx {
         const int lane = lane_id();
         const int32_t o = -(pp.gap_o + pp.gap_e), e = -pp.gap_e;
         const int64_t stripes = (g.R + 31) / 32;
+        // top boundary row (r0, c0+1 .. c0+C) into the stripe hand-off buffer
+        for (int64_t c = lane; c < g.C; c += 32) {
+            const int64_t j = g.c0 + 1 + c;
+            g.rowbuf[c * 3] = M(g.r0, j, m);
+            g.rowbuf[c * 3 + 1] = I(g.r0, j, m);
+            g.rowbuf[c * 3 + 2] = D(g.r0, j, m);
+        }
+        __syncwarp();
         for (int64_t sp = 0; sp < stripes; ++sp) {
             const int64_t rr = sp * 32 + lane;
             const bool row_ok = rr < g.R;
@@ -721,11 +729,7 @@ struct ChainCtx {
                 const int32_t sd_ = __shfl_up_sync(0xffffffffu, pd, 1);
                 const bool act = row_ok && c >= 0 && c < g.C;
                 if (lane == 0) {
-                    if (act) {
-                        const int64_t j = g.c0 + 1 + c;
-                        if (sp == 0) { um = M(i - 1, j, m); ui = I(i - 1, j, m); ud = D(i - 1, j, m); }
-                        else { um = g.rowbuf[c * 3]; ui = g.rowbuf[c * 3 + 1]; ud = g.rowbuf[c * 3 + 2]; }
-                    }
+                    if (act) { um = g.rowbuf[c * 3]; ui = g.rowbuf[c * 3 + 1]; ud = g.rowbuf[c * 3 + 2]; }
                 } else {
                     um = sm_; ui = si_; ud = sd_;
                 }
@@ -970,6 +974,23 @@ __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
             }
             const bool ok = (s == OP_M) ? (i >= 1 && j >= 1) : (s == OP_I) ? (i >= 1) : (j >= 1);
             if (!ok || np >= cap) { flags |= 2; break; }
+            if (s == OP_M && !in_rect && (a.pp.mode == 0 || a.pp.match >= 1)) {
+                // Inside a seed block, diagonal cells d >= 1 have I = D = -inf
+                // (no I-row or D-column overwrite reaches past the block's first
+                // row/column), so matchMax keeps M: walk straight to d = 1.
+                const int mr = x.row_seg(i);
+                if ((mr & 1) && mr == x.col_seg(j)) {
+                    const int k = (mr - 1) >> 1;
+                    const int64_t d = i - x.qf(k) - 1;
+                    if (d == j - x.ts(k) - 1 && d >= 2 && np + d - 1 <= cap) {
+                        for (int64_t q = 0; q < d - 1; ++q) path[np + q] = (uint8_t)OP_M;
+                        np += d - 1;
+                        i -= d - 1;
+                        j -= d - 1;
+                        continue;
+                    }
+                }
+            }
             path[np++] = (uint8_t)s;
             if (s == OP_M) {
                 s = in_rect ? (code & 3) : match_max(x.M(i - 1, j - 1, stage), x.I(i - 1, j - 1, stage), x.D(i - 1, j - 1, stage));

@@ -64,30 +64,27 @@ __device__ inline int64_t dollar_between(const IndexDev& ix, int64_t lo, int64_t
     return a - s;
 }
 
-// Occurrences of $,A,C,G,T in BWT[0 .. i] for -1 <= i < n.
-__device__ inline Occ5 occ5(const IndexDev& ix, int64_t i) {
+// Counts of $,A,C,G,T among the first r symbols of a loaded bucket k.
+__device__ inline Occ5 occ5_in(const IndexDev& ix, int64_t k, int r, const uint4& w0, const uint4& w1,
+                               const uint4& w2, const uint4& w3) {
     Occ5 o;
-    const int64_t j = i + 1;               // exclusive end
-    const int64_t k = j / kBucketSyms;
-    const int r = (int)(j - k * kBucketSyms);
-    const uint4* p = reinterpret_cast<const uint4*>(ix.bkt + k);
-    const uint4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2), w3 = __ldg(p + 3);
     const uint32_t words[12] = {w1.x, w1.y, w1.z, w1.w, w2.x, w2.y, w2.z, w2.w, w3.x, w3.y, w3.z, w3.w};
     uint32_t nA = 0, nC = 0, nG = 0;
+    const int nw = (r + 15) >> 4;
 #pragma unroll
     for (int w = 0; w < 12; ++w) {
-        const int lo = w * 16;
-        uint32_t valid;
-        if (r >= lo + 16) valid = 0x55555555u;
-        else if (r <= lo) valid = 0u;
-        else valid = 0x55555555u & ((1u << (2 * (r - lo))) - 1u);
-        const uint32_t x = words[w];
-        const uint32_t hi = x >> 1, lo_ = x;
-        // code 0 (A): both bits clear; 1 (C): lo set hi clear; 2 (G): hi set lo clear
-        nA += __popc(~lo_ & ~hi & valid);
-        nC += __popc(lo_ & ~hi & valid);
-        nG += __popc(~lo_ & hi & valid);
+        if (w < nw) {
+            const int lo = w * 16;
+            const uint32_t valid = (r >= lo + 16) ? 0x55555555u : (0x55555555u & ((1u << (2 * (r - lo))) - 1u));
+            const uint32_t x = words[w];
+            const uint32_t hi = x >> 1;
+            // code 0 (A or $): both bits clear; 1 (C): low set; 2 (G): high set
+            nA += __popc(~x & ~hi & valid);
+            nC += __popc(x & ~hi & valid);
+            nG += __popc(~x & hi & valid);
+        }
     }
+    const int64_t j = k * kBucketSyms + r;
     const bool has_dollar = (w0.x >> 31) != 0;
     int64_t d_in = 0;
     if (has_dollar && r > 0) d_in = dollar_between(ix, k * kBucketSyms, j);
@@ -97,6 +94,32 @@ __device__ inline Occ5 occ5(const IndexDev& ix, int64_t i) {
     o.c[3] = (int64_t)w0.w + nG;
     o.c[4] = j - o.c[0] - o.c[1] - o.c[2] - o.c[3];
     return o;
+}
+
+// Occurrences of $,A,C,G,T in BWT[0 .. i] for -1 <= i < n.
+__device__ inline Occ5 occ5(const IndexDev& ix, int64_t i) {
+    const int64_t j = i + 1;               // exclusive end
+    const int64_t k = j / kBucketSyms;
+    const int r = (int)(j - k * kBucketSyms);
+    const uint4* p = reinterpret_cast<const uint4*>(ix.bkt + k);
+    const uint4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2), w3 = __ldg(p + 3);
+    return occ5_in(ix, k, r, w0, w1, w2, w3);
+}
+
+// Counts at two rows; one bucket load when both fall in the same bucket.
+__device__ inline void occ5_pair(const IndexDev& ix, int64_t i_lo, int64_t i_hi, Occ5& lo, Occ5& hi) {
+    const int64_t ja = i_lo + 1, jb = i_hi + 1;
+    const int64_t ka = ja / kBucketSyms, kb = jb / kBucketSyms;
+    const uint4* pa = reinterpret_cast<const uint4*>(ix.bkt + ka);
+    const uint4 a0 = __ldg(pa), a1 = __ldg(pa + 1), a2 = __ldg(pa + 2), a3 = __ldg(pa + 3);
+    lo = occ5_in(ix, ka, (int)(ja - ka * kBucketSyms), a0, a1, a2, a3);
+    if (kb == ka) {
+        hi = occ5_in(ix, ka, (int)(jb - ka * kBucketSyms), a0, a1, a2, a3);
+    } else {
+        const uint4* pb = reinterpret_cast<const uint4*>(ix.bkt + kb);
+        const uint4 b0 = __ldg(pb), b1 = __ldg(pb + 1), b2 = __ldg(pb + 2), b3 = __ldg(pb + 3);
+        hi = occ5_in(ix, kb, (int)(jb - kb * kBucketSyms), b0, b1, b2, b3);
+    }
 }
 
 // BWT symbol (nt16) at row i, with its occurrence count in BWT[0 .. i].
@@ -114,8 +137,8 @@ __device__ inline int bwt_at(const IndexDev& ix, int64_t i) {
 __device__ inline int64_t back_ext(const IndexDev& ix, int64_t& p, int64_t& q, int64_t& s, int b) {
     if (!is_basic(b)) return (s = 0);
     const int c = to_int(b);
-    const Occ5 lo = occ5(ix, p - 1);
-    const Occ5 hi = occ5(ix, p + s - 1);
+    Occ5 lo, hi;
+    occ5_pair(ix, p - 1, p + s - 1, lo, hi);
     const int64_t O = lo.c[c];
     int64_t sB[5];
 #pragma unroll

@@ -7,6 +7,8 @@
 // the reference's sequential loop entry by entry (validity by the running
 // size s0, emission while nValid == 0, in-place compaction).
 #pragma once
+#include <math_constants.h>
+
 #include "map_kernels.cuh"
 
 namespace msg {
@@ -29,6 +31,7 @@ struct SmemThreadArgs {
     int32_t* count;
     PrevEntry* prev;        // pv_cap entries per thread
     int64_t pv_cap;
+    double* llsum;          // 2 * pv_cap doubles per thread: prefix and suffix log-likelihood sums
     unsigned long long* work;
     unsigned long long* n_ext;
     uint32_t* status;
@@ -50,6 +53,8 @@ enum SmemPhase : int {
 };
 
 struct ThreadSmem {
+    const double* pre;      // pre[i] = llk[r0] + ... + llk[r(i-1)] (left to right)
+    const double* suf;      // suf[i] = llk[r(L-1)] + ... + llk[r(i)] (right to left)
     const uint8_t* rd;
     int64_t L;
     int64_t* out;
@@ -198,6 +203,26 @@ __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const Index
     }
 }
 
+// SMEM::loglik(from, to) <= thr for the two ranges the walks test
+// (SMEM.cpp:79-81, 134-136): lp plus the bases outside [m.from, m.to) added in
+// read order. The precomputed prefix/suffix sums give the same value up to
+// rounding; both roundings are bounded by (n+2) u sum|terms|, so the sum is
+// made term by term only when the threshold lies within that bound.
+__device__ __forceinline__ bool smem_sig(const ThreadSmem& t, const SmemThreadArgs& a, double lp, bool left,
+                                         int64_t lim) {
+    if (a.thr_all) return true;
+    const double part = left ? t.pre[lim] : t.suf[lim];
+    const double approx = lp + part;
+    if (approx == -CUDART_INF) return true;
+    const int64_t nterm = left ? lim : t.L - lim;
+    const double bound = 4.0 * (double)(nterm + 4) * 1.1102230246251565e-16 * (fabs(lp) + fabs(part)) + 1e-300;
+    if (fabs(approx - a.thr) > bound) return approx <= a.thr;
+    double ll = __dadd_rn(0.0, lp);
+    if (left) { for (int64_t i = 0; i < lim; ++i) ll = __dadd_rn(ll, c_llk[t.base(i)]); }
+    else { for (int64_t i = lim; i < t.L; ++i) ll = __dadd_rn(ll, c_llk[t.base(i)]); }
+    return ll <= a.thr;
+}
+
 __device__ __forceinline__ void smem_push(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, const SmemState& m,
                                           int64_t pos) {
     if (t.n_prev < a.pv_cap) {
@@ -219,15 +244,8 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
             const int nb = t.base(t.m.to);
             if (t.m.to < t.L) t.m.lp = __dadd_rn(t.m.lp, c_llk[nb]);
             t.m.to++;
-            if (t.m.s != t.m0.s && t.m0.to >= a.min_len) {
-                bool sig = a.thr_all != 0;
-                if (!sig) {
-                    double ll = __dadd_rn(0.0, t.m0.lp);
-                    for (int64_t i = 0; i < t.m0.from; ++i) ll = __dadd_rn(ll, c_llk[t.base(i)]);
-                    sig = ll <= a.thr;
-                }
-                if (sig) smem_push(t, a, pv, t.m0, t.m0.to);
-            }
+            if (t.m.s != t.m0.s && t.m0.to >= a.min_len && smem_sig(t, a, t.m0.lp, true, t.m0.from))
+                smem_push(t, a, pv, t.m0, t.m0.to);
             t.m0 = t.m;
             break;
         }
@@ -235,15 +253,8 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
             t.m.p = P; t.m.q = Q; t.m.s = S;
             if (t.m.from > 0) t.m.lp = __dadd_rn(t.m.lp, c_llk[t.base(t.m.from - 1)]);
             t.m.from--;
-            if (t.m.s != t.m0.s && t.L - t.m0.from >= a.min_len) {
-                bool sig = a.thr_all != 0;
-                if (!sig) {
-                    double ll = __dadd_rn(0.0, t.m0.lp);
-                    for (int64_t i = t.m0.to; i < t.L; ++i) ll = __dadd_rn(ll, c_llk[t.base(i)]);
-                    sig = ll <= a.thr;
-                }
-                if (sig) smem_push(t, a, pv, t.m0, t.m0.from);
-            }
+            if (t.m.s != t.m0.s && t.L - t.m0.from >= a.min_len && smem_sig(t, a, t.m0.lp, false, t.m0.to))
+                smem_push(t, a, pv, t.m0, t.m0.from);
             t.m0 = t.m;
             break;
         }
@@ -276,7 +287,11 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
 __global__ void __launch_bounds__(128) k_smem_thread(SmemThreadArgs a, IndexDev ix) {
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     PrevEntry* pv = a.prev + tid * a.pv_cap;
+    double* pre = a.llsum + tid * 2 * a.pv_cap;
+    double* suf = pre + a.pv_cap;
     ThreadSmem t;
+    t.pre = pre;
+    t.suf = suf;
     t.phase = PH_NEXT_READ;
     t.ext = 0;
     t.n_out = 0;
@@ -300,6 +315,14 @@ __global__ void __launch_bounds__(128) k_smem_thread(SmemThreadArgs a, IndexDev 
                 t.out = a.out + 6 * (int64_t)r * a.cap;
                 t.n_out = 0;
                 if (t.L <= 0) { t.phase = PH_DONE; continue; }
+                {
+                    double acc = 0.0;
+                    pre[0] = 0.0;
+                    for (int64_t i = 0; i < t.L; ++i) { acc = __dadd_rn(acc, c_llk[t.base(i)]); pre[i + 1] = acc; }
+                    acc = 0.0;
+                    suf[t.L] = 0.0;
+                    for (int64_t i = t.L - 1; i >= 0; --i) { acc = __dadd_rn(acc, c_llk[t.base(i)]); suf[i] = acc; }
+                }
                 t.from = t.L / 2;  // SMEM.cpp:189-191
                 t.to = t.from + 1;
                 smem_call_fb(t, ix, 0, t.from);
