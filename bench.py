@@ -301,7 +301,8 @@ def main():
     stage_ms = {k: agg[k] for k in ("smem", "locate", "chain", "dp")}
     dom = max(stage_ms, key=stage_ms.get)
     read_bytes = float(reads.offs[min(len(reads), n_batches * bp)]) / n_batches * args.steps
-    smem_bytes = 128.0 * agg["n_ext"] + read_bytes
+    # two 32 B occurrence buckets per bi-interval extension, plus the read bytes
+    smem_bytes = 64.0 * agg["n_ext"] + read_bytes
     achieved = smem_bytes / (agg["smem"] / 1000.0) / 1e9 if agg["smem"] > 0 else 0.0
     roofline = {"kernel": "k_smem (SMEM bi-interval extension)", "bound": "hbm", "achieved": achieved, "peak": hbm,
                 "unit": "GB/s", "frac": achieved / hbm, "traffic": None, "peak_source": peak_note,

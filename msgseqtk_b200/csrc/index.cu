@@ -10,17 +10,17 @@
 
 namespace msg {
 
-// One thread per bucket: pack 192 nt16 BWT symbols into 2-bit codes and count
+// One thread per bucket: pack 64 nt16 BWT symbols into 2-bit codes and count
 // $, A, C, G locally.
 __global__ void k_pack_buckets(const uint8_t* __restrict__ bwt, int64_t n, int64_t nb, Bucket* __restrict__ bkt,
                                uint32_t* __restrict__ cd, uint32_t* __restrict__ ca, uint32_t* __restrict__ cc,
                                uint32_t* __restrict__ cg, uint32_t* __restrict__ bad) {
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= nb) return;
-    uint32_t words[12];
+    uint32_t words[kBucketWords];
     uint32_t nd = 0, na = 0, nc = 0, ng = 0;
     const int64_t base = k * kBucketSyms;
-    for (int w = 0; w < 12; ++w) {
+    for (int w = 0; w < kBucketWords; ++w) {
         uint32_t x = 0;
         for (int t = 0; t < 16; ++t) {
             const int64_t i = base + w * 16 + t;
@@ -40,7 +40,7 @@ __global__ void k_pack_buckets(const uint8_t* __restrict__ bwt, int64_t n, int64
         }
         words[w] = x;
     }
-    for (int w = 0; w < 12; ++w) bkt[k].bits[w] = words[w];
+    for (int w = 0; w < kBucketWords; ++w) bkt[k].bits[w] = words[w];
     cd[k] = nd; ca[k] = na; cc[k] = nc; cg[k] = ng;
 }
 

@@ -221,7 +221,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         int bps = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread, 128, 0));
         n_thr = (int64_t)ctx->num_sms * std::max(1, bps) * 128;
-        CK(ctx->prev.ensure(n_thr * pv_cap * (sizeof(PrevEntry) + 2 * sizeof(double)) + 64));
+        CK(ctx->prev.ensure(n_thr * pv_cap * sizeof(PrevEntry) + 64));
         CK(cudaMemcpyToSymbolAsync(c_llk, im.llk, sizeof(im.llk), 0, cudaMemcpyHostToDevice, st));
     } else {
         CK(ctx->prev.ensure(n_warps * pv_cap * (4 + 8 + 8 + 8 + 8) + 64));
@@ -239,7 +239,6 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             ta.thr = thr; ta.thr_all = thr_all;
             ta.out = ctx->smem.as<int64_t>(); ta.cap = cap; ta.count = ctx->smem_cnt.as<int32_t>();
             ta.prev = ctx->prev.as<PrevEntry>(); ta.pv_cap = pv_cap;
-            ta.llsum = reinterpret_cast<double*>(ta.prev + n_thr * pv_cap);
             ta.work = d_ctr; ta.n_ext = d_ctr + 1; ta.status = d_status;
             if (n_reads > 0) {
                 S.n_launch++, k_smem_thread<<<n_thr / 128, 128, 0, st>>>(ta, ix);
@@ -429,7 +428,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     CK(offsets(ctx, d_cells, h_nchain, d_rect_off, misc, &h_cells));  // d_cells holds bytes per chain
     CK(offsets(ctx, d_pcap, h_nchain, d_path_off, misc, &h_pathtot));
     const int64_t aux_bytes = ((2 * (h_nidx + 1) + h_nchain + 1) * sizeof(int32_t) + 15) / 16 * 16;
-    CK(ctx->scratch.ensure(h_cells + 64 + aux_bytes + (h_nidx + 1) * sizeof(int4)));
+    CK(ctx->scratch.ensure(h_cells + 64 + aux_bytes + (2 * h_nidx + h_nchain + 1) * sizeof(int4)));
     const int64_t P16 = ((h_pathtot + 1 + 15) / 16) * 16;
     CK(ctx->path.ensure(2 * P16 + (h_nchain + 1) * 4 + 64));
     CK(ctx->alnbuf.ensure((h_nchain + 1) * sizeof(msg_aln)));

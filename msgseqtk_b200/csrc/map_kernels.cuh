@@ -174,10 +174,13 @@ struct WarpSmem {
                 m.to++;
                 if (m.s != m0.s && m0.to >= a->min_len) {
                     bool sig = a->thr_all != 0;
-                    if (!sig) {  // SMEM::loglik(0, to) (SMEM.cpp:26-40)
+                    if (!sig) {  // SMEM::loglik(0, to) (SMEM.cpp:26-40); partial sums never increase
                         double ll = __dadd_rn(0.0, m0.lp);
-                        for (int64_t i = 0; i < m0.from; ++i) ll = __dadd_rn(ll, a->llk[base(i)]);
                         sig = ll <= a->thr;
+                        for (int64_t i = 0; i < m0.from && !sig; ++i) {
+                            ll = __dadd_rn(ll, a->llk[base(i)]);
+                            sig = ll <= a->thr;
+                        }
                     }
                     if (sig) push_prev(n_prev, m0, (int32_t)m0.to);
                 }
@@ -215,10 +218,13 @@ struct WarpSmem {
                 m.from--;
                 if (m.s != m0.s && L - m0.from >= a->min_len) {
                     bool sig = a->thr_all != 0;
-                    if (!sig) {  // SMEM::loglik(from, L)
+                    if (!sig) {  // SMEM::loglik(from, L); partial sums never increase
                         double ll = __dadd_rn(0.0, m0.lp);
-                        for (int64_t i = m0.to; i < L; ++i) ll = __dadd_rn(ll, a->llk[base(i)]);
                         sig = ll <= a->thr;
+                        for (int64_t i = m0.to; i < L && !sig; ++i) {
+                            ll = __dadd_rn(ll, a->llk[base(i)]);
+                            sig = ll <= a->thr;
+                        }
                     }
                     if (sig) push_prev(n_prev, m0, (int32_t)m0.from);
                 }
@@ -542,7 +548,7 @@ struct DpParams {
 };
 
 constexpr int kDpWarps = 4;       // warps per block in k_dp
-constexpr int kSmemSeeds = 64;    // chain seeds cached in shared memory per warp
+constexpr int kSmemSeeds = 64;    // chain seeds cached in shared memory per warp (else global)
 
 __device__ __forceinline__ int match_max(int32_t m, int32_t i, int32_t d) {  // Alignment.h:577-589
     int32_t mx = m;
@@ -569,6 +575,8 @@ __device__ __forceinline__ int64_t rect_bytes(int64_t R, int64_t C) {
 
 struct ChainCtx {
     const int4* sd;             // per seed: qf, qt, ts, te (window-relative)
+    const int32_t* rbnd;        // row boundaries b[0..2n+1]: 0, qf_0, qt_0, ..., qf_n-1, qt_n-1, L
+    const int32_t* cbnd;        // column boundaries: 0, ts_0, te_0, ..., T
     int32_t n;                  // seeds in the chain
     int64_t L, T;               // query length, window length
     const uint8_t* query;       // read (FWD) or reverse complement in scratch (REV)
@@ -590,27 +598,17 @@ struct ChainCtx {
         return ((qb & tbb) && qb != 15 && tbb != 15) ? pp.match : -pp.mismatch;
     }
     // row/column boundaries: b[0]=0, b[2k+1]=qf_k, b[2k+2]=qt_k, b[2n+1]=L
-    __device__ int64_t rb(int m) const {
-        if (m <= 0) return 0;
-        if (m >= 2 * n + 1) return L;
-        const int k = (m - 1) >> 1;
-        return (m & 1) ? qf(k) : qt(k);
-    }
-    __device__ int64_t cb(int m) const {
-        if (m <= 0) return 0;
-        if (m >= 2 * n + 1) return T;
-        const int k = (m - 1) >> 1;
-        return (m & 1) ? ts(k) : te(k);
-    }
+    __device__ int64_t rb(int m) const { return rbnd[m]; }
+    __device__ int64_t cb(int m) const { return cbnd[m]; }
     // segment of matrix row i >= 1: smallest m with i <= b[m+1]
     __device__ int row_seg(int64_t i) const {
         int lo = 0, hi = 2 * n;
-        while (lo < hi) { const int mid = (lo + hi) >> 1; if (i <= rb(mid + 1)) hi = mid; else lo = mid + 1; }
+        while (lo < hi) { const int mid = (lo + hi) >> 1; if (i <= rbnd[mid + 1]) hi = mid; else lo = mid + 1; }
         return lo;
     }
     __device__ int col_seg(int64_t j) const {
         int lo = 0, hi = 2 * n;
-        while (lo < hi) { const int mid = (lo + hi) >> 1; if (j <= cb(mid + 1)) hi = mid; else lo = mid + 1; }
+        while (lo < hi) { const int mid = (lo + hi) >> 1; if (j <= cbnd[mid + 1]) hi = mid; else lo = mid + 1; }
         return lo;
     }
     __device__ RectGeo rect(int m) const {
@@ -722,7 +720,8 @@ struct ChainCtx {
             int32_t um = NEG, ui = NEG, ud = NEG;       // up neighbour (i-1, j) of the current step
             int32_t dm = md0, di = id0, dd = dd0;       // diagonal neighbour (i-1, j-1)
             uint8_t* code_base = g.code + sp * (g.C + 31) * 32;
-            for (int64_t t = 0; t < g.C + 31; ++t) {
+            const int64_t rows_here = min((int64_t)32, g.R - sp * 32);  // the last lane with a row
+            for (int64_t t = 0; t < g.C + rows_here - 1; ++t) {
                 const int64_t c = t - lane;
                 const int32_t sm_ = __shfl_up_sync(0xffffffffu, pm, 1);
                 const int32_t si_ = __shfl_up_sync(0xffffffffu, pi, 1);
@@ -840,6 +839,7 @@ __global__ void k_dp_prep(IndexDev ix, const Seed* __restrict__ seeds, const int
 
 __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
     __shared__ int4 s_sd[kDpWarps][kSmemSeeds];
+    __shared__ int32_t s_bnd[kDpWarps][2][2 * kSmemSeeds + 2];
     const int w = threadIdx.x >> 5;
     const int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (c >= a.n_chain) return;
@@ -860,12 +860,25 @@ __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
     x.roff = aux + x.n;
     x.pp = a.pp;
     x.status = a.status;
-    int4* sd = x.n <= kSmemSeeds ? s_sd[w] : a.sdbuf + a.chain_idx_off[c];
+    const bool in_smem = x.n <= kSmemSeeds;
+    int4* gbase = a.sdbuf + 2 * a.chain_idx_off[c] + c;  // 2n+1 int4 per chain when not in shared memory
+    int4* sd = in_smem ? s_sd[w] : gbase;
+    int32_t* rbnd = in_smem ? s_bnd[w][0] : reinterpret_cast<int32_t*>(gbase + x.n);
+    int32_t* cbnd = in_smem ? s_bnd[w][1] : rbnd + 2 * x.n + 2;
     for (int k = lane_id(); k < x.n; k += 32) {
         const Seed s = a.seeds[idx[k]];
-        sd[k] = make_int4(s.from, s.to, (int)(s.start - t_start), (int)(s.end - t_start));
+        const int4 g = make_int4(s.from, s.to, (int)(s.start - t_start), (int)(s.end - t_start));
+        sd[k] = g;
+        rbnd[2 * k + 1] = g.x; rbnd[2 * k + 2] = g.y;
+        cbnd[2 * k + 1] = g.z; cbnd[2 * k + 2] = g.w;
+    }
+    if (lane_id() == 0) {
+        rbnd[0] = 0; cbnd[0] = 0;
+        rbnd[2 * x.n + 1] = (int32_t)x.L; cbnd[2 * x.n + 1] = (int32_t)x.T;
     }
     x.sd = sd;
+    x.rbnd = rbnd;
+    x.cbnd = cbnd;
     const uint8_t* rd = a.rseq + a.roff[r];
     uint8_t* path = a.path + a.path_off[c];
     if (f.strand == FWD) {
@@ -905,12 +918,36 @@ __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
     int s0 = OP_M;
     int32_t flags = 0;
     if (a.pp.mode == 0) {  // backTraceNW: scan the last row, M before I, first strict max
+        // Finite cells of row L are the 3' rectangle's last row plus at most
+        // these: the last seed's diagonal cell when it ends at L, the cell
+        // past a seed ending at L-1, and the I-row copy of that seed's finite
+        // M cells (its diagonal end and the previous seed's past cell). Every
+        // other cell is -inf and cannot win a strict comparison.
         best = NEG;
         bkey = INT64_MAX;
-        for (int64_t j = 1 + lane_id(); j <= x.T; j += 32) {
+        auto consider = [&](int64_t j) {
             const int32_t vm = x.M(x.L, j, stage), vi = x.I(x.L, j, stage);
             if (vm > best || (vm == best && vm != NEG && 2 * j < bkey)) { best = vm; bkey = 2 * j; }
             if (vi > best || (vi == best && vi != NEG && 2 * j + 1 < bkey)) { best = vi; bkey = 2 * j + 1; }
+        };
+        const RectGeo g3 = x.rect(2 * x.n);
+        if (g3.R > 0 && g3.C > 0) {
+            for (int64_t c = lane_id(); c < g3.C; c += 32) {
+                const int64_t j = g3.c0 + 1 + c;
+                const int32_t vm = g3.lastrow[c * 3], vi = g3.lastrow[c * 3 + 1];
+                if (vm > best || (vm == best && vm != NEG && 2 * j < bkey)) { best = vm; bkey = 2 * j; }
+                if (vi > best || (vi == best && vi != NEG && 2 * j + 1 < bkey)) { best = vi; bkey = 2 * j + 1; }
+            }
+        }
+        if (lane_id() == 0) {
+            const int kl = x.n - 1;
+            if (x.qf(kl) < x.L && x.L <= x.qt(kl)) consider(x.ts(kl) + (x.L - x.qf(kl)));
+            const int k = x.seed_by_qt(x.L - 1);
+            if (k >= 0) {
+                if (x.te(k) + 1 <= x.T) consider(x.te(k) + 1);
+                if (x.te(k) >= 1) consider(x.te(k));
+                if (k >= 1 && x.te(k - 1) + 1 >= 1 && x.te(k - 1) + 1 <= x.T) consider(x.te(k - 1) + 1);
+            }
         }
         for (int o = 16; o > 0; o >>= 1) {
             const int32_t ob = __shfl_xor_sync(0xffffffffu, best, o);

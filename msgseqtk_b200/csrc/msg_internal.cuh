@@ -1,11 +1,11 @@
 // Internal device-side layout and primitives of the sm_100a mapping library.
 //
 // Index image in HBM
-//   * occurrence buckets: 64 B each, 192 BWT symbols per bucket.
+//   * occurrence buckets: 32 B each (one DRAM sector), 64 BWT symbols per bucket.
 //       word 0: count of '$' before the bucket (bit 31 set when the bucket holds a '$')
 //       words 1-3: counts of A, C, G before the bucket (T is derived)
-//       words 4-15: 192 symbols x 2 bits (A=0, C=1, G=2, T=3; '$' stored as A)
-//     one 64 B load (4 x 128-bit) gives all five counts at any row.
+//       words 4-7: 64 symbols x 2 bits (A=0, C=1, G=2, T=3; '$' stored as A)
+//     one 32 B load (2 x 128-bit) gives all five counts at any row.
 //   * dollar rows: sorted rows whose BWT symbol is '$' (2 per chromosome).
 //   * full suffix array, uint32 per row (N < 2^32), so locating a row is one
 //     4-byte gather instead of an LF walk.
@@ -16,13 +16,14 @@
 
 namespace msg {
 
-constexpr int kBucketSyms = 192;
+constexpr int kBucketSyms = 64;
+constexpr int kBucketWords = 4;
 
-struct __align__(16) Bucket {
+struct __align__(32) Bucket {
     uint32_t cnt[4];
-    uint32_t bits[12];
+    uint32_t bits[kBucketWords];
 };
-static_assert(sizeof(Bucket) == 64, "bucket must be one 64 B line");
+static_assert(sizeof(Bucket) == 32, "bucket must be one 32 B sector");
 
 // nt16 helpers (DNAalphabet.h:37-191)
 __host__ __device__ inline bool is_basic(int b) { return b == 1 || b == 2 || b == 4 || b == 8; }
@@ -64,26 +65,25 @@ __device__ inline int64_t dollar_between(const IndexDev& ix, int64_t lo, int64_t
     return a - s;
 }
 
-// Counts of $,A,C,G,T among the first r symbols of a loaded bucket k.
-__device__ inline Occ5 occ5_in(const IndexDev& ix, int64_t k, int r, const uint4& w0, const uint4& w1,
-                               const uint4& w2, const uint4& w3) {
+// Counts of $,A,C,G,T among the first r symbols of a loaded bucket k. With
+// lo/hi the low/high code bits of each symbol: T = lo&hi, C = lo-T, G = hi-T,
+// A (and '$') = r - C - G - T.
+__device__ inline Occ5 occ5_in(const IndexDev& ix, int64_t k, int r, const uint4& w0, const uint4& w1) {
     Occ5 o;
-    const uint32_t words[12] = {w1.x, w1.y, w1.z, w1.w, w2.x, w2.y, w2.z, w2.w, w3.x, w3.y, w3.z, w3.w};
-    uint32_t nA = 0, nC = 0, nG = 0;
-    const int nw = (r + 15) >> 4;
+    const uint32_t words[kBucketWords] = {w1.x, w1.y, w1.z, w1.w};
+    uint32_t n_lo = 0, n_hi = 0, n_t = 0;
 #pragma unroll
-    for (int w = 0; w < 12; ++w) {
-        if (w < nw) {
-            const int lo = w * 16;
-            const uint32_t valid = (r >= lo + 16) ? 0x55555555u : (0x55555555u & ((1u << (2 * (r - lo))) - 1u));
-            const uint32_t x = words[w];
-            const uint32_t hi = x >> 1;
-            // code 0 (A or $): both bits clear; 1 (C): low set; 2 (G): high set
-            nA += __popc(~x & ~hi & valid);
-            nC += __popc(x & ~hi & valid);
-            nG += __popc(~x & hi & valid);
-        }
+    for (int w = 0; w < kBucketWords; ++w) {
+        const int nv = min(max(r - 16 * w, 0), 16);
+        const uint32_t m = nv >= 16 ? 0xffffffffu : ((1u << (2 * nv)) - 1u);
+        const uint32_t x = words[w] & m;
+        const uint32_t lo = x & 0x55555555u, hi = (x >> 1) & 0x55555555u;
+        n_lo += __popc(lo);
+        n_hi += __popc(hi);
+        n_t += __popc(lo & hi);
     }
+    const uint32_t nC = n_lo - n_t, nG = n_hi - n_t;
+    const uint32_t nA = (uint32_t)r - nC - nG - n_t;
     const int64_t j = k * kBucketSyms + r;
     const bool has_dollar = (w0.x >> 31) != 0;
     int64_t d_in = 0;
@@ -102,8 +102,8 @@ __device__ inline Occ5 occ5(const IndexDev& ix, int64_t i) {
     const int64_t k = j / kBucketSyms;
     const int r = (int)(j - k * kBucketSyms);
     const uint4* p = reinterpret_cast<const uint4*>(ix.bkt + k);
-    const uint4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2), w3 = __ldg(p + 3);
-    return occ5_in(ix, k, r, w0, w1, w2, w3);
+    const uint4 w0 = __ldg(p), w1 = __ldg(p + 1);
+    return occ5_in(ix, k, r, w0, w1);
 }
 
 // Counts at two rows; one bucket load when both fall in the same bucket.
@@ -111,15 +111,12 @@ __device__ inline void occ5_pair(const IndexDev& ix, int64_t i_lo, int64_t i_hi,
     const int64_t ja = i_lo + 1, jb = i_hi + 1;
     const int64_t ka = ja / kBucketSyms, kb = jb / kBucketSyms;
     const uint4* pa = reinterpret_cast<const uint4*>(ix.bkt + ka);
-    const uint4 a0 = __ldg(pa), a1 = __ldg(pa + 1), a2 = __ldg(pa + 2), a3 = __ldg(pa + 3);
-    lo = occ5_in(ix, ka, (int)(ja - ka * kBucketSyms), a0, a1, a2, a3);
-    if (kb == ka) {
-        hi = occ5_in(ix, ka, (int)(jb - ka * kBucketSyms), a0, a1, a2, a3);
-    } else {
-        const uint4* pb = reinterpret_cast<const uint4*>(ix.bkt + kb);
-        const uint4 b0 = __ldg(pb), b1 = __ldg(pb + 1), b2 = __ldg(pb + 2), b3 = __ldg(pb + 3);
-        hi = occ5_in(ix, kb, (int)(jb - kb * kBucketSyms), b0, b1, b2, b3);
-    }
+    const uint4* pb = reinterpret_cast<const uint4*>(ix.bkt + kb);
+    const uint4 a0 = __ldg(pa), a1 = __ldg(pa + 1);
+    uint4 b0 = a0, b1 = a1;
+    if (kb != ka) { b0 = __ldg(pb); b1 = __ldg(pb + 1); }
+    lo = occ5_in(ix, ka, (int)(ja - ka * kBucketSyms), a0, a1);
+    hi = occ5_in(ix, kb, (int)(jb - kb * kBucketSyms), b0, b1);
 }
 
 // BWT symbol (nt16) at row i, with its occurrence count in BWT[0 .. i].

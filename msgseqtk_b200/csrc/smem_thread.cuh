@@ -13,10 +13,18 @@
 
 namespace msg {
 
+// Interval bounds and sizes are below 2^32 (the index holds fewer than 2^32
+// rows) and read positions below 2^31, so the per-thread state is 32-bit.
 struct PrevEntry {
-    int64_t p, q, s;
     double lp;
-    int64_t pos;  // `to` (fwd-back) or `from` (back-fwd) of the entry
+    uint32_t p, q, s;
+    int32_t pos;  // `to` (fwd-back) or `from` (back-fwd) of the entry
+};
+
+struct SmemState32 {
+    double lp;
+    int32_t from, to;
+    uint32_t p, q, s;
 };
 
 struct SmemThreadArgs {
@@ -31,7 +39,6 @@ struct SmemThreadArgs {
     int32_t* count;
     PrevEntry* prev;        // pv_cap entries per thread
     int64_t pv_cap;
-    double* llsum;          // 2 * pv_cap doubles per thread: prefix and suffix log-likelihood sums
     unsigned long long* work;
     unsigned long long* n_ext;
     uint32_t* status;
@@ -53,32 +60,30 @@ enum SmemPhase : int {
 };
 
 struct ThreadSmem {
-    const double* pre;      // pre[i] = llk[r0] + ... + llk[r(i-1)] (left to right)
-    const double* suf;      // suf[i] = llk[r(L-1)] + ... + llk[r(i)] (right to left)
     const uint8_t* rd;
-    int64_t L;
     int64_t* out;
+    int32_t L;
     int32_t n_out;
-    int64_t r;
+    int32_t r;
     // findAllSMEMS variables and the call in progress
-    int64_t from, to;
-    int site;               // 0: first FB(from,to)  1: FB(from0,to)  2: BF(from,to0)
-    int64_t cf, ct;         // the called function's from/to
+    int32_t from, to;
+    int32_t site;           // 0: first FB(from,to)  1: FB(from0,to)  2: BF(from,to0)
+    int32_t cf, ct;         // the called function's from/to
     // walk state
-    SmemState m, m0;
-    int n_prev;
+    SmemState32 m, m0;
+    int32_t n_prev;
     // pass over prev
-    int k, n_keep;
-    int64_t s0, n_valid;
-    int b2;
+    int32_t k, n_keep, n_valid;
+    uint32_t s0;            // running size; 0 stands for the reference's -1 (sizes compared are >= 1)
+    int32_t b2;
     PrevEntry e0;
-    int phase;
+    int32_t phase;
     unsigned long long ext;
 
-    __device__ int base(int64_t i) const { return (i >= 0 && i < L) ? (int)__ldg(rd + i) : 0; }
+    __device__ int base(int32_t i) const { return (i >= 0 && i < L) ? (int)__ldg(rd + i) : 0; }
 };
 
-__device__ __forceinline__ void smem_emit(ThreadSmem& t, const SmemThreadArgs& a, int64_t from, int64_t to,
+__device__ __forceinline__ void smem_emit(ThreadSmem& t, const SmemThreadArgs& a, int32_t from, int32_t to,
                                           const PrevEntry& e) {
     if (t.n_out < a.cap) {
         int64_t* o = t.out + 6 * (int64_t)t.n_out;
@@ -95,38 +100,36 @@ __device__ __forceinline__ void smem_return(ThreadSmem& t) {
     else { t.from = t.cf; t.phase = PH_OUTER_LOOP; }
 }
 
-__device__ __forceinline__ SmemState smem_init_state(const ThreadSmem& t, int64_t from) {
+__device__ __forceinline__ SmemState32 smem_init_state(const ThreadSmem& t, const IndexDev& ix, int32_t from) {
     const int b = t.base(from);
-    SmemState m;
+    SmemState32 m;
     m.from = from; m.to = from + 1;
-    m.p = 0; m.q = 0; m.s = 0;
+    m.p = (uint32_t)ix.C[b]; m.q = (uint32_t)ix.C[comp16(b)]; m.s = (uint32_t)(ix.C[b + 1] - ix.C[b]);
     m.lp = __dadd_rn(0.0, c_llk[b]);
     return m;
 }
 
 // Enter FB(cf, ct) (SMEM.cpp:64-77).
-__device__ __forceinline__ void smem_call_fb(ThreadSmem& t, const IndexDev& ix, int site, int64_t cf) {
+__device__ __forceinline__ void smem_call_fb(ThreadSmem& t, const IndexDev& ix, int site, int32_t cf) {
     t.site = site;
     t.cf = cf;
     const int b = t.base(cf);
     t.ct = cf + 1;
     if (!is_basic(b)) { smem_return(t); return; }
-    t.m = smem_init_state(t, cf);
-    t.m.p = ix.C[b]; t.m.q = ix.C[comp16(b)]; t.m.s = ix.C[b + 1] - ix.C[b];
+    t.m = smem_init_state(t, ix, cf);
     t.m0 = t.m;
     t.n_prev = 0;
     t.phase = PH_FB_WALK;
 }
 
 // Enter BF(cf, ct) (SMEM.cpp:119-132).
-__device__ __forceinline__ void smem_call_bf(ThreadSmem& t, const IndexDev& ix, int64_t cf) {
+__device__ __forceinline__ void smem_call_bf(ThreadSmem& t, const IndexDev& ix, int32_t cf) {
     t.site = 2;
     t.cf = cf;
     const int b = t.base(cf);
     t.ct = cf + 1;
     if (!is_basic(b)) { smem_return(t); return; }
-    t.m = smem_init_state(t, cf);
-    t.m.p = ix.C[b]; t.m.q = ix.C[comp16(b)]; t.m.s = ix.C[b + 1] - ix.C[b];
+    t.m = smem_init_state(t, ix, cf);
     t.m0 = t.m;
     t.n_prev = 0;
     t.phase = PH_BF_WALK;
@@ -166,7 +169,7 @@ __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const Index
                 continue;
             case PH_FB_ITER:
                 if (!(t.cf >= 0 && t.n_prev > 0)) { smem_return(t); continue; }
-                t.k = 0; t.n_keep = 0; t.s0 = -1; t.n_valid = 0;
+                t.k = 0; t.n_keep = 0; t.s0 = 0; t.n_valid = 0;
                 t.b2 = t.cf > 0 ? t.base(t.cf - 1) : 0;
                 t.phase = PH_FB_ENTRY;
                 continue;
@@ -188,7 +191,7 @@ __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const Index
                 continue;
             case PH_BF_ITER:
                 if (!(t.ct <= t.L && t.n_prev > 0)) { smem_return(t); continue; }
-                t.k = 0; t.n_keep = 0; t.s0 = -1; t.n_valid = 0;
+                t.k = 0; t.n_keep = 0; t.s0 = 0; t.n_valid = 0;
                 t.b2 = t.base(t.ct);
                 t.phase = PH_BF_ENTRY;
                 continue;
@@ -205,26 +208,30 @@ __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const Index
 
 // SMEM::loglik(from, to) <= thr for the two ranges the walks test
 // (SMEM.cpp:79-81, 134-136): lp plus the bases outside [m.from, m.to) added in
-// read order. The precomputed prefix/suffix sums give the same value up to
-// rounding; both roundings are bounded by (n+2) u sum|terms|, so the sum is
-// made term by term only when the threshold lies within that bound.
+// read order. Every term is <= 0 and round-to-nearest of a + b with b <= 0
+// never exceeds a, so the running sum never increases: the exact sequential
+// sum is <= thr as soon as a partial sum is.
 __device__ __forceinline__ bool smem_sig(const ThreadSmem& t, const SmemThreadArgs& a, double lp, bool left,
-                                         int64_t lim) {
+                                         int32_t lim) {
     if (a.thr_all) return true;
-    const double part = left ? t.pre[lim] : t.suf[lim];
-    const double approx = lp + part;
-    if (approx == -CUDART_INF) return true;
-    const int64_t nterm = left ? lim : t.L - lim;
-    const double bound = 4.0 * (double)(nterm + 4) * 1.1102230246251565e-16 * (fabs(lp) + fabs(part)) + 1e-300;
-    if (fabs(approx - a.thr) > bound) return approx <= a.thr;
     double ll = __dadd_rn(0.0, lp);
-    if (left) { for (int64_t i = 0; i < lim; ++i) ll = __dadd_rn(ll, c_llk[t.base(i)]); }
-    else { for (int64_t i = lim; i < t.L; ++i) ll = __dadd_rn(ll, c_llk[t.base(i)]); }
-    return ll <= a.thr;
+    if (ll <= a.thr) return true;
+    if (left) {
+        for (int32_t i = 0; i < lim; ++i) {
+            ll = __dadd_rn(ll, c_llk[t.base(i)]);
+            if (ll <= a.thr) return true;
+        }
+    } else {
+        for (int32_t i = lim; i < t.L; ++i) {
+            ll = __dadd_rn(ll, c_llk[t.base(i)]);
+            if (ll <= a.thr) return true;
+        }
+    }
+    return false;
 }
 
-__device__ __forceinline__ void smem_push(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, const SmemState& m,
-                                          int64_t pos) {
+__device__ __forceinline__ void smem_push(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, const SmemState32& m,
+                                          int32_t pos) {
     if (t.n_prev < a.pv_cap) {
         PrevEntry e;
         e.p = m.p; e.q = m.q; e.s = m.s; e.lp = m.lp; e.pos = pos;
@@ -240,7 +247,7 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
                                            int64_t S) {
     switch (t.phase) {
         case PH_FB_WALK: {  // SMEM.cpp:79-86
-            t.m.q = P; t.m.p = Q; t.m.s = S;
+            t.m.q = (uint32_t)P; t.m.p = (uint32_t)Q; t.m.s = (uint32_t)S;
             const int nb = t.base(t.m.to);
             if (t.m.to < t.L) t.m.lp = __dadd_rn(t.m.lp, c_llk[nb]);
             t.m.to++;
@@ -250,7 +257,7 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
             break;
         }
         case PH_BF_WALK: {  // SMEM.cpp:134-141
-            t.m.p = P; t.m.q = Q; t.m.s = S;
+            t.m.p = (uint32_t)P; t.m.q = (uint32_t)Q; t.m.s = (uint32_t)S;
             if (t.m.from > 0) t.m.lp = __dadd_rn(t.m.lp, c_llk[t.base(t.m.from - 1)]);
             t.m.from--;
             if (t.m.s != t.m0.s && t.L - t.m0.from >= a.min_len && smem_sig(t, a, t.m0.lp, false, t.m0.to))
@@ -262,12 +269,12 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
         case PH_BF_ENTRY: {  // SMEM.cpp:97-112 / 152-167
             const bool fb = t.phase == PH_FB_ENTRY;
             PrevEntry e = t.e0;
-            if (fb) { e.p = P; e.q = Q; } else { e.q = P; e.p = Q; }
-            e.s = S;
+            if (fb) { e.p = (uint32_t)P; e.q = (uint32_t)Q; } else { e.q = (uint32_t)P; e.p = (uint32_t)Q; }
+            e.s = (uint32_t)S;
             const bool add = fb ? (t.cf > 0) : (t.ct < t.L);
             if (add) e.lp = __dadd_rn(e.lp, c_llk[t.b2]);
-            const int64_t e_from = fb ? t.cf : t.e0.pos;
-            const int64_t e_to = fb ? t.e0.pos : t.ct;
+            const int32_t e_from = fb ? t.cf : t.e0.pos;
+            const int32_t e_to = fb ? t.e0.pos : t.ct;
             if (e.s != t.e0.s && t.e0.s >= 1 && t.n_valid == 0 && e_to - e_from >= a.min_len &&
                 (a.thr_all || t.e0.lp <= a.thr))
                 smem_emit(t, a, e_from, e_to, t.e0);
@@ -287,11 +294,7 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
 __global__ void __launch_bounds__(128) k_smem_thread(SmemThreadArgs a, IndexDev ix) {
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     PrevEntry* pv = a.prev + tid * a.pv_cap;
-    double* pre = a.llsum + tid * 2 * a.pv_cap;
-    double* suf = pre + a.pv_cap;
     ThreadSmem t;
-    t.pre = pre;
-    t.suf = suf;
     t.phase = PH_NEXT_READ;
     t.ext = 0;
     t.n_out = 0;
@@ -308,21 +311,13 @@ __global__ void __launch_bounds__(128) k_smem_thread(SmemThreadArgs a, IndexDev 
                 }
                 const unsigned long long r = atomicAdd(a.work, 1ull);
                 if ((int64_t)r >= a.n_reads) { t.phase = -1; break; }
-                t.r = (int64_t)r;
+                t.r = (int32_t)r;
                 const int64_t o0 = a.off[r];
                 t.rd = a.seq + o0;
-                t.L = a.off[r + 1] - o0;
+                t.L = (int32_t)(a.off[r + 1] - o0);
                 t.out = a.out + 6 * (int64_t)r * a.cap;
                 t.n_out = 0;
                 if (t.L <= 0) { t.phase = PH_DONE; continue; }
-                {
-                    double acc = 0.0;
-                    pre[0] = 0.0;
-                    for (int64_t i = 0; i < t.L; ++i) { acc = __dadd_rn(acc, c_llk[t.base(i)]); pre[i + 1] = acc; }
-                    acc = 0.0;
-                    suf[t.L] = 0.0;
-                    for (int64_t i = t.L - 1; i >= 0; --i) { acc = __dadd_rn(acc, c_llk[t.base(i)]); suf[i] = acc; }
-                }
                 t.from = t.L / 2;  // SMEM.cpp:189-191
                 t.to = t.from + 1;
                 smem_call_fb(t, ix, 0, t.from);
