@@ -108,6 +108,25 @@ def dist_setup(args):
     return world, rank, local
 
 
+def reads_seed(rank: int) -> int:
+    """Each rank maps its own pairs (weak scaling; the index is replicated)."""
+    return 1000 + rank
+
+
+def reduce_over_ranks(ms: float, n_reads: float, device) -> tuple[float, float]:
+    """Max of the timed region over ranks and total reads over ranks; the only
+    cross-rank communication of the benchmark (no data-path collective)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return ms, n_reads
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    n = torch.tensor([n_reads], dtype=torch.float64, device=device)
+    dist.all_reduce(n, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(n.item())
+
+
 def make_workload(args, rank, device):
     from msgseqtk_b200 import index_build, synth
     t0 = time.time()
@@ -115,7 +134,7 @@ def make_workload(args, rank, device):
     t1 = time.time()
     view = index_build.build_view(genomes, device=device)
     t2 = time.time()
-    m1, m2 = synth.sample_pairs(genomes, args.pairs, seed=1000 + rank)
+    m1, m2 = synth.sample_pairs(genomes, args.pairs, seed=reads_seed(rank))
     reads = synth.interleave(m1, m2)
     t3 = time.time()
     setup = {"genome_s": round(t1 - t0, 1), "index_s": round(t2 - t1, 1), "reads_s": round(t3 - t2, 1)}
@@ -245,16 +264,7 @@ def main():
     ev1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        n_tot = torch.tensor([agg["n_reads"]], device="cuda", dtype=torch.float64)
-        dist.all_reduce(n_tot)
-        total_reads = float(n_tot.item())
-    else:
-        total_reads = float(agg["n_reads"])
+    ms, total_reads = reduce_over_ranks(ev0.elapsed_time(ev1), float(agg["n_reads"]), "cuda")
     value = total_reads / (ms / 1000.0)
 
     # end to end through the public API: pinned host reads in, host records out
@@ -282,14 +292,7 @@ def main():
         e2e_reads += len(h_offs[k]) - 1
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_e2e = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-        n_tot = torch.tensor([e2e_reads], device="cuda", dtype=torch.float64)
-        dist.all_reduce(n_tot)
-        e2e_reads = float(n_tot.item())
+    ms_e2e, e2e_reads = reduce_over_ranks(e0.elapsed_time(e1), float(e2e_reads), "cuda")
     e2e = {"value": e2e_reads / (ms_e2e / 1000.0), "unit": "reads/s", "h2d_bytes_per_step": int(h2d // args.steps),
            "d2h_bytes_per_step": int(d2h // args.steps)}
 
