@@ -155,6 +155,65 @@ __device__ inline int64_t fwd_ext(const IndexDev& ix, int64_t& p, int64_t& q, in
     return back_ext(ix, q, p, s, comp16(b));
 }
 
+// Occurrences of one base (A,C,G,T: code 0..3) among the first r symbols of a
+// loaded bucket k, 32-bit (rows < 2^32). Stored counts give A, C, G before
+// the bucket; T before it is the rest. '$' is stored as code 0 and removed
+// from A's count.
+__device__ __forceinline__ uint32_t occ1_in(const IndexDev& ix, uint32_t k, uint32_t r, uint32_t code,
+                                            const uint4& w0, const uint4& w1) {
+    const uint32_t words[kBucketWords] = {w1.x, w1.y, w1.z, w1.w};
+    const uint32_t pat = code * 0x55555555u;  // the code in every 2-bit field
+    uint32_t n = 0;
+#pragma unroll
+    for (int w = 0; w < kBucketWords; ++w) {
+        const int nv = min(max((int)r - 16 * w, 0), 16);
+        const uint32_t m = nv >= 16 ? 0x55555555u : (0x55555555u & ((1u << (2 * nv)) - 1u));
+        const uint32_t e = ~(words[w] ^ pat);  // both bits set where the symbol equals the code
+        n += __popc(e & (e >> 1) & m);
+    }
+    const uint32_t dollar = w0.x & 0x7fffffffu;
+    uint32_t before;
+    if (code == 0) before = w0.y;
+    else if (code == 1) before = w0.z;
+    else if (code == 2) before = w0.w;
+    else before = k * (uint32_t)kBucketSyms - dollar - w0.y - w0.z - w0.w;
+    if (code == 0 && (w0.x >> 31) && r > 0)
+        n -= (uint32_t)dollar_between(ix, (int64_t)k * kBucketSyms, (int64_t)k * kBucketSyms + r);
+    return before + n;
+}
+
+// FMDIndex::backExt (FMDIndex.cpp:577-610) on 32-bit bi-intervals. While the
+// size does not change only the extended base is counted at the two rows;
+// the other counts (needed for q) are taken only when it does.
+__device__ inline int64_t back_ext32(const IndexDev& ix, uint32_t& p, uint32_t& q, uint32_t& s, int b) {
+    if (!is_basic(b)) { s = 0; return 0; }
+    const int c = to_int(b);
+    const uint32_t code = (uint32_t)(c - 1);
+    const uint32_t ja = p, jb = p + s;  // exclusive ends of rows p-1 and p+s-1
+    const uint32_t ka = ja >> 6, kb = jb >> 6;
+    const uint4* pa = reinterpret_cast<const uint4*>(ix.bkt + ka);
+    const uint4 a0 = __ldg(pa), a1 = __ldg(pa + 1);
+    uint4 b0 = a0, b1 = a1;
+    if (kb != ka) {
+        const uint4* pb = reinterpret_cast<const uint4*>(ix.bkt + kb);
+        b0 = __ldg(pb); b1 = __ldg(pb + 1);
+    }
+    const uint32_t O = occ1_in(ix, ka, ja & 63u, code, a0, a1);
+    const uint32_t hiO = occ1_in(ix, kb, jb & 63u, code, b0, b1);
+    const uint32_t ns = hiO - O;
+    if (ns == 0) { s = 0; return 0; }
+    if (ns != s) {
+        const Occ5 lo = occ5_in(ix, ka, (int)(ja & 63u), a0, a1);
+        const Occ5 hi = occ5_in(ix, kb, (int)(jb & 63u), b0, b1);
+        uint32_t qq = q + (uint32_t)(hi.c[0] - lo.c[0]);
+        for (int j = 4; j > c; --j) qq += (uint32_t)(hi.c[j] - lo.c[j]);
+        q = qq;
+    }
+    p = (uint32_t)ix.C[b] + O;
+    s = ns;
+    return ns;
+}
+
 // Error bits of the device status word.
 enum : uint32_t {
     kErrInternal = 1u,     // consistency check failed

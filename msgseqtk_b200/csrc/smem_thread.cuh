@@ -72,11 +72,12 @@ struct ThreadSmem {
     // walk state
     SmemState32 m, m0;
     int32_t n_prev;
+    int32_t pv_base;        // the list is pv[pv_base .. pv_base + n_prev), longest first
     // pass over prev
     int32_t k, n_keep, n_valid;
     uint32_t s0;            // running size; 0 stands for the reference's -1 (sizes compared are >= 1)
     int32_t b2;
-    PrevEntry e0;
+    PrevEntry e0, e_next;   // entry being extended, and the next one (loaded early)
     int32_t phase;
     unsigned long long ext;
 
@@ -135,15 +136,11 @@ __device__ __forceinline__ void smem_call_bf(ThreadSmem& t, const IndexDev& ix, 
     t.phase = PH_BF_WALK;
 }
 
-__device__ __forceinline__ void reverse_entries(PrevEntry* pv, int n) {
-    for (int i = 0, j = n - 1; i < j; ++i, --j) { PrevEntry x = pv[i]; pv[i] = pv[j]; pv[j] = x; }
-}
-
 // Advance the state machine until an extension is needed. On return with
 // true, (P,Q,S,B) is a backward extension to perform (forward extensions are
 // expressed as backward ones on the swapped interval).
 __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const IndexDev& ix, PrevEntry* pv,
-                             int64_t& P, int64_t& Q, int64_t& S, int& B) {
+                             uint32_t& P, uint32_t& Q, uint32_t& S, int& B) {
     for (;;) {
         switch (t.phase) {
             case PH_OUTER_LOOP:
@@ -164,18 +161,20 @@ __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const Index
                 }
                 t.ct = t.m.to;
                 if (t.n_prev == 0) { t.cf--; smem_return(t); continue; }
-                reverse_entries(pv, t.n_prev);
+                t.pv_base = (int32_t)a.pv_cap - t.n_prev;
                 t.phase = PH_FB_ITER;
                 continue;
             case PH_FB_ITER:
                 if (!(t.cf >= 0 && t.n_prev > 0)) { smem_return(t); continue; }
                 t.k = 0; t.n_keep = 0; t.s0 = 0; t.n_valid = 0;
                 t.b2 = t.cf > 0 ? t.base(t.cf - 1) : 0;
+                t.e_next = pv[t.pv_base];
                 t.phase = PH_FB_ENTRY;
                 continue;
             case PH_FB_ENTRY:
                 if (t.k == t.n_prev) { t.n_prev = t.n_keep; t.cf--; t.phase = PH_FB_ITER; continue; }
-                t.e0 = pv[t.k];
+                t.e0 = t.e_next;
+                if (t.k + 1 < t.n_prev) t.e_next = pv[t.pv_base + t.k + 1];
                 P = t.e0.p; Q = t.e0.q; S = t.e0.s; B = t.b2;
                 return true;
             case PH_BF_WALK:
@@ -186,18 +185,20 @@ __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const Index
                 }
                 t.cf = t.m.from;
                 if (t.n_prev == 0) { t.ct++; smem_return(t); continue; }
-                reverse_entries(pv, t.n_prev);
+                t.pv_base = (int32_t)a.pv_cap - t.n_prev;
                 t.phase = PH_BF_ITER;
                 continue;
             case PH_BF_ITER:
                 if (!(t.ct <= t.L && t.n_prev > 0)) { smem_return(t); continue; }
                 t.k = 0; t.n_keep = 0; t.s0 = 0; t.n_valid = 0;
                 t.b2 = t.base(t.ct);
+                t.e_next = pv[t.pv_base];
                 t.phase = PH_BF_ENTRY;
                 continue;
             case PH_BF_ENTRY:
                 if (t.k == t.n_prev) { t.n_prev = t.n_keep; t.ct++; t.phase = PH_BF_ITER; continue; }
-                t.e0 = pv[t.k];
+                t.e0 = t.e_next;
+                if (t.k + 1 < t.n_prev) t.e_next = pv[t.pv_base + t.k + 1];
                 P = t.e0.q; Q = t.e0.p; S = t.e0.s; B = comp16(t.b2);
                 return true;
             default:
@@ -230,21 +231,24 @@ __device__ __forceinline__ bool smem_sig(const ThreadSmem& t, const SmemThreadAr
     return false;
 }
 
+// The walks push candidates shortest first; storing them downward from the
+// top of the thread's list leaves pv[pv_base ..] longest first, which is the
+// order the reference gets from std::reverse (SMEM.cpp:90, 145).
 __device__ __forceinline__ void smem_push(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, const SmemState32& m,
                                           int32_t pos) {
     if (t.n_prev < a.pv_cap) {
         PrevEntry e;
         e.p = m.p; e.q = m.q; e.s = m.s; e.lp = m.lp; e.pos = pos;
-        pv[t.n_prev] = e;
+        pv[a.pv_cap - 1 - t.n_prev] = e;
     } else {
-        atomicOr(a.status, kErrOverflow | 0x100u);  // prev capacity: the batch reruns on the warp kernel
+        atomicOr(a.status, kErrOverflow | 0x100u);  // cannot happen: pv_cap exceeds the read length
     }
     t.n_prev++;
 }
 
 // Apply the result of the extension requested by smem_advance.
-__device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, int64_t P, int64_t Q,
-                                           int64_t S) {
+__device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, uint32_t P, uint32_t Q,
+                                           uint32_t S) {
     switch (t.phase) {
         case PH_FB_WALK: {  // SMEM.cpp:79-86
             t.m.q = (uint32_t)P; t.m.p = (uint32_t)Q; t.m.s = (uint32_t)S;
@@ -281,7 +285,7 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
             if (e.s >= 1 && e.s != t.s0) {
                 t.s0 = e.s;
                 t.n_valid++;
-                pv[t.n_keep++] = e;
+                pv[t.pv_base + t.n_keep++] = e;
             }
             t.k++;
             break;
@@ -300,7 +304,7 @@ __global__ void __launch_bounds__(128) k_smem_thread(SmemThreadArgs a, IndexDev 
     t.n_out = 0;
     t.r = -1;
     for (;;) {
-        int64_t P = 0, Q = 0, S = 0;
+        uint32_t P = 0, Q = 0, S = 0;
         int B = 0;
         bool have = false;
         while (!have) {
@@ -327,7 +331,7 @@ __global__ void __launch_bounds__(128) k_smem_thread(SmemThreadArgs a, IndexDev 
         }
         if (t.phase == -1) break;
         if (is_basic(B)) t.ext++;
-        back_ext(ix, P, Q, S, B);
+        back_ext32(ix, P, Q, S, B);
         smem_apply(t, a, pv, P, Q, S);
     }
     if (t.ext) atomicAdd(a.n_ext, t.ext);
