@@ -211,24 +211,28 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     // ---------------- SMEMs ----------------
     // Reads up to 254 bp: one thread per read (k_smem_thread); longer reads:
     // one warp per read with lanes over the candidate list (k_smem).
-    const bool thread_path = Lmax + 2 <= 256;
+    // The thread kernel keeps at most kThreadPrev candidates per read so that
+    // all candidate lists stay in L2; a batch with a longer list reruns on the
+    // warp kernel, whose per-warp lists hold a whole read.
+    constexpr int64_t kThreadPrev = 48;
+    bool thread_path = Lmax + 2 <= 256;
     const int threads = 256;
     const int blocks = ctx->num_sms * 8;
     const int64_t n_warps = (int64_t)blocks * threads / 32;
-    const int64_t pv_cap = Lmax + 2;
+    int64_t pv_cap = thread_path ? std::min<int64_t>(Lmax + 2, kThreadPrev) : Lmax + 2;
     int64_t n_thr = 0;
-    if (thread_path) {
-        int bps = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread, 128, 0));
-        n_thr = (int64_t)ctx->num_sms * std::max(1, bps) * 128;
-        CK(ctx->prev.ensure(n_thr * pv_cap * sizeof(PrevEntry) + 64));
-        CK(cudaMemcpyToSymbolAsync(c_llk, im.llk, sizeof(im.llk), 0, cudaMemcpyHostToDevice, st));
-    } else {
-        CK(ctx->prev.ensure(n_warps * pv_cap * (4 + 8 + 8 + 8 + 8) + 64));
-    }
     int64_t cap = 16;
     int64_t h_nsmem = 0;
-    for (int attempt = 0; attempt < 2; ++attempt) {
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        if (thread_path) {
+            int bps = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread, 128, 0));
+            n_thr = (int64_t)ctx->num_sms * std::max(1, bps) * 128;
+            CK(ctx->prev.ensure(n_thr * pv_cap * sizeof(PrevEntry) + 64));
+            CK(cudaMemcpyToSymbolAsync(c_llk, im.llk, sizeof(im.llk), 0, cudaMemcpyHostToDevice, st));
+        } else {
+            CK(ctx->prev.ensure(n_warps * pv_cap * (4 + 8 + 8 + 8 + 8) + 64));
+        }
         CK(ctx->smem.ensure((size_t)std::max<int64_t>(1, n_reads) * cap * 48));
         CK(ctx->smem_cnt.ensure((n_reads + 1) * sizeof(int32_t)));
         CK(cudaMemsetAsync(d_ctr, 0, 16, st));
@@ -268,9 +272,15 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         uint32_t h_status = 0;
         CK(cudaMemcpyAsync(&h_status, d_status, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        if (h_status & (kErrInternal | 0x100u)) return ctx->fail(MSG_EINTERNAL, "SMEM stage consistency check failed");
+        if (h_status & kErrInternal) return ctx->fail(MSG_EINTERNAL, "SMEM stage consistency check failed");
+        if (h_status & 0x100u) {  // a candidate list outgrew the thread kernel's cap
+            if (!thread_path) return ctx->fail(MSG_EINTERNAL, "SMEM candidate list overflow");
+            thread_path = false;
+            pv_cap = Lmax + 2;
+            continue;
+        }
         if (!(h_status & kErrOverflow)) break;
-        if (attempt == 1) return ctx->fail(MSG_EINTERNAL, "SMEM output overflow after resizing");
+        if (attempt == 2) return ctx->fail(MSG_EINTERNAL, "SMEM output overflow after resizing");
         // rerun with the largest per-read count as capacity
         std::vector<int32_t> cnt(n_reads);
         CK(cudaMemcpy(cnt.data(), ctx->smem_cnt.p, n_reads * 4, cudaMemcpyDeviceToHost));

@@ -73,6 +73,7 @@ struct ThreadSmem {
     SmemState32 m, m0;
     int32_t n_prev;
     int32_t pv_base;        // the list is pv[pv_base .. pv_base + n_prev), longest first
+    int32_t ovf;            // a push found the list full: this read is abandoned (the batch reruns)
     // pass over prev
     int32_t k, n_keep, n_valid;
     uint32_t s0;            // running size; 0 stands for the reference's -1 (sizes compared are >= 1)
@@ -160,6 +161,7 @@ __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const Index
                     return true;
                 }
                 t.ct = t.m.to;
+                if (t.ovf) { t.phase = PH_DONE; return false; }
                 if (t.n_prev == 0) { t.cf--; smem_return(t); continue; }
                 t.pv_base = (int32_t)a.pv_cap - t.n_prev;
                 t.phase = PH_FB_ITER;
@@ -184,6 +186,7 @@ __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const Index
                     return true;
                 }
                 t.cf = t.m.from;
+                if (t.ovf) { t.phase = PH_DONE; return false; }
                 if (t.n_prev == 0) { t.ct++; smem_return(t); continue; }
                 t.pv_base = (int32_t)a.pv_cap - t.n_prev;
                 t.phase = PH_BF_ITER;
@@ -240,10 +243,11 @@ __device__ __forceinline__ void smem_push(ThreadSmem& t, const SmemThreadArgs& a
         PrevEntry e;
         e.p = m.p; e.q = m.q; e.s = m.s; e.lp = m.lp; e.pos = pos;
         pv[a.pv_cap - 1 - t.n_prev] = e;
+        t.n_prev++;
     } else {
-        atomicOr(a.status, kErrOverflow | 0x100u);  // cannot happen: pv_cap exceeds the read length
+        atomicOr(a.status, 0x100u);  // list longer than the cap: the batch reruns on the warp kernel
+        t.ovf = 1;
     }
-    t.n_prev++;
 }
 
 // Apply the result of the extension requested by smem_advance.
@@ -303,24 +307,26 @@ __global__ void __launch_bounds__(128) k_smem_thread(SmemThreadArgs a, IndexDev 
     t.ext = 0;
     t.n_out = 0;
     t.r = -1;
+    bool alive = true;  // this lane still has reads to take
     for (;;) {
         uint32_t P = 0, Q = 0, S = 0;
         int B = 0;
         bool have = false;
-        while (!have) {
+        while (alive && !have) {
             if (t.phase == PH_NEXT_READ || t.phase == PH_DONE) {
                 if (t.phase == PH_DONE) {
                     a.count[t.r] = t.n_out;
                     if (t.n_out > a.cap) atomicOr(a.status, kErrOverflow);
                 }
                 const unsigned long long r = atomicAdd(a.work, 1ull);
-                if ((int64_t)r >= a.n_reads) { t.phase = -1; break; }
+                if ((int64_t)r >= a.n_reads) { alive = false; break; }
                 t.r = (int32_t)r;
                 const int64_t o0 = a.off[r];
                 t.rd = a.seq + o0;
                 t.L = (int32_t)(a.off[r + 1] - o0);
                 t.out = a.out + 6 * (int64_t)r * a.cap;
                 t.n_out = 0;
+                t.ovf = 0;
                 if (t.L <= 0) { t.phase = PH_DONE; continue; }
                 t.from = t.L / 2;  // SMEM.cpp:189-191
                 t.to = t.from + 1;
@@ -329,10 +335,16 @@ __global__ void __launch_bounds__(128) k_smem_thread(SmemThreadArgs a, IndexDev 
             }
             have = smem_advance(t, a, ix, pv, P, Q, S, B);
         }
-        if (t.phase == -1) break;
-        if (is_basic(B)) t.ext++;
-        back_ext32(ix, P, Q, S, B);
-        smem_apply(t, a, pv, P, Q, S);
+        // Reconverge the warp so that every lane with a pending extension
+        // issues its bucket loads in the same instructions.
+        __syncwarp();
+        if (!__any_sync(0xffffffffu, alive)) break;
+        if (have) {
+            if (is_basic(B)) t.ext++;
+            back_ext32(ix, P, Q, S, B);
+        }
+        __syncwarp();
+        if (have) smem_apply(t, a, pv, P, Q, S);
     }
     if (t.ext) atomicAdd(a.n_ext, t.ext);
 }
