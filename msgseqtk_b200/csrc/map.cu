@@ -414,7 +414,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     tm.mark();  // 3
 
     // ---------------- DP ----------------
-    CK(ctx->dpinfo.ensure((h_nchain + 1) * 8 * 8 + 64));
+    CK(ctx->dpinfo.ensure((h_nchain + 1) * 8 * 11 + 64));
     int64_t* d_ts = ctx->dpinfo.as<int64_t>();
     int64_t* d_te = d_ts + (h_nchain + 1);
     int64_t* d_cells = d_te + (h_nchain + 1);
@@ -423,10 +423,17 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     int64_t* d_path_off = d_rect_off + (h_nchain + 1);
     int64_t* d_dpcells = d_path_off + (h_nchain + 1);
     int64_t* d_ncig = d_dpcells + (h_nchain + 1);
+    int64_t* d_area = d_ncig + (h_nchain + 1);
+    int64_t* d_small = d_area + (h_nchain + 1);
+    int64_t* d_big = d_small + (h_nchain + 1);
+    unsigned long long* d_nlist = reinterpret_cast<unsigned long long*>(d_big + (h_nchain + 1));
     int64_t h_cells = 0, h_pathtot = 0;
     if (h_nchain > 0) {
         S.n_launch++, k_dp_prep<<<nblk(h_nchain, 256), 256, 0, st>>>(ix, d_seeds, d_cidx_off, d_clen, d_cread, d_cidx, d_off, h_nchain,
-                                                       d_ts, d_te, d_cells, d_pcap, d_dpcells);
+                                                       d_ts, d_te, d_cells, d_pcap, d_dpcells, d_area);
+        CK(cudaGetLastError());
+        CK(cudaMemsetAsync(d_nlist, 0, 16, st));
+        S.n_launch++, k_dp_split<<<nblk(h_nchain, 256), 256, 0, st>>>(d_area, h_nchain, d_small, d_big, d_nlist);
         CK(cudaGetLastError());
         // total reference cells for the stats
         size_t tb = 0;
@@ -456,6 +463,11 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         da.t_end = d_te; da.scr_off = d_rect_off; da.scr = d_scr; da.aux = d_aux; da.sdbuf = d_sdbuf;
         da.qbuf = d_qbuf; da.path_off = d_path_off; da.path = d_path; da.path_len = d_plen; da.aln = d_aln;
         da.pp = dpp; da.status = d_status;
+        // Both launches are sized for every chain; each reads its list length on
+        // the device, so no host round trip is needed for the split.
+        da.list = d_small; da.n_list = d_nlist;
+        S.n_launch++, k_dp_small<<<nblk(h_nchain, 128), 128, 0, st>>>(da);
+        da.list = d_big; da.n_list = d_nlist + 1;
         S.n_launch++, k_dp<<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
         CK(cudaGetLastError());
     }

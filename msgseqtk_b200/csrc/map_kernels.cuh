@@ -687,6 +687,51 @@ struct ChainCtx {
         return NEG;
     }
 
+    // Single-thread fill of rectangle m, row by row, into the same code layout
+    // (rowbuf holds the row above).
+    __device__ void fill_rect_thread(int m, int32_t& best, int64_t& bkey) {
+        const RectGeo g = rect(m);
+        if (g.R <= 0 || g.C <= 0) return;
+        const int32_t o = -(pp.gap_o + pp.gap_e), e = -pp.gap_e;
+        for (int64_t c = 0; c < g.C; ++c) {
+            const int64_t j = g.c0 + 1 + c;
+            g.rowbuf[c * 3] = M(g.r0, j, m);
+            g.rowbuf[c * 3 + 1] = I(g.r0, j, m);
+            g.rowbuf[c * 3 + 2] = D(g.r0, j, m);
+        }
+        for (int64_t rr = 0; rr < g.R; ++rr) {
+            const int64_t i = g.r0 + 1 + rr;
+            int32_t ml = M(i, g.c0, m), dl = D(i, g.c0, m);
+            int32_t dm = M(i - 1, g.c0, m), di = I(i - 1, g.c0, m), dd = D(i - 1, g.c0, m);
+            const int qb = query[i - 1];
+            const int64_t lane = rr & 31;
+            uint8_t* code_base = g.code + (rr >> 5) * (g.C + 31) * 32;
+            for (int64_t c = 0; c < g.C; ++c) {
+                const int32_t um = g.rowbuf[c * 3], ui = g.rowbuf[c * 3 + 1], ud = g.rowbuf[c * 3 + 2];
+                const int64_t j = g.c0 + 1 + c;
+                const int s = score(qb, tb(j - 1));
+                const int32_t mx = max(max(dm, dd), di);
+                int32_t mv = add_s(mx, s);
+                if (pp.mode == 1) mv = max(mv, 0);
+                const int32_t a1 = sat_add(um, o), a2 = sat_add(ui, e);
+                const int32_t iv = max(a1, a2);
+                const int32_t b1 = sat_add(ml, o), b2 = sat_add(dl, e);
+                const int32_t dv = max(b1, b2);
+                code_base[(c + lane) * 32 + lane] = (uint8_t)(match_max(dm, di, dd) | ((a1 > a2) ? 4 : 0) |
+                                                            ((b1 > b2) ? 8 : 0) | (mv > 0 ? 16 : 0));
+                if (rr == g.R - 1) { g.lastrow[c * 3] = mv; g.lastrow[c * 3 + 1] = iv; g.lastrow[c * 3 + 2] = dv; }
+                if (c == g.C - 1) { g.lastcol[rr * 3] = mv; g.lastcol[rr * 3 + 1] = iv; g.lastcol[rr * 3 + 2] = dv; }
+                if (pp.mode == 1) {
+                    const int64_t key = j * (L + 1) + i;
+                    if (mv > best || (mv == best && key < bkey)) { best = mv; bkey = key; }
+                }
+                dm = um; di = ui; dd = ud;
+                g.rowbuf[c * 3] = mv; g.rowbuf[c * 3 + 1] = iv; g.rowbuf[c * 3 + 2] = dv;
+                ml = mv; dl = dv;
+            }
+        }
+    }
+
     // Warp fill of rectangle m (Alignment::calculateScoresNW/SW,
     // Alignment.cpp:72-133): stripes of 32 rows, lane = row, one column per
     // step along the anti-diagonal wavefront; values travel by shuffles.
@@ -787,6 +832,8 @@ struct DpArgs {
     msg_aln* aln;
     DpParams pp;
     uint32_t* status;
+    const int64_t* list;                  // chains handled by this launch
+    const unsigned long long* n_list;     // its length, on the device
 };
 
 // Alignment ctor window (Alignment.cpp:46-52): tStart = max(0, (int64)(start - 1.1*from)),
@@ -796,7 +843,7 @@ __global__ void k_dp_prep(IndexDev ix, const Seed* __restrict__ seeds, const int
                           const int32_t* __restrict__ chain_len, const int32_t* __restrict__ chain_read,
                           const int64_t* __restrict__ chain_idx, const int64_t* __restrict__ roff, int64_t n_chain,
                           int64_t* __restrict__ t_start, int64_t* __restrict__ t_end, int64_t* __restrict__ bytes,
-                          int64_t* __restrict__ pathcap, int64_t* __restrict__ dpcells) {
+                          int64_t* __restrict__ pathcap, int64_t* __restrict__ dpcells, int64_t* __restrict__ area_out) {
     const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (c >= n_chain) return;
     const int64_t* idx = chain_idx + chain_idx_off[c];
@@ -835,14 +882,15 @@ __global__ void k_dp_prep(IndexDev ix, const Seed* __restrict__ seeds, const int
     bytes[c] = by;
     pathcap[c] = L + T + 1;
     dpcells[c] = area + diag;
+    if (area_out) area_out[c] = area;
 }
 
-__global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
-    __shared__ int4 s_sd[kDpWarps][kSmemSeeds];
-    __shared__ int32_t s_bnd[kDpWarps][2][2 * kSmemSeeds + 2];
-    const int w = threadIdx.x >> 5;
-    const int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (c >= a.n_chain) return;
+// One chain: a warp (WARP = true; lanes share the rectangle wavefront and the
+// last-row scan) or a single thread (chains whose rectangles are all small).
+template <bool WARP>
+__device__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, int32_t* cbnd) {
+    const int lane = WARP ? lane_id() : 0;
+    const int stride = WARP ? 32 : 1;
     ChainCtx x;
     const int64_t* idx = a.chain_idx + a.chain_idx_off[c];
     x.n = a.chain_len[c];
@@ -860,19 +908,14 @@ __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
     x.roff = aux + x.n;
     x.pp = a.pp;
     x.status = a.status;
-    const bool in_smem = x.n <= kSmemSeeds;
-    int4* gbase = a.sdbuf + 2 * a.chain_idx_off[c] + c;  // 2n+1 int4 per chain when not in shared memory
-    int4* sd = in_smem ? s_sd[w] : gbase;
-    int32_t* rbnd = in_smem ? s_bnd[w][0] : reinterpret_cast<int32_t*>(gbase + x.n);
-    int32_t* cbnd = in_smem ? s_bnd[w][1] : rbnd + 2 * x.n + 2;
-    for (int k = lane_id(); k < x.n; k += 32) {
+    for (int k = lane; k < x.n; k += stride) {
         const Seed s = a.seeds[idx[k]];
         const int4 g = make_int4(s.from, s.to, (int)(s.start - t_start), (int)(s.end - t_start));
         sd[k] = g;
         rbnd[2 * k + 1] = g.x; rbnd[2 * k + 2] = g.y;
         cbnd[2 * k + 1] = g.z; cbnd[2 * k + 2] = g.w;
     }
-    if (lane_id() == 0) {
+    if (lane == 0) {
         rbnd[0] = 0; cbnd[0] = 0;
         rbnd[2 * x.n + 1] = (int32_t)x.L; cbnd[2 * x.n + 1] = (int32_t)x.T;
     }
@@ -885,11 +928,11 @@ __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
         x.query = rd;
     } else {  // PrimarySeq::revcom
         uint8_t* qb = a.qbuf + a.path_off[c];
-        for (int64_t i = lane_id(); i < x.L; i += 32) qb[i] = (uint8_t)comp16(rd[x.L - 1 - i]);
+        for (int64_t i = lane; i < x.L; i += stride) qb[i] = (uint8_t)comp16(rd[x.L - 1 - i]);
         x.query = qb;
     }
-    __syncwarp();
-    if (lane_id() == 0) {  // byte offsets of rectangles 0..n in this chain's storage
+    if (WARP) __syncwarp();
+    if (lane == 0) {  // byte offsets of rectangles 0..n in this chain's storage
         int64_t off = 0;
         for (int q = 0; q <= x.n; ++q) {
             const int m = 2 * q;
@@ -897,22 +940,31 @@ __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
             off += rect_bytes(x.rb(m + 1) - x.rb(m), x.cb(m + 1) - x.cb(m));
         }
     }
-    __syncwarp();
+    if (WARP) __syncwarp();
     int32_t best = 0;       // local mode: M(0,0) = 0 is the first candidate
     int64_t bkey = 0;
-    x.fill_rect(0, best, bkey);
+    if (WARP) x.fill_rect(0, best, bkey); else x.fill_rect_thread(0, best, bkey);
     for (int k = 0; k < x.n; ++k) {
         const int m = 2 * k + 1;
-        if (lane_id() == 0) {  // first diagonal cell (Alignment.cpp:146-153): max(M,D,I + s, 0)
+        if (lane == 0) {  // first diagonal cell (Alignment.cpp:146-153): max(M,D,I + s, 0)
             const int64_t i = x.qf(k), j = x.ts(k);
             const int32_t mx = max(max(x.M(i, j, m), x.D(i, j, m)), x.I(i, j, m));
             x.diag[k] = max(add_s(mx, a.pp.match), 0);
         }
-        __syncwarp();
-        x.fill_rect(m + 1, best, bkey);
+        if (WARP) __syncwarp();
+        if (WARP) x.fill_rect(m + 1, best, bkey); else x.fill_rect_thread(m + 1, best, bkey);
     }
-    __syncwarp();
+    if (WARP) __syncwarp();
     const int stage = 2 * x.n + 2;
+    auto reduce = [&]() {
+        if (WARP) {
+            for (int o = 16; o > 0; o >>= 1) {
+                const int32_t ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int64_t ok = __shfl_xor_sync(0xffffffffu, bkey, o);
+                if (ob > best || (ob == best && ok < bkey)) { best = ob; bkey = ok; }
+            }
+        }
+    };
     // ---- traceback ----
     int64_t aln_to = 0, aln_end = 0;
     int s0 = OP_M;
@@ -932,14 +984,14 @@ __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
         };
         const RectGeo g3 = x.rect(2 * x.n);
         if (g3.R > 0 && g3.C > 0) {
-            for (int64_t c = lane_id(); c < g3.C; c += 32) {
+            for (int64_t c = lane; c < g3.C; c += stride) {
                 const int64_t j = g3.c0 + 1 + c;
                 const int32_t vm = g3.lastrow[c * 3], vi = g3.lastrow[c * 3 + 1];
                 if (vm > best || (vm == best && vm != NEG && 2 * j < bkey)) { best = vm; bkey = 2 * j; }
                 if (vi > best || (vi == best && vi != NEG && 2 * j + 1 < bkey)) { best = vi; bkey = 2 * j + 1; }
             }
         }
-        if (lane_id() == 0) {
+        if (lane == 0) {
             const int kl = x.n - 1;
             if (x.qf(kl) < x.L && x.L <= x.qt(kl)) consider(x.ts(kl) + (x.L - x.qf(kl)));
             const int k = x.seed_by_qt(x.L - 1);
@@ -949,11 +1001,7 @@ __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
                 if (k >= 1 && x.te(k - 1) + 1 >= 1 && x.te(k - 1) + 1 <= x.T) consider(x.te(k - 1) + 1);
             }
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            const int32_t ob = __shfl_xor_sync(0xffffffffu, best, o);
-            const int64_t ok = __shfl_xor_sync(0xffffffffu, bkey, o);
-            if (ob > best || (ob == best && ok < bkey)) { best = ob; bkey = ok; }
-        }
+        reduce();
         aln_to = x.L;
         if (best == NEG) { aln_end = 0; s0 = OP_M; flags |= 1; }
         else { aln_end = bkey >> 1; s0 = (bkey & 1) ? OP_I : OP_M; }
@@ -964,11 +1012,11 @@ __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
         };
         for (int k = 0; k < x.n; ++k) {
             const int64_t len = x.qt(k) - x.qf(k);
-            for (int64_t d = lane_id(); d < len; d += 32) {
+            for (int64_t d = lane; d < len; d += stride) {
                 const int64_t i = x.qf(k) + 1 + d, j = x.ts(k) + 1 + d;
                 consider(i, j, x.M(i, j, stage));
             }
-            if (lane_id() == 0) {
+            if (lane == 0) {
                 const int64_t i = x.qt(k) + 1, j = x.te(k) + 1;
                 if (i <= x.L && j <= x.T) {
                     const int mr = x.row_seg(i);
@@ -976,16 +1024,12 @@ __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
                 }
             }
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            const int32_t ob = __shfl_xor_sync(0xffffffffu, best, o);
-            const int64_t ok = __shfl_xor_sync(0xffffffffu, bkey, o);
-            if (ob > best || (ob == best && ok < bkey)) { best = ob; bkey = ok; }
-        }
+        reduce();
         aln_to = bkey % (x.L + 1);
         aln_end = bkey / (x.L + 1);
         s0 = OP_M;
     }
-    if (lane_id() == 0) {
+    if (lane == 0) {
         const int32_t go = a.pp.gap_o, ge = a.pp.gap_e;
         int64_t i = aln_to, j = aln_end;
         int s = s0;
@@ -1059,6 +1103,45 @@ __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
         o.flags = flags;
         if (flags & 2) atomicOr(a.status, kErrTrace);
     }
+}
+
+
+__global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
+    __shared__ int4 s_sd[kDpWarps][kSmemSeeds];
+    __shared__ int32_t s_bnd[kDpWarps][2][2 * kSmemSeeds + 2];
+    const int w = threadIdx.x >> 5;
+    const int64_t wi = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (wi >= (int64_t)*a.n_list) return;
+    const int64_t c = a.list[wi];
+    const int n = a.chain_len[c];
+    int4* gbase = a.sdbuf + 2 * a.chain_idx_off[c] + c;  // 2n+1 int4 per chain when not in shared memory
+    const bool in_smem = n <= kSmemSeeds;
+    int4* sd = in_smem ? s_sd[w] : gbase;
+    int32_t* rbnd = in_smem ? s_bnd[w][0] : reinterpret_cast<int32_t*>(gbase + n);
+    int32_t* cbnd = in_smem ? s_bnd[w][1] : rbnd + 2 * n + 2;
+    dp_chain<true>(a, c, sd, rbnd, cbnd);
+}
+
+// Chains whose rectangles are all small: one thread each.
+__global__ void __launch_bounds__(128) k_dp_small(DpArgs a) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)*a.n_list) return;
+    const int64_t c = a.list[t];
+    const int n = a.chain_len[c];
+    int4* gbase = a.sdbuf + 2 * a.chain_idx_off[c] + c;
+    int32_t* rbnd = reinterpret_cast<int32_t*>(gbase + n);
+    dp_chain<false>(a, c, gbase, rbnd, rbnd + 2 * n + 2);
+}
+
+// Split chains into the thread path (total rectangle area <= kSmallArea) and
+// the warp path.
+constexpr int64_t kSmallArea = 256;
+__global__ void k_dp_split(const int64_t* __restrict__ area, int64_t n_chain, int64_t* __restrict__ small,
+                           int64_t* __restrict__ big, unsigned long long* __restrict__ counts) {
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= n_chain) return;
+    if (area[c] <= kSmallArea) small[atomicAdd(&counts[0], 1ull)] = c;
+    else big[atomicAdd(&counts[1], 1ull)] = c;
 }
 
 // CIGAR runs (Alignment::getAlnCigar): 5' clip, the reversed path in runs, 3' clip.
