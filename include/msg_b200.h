@@ -87,6 +87,24 @@ typedef struct msg_map_params {
     int32_t mode;           /* 0 = GLOBAL (NW, default), 1 = LOCAL (SW) */
     /* ScoreScheme (src/ScoreScheme.cpp:14-18); integral values only */
     double match, mismatch, gap_open, gap_ext;
+    /* Alignment::filter (src/Alignment.cpp:548-555; --min-score, default
+     * 0.65 in msgseqtk-align): records with alnScore < read length *
+     * min_score_rate are removed on the device, as the reference does right
+     * after buildAlignments (src/msgseqtk-align.cpp:628, 704-705). A negative
+     * value (the default here) keeps every record buildAlignments makes. */
+    double min_score_rate;
+    /* DP cells of the 5' and 3' flank rectangles (GLOBAL mode only):
+     * 0 = the reference's whole rectangles (default); 1 = a diagonal band of
+     * half-width band_w around the adjacent seed's diagonal; 2 = a band width
+     * chosen per chain by the model loaded with msg_band_model_set. A banded
+     * chain is kept only under a score-bound certificate: either no path
+     * through a cell outside the band can reach the banded score (the record
+     * is then the reference's), or no path at all can reach the filter's
+     * threshold (the reference would filter the record; needs
+     * min_score_rate >= 0). Any other chain is recomputed on the whole cell
+     * set, so the records never depend on the band. */
+    int32_t band_mode;
+    int32_t band_w;
 } msg_map_params;
 
 /* Fill defaults. */
@@ -155,6 +173,11 @@ typedef struct msg_map_stats {
     int64_t host_sorted;    /* reads whose SMEM order needed the host std::sort */
     int64_t n_launch;       /* kernels of this library launched by the call */
     double ms_total, ms_smem, ms_locate, ms_chain, ms_dp;
+    int64_t dp_cells_done;  /* DP cells actually computed (bands, whole rectangles, recomputations) */
+    int64_t n_band_exact;   /* banded chains certified identical to the reference */
+    int64_t n_band_drop;    /* banded chains certified below the filter threshold */
+    int64_t n_band_fallback;/* banded chains recomputed on the whole cell set */
+    int64_t n_filtered;     /* records removed by min_score_rate (drops included) */
 } msg_map_stats;
 
 /* Map a batch of reads held in HOST memory: the per-read SE task body
@@ -204,6 +227,51 @@ int msg_ctx_stream(const msg_ctx* ctx, void** stream);
 #define MSG_NOALLOC_WARPS 1184
 int msg_smem_batch_noalloc(msg_ctx* ctx, int64_t n_reads, const uint8_t* d_seq, const int64_t* d_off,
                            const msg_map_params* params, int64_t* d_smem, int64_t cap_per_read, int32_t* d_count);
+
+/* ---- Learned band model ----
+ * No counterpart in the reference (its DP always uses the whole rectangles).
+ * The model is a 16 -> 64 -> 64 -> 4 ReLU network over chain statistics whose
+ * classes are band half-widths 7, 15, 31 and "whole rectangle". Parameters
+ * are MSG_BAND_NPARAMS floats: feature mean[16], feature scale[16], W1[64][16],
+ * b1[64], W2[64][64], b2[64], W3[4][64], b3[4]; weights are used in bf16 with
+ * fp32 accumulation. */
+#define MSG_BAND_FEATURES 16
+#define MSG_BAND_HIDDEN 64
+#define MSG_BAND_CLASSES 4
+#define MSG_BAND_NPARAMS 5540
+
+/* Load parameters (host floats) for band_mode 2. */
+int msg_band_model_set(msg_ctx* ctx, const float* params, int64_t n_params);
+
+/* Training data from a batch: per chain (in record order of msg_map_batch),
+ * MSG_BAND_FEATURES features and the label = the class whose DP costs the
+ * fewest cells once certified (an uncertified band costs its cells plus the
+ * whole rectangles; ties go to the wider class), with the certificate of
+ * `params` (min_score_rate included). Host buffers of cap chains;
+ * *n_chain receives the chain count (MSG_EINVAL when it exceeds cap). */
+int msg_band_collect(msg_ctx* ctx, const msg_read_batch* reads, const msg_map_params* params, float* feat,
+                     int32_t* label, int64_t cap, int64_t* n_chain);
+
+typedef struct msg_band_train_params {
+    int32_t epochs;
+    int32_t batch;          /* samples per Adam step */
+    float lr;               /* Adam step size (beta1 0.9, beta2 0.999, eps 1e-8) */
+    uint64_t seed;          /* initialisation and shuffling */
+} msg_band_train_params;
+
+/* Train the model on the GPU (host features and labels of n samples).
+ * params receives the trained parameters (feature mean/scale from the data);
+ * loss (epochs floats, may be NULL) the mean cross entropy of each epoch.
+ * The context's model is set to the result. */
+int msg_band_train(msg_ctx* ctx, const float* feat, const int32_t* label, int64_t n,
+                   const msg_band_train_params* tp, float* params, float* loss);
+
+/* Gradient of the mean cross entropy over n samples at `params` (the first
+ * 2*MSG_BAND_FEATURES entries, mean and scale, are not trained): grad
+ * receives MSG_BAND_NPARAMS - 2*MSG_BAND_FEATURES floats in the parameter
+ * order, *loss the mean loss. For checking the training kernels. */
+int msg_band_grad(msg_ctx* ctx, const float* params, const float* feat, const int32_t* label, int64_t n,
+                  float* grad, float* loss);
 
 /* ---- Single-operation entry points (parity checks of the index layer) ---- */
 

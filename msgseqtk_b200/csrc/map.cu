@@ -13,6 +13,7 @@
 //   k_cigar     Alignment::getAlnCigar (Alignment.cpp:278-303)
 #include "map_kernels.cuh"
 #include "smem_thread.cuh"
+#include "band.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -125,6 +126,20 @@ __global__ void k_aln_cig(msg_aln* __restrict__ aln, const int64_t* __restrict__
     aln[c].pad = 0;
 }
 
+__global__ void k_keep64(const uint8_t* __restrict__ keep, int64_t n, int64_t* __restrict__ out) {
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c < n) out[c] = keep[c];
+}
+
+__global__ void k_compact_aln(const msg_aln* __restrict__ aln, const uint8_t* __restrict__ keep,
+                              const int64_t* __restrict__ kidx, int64_t n, msg_aln* __restrict__ out,
+                              int64_t* __restrict__ map) {
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= n || !keep[c]) return;
+    out[kidx[c]] = aln[c];
+    map[kidx[c]] = c;
+}
+
 struct Timer {
     msg_ctx* ctx;
     int k = 0;
@@ -147,6 +162,9 @@ int check_params(const msg_map_params* p, DpParams* dp) {
         iv[k] = (int32_t)v[k];
     }
     dp->match = iv[0]; dp->mismatch = iv[1]; dp->gap_o = iv[2]; dp->gap_e = iv[3]; dp->mode = p->mode;
+    if (std::isnan(p->min_score_rate) || p->min_score_rate > 1) return MSG_EINVAL;
+    if (p->band_mode < 0 || p->band_mode > 2) return MSG_EINVAL;
+    if (p->band_mode == 1 && (p->band_w < 0 || p->band_w > 100)) return MSG_EINVAL;
     return MSG_OK;
 }
 
@@ -162,13 +180,27 @@ extern "C" void msg_map_params_default(msg_map_params* p) {
     p->mismatch = 3;
     p->gap_open = 5;
     p->gap_ext = 2;
+    p->min_score_rate = -1.0;
+    p->band_mode = 0;
+    p->band_w = 15;
 }
 
+namespace {
+struct BandCollect {
+    float* feat;
+    int32_t* label;
+    int64_t cap;
+    int64_t* n_chain;
+};
+}  // namespace
+
 static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, int64_t n_reads,
-                    const msg_map_params* params, msg_aln_out* out, msg_stage_dump* dump) {
+                    const msg_map_params* params, msg_aln_out* out, msg_stage_dump* dump,
+                    const BandCollect* collect = nullptr) {
     DpParams dpp;
     int rc = check_params(params, &dpp);
     if (rc != MSG_OK) return ctx->fail(rc, rc == MSG_EUNSUPPORTED ? "score scheme must be non-negative integers" : "bad mapping parameters");
+    if (params->band_mode == 2 && !ctx->band_loaded) return ctx->fail(MSG_ESTATE, "band_mode 2 needs a band model");
     const IndexImage& im = ctx->idx;
     const IndexDev& ix = im.dev;
     double thr = 0;
@@ -414,27 +446,43 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     tm.mark();  // 3
 
     // ---------------- DP ----------------
-    CK(ctx->dpinfo.ensure((h_nchain + 1) * 8 * 11 + 64));
+    const int64_t NC = h_nchain + 1;
+    CK(ctx->dpinfo.ensure(NC * 8 * 15 + 256));
     int64_t* d_ts = ctx->dpinfo.as<int64_t>();
-    int64_t* d_te = d_ts + (h_nchain + 1);
-    int64_t* d_cells = d_te + (h_nchain + 1);
-    int64_t* d_pcap = d_cells + (h_nchain + 1);
-    int64_t* d_rect_off = d_pcap + (h_nchain + 1);
-    int64_t* d_path_off = d_rect_off + (h_nchain + 1);
-    int64_t* d_dpcells = d_path_off + (h_nchain + 1);
-    int64_t* d_ncig = d_dpcells + (h_nchain + 1);
-    int64_t* d_area = d_ncig + (h_nchain + 1);
-    int64_t* d_small = d_area + (h_nchain + 1);
-    int64_t* d_big = d_small + (h_nchain + 1);
-    unsigned long long* d_nlist = reinterpret_cast<unsigned long long*>(d_big + (h_nchain + 1));
+    int64_t* d_te = d_ts + NC;
+    int64_t* d_cells = d_te + NC;
+    int64_t* d_pcap = d_cells + NC;
+    int64_t* d_rect_off = d_pcap + NC;
+    int64_t* d_path_off = d_rect_off + NC;
+    int64_t* d_dpcells = d_path_off + NC;
+    int64_t* d_ncig = d_dpcells + NC;
+    int64_t* d_area = d_ncig + NC;
+    int64_t* d_small = d_area + NC;
+    int64_t* d_big = d_small + NC;
+    int64_t* d_fb = d_big + NC;
+    int64_t* d_kidx = d_fb + NC;        // kept-record index per chain (n + 1)
+    int64_t* d_map = d_kidx + NC;       // chain of each kept record
+    unsigned long long* d_ctr2 = reinterpret_cast<unsigned long long*>(d_map + NC);  // 0,1 lists; 2 fallback; 3.. stats
+    unsigned long long* d_bstat = d_ctr2 + 3;
+    CK(ctx->geobuf.ensure(NC * sizeof(int4) + NC * kFeat * sizeof(float) + 64));
+    int4* d_geo = ctx->geobuf.as<int4>();
+    float* d_feat = reinterpret_cast<float*>(d_geo + NC);
+    CK(ctx->bandbuf.ensure(NC * 4 + NC * 8 + 64));
+    int8_t* d_band = ctx->bandbuf.as<int8_t>();                       // 2 per chain
+    uint8_t* d_keep = reinterpret_cast<uint8_t*>(d_band + 2 * NC);    // 1 per chain
+    uint8_t* d_probe = d_keep + NC;                                   // 1 per chain
+    int64_t* d_pcells = reinterpret_cast<int64_t*>(ctx->bandbuf.as<uint8_t>() + (NC * 4 + 7) / 8 * 8);
+    const bool learned = params->band_mode == 2 && dpp.mode == 0;
     int64_t h_cells = 0, h_pathtot = 0;
     if (h_nchain > 0) {
         S.n_launch++, k_dp_prep<<<nblk(h_nchain, 256), 256, 0, st>>>(ix, d_seeds, d_cidx_off, d_clen, d_cread, d_cidx, d_off, h_nchain,
-                                                       d_ts, d_te, d_cells, d_pcap, d_dpcells, d_area);
+                                                       d_ts, d_te, d_cells, d_pcap, d_dpcells, d_area, d_geo);
         CK(cudaGetLastError());
-        CK(cudaMemsetAsync(d_nlist, 0, 16, st));
-        S.n_launch++, k_dp_split<<<nblk(h_nchain, 256), 256, 0, st>>>(d_area, h_nchain, d_small, d_big, d_nlist);
-        CK(cudaGetLastError());
+        if (learned || collect) {
+            S.n_launch++, k_chain_features<<<nblk(h_nchain, 128), 128, 0, st>>>(ix, d_seeds, d_cidx_off, d_clen, d_cread, d_cidx,
+                                                                   d_off, d_seq, d_chain_off, d_geo, h_nchain, dpp, d_feat);
+            CK(cudaGetLastError());
+        }
         // total reference cells for the stats
         size_t tb = 0;
         CK(cub::DeviceReduce::Sum(nullptr, tb, d_dpcells, d_ncig, h_nchain, st));
@@ -456,64 +504,141 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     uint8_t* d_qbuf = d_path + P16;
     int32_t* d_plen = reinterpret_cast<int32_t*>(d_path + 2 * P16);
     msg_aln* d_aln = ctx->alnbuf.as<msg_aln>();
+    DpArgs da{};
+    da.ix = ix; da.seeds = d_seeds; da.chain_idx_off = d_cidx_off; da.chain_len = d_clen; da.chain_read = d_cread;
+    da.chain_idx = d_cidx; da.n_chain = h_nchain; da.rseq = d_seq; da.roff = d_off; da.t_start = d_ts;
+    da.t_end = d_te; da.scr_off = d_rect_off; da.scr = d_scr; da.aux = d_aux; da.sdbuf = d_sdbuf;
+    da.qbuf = d_qbuf; da.path_off = d_path_off; da.path = d_path; da.path_len = d_plen; da.aln = d_aln;
+    da.pp = dpp; da.status = d_status;
+    da.band = d_band; da.min_rate = params->min_score_rate; da.keep = d_keep; da.fb_list = d_fb;
+    da.fb_n = d_ctr2 + 2; da.bstat = d_bstat;
+    const __nv_bfloat16* d_wts = ctx->band_wts.as<__nv_bfloat16>();
+    const float* d_nrm = ctx->band_nrm.as<float>();
+
+    if (collect) {
+        // Certificate of every banded class on every chain; cost per class in cells.
+        if (collect->cap < h_nchain) { *collect->n_chain = h_nchain; return ctx->fail(MSG_EINVAL, "capacity too small"); }
+        *collect->n_chain = h_nchain;
+        if (h_nchain == 0) return MSG_OK;
+        std::vector<int64_t> area(h_nchain), best(h_nchain);
+        std::vector<int32_t> lab(h_nchain, kCls - 1);
+        std::vector<uint8_t> pr(h_nchain);
+        std::vector<int64_t> pc(h_nchain);
+        CK(cudaMemcpyAsync(area.data(), d_area, h_nchain * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(collect->feat, d_feat, h_nchain * kFeat * sizeof(float), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int64_t c = 0; c < h_nchain; ++c) best[c] = area[c];
+        da.probe = d_probe; da.probe_cells = d_pcells;
+        for (int cls = kCls - 2; cls >= 0; --cls) {  // wider classes first: ties keep the wider one
+            CK(cudaMemsetAsync(d_ctr2, 0, 64, st));
+            CK(cudaMemsetAsync(d_probe, 1, h_nchain, st));
+            CK(cudaMemcpyAsync(d_pcells, d_area, h_nchain * 8, cudaMemcpyDeviceToDevice, st));
+            S.n_launch++, k_band_assign<<<nblk(h_nchain, 128), 128, 0, st>>>(h_nchain, d_geo, d_area, d_feat, 1, band_width(cls),
+                                                                nullptr, nullptr, d_band, d_small, d_big, d_ctr2);
+            da.list = d_small; da.n_list = d_ctr2;
+            S.n_launch++, k_dp_small<<<nblk(h_nchain, 128), 128, 0, st>>>(da);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(pr.data(), d_probe, h_nchain, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(pc.data(), d_pcells, h_nchain * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (int64_t c = 0; c < h_nchain; ++c) {
+                const int64_t cost = pr[c] ? pc[c] : pc[c] + area[c];
+                if (cost < best[c]) { best[c] = cost; lab[c] = cls; }
+            }
+        }
+        std::memcpy(collect->label, lab.data(), h_nchain * sizeof(int32_t));
+        uint32_t h_status = 0;
+        CK(cudaMemcpyAsync(&h_status, d_status, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (h_status & kErrInternal) return ctx->fail(MSG_EINTERNAL, "device consistency check failed");
+        return MSG_OK;
+    }
+
+    const bool filtering = params->min_score_rate >= 0;
     if (h_nchain > 0) {
-        DpArgs da{};
-        da.ix = ix; da.seeds = d_seeds; da.chain_idx_off = d_cidx_off; da.chain_len = d_clen; da.chain_read = d_cread;
-        da.chain_idx = d_cidx; da.n_chain = h_nchain; da.rseq = d_seq; da.roff = d_off; da.t_start = d_ts;
-        da.t_end = d_te; da.scr_off = d_rect_off; da.scr = d_scr; da.aux = d_aux; da.sdbuf = d_sdbuf;
-        da.qbuf = d_qbuf; da.path_off = d_path_off; da.path = d_path; da.path_len = d_plen; da.aln = d_aln;
-        da.pp = dpp; da.status = d_status;
-        // Both launches are sized for every chain; each reads its list length on
+        CK(cudaMemsetAsync(d_ctr2, 0, 64, st));
+        const int bmode = dpp.mode != 0 ? 0 : params->band_mode;
+        S.n_launch++, k_band_assign<<<nblk(h_nchain, 128), 128, 0, st>>>(h_nchain, d_geo, d_area, d_feat, bmode, params->band_w,
+                                                            d_wts, d_nrm, d_band, d_small, d_big, d_ctr2);
+        // Every launch is sized for every chain; each reads its list length on
         // the device, so no host round trip is needed for the split.
-        da.list = d_small; da.n_list = d_nlist;
+        da.list = d_small; da.n_list = d_ctr2;
         S.n_launch++, k_dp_small<<<nblk(h_nchain, 128), 128, 0, st>>>(da);
-        da.list = d_big; da.n_list = d_nlist + 1;
+        da.list = d_big; da.n_list = d_ctr2 + 1;
         S.n_launch++, k_dp<<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
+        if (bmode != 0) {  // banded chains without a certificate, on the whole cell set
+            da.list = d_fb; da.n_list = d_ctr2 + 2;
+            S.n_launch++, k_dp<<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
+        }
         CK(cudaGetLastError());
     }
     tm.mark();  // 4
+    // Alignment::filter on the device: compact the kept records.
+    int64_t h_nrec = h_nchain;
+    msg_aln* d_rec = d_aln;
+    const int64_t* d_rmap = nullptr;
+    const int64_t* d_roff = d_chain_off;
+    if (filtering && h_nchain > 0) {
+        S.n_launch++, k_keep64<<<nblk(h_nchain, 256), 256, 0, st>>>(d_keep, h_nchain, d_ncig);
+        CK(offsets(ctx, d_ncig, h_nchain, d_kidx, misc, &h_nrec));
+        CK(ctx->alnbuf2.ensure((h_nrec + 1) * sizeof(msg_aln)));
+        CK(ctx->recoff.ensure((n_reads + 1) * 8));
+        d_rec = ctx->alnbuf2.as<msg_aln>();
+        S.n_launch++, k_compact_aln<<<nblk(h_nchain, 256), 256, 0, st>>>(d_aln, d_keep, d_kidx, h_nchain, d_rec, d_map);
+        S.n_launch++, k_gather_off<<<nblk(n_reads + 1, 256), 256, 0, st>>>(d_chain_off, d_kidx, n_reads, ctx->recoff.as<int64_t>());
+        CK(cudaGetLastError());
+        d_rmap = d_map;
+        d_roff = ctx->recoff.as<int64_t>();
+    }
     int64_t h_ncig = 0;
-    if (h_nchain > 0) {
-        S.n_launch++, k_cigar<<<nblk(h_nchain, 256), 256, 0, st>>>(h_nchain, d_aln, d_off, d_path_off, d_plen, d_path, 0, d_ncig,
-                                                     nullptr, nullptr);
+    if (h_nrec > 0) {
+        S.n_launch++, k_cigar<<<nblk(h_nrec, 256), 256, 0, st>>>(h_nrec, d_rec, d_rmap, d_off, d_path_off, d_plen, d_path, 0, d_ncig,
+                                                   nullptr, nullptr);
         CK(cudaGetLastError());
     }
     int64_t* d_cig_off = d_cells;  // reuse: cells no longer needed after the scan
-    CK(offsets(ctx, d_ncig, h_nchain, d_cig_off, misc, &h_ncig));
+    CK(offsets(ctx, d_ncig, h_nrec, d_cig_off, misc, &h_ncig));
     CK(ctx->cigbuf.ensure((h_ncig + 1) * 4));
-    if (h_nchain > 0) {
-        S.n_launch++, k_cigar<<<nblk(h_nchain, 256), 256, 0, st>>>(h_nchain, d_aln, d_off, d_path_off, d_plen, d_path, 1, nullptr,
-                                                     d_cig_off, ctx->cigbuf.as<uint32_t>());
-        S.n_launch++, k_aln_cig<<<nblk(h_nchain, 256), 256, 0, st>>>(d_aln, d_cig_off, h_nchain);
+    if (h_nrec > 0) {
+        S.n_launch++, k_cigar<<<nblk(h_nrec, 256), 256, 0, st>>>(h_nrec, d_rec, d_rmap, d_off, d_path_off, d_plen, d_path, 1, nullptr,
+                                                   d_cig_off, ctx->cigbuf.as<uint32_t>());
+        S.n_launch++, k_aln_cig<<<nblk(h_nrec, 256), 256, 0, st>>>(d_rec, d_cig_off, h_nrec);
         CK(cudaGetLastError());
     }
     tm.mark();  // 5
     uint32_t h_status = 0;
+    unsigned long long h_bstat[5] = {0, 0, 0, 0, 0};
     CK(cudaMemcpyAsync(&h_status, d_status, 4, cudaMemcpyDeviceToHost, st));
+    if (h_nchain > 0) CK(cudaMemcpyAsync(h_bstat, d_bstat, sizeof(h_bstat), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (h_status & kErrInternal) return ctx->fail(MSG_EINTERNAL, "device consistency check failed");
-    S.n_aln = h_nchain;
+    S.n_aln = h_nrec;
+    S.n_band_fallback = (int64_t)h_bstat[0];
+    S.n_band_exact = (int64_t)h_bstat[1];
+    S.n_band_drop = (int64_t)h_bstat[2];
+    S.dp_cells_done = (int64_t)(h_bstat[3] + h_bstat[4]);
+    S.n_filtered = h_nchain - h_nrec;
     S.ms_smem = tm.ms(0, 1);
     S.ms_locate = tm.ms(1, 2);
     S.ms_chain = tm.ms(2, 3);
     S.ms_dp = tm.ms(3, 5);
 
     // ---------------- results ----------------
-    out->n_aln = h_nchain;
+    out->n_aln = h_nrec;
     out->n_cigar = h_ncig;
-    ctx->res_aln = d_aln;
+    ctx->res_aln = d_rec;
     ctx->res_cigar = ctx->cigbuf.as<uint32_t>();
-    ctx->res_off = d_chain_off;
+    ctx->res_off = d_roff;
     const bool on_device = !out->aln && !out->cigar && !out->read_aln_off;
     if (!on_device) {
-        if (h_nchain > out->aln_cap || h_ncig > out->cigar_cap) return ctx->fail(MSG_EINVAL, "output capacity too small");
-        if (h_nchain > 0) {
+        if (h_nrec > out->aln_cap || h_ncig > out->cigar_cap) return ctx->fail(MSG_EINVAL, "output capacity too small");
+        if (h_nrec > 0) {
             if (!out->aln || !out->cigar) return ctx->fail(MSG_EINVAL, "null output buffer");
-            CK(cudaMemcpyAsync(out->aln, d_aln, h_nchain * sizeof(msg_aln), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(out->aln, d_rec, h_nrec * sizeof(msg_aln), cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(out->cigar, ctx->cigbuf.p, h_ncig * 4, cudaMemcpyDeviceToHost, st));
         }
         if (out->read_aln_off)
-            CK(cudaMemcpyAsync(out->read_aln_off, d_chain_off, (n_reads + 1) * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(out->read_aln_off, d_roff, (n_reads + 1) * 8, cudaMemcpyDeviceToHost, st));
     }
     if (dump) {
         dump->n_smem = h_nsmem;
@@ -558,10 +683,8 @@ extern "C" int msg_map_batch_device(msg_ctx* ctx, const msg_read_batch* reads, c
     return map_impl(ctx, reads->seq, reads->off, reads->n_reads, params, out, dump);
 }
 
-extern "C" int msg_map_batch(msg_ctx* ctx, const msg_read_batch* reads, const msg_map_params* params,
-                             msg_aln_out* out, msg_stage_dump* dump) {
-    if (!ctx || !reads || !params || !out) return MSG_EINVAL;
-    if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
+// Copy a host read batch into the context's device buffers.
+static int upload_reads(msg_ctx* ctx, const msg_read_batch* reads) {
     const int64_t n = reads->n_reads;
     if (n < 0 || (n > 0 && (!reads->seq || !reads->off))) return MSG_EINVAL;
     if (n > INT32_MAX) return MSG_EINVAL;
@@ -582,7 +705,198 @@ extern "C" int msg_map_batch(msg_ctx* ctx, const msg_read_batch* reads, const ms
     if (e != cudaSuccess) return ctx->cuda_fail(e);
     e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return ctx->cuda_fail(e);
-    return map_impl(ctx, ctx->reads.as<uint8_t>(), ctx->offs.as<int64_t>(), n, params, out, dump);
+    return MSG_OK;
+}
+
+extern "C" int msg_map_batch(msg_ctx* ctx, const msg_read_batch* reads, const msg_map_params* params,
+                             msg_aln_out* out, msg_stage_dump* dump) {
+    if (!ctx || !reads || !params || !out) return MSG_EINVAL;
+    if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
+    const int rc = upload_reads(ctx, reads);
+    if (rc != MSG_OK) return rc;
+    return map_impl(ctx, ctx->reads.as<uint8_t>(), ctx->offs.as<int64_t>(), reads->n_reads, params, out, dump);
+}
+
+// ---------------------------------------------------------------------------
+// Band model: parameters, training data, training and gradient check.
+// ---------------------------------------------------------------------------
+namespace {
+uint64_t splitmix64(uint64_t& x) {
+    uint64_t z = (x += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+double unit01(uint64_t& x) { return ((splitmix64(x) >> 11) + 0.5) * (1.0 / 9007199254740992.0); }
+
+// Weights (kNTrain floats at w) into bf16 on the device; mean/scale into nrm.
+int put_model(msg_ctx* ctx, const float* params, msg::DevBuf& wts, msg::DevBuf& nrm) {
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = wts.ensure(kNTrain * sizeof(__nv_bfloat16));
+    if (e == cudaSuccess) e = nrm.ensure(2 * kFeat * sizeof(float));
+    if (e == cudaSuccess) e = ctx->tr_g.ensure(kNTrain * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(nrm.p, params, 2 * kFeat * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->tr_g.p, params + kOffW1, kNTrain * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    k_to_bf16<<<nblk(kNTrain, 256), 256, 0, st>>>(kNTrain, ctx->tr_g.as<float>(), wts.as<__nv_bfloat16>());
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? MSG_OK : ctx->cuda_fail(e);
+}
+
+bool params_ok(const float* params) {
+    for (int k = 0; k < kNParams; ++k) if (!std::isfinite(params[k])) return false;
+    for (int k = 0; k < kFeat; ++k) if (!(params[kOffSd + k] > 0)) return false;
+    return true;
+}
+
+// Normalised features of n samples into ctx->tr_x, labels into tr_y.
+int put_samples(msg_ctx* ctx, const float* feat, const int32_t* label, int64_t n, const float* nrm_host) {
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = ctx->tr_x.ensure(n * kFeat * sizeof(float) * 2 + 64);
+    if (e == cudaSuccess) e = ctx->tr_y.ensure(n * sizeof(int32_t) + 64);
+    if (e == cudaSuccess) e = ctx->tr_loss.ensure(2 * kFeat * sizeof(float) + 64);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    float* raw = ctx->tr_x.as<float>() + n * kFeat;
+    float* d_nrm = ctx->tr_loss.as<float>() + 16;
+    e = cudaMemcpyAsync(raw, feat, n * kFeat * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->tr_y.p, label, n * sizeof(int32_t), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_nrm, nrm_host, 2 * kFeat * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    k_normalize<<<nblk(n * kFeat, 256), 256, 0, st>>>(n, raw, d_nrm, ctx->tr_x.as<float>());
+    e = cudaGetLastError();
+    return e == cudaSuccess ? MSG_OK : ctx->cuda_fail(e);
+}
+
+int grad_smem_ready(msg_ctx* ctx) {
+    const cudaError_t e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGradSmem);
+    return e == cudaSuccess ? MSG_OK : ctx->cuda_fail(e);
+}
+}  // namespace
+
+extern "C" int msg_band_model_set(msg_ctx* ctx, const float* params, int64_t n_params) {
+    if (!ctx || !params || n_params != kNParams) return MSG_EINVAL;
+    if (!params_ok(params)) return ctx->fail(MSG_EINVAL, "non-finite parameter or non-positive feature scale");
+    const int rc = put_model(ctx, params, ctx->band_wts, ctx->band_nrm);
+    if (rc == MSG_OK) ctx->band_loaded = true;
+    return rc;
+}
+
+extern "C" int msg_band_collect(msg_ctx* ctx, const msg_read_batch* reads, const msg_map_params* params, float* feat,
+                                int32_t* label, int64_t cap, int64_t* n_chain) {
+    if (!ctx || !reads || !params || !n_chain || cap < 0 || (cap > 0 && (!feat || !label))) return MSG_EINVAL;
+    if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
+    int rc = upload_reads(ctx, reads);
+    if (rc != MSG_OK) return rc;
+    BandCollect bc{feat, label, cap, n_chain};
+    msg_aln_out out{};
+    return map_impl(ctx, ctx->reads.as<uint8_t>(), ctx->offs.as<int64_t>(), reads->n_reads, params, &out, nullptr, &bc);
+}
+
+extern "C" int msg_band_grad(msg_ctx* ctx, const float* params, const float* feat, const int32_t* label, int64_t n,
+                             float* grad, float* loss) {
+    if (!ctx || !params || !feat || !label || n <= 0 || n > INT32_MAX || !grad || !loss) return MSG_EINVAL;
+    if (!params_ok(params)) return ctx->fail(MSG_EINVAL, "non-finite parameter or non-positive feature scale");
+    for (int64_t k = 0; k < n; ++k) if (label[k] < 0 || label[k] >= kCls) return MSG_EINVAL;
+    int rc = grad_smem_ready(ctx);
+    if (rc != MSG_OK) return rc;
+    msg::DevBuf& wts = ctx->tr_ord;  // bf16 weights of this call
+    rc = put_model(ctx, params, wts, ctx->tr_m);
+    if (rc != MSG_OK) return rc;
+    rc = put_samples(ctx, feat, label, n, params);
+    if (rc != MSG_OK) return rc;
+    cudaStream_t st = ctx->stream;
+    float* d_loss = ctx->tr_loss.as<float>();
+    cudaError_t e = cudaMemsetAsync(ctx->tr_g.p, 0, kNTrain * sizeof(float), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_loss, 0, sizeof(float), st);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    k_mlp_grad<<<(unsigned)nblk(n, kTile), kTile, kGradSmem, st>>>(ctx->tr_x.as<float>(), ctx->tr_y.as<int32_t>(), nullptr, 0,
+                                                              n, wts.as<__nv_bfloat16>(), (float)(1.0 / (double)n),
+                                                              ctx->tr_g.as<float>(), d_loss);
+    e = cudaGetLastError();
+    float h_loss = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(grad, ctx->tr_g.p, kNTrain * sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_loss, d_loss, sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    *loss = (float)((double)h_loss / (double)n);
+    return MSG_OK;
+}
+
+extern "C" int msg_band_train(msg_ctx* ctx, const float* feat, const int32_t* label, int64_t n,
+                              const msg_band_train_params* tp, float* params, float* loss) {
+    if (!ctx || !feat || !label || !tp || !params || n <= 0 || n > INT32_MAX) return MSG_EINVAL;
+    if (tp->epochs <= 0 || tp->batch <= 0 || !(tp->lr > 0)) return MSG_EINVAL;
+    for (int64_t k = 0; k < n; ++k) if (label[k] < 0 || label[k] >= kCls) return MSG_EINVAL;
+    // feature mean and scale from the data
+    for (int i = 0; i < kFeat; ++i) {
+        double m = 0, v = 0;
+        for (int64_t k = 0; k < n; ++k) m += feat[k * kFeat + i];
+        m /= (double)n;
+        for (int64_t k = 0; k < n; ++k) { const double d = feat[k * kFeat + i] - m; v += d * d; }
+        const double sd = std::sqrt(v / (double)n);
+        params[kOffMu + i] = (float)m;
+        params[kOffSd + i] = sd > 1e-6 ? (float)sd : 1.0f;
+    }
+    // He-normal initialisation (Box-Muller on splitmix64), zero biases
+    uint64_t rs = tp->seed;
+    auto normal = [&]() { return std::sqrt(-2.0 * std::log(unit01(rs))) * std::cos(6.283185307179586 * unit01(rs)); };
+    for (int k = kOffW1; k < kNParams; ++k) params[k] = 0.0f;
+    for (int k = 0; k < kHid * kFeat; ++k) params[kOffW1 + k] = (float)(normal() * std::sqrt(2.0 / kFeat));
+    for (int k = 0; k < kHid * kHid; ++k) params[kOffW2 + k] = (float)(normal() * std::sqrt(2.0 / kHid));
+    for (int k = 0; k < kCls * kHid; ++k) params[kOffW3 + k] = (float)(normal() * std::sqrt(1.0 / kHid));
+    int rc = grad_smem_ready(ctx);
+    if (rc != MSG_OK) return rc;
+    rc = put_samples(ctx, feat, label, n, params);
+    if (rc != MSG_OK) return rc;
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = ctx->tr_w.ensure(kNTrain * sizeof(float));
+    if (e == cudaSuccess) e = ctx->tr_m.ensure(2 * kNTrain * sizeof(float));
+    if (e == cudaSuccess) e = ctx->tr_ord.ensure(n * sizeof(int32_t) + kNTrain * sizeof(__nv_bfloat16) + 64);
+    if (e == cudaSuccess) e = ctx->tr_g.ensure(kNTrain * sizeof(float));
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    float* d_w = ctx->tr_w.as<float>();
+    float* d_m = ctx->tr_m.as<float>();
+    float* d_v = d_m + kNTrain;
+    int32_t* d_ord = ctx->tr_ord.as<int32_t>();
+    __nv_bfloat16* d_wb = reinterpret_cast<__nv_bfloat16*>(ctx->tr_ord.as<uint8_t>() + (n * sizeof(int32_t) + 15) / 16 * 16);
+    float* d_loss = ctx->tr_loss.as<float>();
+    e = cudaMemcpyAsync(d_w, params + kOffW1, kNTrain * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_m, 0, 2 * kNTrain * sizeof(float), st);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    k_to_bf16<<<nblk(kNTrain, 256), 256, 0, st>>>(kNTrain, d_w, d_wb);
+    std::vector<int32_t> ord(n);
+    for (int64_t k = 0; k < n; ++k) ord[k] = (int32_t)k;
+    const float b1 = 0.9f, b2 = 0.999f;
+    double p1 = 1.0, p2 = 1.0;
+    for (int ep = 0; ep < tp->epochs; ++ep) {
+        for (int64_t k = n - 1; k > 0; --k) std::swap(ord[k], ord[splitmix64(rs) % (uint64_t)(k + 1)]);
+        e = cudaMemcpyAsync(d_ord, ord.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(d_loss, 0, sizeof(float), st);
+        if (e != cudaSuccess) return ctx->cuda_fail(e);
+        for (int64_t b0 = 0; b0 < n; b0 += tp->batch) {
+            const int64_t b1e = std::min<int64_t>(n, b0 + tp->batch);
+            e = cudaMemsetAsync(ctx->tr_g.p, 0, kNTrain * sizeof(float), st);
+            if (e != cudaSuccess) return ctx->cuda_fail(e);
+            k_mlp_grad<<<(unsigned)nblk(b1e - b0, kTile), kTile, kGradSmem, st>>>(
+                ctx->tr_x.as<float>(), ctx->tr_y.as<int32_t>(), d_ord, b0, b1e, d_wb, (float)(1.0 / (double)(b1e - b0)),
+                ctx->tr_g.as<float>(), d_loss);
+            p1 *= b1;
+            p2 *= b2;
+            k_adam<<<nblk(kNTrain, 256), 256, 0, st>>>(kNTrain, d_w, d_wb, ctx->tr_g.as<float>(), d_m, d_v, tp->lr, b1, b2,
+                                                       1e-8f, (float)(1.0 - p1), (float)(1.0 - p2));
+        }
+        e = cudaGetLastError();
+        float h_loss = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&h_loss, d_loss, sizeof(float), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return ctx->cuda_fail(e);
+        if (loss) loss[ep] = (float)((double)h_loss / (double)n);
+    }
+    e = cudaMemcpyAsync(params + kOffW1, d_w, kNTrain * sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    return msg_band_model_set(ctx, params, kNParams);
 }
 
 extern "C" int msg_result_device(const msg_ctx* ctx, const msg_aln** aln, const uint32_t** cigar,

@@ -688,26 +688,48 @@ struct ChainCtx {
     }
 
     // Single-thread fill of rectangle m, row by row, into the same code layout
-    // (rowbuf holds the row above).
-    __device__ void fill_rect_thread(int m, int32_t& best, int64_t& bkey) {
+    // (rowbuf holds the row above). With w >= 0 only the cells within w
+    // diagonals of the adjacent seed's diagonal are computed (the 5' rectangle
+    // ends on it, the 3' rectangle starts on it); the other cells count as
+    // -inf and their stored last-row/last-column values are -inf. Returns the
+    // number of cells computed.
+    __device__ int64_t fill_rect_thread(int m, int w, int32_t& best, int64_t& bkey) {
         const RectGeo g = rect(m);
-        if (g.R <= 0 || g.C <= 0) return;
+        if (g.R <= 0 || g.C <= 0) return 0;
         const int32_t o = -(pp.gap_o + pp.gap_e), e = -pp.gap_e;
-        for (int64_t c = 0; c < g.C; ++c) {
+        const bool banded = w >= 0;
+        const int64_t dg = m == 0 ? g.C - g.R : 0;  // diagonal offset (column - row) of the seed's diagonal
+        if (banded) {
+            for (int64_t c = 0; c < 3 * g.C; ++c) g.lastrow[c] = NEG;
+            for (int64_t c = 0; c < 3 * g.R; ++c) g.lastcol[c] = NEG;
+        }
+        int64_t plo = 0, phi = g.C - 1;  // columns of the row above held in rowbuf
+        if (banded) { plo = max((int64_t)0, dg - w - 1); phi = min(g.C - 1, dg + w); }
+        for (int64_t c = plo; c <= phi; ++c) {  // the top boundary row
             const int64_t j = g.c0 + 1 + c;
             g.rowbuf[c * 3] = M(g.r0, j, m);
             g.rowbuf[c * 3 + 1] = I(g.r0, j, m);
             g.rowbuf[c * 3 + 2] = D(g.r0, j, m);
         }
+        int64_t cells = 0;
         for (int64_t rr = 0; rr < g.R; ++rr) {
+            const int64_t lo = banded ? max((int64_t)0, rr + dg - w) : 0;
+            const int64_t hi = banded ? min(g.C - 1, rr + dg + w) : g.C - 1;
+            if (lo > hi) { plo = 1; phi = 0; continue; }
             const int64_t i = g.r0 + 1 + rr;
-            int32_t ml = M(i, g.c0, m), dl = D(i, g.c0, m);
-            int32_t dm = M(i - 1, g.c0, m), di = I(i - 1, g.c0, m), dd = D(i - 1, g.c0, m);
+            int32_t ml = NEG, dl = NEG, dm = NEG, di = NEG, dd = NEG;
+            if (lo == 0) {
+                ml = M(i, g.c0, m); dl = D(i, g.c0, m);
+                dm = M(i - 1, g.c0, m); di = I(i - 1, g.c0, m); dd = D(i - 1, g.c0, m);
+            } else if (lo - 1 >= plo && lo - 1 <= phi) {
+                dm = g.rowbuf[(lo - 1) * 3]; di = g.rowbuf[(lo - 1) * 3 + 1]; dd = g.rowbuf[(lo - 1) * 3 + 2];
+            }
             const int qb = query[i - 1];
             const int64_t lane = rr & 31;
             uint8_t* code_base = g.code + (rr >> 5) * (g.C + 31) * 32;
-            for (int64_t c = 0; c < g.C; ++c) {
-                const int32_t um = g.rowbuf[c * 3], ui = g.rowbuf[c * 3 + 1], ud = g.rowbuf[c * 3 + 2];
+            for (int64_t c = lo; c <= hi; ++c) {
+                int32_t um = NEG, ui = NEG, ud = NEG;
+                if (c >= plo && c <= phi) { um = g.rowbuf[c * 3]; ui = g.rowbuf[c * 3 + 1]; ud = g.rowbuf[c * 3 + 2]; }
                 const int64_t j = g.c0 + 1 + c;
                 const int s = score(qb, tb(j - 1));
                 const int32_t mx = max(max(dm, dd), di);
@@ -729,7 +751,10 @@ struct ChainCtx {
                 g.rowbuf[c * 3] = mv; g.rowbuf[c * 3 + 1] = iv; g.rowbuf[c * 3 + 2] = dv;
                 ml = mv; dl = dv;
             }
+            cells += hi - lo + 1;
+            plo = lo; phi = hi;
         }
+        return cells;
     }
 
     // Warp fill of rectangle m (Alignment::calculateScoresNW/SW,
@@ -834,7 +859,22 @@ struct DpArgs {
     uint32_t* status;
     const int64_t* list;                  // chains handled by this launch
     const unsigned long long* n_list;     // its length, on the device
+    // Banded flanks (GLOBAL mode). band[2c], band[2c+1]: half-width of the 5'
+    // and 3' rectangle's band, -1 for the whole rectangle.
+    const int8_t* band;
+    double min_rate;                      // Alignment::filter rate; < 0: keep every record
+    uint8_t* keep;                        // per chain: the record survives the filter
+    int64_t* fb_list;                     // chains whose banded result was not certified
+    unsigned long long* fb_n;
+    unsigned long long* bstat;            // banded, exact, dropped, fallback, cells computed
+    uint8_t* probe;                       // non-null: certificate only (0 none, 1 exact, 2 below the filter)
+    int64_t* probe_cells;
 };
+
+// Alignment::filter (Alignment.cpp:548-555): alnScore < readLen * minScoreRate.
+__device__ __forceinline__ bool below_filter(int64_t score, int64_t L, double rate) {
+    return rate >= 0 && (double)score < __dmul_rn((double)L, rate);
+}
 
 // Alignment ctor window (Alignment.cpp:46-52): tStart = max(0, (int64)(start - 1.1*from)),
 // tEnd = min(chrLen, (int64)(end + 1.1*(qTo - to))) with chrLen counting the
@@ -843,7 +883,8 @@ __global__ void k_dp_prep(IndexDev ix, const Seed* __restrict__ seeds, const int
                           const int32_t* __restrict__ chain_len, const int32_t* __restrict__ chain_read,
                           const int64_t* __restrict__ chain_idx, const int64_t* __restrict__ roff, int64_t n_chain,
                           int64_t* __restrict__ t_start, int64_t* __restrict__ t_end, int64_t* __restrict__ bytes,
-                          int64_t* __restrict__ pathcap, int64_t* __restrict__ dpcells, int64_t* __restrict__ area_out) {
+                          int64_t* __restrict__ pathcap, int64_t* __restrict__ dpcells, int64_t* __restrict__ area_out,
+                          int4* __restrict__ geo) {
     const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (c >= n_chain) return;
     const int64_t* idx = chain_idx + chain_idx_off[c];
@@ -883,6 +924,7 @@ __global__ void k_dp_prep(IndexDev ix, const Seed* __restrict__ seeds, const int
     pathcap[c] = L + T + 1;
     dpcells[c] = area + diag;
     if (area_out) area_out[c] = area;
+    if (geo) geo[c] = make_int4((int)f.from, (int)(f.start - tS), (int)(L - l.to), (int)(tE - l.end));
 }
 
 // One chain: a warp (WARP = true; lanes share the rectangle wavefront and the
@@ -943,18 +985,28 @@ __device__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, in
     if (WARP) __syncwarp();
     int32_t best = 0;       // local mode: M(0,0) = 0 is the first candidate
     int64_t bkey = 0;
-    if (WARP) x.fill_rect(0, best, bkey); else x.fill_rect_thread(0, best, bkey);
+    // band half-widths of the 5' and 3' rectangles (thread path only)
+    const bool may_band = !WARP && a.band && a.pp.mode == 0;
+    const int w5 = may_band ? a.band[2 * c] : -1;
+    const int w3 = may_band ? a.band[2 * c + 1] : -1;
+    const bool banded = w5 >= 0 || w3 >= 0;
+    int64_t cells = 0;
+    int32_t x5 = NEG;       // best state value where the 5' rectangle meets the first seed
+    if (WARP) x.fill_rect(0, best, bkey); else cells += x.fill_rect_thread(0, w5, best, bkey);
     for (int k = 0; k < x.n; ++k) {
         const int m = 2 * k + 1;
         if (lane == 0) {  // first diagonal cell (Alignment.cpp:146-153): max(M,D,I + s, 0)
             const int64_t i = x.qf(k), j = x.ts(k);
             const int32_t mx = max(max(x.M(i, j, m), x.D(i, j, m)), x.I(i, j, m));
             x.diag[k] = max(add_s(mx, a.pp.match), 0);
+            if (k == 0) x5 = mx;
         }
         if (WARP) __syncwarp();
-        if (WARP) x.fill_rect(m + 1, best, bkey); else x.fill_rect_thread(m + 1, best, bkey);
+        if (WARP) x.fill_rect(m + 1, best, bkey);
+        else cells += x.fill_rect_thread(m + 1, m + 1 == 2 * x.n ? w3 : -1, best, bkey);
     }
     if (WARP) __syncwarp();
+    if (!WARP && a.bstat && cells) atomicAdd(a.bstat + 4, (unsigned long long)cells);
     const int stage = 2 * x.n + 2;
     auto reduce = [&]() {
         if (WARP) {
@@ -1002,6 +1054,53 @@ __device__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, in
             }
         }
         reduce();
+        if (banded) {
+            // Score-bound certificate. A path through a cell outside a band
+            // shifts its diagonal by more than w before (5') or after (3') the
+            // seed, so it pays at least one gap of length w+1 and gains at most
+            // `match` per remaining row: in the 5' rectangle it reaches the
+            // first seed with at most ub5, in the 3' rectangle it ends with at
+            // most E + ub3 (E: the last seed's final diagonal value, through
+            // which every complete path passes). If both bounds are strictly
+            // below what the banded paths reach, every cell value the traceback
+            // and the last-row scan compare is the full one (ties included),
+            // so the result is the reference's. Otherwise, since the DP is
+            // monotone and shifts by at most d when an input grows by d, the
+            // full score is at most s_ub; a chain below the filter's threshold
+            // is dropped, any other is recomputed on the whole cell set.
+            const int64_t mt = a.pp.match, go = a.pp.gap_o, ge = a.pp.gap_e;
+            const int kl = x.n - 1;
+            const int64_t E = (int64_t)x.diag[kl] + (x.qt(kl) - x.qf(kl) - 1) * mt;
+            bool ok = true;
+            int64_t d5 = 0;
+            if (w5 >= 0) {
+                const int64_t ub5 = mt * x.qf(0) - go - ge * (w5 + 1);
+                ok = ok && ub5 < (int64_t)x5;
+                d5 = max((int64_t)0, ub5 - (int64_t)x5);
+            }
+            int64_t ub3 = INT64_MIN;
+            if (w3 >= 0) {
+                ub3 = E + mt * (x.L - x.qt(kl)) - go - ge * (w3 + 1);
+                ok = ok && best != NEG && ub3 < (int64_t)best;
+            }
+            int res = 1;
+            if (!ok) {
+                int64_t s_ub = best == NEG ? INT64_MIN : (int64_t)best + d5;
+                if (w3 >= 0) s_ub = max(s_ub, ub3 + d5);
+                res = (s_ub > (int64_t)NEG && below_filter(s_ub, x.L, a.min_rate)) ? 2 : 0;
+            }
+            if (a.probe) {
+                a.probe[c] = (uint8_t)res;
+                a.probe_cells[c] = cells;
+                return;
+            }
+            if (a.bstat) atomicAdd(a.bstat + res, 1ull);  // [1] exact, [2] dropped, [0] fallback (counted below)
+            if (res == 2) { a.keep[c] = 0; return; }
+            if (res == 0) {
+                a.fb_list[atomicAdd(a.fb_n, 1ull)] = c;
+                return;
+            }
+        }
         aln_to = x.L;
         if (best == NEG) { aln_end = 0; s0 = OP_M; flags |= 1; }
         else { aln_end = bkey >> 1; s0 = (bkey & 1) ? OP_I : OP_M; }
@@ -1028,6 +1127,11 @@ __device__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, in
         aln_to = bkey % (x.L + 1);
         aln_end = bkey / (x.L + 1);
         s0 = OP_M;
+    }
+    if (!WARP && a.probe) {  // certificate probe of a chain without a band: exact by construction
+        a.probe[c] = 1;
+        a.probe_cells[c] = cells;
+        return;
     }
     if (lane == 0) {
         const int32_t go = a.pp.gap_o, ge = a.pp.gap_e;
@@ -1102,6 +1206,7 @@ __device__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, in
         o.aln_score = best == NEG ? INT32_MIN : best;
         o.flags = flags;
         if (flags & 2) atomicOr(a.status, kErrTrace);
+        if (a.keep) a.keep[c] = (best == NEG || below_filter(best, x.L, a.min_rate)) && a.min_rate >= 0 ? 0 : 1;
     }
 }
 
@@ -1120,6 +1225,14 @@ __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
     int32_t* rbnd = in_smem ? s_bnd[w][0] : reinterpret_cast<int32_t*>(gbase + n);
     int32_t* cbnd = in_smem ? s_bnd[w][1] : rbnd + 2 * n + 2;
     dp_chain<true>(a, c, sd, rbnd, cbnd);
+    if (a.bstat && lane_id() == 0) {  // cells of the whole cell set
+        int64_t cells = 0;
+        for (int m = 0; m <= 2 * n; m += 2) {
+            const int64_t R = rbnd[m + 1] - rbnd[m], C = cbnd[m + 1] - cbnd[m];
+            if (R > 0 && C > 0) cells += R * C;
+        }
+        atomicAdd(a.bstat + 3, (unsigned long long)cells);
+    }
 }
 
 // Chains whose rectangles are all small: one thread each.
@@ -1133,28 +1246,19 @@ __global__ void __launch_bounds__(128) k_dp_small(DpArgs a) {
     dp_chain<false>(a, c, gbase, rbnd, rbnd + 2 * n + 2);
 }
 
-// Split chains into the thread path (total rectangle area <= kSmallArea) and
-// the warp path.
-constexpr int64_t kSmallArea = 256;
-__global__ void k_dp_split(const int64_t* __restrict__ area, int64_t n_chain, int64_t* __restrict__ small,
-                           int64_t* __restrict__ big, unsigned long long* __restrict__ counts) {
-    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (c >= n_chain) return;
-    if (area[c] <= kSmallArea) small[atomicAdd(&counts[0], 1ull)] = c;
-    else big[atomicAdd(&counts[1], 1ull)] = c;
-}
-
 // CIGAR runs (Alignment::getAlnCigar): 5' clip, the reversed path in runs, 3' clip.
-__global__ void k_cigar(int64_t n_chain, const msg_aln* __restrict__ aln, const int64_t* __restrict__ roff,
-                        const int64_t* __restrict__ path_off, const int32_t* __restrict__ path_len,
-                        const uint8_t* __restrict__ path, int pass, int64_t* __restrict__ n_cig,
-                        const int64_t* __restrict__ cig_off, uint32_t* __restrict__ cig) {
+// Record k belongs to chain map[k] (k itself when map is null).
+__global__ void k_cigar(int64_t n_rec, const msg_aln* __restrict__ aln, const int64_t* __restrict__ map,
+                        const int64_t* __restrict__ roff, const int64_t* __restrict__ path_off,
+                        const int32_t* __restrict__ path_len, const uint8_t* __restrict__ path, int pass,
+                        int64_t* __restrict__ n_cig, const int64_t* __restrict__ cig_off, uint32_t* __restrict__ cig) {
     const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (c >= n_chain) return;
+    if (c >= n_rec) return;
     const msg_aln& a = aln[c];
+    const int64_t ch = map ? map[c] : c;
     const int64_t L = roff[a.read + 1] - roff[a.read];
-    const uint8_t* p = path + path_off[c];
-    const int64_t np = path_len[c];
+    const uint8_t* p = path + path_off[ch];
+    const int64_t np = path_len[ch];
     int64_t k = 0;
     uint32_t* out = pass ? cig + cig_off[c] : nullptr;
     if (a.aln_from > 0) { if (pass) out[k] = (uint32_t)(a.aln_from << 4 | OP_S); ++k; }

@@ -28,7 +28,12 @@ assert ALN_DTYPE.itemsize == 88
 # symbols of the C ABI, in include/msg_b200.h order
 EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy", "msg_index_load", "msg_index_bytes",
            "msg_map_params_default", "msg_map_batch", "msg_map_batch_device", "msg_last_stats", "msg_occ_query",
-           "msg_result_device", "msg_ctx_stream", "msg_smem_batch_noalloc", "msg_bi_ext_query", "msg_sa_query"]
+           "msg_result_device", "msg_ctx_stream", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
+           "msg_band_train", "msg_band_grad", "msg_bi_ext_query", "msg_sa_query"]
+
+# band model (include/msg_b200.h)
+BAND_FEATURES, BAND_HIDDEN, BAND_CLASSES, BAND_NPARAMS = 16, 64, 4, 5540
+BAND_WIDTHS = (7, 15, 31, None)  # class -> band half-width (None: whole rectangles)
 
 
 class FmdView(C.Structure):
@@ -43,7 +48,12 @@ class MtgView(C.Structure):
 
 class MapParams(C.Structure):
     _fields_ = [("min_len", C.c_int64), ("max_evalue", C.c_double), ("max_nseed", C.c_int64), ("mode", C.c_int32),
-                ("match", C.c_double), ("mismatch", C.c_double), ("gap_open", C.c_double), ("gap_ext", C.c_double)]
+                ("match", C.c_double), ("mismatch", C.c_double), ("gap_open", C.c_double), ("gap_ext", C.c_double),
+                ("min_score_rate", C.c_double), ("band_mode", C.c_int32), ("band_w", C.c_int32)]
+
+
+class BandTrainParams(C.Structure):
+    _fields_ = [("epochs", C.c_int32), ("batch", C.c_int32), ("lr", C.c_float), ("seed", C.c_uint64)]
 
 
 class ReadBatch(C.Structure):
@@ -63,7 +73,9 @@ class StageDump(C.Structure):
 class MapStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("n_reads", "n_smem", "n_seed", "n_chain", "n_aln", "n_ext", "n_sa",
                                          "dp_cells", "host_sorted", "n_launch")] + \
-               [(n, C.c_double) for n in ("ms_total", "ms_smem", "ms_locate", "ms_chain", "ms_dp")]
+               [(n, C.c_double) for n in ("ms_total", "ms_smem", "ms_locate", "ms_chain", "ms_dp")] + \
+               [(n, C.c_int64) for n in ("dp_cells_done", "n_band_exact", "n_band_drop", "n_band_fallback",
+                                         "n_filtered")]
 
 
 def build(force: bool = False) -> str:
@@ -104,6 +116,12 @@ def load_library(path: str = LIB_PATH):
     L.msg_ctx_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     L.msg_smem_batch_noalloc.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(MapParams),
                                          C.c_void_p, C.c_int64, C.c_void_p]
+    f32p = C.POINTER(C.c_float)
+    i32p = C.POINTER(C.c_int32)
+    L.msg_band_model_set.argtypes = [C.c_void_p, f32p, C.c_int64]
+    L.msg_band_collect.argtypes = [C.c_void_p, C.POINTER(ReadBatch), C.POINTER(MapParams), f32p, i32p, C.c_int64, i64p]
+    L.msg_band_train.argtypes = [C.c_void_p, f32p, i32p, C.c_int64, C.POINTER(BandTrainParams), f32p, f32p]
+    L.msg_band_grad.argtypes = [C.c_void_p, f32p, f32p, i32p, C.c_int64, f32p, f32p]
     L.msg_occ_query.argtypes = [C.c_void_p, C.c_int64, u8p, i64p, i64p]
     L.msg_bi_ext_query.argtypes = [C.c_void_p, C.c_int64, C.c_int, u8p, i64p, i64p, i64p, i64p]
     L.msg_sa_query.argtypes = [C.c_void_p, C.c_int64, i64p, i64p]
@@ -267,6 +285,55 @@ class Context:
         params = params or default_params()
         return self.lib.msg_smem_batch_noalloc(self.h, n_reads, seq_ptr, off_ptr, C.byref(params), out_ptr,
                                                cap_per_read, count_ptr)
+
+    # ---- band model ----
+    def band_model_set(self, params: np.ndarray):
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(self.lib.msg_band_model_set(self.h, _p(params, C.POINTER(C.c_float)), params.size),
+                    "msg_band_model_set")
+
+    def band_collect(self, seq: np.ndarray, off: np.ndarray, params: MapParams | None = None):
+        """Per-chain features (n x 16 float32) and cheapest certified band
+        class (int32) of a host read batch."""
+        params = params or default_params()
+        seq = np.ascontiguousarray(seq, dtype=np.uint8)
+        off = np.ascontiguousarray(off, dtype=np.int64)
+        rb = ReadBatch(len(off) - 1, _p(seq, u8p), _p(off, i64p))
+        cap = max(16, 4 * (len(off) - 1))
+        while True:
+            feat = np.zeros((cap, BAND_FEATURES), dtype=np.float32)
+            lab = np.zeros(cap, dtype=np.int32)
+            n = C.c_int64(0)
+            rc = self.lib.msg_band_collect(self.h, C.byref(rb), C.byref(params), _p(feat, C.POINTER(C.c_float)),
+                                           _p(lab, C.POINTER(C.c_int32)), cap, C.byref(n))
+            if rc == 1 and n.value > cap:  # MSG_EINVAL: capacity
+                cap = n.value
+                continue
+            self._check(rc, "msg_band_collect")
+            return feat[:n.value], lab[:n.value]
+
+    def band_train(self, feat: np.ndarray, label: np.ndarray, epochs=20, batch=4096, lr=2e-3, seed=1):
+        """Train the band model on the GPU; returns (params, per-epoch loss)."""
+        feat = np.ascontiguousarray(feat, dtype=np.float32)
+        label = np.ascontiguousarray(label, dtype=np.int32)
+        tp = BandTrainParams(epochs, batch, lr, seed)
+        params = np.zeros(BAND_NPARAMS, dtype=np.float32)
+        loss = np.zeros(epochs, dtype=np.float32)
+        self._check(self.lib.msg_band_train(self.h, _p(feat, C.POINTER(C.c_float)), _p(label, C.POINTER(C.c_int32)),
+                                            len(label), C.byref(tp), _p(params, C.POINTER(C.c_float)),
+                                            _p(loss, C.POINTER(C.c_float))), "msg_band_train")
+        return params, loss
+
+    def band_grad(self, params: np.ndarray, feat: np.ndarray, label: np.ndarray):
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        feat = np.ascontiguousarray(feat, dtype=np.float32)
+        label = np.ascontiguousarray(label, dtype=np.int32)
+        grad = np.zeros(BAND_NPARAMS - 2 * BAND_FEATURES, dtype=np.float32)
+        loss = C.c_float(0)
+        self._check(self.lib.msg_band_grad(self.h, _p(params, C.POINTER(C.c_float)), _p(feat, C.POINTER(C.c_float)),
+                                           _p(label, C.POINTER(C.c_int32)), len(label),
+                                           _p(grad, C.POINTER(C.c_float)), C.byref(loss)), "msg_band_grad")
+        return grad, loss.value
 
     def stats(self) -> dict:
         s = MapStats()
