@@ -10,8 +10,16 @@ pairs = 500 k reads) end to end: SMEMs -> seed selection -> locate ->
 redundant-seed removal -> chains -> DP + traceback -> CIGAR. Default parameters
 (min seed 17, e-value 0.01, maxNSeed 500, GLOBAL NW, scores 1/3/5/2).
 
-Reported line (rank 0): `value` = reads/s over all ranks with the reads
-already resident in HBM and results left on the device; `e2e` = the same
+Both paths apply Alignment::filter on the device (-s 0.65, the reference's
+default), so the records are the ones the reference keeps. The plain path
+fills the reference's whole DP rectangles; the learned path lets a classifier
+(trained on the GPU during setup, on chains of fresh reads from the same
+generator) pick a band per chain, certified or recomputed, so its records
+are identical (checked on the validation sample).
+
+Reported line (rank 0): `value` = reads/s of the learned path over all ranks
+with the reads already resident in HBM and results left on the device;
+`plain_gpu` = the same for the plain path; `e2e` = the learned path
 through msg_map_batch with pinned host reads in and host alignment records
 out, copies inside the timed region; `roofline` for the dominant kernel;
 `cpu_baseline` = the reference's own mapping path (compiled from its sources)
@@ -55,6 +63,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--validate", type=int, default=2000, help="reads checked against the oracle after timing")
+    ap.add_argument("--train-pairs", type=int, default=600_000,
+                    help="read pairs (fresh seed) whose chains train the band classifier")
+    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--min-score", type=float, default=0.65, help="Alignment::filter rate (msgseqtk-align -s)")
     return ap.parse_args()
 
 
@@ -223,7 +235,42 @@ def main():
     ctx.load_index(view)
     setup["load_s"] = round(time.time() - t0, 1)
     setup["index_gb"] = round(ctx.index_bytes() / 1e9, 2)
-    params = lib.default_params()
+    # plain: the reference's whole flank rectangles; learned: per-chain band
+    # from the classifier, certified or recomputed (same records)
+    plain_params = lib.default_params(min_score_rate=args.min_score)
+    params = lib.default_params(min_score_rate=args.min_score, band_mode=2)
+
+    # train the band classifier on chains of fresh reads from the same generator
+    from msgseqtk_b200 import synth
+    t0 = time.time()
+    tm1, tm2 = synth.sample_pairs(genomes, args.train_pairs, seed=reads_seed(rank) + 5000)
+    treads = synth.interleave(tm1, tm2)
+    t1 = time.time()
+    feats, labels = [], []
+    tb = 2 * args.batch_pairs
+    for a in range(0, len(treads), tb):
+        b = min(len(treads), a + tb)
+        f, l = ctx.band_collect(treads.seqs[treads.offs[a]:treads.offs[b]], treads.offs[a:b + 1] - treads.offs[a],
+                                plain_params)
+        feats.append(f)
+        labels.append(l)
+    feats = np.concatenate(feats)
+    labels = np.concatenate(labels)
+    n_all = len(labels)
+    keep = labels >= 0  # chains a band can apply to
+    feats, labels = feats[keep], labels[keep]
+    t2 = time.time()
+    bparams, bloss = ctx.band_train(feats, labels, epochs=args.epochs, batch=4096, lr=2e-3, seed=11)
+    torch.cuda.synchronize()
+    t3 = time.time()
+    from oracle import band_mlp
+    train_acc = float(np.mean(band_mlp.classify(bparams, feats) == labels))
+    band_info = {"train_chains": int(len(labels)), "collected_chains": int(n_all),
+                 "label_counts": np.bincount(labels, minlength=4).tolist(),
+                 "classes": "band half-width 7, 15, 31, whole rectangles", "epochs": args.epochs,
+                 "loss_first_last": [float(bloss[0]), float(bloss[-1])], "train_accuracy": round(train_acc, 4),
+                 "collect_s": round(t2 - t1, 2), "train_s": round(t3 - t2, 2), "reads_s": round(t1 - t0, 1)}
+    del treads, tm1, tm2
 
     # batches: reads resident on the device, and pinned host copies for e2e
     bp = 2 * args.batch_pairs
@@ -238,34 +285,60 @@ def main():
               for k in range(n_batches)]
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
 
-    def run_device(k):
+    def run_device(k, prm):
         base = int(reads.offs[k * bp])
-        return ctx.map_device(d_seq.data_ptr() + base, offs_d[k].data_ptr(), len(offs_d[k]) - 1, params)
+        return ctx.map_device(d_seq.data_ptr() + base, offs_d[k].data_ptr(), len(offs_d[k]) - 1, prm)
 
-    for s in range(args.warmup):
-        run_device(s % n_batches)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    clocks = Clocks(local)
-    clocks.start()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    agg = {"smem": 0.0, "locate": 0.0, "chain": 0.0, "dp": 0.0, "n_ext": 0, "dp_cells": 0, "n_reads": 0,
-           "n_launch": 0, "n_aln": 0, "host_sorted": 0, "n_sa": 0}
-    torch.cuda.synchronize()
-    ev0.record(stream)
-    for s in range(args.steps):
-        run_device((args.warmup + s) % n_batches)
-        st = ctx.stats()
-        agg["smem"] += st["ms_smem"]; agg["locate"] += st["ms_locate"]; agg["chain"] += st["ms_chain"]
-        agg["dp"] += st["ms_dp"]
-        for k in ("n_ext", "dp_cells", "n_reads", "n_launch", "n_aln", "host_sorted", "n_sa"):
-            agg[k] += st[k]
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    ms, total_reads = reduce_over_ranks(ev0.elapsed_time(ev1), float(agg["n_reads"]), "cuda")
+    counters = ("n_ext", "dp_cells", "dp_cells_done", "n_reads", "n_launch", "n_aln", "host_sorted", "n_sa",
+                "n_chain", "n_band_exact", "n_band_drop", "n_band_fallback", "n_filtered", "n_dp_warp")
+
+    def timed(prm, clocks=None):
+        """W warm-up steps, then K timed steps on new batches (inputs larger
+        than L2), device-timed on the library's stream, max over ranks."""
+        for s in range(args.warmup):
+            run_device(s % n_batches, prm)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        if clocks:
+            clocks.start()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        agg = {"smem": 0.0, "locate": 0.0, "chain": 0.0, "dp": 0.0}
+        agg.update({k: 0 for k in counters})
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for s in range(args.steps):
+            run_device((args.warmup + s) % n_batches, prm)
+            st = ctx.stats()
+            agg["smem"] += st["ms_smem"]; agg["locate"] += st["ms_locate"]; agg["chain"] += st["ms_chain"]
+            agg["dp"] += st["ms_dp"]
+            for k in counters:
+                agg[k] += st[k]
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop() if clocks else None
+        ms, total_reads = reduce_over_ranks(ev0.elapsed_time(ev1), float(agg["n_reads"]), "cuda")
+        return ms, total_reads, agg, clk
+
+    ms_p, reads_p, agg_p, _ = timed(plain_params)
+    ms, total_reads, agg, clk = timed(params, Clocks(local))
     value = total_reads / (ms / 1000.0)
+    banded = agg["n_band_exact"] + agg["n_band_drop"] + agg["n_band_fallback"]
+
+    def gcups(a):
+        return {"reference_cells": a["dp_cells"] / (a["dp"] / 1000.0) / 1e9 if a["dp"] > 0 else 0.0,
+                "computed_cells": a["dp_cells_done"] / (a["dp"] / 1000.0) / 1e9 if a["dp"] > 0 else 0.0}
+
+    plain = {"value": reads_p / (ms_p / 1000.0), "unit": "reads/s", "ms_per_step": ms_p / args.steps,
+             "dp_ms_per_step": agg_p["dp"] / args.steps, "gcups": gcups(agg_p),
+             "dp_cells_computed": agg_p["dp_cells_done"], "warp_path_chains": agg_p["n_dp_warp"]}
+    band_info.update({"dp_ms_per_step": agg["dp"] / args.steps, "gcups": gcups(agg),
+                      "dp_cells_computed": agg["dp_cells_done"], "dp_cells_reference": agg["dp_cells"],
+                      "warp_path_chains": agg["n_dp_warp"],
+                      "banded_chains": banded, "certified_exact": agg["n_band_exact"],
+                      "certified_filtered": agg["n_band_drop"], "fallback": agg["n_band_fallback"],
+                      "fallback_rate": agg["n_band_fallback"] / banded if banded else 0.0,
+                      "speedup_vs_plain": value / plain["value"] if plain["value"] > 0 else None})
 
     # end to end through the public API: pinned host reads in, host records out
     aln_buf = np.zeros(8 * bp, dtype=lib.ALN_DTYPE)
@@ -311,7 +384,6 @@ def main():
                 "unit": "GB/s", "frac": achieved / hbm, "traffic": None, "peak_source": peak_note,
                 "alg_bytes_per_launch": smem_bytes / args.steps, "dominant_stage": dom,
                 "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()}}
-    gcups = agg["dp_cells"] / (agg["dp"] / 1000.0) / 1e9 if agg["dp"] > 0 else 0.0
 
     # validation: a sample of the timed reads through the oracle
     valid = None
@@ -320,9 +392,12 @@ def main():
         orc = Oracle(view)
         n = min(args.validate, len(reads))
         res = ctx.map(reads.seqs[:reads.offs[n]], reads.offs[:n + 1], params)
+        res_p = ctx.map(reads.seqs[:reads.offs[n]], reads.offs[:n + 1], plain_params)
+        same = all(np.array_equal(res[k], res_p[k]) for k in ("aln", "cigar", "read_aln_off"))
         bad = 0
         for i in range(n):
-            exp = orc.align_read(reads.read(i))
+            L = len(reads.read(i))
+            exp = [e for e in orc.align_read(reads.read(i)) if not (e["aln_score"] < L * args.min_score)]
             got = res["aln"][res["read_aln_off"][i]:res["read_aln_off"][i + 1]]
             if len(exp) != len(got):
                 bad += 1
@@ -336,7 +411,8 @@ def main():
                 if f != ef or w != e["cigar"]:
                     bad += 1
                     break
-        valid = {"reads": n, "mismatching_reads": bad}
+        valid = {"reads": n, "mismatching_reads": bad, "learned_equals_plain": bool(same),
+                 "compared": "records after Alignment::filter (alnScore >= L * %g)" % args.min_score}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -353,9 +429,10 @@ def main():
                            "reads_per_step": bp, "pairs_per_gpu": args.pairs, "bd_symbols": view.n,
                            "l2": "inputs larger than L2 (index %.1f GB, new reads every step)" % setup["index_gb"],
                            "parallelism": f"dp{world}" if world > 1 else "single GPU"},
-                "gcups": gcups, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+                "gcups": gcups(agg), "plain_gpu": plain, "learned_band": band_info,
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
                 "gpu_launches": agg["n_launch"], "validation": valid, "setup": setup,
-                "stats": {k: agg[k] for k in ("n_ext", "n_sa", "n_aln", "dp_cells", "host_sorted")}}
+                "stats": {k: agg[k] for k in counters}}
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

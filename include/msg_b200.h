@@ -95,7 +95,7 @@ typedef struct msg_map_params {
     double min_score_rate;
     /* DP cells of the 5' and 3' flank rectangles (GLOBAL mode only):
      * 0 = the reference's whole rectangles (default); 1 = a diagonal band of
-     * half-width band_w around the adjacent seed's diagonal; 2 = a band width
+     * half-width band_w (0..31) around the adjacent seed's diagonal; 2 = a band width
      * chosen per chain by the model loaded with msg_band_model_set. A banded
      * chain is kept only under a score-bound certificate: either no path
      * through a cell outside the band can reach the banded score (the record
@@ -178,6 +178,7 @@ typedef struct msg_map_stats {
     int64_t n_band_drop;    /* banded chains certified below the filter threshold */
     int64_t n_band_fallback;/* banded chains recomputed on the whole cell set */
     int64_t n_filtered;     /* records removed by min_score_rate (drops included) */
+    int64_t n_dp_warp;      /* chains whose DP ran one warp each (the rest: one thread each) */
 } msg_map_stats;
 
 /* Map a batch of reads held in HOST memory: the per-read SE task body
@@ -247,8 +248,9 @@ int msg_band_model_set(msg_ctx* ctx, const float* params, int64_t n_params);
  * MSG_BAND_FEATURES features and the label = the class whose DP costs the
  * fewest cells once certified (an uncertified band costs its cells plus the
  * whole rectangles; ties go to the wider class), with the certificate of
- * `params` (min_score_rate included). Host buffers of cap chains;
- * *n_chain receives the chain count (MSG_EINVAL when it exceeds cap). */
+ * `params` (min_score_rate included); -1 for chains that never get a band
+ * (small chains, flanks that a band would not cut). Host buffers of cap
+ * chains; *n_chain receives the chain count (MSG_EINVAL when it exceeds cap). */
 int msg_band_collect(msg_ctx* ctx, const msg_read_batch* reads, const msg_map_params* params, float* feat,
                      int32_t* label, int64_t cap, int64_t* n_chain);
 

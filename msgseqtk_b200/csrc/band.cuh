@@ -146,10 +146,17 @@ __device__ inline int mlp_class(const float* __restrict__ xr, const float* __res
 
 constexpr int64_t kSmallArea = 256;  // plain chains up to this many rectangle cells run one thread each
 
-// Band half-widths per chain and the split into the thread path (banded
-// chains and chains of at most kSmallArea cells) and the warp path.
-// mode 0: no band; 1: fixed_w for every chain; 2: the classifier's choice.
-// A flank whose band would cover its whole rectangle is not banded.
+// A band of half-width w is used on an R x C flank rectangle when it covers
+// less than half of it (at most R (2w+1) cells).
+__host__ __device__ inline bool bandable(int R, int C, int w) {
+    return R > 0 && C > 0 && w < max(R, C) - 1 && 2 * (2 * w + 1) < C;
+}
+
+// Band half-widths per chain and the split into the thread path (chains of
+// at most kSmallArea cells, never banded) and the warp path (the rest).
+// mode 0: no band; 1: fixed_w for every larger chain; 2: the classifier's
+// choice for larger chains with a flank that a band of half-width 7 would cut.
+// Each flank is banded only when bandable().
 __global__ void __launch_bounds__(128) k_band_assign(int64_t n_chain, const int4* __restrict__ geo,
                                                      const int64_t* __restrict__ area, const float* __restrict__ feat,
                                                      int mode, int fixed_w, const __nv_bfloat16* __restrict__ wts,
@@ -166,16 +173,17 @@ __global__ void __launch_bounds__(128) k_band_assign(int64_t n_chain, const int4
     const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (c >= n_chain) return;
     const int4 g = geo[c];
-    const int span5 = (g.x > 0 && g.y > 0) ? max(g.x, g.y) - 1 : 0;  // widest useful half-width
-    const int span3 = (g.z > 0 && g.w > 0) ? max(g.z, g.w) - 1 : 0;
     int w = -1;
-    if (mode == 1) w = fixed_w;
-    else if (mode == 2 && (span5 > band_width(0) || span3 > band_width(0))) w = band_width(mlp_class(feat + c * kFeat, sW, sN));
-    const int w5 = (w >= 0 && w < span5) ? w : -1;
-    const int w3 = (w >= 0 && w < span3) ? w : -1;
+    if (area[c] > kSmallArea) {  // small chains stay on the thread path, whole rectangles
+        if (mode == 1) w = fixed_w;
+        else if (mode == 2 && (bandable(g.x, g.y, band_width(0)) || bandable(g.z, g.w, band_width(0))))
+            w = band_width(mlp_class(feat + c * kFeat, sW, sN));
+    }
+    const int w5 = (w >= 0 && bandable(g.x, g.y, w)) ? w : -1;
+    const int w3 = (w >= 0 && bandable(g.z, g.w, w)) ? w : -1;
     band[2 * c] = (int8_t)w5;
     band[2 * c + 1] = (int8_t)w3;
-    if (w5 >= 0 || w3 >= 0 || area[c] <= kSmallArea) small[atomicAdd(&counts[0], 1ull)] = c;
+    if (w5 < 0 && w3 < 0 && area[c] <= kSmallArea) small[atomicAdd(&counts[0], 1ull)] = c;
     else big[atomicAdd(&counts[1], 1ull)] = c;
 }
 

@@ -164,7 +164,7 @@ int check_params(const msg_map_params* p, DpParams* dp) {
     dp->match = iv[0]; dp->mismatch = iv[1]; dp->gap_o = iv[2]; dp->gap_e = iv[3]; dp->mode = p->mode;
     if (std::isnan(p->min_score_rate) || p->min_score_rate > 1) return MSG_EINVAL;
     if (p->band_mode < 0 || p->band_mode > 2) return MSG_EINVAL;
-    if (p->band_mode == 1 && (p->band_w < 0 || p->band_w > 100)) return MSG_EINVAL;
+    if (p->band_mode == 1 && (p->band_w < 0 || p->band_w > 31)) return MSG_EINVAL;
     return MSG_OK;
 }
 
@@ -522,6 +522,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         if (h_nchain == 0) return MSG_OK;
         std::vector<int64_t> area(h_nchain), best(h_nchain);
         std::vector<int32_t> lab(h_nchain, kCls - 1);
+        std::vector<uint8_t> eligible(h_nchain, 0);
         std::vector<uint8_t> pr(h_nchain);
         std::vector<int64_t> pc(h_nchain);
         CK(cudaMemcpyAsync(area.data(), d_area, h_nchain * 8, cudaMemcpyDeviceToHost, st));
@@ -531,21 +532,24 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         da.probe = d_probe; da.probe_cells = d_pcells;
         for (int cls = kCls - 2; cls >= 0; --cls) {  // wider classes first: ties keep the wider one
             CK(cudaMemsetAsync(d_ctr2, 0, 64, st));
-            CK(cudaMemsetAsync(d_probe, 1, h_nchain, st));
+            CK(cudaMemsetAsync(d_probe, 3, h_nchain, st));  // 3: not banded at this class
             CK(cudaMemcpyAsync(d_pcells, d_area, h_nchain * 8, cudaMemcpyDeviceToDevice, st));
             S.n_launch++, k_band_assign<<<nblk(h_nchain, 128), 128, 0, st>>>(h_nchain, d_geo, d_area, d_feat, 1, band_width(cls),
                                                                 nullptr, nullptr, d_band, d_small, d_big, d_ctr2);
-            da.list = d_small; da.n_list = d_ctr2;
-            S.n_launch++, k_dp_small<<<nblk(h_nchain, 128), 128, 0, st>>>(da);
+            da.list = d_big; da.n_list = d_ctr2 + 1;  // banded chains are all on the warp path
+            S.n_launch++, k_dp<<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(pr.data(), d_probe, h_nchain, cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(pc.data(), d_pcells, h_nchain * 8, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             for (int64_t c = 0; c < h_nchain; ++c) {
+                if (pr[c] == 3) continue;
+                eligible[c] = 1;
                 const int64_t cost = pr[c] ? pc[c] : pc[c] + area[c];
                 if (cost < best[c]) { best[c] = cost; lab[c] = cls; }
             }
         }
+        for (int64_t c = 0; c < h_nchain; ++c) if (!eligible[c]) lab[c] = -1;
         std::memcpy(collect->label, lab.data(), h_nchain * sizeof(int32_t));
         uint32_t h_status = 0;
         CK(cudaMemcpyAsync(&h_status, d_status, 4, cudaMemcpyDeviceToHost, st));
@@ -567,7 +571,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         da.list = d_big; da.n_list = d_ctr2 + 1;
         S.n_launch++, k_dp<<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
         if (bmode != 0) {  // banded chains without a certificate, on the whole cell set
-            da.list = d_fb; da.n_list = d_ctr2 + 2;
+            da.list = d_fb; da.n_list = d_ctr2 + 2; da.band = nullptr;
             S.n_launch++, k_dp<<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
         }
         CK(cudaGetLastError());
@@ -607,9 +611,10 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     }
     tm.mark();  // 5
     uint32_t h_status = 0;
-    unsigned long long h_bstat[5] = {0, 0, 0, 0, 0};
+    unsigned long long h_ctr2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const unsigned long long* h_bstat = h_ctr2 + 3;
     CK(cudaMemcpyAsync(&h_status, d_status, 4, cudaMemcpyDeviceToHost, st));
-    if (h_nchain > 0) CK(cudaMemcpyAsync(h_bstat, d_bstat, sizeof(h_bstat), cudaMemcpyDeviceToHost, st));
+    if (h_nchain > 0) CK(cudaMemcpyAsync(h_ctr2, d_ctr2, sizeof(h_ctr2), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (h_status & kErrInternal) return ctx->fail(MSG_EINTERNAL, "device consistency check failed");
     S.n_aln = h_nrec;
@@ -618,6 +623,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     S.n_band_drop = (int64_t)h_bstat[2];
     S.dp_cells_done = (int64_t)(h_bstat[3] + h_bstat[4]);
     S.n_filtered = h_nchain - h_nrec;
+    S.n_dp_warp = (int64_t)h_ctr2[1];
     S.ms_smem = tm.ms(0, 1);
     S.ms_locate = tm.ms(1, 2);
     S.ms_chain = tm.ms(2, 3);

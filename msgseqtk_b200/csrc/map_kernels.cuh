@@ -757,6 +757,151 @@ struct ChainCtx {
         return cells;
     }
 
+    // Warp fill of the band of rectangle m (m = 0 or 2n; GLOBAL mode): the
+    // 2w+1 diagonals within w of the adjacent seed's diagonal. Position
+    // p = lane + 32 h (h < NP) of row rr is column rr + dg - w + p; one row is
+    // one step. M and I read the previous row at p and p + 1 (registers and a
+    // shuffle); D runs along the row, D(p) = max(M(p-1) + o, D(p-1) + e), which
+    // unrolls to a prefix maximum over the row of M(k) + o - e k (plus the left
+    // boundary's contribution at column 0). Boundary cells next to band cells
+    // are read exactly; cells outside the band count as -inf. Codes and the
+    // last row/column go to the same places as the whole-rectangle fills.
+    // Returns the number of cells computed.
+    template <int NP>
+    __device__ int64_t fill_rect_band(int m, int w) {
+        const RectGeo g = rect(m);
+        if (g.R <= 0 || g.C <= 0) return 0;
+        const int lane = lane_id();
+        const unsigned FULL = 0xffffffffu;
+        const int32_t o = -(pp.gap_o + pp.gap_e), e = -pp.gap_e;
+        const int64_t dg = m == 0 ? g.C - g.R : 0;
+        const int NB = 2 * w + 1;
+        constexpr int32_t VNEG = INT32_MIN + (1 << 26);  // "no path" in the prefix maximum, far below NEG
+        for (int64_t c = lane; c < 3 * g.C; c += 32) g.lastrow[c] = NEG;
+        for (int64_t c = lane; c < 3 * g.R; c += 32) g.lastcol[c] = NEG;
+        // row -1 is the top boundary row: position p there is column dg - w + p - 1
+        int32_t pm[NP], pi[NP], pd[NP];
+#pragma unroll
+        for (int h = 0; h < NP; ++h) {
+            const int p = lane + 32 * h;
+            const int64_t c = dg - w + p - 1;
+            pm[h] = pi[h] = pd[h] = NEG;
+            if (p <= NB && c >= -1 && c <= g.C - 1) {
+                const int64_t j = g.c0 + 1 + c;
+                pm[h] = M(g.r0, j, m); pi[h] = I(g.r0, j, m); pd[h] = D(g.r0, j, m);
+            }
+        }
+        __syncwarp();
+        int64_t cells = 0;
+        for (int64_t rr = 0; rr < g.R; ++rr) {
+            const int64_t i = g.r0 + 1 + rr;
+            const int qb = query[i - 1];
+            const int64_t lr = rr & 31;
+            uint8_t* code_base = g.code + (rr >> 5) * (g.C + 31) * 32;
+            int32_t um[NP], ui[NP], mv[NP], iv[NP], U[NP], b1s[NP], b2s[NP];
+            uint8_t code[NP];
+            bool valid[NP], at0[NP];
+            int64_t col[NP];
+#pragma unroll
+            for (int h = 0; h < NP; ++h) {  // up neighbours: previous row at p + 1
+                const int32_t a_m = __shfl_down_sync(FULL, pm[h], 1);
+                const int32_t a_i = __shfl_down_sync(FULL, pi[h], 1);
+                int32_t n_m = NEG, n_i = NEG;
+                if (h + 1 < NP) {
+                    n_m = __shfl_sync(FULL, pm[h + 1 < NP ? h + 1 : h], 0);
+                    n_i = __shfl_sync(FULL, pi[h + 1 < NP ? h + 1 : h], 0);
+                }
+                um[h] = lane < 31 ? a_m : n_m;
+                ui[h] = lane < 31 ? a_i : n_i;
+            }
+#pragma unroll
+            for (int h = 0; h < NP; ++h) {
+                const int p = lane + 32 * h;
+                const int64_t c = rr + dg - w + p;
+                col[h] = c;
+                valid[h] = p < NB && c >= 0 && c < g.C;
+                at0[h] = valid[h] && c == 0;
+                int32_t dm = pm[h], di = pi[h], dd = pd[h];
+                if (at0[h]) { dm = M(i - 1, g.c0, m); di = I(i - 1, g.c0, m); dd = D(i - 1, g.c0, m); }
+                int32_t mvv = NEG, ivv = NEG;
+                uint8_t cd = 0;
+                U[h] = VNEG;
+                b1s[h] = b2s[h] = NEG;
+                if (valid[h]) {
+                    const int64_t j = g.c0 + 1 + c;
+                    const int sc = score(qb, tb(j - 1));
+                    mvv = add_s(max(max(dm, dd), di), sc);
+                    const int32_t a1 = sat_add(um[h], o), a2 = sat_add(ui[h], e);
+                    ivv = max(a1, a2);
+                    cd = (uint8_t)(match_max(dm, di, dd) | ((a1 > a2) ? 4 : 0) | (mvv > 0 ? 16 : 0));
+                    U[h] = mvv + o - e * p;
+                    if (at0[h]) {  // left boundary column
+                        const int32_t b1 = sat_add(M(i, g.c0, m), o), b2 = sat_add(D(i, g.c0, m), e);
+                        b1s[h] = b1; b2s[h] = b2;
+                        U[h] = max(U[h], max(b1, b2) + e - e * p);
+                    }
+                }
+                mv[h] = mvv; iv[h] = ivv; code[h] = cd;
+            }
+            // inclusive prefix maximum of U over positions
+            int32_t P[NP];
+#pragma unroll
+            for (int h = 0; h < NP; ++h) {
+                int32_t x = U[h];
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int32_t y = __shfl_up_sync(FULL, x, d);
+                    if (lane >= d) x = max(x, y);
+                }
+                if (h > 0) x = max(x, __shfl_sync(FULL, P[h > 0 ? h - 1 : 0], 31));
+                P[h] = x;
+            }
+            int32_t dv[NP];
+#pragma unroll
+            for (int h = 0; h < NP; ++h) {
+                const int p = lane + 32 * h;
+                const int32_t t1 = __shfl_up_sync(FULL, P[h], 1);
+                const int32_t t2 = h > 0 ? __shfl_sync(FULL, P[h > 0 ? h - 1 : 0], 31) : VNEG;
+                const int32_t ex = lane > 0 ? t1 : t2;  // max over positions < p
+                int32_t dvv = NEG;
+                if (valid[h]) {
+                    if (at0[h]) dvv = max(b1s[h], b2s[h]);
+                    else dvv = (int32_t)max((int64_t)NEG, (int64_t)e * (p - 1) + (int64_t)ex);
+                }
+                dv[h] = dvv;
+            }
+#pragma unroll
+            for (int h = 0; h < NP; ++h) {  // delMax bit from the left neighbour
+                const int32_t lmA = __shfl_up_sync(FULL, mv[h], 1), ldA = __shfl_up_sync(FULL, dv[h], 1);
+                int32_t lmB = NEG, ldB = NEG;
+                if (h > 0) {
+                    lmB = __shfl_sync(FULL, mv[h > 0 ? h - 1 : 0], 31);
+                    ldB = __shfl_sync(FULL, dv[h > 0 ? h - 1 : 0], 31);
+                }
+                const int32_t lm = lane > 0 ? lmA : lmB, ld = lane > 0 ? ldA : ldB;
+                if (valid[h]) {
+                    const int p = lane + 32 * h;
+                    int32_t b1 = b1s[h], b2 = b2s[h];
+                    if (!at0[h]) {
+                        if (p >= 1 && col[h] >= 1) { b1 = sat_add(lm, o); b2 = sat_add(ld, e); }
+                        else { b1 = NEG; b2 = NEG; }
+                    }
+                    const uint8_t cd = (uint8_t)(code[h] | ((b1 > b2) ? 8 : 0));
+                    const int64_t c = col[h];
+                    code_base[(c + lr) * 32 + lr] = cd;
+                    if (rr == g.R - 1) { g.lastrow[c * 3] = mv[h]; g.lastrow[c * 3 + 1] = iv[h]; g.lastrow[c * 3 + 2] = dv[h]; }
+                    if (c == g.C - 1) { g.lastcol[rr * 3] = mv[h]; g.lastcol[rr * 3 + 1] = iv[h]; g.lastcol[rr * 3 + 2] = dv[h]; }
+                }
+                cells += __popc(__ballot_sync(FULL, valid[h]));
+                pm[h] = valid[h] ? mv[h] : NEG;
+                pi[h] = valid[h] ? iv[h] : NEG;
+                pd[h] = valid[h] ? dv[h] : NEG;
+            }
+        }
+        __syncwarp();
+        return cells;
+    }
+
     // Warp fill of rectangle m (Alignment::calculateScoresNW/SW,
     // Alignment.cpp:72-133): stripes of 32 rows, lane = row, one column per
     // step along the anti-diagonal wavefront; values travel by shuffles.
@@ -985,28 +1130,43 @@ __device__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, in
     if (WARP) __syncwarp();
     int32_t best = 0;       // local mode: M(0,0) = 0 is the first candidate
     int64_t bkey = 0;
-    // band half-widths of the 5' and 3' rectangles (thread path only)
-    const bool may_band = !WARP && a.band && a.pp.mode == 0;
+    // band half-widths of the 5' and 3' rectangles (GLOBAL mode)
+    const bool may_band = a.band && a.pp.mode == 0;
     const int w5 = may_band ? a.band[2 * c] : -1;
     const int w3 = may_band ? a.band[2 * c + 1] : -1;
     const bool banded = w5 >= 0 || w3 >= 0;
+    if (a.probe && !banded) return;  // certificate probe: the whole cell set needs no certificate
     int64_t cells = 0;
     int32_t x5 = NEG;       // best state value where the 5' rectangle meets the first seed
-    if (WARP) x.fill_rect(0, best, bkey); else cells += x.fill_rect_thread(0, w5, best, bkey);
-    for (int k = 0; k < x.n; ++k) {
-        const int m = 2 * k + 1;
-        if (lane == 0) {  // first diagonal cell (Alignment.cpp:146-153): max(M,D,I + s, 0)
-            const int64_t i = x.qf(k), j = x.ts(k);
-            const int32_t mx = max(max(x.M(i, j, m), x.D(i, j, m)), x.I(i, j, m));
-            x.diag[k] = max(add_s(mx, a.pp.match), 0);
-            if (k == 0) x5 = mx;
+    auto fill = [&](int m, int w) {
+        if constexpr (!WARP) {
+            cells += x.fill_rect_thread(m, w, best, bkey);
+        } else {
+            if (w >= 0) {
+                cells += w <= 15 ? x.template fill_rect_band<1>(m, w) : x.template fill_rect_band<2>(m, w);
+                return;
+            }
+            x.fill_rect(m, best, bkey);
+            const int64_t R = x.rb(m + 1) - x.rb(m), C = x.cb(m + 1) - x.cb(m);
+            if (R > 0 && C > 0) cells += R * C;
         }
-        if (WARP) __syncwarp();
-        if (WARP) x.fill_rect(m + 1, best, bkey);
-        else cells += x.fill_rect_thread(m + 1, m + 1 == 2 * x.n ? w3 : -1, best, bkey);
+    };
+    // 5' rectangle, then per seed its first diagonal cell and the rectangle after it
+    for (int q = 0; q <= x.n; ++q) {
+        if (q > 0) {
+            const int k = q - 1, m = 2 * k + 1;
+            if (lane == 0) {  // first diagonal cell (Alignment.cpp:146-153): max(M,D,I + s, 0)
+                const int64_t i = x.qf(k), j = x.ts(k);
+                const int32_t mx = max(max(x.M(i, j, m), x.D(i, j, m)), x.I(i, j, m));
+                x.diag[k] = max(add_s(mx, a.pp.match), 0);
+                if (k == 0) x5 = mx;
+            }
+            if (WARP) __syncwarp();
+        }
+        fill(2 * q, q == 0 ? w5 : q == x.n ? w3 : -1);
     }
     if (WARP) __syncwarp();
-    if (!WARP && a.bstat && cells) atomicAdd(a.bstat + 4, (unsigned long long)cells);
+    if (a.bstat && cells && lane == 0) atomicAdd(a.bstat + (WARP ? 3 : 4), (unsigned long long)cells);
     const int stage = 2 * x.n + 2;
     auto reduce = [&]() {
         if (WARP) {
@@ -1089,15 +1249,18 @@ __device__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, in
                 if (w3 >= 0) s_ub = max(s_ub, ub3 + d5);
                 res = (s_ub > (int64_t)NEG && below_filter(s_ub, x.L, a.min_rate)) ? 2 : 0;
             }
+            if (WARP) res = __shfl_sync(0xffffffffu, res, 0);  // x5 is lane 0's
             if (a.probe) {
-                a.probe[c] = (uint8_t)res;
-                a.probe_cells[c] = cells;
+                if (lane == 0) {
+                    a.probe[c] = (uint8_t)res;
+                    a.probe_cells[c] = cells;
+                }
                 return;
             }
-            if (a.bstat) atomicAdd(a.bstat + res, 1ull);  // [1] exact, [2] dropped, [0] fallback (counted below)
-            if (res == 2) { a.keep[c] = 0; return; }
+            if (a.bstat && lane == 0) atomicAdd(a.bstat + res, 1ull);  // [0] recomputed, [1] exact, [2] dropped
+            if (res == 2) { if (lane == 0) a.keep[c] = 0; return; }
             if (res == 0) {
-                a.fb_list[atomicAdd(a.fb_n, 1ull)] = c;
+                if (lane == 0) a.fb_list[atomicAdd(a.fb_n, 1ull)] = c;
                 return;
             }
         }
@@ -1127,11 +1290,6 @@ __device__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, in
         aln_to = bkey % (x.L + 1);
         aln_end = bkey / (x.L + 1);
         s0 = OP_M;
-    }
-    if (!WARP && a.probe) {  // certificate probe of a chain without a band: exact by construction
-        a.probe[c] = 1;
-        a.probe_cells[c] = cells;
-        return;
     }
     if (lane == 0) {
         const int32_t go = a.pp.gap_o, ge = a.pp.gap_e;
@@ -1225,14 +1383,6 @@ __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
     int32_t* rbnd = in_smem ? s_bnd[w][0] : reinterpret_cast<int32_t*>(gbase + n);
     int32_t* cbnd = in_smem ? s_bnd[w][1] : rbnd + 2 * n + 2;
     dp_chain<true>(a, c, sd, rbnd, cbnd);
-    if (a.bstat && lane_id() == 0) {  // cells of the whole cell set
-        int64_t cells = 0;
-        for (int m = 0; m <= 2 * n; m += 2) {
-            const int64_t R = rbnd[m + 1] - rbnd[m], C = cbnd[m + 1] - cbnd[m];
-            if (R > 0 && C > 0) cells += R * C;
-        }
-        atomicAdd(a.bstat + 3, (unsigned long long)cells);
-    }
 }
 
 // Chains whose rectangles are all small: one thread each.

@@ -75,7 +75,7 @@ class MapStats(C.Structure):
                                          "dp_cells", "host_sorted", "n_launch")] + \
                [(n, C.c_double) for n in ("ms_total", "ms_smem", "ms_locate", "ms_chain", "ms_dp")] + \
                [(n, C.c_int64) for n in ("dp_cells_done", "n_band_exact", "n_band_drop", "n_band_fallback",
-                                         "n_filtered")]
+                                         "n_filtered", "n_dp_warp")]
 
 
 def build(force: bool = False) -> str:
@@ -294,7 +294,8 @@ class Context:
 
     def band_collect(self, seq: np.ndarray, off: np.ndarray, params: MapParams | None = None):
         """Per-chain features (n x 16 float32) and cheapest certified band
-        class (int32) of a host read batch."""
+        class (int32; -1 for chains that never get a band) of a host read
+        batch."""
         params = params or default_params()
         seq = np.ascontiguousarray(seq, dtype=np.uint8)
         off = np.ascontiguousarray(off, dtype=np.int64)

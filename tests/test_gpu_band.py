@@ -105,7 +105,9 @@ def test_gradient_matches_oracle(ctx, world):
     g, _ = world
     _, seq, off = _mixed_reads(g, 81, 300, 150, 80)
     feat, lab = ctx.band_collect(seq, off, lib.default_params(min_score_rate=0.65, min_len=12))
-    assert len(lab) > 100 and set(np.unique(lab)) <= {0, 1, 2, 3}
+    assert set(np.unique(lab)) <= {-1, 0, 1, 2, 3}
+    feat, lab = feat[lab >= 0], lab[lab >= 0]
+    assert len(lab) > 50
     rng = np.random.default_rng(3)
     params = bm.random_params(rng, feat)
     grad, loss = ctx.band_grad(params, feat, lab)
@@ -120,11 +122,13 @@ def test_learned_band_is_exact_and_saves_cells(ctx, world, oracle_built):
     ps = dict(min_len=12, max_evalue=float("inf"), min_score_rate=0.65)
     _, tseq, toff = _mixed_reads(g, 91, 2000, 1000, 500)
     feat, lab = ctx.band_collect(tseq, toff, lib.default_params(**ps))
+    feat, lab = feat[lab >= 0], lab[lab >= 0]
     params, loss = ctx.band_train(feat, lab, epochs=30, batch=512, lr=3e-3, seed=7)
     assert loss[-1] < loss[0]
     # the device classifier and the oracle's agree on most fresh chains
     reads, seq, off = _mixed_reads(g, 101, 800, 400, 200)
     f2, l2 = ctx.band_collect(seq, off, lib.default_params(**ps))
+    f2, l2 = f2[l2 >= 0], l2[l2 >= 0]
     acc = float(np.mean(bm.classify(params, f2) == l2))
     assert acc > 0.5, acc
     plain = ctx.map(seq, off, lib.default_params(**ps))
