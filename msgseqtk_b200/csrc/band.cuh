@@ -152,8 +152,13 @@ __host__ __device__ inline bool bandable(int R, int C, int w) {
     return R > 0 && C > 0 && w < max(R, C) - 1 && 2 * (2 * w + 1) < C;
 }
 
+// List counters: counts[0] thread path, counts[1] warp path (whole cell
+// set), counts[kBandedCount] warp path with a band.
+constexpr int kBandedCount = 8;
+
 // Band half-widths per chain and the split into the thread path (chains of
-// at most kSmallArea cells, never banded) and the warp path (the rest).
+// at most kSmallArea cells, never banded), the warp path and the banded warp
+// path.
 // mode 0: no band; 1: fixed_w for every larger chain; 2: the classifier's
 // choice for larger chains with a flank that a band of half-width 7 would cut.
 // Each flank is banded only when bandable().
@@ -162,6 +167,7 @@ __global__ void __launch_bounds__(128) k_band_assign(int64_t n_chain, const int4
                                                      int mode, int fixed_w, const __nv_bfloat16* __restrict__ wts,
                                                      const float* __restrict__ nrm, int8_t* __restrict__ band,
                                                      int64_t* __restrict__ small, int64_t* __restrict__ big,
+                                                     int64_t* __restrict__ banded,
                                                      unsigned long long* __restrict__ counts) {
     __shared__ float sW[kNTrain];
     __shared__ float sN[2 * kFeat];
@@ -183,7 +189,8 @@ __global__ void __launch_bounds__(128) k_band_assign(int64_t n_chain, const int4
     const int w3 = (w >= 0 && bandable(g.z, g.w, w)) ? w : -1;
     band[2 * c] = (int8_t)w5;
     band[2 * c + 1] = (int8_t)w3;
-    if (w5 < 0 && w3 < 0 && area[c] <= kSmallArea) small[atomicAdd(&counts[0], 1ull)] = c;
+    if (w5 >= 0 || w3 >= 0) banded[atomicAdd(&counts[kBandedCount], 1ull)] = c;
+    else if (area[c] <= kSmallArea) small[atomicAdd(&counts[0], 1ull)] = c;
     else big[atomicAdd(&counts[1], 1ull)] = c;
 }
 

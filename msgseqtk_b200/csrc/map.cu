@@ -447,7 +447,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
 
     // ---------------- DP ----------------
     const int64_t NC = h_nchain + 1;
-    CK(ctx->dpinfo.ensure(NC * 8 * 15 + 256));
+    CK(ctx->dpinfo.ensure(NC * 8 * 15 + 256));  // 15 arrays of NC int64 + counters
     int64_t* d_ts = ctx->dpinfo.as<int64_t>();
     int64_t* d_te = d_ts + NC;
     int64_t* d_cells = d_te + NC;
@@ -462,7 +462,9 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     int64_t* d_fb = d_big + NC;
     int64_t* d_kidx = d_fb + NC;        // kept-record index per chain (n + 1)
     int64_t* d_map = d_kidx + NC;       // chain of each kept record
-    unsigned long long* d_ctr2 = reinterpret_cast<unsigned long long*>(d_map + NC);  // 0,1 lists; 2 fallback; 3.. stats
+    int64_t* d_bandl = d_map + NC;      // chains with a banded flank
+    // counters: 0 thread list, 1 warp list, 2 fallback list, 3..7 band stats, kBandedCount banded list
+    unsigned long long* d_ctr2 = reinterpret_cast<unsigned long long*>(d_bandl + NC);
     unsigned long long* d_bstat = d_ctr2 + 3;
     CK(ctx->geobuf.ensure(NC * sizeof(int4) + NC * kFeat * sizeof(float) + 64));
     int4* d_geo = ctx->geobuf.as<int4>();
@@ -531,13 +533,13 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         for (int64_t c = 0; c < h_nchain; ++c) best[c] = area[c];
         da.probe = d_probe; da.probe_cells = d_pcells;
         for (int cls = kCls - 2; cls >= 0; --cls) {  // wider classes first: ties keep the wider one
-            CK(cudaMemsetAsync(d_ctr2, 0, 64, st));
+            CK(cudaMemsetAsync(d_ctr2, 0, 128, st));
             CK(cudaMemsetAsync(d_probe, 3, h_nchain, st));  // 3: not banded at this class
             CK(cudaMemcpyAsync(d_pcells, d_area, h_nchain * 8, cudaMemcpyDeviceToDevice, st));
             S.n_launch++, k_band_assign<<<nblk(h_nchain, 128), 128, 0, st>>>(h_nchain, d_geo, d_area, d_feat, 1, band_width(cls),
-                                                                nullptr, nullptr, d_band, d_small, d_big, d_ctr2);
-            da.list = d_big; da.n_list = d_ctr2 + 1;  // banded chains are all on the warp path
-            S.n_launch++, k_dp<<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
+                                                                nullptr, nullptr, d_band, d_small, d_big, d_bandl, d_ctr2);
+            da.list = d_bandl; da.n_list = d_ctr2 + kBandedCount;
+            S.n_launch++, k_dp<true><<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(pr.data(), d_probe, h_nchain, cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(pc.data(), d_pcells, h_nchain * 8, cudaMemcpyDeviceToHost, st));
@@ -560,19 +562,22 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
 
     const bool filtering = params->min_score_rate >= 0;
     if (h_nchain > 0) {
-        CK(cudaMemsetAsync(d_ctr2, 0, 64, st));
+        CK(cudaMemsetAsync(d_ctr2, 0, 128, st));
         const int bmode = dpp.mode != 0 ? 0 : params->band_mode;
         S.n_launch++, k_band_assign<<<nblk(h_nchain, 128), 128, 0, st>>>(h_nchain, d_geo, d_area, d_feat, bmode, params->band_w,
-                                                            d_wts, d_nrm, d_band, d_small, d_big, d_ctr2);
+                                                            d_wts, d_nrm, d_band, d_small, d_big, d_bandl, d_ctr2);
         // Every launch is sized for every chain; each reads its list length on
         // the device, so no host round trip is needed for the split.
         da.list = d_small; da.n_list = d_ctr2;
         S.n_launch++, k_dp_small<<<nblk(h_nchain, 128), 128, 0, st>>>(da);
         da.list = d_big; da.n_list = d_ctr2 + 1;
-        S.n_launch++, k_dp<<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
-        if (bmode != 0) {  // banded chains without a certificate, on the whole cell set
+        S.n_launch++, k_dp<false><<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
+        if (bmode != 0) {
+            da.list = d_bandl; da.n_list = d_ctr2 + kBandedCount;
+            S.n_launch++, k_dp<true><<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
+            // banded chains without a certificate, on the whole cell set
             da.list = d_fb; da.n_list = d_ctr2 + 2; da.band = nullptr;
-            S.n_launch++, k_dp<<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
+            S.n_launch++, k_dp<false><<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
         }
         CK(cudaGetLastError());
     }
@@ -611,7 +616,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     }
     tm.mark();  // 5
     uint32_t h_status = 0;
-    unsigned long long h_ctr2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long h_ctr2[kBandedCount + 1] = {0};
     const unsigned long long* h_bstat = h_ctr2 + 3;
     CK(cudaMemcpyAsync(&h_status, d_status, 4, cudaMemcpyDeviceToHost, st));
     if (h_nchain > 0) CK(cudaMemcpyAsync(h_ctr2, d_ctr2, sizeof(h_ctr2), cudaMemcpyDeviceToHost, st));
@@ -623,7 +628,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     S.n_band_drop = (int64_t)h_bstat[2];
     S.dp_cells_done = (int64_t)(h_bstat[3] + h_bstat[4]);
     S.n_filtered = h_nchain - h_nrec;
-    S.n_dp_warp = (int64_t)h_ctr2[1];
+    S.n_dp_warp = (int64_t)(h_ctr2[1] + h_ctr2[kBandedCount]);
     S.ms_smem = tm.ms(0, 1);
     S.ms_locate = tm.ms(1, 2);
     S.ms_chain = tm.ms(2, 3);

@@ -687,13 +687,23 @@ struct ChainCtx {
         return NEG;
     }
 
+    // M, I, D (or M, D) of a boundary cell, out of line: the band fill reads
+    // boundaries at a handful of cells, and inlining each query at each of
+    // its sites would bloat the banded kernel's code.
+    __device__ __noinline__ int3 MID(int64_t i, int64_t j, int stage) const {
+        return make_int3(M(i, j, stage), I(i, j, stage), D(i, j, stage));
+    }
+    __device__ __noinline__ int2 MD(int64_t i, int64_t j, int stage) const {
+        return make_int2(M(i, j, stage), D(i, j, stage));
+    }
+
     // Single-thread fill of rectangle m, row by row, into the same code layout
     // (rowbuf holds the row above). With w >= 0 only the cells within w
     // diagonals of the adjacent seed's diagonal are computed (the 5' rectangle
     // ends on it, the 3' rectangle starts on it); the other cells count as
     // -inf and their stored last-row/last-column values are -inf. Returns the
     // number of cells computed.
-    __device__ int64_t fill_rect_thread(int m, int w, int32_t& best, int64_t& bkey) {
+    __device__ __forceinline__ int64_t fill_rect_thread(int m, int w, int32_t& best, int64_t& bkey) {
         const RectGeo g = rect(m);
         if (g.R <= 0 || g.C <= 0) return 0;
         const int32_t o = -(pp.gap_o + pp.gap_e), e = -pp.gap_e;
@@ -787,8 +797,8 @@ struct ChainCtx {
             const int64_t c = dg - w + p - 1;
             pm[h] = pi[h] = pd[h] = NEG;
             if (p <= NB && c >= -1 && c <= g.C - 1) {
-                const int64_t j = g.c0 + 1 + c;
-                pm[h] = M(g.r0, j, m); pi[h] = I(g.r0, j, m); pd[h] = D(g.r0, j, m);
+                const int3 v = MID(g.r0, g.c0 + 1 + c, m);
+                pm[h] = v.x; pi[h] = v.y; pd[h] = v.z;
             }
         }
         __syncwarp();
@@ -822,7 +832,7 @@ struct ChainCtx {
                 valid[h] = p < NB && c >= 0 && c < g.C;
                 at0[h] = valid[h] && c == 0;
                 int32_t dm = pm[h], di = pi[h], dd = pd[h];
-                if (at0[h]) { dm = M(i - 1, g.c0, m); di = I(i - 1, g.c0, m); dd = D(i - 1, g.c0, m); }
+                if (at0[h]) { const int3 v = MID(i - 1, g.c0, m); dm = v.x; di = v.y; dd = v.z; }
                 int32_t mvv = NEG, ivv = NEG;
                 uint8_t cd = 0;
                 U[h] = VNEG;
@@ -836,7 +846,8 @@ struct ChainCtx {
                     cd = (uint8_t)(match_max(dm, di, dd) | ((a1 > a2) ? 4 : 0) | (mvv > 0 ? 16 : 0));
                     U[h] = mvv + o - e * p;
                     if (at0[h]) {  // left boundary column
-                        const int32_t b1 = sat_add(M(i, g.c0, m), o), b2 = sat_add(D(i, g.c0, m), e);
+                        const int2 l = MD(i, g.c0, m);
+                        const int32_t b1 = sat_add(l.x, o), b2 = sat_add(l.y, e);
                         b1s[h] = b1; b2s[h] = b2;
                         U[h] = max(U[h], max(b1, b2) + e - e * p);
                     }
@@ -906,7 +917,7 @@ struct ChainCtx {
     // Alignment.cpp:72-133): stripes of 32 rows, lane = row, one column per
     // step along the anti-diagonal wavefront; values travel by shuffles.
     // Returns this lane's best (M, column-major key) for local mode.
-    __device__ void fill_rect(int m, int32_t& best, int64_t& bkey) {
+    __device__ __forceinline__ void fill_rect(int m, int32_t& best, int64_t& bkey) {
         const RectGeo g = rect(m);
         if (g.R <= 0 || g.C <= 0) return;
         const int lane = lane_id();
@@ -1074,8 +1085,8 @@ __global__ void k_dp_prep(IndexDev ix, const Seed* __restrict__ seeds, const int
 
 // One chain: a warp (WARP = true; lanes share the rectangle wavefront and the
 // last-row scan) or a single thread (chains whose rectangles are all small).
-template <bool WARP>
-__device__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, int32_t* cbnd) {
+template <bool WARP, bool BAND>
+__device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, int32_t* cbnd) {
     const int lane = WARP ? lane_id() : 0;
     const int stride = WARP ? 32 : 1;
     ChainCtx x;
@@ -1131,10 +1142,10 @@ __device__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, in
     int32_t best = 0;       // local mode: M(0,0) = 0 is the first candidate
     int64_t bkey = 0;
     // band half-widths of the 5' and 3' rectangles (GLOBAL mode)
-    const bool may_band = a.band && a.pp.mode == 0;
+    const bool may_band = BAND && a.band && a.pp.mode == 0;
     const int w5 = may_band ? a.band[2 * c] : -1;
     const int w3 = may_band ? a.band[2 * c + 1] : -1;
-    const bool banded = w5 >= 0 || w3 >= 0;
+    const bool banded = BAND && (w5 >= 0 || w3 >= 0);
     if (a.probe && !banded) return;  // certificate probe: the whole cell set needs no certificate
     int64_t cells = 0;
     int32_t x5 = NEG;       // best state value where the 5' rectangle meets the first seed
@@ -1142,9 +1153,11 @@ __device__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, in
         if constexpr (!WARP) {
             cells += x.fill_rect_thread(m, w, best, bkey);
         } else {
-            if (w >= 0) {
-                cells += w <= 15 ? x.template fill_rect_band<1>(m, w) : x.template fill_rect_band<2>(m, w);
-                return;
+            if constexpr (BAND) {
+                if (w >= 0) {
+                    cells += w <= 15 ? x.template fill_rect_band<1>(m, w) : x.template fill_rect_band<2>(m, w);
+                    return;
+                }
             }
             x.fill_rect(m, best, bkey);
             const int64_t R = x.rb(m + 1) - x.rb(m), C = x.cb(m + 1) - x.cb(m);
@@ -1369,7 +1382,10 @@ __device__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, in
 }
 
 
-__global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
+// One warp per chain. BAND: the chains with a banded flank (GLOBAL mode);
+// kept apart so that each kernel holds only the fills it runs.
+template <bool BAND>
+__global__ void __launch_bounds__(kDpWarps * 32, 4) k_dp(DpArgs a) {
     __shared__ int4 s_sd[kDpWarps][kSmemSeeds];
     __shared__ int32_t s_bnd[kDpWarps][2][2 * kSmemSeeds + 2];
     const int w = threadIdx.x >> 5;
@@ -1382,7 +1398,7 @@ __global__ void __launch_bounds__(kDpWarps * 32) k_dp(DpArgs a) {
     int4* sd = in_smem ? s_sd[w] : gbase;
     int32_t* rbnd = in_smem ? s_bnd[w][0] : reinterpret_cast<int32_t*>(gbase + n);
     int32_t* cbnd = in_smem ? s_bnd[w][1] : rbnd + 2 * n + 2;
-    dp_chain<true>(a, c, sd, rbnd, cbnd);
+    dp_chain<true, BAND>(a, c, sd, rbnd, cbnd);
 }
 
 // Chains whose rectangles are all small: one thread each.
@@ -1393,7 +1409,7 @@ __global__ void __launch_bounds__(128) k_dp_small(DpArgs a) {
     const int n = a.chain_len[c];
     int4* gbase = a.sdbuf + 2 * a.chain_idx_off[c] + c;
     int32_t* rbnd = reinterpret_cast<int32_t*>(gbase + n);
-    dp_chain<false>(a, c, gbase, rbnd, rbnd + 2 * n + 2);
+    dp_chain<false, false>(a, c, gbase, rbnd, rbnd + 2 * n + 2);
 }
 
 // CIGAR runs (Alignment::getAlnCigar): 5' clip, the reversed path in runs, 3' clip.
