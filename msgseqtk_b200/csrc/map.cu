@@ -447,7 +447,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
 
     // ---------------- DP ----------------
     const int64_t NC = h_nchain + 1;
-    CK(ctx->dpinfo.ensure(NC * 8 * 15 + 256));  // 15 arrays of NC int64 + counters
+    CK(ctx->dpinfo.ensure(NC * 8 * 16 + 256));  // 16 arrays of NC int64 + counters
     int64_t* d_ts = ctx->dpinfo.as<int64_t>();
     int64_t* d_te = d_ts + NC;
     int64_t* d_cells = d_te + NC;
@@ -463,8 +463,10 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     int64_t* d_kidx = d_fb + NC;        // kept-record index per chain (n + 1)
     int64_t* d_map = d_kidx + NC;       // chain of each kept record
     int64_t* d_bandl = d_map + NC;      // chains with a banded flank
-    // counters: 0 thread list, 1 warp list, 2 fallback list, 3..7 band stats, kBandedCount banded list
-    unsigned long long* d_ctr2 = reinterpret_cast<unsigned long long*>(d_bandl + NC);
+    int64_t* d_tbl = d_bandl + NC;      // chains traced back by k_traceback
+    // counters: 0 thread list, 1 warp list, 2 fallback list, 3..7 band stats,
+    // kBandedCount banded list, kBandedCount + 1 traceback list
+    unsigned long long* d_ctr2 = reinterpret_cast<unsigned long long*>(d_tbl + NC);
     unsigned long long* d_bstat = d_ctr2 + 3;
     CK(ctx->geobuf.ensure(NC * sizeof(int4) + NC * kFeat * sizeof(float) + 64));
     int4* d_geo = ctx->geobuf.as<int4>();
@@ -514,6 +516,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     da.pp = dpp; da.status = d_status;
     da.band = d_band; da.min_rate = params->min_score_rate; da.keep = d_keep; da.fb_list = d_fb;
     da.fb_n = d_ctr2 + 2; da.bstat = d_bstat;
+    da.tb_list = d_tbl; da.tb_n = d_ctr2 + kBandedCount + 1;
     const __nv_bfloat16* d_wts = ctx->band_wts.as<__nv_bfloat16>();
     const float* d_nrm = ctx->band_nrm.as<float>();
 
@@ -579,6 +582,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             da.list = d_fb; da.n_list = d_ctr2 + 2; da.band = nullptr;
             S.n_launch++, k_dp<false><<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
         }
+        S.n_launch++, k_traceback<<<nblk(h_nchain, 128), 128, 0, st>>>(da);
         CK(cudaGetLastError());
     }
     tm.mark();  // 4

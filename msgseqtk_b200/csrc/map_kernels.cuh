@@ -1015,6 +1015,8 @@ struct DpArgs {
     uint32_t* status;
     const int64_t* list;                  // chains handled by this launch
     const unsigned long long* n_list;     // its length, on the device
+    int64_t* tb_list;                     // chains whose traceback k_traceback runs
+    unsigned long long* tb_n;
     // Banded flanks (GLOBAL mode). band[2c], band[2c+1]: half-width of the 5'
     // and 3' rectangle's band, -1 for the whole rectangle.
     const int8_t* band;
@@ -1085,8 +1087,92 @@ __global__ void k_dp_prep(IndexDev ix, const Seed* __restrict__ seeds, const int
 
 // One chain: a warp (WARP = true; lanes share the rectangle wavefront and the
 // last-row scan) or a single thread (chains whose rectangles are all small).
+// Traceback of one chain (Alignment::backTraceNW/SW, Alignment.cpp:173-276)
+// from the end cell (aln_to, aln_end) in state s0, writing the reversed path
+// and the alignment record.
+__device__ __forceinline__ void dp_traceback(const DpArgs& a, int64_t c, const ChainCtx& x, int64_t r, const Seed& f,
+                                             int64_t t_start, int64_t aln_to, int64_t aln_end, int s0, int32_t best,
+                                             int32_t flags) {
+    const int stage = 2 * x.n + 2;
+    uint8_t* path = a.path + a.path_off[c];
+    const int32_t go = a.pp.gap_o, ge = a.pp.gap_e;
+    int64_t i = aln_to, j = aln_end;
+    int s = s0;
+    int64_t np = 0;
+    const int64_t cap = x.L + x.T + 1;
+    int cur_m = -1;  // rectangle holding (i, j), if any
+    RectGeo g{};
+    for (;;) {
+        // locate (i, j): inside a rectangle -> traceback codes
+        bool in_rect = false;
+        if (i >= 1 && j >= 1) {
+            if (cur_m >= 0 && i > g.r0 && i <= g.r0 + g.R && j > g.c0 && j <= g.c0 + g.C) in_rect = true;
+            else {
+                const int mr = x.row_seg(i);
+                if (mr == x.col_seg(j) && !(mr & 1)) { cur_m = mr; g = x.rect(mr); in_rect = true; }
+            }
+        }
+        const uint8_t code = in_rect ? x.code_at(g, i, j) : 0;
+        if (a.pp.mode == 0) { if (!(i > 0)) break; }
+        else {
+            const bool mpos = in_rect ? ((code >> 4) & 1) : (x.M(i, j, stage) > 0);
+            if (!(s != OP_M || mpos)) break;
+        }
+        const bool ok = (s == OP_M) ? (i >= 1 && j >= 1) : (s == OP_I) ? (i >= 1) : (j >= 1);
+        if (!ok || np >= cap) { flags |= 2; break; }
+        if (s == OP_M && !in_rect && (a.pp.mode == 0 || a.pp.match >= 1)) {
+            // Inside a seed block, diagonal cells d >= 1 have I = D = -inf
+            // (no I-row or D-column overwrite reaches past the block's first
+            // row/column), so matchMax keeps M: walk straight to d = 1.
+            const int mr = x.row_seg(i);
+            if ((mr & 1) && mr == x.col_seg(j)) {
+                const int k = (mr - 1) >> 1;
+                const int64_t d = i - x.qf(k) - 1;
+                if (d == j - x.ts(k) - 1 && d >= 2 && np + d - 1 <= cap) {
+                    for (int64_t q = 0; q < d - 1; ++q) path[np + q] = (uint8_t)OP_M;
+                    np += d - 1;
+                    i -= d - 1;
+                    j -= d - 1;
+                    continue;
+                }
+            }
+        }
+        path[np++] = (uint8_t)s;
+        if (s == OP_M) {
+            s = in_rect ? (code & 3) : match_max(x.M(i - 1, j - 1, stage), x.I(i - 1, j - 1, stage), x.D(i - 1, j - 1, stage));
+            i--; j--;
+        } else if (s == OP_I) {
+            const bool mm = in_rect ? ((code >> 2) & 1)
+                                    : sat_add(x.M(i - 1, j, stage), -(go + ge)) > sat_add(x.I(i - 1, j, stage), -ge);
+            s = mm ? OP_M : OP_I;
+            i--;
+        } else {
+            const bool mm = in_rect ? ((code >> 3) & 1)
+                                    : sat_add(x.M(i, j - 1, stage), -(go + ge)) > sat_add(x.D(i, j - 1, stage), -ge);
+            s = mm ? OP_M : OP_D;
+            j--;
+        }
+    }
+    a.path_len[c] = (int32_t)np;
+    msg_aln& o = a.aln[c];
+    o.read = r;
+    o.tid = f.tid;
+    o.strand = f.strand;
+    o.t_start = t_start;
+    o.t_end = a.t_end[c];
+    o.aln_from = i;
+    o.aln_to = aln_to;
+    o.aln_start = t_start + j;
+    o.aln_end = t_start + aln_end;
+    o.aln_score = best == NEG ? INT32_MIN : best;
+    o.flags = flags;
+    if (flags & 2) atomicOr(a.status, kErrTrace);
+    if (a.keep) a.keep[c] = (best == NEG || below_filter(best, x.L, a.min_rate)) && a.min_rate >= 0 ? 0 : 1;
+}
+
 template <bool WARP, bool BAND>
-__device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, int32_t* cbnd) {
+__device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, int32_t* cbnd,
+                                         int4* gsd) {
     const int lane = WARP ? lane_id() : 0;
     const int stride = WARP ? 32 : 1;
     ChainCtx x;
@@ -1106,22 +1192,35 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
     x.roff = aux + x.n;
     x.pp = a.pp;
     x.status = a.status;
+    // geometry in sd/rbnd/cbnd; a warp working in shared memory also leaves a
+    // copy in the chain's global slot (gsd) for k_traceback
+    int32_t* grb = reinterpret_cast<int32_t*>(gsd + x.n);
+    int32_t* gcb = grb + 2 * x.n + 2;
+    const bool copy = WARP && gsd != sd;
     for (int k = lane; k < x.n; k += stride) {
         const Seed s = a.seeds[idx[k]];
         const int4 g = make_int4(s.from, s.to, (int)(s.start - t_start), (int)(s.end - t_start));
         sd[k] = g;
         rbnd[2 * k + 1] = g.x; rbnd[2 * k + 2] = g.y;
         cbnd[2 * k + 1] = g.z; cbnd[2 * k + 2] = g.w;
+        if (copy) {
+            gsd[k] = g;
+            grb[2 * k + 1] = g.x; grb[2 * k + 2] = g.y;
+            gcb[2 * k + 1] = g.z; gcb[2 * k + 2] = g.w;
+        }
     }
     if (lane == 0) {
         rbnd[0] = 0; cbnd[0] = 0;
         rbnd[2 * x.n + 1] = (int32_t)x.L; cbnd[2 * x.n + 1] = (int32_t)x.T;
+        if (copy) {
+            grb[0] = 0; gcb[0] = 0;
+            grb[2 * x.n + 1] = (int32_t)x.L; gcb[2 * x.n + 1] = (int32_t)x.T;
+        }
     }
     x.sd = sd;
     x.rbnd = rbnd;
     x.cbnd = cbnd;
     const uint8_t* rd = a.rseq + a.roff[r];
-    uint8_t* path = a.path + a.path_off[c];
     if (f.strand == FWD) {
         x.query = rd;
     } else {  // PrimarySeq::revcom
@@ -1304,80 +1403,21 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
         aln_end = bkey / (x.L + 1);
         s0 = OP_M;
     }
-    if (lane == 0) {
-        const int32_t go = a.pp.gap_o, ge = a.pp.gap_e;
-        int64_t i = aln_to, j = aln_end;
-        int s = s0;
-        int64_t np = 0;
-        const int64_t cap = x.L + x.T + 1;
-        int cur_m = -1;  // rectangle holding (i, j), if any
-        RectGeo g{};
-        for (;;) {
-            // locate (i, j): inside a rectangle -> traceback codes
-            bool in_rect = false;
-            if (i >= 1 && j >= 1) {
-                if (cur_m >= 0 && i > g.r0 && i <= g.r0 + g.R && j > g.c0 && j <= g.c0 + g.C) in_rect = true;
-                else {
-                    const int mr = x.row_seg(i);
-                    if (mr == x.col_seg(j) && !(mr & 1)) { cur_m = mr; g = x.rect(mr); in_rect = true; }
-                }
-            }
-            const uint8_t code = in_rect ? x.code_at(g, i, j) : 0;
-            if (a.pp.mode == 0) { if (!(i > 0)) break; }
-            else {
-                const bool mpos = in_rect ? ((code >> 4) & 1) : (x.M(i, j, stage) > 0);
-                if (!(s != OP_M || mpos)) break;
-            }
-            const bool ok = (s == OP_M) ? (i >= 1 && j >= 1) : (s == OP_I) ? (i >= 1) : (j >= 1);
-            if (!ok || np >= cap) { flags |= 2; break; }
-            if (s == OP_M && !in_rect && (a.pp.mode == 0 || a.pp.match >= 1)) {
-                // Inside a seed block, diagonal cells d >= 1 have I = D = -inf
-                // (no I-row or D-column overwrite reaches past the block's first
-                // row/column), so matchMax keeps M: walk straight to d = 1.
-                const int mr = x.row_seg(i);
-                if ((mr & 1) && mr == x.col_seg(j)) {
-                    const int k = (mr - 1) >> 1;
-                    const int64_t d = i - x.qf(k) - 1;
-                    if (d == j - x.ts(k) - 1 && d >= 2 && np + d - 1 <= cap) {
-                        for (int64_t q = 0; q < d - 1; ++q) path[np + q] = (uint8_t)OP_M;
-                        np += d - 1;
-                        i -= d - 1;
-                        j -= d - 1;
-                        continue;
-                    }
-                }
-            }
-            path[np++] = (uint8_t)s;
-            if (s == OP_M) {
-                s = in_rect ? (code & 3) : match_max(x.M(i - 1, j - 1, stage), x.I(i - 1, j - 1, stage), x.D(i - 1, j - 1, stage));
-                i--; j--;
-            } else if (s == OP_I) {
-                const bool mm = in_rect ? ((code >> 2) & 1)
-                                        : sat_add(x.M(i - 1, j, stage), -(go + ge)) > sat_add(x.I(i - 1, j, stage), -ge);
-                s = mm ? OP_M : OP_I;
-                i--;
-            } else {
-                const bool mm = in_rect ? ((code >> 3) & 1)
-                                        : sat_add(x.M(i, j - 1, stage), -(go + ge)) > sat_add(x.D(i, j - 1, stage), -ge);
-                s = mm ? OP_M : OP_D;
-                j--;
-            }
+    if constexpr (WARP) {
+        // Hand the start of the traceback to k_traceback (one thread per
+        // chain): the record carries the end cell, the score and flags, and
+        // `pad` the starting state.
+        if (lane == 0) {
+            msg_aln& o = a.aln[c];
+            o.aln_to = aln_to;
+            o.aln_end = aln_end;
+            o.aln_score = best;
+            o.flags = flags;
+            o.pad = s0;
+            a.tb_list[atomicAdd(a.tb_n, 1ull)] = c;
         }
-        a.path_len[c] = (int32_t)np;
-        msg_aln& o = a.aln[c];
-        o.read = r;
-        o.tid = f.tid;
-        o.strand = f.strand;
-        o.t_start = t_start;
-        o.t_end = a.t_end[c];
-        o.aln_from = i;
-        o.aln_to = aln_to;
-        o.aln_start = t_start + j;
-        o.aln_end = t_start + aln_end;
-        o.aln_score = best == NEG ? INT32_MIN : best;
-        o.flags = flags;
-        if (flags & 2) atomicOr(a.status, kErrTrace);
-        if (a.keep) a.keep[c] = (best == NEG || below_filter(best, x.L, a.min_rate)) && a.min_rate >= 0 ? 0 : 1;
+    } else {
+        dp_traceback(a, c, x, r, f, t_start, aln_to, aln_end, s0, best, flags);
     }
 }
 
@@ -1385,7 +1425,7 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
 // One warp per chain. BAND: the chains with a banded flank (GLOBAL mode);
 // kept apart so that each kernel holds only the fills it runs.
 template <bool BAND>
-__global__ void __launch_bounds__(kDpWarps * 32, 4) k_dp(DpArgs a) {
+__global__ void __launch_bounds__(kDpWarps * 32, BAND ? 4 : 6) k_dp(DpArgs a) {
     __shared__ int4 s_sd[kDpWarps][kSmemSeeds];
     __shared__ int32_t s_bnd[kDpWarps][2][2 * kSmemSeeds + 2];
     const int w = threadIdx.x >> 5;
@@ -1398,7 +1438,7 @@ __global__ void __launch_bounds__(kDpWarps * 32, 4) k_dp(DpArgs a) {
     int4* sd = in_smem ? s_sd[w] : gbase;
     int32_t* rbnd = in_smem ? s_bnd[w][0] : reinterpret_cast<int32_t*>(gbase + n);
     int32_t* cbnd = in_smem ? s_bnd[w][1] : rbnd + 2 * n + 2;
-    dp_chain<true, BAND>(a, c, sd, rbnd, cbnd);
+    dp_chain<true, BAND>(a, c, sd, rbnd, cbnd, gbase);
 }
 
 // Chains whose rectangles are all small: one thread each.
@@ -1409,7 +1449,38 @@ __global__ void __launch_bounds__(128) k_dp_small(DpArgs a) {
     const int n = a.chain_len[c];
     int4* gbase = a.sdbuf + 2 * a.chain_idx_off[c] + c;
     int32_t* rbnd = reinterpret_cast<int32_t*>(gbase + n);
-    dp_chain<false, false>(a, c, gbase, rbnd, rbnd + 2 * n + 2);
+    dp_chain<false, false>(a, c, gbase, rbnd, rbnd + 2 * n + 2, gbase);
+}
+
+// Tracebacks of the chains filled by the warp kernels, one thread each (a
+// traceback is a serial walk; a warp per chain would leave 31 lanes idle).
+__global__ void __launch_bounds__(128, 6) k_traceback(DpArgs a) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)*a.tb_n) return;
+    const int64_t c = a.tb_list[t];
+    ChainCtx x;
+    const int64_t* idx = a.chain_idx + a.chain_idx_off[c];
+    x.n = a.chain_len[c];
+    const int64_t r = a.chain_read[c];
+    x.L = a.roff[r + 1] - a.roff[r];
+    const int64_t t_start = a.t_start[c];
+    x.T = a.t_end[c] - t_start;
+    const Seed f = a.seeds[idx[0]];
+    x.target = a.ix.chr_seq + a.ix.chr_off[f.tid] + t_start;
+    x.target_avail = a.ix.chr_len[f.tid] - t_start;
+    x.scratch = a.scr + a.scr_off[c];
+    int32_t* aux = a.aux + 2 * a.chain_idx_off[c] + c;
+    x.diag = aux;
+    x.roff = aux + x.n;
+    x.pp = a.pp;
+    x.status = a.status;
+    int4* gbase = a.sdbuf + 2 * a.chain_idx_off[c] + c;
+    x.sd = gbase;
+    x.rbnd = reinterpret_cast<int32_t*>(gbase + x.n);
+    x.cbnd = x.rbnd + 2 * x.n + 2;
+    x.query = f.strand == FWD ? a.rseq + a.roff[r] : a.qbuf + a.path_off[c];
+    const msg_aln h = a.aln[c];
+    dp_traceback(a, c, x, r, f, t_start, h.aln_to, h.aln_end, h.pad, h.aln_score, h.flags);
 }
 
 // CIGAR runs (Alignment::getAlnCigar): 5' clip, the reversed path in runs, 3' clip.
