@@ -99,16 +99,21 @@ __global__ void k_i32_to_i64(const int32_t* __restrict__ a, int64_t* __restrict_
 __global__ void k_read_len(const int64_t* __restrict__ off, int64_t n, int64_t* __restrict__ len,
                            unsigned long long* __restrict__ mx) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int64_t l = off[i + 1] - off[i];
-    len[i] = l;
-    atomicMax(mx, (unsigned long long)(l < 0 ? 0 : l));
+    unsigned long long l = 0;
+    if (i < n) {
+        const int64_t v = off[i + 1] - off[i];
+        len[i] = v;
+        l = v < 0 ? 0 : (unsigned long long)v;
+    }
+    for (int o = 16; o > 0; o >>= 1) l = max(l, __shfl_xor_sync(0xffffffffu, l, o));  // one atomic per warp
+    if ((threadIdx.x & 31) == 0 && l > 0) atomicMax(mx, l);
 }
 
+// One warp per read.
 __global__ void k_smem_read(const int64_t* __restrict__ smem_off, int64_t n_reads, int32_t* __restrict__ smem_read) {
-    const int64_t r = blockIdx.x;
+    const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (r >= n_reads) return;
-    for (int64_t k = smem_off[r] + threadIdx.x; k < smem_off[r + 1]; k += blockDim.x) smem_read[k] = (int32_t)r;
+    for (int64_t k = smem_off[r] + (threadIdx.x & 31); k < smem_off[r + 1]; k += 32) smem_read[k] = (int32_t)r;
 }
 
 __global__ void k_gather_off(const int64_t* __restrict__ smem_off, const int64_t* __restrict__ smem_seed_off,
@@ -335,7 +340,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     int32_t* d_fill = d_smem_read + (h_nsmem + 1);
     uint8_t* d_sel = reinterpret_cast<uint8_t*>(d_fill + (h_nsmem + 1));
     if (n_reads > 0) {
-        S.n_launch++, k_compact_smem<<<n_reads, 64, 0, st>>>(ctx->smem.as<int64_t>(), cap, ctx->smem_cnt.as<int32_t>(), d_smem_off,
+        S.n_launch++, k_compact_smem<<<nblk(n_reads * 32, 256), 256, 0, st>>>(ctx->smem.as<int64_t>(), cap, ctx->smem_cnt.as<int32_t>(), d_smem_off,
                                                n_reads, d_smem);
         CK(cudaGetLastError());
     }
@@ -391,7 +396,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     CK(offsets(ctx, d_smem_seed_cnt, h_nsmem, d_smem_seed_off, misc, &h_nseed_raw));
     if (n_reads > 0) {
         S.n_launch++, k_gather_off<<<nblk(n_reads + 1, 256), 256, 0, st>>>(d_smem_off, d_smem_seed_off, n_reads, d_read_seed_off);
-        S.n_launch++, k_smem_read<<<n_reads, 64, 0, st>>>(d_smem_off, n_reads, d_smem_read);
+        S.n_launch++, k_smem_read<<<nblk(n_reads * 32, 256), 256, 0, st>>>(d_smem_off, n_reads, d_smem_read);
         CK(cudaGetLastError());
     }
 

@@ -294,12 +294,13 @@ __global__ void __launch_bounds__(256) k_smem(SmemArgs a, IndexDev ix) {
 }
 
 // Copy each read's SMEMs into a dense array (read r at smem_off[r]).
+// One warp per read.
 __global__ void k_compact_smem(const int64_t* __restrict__ src, int64_t cap, const int32_t* __restrict__ count,
                                const int64_t* __restrict__ smem_off, int64_t n_reads, int64_t* __restrict__ dst) {
-    const int64_t r = blockIdx.x;
+    const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (r >= n_reads) return;
     const int64_t n = min((int64_t)count[r], cap);
-    for (int64_t j = threadIdx.x; j < 6 * n; j += blockDim.x) dst[6 * smem_off[r] + j] = src[6 * r * cap + j];
+    for (int64_t j = lane_id(); j < 6 * n; j += 32) dst[6 * smem_off[r] + j] = src[6 * r * cap + j];
 }
 
 // ======================================================================

@@ -6,6 +6,16 @@
 // lists (`prev`) live in per-thread global scratch; their processing follows
 // the reference's sequential loop entry by entry (validity by the running
 // size s0, emission while nValid == 0, in-place compaction).
+//
+// findFwdBackSMEMS and findBackFwdSMEMS are mirror images: a walk that
+// extends one end of the interval until it fails, then passes over the
+// candidates that extend the other end. Both run on one code path here, with
+// a direction flag `fb` and intervals kept "oriented", i.e. with the two
+// bounds ordered so that the extension at hand is always a backward one
+// (fwdExt(p, q) = backExt(q, p), FMDIndex.h:226-228): the walk's interval is
+// (q, p) in a forward-then-backward call and (p, q) otherwise, and candidates
+// are stored the other way round. Lanes of a warp in either kind of call then
+// execute the same instructions.
 #pragma once
 #include <math_constants.h>
 
@@ -17,14 +27,8 @@ namespace msg {
 // rows) and read positions below 2^31, so the per-thread state is 32-bit.
 struct PrevEntry {
     double lp;
-    uint32_t p, q, s;
-    int32_t pos;  // `to` (fwd-back) or `from` (back-fwd) of the entry
-};
-
-struct SmemState32 {
-    double lp;
-    int32_t from, to;
-    uint32_t p, q, s;
+    uint32_t p, q, s;  // p, q in candidate orientation (see above)
+    int32_t pos;       // `to` (fwd-back) or `from` (back-fwd) of the entry
 };
 
 struct SmemThreadArgs {
@@ -50,12 +54,9 @@ enum SmemPhase : int {
     PH_NEXT_READ = 0,
     PH_OUTER_LOOP,      // while (from > 0 || to < L)
     PH_OUTER_BACK,      // --from; back-fwd call
-    PH_FB_WALK,         // forward walk of findFwdBackSMEMS
-    PH_FB_ITER,         // start of one backward pass over prev
-    PH_FB_ENTRY,        // one prev entry of that pass
-    PH_BF_WALK,         // backward walk of findBackFwdSMEMS
-    PH_BF_ITER,
-    PH_BF_ENTRY,
+    PH_WALK,            // the walk of either call
+    PH_ITER,            // start of one pass over prev
+    PH_ENTRY,           // one prev entry of that pass
     PH_DONE
 };
 
@@ -68,9 +69,15 @@ struct ThreadSmem {
     // findAllSMEMS variables and the call in progress
     int32_t from, to;
     int32_t site;           // 0: first FB(from,to)  1: FB(from0,to)  2: BF(from,to0)
+    int32_t fb;             // the call in progress is findFwdBackSMEMS
     int32_t cf, ct;         // the called function's from/to
-    // walk state
-    SmemState32 m, m0;
+    // walk state: oriented interval (wp, wq, s), log-likelihood, read range
+    double lp;
+    uint32_t wp, wq, s;
+    int32_t mfrom, mto;
+    // the walk's previous state (same range end on the fixed side)
+    double lp0;
+    uint32_t wp0, wq0, s0w;
     int32_t n_prev;
     int32_t pv_base;        // the list is pv[pv_base .. pv_base + n_prev), longest first
     int32_t ovf;            // a push found the list full: this read is abandoned (the batch reruns)
@@ -86,11 +93,11 @@ struct ThreadSmem {
 };
 
 __device__ __forceinline__ void smem_emit(ThreadSmem& t, const SmemThreadArgs& a, int32_t from, int32_t to,
-                                          const PrevEntry& e) {
+                                          uint32_t p, uint32_t q, uint32_t s, double lp) {
     if (t.n_out < a.cap) {
         int64_t* o = t.out + 6 * (int64_t)t.n_out;
-        o[0] = from; o[1] = to; o[2] = e.p; o[3] = e.q; o[4] = e.s;
-        o[5] = __double_as_longlong(e.lp);
+        o[0] = from; o[1] = to; o[2] = p; o[3] = q; o[4] = s;
+        o[5] = __double_as_longlong(lp);
     }
     t.n_out++;
 }
@@ -102,107 +109,78 @@ __device__ __forceinline__ void smem_return(ThreadSmem& t) {
     else { t.from = t.cf; t.phase = PH_OUTER_LOOP; }
 }
 
-__device__ __forceinline__ SmemState32 smem_init_state(const ThreadSmem& t, const IndexDev& ix, int32_t from) {
-    const int b = t.base(from);
-    SmemState32 m;
-    m.from = from; m.to = from + 1;
-    m.p = (uint32_t)ix.C[b]; m.q = (uint32_t)ix.C[comp16(b)]; m.s = (uint32_t)(ix.C[b + 1] - ix.C[b]);
-    m.lp = __dadd_rn(0.0, c_llk[b]);
-    return m;
-}
-
-// Enter FB(cf, ct) (SMEM.cpp:64-77).
-__device__ __forceinline__ void smem_call_fb(ThreadSmem& t, const IndexDev& ix, int site, int32_t cf) {
+// Enter FB(cf, cf + 1) (SMEM.cpp:64-77) when fb, else BF(cf, cf + 1) (SMEM.cpp:119-132).
+__device__ __forceinline__ void smem_call(ThreadSmem& t, const IndexDev& ix, int site, int fb, int32_t cf) {
     t.site = site;
+    t.fb = fb;
     t.cf = cf;
-    const int b = t.base(cf);
     t.ct = cf + 1;
-    if (!is_basic(b)) { smem_return(t); return; }
-    t.m = smem_init_state(t, ix, cf);
-    t.m0 = t.m;
-    t.n_prev = 0;
-    t.phase = PH_FB_WALK;
-}
-
-// Enter BF(cf, ct) (SMEM.cpp:119-132).
-__device__ __forceinline__ void smem_call_bf(ThreadSmem& t, const IndexDev& ix, int32_t cf) {
-    t.site = 2;
-    t.cf = cf;
     const int b = t.base(cf);
-    t.ct = cf + 1;
     if (!is_basic(b)) { smem_return(t); return; }
-    t.m = smem_init_state(t, ix, cf);
-    t.m0 = t.m;
+    const uint32_t p = (uint32_t)ix.C[b], q = (uint32_t)ix.C[comp16(b)];
+    t.wp = fb ? q : p;
+    t.wq = fb ? p : q;
+    t.s = (uint32_t)(ix.C[b + 1] - ix.C[b]);
+    t.lp = __dadd_rn(0.0, c_llk[b]);
+    t.mfrom = cf;
+    t.mto = cf + 1;
+    t.wp0 = t.wp; t.wq0 = t.wq; t.s0w = t.s; t.lp0 = t.lp;
     t.n_prev = 0;
-    t.phase = PH_BF_WALK;
+    t.phase = PH_WALK;
 }
 
 // Advance the state machine until an extension is needed. On return with
-// true, (P,Q,S,B) is a backward extension to perform (forward extensions are
-// expressed as backward ones on the swapped interval).
+// true, (P,Q,S,B) is the backward extension to perform.
 __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const IndexDev& ix, PrevEntry* pv,
                              uint32_t& P, uint32_t& Q, uint32_t& S, int& B) {
     for (;;) {
         switch (t.phase) {
             case PH_OUTER_LOOP:
                 if (!(t.from > 0 || t.to < t.L)) { t.phase = PH_DONE; return false; }
-                if (t.to < t.L) { smem_call_fb(t, ix, 1, t.to); continue; }
+                if (t.to < t.L) { smem_call(t, ix, 1, 1, t.to); continue; }
                 t.phase = PH_OUTER_BACK;
                 continue;
             case PH_OUTER_BACK:
                 t.from -= 1;
-                if (t.from >= 0) { smem_call_bf(t, ix, t.from); continue; }
+                if (t.from >= 0) { smem_call(t, ix, 2, 0, t.from); continue; }
                 t.phase = PH_OUTER_LOOP;
                 continue;
-            case PH_FB_WALK:
-                if (t.m.s >= 1) {  // fwdExt with the base at `to` (0 past the read end)
-                    const int nb = t.base(t.m.to);
-                    P = t.m.q; Q = t.m.p; S = t.m.s; B = comp16(nb);
+            case PH_WALK:
+                if (t.s >= 1) {  // extend at `to` (fb, the base past the read is 0) or before `from`
+                    const int nb = t.fb ? t.base(t.mto) : t.base(t.mfrom - 1);
+                    P = t.wp; Q = t.wq; S = t.s; B = t.fb ? comp16(nb) : nb;
                     return true;
                 }
-                t.ct = t.m.to;
+                if (t.fb) t.ct = t.mto; else t.cf = t.mfrom;
                 if (t.ovf) { t.phase = PH_DONE; return false; }
-                if (t.n_prev == 0) { t.cf--; smem_return(t); continue; }
-                t.pv_base = (int32_t)a.pv_cap - t.n_prev;
-                t.phase = PH_FB_ITER;
-                continue;
-            case PH_FB_ITER:
-                if (!(t.cf >= 0 && t.n_prev > 0)) { smem_return(t); continue; }
-                t.k = 0; t.n_keep = 0; t.s0 = 0; t.n_valid = 0;
-                t.b2 = t.cf > 0 ? t.base(t.cf - 1) : 0;
-                t.e_next = pv[t.pv_base];
-                t.phase = PH_FB_ENTRY;
-                continue;
-            case PH_FB_ENTRY:
-                if (t.k == t.n_prev) { t.n_prev = t.n_keep; t.cf--; t.phase = PH_FB_ITER; continue; }
-                t.e0 = t.e_next;
-                if (t.k + 1 < t.n_prev) t.e_next = pv[t.pv_base + t.k + 1];
-                P = t.e0.p; Q = t.e0.q; S = t.e0.s; B = t.b2;
-                return true;
-            case PH_BF_WALK:
-                if (t.m.s >= 1) {
-                    const int nb = t.m.from > 0 ? t.base(t.m.from - 1) : 0;
-                    P = t.m.p; Q = t.m.q; S = t.m.s; B = nb;
-                    return true;
+                if (t.n_prev == 0) {
+                    if (t.fb) t.cf--; else t.ct++;
+                    smem_return(t);
+                    continue;
                 }
-                t.cf = t.m.from;
-                if (t.ovf) { t.phase = PH_DONE; return false; }
-                if (t.n_prev == 0) { t.ct++; smem_return(t); continue; }
                 t.pv_base = (int32_t)a.pv_cap - t.n_prev;
-                t.phase = PH_BF_ITER;
+                t.phase = PH_ITER;
                 continue;
-            case PH_BF_ITER:
-                if (!(t.ct <= t.L && t.n_prev > 0)) { smem_return(t); continue; }
+            case PH_ITER: {
+                // passes extend the other end: before cf (fb) or at ct (bf)
+                const bool more = t.fb ? t.cf >= 0 : t.ct <= t.L;
+                if (!(more && t.n_prev > 0)) { smem_return(t); continue; }
                 t.k = 0; t.n_keep = 0; t.s0 = 0; t.n_valid = 0;
-                t.b2 = t.base(t.ct);
+                t.b2 = t.fb ? (t.cf > 0 ? t.base(t.cf - 1) : 0) : t.base(t.ct);
                 t.e_next = pv[t.pv_base];
-                t.phase = PH_BF_ENTRY;
+                t.phase = PH_ENTRY;
                 continue;
-            case PH_BF_ENTRY:
-                if (t.k == t.n_prev) { t.n_prev = t.n_keep; t.ct++; t.phase = PH_BF_ITER; continue; }
+            }
+            case PH_ENTRY:
+                if (t.k == t.n_prev) {
+                    t.n_prev = t.n_keep;
+                    if (t.fb) t.cf--; else t.ct++;
+                    t.phase = PH_ITER;
+                    continue;
+                }
                 t.e0 = t.e_next;
                 if (t.k + 1 < t.n_prev) t.e_next = pv[t.pv_base + t.k + 1];
-                P = t.e0.q; Q = t.e0.p; S = t.e0.s; B = comp16(t.b2);
+                P = t.e0.p; Q = t.e0.q; S = t.e0.s; B = t.fb ? t.b2 : comp16(t.b2);
                 return true;
             default:
                 return false;
@@ -215,21 +193,14 @@ __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const Index
 // read order. Every term is <= 0 and round-to-nearest of a + b with b <= 0
 // never exceeds a, so the running sum never increases: the exact sequential
 // sum is <= thr as soon as a partial sum is.
-__device__ __forceinline__ bool smem_sig(const ThreadSmem& t, const SmemThreadArgs& a, double lp, bool left,
-                                         int32_t lim) {
+__device__ __forceinline__ bool smem_sig(const ThreadSmem& t, const SmemThreadArgs& a, double lp, int32_t i0,
+                                         int32_t i1) {
     if (a.thr_all) return true;
     double ll = __dadd_rn(0.0, lp);
     if (ll <= a.thr) return true;
-    if (left) {
-        for (int32_t i = 0; i < lim; ++i) {
-            ll = __dadd_rn(ll, c_llk[t.base(i)]);
-            if (ll <= a.thr) return true;
-        }
-    } else {
-        for (int32_t i = lim; i < t.L; ++i) {
-            ll = __dadd_rn(ll, c_llk[t.base(i)]);
-            if (ll <= a.thr) return true;
-        }
+    for (int32_t i = i0; i < i1; ++i) {
+        ll = __dadd_rn(ll, c_llk[t.base(i)]);
+        if (ll <= a.thr) return true;
     }
     return false;
 }
@@ -237,11 +208,11 @@ __device__ __forceinline__ bool smem_sig(const ThreadSmem& t, const SmemThreadAr
 // The walks push candidates shortest first; storing them downward from the
 // top of the thread's list leaves pv[pv_base ..] longest first, which is the
 // order the reference gets from std::reverse (SMEM.cpp:90, 145).
-__device__ __forceinline__ void smem_push(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, const SmemState32& m,
-                                          int32_t pos) {
+__device__ __forceinline__ void smem_push(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, int32_t pos) {
     if (t.n_prev < a.pv_cap) {
         PrevEntry e;
-        e.p = m.p; e.q = m.q; e.s = m.s; e.lp = m.lp; e.pos = pos;
+        e.p = t.wq0; e.q = t.wp0;  // candidate orientation is the walk's, swapped
+        e.s = t.s0w; e.lp = t.lp0; e.pos = pos;
         pv[a.pv_cap - 1 - t.n_prev] = e;
         t.n_prev++;
     } else {
@@ -253,49 +224,38 @@ __device__ __forceinline__ void smem_push(ThreadSmem& t, const SmemThreadArgs& a
 // Apply the result of the extension requested by smem_advance.
 __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, uint32_t P, uint32_t Q,
                                            uint32_t S) {
-    switch (t.phase) {
-        case PH_FB_WALK: {  // SMEM.cpp:79-86
-            t.m.q = (uint32_t)P; t.m.p = (uint32_t)Q; t.m.s = (uint32_t)S;
-            const int nb = t.base(t.m.to);
-            if (t.m.to < t.L) t.m.lp = __dadd_rn(t.m.lp, c_llk[nb]);
-            t.m.to++;
-            if (t.m.s != t.m0.s && t.m0.to >= a.min_len && smem_sig(t, a, t.m0.lp, true, t.m0.from))
-                smem_push(t, a, pv, t.m0, t.m0.to);
-            t.m0 = t.m;
-            break;
+    if (t.phase == PH_WALK) {  // SMEM.cpp:79-86 (fb) / 134-141 (bf)
+        const bool fb = t.fb;
+        t.wp = P; t.wq = Q; t.s = S;
+        const int32_t np = fb ? t.mto : t.mfrom - 1;  // the base just added
+        if (np >= 0 && np < t.L) t.lp = __dadd_rn(t.lp, c_llk[t.base(np)]);
+        if (fb) t.mto++; else t.mfrom--;
+        if (t.s != t.s0w) {
+            // the previous state: its moving end is one step back
+            const int32_t f0 = fb ? t.mfrom : t.mfrom + 1;
+            const int32_t t0 = fb ? t.mto - 1 : t.mto;
+            const bool long_enough = fb ? t0 >= a.min_len : t.L - f0 >= a.min_len;
+            if (long_enough && (fb ? smem_sig(t, a, t.lp0, 0, f0) : smem_sig(t, a, t.lp0, t0, t.L)))
+                smem_push(t, a, pv, fb ? t0 : f0);
         }
-        case PH_BF_WALK: {  // SMEM.cpp:134-141
-            t.m.p = (uint32_t)P; t.m.q = (uint32_t)Q; t.m.s = (uint32_t)S;
-            if (t.m.from > 0) t.m.lp = __dadd_rn(t.m.lp, c_llk[t.base(t.m.from - 1)]);
-            t.m.from--;
-            if (t.m.s != t.m0.s && t.L - t.m0.from >= a.min_len && smem_sig(t, a, t.m0.lp, false, t.m0.to))
-                smem_push(t, a, pv, t.m0, t.m0.from);
-            t.m0 = t.m;
-            break;
+        t.wp0 = t.wp; t.wq0 = t.wq; t.s0w = t.s; t.lp0 = t.lp;
+    } else if (t.phase == PH_ENTRY) {  // SMEM.cpp:97-112 (fb) / 152-167 (bf)
+        const bool fb = t.fb;
+        PrevEntry e = t.e0;
+        e.p = P; e.q = Q; e.s = S;
+        const bool add = fb ? (t.cf > 0) : (t.ct < t.L);
+        if (add) e.lp = __dadd_rn(e.lp, c_llk[t.b2]);
+        const int32_t e_from = fb ? t.cf : t.e0.pos;
+        const int32_t e_to = fb ? t.e0.pos : t.ct;
+        if (e.s != t.e0.s && t.e0.s >= 1 && t.n_valid == 0 && e_to - e_from >= a.min_len &&
+            (a.thr_all || t.e0.lp <= a.thr))
+            smem_emit(t, a, e_from, e_to, fb ? t.e0.p : t.e0.q, fb ? t.e0.q : t.e0.p, t.e0.s, t.e0.lp);
+        if (e.s >= 1 && e.s != t.s0) {
+            t.s0 = e.s;
+            t.n_valid++;
+            pv[t.pv_base + t.n_keep++] = e;
         }
-        case PH_FB_ENTRY:
-        case PH_BF_ENTRY: {  // SMEM.cpp:97-112 / 152-167
-            const bool fb = t.phase == PH_FB_ENTRY;
-            PrevEntry e = t.e0;
-            if (fb) { e.p = (uint32_t)P; e.q = (uint32_t)Q; } else { e.q = (uint32_t)P; e.p = (uint32_t)Q; }
-            e.s = (uint32_t)S;
-            const bool add = fb ? (t.cf > 0) : (t.ct < t.L);
-            if (add) e.lp = __dadd_rn(e.lp, c_llk[t.b2]);
-            const int32_t e_from = fb ? t.cf : t.e0.pos;
-            const int32_t e_to = fb ? t.e0.pos : t.ct;
-            if (e.s != t.e0.s && t.e0.s >= 1 && t.n_valid == 0 && e_to - e_from >= a.min_len &&
-                (a.thr_all || t.e0.lp <= a.thr))
-                smem_emit(t, a, e_from, e_to, t.e0);
-            if (e.s >= 1 && e.s != t.s0) {
-                t.s0 = e.s;
-                t.n_valid++;
-                pv[t.pv_base + t.n_keep++] = e;
-            }
-            t.k++;
-            break;
-        }
-        default:
-            break;
+        t.k++;
     }
 }
 
@@ -330,7 +290,7 @@ __global__ void __launch_bounds__(128) k_smem_thread(SmemThreadArgs a, IndexDev 
                 if (t.L <= 0) { t.phase = PH_DONE; continue; }
                 t.from = t.L / 2;  // SMEM.cpp:189-191
                 t.to = t.from + 1;
-                smem_call_fb(t, ix, 0, t.from);
+                smem_call(t, ix, 0, 1, t.from);
                 continue;
             }
             have = smem_advance(t, a, ix, pv, P, Q, S, B);
