@@ -259,7 +259,7 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
     }
 }
 
-__global__ void __launch_bounds__(128) k_smem_thread(SmemThreadArgs a, IndexDev ix) {
+__global__ void __launch_bounds__(128, 5) k_smem_thread(SmemThreadArgs a, IndexDev ix) {
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     PrevEntry* pv = a.prev + tid * a.pv_cap;
     ThreadSmem t;
