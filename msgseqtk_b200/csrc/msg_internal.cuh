@@ -155,36 +155,46 @@ __device__ inline int64_t fwd_ext(const IndexDev& ix, int64_t& p, int64_t& q, in
     return back_ext(ix, q, p, s, comp16(b));
 }
 
-// Occurrences of one base (A,C,G,T: code 0..3) among the first r symbols of a
-// loaded bucket k, 32-bit (rows < 2^32). Stored counts give A, C, G before
-// the bucket; T before it is the rest. '$' is stored as code 0 and removed
-// from A's count.
-__device__ __forceinline__ uint32_t occ1_in(const IndexDev& ix, uint32_t k, uint32_t r, uint32_t code,
-                                            const uint4& w0, const uint4& w1) {
+// Counts at row k*64 + r of a loaded bucket k, for one base (A,C,G,T: code
+// 0..3), 32-bit (rows < 2^32): eq = occurrences of the base, gt = occurrences
+// of the bases after it (C,G,T after A; G,T after C; T after G), dl =
+// occurrences of '$', all among the rows before k*64 + r. Stored counts give
+// '$', A, C, G before the bucket (T is the rest); within the bucket one masked
+// popcount per word and count: with lo/hi the low/high code bits, the bases
+// after A are lo|hi, after C hi, after G lo&hi. '$' is stored as A and
+// removed from A's count.
+__device__ __forceinline__ void occ_counts(const IndexDev& ix, uint32_t k, uint32_t r, uint32_t code, const uint4& w0,
+                                           const uint4& w1, uint32_t& eq, uint32_t& gt, uint32_t& dl) {
     const uint32_t words[kBucketWords] = {w1.x, w1.y, w1.z, w1.w};
     const uint32_t pat = code * 0x55555555u;  // the code in every 2-bit field
-    uint32_t n = 0;
+    uint32_t n_eq = 0, n_gt = 0;
 #pragma unroll
     for (int w = 0; w < kBucketWords; ++w) {
         const int nv = min(max((int)r - 16 * w, 0), 16);
         const uint32_t m = nv >= 16 ? 0x55555555u : (0x55555555u & ((1u << (2 * nv)) - 1u));
-        const uint32_t e = ~(words[w] ^ pat);  // both bits set where the symbol equals the code
-        n += __popc(e & (e >> 1) & m);
+        const uint32_t x = words[w];
+        const uint32_t e = ~(x ^ pat);  // both bits set where the symbol equals the code
+        n_eq += __popc(e & (e >> 1) & m);
+        const uint32_t lo = x & 0x55555555u, hi = (x >> 1) & 0x55555555u;
+        const uint32_t g = code == 0 ? (lo | hi) : code == 1 ? hi : code == 2 ? (lo & hi) : 0u;
+        n_gt += __popc(g & m);
     }
     const uint32_t dollar = w0.x & 0x7fffffffu;
-    uint32_t before;
-    if (code == 0) before = w0.y;
-    else if (code == 1) before = w0.z;
-    else if (code == 2) before = w0.w;
-    else before = k * (uint32_t)kBucketSyms - dollar - w0.y - w0.z - w0.w;
-    if (code == 0 && (w0.x >> 31) && r > 0)
-        n -= (uint32_t)dollar_between(ix, (int64_t)k * kBucketSyms, (int64_t)k * kBucketSyms + r);
-    return before + n;
+    uint32_t din = 0;
+    if ((w0.x >> 31) && r > 0)
+        din = (uint32_t)dollar_between(ix, (int64_t)k * kBucketSyms, (int64_t)k * kBucketSyms + r);
+    const uint32_t all = k * (uint32_t)kBucketSyms - dollar;  // bases before the bucket
+    const uint32_t a = w0.y, c = w0.z, g = w0.w;
+    const uint32_t before_eq = code == 0 ? a : code == 1 ? c : code == 2 ? g : all - a - c - g;
+    const uint32_t before_gt = code == 0 ? all - a : code == 1 ? all - a - c : code == 2 ? all - a - c - g : 0u;
+    eq = before_eq + n_eq - (code == 0 ? din : 0u);
+    gt = before_gt + n_gt;
+    dl = dollar + din;
 }
 
-// FMDIndex::backExt (FMDIndex.cpp:577-610) on 32-bit bi-intervals. While the
-// size does not change only the extended base is counted at the two rows;
-// the other counts (needed for q) are taken only when it does.
+// FMDIndex::backExt (FMDIndex.cpp:577-610) on 32-bit bi-intervals: the size
+// from the base's counts at the two rows, and q, when the size changes, from
+// the counts of '$' and of the bases after it (FMDIndex.cpp:592-604).
 __device__ inline int64_t back_ext32(const IndexDev& ix, uint32_t& p, uint32_t& q, uint32_t& s, int b) {
     if (!is_basic(b)) { s = 0; return 0; }
     const int c = to_int(b);
@@ -198,18 +208,13 @@ __device__ inline int64_t back_ext32(const IndexDev& ix, uint32_t& p, uint32_t& 
         const uint4* pb = reinterpret_cast<const uint4*>(ix.bkt + kb);
         b0 = __ldg(pb); b1 = __ldg(pb + 1);
     }
-    const uint32_t O = occ1_in(ix, ka, ja & 63u, code, a0, a1);
-    const uint32_t hiO = occ1_in(ix, kb, jb & 63u, code, b0, b1);
-    const uint32_t ns = hiO - O;
+    uint32_t oa, ga, da, ob, gb, db;
+    occ_counts(ix, ka, ja & 63u, code, a0, a1, oa, ga, da);
+    occ_counts(ix, kb, jb & 63u, code, b0, b1, ob, gb, db);
+    const uint32_t ns = ob - oa;
     if (ns == 0) { s = 0; return 0; }
-    if (ns != s) {
-        const Occ5 lo = occ5_in(ix, ka, (int)(ja & 63u), a0, a1);
-        const Occ5 hi = occ5_in(ix, kb, (int)(jb & 63u), b0, b1);
-        uint32_t qq = q + (uint32_t)(hi.c[0] - lo.c[0]);
-        for (int j = 4; j > c; --j) qq += (uint32_t)(hi.c[j] - lo.c[j]);
-        q = qq;
-    }
-    p = (uint32_t)ix.C[b] + O;
+    if (ns != s) q = q + (db - da) + (gb - ga);
+    p = (uint32_t)ix.C[b] + oa;
     s = ns;
     return ns;
 }
