@@ -278,6 +278,8 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             SmemThreadArgs ta{};
             ta.seq = d_seq; ta.off = d_off; ta.n_reads = n_reads; ta.min_len = params->min_len;
             ta.thr = thr; ta.thr_all = thr_all;
+            ta.llk_min = *std::min_element(im.llk, im.llk + 16);
+            ta.llk_max = *std::max_element(im.llk, im.llk + 16);
             ta.out = ctx->smem.as<int64_t>(); ta.cap = cap; ta.count = ctx->smem_cnt.as<int32_t>();
             ta.prev = ctx->prev.as<PrevEntry>(); ta.pv_cap = pv_cap;
             ta.work = d_ctr; ta.n_ext = d_ctr + 1; ta.status = d_status;

@@ -38,6 +38,7 @@ struct SmemThreadArgs {
     int64_t min_len;
     double thr;
     int thr_all;
+    double llk_min, llk_max;  // extremes of the per-base log-likelihoods
     int64_t* out;
     int64_t cap;
     int32_t* count;
@@ -49,6 +50,9 @@ struct SmemThreadArgs {
 };
 
 __constant__ double c_llk[16];
+// per-block copy of c_llk: lanes index it by their own bases, which shared
+// memory serves in one pass where the constant cache would serialise
+__shared__ double s_llk[16];
 
 enum SmemPhase : int {
     PH_NEXT_READ = 0,
@@ -121,7 +125,7 @@ __device__ __forceinline__ void smem_call(ThreadSmem& t, const IndexDev& ix, int
     t.wp = fb ? q : p;
     t.wq = fb ? p : q;
     t.s = (uint32_t)(ix.C[b + 1] - ix.C[b]);
-    t.lp = __dadd_rn(0.0, c_llk[b]);
+    t.lp = __dadd_rn(0.0, s_llk[b]);
     t.mfrom = cf;
     t.mto = cf + 1;
     t.wp0 = t.wp; t.wq0 = t.wq; t.s0w = t.s; t.lp0 = t.lp;
@@ -192,14 +196,21 @@ __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const Index
 // (SMEM.cpp:79-81, 134-136): lp plus the bases outside [m.from, m.to) added in
 // read order. Every term is <= 0 and round-to-nearest of a + b with b <= 0
 // never exceeds a, so the running sum never increases: the exact sequential
-// sum is <= thr as soon as a partial sum is.
+// sum is <= thr as soon as a partial sum is. Each of the n terms lies in
+// [llk_min, llk_max], so the sum lies within n of them of the start, up to a
+// rounding error of about n * 2^-53 times the magnitudes (below 1e-10 for
+// reads of a few hundred bases): bounds clear of thr by 1e-6 decide at once,
+// and only the rest is summed term by term.
 __device__ __forceinline__ bool smem_sig(const ThreadSmem& t, const SmemThreadArgs& a, double lp, int32_t i0,
                                          int32_t i1) {
     if (a.thr_all) return true;
     double ll = __dadd_rn(0.0, lp);
     if (ll <= a.thr) return true;
+    const double n = (double)max(i1 - i0, 0);
+    if (ll + n * a.llk_max <= a.thr - 1e-6) return true;
+    if (ll + n * a.llk_min > a.thr + 1e-6) return false;
     for (int32_t i = i0; i < i1; ++i) {
-        ll = __dadd_rn(ll, c_llk[t.base(i)]);
+        ll = __dadd_rn(ll, s_llk[t.base(i)]);
         if (ll <= a.thr) return true;
     }
     return false;
@@ -228,7 +239,7 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
         const bool fb = t.fb;
         t.wp = P; t.wq = Q; t.s = S;
         const int32_t np = fb ? t.mto : t.mfrom - 1;  // the base just added
-        if (np >= 0 && np < t.L) t.lp = __dadd_rn(t.lp, c_llk[t.base(np)]);
+        if (np >= 0 && np < t.L) t.lp = __dadd_rn(t.lp, s_llk[t.base(np)]);
         if (fb) t.mto++; else t.mfrom--;
         if (t.s != t.s0w) {
             // the previous state: its moving end is one step back
@@ -244,7 +255,7 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
         PrevEntry e = t.e0;
         e.p = P; e.q = Q; e.s = S;
         const bool add = fb ? (t.cf > 0) : (t.ct < t.L);
-        if (add) e.lp = __dadd_rn(e.lp, c_llk[t.b2]);
+        if (add) e.lp = __dadd_rn(e.lp, s_llk[t.b2]);
         const int32_t e_from = fb ? t.cf : t.e0.pos;
         const int32_t e_to = fb ? t.e0.pos : t.ct;
         if (e.s != t.e0.s && t.e0.s >= 1 && t.n_valid == 0 && e_to - e_from >= a.min_len &&
@@ -260,6 +271,8 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
 }
 
 __global__ void __launch_bounds__(128, 5) k_smem_thread(SmemThreadArgs a, IndexDev ix) {
+    if (threadIdx.x < 16) s_llk[threadIdx.x] = c_llk[threadIdx.x];
+    __syncthreads();
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     PrevEntry* pv = a.prev + tid * a.pv_cap;
     ThreadSmem t;
