@@ -5,8 +5,8 @@ lengths (median 3 Mbp, sigma 0.5, ~600 Mbp, per-genome GC uniform 30-70%),
 indexed as MSGseqTK's bidirectional FMD-index (~1.2 G BWT symbols), and 2 M
 read pairs (2 x 150 bp, fragment ~ Normal(400, 50), 1% substitutions, 0.1%
 indels of 1-3 bp, 5% random pairs). Mates are mapped as single reads, as the
-reference's findSeedsPE does. A step maps one batch of reads (default 250 k
-pairs = 500 k reads) end to end: SMEMs -> seed selection -> locate ->
+reference's findSeedsPE does. A step maps one batch of reads (default 500 k
+pairs = 1 M reads) end to end: SMEMs -> seed selection -> locate ->
 redundant-seed removal -> chains -> DP + traceback -> CIGAR. Default parameters
 (min seed 17, e-value 0.01, maxNSeed 500, GLOBAL NW, scores 1/3/5/2).
 
@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--pairs", type=int, default=2_000_000, help="read pairs per GPU")
-    ap.add_argument("--batch-pairs", type=int, default=250_000)
+    ap.add_argument("--batch-pairs", type=int, default=500_000)
     ap.add_argument("--genomes", type=int, default=200)
     ap.add_argument("--median", type=float, default=3e6)
     ap.add_argument("--seed", type=int, default=2)
