@@ -155,6 +155,16 @@ __host__ __device__ inline bool bandable(int R, int C, int w) {
 // List counters: counts[0] thread path, counts[1] warp path (whole cell
 // set), counts[kBandedCount] warp path with a band.
 constexpr int kBandedCount = 8;
+// With small_key, the thread-path list is built by sorting every chain on
+// this key (small chains: their cell count; others last), so that the
+// threads of a warp get chains of similar size and diverge less.
+constexpr int32_t kNotSmallKey = 1023;
+constexpr int kSmallKeyBits = 10;
+
+__global__ void k_iota(int64_t n, int64_t* __restrict__ v) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) v[i] = i;
+}
 
 // Band half-widths per chain and the split into the thread path (chains of
 // at most kSmallArea cells, never banded), the warp path and the banded warp
@@ -168,7 +178,8 @@ __global__ void __launch_bounds__(128) k_band_assign(int64_t n_chain, const int4
                                                      const float* __restrict__ nrm, int8_t* __restrict__ band,
                                                      int64_t* __restrict__ small, int64_t* __restrict__ big,
                                                      int64_t* __restrict__ banded,
-                                                     unsigned long long* __restrict__ counts) {
+                                                     unsigned long long* __restrict__ counts,
+                                                     int32_t* __restrict__ small_key) {
     __shared__ float sW[kNTrain];
     __shared__ float sN[2 * kFeat];
     if (mode == 2) {
@@ -189,9 +200,13 @@ __global__ void __launch_bounds__(128) k_band_assign(int64_t n_chain, const int4
     const int w3 = (w >= 0 && bandable(g.z, g.w, w)) ? w : -1;
     band[2 * c] = (int8_t)w5;
     band[2 * c + 1] = (int8_t)w3;
+    const bool is_small = w5 < 0 && w3 < 0 && area[c] <= kSmallArea;
+    if (small_key) small_key[c] = is_small ? (int32_t)area[c] : kNotSmallKey;
     if (w5 >= 0 || w3 >= 0) banded[atomicAdd(&counts[kBandedCount], 1ull)] = c;
-    else if (area[c] <= kSmallArea) small[atomicAdd(&counts[0], 1ull)] = c;
-    else big[atomicAdd(&counts[1], 1ull)] = c;
+    else if (is_small) {
+        const unsigned long long k = atomicAdd(&counts[0], 1ull);
+        if (!small_key) small[k] = c;
+    } else big[atomicAdd(&counts[1], 1ull)] = c;
 }
 
 // ---------------------------------------------------------------------------

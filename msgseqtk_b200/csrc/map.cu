@@ -453,6 +453,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     tm.mark();  // 3
 
     // ---------------- DP ----------------
+    if (h_nchain >= INT32_MAX) return ctx->fail(MSG_EINVAL, "too many chains in one batch");
     const int64_t NC = h_nchain + 1;
     CK(ctx->dpinfo.ensure(NC * 8 * 16 + 256));  // 16 arrays of NC int64 + counters
     int64_t* d_ts = ctx->dpinfo.as<int64_t>();
@@ -547,7 +548,8 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             CK(cudaMemsetAsync(d_probe, 3, h_nchain, st));  // 3: not banded at this class
             CK(cudaMemcpyAsync(d_pcells, d_area, h_nchain * 8, cudaMemcpyDeviceToDevice, st));
             S.n_launch++, k_band_assign<<<nblk(h_nchain, 128), 128, 0, st>>>(h_nchain, d_geo, d_area, d_feat, 1, band_width(cls),
-                                                                nullptr, nullptr, d_band, d_small, d_big, d_bandl, d_ctr2);
+                                                                nullptr, nullptr, d_band, d_small, d_big, d_bandl, d_ctr2,
+                                                                nullptr);
             da.list = d_bandl; da.n_list = d_ctr2 + kBandedCount;
             S.n_launch++, k_dp<true><<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
             CK(cudaGetLastError());
@@ -574,8 +576,22 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     if (h_nchain > 0) {
         CK(cudaMemsetAsync(d_ctr2, 0, 128, st));
         const int bmode = dpp.mode != 0 ? 0 : params->band_mode;
+        // thread-path list sorted by cell count (keys and values staged in the
+        // fallback and kept-index arrays, which are not in use yet)
+        int32_t* d_key = reinterpret_cast<int32_t*>(d_fb);
+        int32_t* d_key2 = d_key + NC;
         S.n_launch++, k_band_assign<<<nblk(h_nchain, 128), 128, 0, st>>>(h_nchain, d_geo, d_area, d_feat, bmode, params->band_w,
-                                                            d_wts, d_nrm, d_band, d_small, d_big, d_bandl, d_ctr2);
+                                                            d_wts, d_nrm, d_band, d_small, d_big, d_bandl, d_ctr2,
+                                                            d_key);
+        S.n_launch++, k_iota<<<nblk(h_nchain, 256), 256, 0, st>>>(h_nchain, d_kidx);
+        {
+            size_t tb = 0;
+            CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, d_key, d_key2, d_kidx, d_small, (int)h_nchain, 0,
+                                               kSmallKeyBits, st));
+            CK(misc.ensure(tb));
+            CK(cub::DeviceRadixSort::SortPairs(misc.p, tb, d_key, d_key2, d_kidx, d_small, (int)h_nchain, 0,
+                                               kSmallKeyBits, st));
+        }
         // Every launch is sized for every chain; each reads its list length on
         // the device, so no host round trip is needed for the split.
         da.list = d_small; da.n_list = d_ctr2;
