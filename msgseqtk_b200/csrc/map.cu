@@ -507,20 +507,19 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     const int64_t aux_bytes = ((2 * (h_nidx + 1) + h_nchain + 1) * sizeof(int32_t) + 15) / 16 * 16;
     CK(ctx->scratch.ensure(h_cells + 64 + aux_bytes + (2 * h_nidx + h_nchain + 1) * sizeof(int4)));
     const int64_t P16 = ((h_pathtot + 1 + 15) / 16) * 16;
-    CK(ctx->path.ensure(2 * P16 + (h_nchain + 1) * 4 + 64));
+    CK(ctx->path.ensure(P16 + (h_nchain + 1) * 4 + 64));
     CK(ctx->alnbuf.ensure((h_nchain + 1) * sizeof(msg_aln)));
     uint8_t* d_scr = ctx->scratch.as<uint8_t>();
     int32_t* d_aux = reinterpret_cast<int32_t*>(d_scr + (h_cells + 64) / 16 * 16);
     int4* d_sdbuf = reinterpret_cast<int4*>(reinterpret_cast<uint8_t*>(d_aux) + aux_bytes);
     uint8_t* d_path = ctx->path.as<uint8_t>();
-    uint8_t* d_qbuf = d_path + P16;
-    int32_t* d_plen = reinterpret_cast<int32_t*>(d_path + 2 * P16);
+    int32_t* d_plen = reinterpret_cast<int32_t*>(d_path + P16);
     msg_aln* d_aln = ctx->alnbuf.as<msg_aln>();
     DpArgs da{};
     da.ix = ix; da.seeds = d_seeds; da.chain_idx_off = d_cidx_off; da.chain_len = d_clen; da.chain_read = d_cread;
     da.chain_idx = d_cidx; da.n_chain = h_nchain; da.rseq = d_seq; da.roff = d_off; da.t_start = d_ts;
     da.t_end = d_te; da.scr_off = d_rect_off; da.scr = d_scr; da.aux = d_aux; da.sdbuf = d_sdbuf;
-    da.qbuf = d_qbuf; da.path_off = d_path_off; da.path = d_path; da.path_len = d_plen; da.aln = d_aln;
+    da.path_off = d_path_off; da.path = d_path; da.path_len = d_plen; da.aln = d_aln;
     da.pp = dpp; da.status = d_status;
     da.band = d_band; da.min_rate = params->min_score_rate; da.keep = d_keep; da.fb_list = d_fb;
     da.fb_n = d_ctr2 + 2; da.bstat = d_bstat;

@@ -580,7 +580,8 @@ struct ChainCtx {
     const int32_t* cbnd;        // column boundaries: 0, ts_0, te_0, ..., T
     int32_t n;                  // seeds in the chain
     int64_t L, T;               // query length, window length
-    const uint8_t* query;       // read (FWD) or reverse complement in scratch (REV)
+    const uint8_t* rd;          // the read
+    int rev;                    // the query is the read's reverse complement (PrimarySeq::revcom)
     const uint8_t* target;      // chromosome + t_start
     int64_t target_avail;       // chromosome bases available from t_start (beyond: terminator 0)
     uint8_t* scratch;           // rectangle storage of this chain
@@ -594,6 +595,8 @@ struct ChainCtx {
     __device__ int64_t ts(int k) const { return sd[k].z; }
     __device__ int64_t te(int k) const { return sd[k].w; }
     __device__ int tb(int64_t t) const { return t < target_avail ? (int)__ldg(target + t) : 0; }
+    // query base i (0-based): the read, or its reverse complement read backwards
+    __device__ __forceinline__ int qbase(int64_t i) const { return rev ? comp16(rd[L - 1 - i]) : (int)rd[i]; }
     // ScoreScheme::getScore (ScoreScheme.cpp:20-24)
     __device__ int32_t score(int qb, int tbb) const {
         return ((qb & tbb) && qb != 15 && tbb != 15) ? pp.match : -pp.mismatch;
@@ -723,6 +726,8 @@ struct ChainCtx {
             g.rowbuf[c * 3 + 2] = D(g.r0, j, m);
         }
         int64_t cells = 0;
+        int64_t lrow = -1;         // matrix row whose left boundary cell (lrow, c0) is cached
+        int32_t lm = NEG, li = NEG, ld = NEG;
         for (int64_t rr = 0; rr < g.R; ++rr) {
             const int64_t lo = banded ? max((int64_t)0, rr + dg - w) : 0;
             const int64_t hi = banded ? min(g.C - 1, rr + dg + w) : g.C - 1;
@@ -730,12 +735,15 @@ struct ChainCtx {
             const int64_t i = g.r0 + 1 + rr;
             int32_t ml = NEG, dl = NEG, dm = NEG, di = NEG, dd = NEG;
             if (lo == 0) {
-                ml = M(i, g.c0, m); dl = D(i, g.c0, m);
-                dm = M(i - 1, g.c0, m); di = I(i - 1, g.c0, m); dd = D(i - 1, g.c0, m);
+                if (lrow == i - 1) { dm = lm; di = li; dd = ld; }
+                else { dm = M(i - 1, g.c0, m); di = I(i - 1, g.c0, m); dd = D(i - 1, g.c0, m); }
+                lm = M(i, g.c0, m); li = I(i, g.c0, m); ld = D(i, g.c0, m);
+                lrow = i;
+                ml = lm; dl = ld;
             } else if (lo - 1 >= plo && lo - 1 <= phi) {
                 dm = g.rowbuf[(lo - 1) * 3]; di = g.rowbuf[(lo - 1) * 3 + 1]; dd = g.rowbuf[(lo - 1) * 3 + 2];
             }
-            const int qb = query[i - 1];
+            const int qb = qbase(i - 1);
             const int64_t lane = rr & 31;
             uint8_t* code_base = g.code + (rr >> 5) * (g.C + 31) * 32;
             for (int64_t c = lo; c <= hi; ++c) {
@@ -806,7 +814,7 @@ struct ChainCtx {
         int64_t cells = 0;
         for (int64_t rr = 0; rr < g.R; ++rr) {
             const int64_t i = g.r0 + 1 + rr;
-            const int qb = query[i - 1];
+            const int qb = qbase(i - 1);
             const int64_t lr = rr & 31;
             uint8_t* code_base = g.code + (rr >> 5) * (g.C + 31) * 32;
             int32_t um[NP], ui[NP], mv[NP], iv[NP], U[NP], b1s[NP], b2s[NP];
@@ -942,7 +950,7 @@ struct ChainCtx {
                 ml = M(i, g.c0, m); dl = D(i, g.c0, m);
                 md0 = M(i - 1, g.c0, m); id0 = I(i - 1, g.c0, m); dd0 = D(i - 1, g.c0, m);
             }
-            const int qb = row_ok ? (int)query[i - 1] : 0;
+            const int qb = row_ok ? qbase(i - 1) : 0;
             int32_t pm = NEG, pi = NEG, pd = NEG;       // this lane's output of the previous step
             int32_t um = NEG, ui = NEG, ud = NEG;       // up neighbour (i-1, j) of the current step
             int32_t dm = md0, di = id0, dd = dd0;       // diagonal neighbour (i-1, j-1)
@@ -1007,7 +1015,6 @@ struct DpArgs {
     uint8_t* scr;
     int32_t* aux;               // per chain at 2 * chain_idx_off + chain index: diag (n) and rect offsets (n + 1)
     int4* sdbuf;                // per chain seed geometry when n > kSmemSeeds (at chain_idx_off)
-    uint8_t* qbuf;              // reverse-complement query per chain at path_off
     const int64_t* path_off;    // per chain, capacity L + tLen + 1
     uint8_t* path;
     int32_t* path_len;
@@ -1221,14 +1228,8 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
     x.sd = sd;
     x.rbnd = rbnd;
     x.cbnd = cbnd;
-    const uint8_t* rd = a.rseq + a.roff[r];
-    if (f.strand == FWD) {
-        x.query = rd;
-    } else {  // PrimarySeq::revcom
-        uint8_t* qb = a.qbuf + a.path_off[c];
-        for (int64_t i = lane; i < x.L; i += stride) qb[i] = (uint8_t)comp16(rd[x.L - 1 - i]);
-        x.query = qb;
-    }
+    x.rd = a.rseq + a.roff[r];
+    x.rev = f.strand != FWD;
     if (WARP) __syncwarp();
     if (lane == 0) {  // byte offsets of rectangles 0..n in this chain's storage
         int64_t off = 0;
@@ -1479,7 +1480,8 @@ __global__ void __launch_bounds__(128, 6) k_traceback(DpArgs a) {
     x.sd = gbase;
     x.rbnd = reinterpret_cast<int32_t*>(gbase + x.n);
     x.cbnd = x.rbnd + 2 * x.n + 2;
-    x.query = f.strand == FWD ? a.rseq + a.roff[r] : a.qbuf + a.path_off[c];
+    x.rd = a.rseq + a.roff[r];
+    x.rev = f.strand != FWD;
     const msg_aln h = a.aln[c];
     dp_traceback(a, c, x, r, f, t_start, h.aln_to, h.aln_end, h.pad, h.aln_score, h.flags);
 }
