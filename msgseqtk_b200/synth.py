@@ -114,6 +114,9 @@ class ReadSet:
     def read(self, i: int) -> np.ndarray:
         return self.seqs[self.offs[i]:self.offs[i + 1]]
 
+    def qual(self, i: int) -> np.ndarray:
+        return self.quals[self.offs[i]:self.offs[i + 1]]
+
 
 def sample_reads(genomes, n_reads: int, L: int = 150, seed: int = 3, sub_rate: float = 0.01,
                  indel_rate: float = 0.001, q_lo: int = 20, q_hi: int = 40) -> ReadSet:

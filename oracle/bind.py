@@ -233,6 +233,12 @@ class Reference:
         L.ref_map_batch.argtypes = [C.c_void_p, C.c_int64, u8p, u8p, i64p, C.c_int64, C.c_double, C.c_int64,
                                     C.c_double, C.c_int, C.POINTER(C.c_double), i64p]
         L.ref_max_threads.restype = C.c_int
+        L.ref_sam_batch.restype = C.c_int64
+        L.ref_sam_batch.argtypes = [C.c_void_p, C.c_int64, u8p, u8p, i64p, C.c_int64, C.c_double, C.c_int64,
+                                    C.c_double, C.c_int, C.c_char_p, C.c_int64]
+        L.ref_sam_from_records.restype = C.c_int64
+        L.ref_sam_from_records.argtypes = [C.c_void_p, C.c_int64, u8p, u8p, i64p, C.c_void_p, C.POINTER(C.c_uint32),
+                                           i64p, C.c_double, C.c_int, C.c_char_p, C.c_int64]
         seqs = np.ascontiguousarray(np.concatenate(chroms).astype(np.uint8))
         offs = np.zeros(len(chroms) + 1, dtype=np.int64)
         np.cumsum([len(c) for c in chroms], out=offs[1:])
@@ -348,6 +354,40 @@ class Reference:
             if n <= cap and cu.value <= ccap and mu.value <= mcap:
                 return _aln_records(arr, n, cg, md.raw)
             cap, ccap, mcap = max(cap, n) * 2, max(ccap, cu.value) * 2, max(mcap, mu.value) * 2
+
+    @staticmethod
+    def _text(fn):
+        cap = 1 << 20
+        while True:
+            buf = C.create_string_buffer(cap)
+            n = fn(buf, cap)
+            if n <= cap:
+                return buf.raw[:n].decode().splitlines()
+            cap = n + 1
+
+    def sam_batch(self, reads, quals, offs, min_len=17, max_evalue=0.01, max_nseed=500, min_score_rate=0.65,
+                  max_report=1):
+        """SAM records (text lines, see ref_harness.cpp) of the reference's
+        single-end path."""
+        reads = np.ascontiguousarray(reads, dtype=np.uint8)
+        quals = np.ascontiguousarray(quals, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs, dtype=np.int64)
+        return self._text(lambda b, cap: self.lib.ref_sam_batch(
+            self.h, len(offs) - 1, _p(reads, u8p), _p(quals, u8p), _p(offs, i64p), min_len, max_evalue, max_nseed,
+            min_score_rate, max_report, b, cap))
+
+    def sam_from_records(self, reads, quals, offs, aln, cigar, read_aln_off, min_score_rate=0.65, max_report=1):
+        """SAM records from alignment records of the CUDA library, through the
+        reference's own tail (filter, evaluate, calcMapQ, sort, exportBAM)."""
+        reads = np.ascontiguousarray(reads, dtype=np.uint8)
+        quals = np.ascontiguousarray(quals, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs, dtype=np.int64)
+        aln = np.ascontiguousarray(aln)
+        cigar = np.ascontiguousarray(cigar, dtype=np.uint32)
+        roff = np.ascontiguousarray(read_aln_off, dtype=np.int64)
+        return self._text(lambda b, cap: self.lib.ref_sam_from_records(
+            self.h, len(offs) - 1, _p(reads, u8p), _p(quals, u8p), _p(offs, i64p), aln.ctypes.data,
+            cigar.ctypes.data_as(C.POINTER(C.c_uint32)), _p(roff, i64p), min_score_rate, max_report, b, cap))
 
     def map_batch(self, reads, quals, offs, n_threads=0, min_len=17, max_evalue=0.01, max_nseed=500,
                   min_score_rate=0.65):

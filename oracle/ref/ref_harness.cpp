@@ -334,6 +334,142 @@ int64_t ref_map_batch(void* h, int64_t n_reads, const uint8_t* reads, const uint
     return mapped;
 }
 
+/* ---- SAM records -----------------------------------------------------
+ * Each read's SAM records as text lines, from the reference's own tail:
+ * Alignment::filter/evaluate/calcMapQ/sort and exportBAM, plus the
+ * per-read output step of msgseqtk-align (src/msgseqtk-align.cpp:538-556 for
+ * mapped reads, :583-585 for unmapped ones), which lives in the program file
+ * and is restated here. A line holds the BAM fields the shim records:
+ * QNAME FLAG TID POS MAPQ CIGAR L_SEQ SEQ QUAL then the aux tags in order,
+ * float tags as the hex of their float32 value, so comparisons are exact. */
+static void put_bam(const EGriceLab::SAMtools::BAM& b, std::string& out) {
+    char buf[64];
+    out += b.qname;
+    std::snprintf(buf, sizeof buf, "\t%u\t%d\t%d\t%u\t", (unsigned)b.flag, b.tid, b.pos, (unsigned)b.mapQ);
+    out += buf;
+    for (uint32_t c : b.cigar) {
+        std::snprintf(buf, sizeof buf, "%u%c", c >> 4, "MIDNSHP=XB"[c & 0xf]);
+        out += buf;
+    }
+    if (b.cigar.empty()) out += "*";
+    std::snprintf(buf, sizeof buf, "\t%d\t", b.l_seq);
+    out += buf;
+    for (uint8_t x : b.seq) { std::snprintf(buf, sizeof buf, "%x", (unsigned)x); out += buf; }
+    out += "\t";
+    for (uint8_t x : b.qual) { std::snprintf(buf, sizeof buf, "%02x", (unsigned)x); out += buf; }
+    for (const auto& a : b.aux) {
+        out += "\t" + a.tag + ":" + a.type + ":";
+        if (a.type == 'Z') out += a.str;
+        else if (a.type == 'f') { std::snprintf(buf, sizeof buf, "%a", (double)(float)a.num); out += buf; }
+        else { std::snprintf(buf, sizeof buf, "%lld", (long long)a.num); out += buf; }
+    }
+    out += "\n";
+}
+
+static void sam_read(ALIGN_LIST& alns, const PrimarySeq& read, double min_score_rate, uint32_t max_report,
+                     std::string& out) {
+    using EGriceLab::SAMtools::BAM;
+    Alignment::filter(alns, min_score_rate);
+    if (alns.empty()) {  // output(read, out)
+        put_bam(BAM(read.getName(), read.length(), dna::nt16Encode(read.getSeq()), read.getQual(), BAM_FUNMAP), out);
+        return;
+    }
+    Alignment::evaluate(alns);
+    Alignment::calcMapQ(alns);
+    Alignment::sort(alns);
+    const size_t num_report = max_report == 0 ? alns.size() : std::min((size_t)max_report, alns.size());
+    for (size_t i = 0; i < num_report; ++i) {
+        BAM b = alns[i].exportBAM();
+        b.setSecondaryFlag(i > 0);
+        b.setAux(Alignment::NUM_REPORTED_ALIGNMENT_TAG, num_report);
+        b.setAux(Alignment::NUM_TOTAL_ALIGNMENT_TAG, alns.size());
+        b.setAux(Alignment::ALIGNMENT_POSTERIOR_PROB_TAG, alns[i].getPostP());
+        put_bam(b, out);
+    }
+}
+
+static int64_t put_out(const std::string& s, char* out, int64_t cap) {
+    if ((int64_t)s.size() <= cap && out) std::memcpy(out, s.data(), s.size());
+    return (int64_t)s.size();
+}
+
+/* SAM lines of the reference's single-end path (src/msgseqtk-align.cpp:600-640)
+ * for n reads (GLOBAL mode). Returns the text length; the text is written
+ * only when it fits in cap bytes. */
+int64_t ref_sam_batch(void* h, int64_t n_reads, const uint8_t* reads, const uint8_t* quals, const int64_t* offs,
+                      int64_t min_len, double max_evalue, int64_t max_nseed, double min_score_rate,
+                      int max_report, char* out, int64_t cap) {
+    RefDB* db = (RefDB*)h;
+    std::string text;
+    for (int64_t i = 0; i < n_reads; ++i) {
+        const int64_t L = offs[i + 1] - offs[i];
+        const std::string name = "r" + std::to_string(i);
+        const PrimarySeq r = make_read(reads + offs[i], L, quals ? quals + offs[i] : nullptr, name.c_str());
+        const PrimarySeq rc = r.revcom();
+        SeedList seeds = SMEM_LIST::findSeeds(&r, &db->mtg, &db->fmd, min_len, max_evalue, max_nseed);
+        ALIGN_LIST alns;
+        if (!seeds.empty()) {
+            ChainList chains = SeedChain::getChains(seeds, std::ceil(L * Alignment::MAX_MISMATCH_RATE),
+                                                    std::ceil(L * Alignment::MAX_INDEL_RATE));
+            alns = Alignment::buildAlignments(&r, &rc, db->mtg, chains, Alignment::GLOBAL);
+        }
+        sam_read(alns, r, min_score_rate, (uint32_t)max_report, text);
+    }
+    return put_out(text, out, cap);
+}
+
+/* The same lines with the alignments taken from records of the CUDA library
+ * (msg_aln, include/msg_b200.h; 88 bytes each) and their CIGAR words: each
+ * record sets the fields buildAlignments would set (Alignment.h:357-375), the
+ * path is the CIGAR's M/I/D runs (soft clips are alnFrom/alnTo), and the
+ * reference's tail runs unchanged. */
+int64_t ref_sam_from_records(void* h, int64_t n_reads, const uint8_t* reads, const uint8_t* quals,
+                             const int64_t* offs, const void* records, const uint32_t* cigar,
+                             const int64_t* read_aln_off, double min_score_rate, int max_report, char* out,
+                             int64_t cap) {
+    RefDB* db = (RefDB*)h;
+    struct Rec {
+        int64_t read; int32_t tid, strand; int64_t t_start, t_end, aln_from, aln_to, aln_start, aln_end;
+        int32_t aln_score, flags; int64_t cigar_off; int32_t n_cigar, pad;
+    };
+    static_assert(sizeof(Rec) == 88, "msg_aln layout");
+    const Rec* rec = (const Rec*)records;
+    std::string text;
+    for (int64_t i = 0; i < n_reads; ++i) {
+        const int64_t L = offs[i + 1] - offs[i];
+        const std::string name = "r" + std::to_string(i);
+        const PrimarySeq r = make_read(reads + offs[i], L, quals ? quals + offs[i] : nullptr, name.c_str());
+        const PrimarySeq rc = r.revcom();
+        ALIGN_LIST alns;
+        for (int64_t k = read_aln_off[i]; k < read_aln_off[i + 1]; ++k) {
+            const Rec& g = rec[k];
+            Alignment a(&r);
+            a.rcRead = &rc;
+            a.tid = g.tid;
+            a.target = &db->mtg.getSeq(g.tid);
+            a.qStrand = (GLoc::STRAND)g.strand;
+            a.qFrom = 0;
+            a.qTo = L;
+            a.tStart = g.t_start;
+            a.tEnd = g.t_end;
+            a.alnMode = Alignment::GLOBAL;
+            a.alnFrom = g.aln_from;
+            a.alnTo = g.aln_to;
+            a.alnStart = g.aln_start;
+            a.alnEnd = g.aln_end;
+            a.alnScore = g.aln_score == INT32_MIN ? -std::numeric_limits<double>::infinity() : (double)g.aln_score;
+            for (int32_t w = 0; w < g.n_cigar; ++w) {
+                const uint32_t c = cigar[g.cigar_off + w];
+                if ((c & 0xf) == BAM_CSOFT_CLIP) continue;
+                a.alnPath.append(c >> 4, c & 0xf);
+            }
+            alns.push_back(a);
+        }
+        sam_read(alns, r, min_score_rate, (uint32_t)max_report, text);
+    }
+    return put_out(text, out, cap);
+}
+
 int ref_max_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

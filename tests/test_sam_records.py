@@ -1,0 +1,77 @@
+"""SAM records: alignment records fed through the reference's own tail
+(filter, evaluate, calcMapQ, sort, exportBAM and msgseqtk-align's per-read
+output) must give the same SAM fields as the reference's whole single-end
+path. On the CPU the records come from the oracle; on the GPU (-m gpu) from
+the CUDA library through the C ABI."""
+import os
+
+import numpy as np
+import pytest
+
+from msgseqtk_b200 import lib, synth
+from oracle.bind import REF_SO, Oracle, Reference
+
+needs_ref = pytest.mark.skipif(not os.path.exists(REF_SO), reason="oracle/_ref not built")
+
+
+def _records_from_oracle(orc, reads):
+    recs, cig, roff = [], [], [0]
+    for i, r in enumerate(reads):
+        for e in orc.align_read(r):
+            recs.append((i, e["tid"], e["strand"], e["t_start"], e["t_end"], e["aln_from"], e["aln_to"],
+                         e["aln_start"], e["aln_end"],
+                         int(e["aln_score"]) if np.isfinite(e["aln_score"]) else -(2 ** 31), e["flags"], len(cig),
+                         len(e["cigar"]), 0))
+            cig += e["cigar"]
+        roff.append(len(recs))
+    return (np.array(recs, dtype=lib.ALN_DTYPE), np.array(cig, dtype=np.uint32), np.array(roff, dtype=np.int64))
+
+
+def _workload(seed):
+    g = synth.small_genomes(seed=seed, n_genomes=3, length=60_000)
+    a = synth.sample_reads(g, 300, seed=seed + 1)
+    b = synth.sample_reads(g, 100, seed=seed + 2, sub_rate=0.05, indel_rate=0.01)
+    reads = [a.read(i) for i in range(len(a))] + [b.read(i) for i in range(len(b))]
+    quals = [a.qual(i) for i in range(len(a))] + [b.qual(i) for i in range(len(b))]
+    rng = np.random.default_rng(seed)
+    reads += [synth._BASES[rng.integers(0, 4, 150)] for _ in range(40)]
+    quals += [rng.integers(20, 41, 150).astype(np.uint8) for _ in range(40)]
+    seq = np.concatenate(reads).astype(np.uint8)
+    qual = np.concatenate(quals).astype(np.uint8)
+    off = np.concatenate([[0], np.cumsum([len(x) for x in reads])]).astype(np.int64)
+    return g, reads, seq, qual, off
+
+
+@needs_ref
+def test_tail_on_oracle_records_matches_reference(oracle_built):
+    from msgseqtk_b200 import index_build
+    g, reads, seq, qual, off = _workload(5)
+    ref = Reference(g)
+    orc = Oracle(index_build.build_view(g))
+    aln, cig, roff = _records_from_oracle(orc, reads)
+    for max_report in (1, 0):
+        exp = ref.sam_batch(seq, qual, off, max_report=max_report)
+        got = ref.sam_from_records(seq, qual, off, aln, cig, roff, max_report=max_report)
+        assert got == exp
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_gpu_records_give_reference_sam():
+    from msgseqtk_b200 import index_build
+    g, reads, seq, qual, off = _workload(7)
+    ref = Reference(g)
+    view = index_build.build_view(g)
+    ctx = lib.Context(0)
+    try:
+        ctx.load_index(view)
+        for params in (lib.default_params(min_score_rate=0.65), lib.default_params(),
+                       lib.default_params(min_score_rate=0.65, band_mode=1, band_w=7)):
+            res = ctx.map(seq, off, params)
+            for max_report in (1, 0):
+                exp = ref.sam_batch(seq, qual, off, max_report=max_report)
+                got = ref.sam_from_records(seq, qual, off, res["aln"], res["cigar"], res["read_aln_off"],
+                                           max_report=max_report)
+                assert got == exp
+    finally:
+        ctx.close()
