@@ -221,10 +221,10 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     tm.mark();  // 0
 #define CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return ctx->cuda_fail(e_); } while (0)
     DevBuf& misc = ctx->misc;
-    CK(ctx->status.ensure(64));
+    CK(ctx->status.ensure(128));
     uint32_t* d_status = ctx->status.as<uint32_t>();
     unsigned long long* d_ctr = reinterpret_cast<unsigned long long*>(d_status + 4);
-    CK(cudaMemsetAsync(d_status, 0, 64, st));
+    CK(cudaMemsetAsync(d_status, 0, 128, st));
 
     // read lengths
     CK(ctx->rcount.ensure((n_reads + 1) * sizeof(int64_t) * 8 + 64));
@@ -246,67 +246,87 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     const int64_t Lmax = (int64_t)h_maxlen;
 
     // ---------------- SMEMs ----------------
-    // Reads up to 254 bp: one thread per read (k_smem_thread); longer reads:
-    // one warp per read with lanes over the candidate list (k_smem).
-    // The thread kernel keeps at most kThreadPrev candidates per read so that
-    // all candidate lists stay in L2; a batch with a longer list reruns on the
-    // warp kernel, whose per-warp lists hold a whole read.
+    // Reads are bucketed by length: up to kThreadMaxLen bp one thread per read
+    // (k_smem_thread), longer reads one warp per read with lanes over the
+    // candidate list (k_smem); both launches share the batch. Each read's SMEM
+    // rows go to its own slot, cap rows per 150 bases (at least cap), so long
+    // reads get room in proportion. The thread kernel keeps at most
+    // kThreadPrev candidates per read so that all candidate lists stay in L2;
+    // when a list outgrows it, the short reads rerun on the warp kernel too.
     constexpr int64_t kThreadPrev = 48;
-    bool thread_path = Lmax + 2 <= 256;
+    constexpr int64_t kThreadMaxLen = 254;
     const int threads = 256;
     const int blocks = ctx->num_sms * 8;
     const int64_t n_warps = (int64_t)blocks * threads / 32;
-    int64_t pv_cap = thread_path ? std::min<int64_t>(Lmax + 2, kThreadPrev) : Lmax + 2;
-    int64_t n_thr = 0;
+    CK(ctx->rlist.ensure((n_reads + 1) * 8 * 4 + 64));
+    int64_t* d_short = ctx->rlist.as<int64_t>();
+    int64_t* d_long = d_short + (n_reads + 1);
+    int64_t* d_slot = d_long + (n_reads + 1);        // slot rows per read (n + 1)
+    int64_t* d_slot_off = d_slot + (n_reads + 1);    // slot offsets (n + 1)
+    unsigned long long h_split[2] = {0, 0};
+    if (n_reads > 0) {
+        CK(cudaMemsetAsync(d_ctr + 4, 0, 16, st));
+        S.n_launch++, k_split_len<<<nblk(n_reads, 256), 256, 0, st>>>(d_rlen, n_reads, kThreadMaxLen, d_short, d_long,
+                                                                      d_ctr + 4);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(h_split, d_ctr + 4, 16, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    bool thread_path = h_split[0] > 0;
     int64_t cap = 16;
     int64_t h_nsmem = 0;
-    for (int attempt = 0; attempt < 3; ++attempt) {
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        int64_t h_rows = 0;
+        if (n_reads > 0) S.n_launch++, k_slot_rows<<<nblk(n_reads, 256), 256, 0, st>>>(d_rlen, n_reads, cap, d_slot);
+        CK(offsets(ctx, d_slot, n_reads, d_slot_off, misc, &h_rows));
+        CK(ctx->smem.ensure((size_t)std::max<int64_t>(1, h_rows) * 48));
+        CK(ctx->smem_cnt.ensure((n_reads + 1) * sizeof(int32_t)));
+        CK(cudaMemsetAsync(d_ctr, 0, 8 * 4, st));
+        CK(cudaMemsetAsync(d_status, 0, 4, st));
+        // short reads on the thread kernel
         if (thread_path) {
             int bps = 0;
             CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread, 128, 0));
-            n_thr = (int64_t)ctx->num_sms * std::max(1, bps) * 128;
+            const int64_t n_thr = (int64_t)ctx->num_sms * std::max(1, bps) * 128;
+            const int64_t pv_cap = kThreadPrev;
             CK(ctx->prev.ensure(n_thr * pv_cap * sizeof(PrevEntry) + 64));
             CK(cudaMemcpyToSymbolAsync(c_llk, im.llk, sizeof(im.llk), 0, cudaMemcpyHostToDevice, st));
-        } else {
-            CK(ctx->prev.ensure(n_warps * pv_cap * (4 + 8 + 8 + 8 + 8) + 64));
-        }
-        CK(ctx->smem.ensure((size_t)std::max<int64_t>(1, n_reads) * cap * 48));
-        CK(ctx->smem_cnt.ensure((n_reads + 1) * sizeof(int32_t)));
-        CK(cudaMemsetAsync(d_ctr, 0, 16, st));
-        CK(cudaMemsetAsync(d_status, 0, 4, st));
-        if (thread_path) {
             SmemThreadArgs ta{};
-            ta.seq = d_seq; ta.off = d_off; ta.n_reads = n_reads; ta.min_len = params->min_len;
+            ta.seq = d_seq; ta.off = d_off; ta.n_reads = (int64_t)h_split[0]; ta.min_len = params->min_len;
             ta.thr = thr; ta.thr_all = thr_all;
             ta.llk_min = *std::min_element(im.llk, im.llk + 16);
             ta.llk_max = *std::max_element(im.llk, im.llk + 16);
-            ta.out = ctx->smem.as<int64_t>(); ta.cap = cap; ta.count = ctx->smem_cnt.as<int32_t>();
+            ta.out = ctx->smem.as<int64_t>(); ta.cap = cap; ta.out_off = d_slot_off; ta.list = d_short;
+            ta.count = ctx->smem_cnt.as<int32_t>();
             ta.prev = ctx->prev.as<PrevEntry>(); ta.pv_cap = pv_cap;
             ta.work = d_ctr; ta.n_ext = d_ctr + 1; ta.status = d_status;
-            if (n_reads > 0) {
-                S.n_launch++, k_smem_thread<<<n_thr / 128, 128, 0, st>>>(ta, ix);
-                CK(cudaGetLastError());
-            }
-        } else {
+            S.n_launch++, k_smem_thread<<<n_thr / 128, 128, 0, st>>>(ta, ix);
+            CK(cudaGetLastError());
+        }
+        // long reads (all reads once the thread kernel has given up) on the warp kernel
+        const int64_t n_warp_reads = thread_path ? (int64_t)h_split[1] : n_reads;
+        if (n_warp_reads > 0) {
+            const int64_t pv_cap = Lmax + 2;
+            CK(ctx->prevw.ensure(n_warps * pv_cap * (4 + 8 + 8 + 8 + 8) + 64));
             SmemArgs sa{};
-            sa.seq = d_seq; sa.off = d_off; sa.n_reads = n_reads; sa.min_len = params->min_len;
+            sa.seq = d_seq; sa.off = d_off; sa.n_reads = n_warp_reads; sa.min_len = params->min_len;
             sa.thr = thr; sa.thr_all = thr_all;
             for (int b = 0; b < 16; ++b) sa.llk[b] = im.llk[b];
-            sa.out = ctx->smem.as<int64_t>(); sa.cap = cap; sa.count = ctx->smem_cnt.as<int32_t>();
-            char* pv = ctx->prev.as<char>();
+            sa.out = ctx->smem.as<int64_t>(); sa.cap = cap; sa.out_off = d_slot_off;
+            sa.list = thread_path ? d_long : nullptr;
+            sa.count = ctx->smem_cnt.as<int32_t>();
+            char* pv = ctx->prevw.as<char>();
             sa.pv_p = reinterpret_cast<int64_t*>(pv);
             sa.pv_q = sa.pv_p + n_warps * pv_cap;
             sa.pv_s = sa.pv_q + n_warps * pv_cap;
             sa.pv_lp = reinterpret_cast<double*>(sa.pv_s + n_warps * pv_cap);
             sa.pv_pos = reinterpret_cast<int32_t*>(sa.pv_lp + n_warps * pv_cap);
             sa.pv_cap = pv_cap;
-            sa.work = d_ctr;
+            sa.work = d_ctr + 3;
             sa.n_ext = d_ctr + 1;
             sa.status = d_status;
-            if (n_reads > 0) {
-                S.n_launch++, k_smem<<<blocks, threads, 0, st>>>(sa, ix);
-                CK(cudaGetLastError());
-            }
+            S.n_launch++, k_smem<<<blocks, threads, 0, st>>>(sa, ix);
+            CK(cudaGetLastError());
         }
         uint32_t h_status = 0;
         CK(cudaMemcpyAsync(&h_status, d_status, 4, cudaMemcpyDeviceToHost, st));
@@ -315,15 +335,19 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         if (h_status & 0x100u) {  // a candidate list outgrew the thread kernel's cap
             if (!thread_path) return ctx->fail(MSG_EINTERNAL, "SMEM candidate list overflow");
             thread_path = false;
-            pv_cap = Lmax + 2;
             continue;
         }
         if (!(h_status & kErrOverflow)) break;
-        if (attempt == 2) return ctx->fail(MSG_EINTERNAL, "SMEM output overflow after resizing");
-        // rerun with the largest per-read count as capacity
+        if (attempt == 3) return ctx->fail(MSG_EINTERNAL, "SMEM output overflow after resizing");
+        // rerun with a per-150-base capacity that fits every read's count
         std::vector<int32_t> cnt(n_reads);
+        std::vector<int64_t> len(n_reads);
         CK(cudaMemcpy(cnt.data(), ctx->smem_cnt.p, n_reads * 4, cudaMemcpyDeviceToHost));
-        cap = *std::max_element(cnt.begin(), cnt.end());
+        CK(cudaMemcpy(len.data(), d_rlen, n_reads * 8, cudaMemcpyDeviceToHost));
+        for (int64_t r = 0; r < n_reads; ++r) {
+            const int64_t per = std::max<int64_t>(len[r], kSlotBases);
+            cap = std::max<int64_t>(cap, ((int64_t)cnt[r] * kSlotBases + per - 1) / per);
+        }
     }
     {
         unsigned long long e = 0;
@@ -342,8 +366,9 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     int32_t* d_fill = d_smem_read + (h_nsmem + 1);
     uint8_t* d_sel = reinterpret_cast<uint8_t*>(d_fill + (h_nsmem + 1));
     if (n_reads > 0) {
-        S.n_launch++, k_compact_smem<<<nblk(n_reads * 32, 256), 256, 0, st>>>(ctx->smem.as<int64_t>(), cap, ctx->smem_cnt.as<int32_t>(), d_smem_off,
-                                               n_reads, d_smem);
+        S.n_launch++, k_compact_smem<<<nblk(n_reads * 32, 256), 256, 0, st>>>(ctx->smem.as<int64_t>(), d_slot_off,
+                                                                             ctx->smem_cnt.as<int32_t>(), d_smem_off,
+                                                                             n_reads, d_smem);
         CK(cudaGetLastError());
     }
     tm.mark();  // 1

@@ -32,9 +32,11 @@ struct SmemArgs {
     double thr;        // largest log-likelihood whose e-value passes (host-computed)
     int thr_all;       // 1 when max_evalue is +inf: every SMEM passes
     double llk[16];
-    int64_t* out;      // 6 x int64 rows; read r's slot starts at row r * cap
-    int64_t cap;
-    int32_t* count;    // per read: SMEMs emitted (may exceed cap)
+    int64_t* out;      // 6 x int64 rows; read r's slot starts at row out_off[r] (r * cap when null)
+    int64_t cap;       // slot rows when out_off is null
+    const int64_t* out_off;  // per-read slot offsets (n + 1), or null
+    const int64_t* list;     // reads handled by this launch (read k when null)
+    int32_t* count;    // per read: SMEMs emitted (may exceed its slot)
     int32_t* pv_pos;   // per-warp prev lists, pv_cap entries each
     int64_t* pv_p;
     int64_t* pv_q;
@@ -58,6 +60,7 @@ struct WarpSmem {
     int64_t L;
     int64_t* out;
     int32_t n_out;
+    int64_t cap_r;     // rows of this read's slot
     int32_t* pv_pos;
     int64_t *pv_p, *pv_q, *pv_s;
     double* pv_lp;
@@ -69,7 +72,7 @@ struct WarpSmem {
         const unsigned m = __ballot_sync(0xffffffffu, cand);
         if (cand) {
             const int64_t k = n_out + __popc(m & lanemask_lt());
-            if (k < a->cap) {
+            if (k < cap_r) {
                 int64_t* o = out + 6 * k;
                 o[0] = from; o[1] = to; o[2] = p; o[3] = q; o[4] = s;
                 o[5] = __double_as_longlong(lp);
@@ -276,15 +279,18 @@ __global__ void __launch_bounds__(256) k_smem(SmemArgs a, IndexDev ix) {
         if (lane_id() == 0) r = atomicAdd(a.work, 1ull);
         r = __shfl_sync(0xffffffffu, r, 0);
         if ((int64_t)r >= a.n_reads) break;
+        if (a.list) r = (unsigned long long)a.list[r];
         const int64_t o0 = a.off[r];
         w.rd = a.seq + o0;
         w.L = a.off[r + 1] - o0;
-        w.out = a.out + 6 * (int64_t)r * a.cap;
+        const int64_t slot = a.out_off ? a.out_off[r] : (int64_t)r * a.cap;
+        w.cap_r = a.out_off ? a.out_off[r + 1] - slot : a.cap;
+        w.out = a.out + 6 * slot;
         w.n_out = 0;
         if (w.L > 0) w.find_all();
         if (lane_id() == 0) {
             a.count[r] = w.n_out;
-            if (w.n_out > a.cap) atomicOr(a.status, kErrOverflow);
+            if (w.n_out > w.cap_r) atomicOr(a.status, kErrOverflow);
         }
     }
     // lanes count their own extensions
@@ -293,14 +299,32 @@ __global__ void __launch_bounds__(256) k_smem(SmemArgs a, IndexDev ix) {
     if (lane_id() == 0 && e) atomicAdd(a.n_ext, e);
 }
 
-// Copy each read's SMEMs into a dense array (read r at smem_off[r]).
-// One warp per read.
-__global__ void k_compact_smem(const int64_t* __restrict__ src, int64_t cap, const int32_t* __restrict__ count,
-                               const int64_t* __restrict__ smem_off, int64_t n_reads, int64_t* __restrict__ dst) {
+// Copy each read's SMEMs from its slot (slot_off) into a dense array (read r
+// at smem_off[r]). One warp per read.
+__global__ void k_compact_smem(const int64_t* __restrict__ src, const int64_t* __restrict__ slot_off,
+                               const int32_t* __restrict__ count, const int64_t* __restrict__ smem_off,
+                               int64_t n_reads, int64_t* __restrict__ dst) {
     const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (r >= n_reads) return;
-    const int64_t n = min((int64_t)count[r], cap);
-    for (int64_t j = lane_id(); j < 6 * n; j += 32) dst[6 * smem_off[r] + j] = src[6 * r * cap + j];
+    const int64_t n = min((int64_t)count[r], slot_off[r + 1] - slot_off[r]);
+    for (int64_t j = lane_id(); j < 6 * n; j += 32) dst[6 * smem_off[r] + j] = src[6 * slot_off[r] + j];
+}
+
+// Reads up to max_len bp into `short_list`, longer ones into `long_list`.
+__global__ void k_split_len(const int64_t* __restrict__ len, int64_t n, int64_t max_len,
+                            int64_t* __restrict__ short_list, int64_t* __restrict__ long_list,
+                            unsigned long long* __restrict__ counts) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    if (len[r] <= max_len) short_list[atomicAdd(&counts[0], 1ull)] = r;
+    else long_list[atomicAdd(&counts[1], 1ull)] = r;
+}
+
+// SMEM slot rows per read: cap per 150 bases, at least cap.
+constexpr int64_t kSlotBases = 150;
+__global__ void k_slot_rows(const int64_t* __restrict__ len, int64_t n, int64_t cap, int64_t* __restrict__ rows) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r < n) rows[r] = max(cap, (len[r] * cap + kSlotBases - 1) / kSlotBases);
 }
 
 // ======================================================================

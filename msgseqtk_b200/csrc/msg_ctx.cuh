@@ -56,7 +56,7 @@ struct msg_ctx {
     msg_map_stats stats{};
     // batch buffers
     msg::DevBuf reads, offs, smem, smem_cnt, prev, sel, seedoff, seeds, seeds2, rcount, chains, chainidx, dpinfo,
-        scratch, path, alnbuf, cigbuf, misc, status, geobuf, bandbuf, alnbuf2, recoff;
+        scratch, path, alnbuf, cigbuf, misc, status, geobuf, bandbuf, alnbuf2, recoff, rlist, prevw;
     // band model (bf16 weights, fp32 feature mean/scale) and training buffers
     msg::DevBuf band_wts, band_nrm, tr_x, tr_y, tr_ord, tr_w, tr_m, tr_v, tr_g, tr_loss;
     bool band_loaded = false;

@@ -40,7 +40,9 @@ struct SmemThreadArgs {
     int thr_all;
     double llk_min, llk_max;  // extremes of the per-base log-likelihoods
     int64_t* out;
-    int64_t cap;
+    int64_t cap;            // slot rows when out_off is null
+    const int64_t* out_off; // per-read slot offsets (n + 1), or null: slot r at row r * cap
+    const int64_t* list;    // reads handled by this launch (read k when null)
     int32_t* count;
     PrevEntry* prev;        // pv_cap entries per thread
     int64_t pv_cap;
@@ -69,6 +71,7 @@ struct ThreadSmem {
     int64_t* out;
     int32_t L;
     int32_t n_out;
+    int32_t cap_r;          // rows of this read's slot
     int32_t r;
     // findAllSMEMS variables and the call in progress
     int32_t from, to;
@@ -98,7 +101,7 @@ struct ThreadSmem {
 
 __device__ __forceinline__ void smem_emit(ThreadSmem& t, const SmemThreadArgs& a, int32_t from, int32_t to,
                                           uint32_t p, uint32_t q, uint32_t s, double lp) {
-    if (t.n_out < a.cap) {
+    if (t.n_out < t.cap_r) {
         int64_t* o = t.out + 6 * (int64_t)t.n_out;
         o[0] = from; o[1] = to; o[2] = p; o[3] = q; o[4] = s;
         o[5] = __double_as_longlong(lp);
@@ -289,15 +292,18 @@ __global__ void __launch_bounds__(128, 5) k_smem_thread(SmemThreadArgs a, IndexD
             if (t.phase == PH_NEXT_READ || t.phase == PH_DONE) {
                 if (t.phase == PH_DONE) {
                     a.count[t.r] = t.n_out;
-                    if (t.n_out > a.cap) atomicOr(a.status, kErrOverflow);
+                    if (t.n_out > t.cap_r) atomicOr(a.status, kErrOverflow);
                 }
-                const unsigned long long r = atomicAdd(a.work, 1ull);
+                unsigned long long r = atomicAdd(a.work, 1ull);
                 if ((int64_t)r >= a.n_reads) { alive = false; break; }
+                if (a.list) r = (unsigned long long)a.list[r];
                 t.r = (int32_t)r;
                 const int64_t o0 = a.off[r];
                 t.rd = a.seq + o0;
                 t.L = (int32_t)(a.off[r + 1] - o0);
-                t.out = a.out + 6 * (int64_t)r * a.cap;
+                const int64_t slot = a.out_off ? a.out_off[r] : (int64_t)r * a.cap;
+                t.cap_r = (int32_t)(a.out_off ? a.out_off[r + 1] - slot : a.cap);
+                t.out = a.out + 6 * slot;
                 t.n_out = 0;
                 t.ovf = 0;
                 if (t.L <= 0) { t.phase = PH_DONE; continue; }

@@ -171,3 +171,37 @@ def test_unsupported_inputs_fail_loudly(ctx):
     with pytest.raises(lib.MsgError) as e:
         ctx.load_index(index_build.build_view(gn))
     assert e.value.code == lib.MSG_EUNSUPPORTED
+
+
+def test_uneven_lengths_match_oracle(ctx, oracle_built):
+    """One batch mixing read lengths as the uneven-length workload does (75-150,
+    250-300 and 1-2 kbp; 5% errors, 70% substitutions / 30% indels): short
+    reads take the thread SMEM kernel, the others the warp kernel."""
+    g = synth.small_genomes(seed=61, n_genomes=3, length=100_000)
+    view = index_build.build_view(g)
+    ctx.load_index(view)
+    orc = Oracle(view)
+    rng = np.random.default_rng(62)
+    lens = list(rng.integers(75, 151, 40)) + list(rng.integers(250, 301, 20)) + list(rng.integers(1000, 2001, 8))
+    reads = []
+    for k, L in enumerate(lens):
+        rs = synth.sample_reads(g, 1, L=int(L), seed=1000 + k, sub_rate=0.035, indel_rate=0.015)
+        reads.append(rs.read(0).copy())
+    order = rng.permutation(len(reads))
+    reads = [reads[k] for k in order]
+    seq = np.concatenate(reads).astype(np.uint8)
+    off = np.concatenate([[0], np.cumsum([len(x) for x in reads])]).astype(np.int64)
+    res = ctx.map(seq, off)
+    compare_with_oracle(res, orc, lambda i: reads[i], len(reads), g)
+    res = ctx.map(seq, off, lib.default_params(min_score_rate=0.65, band_mode=1, band_w=15))
+    n_kept = 0
+    for i, r in enumerate(reads):
+        exp = [e for e in orc.align_read(r) if not (e["aln_score"] < len(r) * 0.65)]
+        got = aln_records(res, i)
+        assert len(got) == len(exp), i
+        n_kept += len(got)
+        for (fields, words, flags), e in zip(got, exp):
+            assert fields[:8] == [e["tid"], e["strand"], e["t_start"], e["t_end"], e["aln_from"], e["aln_to"],
+                                  e["aln_start"], e["aln_end"]], i
+            assert words == e["cigar"], i
+    assert n_kept > 0
