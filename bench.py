@@ -45,6 +45,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "mapped reads/sec/GPU (2x150bp) + DP GCUPS, learned-band vs plain GPU, bit-exact SAM"
+WORKLOADS = {
+    "scale": "scale: 200 genomes ~600 Mbp (log-normal, GC 30-70%), 2x150 bp pairs, insert N(400,50), 1% sub, "
+             "0.1% indel, 5% random pairs; mates mapped as single reads (findSeedsPE)",
+    "uneven": "uneven: 200 genomes ~600 Mbp; single-end reads 60% 75-150 bp, 30% 250-300 bp, 10% 1-10 kbp, "
+              "5% errors (70% substitutions, 30% indels); one batch",
+}
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 HBM_FALLBACK = 6650.0
 
@@ -67,6 +73,9 @@ def parse():
                     help="read pairs (fresh seed) whose chains train the band classifier")
     ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--min-score", type=float, default=0.65, help="Alignment::filter rate (msgseqtk-align -s)")
+    ap.add_argument("--workload", default="scale", choices=["scale", "uneven"],
+                    help="scale: 2x150 bp pairs; uneven: single-end reads of mixed lengths (one batch)")
+    ap.add_argument("--uneven-reads", type=int, default=500_000)
     return ap.parse_args()
 
 
@@ -139,6 +148,33 @@ def reduce_over_ranks(ms: float, n_reads: float, device) -> tuple[float, float]:
     return float(t.item()), float(n.item())
 
 
+def uneven_reads(genomes, n, seed):
+    """Single-end reads of mixed lengths: 60% U{75..150}, 30% U{250..300},
+    10% U{1000..10000} bp, all with 5% errors (70% substitutions, 30% indels
+    of 1-3 bp), shuffled. Each group is sampled at its longest length and every
+    read cut to its own length (a prefix of a read is a read of the same error
+    model)."""
+    from msgseqtk_b200 import synth
+    rng = np.random.default_rng(seed)
+    groups = [(int(0.6 * n), 75, 150), (int(0.3 * n), 250, 300), (n - int(0.6 * n) - int(0.3 * n), 1000, 10000)]
+    seqs, quals = [], []
+    for k, (m, lo, hi) in enumerate(groups):
+        if m <= 0:
+            continue
+        rs = synth.sample_reads(genomes, m, L=hi, seed=seed * 10 + k, sub_rate=0.035, indel_rate=0.015)
+        lens = rng.integers(lo, hi + 1, m)
+        for i in range(m):
+            seqs.append(rs.read(i)[:lens[i]])
+            quals.append(rs.quals[rs.offs[i]:rs.offs[i] + lens[i]])
+    order = rng.permutation(len(seqs))
+    seqs = [seqs[k] for k in order]
+    quals = [quals[k] for k in order]
+    offs = np.zeros(len(seqs) + 1, dtype=np.int64)
+    np.cumsum([len(x) for x in seqs], out=offs[1:])
+    return synth.ReadSet(np.concatenate(seqs).astype(np.uint8), offs, np.concatenate(quals).astype(np.uint8),
+                         np.zeros((len(seqs), 3), dtype=np.int64))
+
+
 def make_workload(args, rank, device):
     from msgseqtk_b200 import index_build, synth
     t0 = time.time()
@@ -146,8 +182,11 @@ def make_workload(args, rank, device):
     t1 = time.time()
     view = index_build.build_view(genomes, device=device)
     t2 = time.time()
-    m1, m2 = synth.sample_pairs(genomes, args.pairs, seed=reads_seed(rank))
-    reads = synth.interleave(m1, m2)
+    if args.workload == "uneven":
+        reads = uneven_reads(genomes, args.uneven_reads, seed=reads_seed(rank))
+    else:
+        m1, m2 = synth.sample_pairs(genomes, args.pairs, seed=reads_seed(rank))
+        reads = synth.interleave(m1, m2)
     t3 = time.time()
     setup = {"genome_s": round(t1 - t0, 1), "index_s": round(t2 - t1, 1), "reads_s": round(t3 - t2, 1)}
     return genomes, view, reads, setup
@@ -273,7 +312,7 @@ def main():
     del treads, tm1, tm2
 
     # batches: reads resident on the device, and pinned host copies for e2e
-    bp = 2 * args.batch_pairs
+    bp = 2 * args.batch_pairs if args.workload == "scale" else len(reads)
     n_batches = max(1, len(reads) // bp)
     d_seq = torch.from_numpy(reads.seqs).cuda()
     offs_d = []
@@ -395,8 +434,12 @@ def main():
         res_p = ctx.map(reads.seqs[:reads.offs[n]], reads.offs[:n + 1], plain_params)
         same = all(np.array_equal(res[k], res_p[k]) for k in ("aln", "cigar", "read_aln_off"))
         bad = 0
+        checked = 0
         for i in range(n):
             L = len(reads.read(i))
+            if L > 2000:
+                continue  # the oracle fills whole double matrices: long reads are checked by the tests
+            checked += 1
             exp = [e for e in orc.align_read(reads.read(i)) if not (e["aln_score"] < L * args.min_score)]
             got = res["aln"][res["read_aln_off"][i]:res["read_aln_off"][i + 1]]
             if len(exp) != len(got):
@@ -411,11 +454,11 @@ def main():
                 if f != ef or w != e["cigar"]:
                     bad += 1
                     break
-        valid = {"reads": n, "mismatching_reads": bad, "learned_equals_plain": bool(same),
+        valid = {"reads": checked, "mismatching_reads": bad, "learned_equals_plain": bool(same),
                  "compared": "records after Alignment::filter (alnScore >= L * %g)" % args.min_score}
 
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and not args.no_cpu_baseline and args.workload == "scale":
         r = cpu_baseline(genomes, view, reads, args.cpu_seconds)
         cpu = r[0] if r else None
 
@@ -423,11 +466,11 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-                "config": {"workload": "scale: 200 genomes ~600 Mbp (log-normal, GC 30-70%), 2x150 bp pairs, "
-                                       "insert N(400,50), 1% sub, 0.1% indel, 5% random pairs; mates mapped as "
-                                       "single reads (findSeedsPE)",
+                "config": {"workload": WORKLOADS[args.workload],
                            "reads_per_step": bp, "pairs_per_gpu": args.pairs, "bd_symbols": view.n,
-                           "l2": "inputs larger than L2 (index %.1f GB, new reads every step)" % setup["index_gb"],
+                           "l2": ("inputs larger than L2 (index %.1f GB, new reads every step)" % setup["index_gb"]
+                                  if n_batches > 1 else "inputs larger than L2 (index %.1f GB, %.0f MB of reads "
+                                  "per step)" % (setup["index_gb"], reads.offs[-1] / 1e6)),
                            "parallelism": f"dp{world}" if world > 1 else "single GPU"},
                 "gcups": gcups(agg), "plain_gpu": plain, "learned_band": band_info,
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,

@@ -205,6 +205,14 @@ int msg_result_device(const msg_ctx* ctx, const msg_aln** aln, const uint32_t** 
  * own work or events against the library's. */
 int msg_ctx_stream(const msg_ctx* ctx, void** stream);
 
+/* Bound the device memory the DP uses for its rectangle storage (default
+ * 16 GiB). No reference counterpart (the reference allocates three
+ * (L+1) x (T+1) double matrices per chain). A batch whose chains need more
+ * (long reads with large flanks) is aligned over consecutive ranges of
+ * chains that fit; a single larger chain gets a range of its own. Results do
+ * not depend on the limit. */
+int msg_ctx_set_scratch_limit(msg_ctx* ctx, int64_t bytes);
+
 /* ---- Seeding that allocates nothing ----
  * No counterpart in the reference: it exists for callers that cannot call
  * cudaMalloc/cudaFree while mapping -- a host application whose GPU memory is

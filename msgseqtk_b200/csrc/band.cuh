@@ -161,9 +161,9 @@ constexpr int kBandedCount = 8;
 constexpr int32_t kNotSmallKey = 1023;
 constexpr int kSmallKeyBits = 10;
 
-__global__ void k_iota(int64_t n, int64_t* __restrict__ v) {
+__global__ void k_iota(int64_t c0, int64_t n, int64_t* __restrict__ v) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i < n) v[i] = i;
+    if (i < n) v[i] = c0 + i;
 }
 
 // Band half-widths per chain and the split into the thread path (chains of
@@ -172,7 +172,7 @@ __global__ void k_iota(int64_t n, int64_t* __restrict__ v) {
 // mode 0: no band; 1: fixed_w for every larger chain; 2: the classifier's
 // choice for larger chains with a flank that a band of half-width 7 would cut.
 // Each flank is banded only when bandable().
-__global__ void __launch_bounds__(128) k_band_assign(int64_t n_chain, const int4* __restrict__ geo,
+__global__ void __launch_bounds__(128) k_band_assign(int64_t c0, int64_t n_chain, const int4* __restrict__ geo,
                                                      const int64_t* __restrict__ area, const float* __restrict__ feat,
                                                      int mode, int fixed_w, const __nv_bfloat16* __restrict__ wts,
                                                      const float* __restrict__ nrm, int8_t* __restrict__ band,
@@ -187,8 +187,9 @@ __global__ void __launch_bounds__(128) k_band_assign(int64_t n_chain, const int4
         for (int k = threadIdx.x; k < 2 * kFeat; k += blockDim.x) sN[k] = nrm[k];
         __syncthreads();
     }
-    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (c >= n_chain) return;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // chains c0 .. c0 + n_chain
+    if (t >= n_chain) return;
+    const int64_t c = c0 + t;
     const int4 g = geo[c];
     int w = -1;
     if (area[c] > kSmallArea) {  // small chains stay on the thread path, whole rectangles
@@ -201,7 +202,7 @@ __global__ void __launch_bounds__(128) k_band_assign(int64_t n_chain, const int4
     band[2 * c] = (int8_t)w5;
     band[2 * c + 1] = (int8_t)w3;
     const bool is_small = w5 < 0 && w3 < 0 && area[c] <= kSmallArea;
-    if (small_key) small_key[c] = is_small ? (int32_t)area[c] : kNotSmallKey;
+    if (small_key) small_key[t] = is_small ? (int32_t)area[c] : kNotSmallKey;
     if (w5 >= 0 || w3 >= 0) banded[atomicAdd(&counts[kBandedCount], 1ull)] = c;
     else if (is_small) {
         const unsigned long long k = atomicAdd(&counts[0], 1ull);

@@ -530,12 +530,35 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     CK(offsets(ctx, d_cells, h_nchain, d_rect_off, misc, &h_cells));  // d_cells holds bytes per chain
     CK(offsets(ctx, d_pcap, h_nchain, d_path_off, misc, &h_pathtot));
     const int64_t aux_bytes = ((2 * (h_nidx + 1) + h_nchain + 1) * sizeof(int32_t) + 15) / 16 * 16;
-    CK(ctx->scratch.ensure(h_cells + 64 + aux_bytes + (2 * h_nidx + h_nchain + 1) * sizeof(int4)));
+    // Rectangle storage of at most scratch_limit bytes at a time: when the
+    // batch needs more (long reads with large flanks), the DP runs over
+    // consecutive ranges of chains that fit (a single larger chain alone).
+    const int64_t kScratchBudget = ctx->scratch_limit;
+    std::vector<int64_t> bounds{0, h_nchain};
+    int64_t rect_cap = h_cells;
+    if (h_cells > kScratchBudget && h_nchain > 0) {
+        std::vector<int64_t> ro(h_nchain + 1);
+        CK(cudaMemcpy(ro.data(), d_rect_off, (h_nchain + 1) * 8, cudaMemcpyDeviceToHost));
+        bounds.assign(1, 0);
+        rect_cap = 0;
+        int64_t c0 = 0;
+        for (int64_t c = 1; c <= h_nchain; ++c) {
+            if (c == h_nchain || (ro[c + 1] - ro[c0] > kScratchBudget && c > c0)) {
+                bounds.push_back(c);
+                rect_cap = std::max(rect_cap, ro[c] - ro[c0]);
+                c0 = c;
+            }
+        }
+    }
+    CK(ctx->scratch.ensure(rect_cap + 64 + aux_bytes + (2 * h_nidx + h_nchain + 1) * sizeof(int4)));
+    std::vector<int64_t> h_rect_off(bounds.size());
+    for (size_t b = 0; b < bounds.size(); ++b)
+        CK(cudaMemcpy(&h_rect_off[b], d_rect_off + bounds[b], 8, cudaMemcpyDeviceToHost));
     const int64_t P16 = ((h_pathtot + 1 + 15) / 16) * 16;
     CK(ctx->path.ensure(P16 + (h_nchain + 1) * 4 + 64));
     CK(ctx->alnbuf.ensure((h_nchain + 1) * sizeof(msg_aln)));
     uint8_t* d_scr = ctx->scratch.as<uint8_t>();
-    int32_t* d_aux = reinterpret_cast<int32_t*>(d_scr + (h_cells + 64) / 16 * 16);
+    int32_t* d_aux = reinterpret_cast<int32_t*>(d_scr + (rect_cap + 64) / 16 * 16);
     int4* d_sdbuf = reinterpret_cast<int4*>(reinterpret_cast<uint8_t*>(d_aux) + aux_bytes);
     uint8_t* d_path = ctx->path.as<uint8_t>();
     int32_t* d_plen = reinterpret_cast<int32_t*>(d_path + P16);
@@ -554,6 +577,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
 
     if (collect) {
         // Certificate of every banded class on every chain; cost per class in cells.
+        if (bounds.size() > 2) return ctx->fail(MSG_EINVAL, "batch too large for one collection; split it");
         if (collect->cap < h_nchain) { *collect->n_chain = h_nchain; return ctx->fail(MSG_EINVAL, "capacity too small"); }
         *collect->n_chain = h_nchain;
         if (h_nchain == 0) return MSG_OK;
@@ -571,7 +595,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             CK(cudaMemsetAsync(d_ctr2, 0, 128, st));
             CK(cudaMemsetAsync(d_probe, 3, h_nchain, st));  // 3: not banded at this class
             CK(cudaMemcpyAsync(d_pcells, d_area, h_nchain * 8, cudaMemcpyDeviceToDevice, st));
-            S.n_launch++, k_band_assign<<<nblk(h_nchain, 128), 128, 0, st>>>(h_nchain, d_geo, d_area, d_feat, 1, band_width(cls),
+            S.n_launch++, k_band_assign<<<nblk(h_nchain, 128), 128, 0, st>>>(0, h_nchain, d_geo, d_area, d_feat, 1, band_width(cls),
                                                                 nullptr, nullptr, d_band, d_small, d_big, d_bandl, d_ctr2,
                                                                 nullptr);
             da.list = d_bandl; da.n_list = d_ctr2 + kBandedCount;
@@ -597,40 +621,53 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     }
 
     const bool filtering = params->min_score_rate >= 0;
-    if (h_nchain > 0) {
-        CK(cudaMemsetAsync(d_ctr2, 0, 128, st));
+    if (h_nchain > 0) CK(cudaMemsetAsync(d_ctr2, 0, 128, st));
+    for (size_t ch = 0; ch + 1 < bounds.size(); ++ch) {
+        const int64_t c0 = bounds[ch], nch = bounds[ch + 1] - bounds[ch];
+        if (nch <= 0) continue;
+        if (ch > 0) {  // list counters start again; the band statistics accumulate
+            CK(cudaMemsetAsync(d_ctr2, 0, 3 * 8, st));
+            CK(cudaMemsetAsync(d_ctr2 + kBandedCount, 0, 2 * 8, st));
+        }
+        da.scr_base = h_rect_off[ch];
+        da.band = d_band;
         const int bmode = dpp.mode != 0 ? 0 : params->band_mode;
         // thread-path list sorted by cell count (keys and values staged in the
         // fallback and kept-index arrays, which are not in use yet)
         int32_t* d_key = reinterpret_cast<int32_t*>(d_fb);
         int32_t* d_key2 = d_key + NC;
-        S.n_launch++, k_band_assign<<<nblk(h_nchain, 128), 128, 0, st>>>(h_nchain, d_geo, d_area, d_feat, bmode, params->band_w,
-                                                            d_wts, d_nrm, d_band, d_small, d_big, d_bandl, d_ctr2,
-                                                            d_key);
-        S.n_launch++, k_iota<<<nblk(h_nchain, 256), 256, 0, st>>>(h_nchain, d_kidx);
+        S.n_launch++, k_band_assign<<<nblk(nch, 128), 128, 0, st>>>(c0, nch, d_geo, d_area, d_feat, bmode,
+                                                                     params->band_w, d_wts, d_nrm, d_band, d_small,
+                                                                     d_big, d_bandl, d_ctr2, d_key);
+        S.n_launch++, k_iota<<<nblk(nch, 256), 256, 0, st>>>(c0, nch, d_kidx);
         {
             size_t tb = 0;
-            CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, d_key, d_key2, d_kidx, d_small, (int)h_nchain, 0,
+            CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, d_key, d_key2, d_kidx, d_small, (int)nch, 0,
                                                kSmallKeyBits, st));
             CK(misc.ensure(tb));
-            CK(cub::DeviceRadixSort::SortPairs(misc.p, tb, d_key, d_key2, d_kidx, d_small, (int)h_nchain, 0,
+            CK(cub::DeviceRadixSort::SortPairs(misc.p, tb, d_key, d_key2, d_kidx, d_small, (int)nch, 0,
                                                kSmallKeyBits, st));
         }
-        // Every launch is sized for every chain; each reads its list length on
-        // the device, so no host round trip is needed for the split.
+        // Every launch is sized for every chain of the range; each reads its
+        // list length on the device, so no host round trip is needed.
         da.list = d_small; da.n_list = d_ctr2;
-        S.n_launch++, k_dp_small<<<nblk(h_nchain, 128), 128, 0, st>>>(da);
+        S.n_launch++, k_dp_small<<<nblk(nch, 128), 128, 0, st>>>(da);
         da.list = d_big; da.n_list = d_ctr2 + 1;
-        S.n_launch++, k_dp<false><<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
+        S.n_launch++, k_dp<false><<<nblk(nch * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
         if (bmode != 0) {
             da.list = d_bandl; da.n_list = d_ctr2 + kBandedCount;
-            S.n_launch++, k_dp<true><<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
+            S.n_launch++, k_dp<true><<<nblk(nch * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
             // banded chains without a certificate, on the whole cell set
             da.list = d_fb; da.n_list = d_ctr2 + 2; da.band = nullptr;
-            S.n_launch++, k_dp<false><<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
+            S.n_launch++, k_dp<false><<<nblk(nch * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
         }
-        S.n_launch++, k_traceback<<<nblk(h_nchain, 128), 128, 0, st>>>(da);
+        S.n_launch++, k_traceback<<<nblk(nch, 128), 128, 0, st>>>(da);
         CK(cudaGetLastError());
+        if (bounds.size() > 2) {  // warp-path chains of this range, for the statistics
+            unsigned long long w[kBandedCount + 1];
+            CK(cudaMemcpy(w, d_ctr2, sizeof(w), cudaMemcpyDeviceToHost));
+            S.n_dp_warp += (int64_t)(w[1] + w[kBandedCount]);
+        }
     }
     tm.mark();  // 4
     // Alignment::filter on the device: compact the kept records.
@@ -679,7 +716,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     S.n_band_drop = (int64_t)h_bstat[2];
     S.dp_cells_done = (int64_t)(h_bstat[3] + h_bstat[4]);
     S.n_filtered = h_nchain - h_nrec;
-    S.n_dp_warp = (int64_t)(h_ctr2[1] + h_ctr2[kBandedCount]);
+    if (bounds.size() <= 2) S.n_dp_warp = (int64_t)(h_ctr2[1] + h_ctr2[kBandedCount]);
     S.ms_smem = tm.ms(0, 1);
     S.ms_locate = tm.ms(1, 2);
     S.ms_chain = tm.ms(2, 3);
@@ -967,6 +1004,12 @@ extern "C" int msg_result_device(const msg_ctx* ctx, const msg_aln** aln, const 
     if (aln) *aln = ctx->res_aln;
     if (cigar) *cigar = ctx->res_cigar;
     if (read_aln_off) *read_aln_off = ctx->res_off;
+    return MSG_OK;
+}
+
+extern "C" int msg_ctx_set_scratch_limit(msg_ctx* ctx, int64_t bytes) {
+    if (!ctx || bytes <= 0) return MSG_EINVAL;
+    ctx->scratch_limit = bytes;
     return MSG_OK;
 }
 

@@ -1035,8 +1035,9 @@ struct DpArgs {
     const int64_t* roff;
     const int64_t* t_start;
     const int64_t* t_end;
-    const int64_t* scr_off;     // per chain, bytes of rectangle storage
-    uint8_t* scr;
+    const int64_t* scr_off;     // per chain, byte offset of its rectangle storage
+    uint8_t* scr;               // rectangle storage of the chains of this launch
+    int64_t scr_base;           // scr_off of the first chain of this launch
     int32_t* aux;               // per chain at 2 * chain_idx_off + chain index: diag (n) and rect offsets (n + 1)
     int4* sdbuf;                // per chain seed geometry when n > kSmemSeeds (at chain_idx_off)
     const int64_t* path_off;    // per chain, capacity L + tLen + 1
@@ -1218,7 +1219,7 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
     const int64_t chr_len = a.ix.chr_len[f.tid];
     x.target = a.ix.chr_seq + a.ix.chr_off[f.tid] + t_start;
     x.target_avail = chr_len - t_start;
-    x.scratch = a.scr + a.scr_off[c];
+    x.scratch = a.scr + (a.scr_off[c] - a.scr_base);
     int32_t* aux = a.aux + 2 * a.chain_idx_off[c] + c;
     x.diag = aux;
     x.roff = aux + x.n;
@@ -1494,7 +1495,7 @@ __global__ void __launch_bounds__(128, 6) k_traceback(DpArgs a) {
     const Seed f = a.seeds[idx[0]];
     x.target = a.ix.chr_seq + a.ix.chr_off[f.tid] + t_start;
     x.target_avail = a.ix.chr_len[f.tid] - t_start;
-    x.scratch = a.scr + a.scr_off[c];
+    x.scratch = a.scr + (a.scr_off[c] - a.scr_base);
     int32_t* aux = a.aux + 2 * a.chain_idx_off[c] + c;
     x.diag = aux;
     x.roff = aux + x.n;

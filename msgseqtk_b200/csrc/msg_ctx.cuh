@@ -60,6 +60,7 @@ struct msg_ctx {
     // band model (bf16 weights, fp32 feature mean/scale) and training buffers
     msg::DevBuf band_wts, band_nrm, tr_x, tr_y, tr_ord, tr_w, tr_m, tr_v, tr_g, tr_loss;
     bool band_loaded = false;
+    int64_t scratch_limit = 16ll << 30;  // DP rectangle storage per pass (msg_ctx_set_scratch_limit)
     cudaEvent_t ev[8];
     const msg_aln* res_aln = nullptr;
     const uint32_t* res_cigar = nullptr;

@@ -28,7 +28,7 @@ assert ALN_DTYPE.itemsize == 88
 # symbols of the C ABI, in include/msg_b200.h order
 EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy", "msg_index_load", "msg_index_bytes",
            "msg_map_params_default", "msg_map_batch", "msg_map_batch_device", "msg_last_stats", "msg_occ_query",
-           "msg_result_device", "msg_ctx_stream", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
+           "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
            "msg_band_train", "msg_band_grad", "msg_bi_ext_query", "msg_sa_query"]
 
 # band model (include/msg_b200.h)
@@ -114,6 +114,7 @@ def load_library(path: str = LIB_PATH):
     L.msg_last_stats.argtypes = [C.c_void_p, C.POINTER(MapStats)]
     L.msg_result_device.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     L.msg_ctx_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    L.msg_ctx_set_scratch_limit.argtypes = [C.c_void_p, C.c_int64]
     L.msg_smem_batch_noalloc.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(MapParams),
                                          C.c_void_p, C.c_int64, C.c_void_p]
     f32p = C.POINTER(C.c_float)
@@ -335,6 +336,9 @@ class Context:
                                            _p(label, C.POINTER(C.c_int32)), len(label),
                                            _p(grad, C.POINTER(C.c_float)), C.byref(loss)), "msg_band_grad")
         return grad, loss.value
+
+    def set_scratch_limit(self, nbytes: int):
+        self._check(self.lib.msg_ctx_set_scratch_limit(self.h, int(nbytes)), "msg_ctx_set_scratch_limit")
 
     def stats(self) -> dict:
         s = MapStats()

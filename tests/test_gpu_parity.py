@@ -205,3 +205,27 @@ def test_uneven_lengths_match_oracle(ctx, oracle_built):
                                   e["aln_start"], e["aln_end"]], i
             assert words == e["cigar"], i
     assert n_kept > 0
+
+
+def test_scratch_limit_gives_same_records(oracle_built):
+    """With the DP's rectangle storage capped far below the batch's need, the
+    chains are aligned range by range; the records are unchanged."""
+    g = synth.small_genomes(seed=71, n_genomes=3, length=80_000)
+    view = index_build.build_view(g)
+    c = lib.Context(0)
+    try:
+        c.load_index(view)
+        rs = synth.sample_reads(g, 600, seed=72, sub_rate=0.035, indel_rate=0.015)
+        rng = np.random.default_rng(73)
+        rand = synth._BASES[rng.integers(0, 4, 150 * 60)]
+        seq = np.concatenate([rs.seqs, rand]).astype(np.uint8)
+        off = np.concatenate([rs.offs, rs.offs[-1] + 150 * np.arange(1, 61)]).astype(np.int64)
+        for params in (lib.default_params(min_len=12), lib.default_params(min_score_rate=0.65, band_mode=1, band_w=7)):
+            full = c.map(seq, off, params)
+            c.set_scratch_limit(1 << 16)
+            part = c.map(seq, off, params)
+            c.set_scratch_limit(16 << 30)
+            for k in ("aln", "cigar", "read_aln_off"):
+                assert np.array_equal(full[k], part[k]), k
+    finally:
+        c.close()
