@@ -978,24 +978,48 @@ struct ChainCtx {
             int32_t pm = NEG, pi = NEG, pd = NEG;       // this lane's output of the previous step
             int32_t um = NEG, ui = NEG, ud = NEG;       // up neighbour (i-1, j) of the current step
             int32_t dm = md0, di = id0, dd = dd0;       // diagonal neighbour (i-1, j-1)
+            int tcur = 0;                               // target base of this lane's column
             uint8_t* code_base = g.code + sp * (g.C + 31) * 32;
-            const int64_t rows_here = min((int64_t)32, g.R - sp * 32);  // the last lane with a row
-            for (int64_t t = 0; t < g.C + rows_here - 1; ++t) {
-                const int64_t c = t - lane;
+            const int rows_here = (int)min((int64_t)32, g.R - sp * 32);  // the last lane with a row
+            const int C = (int)g.C;
+            // Lane 0's inputs for the next 32 steps (the row above from rowbuf,
+            // the target bases of columns t .. t+31) are loaded together, one
+            // column per lane, and handed to lane 0 by shuffles; the other lanes
+            // take theirs from the lane before.
+            int32_t pre_m = NEG, pre_i = NEG, pre_d = NEG;
+            int pre_t = 0;
+            for (int t = 0; t < C + rows_here - 1; ++t) {
+                if ((t & 31) == 0) {
+                    const int cc = t + lane;
+                    pre_m = pre_i = pre_d = NEG;
+                    pre_t = 0;
+                    if (cc < C) {
+                        pre_m = g.rowbuf[cc * 3]; pre_i = g.rowbuf[cc * 3 + 1]; pre_d = g.rowbuf[cc * 3 + 2];
+                        pre_t = tb(g.c0 + cc);
+                    }
+                }
+                const int c = t - lane;
                 const int32_t sm_ = __shfl_up_sync(0xffffffffu, pm, 1);
                 const int32_t si_ = __shfl_up_sync(0xffffffffu, pi, 1);
                 const int32_t sd_ = __shfl_up_sync(0xffffffffu, pd, 1);
-                const bool act = row_ok && c >= 0 && c < g.C;
+                const int st_ = __shfl_up_sync(0xffffffffu, tcur, 1);
+                const int32_t r_m = __shfl_sync(0xffffffffu, pre_m, t & 31);
+                const int32_t r_i = __shfl_sync(0xffffffffu, pre_i, t & 31);
+                const int32_t r_d = __shfl_sync(0xffffffffu, pre_d, t & 31);
+                const int r_t = __shfl_sync(0xffffffffu, pre_t, t & 31);
+                const bool act = row_ok && c >= 0 && c < C;
                 if (lane == 0) {
-                    if (act) { um = g.rowbuf[c * 3]; ui = g.rowbuf[c * 3 + 1]; ud = g.rowbuf[c * 3 + 2]; }
+                    if (act) { um = r_m; ui = r_i; ud = r_d; }
+                    tcur = r_t;
                 } else {
                     um = sm_; ui = si_; ud = sd_;
+                    tcur = st_;
                 }
                 if (act) {
                     const int64_t j = g.c0 + 1 + c;
                     const int32_t lm = c == 0 ? ml : pm;
                     const int32_t ld = c == 0 ? dl : pd;
-                    const int s = score(qb, tb(j - 1));
+                    const int s = score(qb, tcur);
                     const int32_t mx = max(max(dm, dd), di);
                     int32_t mv = add_s(mx, s);
                     if (pp.mode == 1) mv = max(mv, 0);
@@ -1007,7 +1031,7 @@ struct ChainCtx {
                                                    ((b1 > b2) ? 8 : 0) | (mv > 0 ? 16 : 0));
                     code_base[(c + lane) * 32 + lane] = code;
                     if (rr == g.R - 1) { g.lastrow[c * 3] = mv; g.lastrow[c * 3 + 1] = iv; g.lastrow[c * 3 + 2] = dv; }
-                    if (c == g.C - 1) { g.lastcol[rr * 3] = mv; g.lastcol[rr * 3 + 1] = iv; g.lastcol[rr * 3 + 2] = dv; }
+                    if (c == C - 1) { g.lastcol[rr * 3] = mv; g.lastcol[rr * 3 + 1] = iv; g.lastcol[rr * 3 + 2] = dv; }
                     if (lane == 31) { g.rowbuf[c * 3] = mv; g.rowbuf[c * 3 + 1] = iv; g.rowbuf[c * 3 + 2] = dv; }
                     if (pp.mode == 1) {
                         const int64_t key = j * (L + 1) + i;
