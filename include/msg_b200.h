@@ -76,6 +76,20 @@ typedef struct msg_mtg_view {
  * on the device from the SA samples), and the chromosome table. */
 int msg_index_load(msg_ctx* ctx, const msg_fmd_view* fmd, const msg_mtg_view* mtg);
 
+/* ---- Database files ----
+ * Read a database as msgseqtk-build writes it (src/msgseqtk-build.cpp:382-426):
+ * the MetaGenome (.mtg, MetaGenome::save), its sequences (.mgs,
+ * MetaGenome::saveSeq) and the FMD-index (.fmd, FMDIndex::save, whose BWT is
+ * an RRR-compressed wavelet tree). The BWT is decoded on n_threads host
+ * threads. Replaces MetaGenome::load/loadSeq + FMDIndex::load
+ * (src/msgseqtk-align.cpp:444-508) for callers without the reference's
+ * libraries. msg_db_views then gives the views msg_index_load takes (valid
+ * until msg_db_free). MSG_EINVAL for unreadable or inconsistent files. */
+typedef struct msg_db msg_db;
+int msg_db_read(const char* mtg_path, const char* mgs_path, const char* fmd_path, int n_threads, msg_db** db);
+int msg_db_views(const msg_db* db, msg_fmd_view* fmd, msg_mtg_view* mtg);
+void msg_db_free(msg_db* db);
+
 /* Device bytes held by the loaded index. */
 int msg_index_bytes(const msg_ctx* ctx, int64_t* bytes);
 

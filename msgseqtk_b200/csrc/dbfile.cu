@@ -1,0 +1,391 @@
+// Reading a database written by msgseqtk-build (src/msgseqtk-build.cpp:382-426)
+// into the host views msg_index_load takes: the MetaGenome (.mtg) and its
+// sequences (.mgs), and the FMD-index (.fmd) whose BWT is stored as a wavelet
+// tree of RRR-compressed bit sequences (libsds).
+//
+// File formats (all little-endian, as written by the reference on x86-64):
+//   program header (.mtg, .fmd; ProgEnv.cpp:24-28): the 8 characters
+//     "MSGseqTK", then three int32 version numbers (VersionSequence::save).
+//   MetaGenome::save (MetaGenome.cpp:42-49): size_t #genomes; per genome
+//     (Genome.cpp:66-74) id and name as size_t length + bytes, size_t
+//     #chromosomes; per chromosome (Genome.cpp:23-27) name as length + bytes
+//     and int64 length.
+//   MetaGenome::saveSeq (.mgs, no header; Genome.cpp:29-32): per chromosome
+//     its nt16 codes and one terminating 0.
+//   FMDIndex::save (FMDIndex.cpp:142-150): int64 B[256], int64 C[256], the
+//     wavelet tree, gapSA (size_t length + int64s), SAidx (an RRR bit
+//     sequence marking sampled rows), SAsampled (size_t length + int64s).
+//   WaveletTreeRRR::save (WaveletTreeRRR.cpp:14-29): size_t n, sigma,
+//     height, wid, min, max, sample_rate, #OCC, OCC[#OCC], then `height`
+//     RRR bit sequences, level 0 holding the symbols' top bit.
+//   BitSeqRRR::save (BitSeqRRR.cpp:308-333): size_t n, ones; BitStr32 C
+//     (4-bit block classes); BitStr32 O (variable-width block offsets);
+//     size_t nC, wC, nO, wO; BitStr64 Csampled, Osampled; size_t nCsampled,
+//     wCsampled, nOsampled, wOsampled, sample_rate.
+//   BitStr::save (BitStr.h:386-392): the word width (a 32-bit field written
+//     as 8 bytes, the upper 4 undefined), bit length and word count as size_t,
+//     then the words; bits are numbered from the least significant bit of
+//     word 0.
+//
+// An RRR block of 15 bits is stored as its class k (popcount) and its offset
+// among the k-subsets of {0..14} listed in lexicographic order of their
+// positions (the table BitSeqRRR::TableOffset builds); the offset takes
+// bits(C(15, k) - 1) bits. Decoding unranks it. The wavelet tree is decoded
+// with the same walk as WaveletTreeRRR::access (WaveletTreeRRR.cpp:58-76)
+// over plain bit vectors with a rank directory, on several host threads.
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/msg_b200.h"
+
+struct msg_db {
+    // FMD-index view data
+    std::vector<uint8_t> bwt;
+    int64_t base_count[16] = {0};
+    std::vector<int64_t> sample_rows, sample_vals;
+    // MetaGenome view data
+    std::vector<int64_t> bd_start, bd_end, chr_len, chr_off;
+    std::vector<uint8_t> chr_seq;
+    std::vector<std::string> chr_names;
+};
+
+namespace {
+
+struct Reader {
+    std::ifstream in;
+    bool ok = true;
+    explicit Reader(const char* path) : in(path, std::ios::binary) { ok = (bool)in; }
+    template <typename T> T get() {
+        T v{};
+        if (ok) { in.read(reinterpret_cast<char*>(&v), sizeof(T)); ok = (bool)in; }
+        return v;
+    }
+    void bytes(void* p, size_t n) {
+        if (ok && n) { in.read(reinterpret_cast<char*>(p), (std::streamsize)n); ok = (bool)in; }
+    }
+    std::string str() {  // size_t length + bytes
+        const uint64_t n = get<uint64_t>();
+        if (!ok || n > (1u << 20)) { ok = false; return std::string(); }
+        std::string s(n, '\0');
+        bytes(&s[0], n);
+        return s;
+    }
+    bool header() {  // saveProgInfo
+        char name[8];
+        bytes(name, 8);
+        get<int32_t>(); get<int32_t>(); get<int32_t>();
+        return ok && std::memcmp(name, "MSGseqTK", 8) == 0;
+    }
+};
+
+// A libsds BitStr: words of `wid` bits, bits numbered from bit 0 of word 0.
+struct Bits {
+    uint64_t wid = 0, nbits = 0;
+    std::vector<uint64_t> w;  // words widened to 64 bits when wid == 32
+    bool read(Reader& r, uint64_t want_wid) {
+        // BitStr::save writes its 32-bit word width with sizeof(size_t) bytes:
+        // only the low 4 are the value
+        wid = r.get<uint64_t>() & 0xffffffffull;
+        nbits = r.get<uint64_t>();
+        const uint64_t n = r.get<uint64_t>();
+        if (!r.ok || wid != want_wid || n > (nbits / wid) + 2 || n * wid < nbits) return false;
+        if (wid == 64) {
+            w.resize(n);
+            r.bytes(w.data(), n * 8);
+        } else {
+            std::vector<uint32_t> t(n);
+            r.bytes(t.data(), n * 4);
+            w.resize((n + 1) / 2, 0);
+            for (uint64_t k = 0; k < n; ++k) w[k / 2] |= (uint64_t)t[k] << (32 * (k % 2));
+        }
+        return r.ok;
+    }
+    // bits [start, start + len), len <= 57
+    uint64_t get(uint64_t start, int len) const {
+        if (len == 0) return 0;
+        const uint64_t i = start >> 6;
+        const int j = (int)(start & 63);
+        uint64_t v = w[i] >> j;
+        if (j + len > 64 && i + 1 < w.size()) v |= w[i + 1] << (64 - j);
+        return len >= 64 ? v : (v & ((1ull << len) - 1));
+    }
+};
+
+int nbits_of(uint64_t x) { int b = 0; for (; x; x >>= 1) ++b; return b; }
+
+struct Rrr {
+    uint32_t binom[16][16];
+    int offbits[16];
+    Rrr() {
+        for (int i = 0; i < 16; ++i)
+            for (int j = 0; j < 16; ++j) binom[i][j] = (j == 0 || j == i) ? 1 : (j > i ? 0 : 0);
+        for (int i = 1; i < 16; ++i)
+            for (int j = 1; j < i; ++j) binom[i][j] = binom[i - 1][j - 1] + binom[i - 1][j];
+        for (int k = 0; k < 16; ++k) offbits[k] = nbits_of(binom[15][k] - 1);
+    }
+    // the offset-th k-subset of {0..14} in lexicographic order, as a bitmap
+    uint32_t unrank(int k, uint64_t off) const {
+        if (k == 0) return 0;
+        if (k == 15) return 0x7fff;
+        uint32_t v = 0;
+        int r = k;
+        for (int i = 0; i < 15 && r > 0; ++i) {
+            const uint32_t cnt = binom[14 - i][r - 1];  // subsets whose next element is i
+            if (off < cnt) { v |= 1u << i; --r; }
+            else off -= cnt;
+        }
+        return v;
+    }
+};
+
+// A decoded RRR bit sequence: plain bits and a rank directory (ones before
+// each 64-bit word).
+struct Plain {
+    uint64_t n = 0, ones = 0;
+    std::vector<uint64_t> w;
+    std::vector<uint64_t> dir;
+    bool bit(uint64_t i) const { return (w[i >> 6] >> (i & 63)) & 1; }
+    uint64_t rank1(uint64_t i) const {  // ones in [0, i]
+        const uint64_t k = i >> 6;
+        const int r = (int)(i & 63);
+        const uint64_t m = r == 63 ? ~0ull : ((2ull << r) - 1);
+        return dir[k] + (uint64_t)__builtin_popcountll(w[k] & m);
+    }
+};
+
+bool read_rrr(Reader& r, const Rrr& tab, Plain& out) {
+    out.n = r.get<uint64_t>();
+    out.ones = r.get<uint64_t>();
+    Bits C, O, Cs, Os;
+    if (!C.read(r, 32) || !O.read(r, 32)) return false;
+    const uint64_t nC = r.get<uint64_t>(), wC = r.get<uint64_t>(), nO = r.get<uint64_t>(), wO = r.get<uint64_t>();
+    if (!Cs.read(r, 64) || !Os.read(r, 64)) return false;
+    for (int k = 0; k < 5; ++k) r.get<uint64_t>();  // nCsampled, wCsampled, nOsampled, wOsampled, sample_rate
+    if (!r.ok || wC != 4 || wO != 1 || nC != (out.n + 14) / 15 || O.nbits < nO) return false;
+    out.w.assign((out.n + 63) / 64 + 1, 0);
+    uint64_t pos = 0, ones = 0;
+    for (uint64_t b = 0; b < nC; ++b) {
+        const int k = (int)C.get(b * 4, 4);
+        if (k > 15) return false;
+        const int len = tab.offbits[k];
+        if (pos + len > O.nbits) return false;
+        const uint32_t v = tab.unrank(k, O.get(pos, len));
+        pos += len;
+        ones += (uint64_t)k;
+        const uint64_t s = b * 15;  // block b holds bits s .. s+14
+        const uint64_t i = s >> 6;
+        const int j = (int)(s & 63);
+        out.w[i] |= (uint64_t)v << j;
+        if (j > 49 && i + 1 < out.w.size()) out.w[i + 1] |= (uint64_t)v >> (64 - j);
+    }
+    if (ones != out.ones) return false;
+    if (out.n % 64) out.w[out.n / 64] &= (1ull << (out.n % 64)) - 1;  // bits past n are not part of the sequence
+    out.dir.resize(out.w.size() + 1);
+    uint64_t acc = 0;
+    for (size_t k = 0; k < out.w.size(); ++k) { out.dir[k] = acc; acc += (uint64_t)__builtin_popcountll(out.w[k]); }
+    out.dir[out.w.size()] = acc;
+    return acc == out.ones;
+}
+
+bool read_i64s(Reader& r, std::vector<int64_t>& v) {
+    const uint64_t n = r.get<uint64_t>();
+    if (!r.ok || n > (1ull << 36)) return false;
+    v.resize(n);
+    r.bytes(v.data(), n * 8);
+    return r.ok;
+}
+
+bool read_fmd(const char* path, int n_threads, msg_db& db) {
+    Reader r(path);
+    if (!r.ok || !r.header()) return false;
+    int64_t B[256], C[256];
+    r.bytes(B, sizeof(B));
+    r.bytes(C, sizeof(C));
+    // wavelet tree
+    const uint64_t n = r.get<uint64_t>();
+    r.get<uint64_t>();  // sigma
+    const uint64_t height = r.get<uint64_t>();
+    r.get<uint64_t>();  // wid
+    r.get<uint64_t>();  // min
+    r.get<uint64_t>();  // max
+    r.get<uint64_t>();  // sample_rate
+    const uint64_t nocc = r.get<uint64_t>();
+    if (!r.ok || height == 0 || height > 8 || nocc > 1024) return false;
+    std::vector<uint64_t> occ(nocc);
+    r.bytes(occ.data(), nocc * 8);
+    const Rrr tab;
+    std::vector<Plain> lv(height);
+    for (uint64_t l = 0; l < height; ++l)
+        if (!read_rrr(r, tab, lv[l]) || lv[l].n != n) return false;
+    std::vector<int64_t> gap_sa, sa_sampled;
+    Plain saidx;
+    if (!read_i64s(r, gap_sa) || !read_rrr(r, tab, saidx) || !read_i64s(r, sa_sampled)) return false;
+    if (saidx.n != n || (saidx.ones != sa_sampled.size() && saidx.ones != sa_sampled.size() + 1)) return false;
+    for (int b = 0; b < 16; ++b) db.base_count[b] = B[b];
+    // BWT symbols: the walk of WaveletTreeRRR::access per row
+    db.bwt.resize(n);
+    bool bad = false;
+    auto decode = [&](uint64_t lo, uint64_t hi) {
+        for (uint64_t row = lo; row < hi; ++row) {
+            uint64_t s = 0, start = 0, i = row;
+            for (uint64_t l = 0; l < height; ++l) {
+                const Plain& p = lv[l];
+                const uint64_t before = start > 0 ? p.rank1(start - 1) : 0;
+                const uint64_t r1 = p.rank1(i);
+                if (p.bit(i)) {
+                    s |= 1ull << (height - l - 1);
+                    if (s >= occ.size()) { bad = true; return; }
+                    start = occ[s];
+                    i = r1 - 1 - before + start;
+                } else {
+                    i = (i + 1 - r1) - 1 + before;
+                }
+                if (i >= n) { bad = true; return; }
+            }
+            db.bwt[row] = (uint8_t)s;
+        }
+    };
+    const int nt = std::max(1, n_threads);
+    std::vector<std::thread> th;
+    const uint64_t chunk = (n + nt - 1) / nt;
+    for (int t = 0; t < nt; ++t) {
+        const uint64_t lo = std::min<uint64_t>(n, t * chunk), hi = std::min<uint64_t>(n, lo + chunk);
+        th.emplace_back(decode, lo, hi);
+    }
+    for (auto& x : th) x.join();
+    if (bad) return false;
+    // FMDIndex::buildSA sizes SAsampled by SAidx.numOnes() (FMDIndex.cpp:495),
+    // which can be one short of the marked rows; the last sample's value then
+    // lies past the saved array (an index built in memory still holds it; one
+    // loaded from its file reads the string's terminator). Recompute it here
+    // as accessSA would have had it: walk LF from that row to the next
+    // sampled row with a stored value, SA = that value + the distance.
+    if (saidx.ones == sa_sampled.size() + 1) {
+        auto rank = [&](uint64_t sym, uint64_t i) -> uint64_t {  // WaveletTreeRRR::rank (occurrences in [0, i])
+            uint64_t start = 0, r = ~0ull;
+            for (uint64_t l = 0; r != 0 && l < height; ++l) {
+                const Plain& p = lv[l];
+                const uint64_t before = start > 0 ? p.rank1(start - 1) : 0;
+                if ((sym >> (height - l - 1)) & 1) {
+                    const uint64_t masked = (sym >> (height - l - 1)) << (height - l - 1);
+                    r = p.rank1(i) - before;
+                    if (masked >= occ.size()) return 0;
+                    start = occ[masked];
+                } else {
+                    r = i - start + before - p.rank1(i) + 1;
+                }
+                if (r == 0) return 0;
+                i = r + start - 1;
+            }
+            return r;
+        };
+        uint64_t j = 0;  // the last marked row
+        for (size_t k = saidx.w.size(); k-- > 0;)
+            if (saidx.w[k]) { j = k * 64 + 63 - (uint64_t)__builtin_clzll(saidx.w[k]); break; }
+        uint64_t i = j;
+        int64_t dist = 0;
+        for (;;) {
+            const uint64_t b = db.bwt[i];
+            if (b == 0 || dist > (int64_t)n) return false;  // a '$' row is always sampled and stored
+            i = (uint64_t)C[b] + rank(b, i) - 1;            // LF(b, i) - 1 (FMDIndex.h:130-141)
+            ++dist;
+            if (saidx.bit(i) && saidx.rank1(i) - 1 < sa_sampled.size()) break;
+        }
+        sa_sampled.push_back(sa_sampled[saidx.rank1(i) - 1] + dist);
+    }
+    // sampled rows: the set bits of SAidx, in order
+    db.sample_rows.clear();
+    db.sample_rows.reserve(saidx.ones);
+    for (size_t k = 0; k < saidx.w.size(); ++k) {
+        uint64_t x = saidx.w[k];
+        while (x) {
+            const int b = __builtin_ctzll(x);
+            db.sample_rows.push_back((int64_t)(k * 64 + b));
+            x &= x - 1;
+        }
+    }
+    db.sample_vals = std::move(sa_sampled);
+    return db.sample_rows.size() == db.sample_vals.size();
+}
+
+bool read_mtg(const char* mtg_path, const char* mgs_path, msg_db& db) {
+    Reader r(mtg_path);
+    if (!r.ok || !r.header()) return false;
+    const uint64_t ng = r.get<uint64_t>();
+    if (!r.ok || ng > (1u << 28)) return false;
+    int64_t bd = 0;
+    for (uint64_t g = 0; g < ng; ++g) {
+        r.str();  // genome id
+        r.str();  // genome name
+        const uint64_t nc = r.get<uint64_t>();
+        if (!r.ok || nc > (1u << 28)) return false;
+        for (uint64_t c = 0; c < nc; ++c) {
+            db.chr_names.push_back(r.str());
+            const int64_t len = r.get<int64_t>();
+            if (!r.ok || len < 0) return false;
+            db.chr_len.push_back(len);
+            db.bd_start.push_back(bd);  // MetaGenome::updateIndex (MetaGenome.cpp:195-213)
+            bd += (len + 1) * 2;
+            db.bd_end.push_back(bd);
+        }
+    }
+    Reader s(mgs_path);
+    if (!s.ok) return false;
+    int64_t total = 0;
+    for (int64_t len : db.chr_len) total += len;
+    db.chr_seq.resize(total);
+    db.chr_off.assign(1, 0);
+    int64_t at = 0;
+    for (int64_t len : db.chr_len) {
+        s.bytes(db.chr_seq.data() + at, len);
+        const uint8_t term = s.get<uint8_t>();
+        if (!s.ok || term != 0) return false;
+        at += len;
+        db.chr_off.push_back(at);
+    }
+    return true;
+}
+
+}  // namespace
+
+extern "C" int msg_db_read(const char* mtg_path, const char* mgs_path, const char* fmd_path, int n_threads,
+                           msg_db** db) {
+    if (!mtg_path || !mgs_path || !fmd_path || !db) return MSG_EINVAL;
+    *db = nullptr;
+    msg_db* d = new (std::nothrow) msg_db();
+    if (!d) return MSG_ENOMEM;
+    try {
+        if (!read_mtg(mtg_path, mgs_path, *d) || !read_fmd(fmd_path, n_threads, *d)) { delete d; return MSG_EINVAL; }
+    } catch (const std::bad_alloc&) {
+        delete d;
+        return MSG_ENOMEM;
+    }
+    const int64_t n = (int64_t)d->bwt.size();
+    if (d->bd_end.empty() || d->bd_end.back() != n) { delete d; return MSG_EINVAL; }
+    *db = d;
+    return MSG_OK;
+}
+
+extern "C" void msg_db_free(msg_db* db) { delete db; }
+
+extern "C" int msg_db_views(const msg_db* db, msg_fmd_view* fmd, msg_mtg_view* mtg) {
+    if (!db || !fmd || !mtg) return MSG_EINVAL;
+    fmd->n = (int64_t)db->bwt.size();
+    fmd->bwt = db->bwt.data();
+    fmd->base_count = db->base_count;
+    fmd->n_samples = (int64_t)db->sample_rows.size();
+    fmd->sample_rows = db->sample_rows.data();
+    fmd->sample_vals = db->sample_vals.data();
+    mtg->n_chrom = (int64_t)db->chr_len.size();
+    mtg->bd_start = db->bd_start.data();
+    mtg->bd_end = db->bd_end.data();
+    mtg->chr_len = db->chr_len.data();
+    mtg->chr_seq = db->chr_seq.data();
+    mtg->chr_off = db->chr_off.data();
+    return MSG_OK;
+}

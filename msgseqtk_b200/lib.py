@@ -26,7 +26,8 @@ ALN_DTYPE = np.dtype([("read", "<i8"), ("tid", "<i4"), ("strand", "<i4"), ("t_st
 assert ALN_DTYPE.itemsize == 88
 
 # symbols of the C ABI, in include/msg_b200.h order
-EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy", "msg_index_load", "msg_index_bytes",
+EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy", "msg_index_load", "msg_db_read",
+           "msg_db_views", "msg_db_free", "msg_index_bytes",
            "msg_map_params_default", "msg_map_batch", "msg_map_batch_device", "msg_last_stats", "msg_occ_query",
            "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
            "msg_band_train", "msg_band_grad", "msg_bi_ext_query", "msg_sa_query"]
@@ -106,6 +107,10 @@ def load_library(path: str = LIB_PATH):
     L.msg_ctx_destroy.argtypes = [C.c_void_p]
     L.msg_index_load.argtypes = [C.c_void_p, C.POINTER(FmdView), C.POINTER(MtgView)]
     L.msg_index_bytes.argtypes = [C.c_void_p, i64p]
+    L.msg_db_read.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]
+    L.msg_db_views.argtypes = [C.c_void_p, C.POINTER(FmdView), C.POINTER(MtgView)]
+    L.msg_db_free.argtypes = [C.c_void_p]
+    L.msg_db_free.restype = None
     L.msg_map_params_default.argtypes = [C.POINTER(MapParams)]
     L.msg_map_params_default.restype = None
     L.msg_map_batch.argtypes = [C.c_void_p, C.POINTER(ReadBatch), C.POINTER(MapParams), C.POINTER(AlnOut),
@@ -182,6 +187,10 @@ class Context:
         f = FmdView(view.n, _p(k[0], u8p), _p(k[1], i64p), len(k[2]), _p(k[2], i64p), _p(k[3], i64p))
         m = MtgView(len(k[4]), _p(k[4], i64p), _p(k[5], i64p), _p(k[6], i64p), _p(k[7], u8p), _p(k[8], i64p))
         self._check(self.lib.msg_index_load(self.h, C.byref(f), C.byref(m)), "msg_index_load")
+
+    def load_database(self, db: "Database"):
+        """msg_index_load from a database read with msg_db_read."""
+        self._check(self.lib.msg_index_load(self.h, C.byref(db.fmd), C.byref(db.mtg)), "msg_index_load")
 
     def index_bytes(self) -> int:
         b = C.c_int64(0)
@@ -386,3 +395,38 @@ def md_tag(cigar_words, query: np.ndarray, target_at, aln_from: int, aln_start: 
             prev = o
     md.append(str(ln))
     return "".join(md)
+
+
+class Database:
+    """A database read from msgseqtk-build files (msg_db_read): host arrays of
+    the FMD-index and the MetaGenome, as numpy views."""
+
+    def __init__(self, mtg_path, mgs_path, fmd_path, n_threads: int = 8):
+        self.lib = load_library()
+        self.h = C.c_void_p()
+        rc = self.lib.msg_db_read(str(mtg_path).encode(), str(mgs_path).encode(), str(fmd_path).encode(),
+                                  n_threads, C.byref(self.h))
+        if rc != MSG_OK:
+            raise MsgError(rc, "msg_db_read")
+        self.fmd = FmdView()
+        self.mtg = MtgView()
+        self.lib.msg_db_views(self.h, C.byref(self.fmd), C.byref(self.mtg))
+
+    def arrays(self):
+        f, m = self.fmd, self.mtg
+        arr = lambda p, n: np.ctypeslib.as_array(p, shape=(n,)).copy() if n > 0 else np.zeros(0)
+        return dict(bwt=arr(f.bwt, f.n), B=arr(f.base_count, 16), sample_rows=arr(f.sample_rows, f.n_samples),
+                    sample_vals=arr(f.sample_vals, f.n_samples), bd_start=arr(m.bd_start, m.n_chrom),
+                    bd_end=arr(m.bd_end, m.n_chrom), chr_len=arr(m.chr_len, m.n_chrom),
+                    chr_off=arr(m.chr_off, m.n_chrom + 1), chr_seq=arr(m.chr_seq, int(m.chr_off[m.n_chrom])))
+
+    def close(self):
+        if self.h:
+            self.lib.msg_db_free(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

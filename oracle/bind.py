@@ -233,6 +233,8 @@ class Reference:
         L.ref_map_batch.argtypes = [C.c_void_p, C.c_int64, u8p, u8p, i64p, C.c_int64, C.c_double, C.c_int64,
                                     C.c_double, C.c_int, C.POINTER(C.c_double), i64p]
         L.ref_max_threads.restype = C.c_int
+        L.ref_db_save.restype = C.c_int
+        L.ref_db_save.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p]
         L.ref_sam_batch.restype = C.c_int64
         L.ref_sam_batch.argtypes = [C.c_void_p, C.c_int64, u8p, u8p, i64p, C.c_int64, C.c_double, C.c_int64,
                                     C.c_double, C.c_int, C.c_char_p, C.c_int64]
@@ -354,6 +356,12 @@ class Reference:
             if n <= cap and cu.value <= ccap and mu.value <= mcap:
                 return _aln_records(arr, n, cg, md.raw)
             cap, ccap, mcap = max(cap, n) * 2, max(ccap, cu.value) * 2, max(mcap, mu.value) * 2
+
+    def save(self, mtg_path, mgs_path, fmd_path):
+        """Write the DB files as msgseqtk-build does."""
+        rc = self.lib.ref_db_save(self.h, str(mtg_path).encode(), str(mgs_path).encode(), str(fmd_path).encode())
+        if rc != 0:
+            raise RuntimeError(f"ref_db_save failed ({rc})")
 
     @staticmethod
     def _text(fn):

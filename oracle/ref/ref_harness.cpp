@@ -23,6 +23,7 @@
 #include <unordered_set>
 #include <iostream>
 #include <sstream>
+#include <fstream>
 #include <regex>
 #include <limits>
 #include <stdexcept>
@@ -39,6 +40,7 @@
 #include "SMEM.h"
 #include "SeedChain.h"
 #include "Alignment.h"
+#include "ProgEnv.h"
 #undef private
 #undef protected
 
@@ -468,6 +470,22 @@ int64_t ref_sam_from_records(void* h, int64_t n_reads, const uint8_t* reads, con
         sam_read(alns, r, min_score_rate, (uint32_t)max_report, text);
     }
     return put_out(text, out, cap);
+}
+
+/* Write the DB as msgseqtk-build does (src/msgseqtk-build.cpp:382-426):
+ * program header + MetaGenome::save, MetaGenome::saveSeq, program header +
+ * FMDIndex::save. Returns 0 on success. */
+int ref_db_save(void* h, const char* mtg_path, const char* mgs_path, const char* fmd_path) {
+    RefDB* db = (RefDB*)h;
+    std::ofstream mtgOut(mtg_path, std::ios::binary), mgsOut(mgs_path, std::ios::binary),
+        fmdOut(fmd_path, std::ios::binary);
+    if (!mtgOut || !mgsOut || !fmdOut) return 1;
+    EGriceLab::saveProgInfo(mtgOut);
+    db->mtg.save(mtgOut);
+    db->mtg.saveSeq(mgsOut);
+    EGriceLab::saveProgInfo(fmdOut);
+    db->fmd.save(fmdOut);
+    return (mtgOut && mgsOut && fmdOut) ? 0 : 2;
 }
 
 int ref_max_threads(void) {
