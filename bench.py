@@ -52,6 +52,7 @@ WORKLOADS = {
               "5% errors (70% substitutions, 30% indels); one batch",
 }
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+SMEM_DRAM_BYTES_PER_EXT = 2.641e9 / 44.86e6
 HBM_FALLBACK = 6650.0
 
 
@@ -419,8 +420,14 @@ def main():
     # two 32 B occurrence buckets per bi-interval extension, plus the read bytes
     smem_bytes = 64.0 * agg["n_ext"] + read_bytes
     achieved = smem_bytes / (agg["smem"] / 1000.0) / 1e9 if agg["smem"] > 0 else 0.0
+    # DRAM bytes per extension measured by ncu on the 60-genome workload shape
+    # (2.641 GB read + written for 44.86 M extensions), scaled to this launch
+    traffic = SMEM_DRAM_BYTES_PER_EXT * agg["n_ext"] / args.steps
     roofline = {"kernel": "k_smem (SMEM bi-interval extension)", "bound": "hbm", "achieved": achieved, "peak": hbm,
-                "unit": "GB/s", "frac": achieved / hbm, "traffic": None, "peak_source": peak_note,
+                "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_smem_thread launch on "
+                                  "the 60-genome shape, per extension, times this launch's extensions",
+                "peak_source": peak_note,
                 "alg_bytes_per_launch": smem_bytes / args.steps, "dominant_stage": dom,
                 "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()}}
 

@@ -376,13 +376,20 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     // ---------------- selection (maxNSeed) ----------------
     int32_t* d_hflag = reinterpret_cast<int32_t*>(d_cnt64);  // reuse scratch (n int32)
     if (n_reads > 0) {
-        S.n_launch++, k_select<<<nblk(n_reads, 256), 256, 0, st>>>(d_smem, d_smem_off, n_reads, params->max_nseed, d_sel, d_hflag);
+        CK(cudaMemsetAsync(d_ctr + 6, 0, 8, st));
+        S.n_launch++, k_select<<<nblk(n_reads, 256), 256, 0, st>>>(d_smem, d_smem_off, n_reads, params->max_nseed, d_sel, d_hflag,
+                                                                   d_ctr + 6);
         CK(cudaGetLastError());
-        std::vector<int32_t> hflag(n_reads);
-        CK(cudaMemcpyAsync(hflag.data(), d_hflag, n_reads * 4, cudaMemcpyDeviceToHost, st));
+        unsigned long long h_nflag = 0;
+        CK(cudaMemcpyAsync(&h_nflag, d_ctr + 6, 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         std::vector<int64_t> flagged;
-        for (int64_t r = 0; r < n_reads; ++r) if (hflag[r]) flagged.push_back(r);
+        if (h_nflag > 0) {  // only then are the per-read flags needed on the host
+            std::vector<int32_t> hflag(n_reads);
+            CK(cudaMemcpyAsync(hflag.data(), d_hflag, n_reads * 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (int64_t r = 0; r < n_reads; ++r) if (hflag[r]) flagged.push_back(r);
+        }
         if (!flagged.empty()) {
             // SMEM_LIST::findSeeds (SMEM.cpp:275-291): std::sort by loglik (not
             // stable; same libstdc++ algorithm on the same emission order), then

@@ -336,7 +336,8 @@ __global__ void k_slot_rows(const int64_t* __restrict__ len, int64_t n, int64_t 
 // read is flagged for the host, which runs the same std::sort.
 // ======================================================================
 __global__ void k_select(const int64_t* __restrict__ smem, const int64_t* __restrict__ smem_off, int64_t n_reads,
-                         int64_t max_nseed, uint8_t* __restrict__ sel, int32_t* __restrict__ host_flag) {
+                         int64_t max_nseed, uint8_t* __restrict__ sel, int32_t* __restrict__ host_flag,
+                         unsigned long long* __restrict__ n_flagged) {
     const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (r >= n_reads) return;
     const int64_t a = smem_off[r], b = smem_off[r + 1];
@@ -349,6 +350,7 @@ __global__ void k_select(const int64_t* __restrict__ smem, const int64_t* __rest
     const bool all = (b == a) || (tot - mn < max_nseed);
     for (int64_t k = a; k < b; ++k) sel[k] = all ? 1 : 0;
     host_flag[r] = all ? 0 : 1;
+    if (!all) atomicAdd(n_flagged, 1ull);
 }
 
 __global__ void k_seed_counts(const int64_t* __restrict__ smem, const uint8_t* __restrict__ sel, int64_t n,
