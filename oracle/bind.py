@@ -87,6 +87,9 @@ class Oracle:
         L.orc_find_smems.argtypes = [C.c_void_p, u8p, C.c_int64, C.c_int64, C.c_double, i64p, C.c_int64]
         L.orc_find_seeds.restype = C.c_int64
         L.orc_find_seeds.argtypes = [C.c_void_p, u8p, C.c_int64, C.c_int64, C.c_double, C.c_int64, i64p, C.c_int64]
+        L.orc_find_mems.restype = C.c_int64
+        L.orc_find_mems.argtypes = [C.c_void_p, u8p, C.c_int64, C.c_int64, C.c_double, i64p, C.c_int64,
+                                    C.POINTER(C.c_double)]
         L.orc_get_chains.restype = C.c_int64
         L.orc_get_chains.argtypes = [i64p, C.c_int64, C.c_int64, C.c_int64, i64p, i64p, C.c_int64, C.c_int64]
         L.orc_align_read.restype = C.c_int64
@@ -138,6 +141,16 @@ class Oracle:
             if n <= cap:
                 return out[:n]
             cap = n
+
+    def mems(self, read, min_len=17, max_evalue=0.01):
+        """SMEM_LIST::findMEMS rows (6 int64) and the list's loglik."""
+        read = np.ascontiguousarray(read, dtype=np.uint8)
+        cap = len(read) + 2
+        out = np.zeros((cap, 6), dtype=np.int64)
+        ll = C.c_double(0)
+        n = self.lib.orc_find_mems(self.h, _p(read, u8p), len(read), min_len, max_evalue, _p(out, i64p), cap, C.byref(ll))
+        assert n <= cap
+        return out[:n], ll.value
 
     def seeds(self, read, min_len=17, max_evalue=0.01, max_nseed=500):
         read = np.ascontiguousarray(read, dtype=np.uint8)
@@ -223,6 +236,13 @@ class Reference:
         L.ref_find_smems.argtypes = [C.c_void_p, u8p, C.c_int64, C.c_int64, C.c_double, i64p, C.c_int64]
         L.ref_find_seeds.restype = C.c_int64
         L.ref_find_seeds.argtypes = [C.c_void_p, u8p, C.c_int64, C.c_int64, C.c_double, C.c_int64, i64p, C.c_int64]
+        L.ref_find_mems.restype = C.c_int64
+        L.ref_find_mems.argtypes = [C.c_void_p, u8p, C.c_int64, C.c_int64, C.c_double, i64p, C.c_int64,
+                                    C.POINTER(C.c_double)]
+        L.ref_clean_batch.restype = C.c_int64
+        L.ref_clean_batch.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, u8p, i64p, u8p, i64p, C.c_int64, C.c_double,
+                                      C.c_double, C.c_int] + [C.POINTER(C.c_double)] * 3 + [u8p,
+                                                                                           C.POINTER(C.c_double)]
         L.ref_get_chains.restype = C.c_int64
         L.ref_get_chains.argtypes = [i64p, C.c_int64, C.c_int64, C.c_int64, i64p, i64p, C.c_int64, C.c_int64]
         L.ref_align_read.restype = C.c_int64
@@ -319,6 +339,16 @@ class Reference:
                 return out[:n]
             cap = n
 
+    def mems(self, read, min_len=17, max_evalue=0.01):
+        """SMEM_LIST::findMEMS rows (6 int64) and the list's loglik."""
+        read = np.ascontiguousarray(read, dtype=np.uint8)
+        cap = len(read) + 2
+        out = np.zeros((cap, 6), dtype=np.int64)
+        ll = C.c_double(0)
+        n = self.lib.ref_find_mems(self.h, _p(read, u8p), len(read), min_len, max_evalue, _p(out, i64p), cap, C.byref(ll))
+        assert n <= cap
+        return out[:n], ll.value
+
     def seeds(self, read, min_len=17, max_evalue=0.01, max_nseed=500):
         read = np.ascontiguousarray(read, dtype=np.uint8)
         cap = 4096
@@ -407,3 +437,24 @@ class Reference:
         m = self.lib.ref_map_batch(self.h, len(offs) - 1, _p(reads, u8p), _p(quals, u8p), _p(offs, i64p), min_len,
                                    max_evalue, max_nseed, min_score_rate, n_threads, C.byref(sec), C.byref(na))
         return m, na.value, sec.value
+
+    def clean_batch(self, bg, reads, offs, rev_reads=None, rev_offs=None, min_len=17, max_evalue=0.01, min_lod=0.0,
+                    n_threads=0):
+        """msgseqtk-clean's task body over a batch (this DB = reference
+        genomes, `bg` = background): per read (pair) refLoglik, bgLoglik,
+        lod and the keep decision, plus the OpenMP time in seconds."""
+        reads = np.ascontiguousarray(reads, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs, dtype=np.int64)
+        n = len(offs) - 1
+        pe = rev_reads is not None
+        rr = np.ascontiguousarray(rev_reads if pe else np.zeros(1), dtype=np.uint8)
+        ro = np.ascontiguousarray(rev_offs if pe else np.zeros(1), dtype=np.int64)
+        out = [np.zeros(n, dtype=np.float64) for _ in range(3)]
+        keep = np.zeros(n, dtype=np.uint8)
+        sec = C.c_double(0)
+        dp = C.POINTER(C.c_double)
+        self.lib.ref_clean_batch(self.h, bg.h, n, _p(reads, u8p), _p(offs, i64p), _p(rr, u8p) if pe else None,
+                                 _p(ro, i64p) if pe else None, min_len, max_evalue, min_lod, n_threads,
+                                 out[0].ctypes.data_as(dp), out[1].ctypes.data_as(dp), out[2].ctypes.data_as(dp),
+                                 _p(keep, u8p), C.byref(sec))
+        return out[0], out[1], out[2], keep.astype(bool), sec.value

@@ -638,6 +638,40 @@ int64_t do_align(const orc_index* ix, const Read& r, const std::vector<Seed>& ch
     return (int64_t)((R - 1) * (Cc - 1));
 }
 
+/* SMEM::findMEM (SMEM.cpp:42-62). The backward pass starts from the state
+ * left by the failed forward extension, whose size is 0, so it never extends:
+ * the returned MEM keeps `from`, ends one past the last matching base
+ * (to_good + 1) with the failed state's size (0) and bi-interval, and its logP
+ * includes that extra base when it lies inside the read. `to` returns to_good. */
+Smem find_mem(const orc_index* ix, const Read& r, int64_t& from, int64_t& to) {
+    Smem mem = smem_init(ix, r, from);
+    Smem mem0 = mem;
+    for (;;) {
+        smem_fwd(ix, r, mem);
+        if (mem.s <= 0) break;
+        mem0 = mem;
+    }
+    to = mem0.to;
+    mem0 = mem;
+    for (;;) {
+        smem_back(ix, r, mem);
+        if (mem.s <= 0) break;
+        mem0 = mem;
+    }
+    from = mem0.from;
+    return mem0;
+}
+
+/* SMEM_LIST::findMEMS (SMEM.cpp:174-184) */
+std::vector<Smem> find_mems(const orc_index* ix, const Read& r, int64_t minLen, double maxEvalue) {
+    std::vector<Smem> mems;
+    for (int64_t from = 0, to = 1; from < r.L; from = to + 1) {
+        Smem m = find_mem(ix, r, from, to);
+        if (m.to - m.from >= minLen && evalue_of(ix, m.logP) <= maxEvalue) mems.push_back(m);
+    }
+    return mems;
+}
+
 std::vector<Seed> seeds_from_rows(const int64_t* rows, int64_t n) {
     std::vector<Seed> v;
     for (int64_t i = 0; i < n; ++i) {
@@ -658,6 +692,22 @@ extern "C" int64_t orc_find_smems(const orc_index* ix, const uint8_t* read, int6
         o[0] = v[k].from; o[1] = v[k].to; o[2] = v[k].p; o[3] = v[k].q; o[4] = v[k].s;
         std::memcpy(&o[5], &v[k].logP, 8);
     }
+    return (int64_t)v.size();
+}
+
+extern "C" int64_t orc_find_mems(const orc_index* ix, const uint8_t* read, int64_t L, int64_t min_len,
+                                 double max_evalue, int64_t* out, int64_t cap, double* loglik) {
+    Read r{read, L};
+    std::vector<Smem> v = find_mems(ix, r, min_len, max_evalue);
+    double ll = 0;  // SMEM_LIST::loglik (SMEM.cpp:307-312)
+    for (int64_t k = 0; k < (int64_t)v.size(); ++k) {
+        ll += v[k].logP;
+        if (k >= cap) continue;
+        int64_t* o = out + 6 * k;
+        o[0] = v[k].from; o[1] = v[k].to; o[2] = v[k].p; o[3] = v[k].q; o[4] = v[k].s;
+        std::memcpy(&o[5], &v[k].logP, 8);
+    }
+    if (loglik) *loglik = ll;
     return (int64_t)v.size();
 }
 

@@ -40,6 +40,11 @@ double orc_loglik(const orc_index* ix, int b);
 int64_t orc_find_smems(const orc_index* ix, const uint8_t* read, int64_t L, int64_t min_len,
                        double max_evalue, int64_t* out, int64_t cap);
 
+/* SMEM_LIST::findMEMS (msgseqtk-clean's search); rows of 6 int64 as for
+ * SMEMs; *loglik receives SMEM_LIST::loglik of the list. Returns count. */
+int64_t orc_find_mems(const orc_index* ix, const uint8_t* read, int64_t L, int64_t min_len,
+                      double max_evalue, int64_t* out, int64_t cap, double* loglik);
+
 /* SMEM_LIST::findSeeds; rows of 6 int64: from, to, start, end, tid, strand. */
 int64_t orc_find_seeds(const orc_index* ix, const uint8_t* read, int64_t L, int64_t min_len,
                        double max_evalue, int64_t max_nseed, int64_t* out, int64_t cap);

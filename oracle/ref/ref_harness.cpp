@@ -336,6 +336,70 @@ int64_t ref_map_batch(void* h, int64_t n_reads, const uint8_t* reads, const uint
     return mapped;
 }
 
+/* SMEM_LIST::findMEMS (SMEM.cpp:174-184): rows of 6 as ref_find_smems;
+ * *loglik = MEM_LIST::loglik (SMEM.cpp:307-312). Returns the MEM count. */
+int64_t ref_find_mems(void* h, const uint8_t* read, int64_t L, int64_t min_len, double max_evalue,
+                      int64_t* out, int64_t cap, double* loglik) {
+    RefDB* db = (RefDB*)h;
+    PrimarySeq r = make_read(read, L, nullptr, "r");
+    MEM_LIST mems = SMEM_LIST::findMEMS(&r, &db->mtg, &db->fmd, min_len, max_evalue);
+    int64_t k = 0;
+    for (const MEM& m : mems) {
+        if (k < cap) {
+            int64_t* o = out + 6 * k;
+            o[0] = m.from; o[1] = m.to; o[2] = m.fwdStart; o[3] = m.revStart; o[4] = m.size;
+            std::memcpy(&o[5], &m.logP, 8);
+        }
+        ++k;
+    }
+    if (loglik) *loglik = mems.loglik();
+    return k;
+}
+
+/* msgseqtk-clean's per-read task body (msgseqtk-clean.cpp:425-438 single-end,
+ * :462-475 paired-end when rev_reads is not NULL) over a batch with OpenMP:
+ * findMEMS on the reference and on the background index, the lists' loglik,
+ * lod = -refLoglik + bgLoglik, kept when lod > min_lod. Outputs may be NULL;
+ * *seconds gets the steady_clock time. Returns the number of kept reads. */
+int64_t ref_clean_batch(void* h_ref, void* h_bg, int64_t n_reads, const uint8_t* reads, const int64_t* offs,
+                        const uint8_t* rev_reads, const int64_t* rev_offs, int64_t min_len, double max_evalue,
+                        double min_lod, int n_threads, double* ref_ll, double* bg_ll, double* lod_out,
+                        uint8_t* keep, double* seconds) {
+    RefDB* rdb = (RefDB*)h_ref;
+    RefDB* bdb = (RefDB*)h_bg;
+#ifdef _OPENMP
+    if (n_threads > 0) omp_set_num_threads(n_threads);
+#endif
+    int64_t kept = 0;
+    auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : kept)
+    for (int64_t i = 0; i < n_reads; ++i) {
+        const PrimarySeq fwd = make_read(reads + offs[i], offs[i + 1] - offs[i], nullptr, "r");
+        double refLoglik, bgLoglik;
+        if (rev_reads) {
+            const PrimarySeq rev = make_read(rev_reads + rev_offs[i], rev_offs[i + 1] - rev_offs[i], nullptr, "r");
+            MEM_LIST_PE refMemsPE = SMEM_LIST::findMEMS_PE(&fwd, &rev, &rdb->mtg, &rdb->fmd, min_len, max_evalue);
+            MEM_LIST_PE bgMemsPE = SMEM_LIST::findMEMS_PE(&fwd, &rev, &bdb->mtg, &bdb->fmd, min_len, max_evalue);
+            refLoglik = SMEM_LIST::loglik(refMemsPE);
+            bgLoglik = SMEM_LIST::loglik(bgMemsPE);
+        } else {
+            MEM_LIST refMems = SMEM_LIST::findMEMS(&fwd, &rdb->mtg, &rdb->fmd, min_len, max_evalue);
+            MEM_LIST bgMems = SMEM_LIST::findMEMS(&fwd, &bdb->mtg, &bdb->fmd, min_len, max_evalue);
+            refLoglik = refMems.loglik();
+            bgLoglik = bgMems.loglik();
+        }
+        const double lod = -refLoglik + bgLoglik;
+        if (ref_ll) ref_ll[i] = refLoglik;
+        if (bg_ll) bg_ll[i] = bgLoglik;
+        if (lod_out) lod_out[i] = lod;
+        if (keep) keep[i] = lod > min_lod;
+        kept += lod > min_lod;
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+    return kept;
+}
+
 /* ---- SAM records -----------------------------------------------------
  * Each read's SAM records as text lines, from the reference's own tail:
  * Alignment::filter/evaluate/calcMapQ/sort and exportBAM, plus the
