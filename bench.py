@@ -27,6 +27,16 @@ on a bounded sample of the same reads with all host threads.
 
 `--impl reference` times that reference CPU path alone (rank 0; other ranks
 exit without work).
+
+`--workload clean` measures msgseqtk-clean's path instead: findMEMS of every
+mate against a reference index (the scale metagenome) and a background index
+(a second metagenome of half as many genomes, another seed), the two lists'
+log-likelihoods and the log-odds keep decision per pair, on 2 x 150 bp pairs
+drawn half from each genome set. `value` = reads/s (each mate counts) through
+msg_clean_batch_device with the reads resident in HBM, `e2e` = the same
+through msg_clean_batch from pinned host reads; the reference arm times the
+reference's own clean task body (findMEMS_PE on both indexes) with all host
+threads.
 """
 from __future__ import annotations
 
@@ -50,7 +60,11 @@ WORKLOADS = {
              "0.1% indel, 5% random pairs; mates mapped as single reads (findSeedsPE)",
     "uneven": "uneven: 200 genomes ~600 Mbp; single-end reads 60% 75-150 bp, 30% 250-300 bp, 10% 1-10 kbp, "
               "5% errors (70% substitutions, 30% indels); one batch",
+    "clean": "clean: reference index = 200 genomes ~600 Mbp, background index = 100 genomes ~300 Mbp (other "
+             "seed); 2x150 bp pairs, half from each set, insert N(400,50), 1% sub, 0.1% indel, 5% random pairs; "
+             "findMEMS (min seed 17, e-value 0.01) on both indexes, log-odds > 0 keeps the pair",
 }
+CLEAN_METRIC = "cleaned reads/sec/GPU (2x150bp pairs, findMEMS on reference + background index, log-odds decision)"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 SMEM_DRAM_BYTES_PER_EXT = 2.641e9 / 44.86e6
 HBM_FALLBACK = 6650.0
@@ -74,8 +88,9 @@ def parse():
                     help="read pairs (fresh seed) whose chains train the band classifier")
     ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--min-score", type=float, default=0.65, help="Alignment::filter rate (msgseqtk-align -s)")
-    ap.add_argument("--workload", default="scale", choices=["scale", "uneven"],
-                    help="scale: 2x150 bp pairs; uneven: single-end reads of mixed lengths (one batch)")
+    ap.add_argument("--workload", default="scale", choices=["scale", "uneven", "clean"],
+                    help="scale: 2x150 bp pairs; uneven: single-end reads of mixed lengths (one batch); "
+                         "clean: msgseqtk-clean's MEM log-odds path on two indexes")
     ap.add_argument("--uneven-reads", type=int, default=500_000)
     return ap.parse_args()
 
@@ -257,11 +272,228 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def clean_workload(args, rank, device):
+    """Reference and background metagenomes, their index views, and pairs
+    drawn half from each (shuffled): (g_ref, g_bg, v_ref, v_bg, mates1,
+    offs1, mates2, offs2, setup)."""
+    from msgseqtk_b200 import index_build, synth
+    t0 = time.time()
+    g_ref = synth.scale_genomes(seed=args.seed, n_genomes=args.genomes, median=args.median)
+    g_bg = synth.scale_genomes(seed=args.seed + 100, n_genomes=max(1, args.genomes // 2), median=args.median)
+    t1 = time.time()
+    v_ref = index_build.build_view(g_ref, device=device)
+    v_bg = index_build.build_view(g_bg, device=device)
+    t2 = time.time()
+    half = args.pairs // 2
+    a1, a2 = synth.sample_pairs(g_ref, half, seed=reads_seed(rank))
+    b1, b2 = synth.sample_pairs(g_bg, args.pairs - half, seed=reads_seed(rank) + 500)
+    order = np.random.default_rng(reads_seed(rank)).permutation(args.pairs)
+    mates = []
+    for x, y in ((a1, b1), (a2, b2)):
+        lens = np.concatenate([np.diff(x.offs), np.diff(y.offs)])[order]
+        starts = np.concatenate([x.offs[:-1], len(x.seqs) + y.offs[:-1]])[order]
+        flat = np.concatenate([x.seqs, y.seqs])
+        offs = np.zeros(args.pairs + 1, dtype=np.int64)
+        np.cumsum(lens, out=offs[1:])
+        idx = np.repeat(starts - offs[:-1], lens) + np.arange(offs[-1])
+        mates += [flat[idx], offs]
+    t3 = time.time()
+    setup = {"genome_s": round(t1 - t0, 1), "index_s": round(t2 - t1, 1), "reads_s": round(t3 - t2, 1)}
+    return (g_ref, g_bg, v_ref, v_bg, *mates, setup)
+
+
+def main_clean(args, world, rank, local):
+    import torch
+    import torch.distributed as dist
+    from msgseqtk_b200 import lib
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://")
+    g_ref, g_bg, v_ref, v_bg, s1, o1, s2, o2, setup = clean_workload(args, rank, f"cuda:{local}")
+    torch.cuda.empty_cache()
+    ref, bg = lib.Context(local), lib.Context(local)
+    t0 = time.time()
+    ref.load_index(v_ref)
+    bg.load_index(v_bg)
+    setup["load_s"] = round(time.time() - t0, 1)
+    setup["index_gb"] = round((ref.index_bytes() + bg.index_bytes()) / 1e9, 2)
+    params = lib.mem_params()
+    bp = min(args.batch_pairs, args.pairs)
+    n_batches = max(1, args.pairs // bp)
+    d1, d2 = torch.from_numpy(s1).cuda(), torch.from_numpy(s2).cuda()
+    offd = []
+    for k in range(n_batches):
+        offd.append((torch.from_numpy(o1[k * bp:(k + 1) * bp + 1] - o1[k * bp]).cuda(),
+                     torch.from_numpy(o2[k * bp:(k + 1) * bp + 1] - o2[k * bp]).cuda()))
+    stream = torch.cuda.ExternalStream(ref.stream_handle())
+
+    def run_device(k):
+        a1, a2 = int(o1[k * bp]), int(o2[k * bp])
+        return ref.clean_device(bg, d1.data_ptr() + a1, offd[k][0].data_ptr(), bp, d2.data_ptr() + a2,
+                                offd[k][1].data_ptr(), params)
+
+    for s in range(args.warmup):
+        run_device(s % n_batches)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    agg = {"n_ext": 0, "n_launch": 0, "ms_mem": 0.0, "kept": 0}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for s in range(args.steps):
+        res = run_device((args.warmup + s) % n_batches)
+        st = ref.stats()
+        agg["n_ext"] += st["n_ext"]; agg["n_launch"] += st["n_launch"]; agg["ms_mem"] += st["ms_smem"]
+        agg["kept"] += int(res[3].sum())
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms, total_reads = reduce_over_ranks(ev0.elapsed_time(ev1), 2.0 * bp * args.steps, "cuda")
+    value = total_reads / (ms / 1000.0)
+
+    # end to end: pinned host mates in, host decisions out
+    h1 = torch.from_numpy(s1).pin_memory().numpy()
+    h2 = torch.from_numpy(s2).pin_memory().numpy()
+    hoff = [(torch.from_numpy(o1[k * bp:(k + 1) * bp + 1] - o1[k * bp]).pin_memory().numpy(),
+             torch.from_numpy(o2[k * bp:(k + 1) * bp + 1] - o2[k * bp]).pin_memory().numpy())
+            for k in range(n_batches)]
+
+    def run_host(k):
+        a1, b1 = int(o1[k * bp]), int(o1[(k + 1) * bp])
+        a2, b2 = int(o2[k * bp]), int(o2[(k + 1) * bp])
+        return ref.clean(bg, h1[a1:b1], hoff[k][0], h2[a2:b2], hoff[k][1], params), (b1 - a1) + (b2 - a2)
+
+    run_host(0)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    h2d = 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for s in range(args.steps):
+        k = (args.warmup + s) % n_batches
+        _, nbytes = run_host(k)
+        h2d += nbytes + hoff[k][0].nbytes + hoff[k][1].nbytes
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e, e2e_reads = reduce_over_ranks(e0.elapsed_time(e1), 2.0 * bp * args.steps, "cuda")
+    e2e = {"value": e2e_reads / (ms_e2e / 1000.0), "unit": "reads/s", "h2d_bytes_per_step": int(h2d // args.steps),
+           "d2h_bytes_per_step": int(25 * bp)}
+
+    peaks = json.load(open(PEAKS)) if os.path.exists(PEAKS) else {}
+    hbm = peaks.get("hbm_gbs")
+    peak_note = "measured" if hbm else "fallback"
+    hbm = hbm or HBM_FALLBACK
+    # two 32 B occurrence buckets per extension, plus each mate's bases once per index
+    alg = 64.0 * agg["n_ext"] + 2.0 * float(o1[bp] + o2[bp]) * args.steps
+    achieved = alg / (agg["ms_mem"] / 1000.0) / 1e9 if agg["ms_mem"] > 0 else 0.0
+    roofline = {"kernel": "k_mems (MEM forward extension, both indexes)", "bound": "hbm", "achieved": achieved,
+                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                "peak_source": peak_note, "alg_bytes_per_launch": alg / args.steps,
+                "kernel_ms_per_step": agg["ms_mem"] / args.steps,
+                "extensions_per_step": agg["n_ext"] / args.steps}
+
+    valid = None
+    if rank == 0 and args.validate > 0:
+        from oracle.bind import Oracle
+        orc_r, orc_b = Oracle(v_ref), Oracle(v_bg)
+        n = min(args.validate, bp)
+        r, g, lod, keep = ref.clean(bg, s1[:o1[n]], o1[:n + 1], s2[:o2[n]], o2[:n + 1], params)
+        bad = 0
+        for i in range(n):
+            m1, m2 = s1[o1[i]:o1[i + 1]], s2[o2[i]:o2[i + 1]]
+            er = orc_r.mems(m1)[1] + orc_r.mems(m2)[1]
+            eb = orc_b.mems(m1)[1] + orc_b.mems(m2)[1]
+            if not (np.float64(er).view(np.int64) == np.float64(r[i]).view(np.int64)
+                    and np.float64(eb).view(np.int64) == np.float64(g[i]).view(np.int64)
+                    and bool(keep[i]) == bool(-er + eb > 0)):
+                bad += 1
+        valid = {"pairs": n, "mismatching_pairs": bad, "compared": "refLoglik, bgLoglik bit patterns and keep"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = clean_cpu_rate(g_ref, g_bg, v_ref, v_bg, s1, o1, s2, o2, args.cpu_seconds)
+
+    if rank == 0:
+        line = {"metric": CLEAN_METRIC, "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOADS["clean"], "pairs_per_step": bp, "reads_per_step": 2 * bp,
+                           "bd_symbols": [v_ref.n, v_bg.n],
+                           "l2": "inputs larger than L2 (indexes %.1f GB, new reads every step)" % setup["index_gb"],
+                           "parallelism": f"dp{world}" if world > 1 else "single GPU"},
+                "kept_fraction": agg["kept"] / (bp * args.steps),
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+                "gpu_launches": agg["n_launch"], "validation": valid, "setup": setup}
+        print(json.dumps(line), flush=True)
+    ref.close()
+    bg.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def clean_cpu_rate(g_ref, g_bg, v_ref, v_bg, s1, o1, s2, o2, target_s, steps=1, warmup=0):
+    """The reference's clean task body (oracle/_ref) on bounded samples of the
+    pairs with all host threads: reads/s and the sample description."""
+    from oracle.bind import REF_SO, Reference
+    if not os.path.exists(REF_SO):
+        return None
+    ref, bg = Reference(g_ref, view=v_ref), Reference(g_bg, view=v_bg)
+    threads = ref.lib.ref_max_threads()
+    n_pairs = len(o1) - 1
+
+    def run(a, n):
+        return ref.clean_batch(bg, s1[o1[a]:o1[a + n]], o1[a:a + n + 1] - o1[a], s2[o2[a]:o2[a + n]],
+                               o2[a:a + n + 1] - o2[a], n_threads=threads)[4]
+
+    n_cal = min(n_pairs, 500 * threads)
+    rate = n_cal / max(run(0, n_cal), 1e-9)
+    n = int(min(n_pairs // max(1, steps), max(n_cal, rate * target_s)))
+    times = [run((k * n) % max(1, n_pairs - n + 1), n) for k in range(steps)]
+    timed = times[-1:] if steps == 1 else times[warmup:]
+    value = 2.0 * n * len(timed) / sum(timed)
+    return {"value": value, "unit": "reads/s", "cores": threads, "kind": "reference",
+            "sample": f"{n} pairs per step of the workload (of {n_pairs}), the reference's findMEMS_PE on both "
+                      f"indexes + loglik + log-odds per pair, OpenMP {threads} threads",
+            "seconds": round(sum(timed), 2), "ms_per_step": 1000.0 * sum(timed) / len(timed)}
+
+
+def run_reference_clean(args, world, rank):
+    if rank != 0:
+        return
+    import torch
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    g_ref, g_bg, v_ref, v_bg, s1, o1, s2, o2, setup = clean_workload(args, rank, dev)
+    from oracle.bind import REF_SO
+    if not os.path.exists(REF_SO):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmsgref.so was not built"}))
+        return
+    per = max(1.0, args.cpu_seconds / 2)
+    cpu = clean_cpu_rate(g_ref, g_bg, v_ref, v_bg, s1, o1, s2, o2, per, steps=args.warmup + args.steps,
+                         warmup=args.warmup)
+    value = cpu["value"]
+    line = {"metric": CLEAN_METRIC, "value": value, "unit": "reads/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": cpu.pop("ms_per_step"), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOADS["clean"], "bd_symbols": [v_ref.n, v_bg.n],
+                       "parallelism": f"omp{cpu['cores']}"},
+            "cpu_baseline": cpu, "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0,
+                                          "d2h_bytes_per_step": 0}, "setup": setup}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
+    if args.impl == "reference" and args.workload == "clean":
+        return run_reference_clean(args, world, rank)
     if args.impl == "reference":
         return run_reference(args, world, rank)
+    if args.workload == "clean":
+        return main_clean(args, world, rank, local)
     import torch
     import torch.distributed as dist
     from msgseqtk_b200 import lib

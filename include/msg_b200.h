@@ -297,6 +297,47 @@ int msg_band_train(msg_ctx* ctx, const float* feat, const int32_t* label, int64_
 int msg_band_grad(msg_ctx* ctx, const float* params, const float* feat, const int32_t* label, int64_t n,
                   float* grad, float* loss);
 
+/* ---- MEM search and read cleaning (msgseqtk-clean) ---- */
+
+typedef struct msg_mem_params {
+    int64_t min_len;        /* --min-seed, SMEM::MIN_LENGTH = 17 */
+    double max_evalue;      /* --max-evalue, 0.01; +inf for no limit */
+} msg_mem_params;
+
+void msg_mem_params_default(msg_mem_params* p);
+
+/* SMEM_LIST::findMEMS (src/SMEM.cpp:174-184, SMEM::findMEM :42-62) on each
+ * read of a batch in HOST memory against the context's index, with
+ * MEM_LIST::loglik (src/SMEM.cpp:307-312) of each read's list. loglik and
+ * n_mem get n_reads entries (either may be NULL). rows (may be NULL): the MEMs
+ * of all reads in read order, 6 int64 each (from, to, fwdStart, revStart,
+ * size, logP bit pattern, the SMEM fields of src/SMEM.h:196-200); *n_rows
+ * receives their count, and MSG_EINVAL is returned with rows untouched when it
+ * exceeds row_cap. msg_last_stats afterwards: n_reads, n_smem (MEMs kept),
+ * n_ext, n_launch, ms_smem (search) and ms_total. */
+int msg_mem_batch(msg_ctx* ctx, const msg_read_batch* reads, const msg_mem_params* params, double* loglik,
+                  int32_t* n_mem, int64_t* rows, int64_t row_cap, int64_t* n_rows);
+
+/* msgseqtk-clean's per-read task (src/msgseqtk-clean.cpp:413-446 single-end,
+ * :448-486 paired-end): findMEMS of each read against the reference genomes
+ * (ref's index) and the background genomes (bg's index); refLoglik and
+ * bgLoglik are the lists' loglik (for a pair, first mate's + second mate's,
+ * src/SMEM.h:391-393); lod = -refLoglik + bgLoglik; keep = lod > min_lod.
+ * fwd holds the reads (first mates), rev the second mates or NULL for
+ * single-end data (same n_reads). Both contexts must live on the same device
+ * with their indexes loaded; the call runs on ref's stream and reads bg's
+ * index, so no other call may use bg meanwhile. Host outputs of n_reads
+ * entries; any may be NULL. msg_last_stats(ref) as for msg_mem_batch. */
+int msg_clean_batch(msg_ctx* ref, msg_ctx* bg, const msg_read_batch* fwd, const msg_read_batch* rev,
+                    const msg_mem_params* params, double min_lod, double* ref_loglik, double* bg_loglik,
+                    double* lod, uint8_t* keep);
+
+/* Same with the reads already in device memory (seq and off of fwd and rev are
+ * device pointers); results still land in the caller's host buffers. */
+int msg_clean_batch_device(msg_ctx* ref, msg_ctx* bg, const msg_read_batch* dev_fwd,
+                           const msg_read_batch* dev_rev, const msg_mem_params* params, double min_lod,
+                           double* ref_loglik, double* bg_loglik, double* lod, uint8_t* keep);
+
 /* ---- Single-operation entry points (parity checks of the index layer) ---- */
 
 /* WaveletTreeRRR::rank (src/libsds/src/WaveletTreeRRR.cpp:101-125) through

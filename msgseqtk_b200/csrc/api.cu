@@ -42,10 +42,7 @@ extern "C" void msg_ctx_destroy(msg_ctx* c) {
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     c->index_free();
-    for (msg::DevBuf* b : {&c->reads, &c->offs, &c->smem, &c->smem_cnt, &c->prev, &c->sel, &c->seedoff, &c->seeds,
-                           &c->seeds2, &c->rcount, &c->chains, &c->chainidx, &c->dpinfo, &c->scratch, &c->path,
-                           &c->alnbuf, &c->cigbuf, &c->misc, &c->status})
-        b->release();
+    c->buffers_free();
     for (auto& e : c->ev) cudaEventDestroy(e);
     cudaStreamDestroy(c->stream);
     delete c;

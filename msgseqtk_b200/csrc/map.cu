@@ -32,6 +32,10 @@ namespace {
 
 int64_t nblk(int64_t n, int t) { return (n + t - 1) / t; }
 
+}  // namespace
+
+namespace msg {
+
 // Largest double ll with n * exp(ll) <= max_e (the e-value test of
 // SMEM::evalue, SMEM.h:102-110, made with the host's own exp exactly as the
 // reference makes it). The predicate is monotone in ll, so SMEM stages compare
@@ -68,6 +72,10 @@ int evalue_threshold(int64_t n, double max_e, double* thr, int* all) {
     *thr = dval(lo);
     return MSG_OK;
 }
+
+}  // namespace msg
+
+namespace {
 
 template <typename T>
 cudaError_t scan_excl(msg_ctx* ctx, const T* in, T* out, int64_t n, DevBuf& tmpb) {
@@ -290,8 +298,8 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             const int64_t n_thr = (int64_t)ctx->num_sms * std::max(1, bps) * 128;
             const int64_t pv_cap = kThreadPrev;
             CK(ctx->prev.ensure(n_thr * pv_cap * sizeof(PrevEntry) + 64));
-            CK(cudaMemcpyToSymbolAsync(c_llk, im.llk, sizeof(im.llk), 0, cudaMemcpyHostToDevice, st));
             SmemThreadArgs ta{};
+            for (int b = 0; b < 16; ++b) ta.llk[b] = im.llk[b];
             ta.seq = d_seq; ta.off = d_off; ta.n_reads = (int64_t)h_split[0]; ta.min_len = params->min_len;
             ta.thr = thr; ta.thr_all = thr_all;
             ta.llk_min = *std::min_element(im.llk, im.llk + 16);

@@ -59,6 +59,8 @@ struct msg_ctx {
         scratch, path, alnbuf, cigbuf, misc, status, geobuf, bandbuf, alnbuf2, recoff, rlist, prevw;
     // band model (bf16 weights, fp32 feature mean/scale) and training buffers
     msg::DevBuf band_wts, band_nrm, tr_x, tr_y, tr_ord, tr_w, tr_m, tr_v, tr_g, tr_loss;
+    // MEM search / read cleaning: per-unit loglik and counts, clean outputs, MEM rows, row slots
+    msg::DevBuf memo, memo2, memrows, memslot;
     bool band_loaded = false;
     int64_t scratch_limit = 16ll << 30;  // DP rectangle storage per pass (msg_ctx_set_scratch_limit)
     cudaEvent_t ev[8];
@@ -73,6 +75,13 @@ struct msg_ctx {
     int cuda_fail(cudaError_t e) {
         last_error = cudaGetErrorString(e);
         return e == cudaErrorMemoryAllocation ? MSG_ENOMEM : MSG_ECUDA;
+    }
+    void buffers_free() {
+        for (msg::DevBuf* b : {&reads, &offs, &smem, &smem_cnt, &prev, &sel, &seedoff, &seeds, &seeds2, &rcount,
+                               &chains, &chainidx, &dpinfo, &scratch, &path, &alnbuf, &cigbuf, &misc, &status, &geobuf,
+                               &bandbuf, &alnbuf2, &recoff, &rlist, &prevw, &band_wts, &band_nrm, &tr_x, &tr_y,
+                               &tr_ord, &tr_w, &tr_m, &tr_v, &tr_g, &tr_loss, &memo, &memo2, &memrows, &memslot})
+            b->release();
     }
     void index_free() {
         if (idx.bkt) cudaFree(idx.bkt);

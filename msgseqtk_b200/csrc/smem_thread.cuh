@@ -39,6 +39,7 @@ struct SmemThreadArgs {
     double thr;
     int thr_all;
     double llk_min, llk_max;  // extremes of the per-base log-likelihoods
+    double llk[16];           // FMDIndex::loglik per nt16 code (by value: each context's own table)
     int64_t* out;
     int64_t cap;            // slot rows when out_off is null
     const int64_t* out_off; // per-read slot offsets (n + 1), or null: slot r at row r * cap
@@ -51,9 +52,9 @@ struct SmemThreadArgs {
     uint32_t* status;
 };
 
-__constant__ double c_llk[16];
-// per-block copy of c_llk: lanes index it by their own bases, which shared
-// memory serves in one pass where the constant cache would serialise
+// per-block copy of the argument table: lanes index it by their own bases,
+// which shared memory serves in one pass where the parameter (constant) bank
+// would serialise
 __shared__ double s_llk[16];
 
 enum SmemPhase : int {
@@ -274,7 +275,7 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
 }
 
 __global__ void __launch_bounds__(128, 5) k_smem_thread(SmemThreadArgs a, IndexDev ix) {
-    if (threadIdx.x < 16) s_llk[threadIdx.x] = c_llk[threadIdx.x];
+    if (threadIdx.x < 16) s_llk[threadIdx.x] = a.llk[threadIdx.x];
     __syncthreads();
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     PrevEntry* pv = a.prev + tid * a.pv_cap;

@@ -28,9 +28,10 @@ assert ALN_DTYPE.itemsize == 88
 # symbols of the C ABI, in include/msg_b200.h order
 EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy", "msg_index_load", "msg_db_read",
            "msg_db_views", "msg_db_free", "msg_index_bytes",
-           "msg_map_params_default", "msg_map_batch", "msg_map_batch_device", "msg_last_stats", "msg_occ_query",
+           "msg_map_params_default", "msg_map_batch", "msg_map_batch_device", "msg_last_stats",
            "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
-           "msg_band_train", "msg_band_grad", "msg_bi_ext_query", "msg_sa_query"]
+           "msg_band_train", "msg_band_grad", "msg_mem_params_default", "msg_mem_batch", "msg_clean_batch",
+           "msg_clean_batch_device", "msg_occ_query", "msg_bi_ext_query", "msg_sa_query"]
 
 # band model (include/msg_b200.h)
 BAND_FEATURES, BAND_HIDDEN, BAND_CLASSES, BAND_NPARAMS = 16, 64, 4, 5540
@@ -55,6 +56,10 @@ class MapParams(C.Structure):
 
 class BandTrainParams(C.Structure):
     _fields_ = [("epochs", C.c_int32), ("batch", C.c_int32), ("lr", C.c_float), ("seed", C.c_uint64)]
+
+
+class MemParams(C.Structure):
+    _fields_ = [("min_len", C.c_int64), ("max_evalue", C.c_double)]
 
 
 class ReadBatch(C.Structure):
@@ -128,6 +133,14 @@ def load_library(path: str = LIB_PATH):
     L.msg_band_collect.argtypes = [C.c_void_p, C.POINTER(ReadBatch), C.POINTER(MapParams), f32p, i32p, C.c_int64, i64p]
     L.msg_band_train.argtypes = [C.c_void_p, f32p, i32p, C.c_int64, C.POINTER(BandTrainParams), f32p, f32p]
     L.msg_band_grad.argtypes = [C.c_void_p, f32p, f32p, i32p, C.c_int64, f32p, f32p]
+    f64p = C.POINTER(C.c_double)
+    L.msg_mem_params_default.argtypes = [C.POINTER(MemParams)]
+    L.msg_mem_params_default.restype = None
+    L.msg_mem_batch.argtypes = [C.c_void_p, C.POINTER(ReadBatch), C.POINTER(MemParams), f64p, i32p, i64p, C.c_int64,
+                                i64p]
+    L.msg_clean_batch.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(ReadBatch), C.POINTER(ReadBatch),
+                                  C.POINTER(MemParams), C.c_double, f64p, f64p, f64p, u8p]
+    L.msg_clean_batch_device.argtypes = L.msg_clean_batch.argtypes
     L.msg_occ_query.argtypes = [C.c_void_p, C.c_int64, u8p, i64p, i64p]
     L.msg_bi_ext_query.argtypes = [C.c_void_p, C.c_int64, C.c_int, u8p, i64p, i64p, i64p, i64p]
     L.msg_sa_query.argtypes = [C.c_void_p, C.c_int64, i64p, i64p]
@@ -149,6 +162,14 @@ def _p(a, t):
 def default_params(**kw) -> MapParams:
     p = MapParams()
     load_library().msg_map_params_default(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def mem_params(**kw) -> MemParams:
+    p = MemParams()
+    load_library().msg_mem_params_default(C.byref(p))
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -295,6 +316,68 @@ class Context:
         params = params or default_params()
         return self.lib.msg_smem_batch_noalloc(self.h, n_reads, seq_ptr, off_ptr, C.byref(params), out_ptr,
                                                cap_per_read, count_ptr)
+
+    # ---- MEM search and read cleaning ----
+    def mems(self, seq, off, params: MemParams | None = None, rows: bool = True):
+        """SMEM_LIST::findMEMS per read: (loglik[n], n_mem[n], rows[m, 6] or
+        None) with rows in read order."""
+        params = params or mem_params()
+        seq = np.ascontiguousarray(seq, dtype=np.uint8)
+        off = np.ascontiguousarray(off, dtype=np.int64)
+        n = len(off) - 1
+        batch = ReadBatch(n, _p(seq, u8p), _p(off, i64p))
+        ll = np.zeros(n, dtype=np.float64)
+        cnt = np.zeros(n, dtype=np.int32)
+        nr = C.c_int64(0)
+        f64p, i32p = C.POINTER(C.c_double), C.POINTER(C.c_int32)
+        if not rows:
+            self._check(self.lib.msg_mem_batch(self.h, C.byref(batch), C.byref(params), _p(ll, f64p), _p(cnt, i32p),
+                                               None, 0, C.byref(nr)), "msg_mem_batch")
+            return ll, cnt, None
+        cap = max(16, n)
+        while True:
+            out = np.zeros((cap, 6), dtype=np.int64)
+            rc = self.lib.msg_mem_batch(self.h, C.byref(batch), C.byref(params), _p(ll, f64p), _p(cnt, i32p),
+                                        _p(out, i64p), cap, C.byref(nr))
+            if rc == MSG_EINVAL and nr.value > cap:
+                cap = nr.value
+                continue
+            self._check(rc, "msg_mem_batch")
+            return ll, cnt, out[:nr.value].copy()
+
+    def clean(self, bg: "Context", seq, off, rev_seq=None, rev_off=None, params: MemParams | None = None,
+              min_lod: float = 0.0):
+        """msgseqtk-clean's decision with this context's index as the
+        reference genomes and bg's as the background, reads in host memory:
+        (ref_loglik, bg_loglik, lod, keep)."""
+        seq = np.ascontiguousarray(seq, dtype=np.uint8)
+        off = np.ascontiguousarray(off, dtype=np.int64)
+        n = len(off) - 1
+        fb = ReadBatch(n, _p(seq, u8p), _p(off, i64p))
+        rb = None
+        if rev_seq is not None:
+            rev_seq = np.ascontiguousarray(rev_seq, dtype=np.uint8)
+            rev_off = np.ascontiguousarray(rev_off, dtype=np.int64)
+            rb = ReadBatch(n, _p(rev_seq, u8p), _p(rev_off, i64p))
+        return self._clean(self.lib.msg_clean_batch, bg, n, fb, rb, params, min_lod)
+
+    def clean_device(self, bg: "Context", seq_ptr: int, off_ptr: int, n: int, rev_seq_ptr: int | None = None,
+                     rev_off_ptr: int | None = None, params: MemParams | None = None, min_lod: float = 0.0):
+        """clean() with the reads already in device memory (pointers)."""
+        fb = ReadBatch(n, C.cast(C.c_void_p(seq_ptr), u8p), C.cast(C.c_void_p(off_ptr), i64p))
+        rb = None
+        if rev_seq_ptr is not None:
+            rb = ReadBatch(n, C.cast(C.c_void_p(rev_seq_ptr), u8p), C.cast(C.c_void_p(rev_off_ptr), i64p))
+        return self._clean(self.lib.msg_clean_batch_device, bg, n, fb, rb, params, min_lod)
+
+    def _clean(self, fn, bg, n, fb, rb, params, min_lod):
+        params = params or mem_params()
+        f64p = C.POINTER(C.c_double)
+        out = [np.zeros(n, dtype=np.float64) for _ in range(3)]
+        keep = np.zeros(n, dtype=np.uint8)
+        self._check(fn(self.h, bg.h, C.byref(fb), C.byref(rb) if rb is not None else None, C.byref(params), min_lod,
+                       _p(out[0], f64p), _p(out[1], f64p), _p(out[2], f64p), _p(keep, u8p)), "msg_clean_batch")
+        return out[0], out[1], out[2], keep.astype(bool)
 
     # ---- band model ----
     def band_model_set(self, params: np.ndarray):

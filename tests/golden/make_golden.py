@@ -6,7 +6,14 @@ exists:  python tests/golden/make_golden.py
 Each fixture holds the synthetic genome (seeded), the reads, and what the
 reference computes for them: the FMD-index view (BWT, counts, SA samples,
 chromosome table), SMEM lists, seed lists after removeRedundant, and the
-per-chain alignments (window, score, coordinates, CIGAR, MD).
+per-chain alignments (window, score, coordinates, CIGAR, MD). The "clean"
+fixture holds msgseqtk-clean's path: two genome sets (reference and
+background), reads from both plus random and odd-symbol reads, the
+reference's findMEMS lists and loglik, and its clean decisions for single
+reads and pairs.
+
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py clean      # only the named ones
 """
 import os
 import sys
@@ -34,9 +41,69 @@ CASES = {
 }
 
 
+CLEAN_PARAMS = [(17, 0.01), (1, float("inf")), (9, 1e3)]  # (min_len, max_evalue)
+CLEAN_LOD = [0.0, 25.0]
+
+
+def clean_reads(g_ref, g_bg, seed):
+    """Reads from both genome sets, random reads, and reads holding the
+    symbols the reference's encoder can produce besides A/C/G/T (0 for
+    unknown characters, N, IUPAC codes), an empty read and a 1-base read."""
+    rng = np.random.default_rng(seed)
+    a = synth.sample_reads(g_ref, 60, seed=seed + 1)
+    b = synth.sample_reads(g_bg, 60, seed=seed + 2, sub_rate=0.03, indel_rate=0.01)
+    reads = [a.read(i) for i in range(len(a))] + [b.read(i) for i in range(len(b))]
+    reads += [synth._BASES[rng.integers(0, 4, int(rng.integers(20, 200)))] for _ in range(20)]
+    for i in range(20):
+        r = reads[i].copy()
+        pos = rng.integers(0, len(r), 4)
+        r[pos] = rng.choice(np.array([0, 15, 5, 3, 14], dtype=np.uint8), 4)
+        reads.append(r)
+    reads += [np.zeros(0, np.uint8), np.array([4], np.uint8), np.array([0, 0, 1, 2, 0], np.uint8)]
+    reads += [synth._BASES[rng.integers(0, 4, 1500)]]
+    off = np.cumsum([0] + [len(r) for r in reads]).astype(np.int64)
+    return np.concatenate(reads).astype(np.uint8), off
+
+
+def make_clean():
+    g_ref = synth.small_genomes(seed=111, n_genomes=3, length=20000)
+    g_bg = synth.small_genomes(seed=112, n_genomes=2, length=25000)
+    ref, bg = Reference(g_ref), Reference(g_bg)
+    seq, off = clean_reads(g_ref, g_bg, 113)
+    seq2, off2 = clean_reads(g_bg, g_ref, 114)  # second mates (same count)
+    data = dict(ref_genome=np.concatenate(g_ref).astype(np.uint8),
+                ref_genome_off=np.cumsum([0] + [len(x) for x in g_ref]).astype(np.int64),
+                bg_genome=np.concatenate(g_bg).astype(np.uint8),
+                bg_genome_off=np.cumsum([0] + [len(x) for x in g_bg]).astype(np.int64),
+                reads=seq, read_off=off, mates=seq2, mate_off=off2,
+                params=np.array(CLEAN_PARAMS, dtype=np.float64), lods=np.array(CLEAN_LOD))
+    n = len(off) - 1
+    for k, (ml, me) in enumerate(CLEAN_PARAMS):
+        rows, roff, ll = [], [0], []
+        for i in range(n):
+            m, l = ref.mems(seq[off[i]:off[i + 1]], ml, me)
+            rows.append(m); roff.append(roff[-1] + len(m)); ll.append(l)
+        data[f"p{k}_mem"] = np.concatenate(rows)
+        data[f"p{k}_mem_off"] = np.array(roff, dtype=np.int64)
+        data[f"p{k}_mem_ll"] = np.array(ll, dtype=np.float64)
+        for j, lod in enumerate(CLEAN_LOD):
+            se = ref.clean_batch(bg, seq, off, min_len=ml, max_evalue=me, min_lod=lod, n_threads=4)
+            pe = ref.clean_batch(bg, seq, off, seq2, off2, min_len=ml, max_evalue=me, min_lod=lod, n_threads=4)
+            for tag, res in (("se", se), ("pe", pe)):
+                data[f"p{k}_l{j}_{tag}"] = np.stack(res[:3])
+                data[f"p{k}_l{j}_{tag}_keep"] = res[3]
+    np.savez_compressed(os.path.join(OUT, "clean.npz"), **data)
+    print("clean", {k: v.shape for k, v in data.items() if hasattr(v, "shape")})
+
+
 def main():
     build_reference()
+    names = sys.argv[1:] or list(CASES) + ["clean"]
+    if "clean" in names:
+        make_clean()
     for name, (gb, rb, psets) in CASES.items():
+        if name not in names:
+            continue
         g = gb()
         ref = Reference(g)
         rs = rb(g)

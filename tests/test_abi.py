@@ -31,6 +31,8 @@ def test_status_strings_and_defaults():
     p = lib.default_params()
     assert (p.min_len, p.max_evalue, p.max_nseed, p.mode) == (17, 0.01, 500, 0)
     assert (p.match, p.mismatch, p.gap_open, p.gap_ext) == (1, 3, 5, 2)
+    m = lib.mem_params()  # msgseqtk-clean defaults: --min-seed 17, --max-evalue 0.01
+    assert (m.min_len, m.max_evalue) == (17, 0.01)
 
 
 def test_null_arguments_rejected_without_device():
@@ -39,3 +41,6 @@ def test_null_arguments_rejected_without_device():
     assert L.msg_index_load(None, None, None) == lib.MSG_EINVAL
     assert L.msg_map_batch(None, None, None, None, None) == lib.MSG_EINVAL
     assert L.msg_last_stats(None, None) == lib.MSG_EINVAL
+    assert L.msg_mem_batch(None, None, None, None, None, None, 0, None) == lib.MSG_EINVAL
+    assert L.msg_clean_batch(None, None, None, None, None, 0.0, None, None, None, None) == lib.MSG_EINVAL
+    assert L.msg_clean_batch_device(None, None, None, None, None, 0.0, None, None, None, None) == lib.MSG_EINVAL
