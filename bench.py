@@ -67,6 +67,9 @@ WORKLOADS = {
 CLEAN_METRIC = "cleaned reads/sec/GPU (2x150bp pairs, findMEMS on reference + background index, log-odds decision)"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 SMEM_DRAM_BYTES_PER_EXT = 2.641e9 / 44.86e6
+# DRAM bytes per MEM extension, ncu on the 60 + 30 genome clean shape
+# (4.437 GB read + written for 57.32 M extensions)
+MEM_DRAM_BYTES_PER_EXT = 4.437e9 / 57.32e6
 HBM_FALLBACK = 6650.0
 
 
@@ -391,7 +394,10 @@ def main_clean(args, world, rank, local):
     alg = 64.0 * agg["n_ext"] + 2.0 * float(o1[bp] + o2[bp]) * args.steps
     achieved = alg / (agg["ms_mem"] / 1000.0) / 1e9 if agg["ms_mem"] > 0 else 0.0
     roofline = {"kernel": "k_mems (MEM forward extension, both indexes)", "bound": "hbm", "achieved": achieved,
-                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": MEM_DRAM_BYTES_PER_EXT * agg["n_ext"] / args.steps,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_mems launch on the "
+                                  "60 + 30 genome shape, per extension, times this launch's extensions",
                 "peak_source": peak_note, "alg_bytes_per_launch": alg / args.steps,
                 "kernel_ms_per_step": agg["ms_mem"] / args.steps,
                 "extensions_per_step": agg["n_ext"] / args.steps}

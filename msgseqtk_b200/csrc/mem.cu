@@ -28,30 +28,46 @@ namespace {
 
 int64_t nblk(int64_t n, int t) { return (n + t - 1) / t; }
 
-// FMDIndex::backExt (src/FMDIndex.cpp:577-610) for the MEM walk. Unlike the
-// SMEM search, findMEM starts intervals on any read symbol, so a gap symbol
-// (nt16 0, what the reference's encoder gives every unknown character) opens
-// the '$' interval at row 0, and the next extension asks
-// WaveletTreeRRR::rank(b, p - 1) with p - 1 = -1; that rank answers
-// (size_t)-1 for every symbol (src/libsds/src/WaveletTreeRRR.cpp:102-103),
-// i.e. -1 after the cast, which this function reproduces. A size of 0 stays 0.
-__device__ __forceinline__ void mem_back_ext(const IndexDev& ix, uint32_t& p, uint32_t& q, uint32_t& s, int b,
-                                             uint32_t& n_ext) {
+// The two occurrence buckets one extension of bi-interval (p, s) reads: rows
+// p-1 and p+s-1 (exclusive ends p and p+s), one 32 B sector each, one load
+// when both rows fall in the same bucket.
+struct Bkt {
+    uint4 a0, a1, b0, b1;
+    uint32_t ja, jb;
+};
+
+__device__ __forceinline__ void mem_load(const IndexDev& ix, uint32_t p, uint32_t s, Bkt& k) {
+    k.ja = p;
+    k.jb = p + s;
+    const uint32_t ka = k.ja >> 6, kb = k.jb >> 6;
+    const uint4* pa = reinterpret_cast<const uint4*>(ix.bkt + ka);
+    k.a0 = __ldg(pa);
+    k.a1 = __ldg(pa + 1);
+    k.b0 = k.a0;
+    k.b1 = k.a1;
+    if (kb != ka) {
+        const uint4* pb = reinterpret_cast<const uint4*>(ix.bkt + kb);
+        k.b0 = __ldg(pb);
+        k.b1 = __ldg(pb + 1);
+    }
+}
+
+// FMDIndex::backExt (src/FMDIndex.cpp:577-610) for the MEM walk, on buckets
+// loaded by mem_load(p, s). Unlike the SMEM search, findMEM starts intervals
+// on any read symbol, so a gap symbol (nt16 0, what the reference's encoder
+// gives every unknown character) opens the '$' interval at row 0, and the
+// next extension asks WaveletTreeRRR::rank(b, p - 1) with p - 1 = -1; that
+// rank answers (size_t)-1 for every symbol
+// (src/libsds/src/WaveletTreeRRR.cpp:102-103), i.e. -1 after the cast, which
+// this function reproduces. A size of 0 stays 0.
+__device__ __forceinline__ void mem_back_ext(const IndexDev& ix, const Bkt& k, uint32_t& p, uint32_t& q,
+                                             uint32_t& s, int b, uint32_t& n_ext) {
     if (!is_basic(b) || s == 0) { s = 0; return; }
     n_ext++;
     const uint32_t code = (uint32_t)(to_int(b) - 1);
-    const uint32_t ja = p, jb = p + s;  // exclusive ends of rows p-1 and p+s-1
-    const uint32_t ka = ja >> 6, kb = jb >> 6;
-    const uint4* pa = reinterpret_cast<const uint4*>(ix.bkt + ka);
-    const uint4 a0 = __ldg(pa), a1 = __ldg(pa + 1);
-    uint4 b0 = a0, b1 = a1;
-    if (kb != ka) {
-        const uint4* pb = reinterpret_cast<const uint4*>(ix.bkt + kb);
-        b0 = __ldg(pb); b1 = __ldg(pb + 1);
-    }
     uint32_t oa, ga, da, ob, gb, db;
-    occ_counts(ix, ka, ja & 63u, code, a0, a1, oa, ga, da);
-    occ_counts(ix, kb, jb & 63u, code, b0, b1, ob, gb, db);
+    occ_counts(ix, k.ja >> 6, k.ja & 63u, code, k.a0, k.a1, oa, ga, da);
+    occ_counts(ix, k.jb >> 6, k.jb & 63u, code, k.b0, k.b1, ob, gb, db);
     if (p == 0) {  // every count at row -1 is -1: (3 - code) bases after b
         oa = 0xffffffffu;
         da = 0xffffffffu;
@@ -69,7 +85,6 @@ struct MemArgs {
     double llk0[16], llk1[16]; // FMDIndex::loglik per nt16 code of each index
     double thr0, thr1;         // e-value thresholds on the log-likelihood
     int all0, all1;            // 1: no e-value limit
-    int n_idx;                 // 1 or 2 indexes
     int n_set;                 // 1 (single reads) or 2 (first and second mates)
     const uint8_t* seq0;
     const int64_t* off0;
@@ -77,51 +92,75 @@ struct MemArgs {
     const int64_t* off1;
     int64_t n;                 // reads per set
     int64_t min_len;
-    const int64_t* slot;       // first output row of each unit (rows != null)
+    const int64_t* slot;       // first output row of each read (one index, one set; rows != null)
     int64_t* rows;             // 6 int64 per MEM: from, to, fwdStart, revStart, size, logP bits
-    double* ll;                // per unit: MEM_LIST::loglik
-    int32_t* cnt;              // per unit: MEMs kept
-    unsigned long long* n_ext;
+    double* ll;                // per (index, set, read): MEM_LIST::loglik
+    int32_t* cnt;              // per (index, set, read): MEMs kept
+    unsigned long long* n_ext; // [0]: extensions; word 2 of the same buffer: error bits
 };
 
-// SMEM_LIST::findMEMS over one read. The reference's findMEM runs its backward
-// pass from the state the failed forward extension left (size 0), so that pass
-// never extends: each MEM keeps its start, ends one past the last matching
-// base with the failed state's fields, and the next search starts there.
-__device__ __forceinline__ void mem_read(const IndexDev& ix, const double* llk, double thr, int all,
-                                         const uint8_t* __restrict__ sq, int64_t L, int64_t min_len,
-                                         int64_t* __restrict__ out, double& ll_sum, int32_t& n_kept,
-                                         uint32_t& n_ext) {
-    ll_sum = 0.0;
-    n_kept = 0;
-    int64_t from = 0;
-    while (from < L) {
-        int b = sq[from];
-        uint32_t P = (uint32_t)ix.C[b], Q = (uint32_t)ix.C[comp16(b)];
-        uint32_t S = (uint32_t)(ix.C[b + 1] - ix.C[b]);
-        double lp = __dadd_rn(0.0, llk[b]);  // SMEM::evaluate
-        int64_t to = from + 1;
-        for (;;) {  // SMEM::fwdExt + fwdEvaluate until the size drops to 0
-            const int nb = to < L ? sq[to] : 0;
-            mem_back_ext(ix, Q, P, S, comp16(nb), n_ext);
-            if (to < L) lp = __dadd_rn(lp, llk[nb]);
-            ++to;
-            if (S == 0) break;
-        }
-        if (to - from >= min_len && (all || lp <= thr)) {
-            if (out) {
-                int64_t* o = out + 6 * (int64_t)n_kept;
-                o[0] = from; o[1] = to; o[2] = P; o[3] = Q; o[4] = 0;
-                o[5] = __double_as_longlong(lp);
-            }
-            ll_sum = __dadd_rn(ll_sum, lp);
-            n_kept++;
-        }
-        from = to;
-    }
+constexpr int64_t kMemMaxLen = 0x7ffffffdll;  // `to` reaches L + 1 in 32 bits
+
+// One SMEM_LIST::findMEMS walk (src/SMEM.cpp:174-184): the current MEM's
+// start `from` and end `to`, its bi-interval (fwdStart P, revStart Q, size S)
+// and log-likelihood lp, the next base nb, and the kept list's loglik/count.
+// The reference's findMEM (src/SMEM.cpp:42-62) runs its backward pass from
+// the state the failed forward extension left (size 0), so that pass never
+// extends: each MEM keeps its start, ends one past the last matching base
+// with the failed state's fields, and the next search starts there.
+struct Walk {
+    const uint8_t* sq;
+    int32_t L, from, to;  // reads are below 2^31 - 2 bases (checked)
+    uint32_t P, Q, S;
+    int nb;
+    double lp, ll;
+    int32_t cnt;
+};
+
+// SMEM's constructor + evaluate at `from` (SMEM.h:48-54, SMEM.cpp:19-24).
+__device__ __forceinline__ void walk_start(const IndexDev& ix, const double* llk, Walk& w) {
+    const int b = w.sq[w.from];
+    w.P = (uint32_t)ix.C[b];
+    w.Q = (uint32_t)ix.C[comp16(b)];
+    w.S = (uint32_t)(ix.C[b + 1] - ix.C[b]);
+    w.lp = __dadd_rn(0.0, llk[b]);
+    w.to = w.from + 1;
+    w.nb = w.to < w.L ? w.sq[w.to] : 0;
 }
 
-__global__ void __launch_bounds__(256) k_mems(MemArgs a) {
+// One SMEM::fwdExt + fwdEvaluate (SMEM.h:140-145,166-170); when the size
+// drops to 0 the MEM ends: findMEMS's length and e-value test, then the next
+// MEM starts at the end.
+template <bool ROWS>
+__device__ __forceinline__ void walk_step(const IndexDev& ix, const double* llk, double thr, int all, int64_t min_len,
+                                          const Bkt& k, int nn, Walk& w, int64_t* __restrict__ out, uint32_t& n_ext) {
+    mem_back_ext(ix, k, w.Q, w.P, w.S, comp16(w.nb), n_ext);
+    if (w.to < w.L) w.lp = __dadd_rn(w.lp, llk[w.nb]);
+    ++w.to;
+    w.nb = nn;
+    if (w.S != 0) return;
+    if (w.to - w.from >= min_len && (all || w.lp <= thr)) {
+        if (ROWS) {
+            int64_t* o = out + 6 * (int64_t)w.cnt;
+            o[0] = w.from; o[1] = w.to; o[2] = w.P; o[3] = w.Q; o[4] = 0;
+            o[5] = __double_as_longlong(w.lp);
+        }
+        w.ll = __dadd_rn(w.ll, w.lp);
+        w.cnt++;
+    }
+    w.from = w.to;
+    if (w.from < w.L) walk_start(ix, llk, w);
+}
+
+// NW walks per thread in one flat loop: every iteration issues the bucket
+// loads of all live walks, then advances each by one extension, so a thread
+// keeps NW independent loads in flight and a warp's threads stay in step
+// whatever their MEM lengths (nested per-MEM loops leave most lanes idle
+// while the longest MEM of the warp finishes). NW == 2: a thread per read
+// (or mate) against both indexes, walk j on index j; NW == 1: a thread per
+// read (or mate) on index 0.
+template <int NW, bool ROWS>
+__global__ void __launch_bounds__(256, NW == 1 ? 4 : 3) k_mems(MemArgs a) {
     __shared__ double s_llk[2][16];
     if (threadIdx.x < 32) {
         const int b = threadIdx.x & 15;
@@ -131,21 +170,51 @@ __global__ void __launch_bounds__(256) k_mems(MemArgs a) {
     const int64_t per_idx = a.n * a.n_set;
     const int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     uint32_t n_ext = 0;
-    if (u < per_idx * a.n_idx) {
-        const int k = u >= per_idx;
-        const int64_t rem = u - k * per_idx;
-        const int set = rem >= a.n;
-        const int64_t r = rem - set * a.n;
-        const uint8_t* sq = set ? a.seq1 : a.seq0;
+    if (u < per_idx) {
+        const int set = u >= a.n;
+        const int64_t r = u - set * a.n;
         const int64_t* of = set ? a.off1 : a.off0;
-        const int64_t o0 = of[r], L = of[r + 1] - o0;
-        int64_t* out = a.rows ? a.rows + 6 * a.slot[u] : nullptr;
-        double ll;
-        int32_t c;
-        if (k == 0) mem_read(a.ix0, s_llk[0], a.thr0, a.all0, sq + o0, L, a.min_len, out, ll, c, n_ext);
-        else mem_read(a.ix1, s_llk[1], a.thr1, a.all1, sq + o0, L, a.min_len, out, ll, c, n_ext);
-        a.ll[u] = ll;
-        a.cnt[u] = c;
+        const int64_t o0 = of[r], len = of[r + 1] - o0;
+        if (len > kMemMaxLen) atomicOr(reinterpret_cast<uint32_t*>(a.n_ext) + 2, 1u);
+        Walk w[NW];
+#pragma unroll
+        for (int j = 0; j < NW; ++j) {
+            w[j].sq = (set ? a.seq1 : a.seq0) + o0;
+            w[j].L = len > kMemMaxLen ? 0 : (int32_t)len;
+            w[j].from = 0;
+            w[j].ll = 0.0;
+            w[j].cnt = 0;
+            if (w[j].L > 0) walk_start(j ? a.ix1 : a.ix0, s_llk[j], w[j]);
+        }
+        int64_t* out = ROWS ? a.rows + 6 * a.slot[u] : nullptr;
+        for (;;) {
+            Bkt k[NW];
+            bool live[NW];
+            bool any = false;
+#pragma unroll
+            for (int j = 0; j < NW; ++j) {
+                live[j] = w[j].from < w[j].L;
+                any |= live[j];
+                if (live[j]) mem_load(j ? a.ix1 : a.ix0, w[j].Q, w[j].S, k[j]);
+            }
+            if (!any) break;
+            int nn[NW];
+#pragma unroll
+            for (int j = 0; j < NW; ++j) nn[j] = live[j] && w[j].to + 1 < w[j].L ? w[j].sq[w[j].to + 1] : 0;
+#pragma unroll
+            for (int j = 0; j < NW; ++j) {
+                if (!live[j]) continue;
+                if (j)
+                    walk_step<ROWS>(a.ix1, s_llk[1], a.thr1, a.all1, a.min_len, k[j], nn[j], w[j], out, n_ext);
+                else
+                    walk_step<ROWS>(a.ix0, s_llk[0], a.thr0, a.all0, a.min_len, k[j], nn[j], w[j], out, n_ext);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NW; ++j) {
+            a.ll[j * per_idx + u] = w[j].ll;
+            a.cnt[j * per_idx + u] = w[j].cnt;
+        }
     }
     unsigned long long e = n_ext;
 #pragma unroll
@@ -255,7 +324,6 @@ int mem_launch(msg_ctx* ctx, const msg_ctx* bg, const Set* sets, int n_set, int6
         rc = evalue_threshold(bg->idx.dev.n, p->max_evalue, &a.thr1, &a.all1);
         if (rc != MSG_OK) return ctx->fail(rc, "e-value threshold");
     }
-    a.n_idx = n_idx;
     a.n_set = n_set;
     a.seq0 = sets[0].seq; a.off0 = sets[0].off;
     a.seq1 = n_set > 1 ? sets[1].seq : sets[0].seq;
@@ -273,7 +341,11 @@ int mem_launch(msg_ctx* ctx, const msg_ctx* bg, const Set* sets, int n_set, int6
     e = cudaMemsetAsync(ctx->status.p, 0, 128, ctx->stream);
     if (e != cudaSuccess) return ctx->cuda_fail(e);
     if (n_units > 0) {
-        k_mems<<<nblk(n_units, 256), 256, 0, ctx->stream>>>(a);
+        cudaStream_t st = ctx->stream;
+        const int64_t g = nblk(n * n_set, 256);
+        if (n_idx == 1 && d_rows) k_mems<1, true><<<g, 256, 0, st>>>(a);
+        else if (n_idx == 1) k_mems<1, false><<<g, 256, 0, st>>>(a);
+        else k_mems<2, false><<<g, 256, 0, st>>>(a);
         ctx->stats.n_launch++;
         e = cudaGetLastError();
         if (e != cudaSuccess) return ctx->cuda_fail(e);
@@ -291,10 +363,12 @@ void stats_begin(msg_ctx* ctx, int64_t n_reads) {
 
 int stats_end(msg_ctx* ctx) {
     cudaEventRecord(ctx->ev[2], ctx->stream);
-    unsigned long long n_ext = 0;
-    cudaError_t e = cudaMemcpyAsync(&n_ext, ctx->status.p, 8, cudaMemcpyDeviceToHost, ctx->stream);
+    unsigned long long st[2] = {0, 0};  // extensions, error bits
+    cudaError_t e = cudaMemcpyAsync(st, ctx->status.p, 16, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return ctx->cuda_fail(e);
+    const unsigned long long n_ext = st[0];
+    if (st[1] & 1u) return ctx->fail(MSG_EUNSUPPORTED, "a read of 2^31 - 2 bases or more");
     float t0 = 0, t1 = 0;
     cudaEventElapsedTime(&t0, ctx->ev[0], ctx->ev[1]);
     cudaEventElapsedTime(&t1, ctx->ev[0], ctx->ev[2]);

@@ -358,7 +358,7 @@ class Context:
         if rev_seq is not None:
             rev_seq = np.ascontiguousarray(rev_seq, dtype=np.uint8)
             rev_off = np.ascontiguousarray(rev_off, dtype=np.int64)
-            rb = ReadBatch(n, _p(rev_seq, u8p), _p(rev_off, i64p))
+            rb = ReadBatch(len(rev_off) - 1, _p(rev_seq, u8p), _p(rev_off, i64p))  # the library checks the counts
         return self._clean(self.lib.msg_clean_batch, bg, n, fb, rb, params, min_lod)
 
     def clean_device(self, bg: "Context", seq_ptr: int, off_ptr: int, n: int, rev_seq_ptr: int | None = None,
