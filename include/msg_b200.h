@@ -297,6 +297,50 @@ int msg_band_train(msg_ctx* ctx, const float* feat, const int32_t* label, int64_
 int msg_band_grad(msg_ctx* ctx, const float* params, const float* feat, const int32_t* label, int64_t n,
                   float* grad, float* loss);
 
+/* ---- Host tail of the single-end task (runs on host threads, no GPU) ---- */
+
+typedef struct msg_tail_params {
+    double min_score_rate;  /* -s: Alignment::filter rate (0.65) */
+    uint32_t max_report;    /* -k: records per read (1); 0 for every alignment */
+    int32_t n_threads;      /* host threads; 0 for all hardware threads */
+    double gap_open, gap_ext, clip;  /* ScoreScheme gapO, gapE (5, 2) and clip penalty (4) */
+} msg_tail_params;
+
+void msg_tail_params_default(msg_tail_params* p);
+
+/* One SAM record as msgseqtk-align writes it: exportBAM
+ * (src/Alignment.cpp:429-444) plus output's flags and tags
+ * (src/msgseqtk-align.cpp:538-556), or an unmapped record (flag 0x4, tid -1,
+ * no CIGAR or tags; :583-585). SEQ and QUAL are the read's, reverse-
+ * complemented and reversed when flag has 0x10. CIGAR words are the input
+ * records' (cigar[cigar_off .. +n_cigar)); the MD:Z text is md[md_off ..
+ * +md_len). XH:f and XP:f are float32 as the reference stores them. */
+typedef struct msg_sam_rec {
+    int64_t read;           /* read index in the batch */
+    int32_t flag, tid;
+    int64_t pos;            /* 0-based leftmost target position (alnStart) */
+    int32_t mapq;
+    int32_t as;             /* AS:i alignment score */
+    float xh, xp;           /* XH:f log10 likelihood, XP:f posterior probability */
+    int32_t nh, xn;         /* NH:i reported records of the read, XN:i alignments kept */
+    int64_t cigar_off;
+    int32_t n_cigar, md_len;
+    int64_t md_off;
+} msg_sam_rec;
+
+/* msgseqtk-align's per-read tail (src/msgseqtk-align.cpp:619-628): on each
+ * read's records from msg_map_batch (aln, cigar, read_aln_off as returned),
+ * Alignment::filter, evaluate, calcMapQ and sort (src/Alignment.cpp:446-555,
+ * src/Alignment.h:629-633), then the reported records in output order. quals
+ * holds phred values (not ASCII) at the reads' offsets (NULL: all 0); mtg
+ * gives the forward chromosome sequences. Records go to out (out_cap), MD
+ * texts to md (md_cap bytes); *n_out and *md_len receive the sizes needed,
+ * and MSG_EINVAL is returned with nothing written when either exceeds its
+ * capacity. Host memory only; threads as p->n_threads. */
+int msg_tail_batch(const msg_mtg_view* mtg, const msg_read_batch* reads, const uint8_t* quals, const msg_aln* aln,
+                   const uint32_t* cigar, const int64_t* read_aln_off, const msg_tail_params* p, msg_sam_rec* out,
+                   int64_t out_cap, char* md, int64_t md_cap, int64_t* n_out, int64_t* md_len);
+
 /* ---- MEM search and read cleaning (msgseqtk-clean) ---- */
 
 typedef struct msg_mem_params {

@@ -1,8 +1,9 @@
 """SAM records: alignment records fed through the reference's own tail
 (filter, evaluate, calcMapQ, sort, exportBAM and msgseqtk-align's per-read
 output) must give the same SAM fields as the reference's whole single-end
-path. On the CPU the records come from the oracle; on the GPU (-m gpu) from
-the CUDA library through the C ABI."""
+path, and the library's own host tail (msg_tail_batch) must give the same
+fields as the reference's tail. On the CPU the records come from the oracle;
+on the GPU (-m gpu) from the CUDA library through the C ABI."""
 import os
 
 import numpy as np
@@ -42,6 +43,72 @@ def _workload(seed):
     return g, reads, seq, qual, off
 
 
+_COMP = np.array([0, 8, 4, 12, 2, 10, 6, 14, 1, 9, 5, 13, 3, 11, 7, 15], dtype=np.uint8)
+
+
+def _ours_as_fields(recs, md, seq, qual, off, cigar):
+    """The library's tail records as the fields of the reference harness's
+    lines: QNAME FLAG TID POS MAPQ CIGAR L_SEQ SEQ QUAL then aux (floats as
+    float values, compared exactly)."""
+    rows = []
+    for r in recs:
+        i = int(r["read"])
+        q = seq[off[i]:off[i + 1]]
+        ql = qual[off[i]:off[i + 1]]
+        if r["flag"] & 0x10:
+            q, ql = _COMP[q[::-1]], ql[::-1]
+        cg = cigar[r["cigar_off"]:r["cigar_off"] + r["n_cigar"]] if r["n_cigar"] else []
+        cs = "".join(f"{int(c) >> 4}{'MIDNSHP=XB'[int(c) & 15]}" for c in cg) or "*"
+        f = [f"r{i}", str(int(r["flag"])), str(int(r["tid"])), str(int(r["pos"])), str(int(r["mapq"])), cs,
+             str(len(q)), "".join(f"{int(x):x}" for x in q), "".join(f"{int(x):02x}" for x in ql)]
+        if not r["flag"] & 0x4:
+            m = md[r["md_off"]:r["md_off"] + r["md_len"]].decode()
+            f += [f"AS:i:{int(r['as'])}", f"MD:Z:{m}", ("XH", float(r["xh"])), f"NH:i:{int(r['nh'])}",
+                  f"XN:i:{int(r['xn'])}", ("XP", float(r["xp"]))]
+        rows.append(f)
+    return rows
+
+
+def _ref_as_fields(lines):
+    rows = []
+    for line in lines:
+        f = line.split("\t")
+        out = f[:9]
+        for a in f[9:]:
+            tag, typ, val = a.split(":", 2)
+            out.append((tag, float.fromhex(val)) if typ == "f" else a)
+        rows.append(out)
+    return rows
+
+
+def _check_tail(view, ref, seq, qual, off, aln, cig, roff, rate, max_report):
+    from msgseqtk_b200 import lib
+    exp = _ref_as_fields(ref.sam_from_records(seq, qual, off, aln, cig, roff, min_score_rate=rate,
+                                              max_report=max_report))
+    for nt in (1, 3):
+        recs, md = lib.tail(view, seq, off, qual, aln, cig, roff,
+                            lib.tail_params(min_score_rate=rate, max_report=max_report, n_threads=nt))
+        got = _ours_as_fields(recs, md, seq, qual, off, cig)
+        assert len(got) == len(exp)
+        for g, e in zip(got, exp):
+            assert g == e, (g, e)
+
+
+@needs_ref
+def test_library_tail_matches_reference_tail_on_oracle_records(oracle_built):
+    """msg_tail_batch (host C++ in the library) against the reference's own
+    filter/evaluate/calcMapQ/sort/output on the same records: every field,
+    float tags to the bit."""
+    from msgseqtk_b200 import index_build
+    g, reads, seq, qual, off = _workload(9)
+    ref = Reference(g)
+    view = index_build.build_view(g)
+    orc = Oracle(view)
+    aln, cig, roff = _records_from_oracle(orc, reads)
+    for rate, max_report in ((0.65, 1), (0.65, 0), (0.3, 3), (-1.0, 0)):
+        _check_tail(view, ref, seq, qual, off, aln, cig, roff, rate, max_report)
+
+
 @needs_ref
 def test_tail_on_oracle_records_matches_reference(oracle_built):
     from msgseqtk_b200 import index_build
@@ -73,5 +140,7 @@ def test_gpu_records_give_reference_sam():
                 got = ref.sam_from_records(seq, qual, off, res["aln"], res["cigar"], res["read_aln_off"],
                                            max_report=max_report)
                 assert got == exp
+                _check_tail(view, ref, seq, qual, off, res["aln"], res["cigar"], res["read_aln_off"], 0.65,
+                            max_report)
     finally:
         ctx.close()
