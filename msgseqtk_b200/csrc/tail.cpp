@@ -54,6 +54,13 @@ struct ReadOut {
     std::string md;
 };
 
+inline void put_count(std::string& s, uint32_t v) {  // boost::lexical_cast<string>(uint32_t)
+    char b[10];
+    int n = 0;
+    do { b[n++] = (char)('0' + v % 10); v /= 10; } while (v);
+    while (n) s.push_back(b[--n]);
+}
+
 // Alignment::getAlnMDTag (src/Alignment.cpp:305-353): runs of '=' as counts,
 // a mismatch as the count then the target base, an insertion as the count
 // (at its start) then '^' and the inserted query bases; deletions add
@@ -70,13 +77,13 @@ void md_tag(const uint8_t* q, const uint8_t* t, int64_t i, int64_t j, const uint
             switch (o) {
                 case 7: ++i; ++j; ++len; break;
                 case 8:
-                    md += std::to_string(len);
+                    put_count(md, len);
                     len = 0;
                     md.push_back(kDecode[t[j] & 15]);
                     ++i; ++j;
                     break;
                 case kOpI:
-                    if (prev != kOpI) md += std::to_string(len);
+                    if (prev != kOpI) put_count(md, len);
                     len = 0;
                     if (o != prev) md.push_back('^');
                     md.push_back(kDecode[q[i] & 15]);
@@ -88,7 +95,7 @@ void md_tag(const uint8_t* q, const uint8_t* t, int64_t i, int64_t j, const uint
             prev = o;
         }
     }
-    md += std::to_string(len);
+    put_count(md, len);
 }
 
 // Alignment::evaluate (src/Alignment.cpp:446-489) over the record's path.
@@ -106,13 +113,15 @@ double evaluate(const uint8_t* q, const uint8_t* qual, int64_t L, const uint8_t*
     for (int32_t w = 0; w < a.n_cigar; ++w) {
         const int op = cg[w] & 0xf;
         if (op == kOpS) continue;
-        for (uint32_t r = 0; r < (cg[w] >> 4); ++r) {
+        const uint32_t run = cg[w] >> 4;
+        if (op == kOpM) {  // query bases of an M run lie inside the read (checked)
+            for (uint32_t r = 0; r < run; ++r, ++i, ++j) ll += (q[i] & t[j]) ? T.match[qual[i]] : T.mis[qual[i]];
+            if (run) prev = kOpM;
+            continue;
+        }
+        for (uint32_t r = 0; r < run; ++r) {
             const int qv = i < L ? qual[i] : 0;  // a QualStr reads its terminator at L
             switch (op) {
-                case kOpM:
-                    ll += (q[i] & t[j]) ? T.match[qv] : T.mis[qv];
-                    ++i; ++j;
-                    break;
                 case kOpI:
                     if (prev != kOpI) ll += T.mis[qv] - p.gap_open;
                     ll += -p.gap_ext;
@@ -163,12 +172,16 @@ void tail_read(int64_t r, const uint8_t* seq, const uint8_t* qual, int64_t L, co
         out.rec.push_back(u);
         return;
     }
-    rc.resize(L);
+    bool any_rev = false;
+    for (int64_t k : keep) any_rev |= aln[k].strand == 2;
     rq.resize(2 * L);  // reversed quality, then zeros for reads without one
-    for (int64_t i = 0; i < L; ++i) {  // PrimarySeq::revcom: reversed, complemented; quality reversed
-        rc[i] = kComp[seq[L - 1 - i] & 15];
-        rq[i] = qual ? qual[L - 1 - i] : 0;
-        rq[L + i] = 0;
+    if (!qual) std::fill(rq.begin() + L, rq.end(), 0);
+    if (any_rev) {  // PrimarySeq::revcom: reversed, complemented; quality reversed
+        rc.resize(L);
+        for (int64_t i = 0; i < L; ++i) {
+            rc[i] = kComp[seq[L - 1 - i] & 15];
+            rq[i] = qual ? qual[L - 1 - i] : 0;
+        }
     }
     const uint8_t* fq = qual ? qual : rq.data() + L;
     const size_t N = keep.size();
@@ -192,17 +205,25 @@ void tail_read(int64_t r, const uint8_t* seq, const uint8_t* qual, int64_t L, co
     }
     // Alignment::calcMapQ (src/Alignment.cpp:491-512); loglik = log10lik / log10(e)
     std::vector<double>& pr = sc.pr;
-    for (size_t n = 0; n < N; ++n) pr[n] = l10[n] / std::log10(M_E);
+    static const double log10e = std::log10(M_E);
+    for (size_t n = 0; n < N; ++n) pr[n] = l10[n] / log10e;
     double maxV = pr[0];
     for (double x : pr) if (x > maxV) maxV = x;
     const double scale = maxV != -INFINITY && maxV < kMinLoglikExp ? kMinLoglikExp - maxV : 0;
-    for (double& x : pr) x = std::exp(x + scale);
-    double sum = 0;
-    for (double x : pr) sum += x;
-    for (size_t n = 0; n < N; ++n) {
-        post[n] = pr[n] / sum;
-        const double mq = kPhredScale * std::log10(1 - post[n]);
-        mapq[n] = (int)(uint8_t)std::min(std::round(mq), kMaxQ);
+    if (N == 1 && std::isfinite(pr[0]) && pr[0] + scale < 700) {
+        // exp(x + scale) is finite and above 0 (x + scale >= -256), so postP = pr / pr = 1 and
+        // MAPQ = min(round(-10 * log10(0)), 250) = 250
+        post[0] = 1.0;
+        mapq[0] = (int)kMaxQ;
+    } else {
+        for (double& x : pr) x = std::exp(x + scale);
+        double sum = 0;
+        for (double x : pr) sum += x;
+        for (size_t n = 0; n < N; ++n) {
+            post[n] = pr[n] / sum;
+            const double mq = kPhredScale * std::log10(1 - post[n]);
+            mapq[n] = (int)(uint8_t)std::min(std::round(mq), kMaxQ);
+        }
     }
     // Alignment::sort (src/Alignment.h:629-633): std::sort by log10P, decreasing
     std::vector<size_t>& ord = sc.ord;
@@ -258,13 +279,13 @@ extern "C" int msg_tail_batch(const msg_mtg_view* mtg, const msg_read_batch* rea
     std::vector<Target> tg(mtg->n_chrom);
     for (int64_t t = 0; t < mtg->n_chrom; ++t) tg[t] = Target{mtg->chr_seq + mtg->chr_off[t], mtg->chr_len[t]};
     // every record must lie inside its read, its chromosome and the CIGAR array
-    for (int64_t i = 0; i < n; ++i) {
+    auto valid = [&](int64_t i) {
         const int64_t L = reads->off[i + 1] - reads->off[i];
-        if (L < 0 || read_aln_off[i + 1] < read_aln_off[i]) return MSG_EINVAL;
+        if (L < 0 || read_aln_off[i + 1] < read_aln_off[i]) return false;
         for (int64_t k = read_aln_off[i]; k < read_aln_off[i + 1]; ++k) {
             const msg_aln& a = aln[k];
             if (a.tid < 0 || a.tid >= mtg->n_chrom || a.aln_from < 0 || a.aln_start < 0 || a.n_cigar < 0)
-                return MSG_EINVAL;
+                return false;
             int64_t qi = 0, tj = 0;
             for (int32_t w = 0; w < a.n_cigar; ++w) {
                 const uint32_t c = cigar[a.cigar_off + w];
@@ -272,41 +293,51 @@ extern "C" int msg_tail_batch(const msg_mtg_view* mtg, const msg_read_batch* rea
                 if (op == kOpM) { qi += c >> 4; tj += c >> 4; }
                 else if (op == kOpI) qi += c >> 4;
                 else if (op == kOpD) tj += c >> 4;
-                else if (op != kOpS) return MSG_EINVAL;
+                else if (op != kOpS) return false;
             }
-            if (a.aln_from + qi > L || a.aln_start + tj > tg[a.tid].len) return MSG_EINVAL;
+            if (a.aln_from + qi > L || a.aln_start + tj > tg[a.tid].len) return false;
         }
-    }
+        return true;
+    };
     int nt = p->n_threads > 0 ? p->n_threads : (int)std::max(1u, std::thread::hardware_concurrency());
     nt = (int)std::max<int64_t>(1, std::min<int64_t>(nt, (n + 255) / 256));
     std::vector<ReadOut> parts(nt);
+    std::vector<char> bad(nt, 0);
     auto work = [&](int w) {
         Scratch sc;
         const int64_t a = n * w / nt, b = n * (w + 1) / nt;
         parts[w].rec.reserve((size_t)(b - a) * std::max<uint32_t>(1, p->max_report));
         for (int64_t i = a; i < b; ++i) {
+            if (!valid(i)) { bad[w] = 1; return; }
             const int64_t o = reads->off[i];
             tail_read(i, reads->seq + o, quals ? quals + o : nullptr, reads->off[i + 1] - o, aln, read_aln_off[i],
                       read_aln_off[i + 1], cigar, tg, *p, sc, parts[w]);
         }
     };
-    std::vector<std::thread> th;
-    for (int w = 1; w < nt; ++w) th.emplace_back(work, w);
-    work(0);
-    for (auto& t : th) t.join();
-    int64_t nr = 0, nm = 0;
-    for (const ReadOut& r : parts) { nr += (int64_t)r.rec.size(); nm += (int64_t)r.md.size(); }
-    *n_out = nr;
-    *md_len = nm;
-    if (nr > out_cap || nm > md_cap || (nr > 0 && !out) || (nm > 0 && !md)) return MSG_EINVAL;
-    int64_t ro = 0, mo = 0;
-    for (const ReadOut& r : parts) {
-        for (msg_sam_rec x : r.rec) {
-            x.md_off += mo;
-            out[ro++] = x;
-        }
-        if (!r.md.empty()) std::memcpy(md + mo, r.md.data(), r.md.size());
-        mo += (int64_t)r.md.size();
+    auto run = [&](auto fn) {
+        std::vector<std::thread> th;
+        for (int w = 1; w < nt; ++w) th.emplace_back(fn, w);
+        fn(0);
+        for (auto& t : th) t.join();
+    };
+    run(work);
+    for (char x : bad) if (x) return MSG_EINVAL;
+    std::vector<int64_t> ro(nt + 1, 0), mo(nt + 1, 0);
+    for (int w = 0; w < nt; ++w) {
+        ro[w + 1] = ro[w] + (int64_t)parts[w].rec.size();
+        mo[w + 1] = mo[w] + (int64_t)parts[w].md.size();
     }
+    *n_out = ro[nt];
+    *md_len = mo[nt];
+    if (ro[nt] > out_cap || mo[nt] > md_cap || (ro[nt] > 0 && !out) || (mo[nt] > 0 && !md)) return MSG_EINVAL;
+    run([&](int w) {  // each thread places its own records and MD text
+        msg_sam_rec* o = out + ro[w];
+        for (const msg_sam_rec& x : parts[w].rec) {
+            *o = x;
+            o->md_off += mo[w];
+            ++o;
+        }
+        if (!parts[w].md.empty()) std::memcpy(md + mo[w], parts[w].md.data(), parts[w].md.size());
+    });
     return MSG_OK;
 }
