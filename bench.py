@@ -647,12 +647,16 @@ def main():
     e2e = {"value": e2e_reads / (ms_e2e / 1000.0), "unit": "reads/s", "h2d_bytes_per_step": int(h2d // args.steps),
            "d2h_bytes_per_step": int(d2h // args.steps)}
 
-    # to SAM records: the same calls, with the library's host tail (filter,
-    # evaluate, calcMapQ, sort, output fields) of batch k on host threads
-    # while the GPU maps batch k + 1; wall clock, since the host work counts
+    # to SAM records: the same calls, with the library's host tail of batch k
+    # on host threads while the GPU maps batch k + 1 (wall clock, since the
+    # host work counts). Pairs (scale workload): msgseqtk-align's paired-end
+    # tail with -m 400 -d 50 (insert range [-100, 900]); single reads: the
+    # single-end tail.
     from concurrent.futures import ThreadPoolExecutor
     tail_threads = max(1, (os.cpu_count() or 2) - 1)
     tprm = lib.tail_params(min_score_rate=args.min_score, max_report=1, n_threads=tail_threads)
+    pairing = lib.pair_params(mean=400.0, sd=50.0, min_ins=-100.0, max_ins=900.0) if args.workload == "scale" \
+        else None
     bufs = [(np.zeros(8 * bp, dtype=lib.ALN_DTYPE), np.zeros(64 * bp, dtype=np.uint32), np.zeros(bp + 1, np.int64))
             for _ in range(2)]
     n_sam = 0
@@ -664,7 +668,8 @@ def main():
         na, nc = ctx.map_into(h_seq[a:b], h_offs[k], al, cg, ro, params)
         if fut is not None:
             fut.result()
-        return pool.submit(lib.tail, view, h_seq[a:b], h_offs[k], reads.quals[a:b], al[:na], cg[:nc], ro, tprm)
+        return pool.submit(lib.tail, view, h_seq[a:b], h_offs[k], reads.quals[a:b], al[:na], cg[:nc], ro, tprm,
+                           pairing)
 
     with ThreadPoolExecutor(1) as pool:
         fut = sam_step(0, pool, None)
@@ -679,8 +684,10 @@ def main():
         t1 = time.perf_counter()
     ms_sam, n_sam = reduce_over_ranks(1000.0 * (t1 - t0), float(n_sam), "cuda")
     e2e_sam = {"value": n_sam / (ms_sam / 1000.0), "unit": "reads/s", "tail_threads": tail_threads,
-               "timing": "wall clock: msg_map_batch from pinned host reads, then msg_tail_batch of that batch on "
-                         "host threads overlapped with the next batch's mapping; ends with every SAM record built",
+               "timing": "wall clock: msg_map_batch from pinned host reads, then the host tail of that batch "
+                         "(msg_tail_pe_batch for pairs, -m 400 -d 50; msg_tail_batch for single reads) on host "
+                         "threads overlapped with the next batch's mapping; ends with every SAM record built",
+               "tail": "paired-end" if pairing is not None else "single-end",
                "records_last_step": int(len(recs))}
 
     # roofline of the dominant stage

@@ -326,6 +326,8 @@ typedef struct msg_sam_rec {
     int64_t cigar_off;
     int32_t n_cigar, md_len;
     int64_t md_off;
+    int32_t isize;          /* TLEN: pairs only (AlignmentPE::exportFwdBAM/exportRevBAM) */
+    int32_t pad;
 } msg_sam_rec;
 
 /* msgseqtk-align's per-read tail (src/msgseqtk-align.cpp:619-628): on each
@@ -340,6 +342,36 @@ typedef struct msg_sam_rec {
 int msg_tail_batch(const msg_mtg_view* mtg, const msg_read_batch* reads, const uint8_t* quals, const msg_aln* aln,
                    const uint32_t* cigar, const int64_t* read_aln_off, const msg_tail_params* p, msg_sam_rec* out,
                    int64_t out_cap, char* md, int64_t md_cap, int64_t* n_out, int64_t* md_len);
+
+/* Pairing of msgseqtk-align's paired-end mode: AlignmentPE::ps as the
+ * program leaves it after its options (-m/-d/-I/-X, src/msgseqtk-align.cpp:
+ * 267-300, 400; an sd of 0 becomes mean * 0.1 and a mean of 0 makes every
+ * insert size equally likely, PairingScheme::updateParam) and the pair
+ * filters (--no-mixed, --no-discordant, --no-tail-over, --no-contain,
+ * --no-overlap, --max-npair; 0 = no limit). The insert-size density is the
+ * normal pdf exp(-z^2/2) / (sd sqrt(2 pi)). */
+typedef struct msg_pair_params {
+    double mean, sd, min_ins, max_ins;
+    int32_t no_mixed, no_discordant, no_tail_over, no_contain, no_overlap;
+    int32_t pad;
+    int64_t max_npair;
+} msg_pair_params;
+
+/* Defaults: mean 200, sd 20, inserts [0, 400], no filters. */
+void msg_pair_params_default(msg_pair_params* q);
+
+/* msgseqtk-align's paired-end tail (src/msgseqtk-align.cpp:703-748) for
+ * pairs whose mates are reads 2i and 2i+1 of the batch (n_reads even), on
+ * their records from msg_map_batch: Alignment::filter and evaluate per mate,
+ * AlignmentPE::getPairs/sort/filter/calcMapQ (src/Alignment.cpp:514-581) and
+ * the pair records (flags 0x1|0x2|0x40/0x80, the pair's MAPQ and XP, TLEN),
+ * or each mate's own records with flags 0x1|0x40/0x80 when no pair is left
+ * (unless no_mixed), or two unmapped records (flags 77 and 141) when neither
+ * mate keeps an alignment. Output as msg_tail_batch. */
+int msg_tail_pe_batch(const msg_mtg_view* mtg, const msg_read_batch* reads, const uint8_t* quals,
+                      const msg_aln* aln, const uint32_t* cigar, const int64_t* read_aln_off,
+                      const msg_tail_params* p, const msg_pair_params* q, msg_sam_rec* out, int64_t out_cap,
+                      char* md, int64_t md_cap, int64_t* n_out, int64_t* md_len);
 
 /* ---- MEM search and read cleaning (msgseqtk-clean) ---- */
 

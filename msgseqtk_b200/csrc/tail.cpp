@@ -141,118 +141,250 @@ double evaluate(const uint8_t* q, const uint8_t* qual, int64_t L, const uint8_t*
     return ll;
 }
 
-// Per-thread buffers reused across reads.
-struct Scratch {
-    std::vector<uint8_t> rc, rq;
-    std::vector<int64_t> keep;
-    std::vector<double> l10, post, pr;
+// One read's alignments after Alignment::filter and evaluate, with the
+// reverse-complemented read (PrimarySeq::revcom: bases reversed and
+// complemented, quality reversed) when a record needs it.
+struct Mate {
+    int64_t read = 0, L = 0;
+    const uint8_t* seq = nullptr;
+    const uint8_t* fq = nullptr;   // forward quality (zeros without one)
+    std::vector<uint8_t> rc, rq;   // reverse complement; reversed quality then zeros
+    std::vector<int64_t> keep;     // record indices kept by the filter, in record order
+    std::vector<double> l10;       // log10P of each kept record
+    std::vector<char> empty;       // a record without a path (evaluate skips it)
+    std::vector<double> pr, post;  // calcMapQ work and posterior
     std::vector<int> mapq;
-    std::vector<char> empty;
     std::vector<size_t> ord;
 };
 
-void tail_read(int64_t r, const uint8_t* seq, const uint8_t* qual, int64_t L, const msg_aln* aln, int64_t k0,
-               int64_t k1, const uint32_t* cigar, const std::vector<Target>& tg, const msg_tail_params& p,
-               Scratch& sc, ReadOut& out) {
+void mate_eval(Mate& m, int64_t r, const uint8_t* seq, const uint8_t* qual, int64_t L, const msg_aln* aln,
+               int64_t k0, int64_t k1, const uint32_t* cigar, const std::vector<Target>& tg,
+               const msg_tail_params& p) {
     static const uint8_t kComp[16] = {0, 8, 4, 12, 2, 10, 6, 14, 1, 9, 5, 13, 3, 11, 7, 15};
-    std::vector<uint8_t>& rc = sc.rc;
-    std::vector<uint8_t>& rq = sc.rq;
-    // Alignment::filter (src/Alignment.cpp:548-555)
-    std::vector<int64_t>& keep = sc.keep;
-    keep.clear();
-    for (int64_t k = k0; k < k1; ++k) {
+    m.read = r;
+    m.seq = seq;
+    m.L = L;
+    m.keep.clear();
+    for (int64_t k = k0; k < k1; ++k) {  // Alignment::filter (src/Alignment.cpp:548-555)
         const double score = aln[k].aln_score == INT32_MIN ? -INFINITY : (double)aln[k].aln_score;
-        if (!(score < L * p.min_score_rate)) keep.push_back(k);
+        if (!(score < L * p.min_score_rate)) m.keep.push_back(k);
     }
-    if (keep.empty()) {  // output(read, out): an unmapped record (src/msgseqtk-align.cpp:583-585)
-        msg_sam_rec u{};
-        u.read = r;
-        u.flag = kFlagUnmapped;
-        u.tid = -1;
-        out.rec.push_back(u);
-        return;
-    }
+    const size_t N = m.keep.size();
+    if (N == 0) return;
     bool any_rev = false;
-    for (int64_t k : keep) any_rev |= aln[k].strand == 2;
-    rq.resize(2 * L);  // reversed quality, then zeros for reads without one
-    if (!qual) std::fill(rq.begin() + L, rq.end(), 0);
-    if (any_rev) {  // PrimarySeq::revcom: reversed, complemented; quality reversed
-        rc.resize(L);
+    for (int64_t k : m.keep) any_rev |= aln[k].strand == 2;
+    m.rq.resize(2 * L);
+    if (!qual) std::fill(m.rq.begin() + L, m.rq.end(), 0);
+    if (any_rev) {
+        m.rc.resize(L);
         for (int64_t i = 0; i < L; ++i) {
-            rc[i] = kComp[seq[L - 1 - i] & 15];
-            rq[i] = qual ? qual[L - 1 - i] : 0;
+            m.rc[i] = kComp[seq[L - 1 - i] & 15];
+            m.rq[i] = qual ? qual[L - 1 - i] : 0;
         }
     }
-    const uint8_t* fq = qual ? qual : rq.data() + L;
-    const size_t N = keep.size();
-    sc.l10.resize(N);
-    sc.post.resize(N);
-    sc.pr.resize(N);
-    sc.mapq.resize(N);
-    sc.empty.resize(N);
-    sc.ord.resize(N);
-    std::vector<double>& l10 = sc.l10;
-    std::vector<double>& post = sc.post;
-    std::vector<int>& mapq = sc.mapq;
-    std::vector<char>& empty = sc.empty;
+    m.fq = qual ? qual : m.rq.data() + L;
+    m.l10.resize(N);
+    m.empty.resize(N);
     for (size_t n = 0; n < N; ++n) {
-        const msg_aln& a = aln[keep[n]];
+        const msg_aln& a = aln[m.keep[n]];
         const bool rev = a.strand == 2;
         bool e;
-        l10[n] = evaluate(rev ? rc.data() : seq, rev ? rq.data() : fq, L, tg[a.tid].seq, a, cigar + a.cigar_off, p,
-                          &e);
-        empty[n] = e;
+        m.l10[n] = evaluate(rev ? m.rc.data() : seq, rev ? m.rq.data() : m.fq, L, tg[a.tid].seq, a,
+                            cigar + a.cigar_off, p, &e);
+        m.empty[n] = e;
     }
-    // Alignment::calcMapQ (src/Alignment.cpp:491-512); loglik = log10lik / log10(e)
-    std::vector<double>& pr = sc.pr;
-    static const double log10e = std::log10(M_E);
-    for (size_t n = 0; n < N; ++n) pr[n] = l10[n] / log10e;
+}
+
+const double kLog10e = std::log10(M_E);
+
+// The posterior/MAPQ step shared by Alignment::calcMapQ and
+// AlignmentPE::calcMapQ (src/Alignment.cpp:491-537) on log-likelihoods pr:
+// shift by MIN_LOGLIK_EXP when all are below it, exp, normalise by the
+// left-to-right sum (pairs: 1/N each when the sum is 0), MAPQ =
+// min(round(phredP2Q(1 - postP)), 250).
+void posterior(std::vector<double>& pr, std::vector<double>& post, std::vector<int>& mapq, bool pairs) {
+    const size_t N = pr.size();
+    post.resize(N);
+    mapq.resize(N);
     double maxV = pr[0];
     for (double x : pr) if (x > maxV) maxV = x;
     const double scale = maxV != -INFINITY && maxV < kMinLoglikExp ? kMinLoglikExp - maxV : 0;
     if (N == 1 && std::isfinite(pr[0]) && pr[0] + scale < 700) {
-        // exp(x + scale) is finite and above 0 (x + scale >= -256), so postP = pr / pr = 1 and
-        // MAPQ = min(round(-10 * log10(0)), 250) = 250
+        // exp(x + scale) is finite and above 0 (x + scale >= -256), so postP =
+        // pr / pr = 1 and MAPQ = min(round(-10 * log10(0)), 250) = 250
         post[0] = 1.0;
         mapq[0] = (int)kMaxQ;
-    } else {
-        for (double& x : pr) x = std::exp(x + scale);
-        double sum = 0;
-        for (double x : pr) sum += x;
-        for (size_t n = 0; n < N; ++n) {
-            post[n] = pr[n] / sum;
-            const double mq = kPhredScale * std::log10(1 - post[n]);
-            mapq[n] = (int)(uint8_t)std::min(std::round(mq), kMaxQ);
-        }
+        return;
     }
-    // Alignment::sort (src/Alignment.h:629-633): std::sort by log10P, decreasing
-    std::vector<size_t>& ord = sc.ord;
-    for (size_t n = 0; n < N; ++n) ord[n] = n;
-    std::sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return l10[x] > l10[y]; });
+    for (double& x : pr) x = std::exp(x + scale);
+    double sum = 0;
+    for (double x : pr) sum += x;
+    for (size_t n = 0; n < N; ++n) {
+        post[n] = pairs && !(sum > 0) ? 1.0 / N : pr[n] / sum;
+        const double mq = kPhredScale * std::log10(1 - post[n]);
+        mapq[n] = (int)(uint8_t)std::min(std::round(mq), kMaxQ);
+    }
+}
+
+// The record exportBAM builds for kept alignment n of a mate (flags, MAPQ
+// and pair fields are set by the caller).
+msg_sam_rec export_rec(const Mate& m, size_t n, const msg_aln* aln, const uint32_t* cigar,
+                       const std::vector<Target>& tg, std::string& md) {
+    const msg_aln& a = aln[m.keep[n]];
+    msg_sam_rec o{};
+    o.read = m.read;
+    o.flag = a.strand == 2 ? kFlagReverse : 0;
+    o.tid = a.tid;
+    o.pos = a.aln_start;
+    o.as = (int32_t)std::round((double)a.aln_score);
+    o.xh = (float)m.l10[n];
+    o.cigar_off = a.cigar_off;
+    o.n_cigar = a.n_cigar;
+    o.md_off = (int64_t)md.size();
+    if (!m.empty[n])
+        md_tag(a.strand == 2 ? m.rc.data() : m.seq, tg[a.tid].seq, a.aln_from, a.aln_start, cigar + a.cigar_off,
+               a.n_cigar, md);
+    o.md_len = (int32_t)((int64_t)md.size() - o.md_off);
+    return o;
+}
+
+// calcMapQ + sort + output(alnList, out, maxReport, extraFlag) for one mate
+// (src/Alignment.cpp:491-512, src/Alignment.h:629-633,
+// src/msgseqtk-align.cpp:538-556).
+void mate_out(Mate& m, const msg_aln* aln, const uint32_t* cigar, const std::vector<Target>& tg,
+              const msg_tail_params& p, int extra, ReadOut& out) {
+    const size_t N = m.keep.size();
+    m.pr.resize(N);
+    for (size_t n = 0; n < N; ++n) m.pr[n] = m.l10[n] / kLog10e;  // Alignment::loglik
+    posterior(m.pr, m.post, m.mapq, false);
+    m.ord.resize(N);
+    for (size_t n = 0; n < N; ++n) m.ord[n] = n;
+    const std::vector<double>& l10 = m.l10;
+    std::sort(m.ord.begin(), m.ord.end(), [&](size_t x, size_t y) { return l10[x] > l10[y]; });
     const size_t num = p.max_report == 0 ? N : std::min<size_t>(p.max_report, N);
     for (size_t s = 0; s < num; ++s) {
-        const size_t n = ord[s];
-        const msg_aln& a = aln[keep[n]];
-        msg_sam_rec o{};
-        o.read = r;
-        o.flag = (a.strand == 2 ? kFlagReverse : 0) | (s > 0 ? kFlagSecondary : 0);
-        o.tid = a.tid;
-        o.pos = a.aln_start;
-        o.mapq = mapq[n];
-        o.as = (int32_t)std::round((double)a.aln_score);
-        o.xh = (float)l10[n];
-        o.xp = (float)post[n];
+        const size_t n = m.ord[s];
+        msg_sam_rec o = export_rec(m, n, aln, cigar, tg, out.md);
+        o.flag |= (s > 0 ? kFlagSecondary : 0) | extra;
+        o.mapq = m.mapq[n];
+        o.xp = (float)m.post[n];
         o.nh = (int32_t)num;
         o.xn = (int32_t)N;
-        o.cigar_off = a.cigar_off;
-        o.n_cigar = a.n_cigar;
-        o.md_off = (int64_t)out.md.size();
-        if (!empty[n]) {
-            const uint8_t* q = a.strand == 2 ? rc.data() : seq;
-            md_tag(q, tg[a.tid].seq, a.aln_from, a.aln_start, cigar + a.cigar_off, a.n_cigar, out.md);
-        }
-        o.md_len = (int32_t)((int64_t)out.md.size() - o.md_off);
         out.rec.push_back(o);
+    }
+}
+
+msg_sam_rec unmapped(int64_t r, int flag) {
+    msg_sam_rec u{};
+    u.read = r;
+    u.flag = flag;
+    u.tid = -1;
+    return u;
+}
+
+// Single-end task tail (src/msgseqtk-align.cpp:619-628).
+void tail_se(Mate& m, const msg_aln* aln, const uint32_t* cigar, const std::vector<Target>& tg,
+             const msg_tail_params& p, ReadOut& out) {
+    if (m.keep.empty()) {
+        out.rec.push_back(unmapped(m.read, kFlagUnmapped));  // output(read, out), :583-585
+        return;
+    }
+    mate_out(m, aln, cigar, tg, p, 0, out);
+}
+
+// PairingScheme::pr (src/PairingScheme.cpp:18-25) with the normal pdf
+// exp(-z^2 / 2) / (sd * sqrt(2 pi)), z = (x - mean) / sd.
+double pairing_pr(const msg_pair_params& q, double sd, double x) {
+    if (q.mean == 0) return 1;
+    if (q.min_ins <= x && x <= q.max_ins) {
+        const double z = (x - q.mean) / sd;
+        return std::exp(-0.5 * z * z) / (sd * std::sqrt(2.0 * M_PI));
+    }
+    return 0;
+}
+
+struct Pair {
+    size_t f, r;       // kept-record indices of the two mates
+    int32_t isize;
+    double l10, ll;    // AlignmentPE::log10lik and loglik
+};
+
+// Paired-end task tail (src/msgseqtk-align.cpp:703-748): AlignmentPE::getPairs,
+// sort, filter, calcMapQ and output(pairList) (src/Alignment.cpp:514-581,
+// src/Alignment.h:636-640, src/msgseqtk-align.cpp:558-581), or the unpaired
+// records of each mate, or an unmapped pair.
+void tail_pe(Mate& f, Mate& r, const msg_aln* aln, const uint32_t* cigar, const std::vector<Target>& tg,
+             const msg_tail_params& p, const msg_pair_params& q, double sd, std::vector<Pair>& pairs,
+             std::vector<double>& pr, std::vector<double>& post, std::vector<int>& mapq, ReadOut& out) {
+    constexpr int kPaired = 0x1, kProper = 0x2, kMateUnmapped = 0x8, kRead1 = 0x40, kRead2 = 0x80;
+    if (f.keep.empty() && r.keep.empty()) {  // output(fwdRead, revRead, out), :587-591
+        out.rec.push_back(unmapped(f.read, kFlagUnmapped | kMateUnmapped | kPaired | kRead1));
+        out.rec.push_back(unmapped(r.read, kFlagUnmapped | kMateUnmapped | kPaired | kRead2));
+        return;
+    }
+    pairs.clear();
+    for (size_t i = 0; i < f.keep.size(); ++i)  // getPairs: mates on different strands
+        for (size_t j = 0; j < r.keep.size(); ++j) {
+            const msg_aln& a = aln[f.keep[i]];
+            const msg_aln& b = aln[r.keep[j]];
+            if ((a.strand & b.strand) != 0) continue;
+            Pair x;
+            x.f = i;
+            x.r = j;
+            x.isize = a.tid != b.tid ? -1
+                                     : (int32_t)(std::max(a.aln_end, b.aln_end) - std::min(a.aln_start, b.aln_start));
+            const double ppr = pairing_pr(q, sd, (double)x.isize);
+            x.l10 = f.l10[i] + r.l10[j] + std::log10(ppr);
+            x.ll = f.l10[i] / kLog10e + r.l10[j] / kLog10e + std::log(ppr);
+            pairs.push_back(x);
+        }
+    std::sort(pairs.begin(), pairs.end(), [](const Pair& x, const Pair& y) { return x.l10 > y.l10; });
+    auto drop = [&](auto pred) { pairs.erase(std::remove_if(pairs.begin(), pairs.end(), pred), pairs.end()); };
+    drop([&](const Pair& x) { return !(q.min_ins <= x.isize && x.isize <= q.max_ins); });
+    auto A = [&](const Pair& x) -> const msg_aln& { return aln[f.keep[x.f]]; };
+    auto B = [&](const Pair& x) -> const msg_aln& { return aln[r.keep[x.r]]; };
+    if (q.no_discordant)
+        drop([&](const Pair& x) { return !(A(x).tid == B(x).tid && (A(x).strand & B(x).strand) == 0); });
+    if (q.no_tail_over)
+        drop([&](const Pair& x) {
+            const msg_aln &a = A(x), &b = B(x);
+            return (a.aln_start <= b.aln_start && a.aln_end > b.aln_start) ||
+                   (b.aln_start <= a.aln_start && b.aln_end > a.aln_start);
+        });
+    if (q.no_contain)
+        drop([&](const Pair& x) {
+            const msg_aln &a = A(x), &b = B(x);
+            return (a.aln_start <= b.aln_start && a.aln_end >= b.aln_end) ||
+                   (b.aln_start <= a.aln_start && b.aln_end >= a.aln_end);
+        });
+    if (q.no_overlap)
+        drop([&](const Pair& x) { return A(x).aln_start < B(x).aln_end && A(x).aln_end > B(x).aln_start; });
+    if (q.max_npair > 0 && (int64_t)pairs.size() > q.max_npair) pairs.resize(q.max_npair);
+    if (!pairs.empty()) {
+        const size_t N = pairs.size();
+        pr.resize(N);
+        for (size_t n = 0; n < N; ++n) pr[n] = pairs[n].ll;
+        posterior(pr, post, mapq, true);
+        const size_t num = p.max_report == 0 ? N : std::min<size_t>(p.max_report, N);
+        for (size_t s = 0; s < num; ++s) {
+            const Pair& x = pairs[s];
+            const bool fwd_first = A(x).aln_start < B(x).aln_start;
+            msg_sam_rec a = export_rec(f, x.f, aln, cigar, tg, out.md);  // exportFwdBAM
+            msg_sam_rec b = export_rec(r, x.r, aln, cigar, tg, out.md);  // exportRevBAM
+            a.flag |= kPaired | kProper | kRead1 | (s > 0 ? kFlagSecondary : 0);
+            b.flag |= kPaired | kProper | kRead2 | (s > 0 ? kFlagSecondary : 0);
+            a.isize = fwd_first ? x.isize : -x.isize;
+            b.isize = fwd_first ? -x.isize : x.isize;
+            a.mapq = b.mapq = mapq[s];
+            a.nh = b.nh = (int32_t)num;
+            a.xn = b.xn = (int32_t)N;
+            a.xp = b.xp = (float)post[s];
+            out.rec.push_back(a);
+            out.rec.push_back(b);
+        }
+    } else if (!q.no_mixed) {
+        if (!f.keep.empty()) mate_out(f, aln, cigar, tg, p, kPaired | kRead1, out);
+        if (!r.keep.empty()) mate_out(r, aln, cigar, tg, p, kPaired | kRead2, out);
     }
 }
 
@@ -268,14 +400,33 @@ extern "C" void msg_tail_params_default(msg_tail_params* p) {
     p->clip = 4;
 }
 
-extern "C" int msg_tail_batch(const msg_mtg_view* mtg, const msg_read_batch* reads, const uint8_t* quals,
-                              const msg_aln* aln, const uint32_t* cigar, const int64_t* read_aln_off,
-                              const msg_tail_params* p, msg_sam_rec* out, int64_t out_cap, char* md, int64_t md_cap,
-                              int64_t* n_out, int64_t* md_len) {
+extern "C" void msg_pair_params_default(msg_pair_params* q) {
+    if (!q) return;
+    // PairingScheme after msgseqtk-align's options without -m/-d/-I/-X
+    // (src/PairingScheme.h:34-37, 84-97; src/msgseqtk-align.cpp:267-300, 400)
+    q->mean = 200;
+    q->sd = 20;
+    q->min_ins = 0;
+    q->max_ins = 400;
+    q->no_mixed = q->no_discordant = q->no_tail_over = q->no_contain = q->no_overlap = 0;
+    q->max_npair = 0;
+}
+
+namespace {
+
+int tail_run(const msg_mtg_view* mtg, const msg_read_batch* reads, const uint8_t* quals, const msg_aln* aln,
+             const uint32_t* cigar, const int64_t* read_aln_off, const msg_tail_params* p,
+             const msg_pair_params* q, msg_sam_rec* out, int64_t out_cap, char* md, int64_t md_cap, int64_t* n_out,
+             int64_t* md_len) {
     if (!mtg || !reads || !read_aln_off || !p || !n_out || !md_len) return MSG_EINVAL;
     const int64_t n = reads->n_reads;
     if (n < 0 || (n > 0 && (!reads->seq || !reads->off))) return MSG_EINVAL;
+    if (q && (n % 2 != 0)) return MSG_EINVAL;
     if (std::isnan(p->min_score_rate)) return MSG_EINVAL;
+    // PairingScheme::updateParam (src/PairingScheme.h:72-78)
+    const double sd = q ? (q->mean == 0 ? 1 : q->sd == 0 ? q->mean * 0.1 : q->sd) : 0;
+    if (q && (std::isnan(q->mean) || std::isnan(sd) || std::isnan(q->min_ins) || std::isnan(q->max_ins)))
+        return MSG_EINVAL;
     std::vector<Target> tg(mtg->n_chrom);
     for (int64_t t = 0; t < mtg->n_chrom; ++t) tg[t] = Target{mtg->chr_seq + mtg->chr_off[t], mtg->chr_len[t]};
     // every record must lie inside its read, its chromosome and the CIGAR array
@@ -299,19 +450,34 @@ extern "C" int msg_tail_batch(const msg_mtg_view* mtg, const msg_read_batch* rea
         }
         return true;
     };
+    const int64_t units = q ? n / 2 : n;
     int nt = p->n_threads > 0 ? p->n_threads : (int)std::max(1u, std::thread::hardware_concurrency());
-    nt = (int)std::max<int64_t>(1, std::min<int64_t>(nt, (n + 255) / 256));
+    nt = (int)std::max<int64_t>(1, std::min<int64_t>(nt, (units + 127) / 128));
     std::vector<ReadOut> parts(nt);
     std::vector<char> bad(nt, 0);
+    auto prep = [&](Mate& m, int64_t i) {
+        const int64_t o = reads->off[i];
+        mate_eval(m, i, reads->seq + o, quals ? quals + o : nullptr, reads->off[i + 1] - o, aln, read_aln_off[i],
+                  read_aln_off[i + 1], cigar, tg, *p);
+    };
     auto work = [&](int w) {
-        Scratch sc;
-        const int64_t a = n * w / nt, b = n * (w + 1) / nt;
-        parts[w].rec.reserve((size_t)(b - a) * std::max<uint32_t>(1, p->max_report));
-        for (int64_t i = a; i < b; ++i) {
-            if (!valid(i)) { bad[w] = 1; return; }
-            const int64_t o = reads->off[i];
-            tail_read(i, reads->seq + o, quals ? quals + o : nullptr, reads->off[i + 1] - o, aln, read_aln_off[i],
-                      read_aln_off[i + 1], cigar, tg, *p, sc, parts[w]);
+        Mate m0, m1;
+        std::vector<Pair> pairs;
+        std::vector<double> pr, post;
+        std::vector<int> mapq;
+        const int64_t a = units * w / nt, b = units * (w + 1) / nt;
+        parts[w].rec.reserve((size_t)(b - a) * (q ? 2 : 1) * std::max<uint32_t>(1, p->max_report));
+        for (int64_t u = a; u < b; ++u) {
+            if (q) {
+                if (!valid(2 * u) || !valid(2 * u + 1)) { bad[w] = 1; return; }
+                prep(m0, 2 * u);
+                prep(m1, 2 * u + 1);
+                tail_pe(m0, m1, aln, cigar, tg, *p, *q, sd, pairs, pr, post, mapq, parts[w]);
+            } else {
+                if (!valid(u)) { bad[w] = 1; return; }
+                prep(m0, u);
+                tail_se(m0, aln, cigar, tg, *p, parts[w]);
+            }
         }
     };
     auto run = [&](auto fn) {
@@ -340,4 +506,21 @@ extern "C" int msg_tail_batch(const msg_mtg_view* mtg, const msg_read_batch* rea
         if (!parts[w].md.empty()) std::memcpy(md + mo[w], parts[w].md.data(), parts[w].md.size());
     });
     return MSG_OK;
+}
+
+}  // namespace
+
+extern "C" int msg_tail_batch(const msg_mtg_view* mtg, const msg_read_batch* reads, const uint8_t* quals,
+                              const msg_aln* aln, const uint32_t* cigar, const int64_t* read_aln_off,
+                              const msg_tail_params* p, msg_sam_rec* out, int64_t out_cap, char* md, int64_t md_cap,
+                              int64_t* n_out, int64_t* md_len) {
+    return tail_run(mtg, reads, quals, aln, cigar, read_aln_off, p, nullptr, out, out_cap, md, md_cap, n_out, md_len);
+}
+
+extern "C" int msg_tail_pe_batch(const msg_mtg_view* mtg, const msg_read_batch* reads, const uint8_t* quals,
+                                 const msg_aln* aln, const uint32_t* cigar, const int64_t* read_aln_off,
+                                 const msg_tail_params* p, const msg_pair_params* q, msg_sam_rec* out,
+                                 int64_t out_cap, char* md, int64_t md_cap, int64_t* n_out, int64_t* md_len) {
+    if (!q) return MSG_EINVAL;
+    return tail_run(mtg, reads, quals, aln, cigar, read_aln_off, p, q, out, out_cap, md, md_cap, n_out, md_len);
 }

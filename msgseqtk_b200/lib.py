@@ -30,13 +30,15 @@ EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy"
            "msg_db_views", "msg_db_free", "msg_index_bytes",
            "msg_map_params_default", "msg_map_batch", "msg_map_batch_device", "msg_last_stats",
            "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
-           "msg_band_train", "msg_band_grad", "msg_tail_params_default", "msg_tail_batch", "msg_mem_params_default", "msg_mem_batch", "msg_clean_batch",
+           "msg_band_train", "msg_band_grad", "msg_tail_params_default", "msg_tail_batch", "msg_pair_params_default", "msg_tail_pe_batch",
+           "msg_mem_params_default", "msg_mem_batch", "msg_clean_batch",
            "msg_clean_batch_device", "msg_occ_query", "msg_bi_ext_query", "msg_sa_query"]
 
 SAM_DTYPE = np.dtype([("read", "<i8"), ("flag", "<i4"), ("tid", "<i4"), ("pos", "<i8"), ("mapq", "<i4"),
                       ("as", "<i4"), ("xh", "<f4"), ("xp", "<f4"), ("nh", "<i4"), ("xn", "<i4"),
-                      ("cigar_off", "<i8"), ("n_cigar", "<i4"), ("md_len", "<i4"), ("md_off", "<i8")])
-assert SAM_DTYPE.itemsize == 72
+                      ("cigar_off", "<i8"), ("n_cigar", "<i4"), ("md_len", "<i4"), ("md_off", "<i8"),
+                      ("isize", "<i4"), ("pad", "<i4")])
+assert SAM_DTYPE.itemsize == 80
 
 # band model (include/msg_b200.h)
 BAND_FEATURES, BAND_HIDDEN, BAND_CLASSES, BAND_NPARAMS = 16, 64, 4, 5540
@@ -66,6 +68,12 @@ class BandTrainParams(C.Structure):
 class TailParams(C.Structure):
     _fields_ = [("min_score_rate", C.c_double), ("max_report", C.c_uint32), ("n_threads", C.c_int32),
                 ("gap_open", C.c_double), ("gap_ext", C.c_double), ("clip", C.c_double)]
+
+
+class PairParams(C.Structure):
+    _fields_ = [("mean", C.c_double), ("sd", C.c_double), ("min_ins", C.c_double), ("max_ins", C.c_double),
+                ("no_mixed", C.c_int32), ("no_discordant", C.c_int32), ("no_tail_over", C.c_int32),
+                ("no_contain", C.c_int32), ("no_overlap", C.c_int32), ("pad", C.c_int32), ("max_npair", C.c_int64)]
 
 
 class MemParams(C.Structure):
@@ -148,6 +156,10 @@ def load_library(path: str = LIB_PATH):
     L.msg_tail_batch.argtypes = [C.POINTER(MtgView), C.POINTER(ReadBatch), u8p, C.c_void_p, C.POINTER(C.c_uint32),
                                  i64p, C.POINTER(TailParams), C.c_void_p, C.c_int64, C.c_char_p, C.c_int64, i64p,
                                  i64p]
+    L.msg_pair_params_default.argtypes = [C.POINTER(PairParams)]
+    L.msg_pair_params_default.restype = None
+    L.msg_tail_pe_batch.argtypes = L.msg_tail_batch.argtypes[:7] + [C.POINTER(PairParams)] + \
+        L.msg_tail_batch.argtypes[7:]
     f64p = C.POINTER(C.c_double)
     L.msg_mem_params_default.argtypes = [C.POINTER(MemParams)]
     L.msg_mem_params_default.restype = None
@@ -196,9 +208,19 @@ def mtg_view(view):
     return MtgView(len(k[0]), _p(k[0], i64p), _p(k[1], i64p), _p(k[2], i64p), _p(k[3], u8p), _p(k[4], i64p)), k
 
 
-def tail(view, seq, off, qual, aln, cigar, read_aln_off, params: TailParams | None = None):
-    """msgseqtk-align's single-end tail (filter, evaluate, calcMapQ, sort,
-    output) on host threads: (records as SAM_DTYPE, MD text bytes)."""
+def pair_params(**kw) -> PairParams:
+    q = PairParams()
+    load_library().msg_pair_params_default(C.byref(q))
+    for k, v in kw.items():
+        setattr(q, k, v)
+    return q
+
+
+def tail(view, seq, off, qual, aln, cigar, read_aln_off, params: TailParams | None = None,
+         pairing: PairParams | None = None):
+    """msgseqtk-align's tail on host threads: single-end (filter, evaluate,
+    calcMapQ, sort, output), or paired-end when `pairing` is given (mates at
+    reads 2i and 2i+1). Returns (records as SAM_DTYPE, MD text bytes)."""
     L = load_library()
     params = params or tail_params()
     m, keep = mtg_view(view)
@@ -213,15 +235,17 @@ def tail(view, seq, off, qual, aln, cigar, read_aln_off, params: TailParams | No
     # a first guess that fits: one record per read or per alignment, an MD text
     # of at most two characters per query base plus the counts
     n = len(off) - 1
-    cap = n + (len(aln) if params.max_report != 1 else 0)
+    cap = n + (len(aln) if params.max_report != 1 or pairing is not None else 0)
     mcap = 2 * int(off[-1] - off[0]) * max(1, min(int(params.max_report) or len(aln) + 1, len(aln) + 1)) + 16 * cap
     while True:
         out = np.empty(max(cap, 1), dtype=SAM_DTYPE)  # untouched pages cost nothing
         md = np.empty(max(mcap, 1), dtype=np.uint8)
-        rc = L.msg_tail_batch(C.byref(m), C.byref(rb), _p(qual, u8p) if qual is not None else None,
-                              aln.ctypes.data, cigar.ctypes.data_as(C.POINTER(C.c_uint32)), _p(roff, i64p),
-                              C.byref(params), out.ctypes.data, cap, md.ctypes.data_as(C.c_char_p), mcap,
-                              C.byref(n_out), C.byref(md_len))
+        args = [C.byref(m), C.byref(rb), _p(qual, u8p) if qual is not None else None, aln.ctypes.data,
+                cigar.ctypes.data_as(C.POINTER(C.c_uint32)), _p(roff, i64p), C.byref(params)]
+        if pairing is not None:
+            args.append(C.byref(pairing))
+        args += [out.ctypes.data, cap, md.ctypes.data_as(C.c_char_p), mcap, C.byref(n_out), C.byref(md_len)]
+        rc = (L.msg_tail_pe_batch if pairing is not None else L.msg_tail_batch)(*args)
         if rc == MSG_EINVAL and (n_out.value > cap or md_len.value > mcap):
             cap, mcap = n_out.value, md_len.value
             continue

@@ -258,6 +258,16 @@ class Reference:
         L.ref_sam_batch.restype = C.c_int64
         L.ref_sam_batch.argtypes = [C.c_void_p, C.c_int64, u8p, u8p, i64p, C.c_int64, C.c_double, C.c_int64,
                                     C.c_double, C.c_int, C.c_char_p, C.c_int64]
+        ip = C.POINTER(C.c_int)
+        L.ref_sam_pe_batch.restype = C.c_int64
+        L.ref_sam_pe_batch.argtypes = [C.c_void_p, C.c_int64, u8p, u8p, i64p, C.c_int64, C.c_double, C.c_int64,
+                                       C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, ip,
+                                       C.c_int64, C.c_char_p, C.c_int64]
+        L.ref_sam_pe_from_records.restype = C.c_int64
+        L.ref_sam_pe_from_records.argtypes = [C.c_void_p, C.c_int64, u8p, u8p, i64p, C.c_void_p,
+                                              C.POINTER(C.c_uint32), i64p, C.c_double, C.c_int, C.c_double,
+                                              C.c_double, C.c_double, C.c_double, ip, C.c_int64, C.c_char_p,
+                                              C.c_int64]
         L.ref_sam_from_records.restype = C.c_int64
         L.ref_sam_from_records.argtypes = [C.c_void_p, C.c_int64, u8p, u8p, i64p, C.c_void_p, C.POINTER(C.c_uint32),
                                            i64p, C.c_double, C.c_int, C.c_char_p, C.c_int64]
@@ -426,6 +436,45 @@ class Reference:
         return self._text(lambda b, cap: self.lib.ref_sam_from_records(
             self.h, len(offs) - 1, _p(reads, u8p), _p(quals, u8p), _p(offs, i64p), aln.ctypes.data,
             cigar.ctypes.data_as(C.POINTER(C.c_uint32)), _p(roff, i64p), min_score_rate, max_report, b, cap))
+
+    @staticmethod
+    def _pairing(pairing):
+        """(mean, sd, min, max, opt[5], max_npair) from a dict; defaults are
+        PairingScheme's after msgseqtk-align's option handling without -m/-d:
+        mean 200, sd 20, range [0, 400], every pair kind allowed."""
+        p = dict(mean=200.0, sd=20.0, min=0.0, max=400.0, no_mixed=0, no_discordant=0, no_tail_over=0,
+                 no_contain=0, no_overlap=0, max_npair=0)
+        p.update(pairing or {})
+        opt = (C.c_int * 5)(p["no_mixed"], p["no_discordant"], p["no_tail_over"], p["no_contain"], p["no_overlap"])
+        return p["mean"], p["sd"], p["min"], p["max"], opt, p["max_npair"]
+
+    def sam_pe_batch(self, reads, quals, offs, min_len=17, max_evalue=0.01, max_nseed=500, min_score_rate=0.65,
+                     max_report=1, pairing=None):
+        """SAM records of the reference's paired-end path; reads 2i and 2i+1
+        are the mates of pair i."""
+        reads = np.ascontiguousarray(reads, dtype=np.uint8)
+        quals = np.ascontiguousarray(quals, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs, dtype=np.int64)
+        m, sd, lo, hi, opt, mx = self._pairing(pairing)
+        return self._text(lambda b, cap: self.lib.ref_sam_pe_batch(
+            self.h, (len(offs) - 1) // 2, _p(reads, u8p), _p(quals, u8p), _p(offs, i64p), min_len, max_evalue,
+            max_nseed, min_score_rate, max_report, m, sd, lo, hi, opt, mx, b, cap))
+
+    def sam_pe_from_records(self, reads, quals, offs, aln, cigar, read_aln_off, min_score_rate=0.65, max_report=1,
+                            pairing=None):
+        """The reference's paired-end tail on alignment records of the CUDA
+        library (mates at reads 2i, 2i+1)."""
+        reads = np.ascontiguousarray(reads, dtype=np.uint8)
+        quals = np.ascontiguousarray(quals, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs, dtype=np.int64)
+        aln = np.ascontiguousarray(aln)
+        cigar = np.ascontiguousarray(cigar, dtype=np.uint32)
+        roff = np.ascontiguousarray(read_aln_off, dtype=np.int64)
+        m, sd, lo, hi, opt, mx = self._pairing(pairing)
+        return self._text(lambda b, cap: self.lib.ref_sam_pe_from_records(
+            self.h, (len(offs) - 1) // 2, _p(reads, u8p), _p(quals, u8p), _p(offs, i64p), aln.ctypes.data,
+            cigar.ctypes.data_as(C.POINTER(C.c_uint32)), _p(roff, i64p), min_score_rate, max_report, m, sd, lo, hi,
+            opt, mx, b, cap))
 
     def map_batch(self, reads, quals, offs, n_threads=0, min_len=17, max_evalue=0.01, max_nseed=500,
                   min_score_rate=0.65):

@@ -406,7 +406,7 @@ int64_t ref_clean_batch(void* h_ref, void* h_bg, int64_t n_reads, const uint8_t*
  * per-read output step of msgseqtk-align (src/msgseqtk-align.cpp:538-556 for
  * mapped reads, :583-585 for unmapped ones), which lives in the program file
  * and is restated here. A line holds the BAM fields the shim records:
- * QNAME FLAG TID POS MAPQ CIGAR L_SEQ SEQ QUAL then the aux tags in order,
+ * QNAME FLAG TID POS MAPQ CIGAR L_SEQ SEQ QUAL ISIZE then the aux tags in order,
  * float tags as the hex of their float32 value, so comparisons are exact. */
 static void put_bam(const EGriceLab::SAMtools::BAM& b, std::string& out) {
     char buf[64];
@@ -423,6 +423,8 @@ static void put_bam(const EGriceLab::SAMtools::BAM& b, std::string& out) {
     for (uint8_t x : b.seq) { std::snprintf(buf, sizeof buf, "%x", (unsigned)x); out += buf; }
     out += "\t";
     for (uint8_t x : b.qual) { std::snprintf(buf, sizeof buf, "%02x", (unsigned)x); out += buf; }
+    std::snprintf(buf, sizeof buf, "\t%d", b.isize);
+    out += buf;
     for (const auto& a : b.aux) {
         out += "\t" + a.tag + ":" + a.type + ":";
         if (a.type == 'Z') out += a.str;
@@ -459,6 +461,121 @@ static int64_t put_out(const std::string& s, char* out, int64_t cap) {
     return (int64_t)s.size();
 }
 
+/* The paired-end output steps of msgseqtk-align (src/msgseqtk-align.cpp:558-581
+ * for pairs, :538-556 with extra flags for unpaired mates, :587-591 for an
+ * unmapped pair), restated (they live in the program file), and its per-pair
+ * tail after buildAlignments (:703-748). */
+static void sam_pair_out(const PAIR_LIST& pairs, uint32_t max_report, std::string& out) {
+    const size_t num = max_report == 0 ? pairs.size() : std::min<size_t>(max_report, pairs.size());
+    for (size_t i = 0; i < num; ++i) {
+        const AlignmentPE& pair = pairs[i];
+        EGriceLab::SAMtools::BAM f = pair.exportFwdBAM(), r = pair.exportRevBAM();
+        f.setSecondaryFlag(i > 0);
+        r.setSecondaryFlag(i > 0);
+        f.setAux(Alignment::NUM_REPORTED_ALIGNMENT_TAG, num);
+        f.setAux(Alignment::NUM_TOTAL_ALIGNMENT_TAG, pairs.size());
+        r.setAux(Alignment::NUM_REPORTED_ALIGNMENT_TAG, num);
+        r.setAux(Alignment::NUM_TOTAL_ALIGNMENT_TAG, pairs.size());
+        f.setAux(Alignment::ALIGNMENT_POSTERIOR_PROB_TAG, pair.postP);
+        r.setAux(Alignment::ALIGNMENT_POSTERIOR_PROB_TAG, pair.postP);
+        put_bam(f, out);
+        put_bam(r, out);
+    }
+}
+
+static void sam_list_out(const ALIGN_LIST& alns, uint32_t max_report, uint16_t extra, std::string& out) {
+    const size_t num = max_report == 0 ? alns.size() : std::min((size_t)max_report, alns.size());
+    for (size_t i = 0; i < num; ++i) {
+        EGriceLab::SAMtools::BAM b = alns[i].exportBAM();
+        b.setSecondaryFlag(i > 0);
+        b.setFlag(b.getFlag() | extra);
+        b.setAux(Alignment::NUM_REPORTED_ALIGNMENT_TAG, num);
+        b.setAux(Alignment::NUM_TOTAL_ALIGNMENT_TAG, alns.size());
+        b.setAux(Alignment::ALIGNMENT_POSTERIOR_PROB_TAG, alns[i].getPostP());
+        put_bam(b, out);
+    }
+}
+
+static void sam_pair(ALIGN_LIST& fa, ALIGN_LIST& ra, const PrimarySeq& f, const PrimarySeq& r, double min_score_rate,
+                     uint32_t max_report, const int* opt, int64_t max_npair, std::string& out) {
+    using EGriceLab::SAMtools::BAM;
+    Alignment::filter(fa, min_score_rate);
+    Alignment::filter(ra, min_score_rate);
+    if (fa.empty() && ra.empty()) {  // output(fwdRead, revRead, out)
+        put_bam(BAM(f.getName(), f.length(), dna::nt16Encode(f.getSeq()), f.getQual(),
+                    BAM_FUNMAP | BAM_FMUNMAP | BAM_FPAIRED | BAM_FREAD1), out);
+        put_bam(BAM(r.getName(), r.length(), dna::nt16Encode(r.getSeq()), r.getQual(),
+                    BAM_FUNMAP | BAM_FMUNMAP | BAM_FPAIRED | BAM_FREAD2), out);
+        return;
+    }
+    Alignment::evaluate(fa);
+    Alignment::evaluate(ra);
+    PAIR_LIST pairs = AlignmentPE::getPairs(fa, ra);
+    AlignmentPE::sort(pairs);
+    AlignmentPE::filter(pairs, opt[1], opt[2], opt[3], opt[4], max_npair);
+    if (!pairs.empty()) {
+        AlignmentPE::calcMapQ(pairs);
+        sam_pair_out(pairs, max_report, out);
+    } else if (!opt[0]) {
+        if (!fa.empty()) {
+            Alignment::calcMapQ(fa);
+            Alignment::sort(fa);
+            sam_list_out(fa, max_report, BAM_FPAIRED | BAM_FREAD1, out);
+        }
+        if (!ra.empty()) {
+            Alignment::calcMapQ(ra);
+            Alignment::sort(ra);
+            sam_list_out(ra, max_report, BAM_FPAIRED | BAM_FREAD2, out);
+        }
+    }
+}
+
+/* AlignmentPE::ps as msgseqtk-align leaves it after its options
+ * (src/msgseqtk-align.cpp:267-300, 400): mean, sd, insert range, then
+ * updateParam. */
+static void set_pairing(double mean, double sd, double min_ins, double max_ins) {
+    AlignmentPE::ps.setMean(mean);
+    AlignmentPE::ps.setSD(sd);
+    AlignmentPE::ps.setRange(min_ins, max_ins);
+    AlignmentPE::ps.updateParam();
+}
+
+/* SAM lines of the reference's paired-end path (src/msgseqtk-align.cpp:680-748)
+ * for n_pairs pairs whose mates are reads 2i and 2i+1 of the batch (GLOBAL
+ * mode). opt = {noMixed, noDiscordant, noTailOver, noContain, noOverlap}.
+ * Returns the text length; written only when it fits in cap bytes. */
+int64_t ref_sam_pe_batch(void* h, int64_t n_pairs, const uint8_t* reads, const uint8_t* quals, const int64_t* offs,
+                         int64_t min_len, double max_evalue, int64_t max_nseed, double min_score_rate,
+                         int max_report, double mean, double sd, double min_ins, double max_ins, const int* opt,
+                         int64_t max_npair, char* out, int64_t cap) {
+    RefDB* db = (RefDB*)h;
+    set_pairing(mean, sd, min_ins, max_ins);
+    std::string text;
+    for (int64_t i = 0; i < n_pairs; ++i) {
+        const std::string name = "p" + std::to_string(i);
+        // const, so that revcom() makes a copy (the non-const overload reverses
+        // in place; main_PE casts to const for the same reason)
+        const PrimarySeq f = make_read(reads + offs[2 * i], offs[2 * i + 1] - offs[2 * i],
+                                       quals ? quals + offs[2 * i] : nullptr, name.c_str());
+        const PrimarySeq r = make_read(reads + offs[2 * i + 1], offs[2 * i + 2] - offs[2 * i + 1],
+                                       quals ? quals + offs[2 * i + 1] : nullptr, name.c_str());
+        const PrimarySeq rcf = f.revcom(), rcr = r.revcom();
+        SeedListPE seeds = SMEM_LIST::findSeedsPE(&f, &r, &db->mtg, &db->fmd, min_len, max_evalue, max_nseed);
+        ALIGN_LIST fa, ra;
+        if (!(seeds.first.empty() && seeds.second.empty())) {
+            const int64_t fL = f.length(), rL = r.length();
+            ChainList fc = SeedChain::getChains(seeds.first, std::ceil(fL * Alignment::MAX_MISMATCH_RATE),
+                                                std::ceil(fL * Alignment::MAX_INDEL_RATE));
+            ChainList rch = SeedChain::getChains(seeds.second, std::ceil(rL * Alignment::MAX_MISMATCH_RATE),
+                                                 std::ceil(rL * Alignment::MAX_INDEL_RATE));
+            fa = Alignment::buildAlignments(&f, &rcf, db->mtg, fc, Alignment::GLOBAL);
+            ra = Alignment::buildAlignments(&r, &rcr, db->mtg, rch, Alignment::GLOBAL);
+        }
+        sam_pair(fa, ra, f, r, min_score_rate, (uint32_t)max_report, opt, max_npair, text);
+    }
+    return put_out(text, out, cap);
+}
+
 /* SAM lines of the reference's single-end path (src/msgseqtk-align.cpp:600-640)
  * for n reads (GLOBAL mode). Returns the text length; the text is written
  * only when it fits in cap bytes. */
@@ -484,54 +601,89 @@ int64_t ref_sam_batch(void* h, int64_t n_reads, const uint8_t* reads, const uint
     return put_out(text, out, cap);
 }
 
+struct RecAln {  // msg_aln (include/msg_b200.h), 88 bytes
+    int64_t read; int32_t tid, strand; int64_t t_start, t_end, aln_from, aln_to, aln_start, aln_end;
+    int32_t aln_score, flags; int64_t cigar_off; int32_t n_cigar, pad;
+};
+static_assert(sizeof(RecAln) == 88, "msg_aln layout");
+
+/* The alignments of records k0..k1 of the CUDA library: each record sets the
+ * fields buildAlignments would set (Alignment.h:357-375), the path is the
+ * CIGAR's M/I/D runs (soft clips are alnFrom/alnTo). */
+static ALIGN_LIST records_to_alignments(RefDB* db, const PrimarySeq* r, const PrimarySeq* rc, int64_t L,
+                                        const void* records, const uint32_t* cigar, int64_t k0, int64_t k1) {
+    const RecAln* rec = (const RecAln*)records;
+    ALIGN_LIST alns;
+    for (int64_t k = k0; k < k1; ++k) {
+        const RecAln& g = rec[k];
+        Alignment a(r);
+        a.rcRead = rc;
+        a.tid = g.tid;
+        a.target = &db->mtg.getSeq(g.tid);
+        a.qStrand = (GLoc::STRAND)g.strand;
+        a.qFrom = 0;
+        a.qTo = L;
+        a.tStart = g.t_start;
+        a.tEnd = g.t_end;
+        a.alnMode = Alignment::GLOBAL;
+        a.alnFrom = g.aln_from;
+        a.alnTo = g.aln_to;
+        a.alnStart = g.aln_start;
+        a.alnEnd = g.aln_end;
+        a.alnScore = g.aln_score == INT32_MIN ? -std::numeric_limits<double>::infinity() : (double)g.aln_score;
+        for (int32_t w = 0; w < g.n_cigar; ++w) {
+            const uint32_t c = cigar[g.cigar_off + w];
+            if ((c & 0xf) == BAM_CSOFT_CLIP) continue;
+            a.alnPath.append(c >> 4, c & 0xf);
+        }
+        alns.push_back(a);
+    }
+    return alns;
+}
+
 /* The same lines with the alignments taken from records of the CUDA library
- * (msg_aln, include/msg_b200.h; 88 bytes each) and their CIGAR words: each
- * record sets the fields buildAlignments would set (Alignment.h:357-375), the
- * path is the CIGAR's M/I/D runs (soft clips are alnFrom/alnTo), and the
- * reference's tail runs unchanged. */
+ * (msg_aln, include/msg_b200.h; 88 bytes each) and their CIGAR words, through
+ * records_to_alignments; the reference's tail runs unchanged. */
 int64_t ref_sam_from_records(void* h, int64_t n_reads, const uint8_t* reads, const uint8_t* quals,
                              const int64_t* offs, const void* records, const uint32_t* cigar,
                              const int64_t* read_aln_off, double min_score_rate, int max_report, char* out,
                              int64_t cap) {
     RefDB* db = (RefDB*)h;
-    struct Rec {
-        int64_t read; int32_t tid, strand; int64_t t_start, t_end, aln_from, aln_to, aln_start, aln_end;
-        int32_t aln_score, flags; int64_t cigar_off; int32_t n_cigar, pad;
-    };
-    static_assert(sizeof(Rec) == 88, "msg_aln layout");
-    const Rec* rec = (const Rec*)records;
     std::string text;
     for (int64_t i = 0; i < n_reads; ++i) {
         const int64_t L = offs[i + 1] - offs[i];
         const std::string name = "r" + std::to_string(i);
         const PrimarySeq r = make_read(reads + offs[i], L, quals ? quals + offs[i] : nullptr, name.c_str());
         const PrimarySeq rc = r.revcom();
-        ALIGN_LIST alns;
-        for (int64_t k = read_aln_off[i]; k < read_aln_off[i + 1]; ++k) {
-            const Rec& g = rec[k];
-            Alignment a(&r);
-            a.rcRead = &rc;
-            a.tid = g.tid;
-            a.target = &db->mtg.getSeq(g.tid);
-            a.qStrand = (GLoc::STRAND)g.strand;
-            a.qFrom = 0;
-            a.qTo = L;
-            a.tStart = g.t_start;
-            a.tEnd = g.t_end;
-            a.alnMode = Alignment::GLOBAL;
-            a.alnFrom = g.aln_from;
-            a.alnTo = g.aln_to;
-            a.alnStart = g.aln_start;
-            a.alnEnd = g.aln_end;
-            a.alnScore = g.aln_score == INT32_MIN ? -std::numeric_limits<double>::infinity() : (double)g.aln_score;
-            for (int32_t w = 0; w < g.n_cigar; ++w) {
-                const uint32_t c = cigar[g.cigar_off + w];
-                if ((c & 0xf) == BAM_CSOFT_CLIP) continue;
-                a.alnPath.append(c >> 4, c & 0xf);
-            }
-            alns.push_back(a);
-        }
+        ALIGN_LIST alns = records_to_alignments(db, &r, &rc, L, records, cigar, read_aln_off[i], read_aln_off[i + 1]);
         sam_read(alns, r, min_score_rate, (uint32_t)max_report, text);
+    }
+    return put_out(text, out, cap);
+}
+
+/* ref_sam_pe_batch's tail on records of the CUDA library (reads 2i and 2i+1
+ * of the batch are the mates of pair i), as ref_sam_from_records does for
+ * single reads. */
+int64_t ref_sam_pe_from_records(void* h, int64_t n_pairs, const uint8_t* reads, const uint8_t* quals,
+                                const int64_t* offs, const void* records, const uint32_t* cigar,
+                                const int64_t* read_aln_off, double min_score_rate, int max_report, double mean,
+                                double sd, double min_ins, double max_ins, const int* opt, int64_t max_npair,
+                                char* out, int64_t cap) {
+    RefDB* db = (RefDB*)h;
+    set_pairing(mean, sd, min_ins, max_ins);
+    std::string text;
+    for (int64_t i = 0; i < n_pairs; ++i) {
+        const std::string name = "p" + std::to_string(i);
+        const PrimarySeq m[2] = {make_read(reads + offs[2 * i], offs[2 * i + 1] - offs[2 * i],
+                                     quals ? quals + offs[2 * i] : nullptr, name.c_str()),
+                           make_read(reads + offs[2 * i + 1], offs[2 * i + 2] - offs[2 * i + 1],
+                                     quals ? quals + offs[2 * i + 1] : nullptr, name.c_str())};
+        const PrimarySeq rc[2] = {m[0].revcom(), m[1].revcom()};
+        ALIGN_LIST lists[2];
+        for (int x = 0; x < 2; ++x)
+            lists[x] = records_to_alignments(db, &m[x], &rc[x], (int64_t)m[x].length(), records, cigar,
+                                             read_aln_off[2 * i + x], read_aln_off[2 * i + x + 1]);
+        sam_pair(lists[0], lists[1], m[0], m[1], min_score_rate, (uint32_t)max_report, opt, max_npair, text);
     }
     return put_out(text, out, cap);
 }

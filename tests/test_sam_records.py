@@ -46,21 +46,23 @@ def _workload(seed):
 _COMP = np.array([0, 8, 4, 12, 2, 10, 6, 14, 1, 9, 5, 13, 3, 11, 7, 15], dtype=np.uint8)
 
 
-def _ours_as_fields(recs, md, seq, qual, off, cigar):
+def _ours_as_fields(recs, md, seq, qual, off, cigar, pairs=False):
     """The library's tail records as the fields of the reference harness's
-    lines: QNAME FLAG TID POS MAPQ CIGAR L_SEQ SEQ QUAL then aux (floats as
-    float values, compared exactly)."""
+    lines: QNAME FLAG TID POS MAPQ CIGAR L_SEQ SEQ QUAL ISIZE then aux (floats
+    as float values, compared exactly)."""
     rows = []
     for r in recs:
         i = int(r["read"])
+        name = f"p{i // 2}" if pairs else f"r{i}"
         q = seq[off[i]:off[i + 1]]
         ql = qual[off[i]:off[i + 1]]
         if r["flag"] & 0x10:
             q, ql = _COMP[q[::-1]], ql[::-1]
         cg = cigar[r["cigar_off"]:r["cigar_off"] + r["n_cigar"]] if r["n_cigar"] else []
         cs = "".join(f"{int(c) >> 4}{'MIDNSHP=XB'[int(c) & 15]}" for c in cg) or "*"
-        f = [f"r{i}", str(int(r["flag"])), str(int(r["tid"])), str(int(r["pos"])), str(int(r["mapq"])), cs,
-             str(len(q)), "".join(f"{int(x):x}" for x in q), "".join(f"{int(x):02x}" for x in ql)]
+        f = [name, str(int(r["flag"])), str(int(r["tid"])), str(int(r["pos"])), str(int(r["mapq"])), cs,
+             str(len(q)), "".join(f"{int(x):x}" for x in q), "".join(f"{int(x):02x}" for x in ql),
+             str(int(r["isize"]))]
         if not r["flag"] & 0x4:
             m = md[r["md_off"]:r["md_off"] + r["md_len"]].decode()
             f += [f"AS:i:{int(r['as'])}", f"MD:Z:{m}", ("XH", float(r["xh"])), f"NH:i:{int(r['nh'])}",
@@ -73,8 +75,8 @@ def _ref_as_fields(lines):
     rows = []
     for line in lines:
         f = line.split("\t")
-        out = f[:9]
-        for a in f[9:]:
+        out = f[:10]
+        for a in f[10:]:
             tag, typ, val = a.split(":", 2)
             out.append((tag, float.fromhex(val)) if typ == "f" else a)
         rows.append(out)
@@ -92,6 +94,74 @@ def _check_tail(view, ref, seq, qual, off, aln, cig, roff, rate, max_report):
         assert len(got) == len(exp)
         for g, e in zip(got, exp):
             assert g == e, (g, e)
+
+
+def _check_tail_pe(view, ref, seq, qual, off, aln, cig, roff, rate, max_report, pairing):
+    from msgseqtk_b200 import lib
+    exp = _ref_as_fields(ref.sam_pe_from_records(seq, qual, off, aln, cig, roff, min_score_rate=rate,
+                                                 max_report=max_report, pairing=pairing))
+    q = {"min_ins" if k == "min" else "max_ins" if k == "max" else k: v for k, v in pairing.items()}
+    for nt in (1, 3):
+        recs, md = lib.tail(view, seq, off, qual, aln, cig, roff,
+                            lib.tail_params(min_score_rate=rate, max_report=max_report, n_threads=nt),
+                            pairing=lib.pair_params(**q))
+        got = _ours_as_fields(recs, md, seq, qual, off, cig, pairs=True)
+        assert len(got) == len(exp)
+        for g, e in zip(got, exp):
+            assert g == e, (g, e)
+    return exp
+
+
+def _pair_workload(seed):
+    """Pairs (mates at 2i, 2i+1): proper pairs, pairs with wide inserts,
+    pairs with one random mate, random pairs."""
+    g = synth.small_genomes(seed=seed, n_genomes=3, length=60_000)
+    m1, m2 = synth.sample_pairs(g, 200, seed=seed + 1, ins_mean=400, ins_sd=50)
+    w1, w2 = synth.sample_pairs(g, 40, seed=seed + 2, ins_mean=900, ins_sd=200, sub_rate=0.04, indel_rate=0.01)
+    rng = np.random.default_rng(seed)
+    mates, quals = [], []
+    for a, b in ((m1, m2), (w1, w2)):
+        for i in range(len(a)):
+            mates += [a.read(i), b.read(i)]
+            quals += [a.qual(i), b.qual(i)]
+    for i in range(30):  # one mate random
+        mates += [m1.read(i), synth._BASES[rng.integers(0, 4, 150)]]
+        quals += [m1.qual(i), rng.integers(20, 41, 150).astype(np.uint8)]
+    for i in range(20):
+        mates += [synth._BASES[rng.integers(0, 4, 150)] for _ in range(2)]
+        quals += [rng.integers(20, 41, 150).astype(np.uint8) for _ in range(2)]
+    seq = np.concatenate(mates).astype(np.uint8)
+    qual = np.concatenate(quals).astype(np.uint8)
+    off = np.concatenate([[0], np.cumsum([len(x) for x in mates])]).astype(np.int64)
+    return g, mates, seq, qual, off
+
+
+PAIRINGS = [dict(), dict(mean=400.0, sd=50.0, min=-100.0, max=900.0),
+            dict(mean=400.0, sd=50.0, min=-100.0, max=900.0, no_mixed=1, max_npair=2),
+            dict(mean=0.0, sd=1.0, min=0.0, max=2000.0, no_overlap=1, no_contain=1)]
+
+
+@needs_ref
+def test_library_pe_tail_matches_reference_on_oracle_records(oracle_built):
+    """msg_tail_pe_batch against the reference's paired-end tail
+    (AlignmentPE pairing, filters, MAPQ, unpaired and unmapped fallbacks) on
+    the same records, and those records through the reference's tail against
+    its whole paired-end path."""
+    from msgseqtk_b200 import index_build
+    g, mates, seq, qual, off = _pair_workload(21)
+    ref = Reference(g)
+    view = index_build.build_view(g)
+    aln, cig, roff = _records_from_oracle(Oracle(view), mates)
+    kinds = set()
+    for pairing in PAIRINGS:
+        for rate, max_report in ((0.65, 1), (0.65, 0), (0.3, 2)):
+            exp = _check_tail_pe(view, ref, seq, qual, off, aln, cig, roff, rate, max_report, pairing)
+            kinds |= {int(e[1]) & 0x1cf for e in exp}
+            if rate == 0.65:
+                full = ref.sam_pe_batch(seq, qual, off, min_score_rate=rate, max_report=max_report, pairing=pairing)
+                assert _ref_as_fields(full) == exp
+    # proper pairs, unpaired mates and unmapped pairs all occur
+    assert {0x43, 0x83} & kinds and {0x41, 0x81} & kinds and {77, 141} <= kinds
 
 
 @needs_ref
@@ -142,5 +212,28 @@ def test_gpu_records_give_reference_sam():
                 assert got == exp
                 _check_tail(view, ref, seq, qual, off, res["aln"], res["cigar"], res["read_aln_off"], 0.65,
                             max_report)
+    finally:
+        ctx.close()
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_gpu_records_through_library_pe_tail_give_reference_pairs():
+    """GPU records of interleaved mates through msg_tail_pe_batch equal the
+    reference's whole paired-end path."""
+    from msgseqtk_b200 import index_build
+    g, mates, seq, qual, off = _pair_workload(23)
+    ref = Reference(g)
+    view = index_build.build_view(g)
+    ctx = lib.Context(0)
+    try:
+        ctx.load_index(view)
+        res = ctx.map(seq, off, lib.default_params(min_score_rate=0.65))
+        for pairing in PAIRINGS[:2]:
+            for max_report in (1, 0):
+                full = _ref_as_fields(ref.sam_pe_batch(seq, qual, off, max_report=max_report, pairing=pairing))
+                got = _check_tail_pe(view, ref, seq, qual, off, res["aln"], res["cigar"], res["read_aln_off"], 0.65,
+                                     max_report, pairing)
+                assert got == full
     finally:
         ctx.close()
