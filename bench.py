@@ -618,10 +618,15 @@ def main():
                       "fallback_rate": agg["n_band_fallback"] / banded if banded else 0.0,
                       "speedup_vs_plain": value / plain["value"] if plain["value"] > 0 else None})
 
-    # end to end through the public API: pinned host reads in, host records out
-    aln_buf = np.zeros(8 * bp, dtype=lib.ALN_DTYPE)
-    cig_buf = np.zeros(64 * bp, dtype=np.uint32)
-    roff_buf = np.zeros(bp + 1, dtype=np.int64)
+    # end to end through the public API: pinned host reads in, records out
+    # into pinned host buffers
+    def pinned(n, dtype):
+        dt = np.dtype(dtype)
+        return torch.empty(n * dt.itemsize, dtype=torch.uint8).pin_memory().numpy().view(dt)
+
+    aln_buf = pinned(8 * bp, lib.ALN_DTYPE)
+    cig_buf = pinned(64 * bp, np.uint32)
+    roff_buf = pinned(bp + 1, np.int64)
     for s in range(min(args.warmup, 1)):
         k = s % n_batches
         ctx.map_into(h_seq[reads.offs[k * bp]:], h_offs[k], aln_buf, cig_buf, roff_buf, params)
@@ -657,8 +662,8 @@ def main():
     tprm = lib.tail_params(min_score_rate=args.min_score, max_report=1, n_threads=tail_threads)
     pairing = lib.pair_params(mean=400.0, sd=50.0, min_ins=-100.0, max_ins=900.0) if args.workload == "scale" \
         else None
-    bufs = [(np.zeros(8 * bp, dtype=lib.ALN_DTYPE), np.zeros(64 * bp, dtype=np.uint32), np.zeros(bp + 1, np.int64))
-            for _ in range(2)]
+    bufs = [(aln_buf, cig_buf, roff_buf), (pinned(8 * bp, lib.ALN_DTYPE), pinned(64 * bp, np.uint32),
+                                            pinned(bp + 1, np.int64))]
     n_sam = 0
 
     def sam_step(s, pool, fut):

@@ -153,6 +153,12 @@ __global__ void k_compact_aln(const msg_aln* __restrict__ aln, const uint8_t* __
     map[kidx[c]] = c;
 }
 
+// off[i] -= base for i < n (host offsets rebased to the batch's first read).
+__global__ void k_rebase(int64_t* __restrict__ off, int64_t n, int64_t base) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) off[i] -= base;
+}
+
 struct Timer {
     msg_ctx* ctx;
     int k = 0;
@@ -809,17 +815,23 @@ static int upload_reads(msg_ctx* ctx, const msg_read_batch* reads) {
     if (e != cudaSuccess) return ctx->cuda_fail(e);
     e = ctx->offs.ensure((n + 1) * 8);
     if (e != cudaSuccess) return ctx->cuda_fail(e);
-    std::vector<int64_t> off0(n + 1);
-    for (int64_t i = 0; i <= n; ++i) off0[i] = n > 0 ? reads->off[i] - reads->off[0] : 0;
+    // the caller's buffers are copied as they are (straight from pinned
+    // memory when the caller pinned them) and the offsets rebased to the
+    // first read on the device; the copies complete before the call returns
     if (bytes > 0) {
         e = cudaMemcpyAsync(ctx->reads.p, reads->seq + reads->off[0], bytes, cudaMemcpyHostToDevice, ctx->stream);
         if (e != cudaSuccess) return ctx->cuda_fail(e);
     }
-    e = cudaMemcpyAsync(ctx->offs.p, off0.data(), (n + 1) * 8, cudaMemcpyHostToDevice, ctx->stream);
-    if (e != cudaSuccess) return ctx->cuda_fail(e);
-    e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) return ctx->cuda_fail(e);
-    return MSG_OK;
+    if (n > 0) {
+        e = cudaMemcpyAsync(ctx->offs.p, reads->off, (n + 1) * 8, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess && reads->off[0] != 0) {
+            k_rebase<<<nblk(n + 1, 256), 256, 0, ctx->stream>>>(ctx->offs.as<int64_t>(), n + 1, reads->off[0]);
+            e = cudaGetLastError();
+        }
+    } else {
+        e = cudaMemsetAsync(ctx->offs.p, 0, 8, ctx->stream);
+    }
+    return e == cudaSuccess ? MSG_OK : ctx->cuda_fail(e);
 }
 
 extern "C" int msg_map_batch(msg_ctx* ctx, const msg_read_batch* reads, const msg_map_params* params,
