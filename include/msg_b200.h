@@ -204,6 +204,17 @@ typedef struct msg_map_stats {
 int msg_map_batch(msg_ctx* ctx, const msg_read_batch* reads, const msg_map_params* params,
                   msg_aln_out* out, msg_stage_dump* dump);
 
+/* msg_map_batch over n_batches batches in HOST memory, with the copies
+ * overlapped: batch k+1's reads go to the device on a second stream while
+ * batch k is mapped, and batch k's records come back while batch k+1 is
+ * mapped (pin the host buffers for the copies to overlap). outs[k] receives
+ * batch k's results exactly as msg_map_batch would (every output pointer
+ * required except read_aln_off). When a batch's counts exceed its capacities
+ * the call still maps the others and returns MSG_EINVAL with those counts in
+ * outs[k]. No reference counterpart (a batching form of msg_map_batch). */
+int msg_map_batches(msg_ctx* ctx, int64_t n_batches, const msg_read_batch* reads, const msg_map_params* params,
+                    msg_aln_out* outs);
+
 /* Same as msg_map_batch with the reads already in device memory (seq and off
  * are device pointers); results still land in the caller's host buffers. */
 int msg_map_batch_device(msg_ctx* ctx, const msg_read_batch* dev_reads, const msg_map_params* params,

@@ -843,6 +843,88 @@ extern "C" int msg_map_batch(msg_ctx* ctx, const msg_read_batch* reads, const ms
     return map_impl(ctx, ctx->reads.as<uint8_t>(), ctx->offs.as<int64_t>(), reads->n_reads, params, out, dump);
 }
 
+extern "C" int msg_map_batches(msg_ctx* ctx, int64_t n_batches, const msg_read_batch* reads,
+                               const msg_map_params* params, msg_aln_out* outs) {
+    if (!ctx || n_batches < 0 || (n_batches > 0 && (!reads || !outs)) || !params) return MSG_EINVAL;
+    if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
+    for (int64_t k = 0; k < n_batches; ++k) {
+        const msg_read_batch& r = reads[k];
+        if (r.n_reads < 0 || r.n_reads > INT32_MAX || (r.n_reads > 0 && (!r.seq || !r.off))) return MSG_EINVAL;
+        for (int64_t i = 0; i < r.n_reads; ++i)
+            if (r.off[i + 1] < r.off[i]) return MSG_EINVAL;
+        if (!outs[k].aln || !outs[k].cigar) return ctx->fail(MSG_EINVAL, "null output buffer");
+    }
+#define CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { cudaStreamSynchronize(ctx->cstream); return ctx->cuda_fail(e_); } } while (0)
+    if (!ctx->cstream) {
+        if (cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking) != cudaSuccess)
+            return ctx->fail(MSG_ECUDA, "copy stream");
+        for (cudaEvent_t& e : ctx->pev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    }
+    cudaStream_t cs = ctx->cstream, st = ctx->stream;
+    // batch k's reads into input slot k % 2 on the copy stream; the slot's
+    // previous batch (k - 2) finished before batch k - 1 started
+    auto upload = [&](int64_t k) -> cudaError_t {
+        const msg_read_batch& r = reads[k];
+        const int sl = (int)(k & 1);
+        const int64_t n = r.n_reads;
+        const int64_t bytes = n > 0 ? r.off[n] - r.off[0] : 0;
+        cudaError_t e = ctx->in_seq[sl].ensure(bytes + 16);
+        if (e == cudaSuccess) e = ctx->in_off[sl].ensure((n + 1) * 8);
+        if (e != cudaSuccess) return e;
+        if (bytes > 0) e = cudaMemcpyAsync(ctx->in_seq[sl].p, r.seq + r.off[0], bytes, cudaMemcpyHostToDevice, cs);
+        if (e != cudaSuccess) return e;
+        if (n > 0) {
+            e = cudaMemcpyAsync(ctx->in_off[sl].p, r.off, (n + 1) * 8, cudaMemcpyHostToDevice, cs);
+            if (e == cudaSuccess && r.off[0] != 0) {
+                k_rebase<<<nblk(n + 1, 256), 256, 0, cs>>>(ctx->in_off[sl].as<int64_t>(), n + 1, r.off[0]);
+                e = cudaGetLastError();
+            }
+        } else {
+            e = cudaMemsetAsync(ctx->in_off[sl].p, 0, 8, cs);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->pev[sl], cs);
+        return e;
+    };
+    int status = MSG_OK;
+    if (n_batches > 0) CK(upload(0));
+    for (int64_t k = 0; k < n_batches; ++k) {
+        const int sl = (int)(k & 1);
+        // the device buffers of the next batch's upload are not reallocated
+        // while this batch runs: upload k + 1 goes to the other slot
+        if (k + 1 < n_batches) CK(upload(k + 1));
+        CK(cudaStreamWaitEvent(st, ctx->pev[sl], 0));
+        msg_aln_out dev{};  // results stay on the device
+        const int rc = map_impl(ctx, ctx->in_seq[sl].as<uint8_t>(), ctx->in_off[sl].as<int64_t>(), reads[k].n_reads,
+                                params, &dev, nullptr);
+        if (rc != MSG_OK) { cudaStreamSynchronize(cs); return rc; }
+        msg_aln_out& o = outs[k];
+        o.n_aln = dev.n_aln;
+        o.n_cigar = dev.n_cigar;
+        if (dev.n_aln > o.aln_cap || dev.n_cigar > o.cigar_cap) { status = MSG_EINVAL; continue; }
+        // stage the records (the next batch overwrites the context's result
+        // buffers) and copy them back on the copy stream while it runs
+        const int64_t n = reads[k].n_reads;
+        const size_t ab = dev.n_aln * sizeof(msg_aln), cb = dev.n_cigar * 4, ob = (n + 1) * 8;
+        CK(cudaStreamWaitEvent(st, ctx->pev[4 + sl], 0));  // slot's download from batch k - 2 done
+        CK(ctx->stage[sl].ensure(ab + cb + ob + 64));
+        char* sg = ctx->stage[sl].as<char>();
+        if (ab) CK(cudaMemcpyAsync(sg, ctx->res_aln, ab, cudaMemcpyDeviceToDevice, st));
+        if (cb) CK(cudaMemcpyAsync(sg + ab, ctx->res_cigar, cb, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(sg + ab + cb, ctx->res_off, ob, cudaMemcpyDeviceToDevice, st));
+        CK(cudaEventRecord(ctx->pev[2 + sl], st));
+        CK(cudaStreamWaitEvent(cs, ctx->pev[2 + sl], 0));
+        if (ab) CK(cudaMemcpyAsync(o.aln, sg, ab, cudaMemcpyDeviceToHost, cs));
+        if (cb) CK(cudaMemcpyAsync(o.cigar, sg + ab, cb, cudaMemcpyDeviceToHost, cs));
+        if (o.read_aln_off) CK(cudaMemcpyAsync(o.read_aln_off, sg + ab + cb, ob, cudaMemcpyDeviceToHost, cs));
+        CK(cudaEventRecord(ctx->pev[4 + sl], cs));
+    }
+    CK(cudaStreamSynchronize(cs));
+    CK(cudaStreamSynchronize(st));
+#undef CK
+    if (status != MSG_OK) return ctx->fail(status, "output capacity too small");
+    return MSG_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Band model: parameters, training data, training and gradient check.
 // ---------------------------------------------------------------------------

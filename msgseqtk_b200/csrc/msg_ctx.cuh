@@ -61,6 +61,10 @@ struct msg_ctx {
     msg::DevBuf band_wts, band_nrm, tr_x, tr_y, tr_ord, tr_w, tr_m, tr_v, tr_g, tr_loss;
     // MEM search / read cleaning: per-unit loglik and counts, clean outputs, MEM rows, row slots
     msg::DevBuf memo, memo2, memrows, memslot;
+    // msg_map_batches: a copy stream, two input slots and two result staging slots
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t pev[6] = {};  // [0..1] upload done, [2..3] staged, [4..5] download done
+    msg::DevBuf in_seq[2], in_off[2], stage[2];
     bool band_loaded = false;
     int64_t scratch_limit = 16ll << 30;  // DP rectangle storage per pass (msg_ctx_set_scratch_limit)
     cudaEvent_t ev[8];
@@ -80,8 +84,14 @@ struct msg_ctx {
         for (msg::DevBuf* b : {&reads, &offs, &smem, &smem_cnt, &prev, &sel, &seedoff, &seeds, &seeds2, &rcount,
                                &chains, &chainidx, &dpinfo, &scratch, &path, &alnbuf, &cigbuf, &misc, &status, &geobuf,
                                &bandbuf, &alnbuf2, &recoff, &rlist, &prevw, &band_wts, &band_nrm, &tr_x, &tr_y,
-                               &tr_ord, &tr_w, &tr_m, &tr_v, &tr_g, &tr_loss, &memo, &memo2, &memrows, &memslot})
+                               &tr_ord, &tr_w, &tr_m, &tr_v, &tr_g, &tr_loss, &memo, &memo2, &memrows, &memslot,
+                               &in_seq[0], &in_seq[1], &in_off[0], &in_off[1], &stage[0], &stage[1]})
             b->release();
+        if (cstream) {
+            for (cudaEvent_t& e : pev) cudaEventDestroy(e);
+            cudaStreamDestroy(cstream);
+            cstream = nullptr;
+        }
     }
     void index_free() {
         if (idx.bkt) cudaFree(idx.bkt);

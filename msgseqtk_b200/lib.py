@@ -28,7 +28,7 @@ assert ALN_DTYPE.itemsize == 88
 # symbols of the C ABI, in include/msg_b200.h order
 EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy", "msg_index_load", "msg_db_read",
            "msg_db_views", "msg_db_free", "msg_index_bytes",
-           "msg_map_params_default", "msg_map_batch", "msg_map_batch_device", "msg_last_stats",
+           "msg_map_params_default", "msg_map_batch", "msg_map_batches", "msg_map_batch_device", "msg_last_stats",
            "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
            "msg_band_train", "msg_band_grad", "msg_tail_params_default", "msg_tail_batch", "msg_pair_params_default", "msg_tail_pe_batch",
            "msg_mem_params_default", "msg_mem_batch", "msg_clean_batch",
@@ -139,6 +139,8 @@ def load_library(path: str = LIB_PATH):
     L.msg_map_batch.argtypes = [C.c_void_p, C.POINTER(ReadBatch), C.POINTER(MapParams), C.POINTER(AlnOut),
                                 C.POINTER(StageDump)]
     L.msg_map_batch_device.argtypes = L.msg_map_batch.argtypes
+    L.msg_map_batches.argtypes = [C.c_void_p, C.c_int64, C.POINTER(ReadBatch), C.POINTER(MapParams),
+                                  C.POINTER(AlnOut)]
     L.msg_last_stats.argtypes = [C.c_void_p, C.POINTER(MapStats)]
     L.msg_result_device.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     L.msg_ctx_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
@@ -395,6 +397,18 @@ class Context:
         self._check(self.lib.msg_map_batch(self.h, C.byref(batch), C.byref(params), C.byref(out), None),
                     "msg_map_batch")
         return out.n_aln, out.n_cigar
+
+    def map_batches(self, batches, outs, params: MapParams | None = None):
+        """msg_map_batches: batches = [(seq, off)], outs = [(aln, cigar,
+        read_aln_off)] host arrays (pinned for overlapped copies). Returns
+        [(n_aln, n_cigar)] per batch."""
+        params = params or default_params()
+        n = len(batches)
+        rb = (ReadBatch * n)(*[ReadBatch(len(o) - 1, _p(q, u8p), _p(o, i64p)) for q, o in batches])
+        ao = (AlnOut * n)(*[AlnOut(len(a), a.ctypes.data, len(c), c.ctypes.data, 0, 0, _p(r, i64p))
+                            for a, c, r in outs])
+        self._check(self.lib.msg_map_batches(self.h, n, rb, C.byref(params), ao), "msg_map_batches")
+        return [(ao[k].n_aln, ao[k].n_cigar) for k in range(n)]
 
     def smem_noalloc(self, seq_ptr: int, off_ptr: int, n_reads: int, out_ptr: int, cap_per_read: int,
                      count_ptr: int, params: MapParams | None = None) -> int:

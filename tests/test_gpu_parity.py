@@ -229,3 +229,51 @@ def test_scratch_limit_gives_same_records(oracle_built):
                 assert np.array_equal(full[k], part[k]), k
     finally:
         c.close()
+
+
+def test_map_batches_equals_map_batch(oracle_built):
+    """msg_map_batches (copies overlapped with the neighbouring batches'
+    mapping) gives each batch exactly msg_map_batch's records: batches of
+    different sizes, an empty one, offsets that do not start at 0, pinned and
+    pageable host buffers."""
+    import torch
+    g = synth.small_genomes(seed=81, n_genomes=3, length=80_000)
+    view = index_build.build_view(g)
+    c = lib.Context(0)
+    try:
+        c.load_index(view)
+        rs = synth.sample_reads(g, 1500, seed=82, sub_rate=0.02, indel_rate=0.005)
+        params = lib.default_params(min_score_rate=0.65)
+        cuts = [0, 700, 700, 1100, 1101, 1500]
+        batches, expect = [], []
+        for a, b in zip(cuts[:-1], cuts[1:]):
+            batches.append((rs.seqs, np.ascontiguousarray(rs.offs[a:b + 1])))  # offsets into the whole array
+            o = rs.offs[a:b + 1] - rs.offs[a]
+            expect.append(c.map(rs.seqs[rs.offs[a]:rs.offs[b]], o, params))
+
+        def pinned(n, dt):
+            dt = np.dtype(dt)
+            return torch.empty(n * dt.itemsize, dtype=torch.uint8).pin_memory().numpy().view(dt)
+
+        for pin in (True, False):
+            outs = []
+            for (s, o) in batches:
+                n = len(o) - 1
+                mk = pinned if pin else (lambda k, dt: np.zeros(k, dtype=dt))
+                outs.append((mk(4 * n + 16, lib.ALN_DTYPE), mk(64 * n + 64, np.uint32), mk(n + 1, np.int64)))
+            counts = c.map_batches(batches, outs, params)
+            for (na, nc), (al, cg, ro), ex in zip(counts, outs, expect):
+                assert np.array_equal(al[:na], ex["aln"])
+                assert np.array_equal(cg[:nc], ex["cigar"])
+                assert np.array_equal(ro, ex["read_aln_off"])
+        # a batch whose records do not fit: MSG_EINVAL, the others still mapped
+        outs = [(np.zeros(4 * (len(o) - 1) + 16, lib.ALN_DTYPE), np.zeros(64 * len(o), np.uint32),
+                 np.zeros(len(o), np.int64)) for _, o in batches]
+        outs[0] = (np.zeros(1, lib.ALN_DTYPE), outs[0][1], outs[0][2])
+        with pytest.raises(lib.MsgError) as e:
+            c.map_batches(batches, outs, params)
+        assert e.value.code == lib.MSG_EINVAL
+        al, cg, ro = outs[2]
+        assert np.array_equal(ro, expect[2]["read_aln_off"])
+    finally:
+        c.close()
