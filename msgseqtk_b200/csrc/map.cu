@@ -906,6 +906,7 @@ extern "C" int msg_map_batches(msg_ctx* ctx, int64_t n_batches, const msg_read_b
         const int64_t n = reads[k].n_reads;
         const size_t ab = dev.n_aln * sizeof(msg_aln), cb = dev.n_cigar * 4, ob = (n + 1) * 8;
         CK(cudaStreamWaitEvent(st, ctx->pev[4 + sl], 0));  // slot's download from batch k - 2 done
+        if (ab + cb + ob + 64 > ctx->stage[sl].cap) CK(cudaStreamSynchronize(cs));  // before the slot is replaced
         CK(ctx->stage[sl].ensure(ab + cb + ob + 64));
         char* sg = ctx->stage[sl].as<char>();
         if (ab) CK(cudaMemcpyAsync(sg, ctx->res_aln, ab, cudaMemcpyDeviceToDevice, st));
