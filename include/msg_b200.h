@@ -384,6 +384,52 @@ int msg_tail_pe_batch(const msg_mtg_view* mtg, const msg_read_batch* reads, cons
                       const msg_tail_params* p, const msg_pair_params* q, msg_sam_rec* out, int64_t out_cap,
                       char* md, int64_t md_cap, int64_t* n_out, int64_t* md_len);
 
+/* ---- Reads in, SAM text out (host only) ---- */
+
+/* Caller-owned buffers for msg_fastq_parse: nt16 codes and phred values of
+ * the reads at off[i] .. off[i+1] (cap_bases each), and per read a text line
+ * "name\tdescription\n" at text[name_off[i] .. name_off[i+1]) (cap_text
+ * bytes); off and name_off hold cap_reads + 1 entries. */
+typedef struct msg_fastq_batch {
+    int64_t cap_reads, cap_bases, cap_text;
+    uint8_t* seq;
+    uint8_t* qual;
+    int64_t* off;
+    char* text;
+    int64_t* name_off;
+    int64_t n_reads, n_bases, n_text;  /* out */
+} msg_fastq_batch;
+
+/* FASTQ records from text[0 .. len) as msgseqtk-align's reader makes them
+ * (while the next character is '@': SeqIO::nextFastqSeq, src/SeqIO.cpp:74-87):
+ * the name is the first word after '@' (leading whitespace, newlines
+ * included, skipped), the description the rest of that line after its
+ * blanks, then the sequence line, the separator line and the quality line,
+ * each up to '\n' ('\r' is kept as a character). Bases are encoded with
+ * DNAalphabet's table (characters it does not list become 0), qualities as
+ * max(uint8(c - 33), 2), and a quality string of another length is cut or
+ * padded with 33 to the sequence's length (PrimarySeq::fixQual). Parsing
+ * stops at the first record that does not fit the buffers, at the first
+ * record whose four lines are not all in the text unless at_eof (then
+ * missing lines are empty, as at the end of a stream), or at a line that
+ * does not start with '@'. *consumed receives the bytes of the records
+ * parsed, so a caller streams a file by passing the rest again. */
+int msg_fastq_parse(const char* text, int64_t len, int at_eof, msg_fastq_batch* out, int64_t* consumed);
+
+/* SAM text lines of msg_tail_batch / msg_tail_pe_batch records, laid out as
+ * htslib's sam_format1 prints the BAM records msgseqtk-align writes: QNAME
+ * (the read's name from its "name\tdescription" text line), FLAG, RNAME
+ * (chrom_names[tid], '*' when unmapped), POS (pos + 1), MAPQ, CIGAR ('*'
+ * when empty), RNEXT '*' and PNEXT 1 (the records' mate fields are left at
+ * -1 and 0, src/SAMtools/BAM.h:61-75), TLEN, SEQ and QUAL (reverse-
+ * complemented and reversed when flag has 0x10; phred + 33), then AS:i, MD:Z,
+ * XH:f, NH:i, XN:i, XP:f for mapped records, floats with %g (htslib's
+ * exact float formatting is not pinned). Writes *text_len bytes into out
+ * (cap bytes; MSG_EINVAL with *text_len set when they do not fit). */
+int msg_sam_format(const msg_sam_rec* recs, int64_t n_recs, const char* md, const msg_read_batch* reads,
+                   const uint8_t* quals, const uint32_t* cigar, const char* names, const int64_t* name_off,
+                   const char* const* chrom_names, int64_t n_chrom, char* out, int64_t cap, int64_t* text_len);
+
 /* ---- MEM search and read cleaning (msgseqtk-clean) ---- */
 
 typedef struct msg_mem_params {

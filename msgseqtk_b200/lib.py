@@ -31,6 +31,7 @@ EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy"
            "msg_map_params_default", "msg_map_batch", "msg_map_batches", "msg_map_batch_device", "msg_last_stats",
            "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
            "msg_band_train", "msg_band_grad", "msg_tail_params_default", "msg_tail_batch", "msg_pair_params_default", "msg_tail_pe_batch",
+           "msg_fastq_parse", "msg_sam_format",
            "msg_mem_params_default", "msg_mem_batch", "msg_clean_batch",
            "msg_clean_batch_device", "msg_occ_query", "msg_bi_ext_query", "msg_sa_query"]
 
@@ -74,6 +75,12 @@ class PairParams(C.Structure):
     _fields_ = [("mean", C.c_double), ("sd", C.c_double), ("min_ins", C.c_double), ("max_ins", C.c_double),
                 ("no_mixed", C.c_int32), ("no_discordant", C.c_int32), ("no_tail_over", C.c_int32),
                 ("no_contain", C.c_int32), ("no_overlap", C.c_int32), ("pad", C.c_int32), ("max_npair", C.c_int64)]
+
+
+class FastqBatch(C.Structure):
+    _fields_ = [("cap_reads", C.c_int64), ("cap_bases", C.c_int64), ("cap_text", C.c_int64), ("seq", u8p),
+                ("qual", u8p), ("off", i64p), ("text", C.c_char_p), ("name_off", i64p), ("n_reads", C.c_int64),
+                ("n_bases", C.c_int64), ("n_text", C.c_int64)]
 
 
 class MemParams(C.Structure):
@@ -162,6 +169,10 @@ def load_library(path: str = LIB_PATH):
     L.msg_pair_params_default.restype = None
     L.msg_tail_pe_batch.argtypes = L.msg_tail_batch.argtypes[:7] + [C.POINTER(PairParams)] + \
         L.msg_tail_batch.argtypes[7:]
+    L.msg_fastq_parse.argtypes = [C.c_char_p, C.c_int64, C.c_int, C.POINTER(FastqBatch), i64p]
+    L.msg_sam_format.argtypes = [C.c_void_p, C.c_int64, C.c_char_p, C.POINTER(ReadBatch), u8p,
+                                 C.POINTER(C.c_uint32), C.c_char_p, i64p, C.POINTER(C.c_char_p), C.c_int64, C.c_char_p,
+                                 C.c_int64, i64p]
     f64p = C.POINTER(C.c_double)
     L.msg_mem_params_default.argtypes = [C.POINTER(MemParams)]
     L.msg_mem_params_default.restype = None
@@ -254,6 +265,54 @@ def tail(view, seq, off, qual, aln, cigar, read_aln_off, params: TailParams | No
         if rc != MSG_OK:
             raise MsgError(rc, "msg_tail_batch")
         return out[:n_out.value], md[:md_len.value].tobytes()
+
+
+def fastq_parse(text: bytes, at_eof: bool = True, max_reads: int | None = None):
+    """msg_fastq_parse on a bytes object: dict(seq, qual, off, text, name_off,
+    consumed), text holding "name\tdescription\n" per read."""
+    L = load_library()
+    cap_r = max_reads if max_reads is not None else text.count(b"\n") // 4 + 2
+    cap_b = len(text) + 1
+    seq = np.empty(cap_b, np.uint8)
+    qual = np.empty(cap_b, np.uint8)
+    off = np.empty(cap_r + 1, np.int64)
+    nm = np.empty(len(text) + 2 * cap_r + 1, np.uint8)
+    noff = np.empty(cap_r + 1, np.int64)
+    b = FastqBatch(cap_r, cap_b, len(nm), _p(seq, u8p), _p(qual, u8p), _p(off, i64p),
+                   nm.ctypes.data_as(C.c_char_p), _p(noff, i64p), 0, 0, 0)
+    used = C.c_int64(0)
+    rc = L.msg_fastq_parse(text, len(text), int(at_eof), C.byref(b), C.byref(used))
+    if rc != MSG_OK:
+        raise MsgError(rc, "msg_fastq_parse")
+    n = b.n_reads
+    return dict(seq=seq[:b.n_bases].copy(), qual=qual[:b.n_bases].copy(), off=off[:n + 1].copy(),
+                text=nm[:b.n_text].tobytes(), name_off=noff[:n + 1].copy(), consumed=used.value)
+
+
+def sam_format(recs, md: bytes, seq, off, qual, cigar, names: bytes, name_off, chrom_names) -> bytes:
+    """msg_sam_format: SAM text lines of tail records."""
+    L = load_library()
+    recs = np.ascontiguousarray(recs, dtype=SAM_DTYPE)
+    seq = np.ascontiguousarray(seq, dtype=np.uint8)
+    off = np.ascontiguousarray(off, dtype=np.int64)
+    qual = np.ascontiguousarray(qual, dtype=np.uint8)
+    cigar = np.ascontiguousarray(cigar, dtype=np.uint32)
+    name_off = np.ascontiguousarray(name_off, dtype=np.int64)
+    cn = (C.c_char_p * max(1, len(chrom_names)))(*[c.encode() for c in chrom_names])
+    rb = ReadBatch(len(off) - 1, _p(seq, u8p), _p(off, i64p))
+    n = C.c_int64(0)
+    cap = 1 << 16
+    while True:
+        buf = C.create_string_buffer(cap)
+        rc = L.msg_sam_format(recs.ctypes.data, len(recs), md, C.byref(rb), _p(qual, u8p),
+                              cigar.ctypes.data_as(C.POINTER(C.c_uint32)), names, _p(name_off, i64p), cn,
+                              len(chrom_names), buf, cap, C.byref(n))
+        if rc == MSG_EINVAL and n.value > cap:
+            cap = n.value
+            continue
+        if rc != MSG_OK:
+            raise MsgError(rc, "msg_sam_format")
+        return buf.raw[:n.value]
 
 
 def mem_params(**kw) -> MemParams:

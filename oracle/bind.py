@@ -268,6 +268,8 @@ class Reference:
                                               C.POINTER(C.c_uint32), i64p, C.c_double, C.c_int, C.c_double,
                                               C.c_double, C.c_double, C.c_double, ip, C.c_int64, C.c_char_p,
                                               C.c_int64]
+        L.ref_fastq_parse.restype = C.c_int64
+        L.ref_fastq_parse.argtypes = [C.c_char_p, C.c_int64, C.c_char_p, C.c_int64]
         L.ref_sam_from_records.restype = C.c_int64
         L.ref_sam_from_records.argtypes = [C.c_void_p, C.c_int64, u8p, u8p, i64p, C.c_void_p, C.POINTER(C.c_uint32),
                                            i64p, C.c_double, C.c_int, C.c_char_p, C.c_int64]
@@ -436,6 +438,16 @@ class Reference:
         return self._text(lambda b, cap: self.lib.ref_sam_from_records(
             self.h, len(offs) - 1, _p(reads, u8p), _p(quals, u8p), _p(offs, i64p), aln.ctypes.data,
             cigar.ctypes.data_as(C.POINTER(C.c_uint32)), _p(roff, i64p), min_score_rate, max_report, b, cap))
+
+    def fastq_parse(self, text: bytes):
+        """The reference's FASTQ reading: lines "name\tdesc\tSEQHEX\tQUALHEX"
+        (split on '\n' only: names and descriptions may hold '\r')."""
+        cap = 4 * len(text) + 1024
+        buf = C.create_string_buffer(cap)
+        n = self.lib.ref_fastq_parse(text, len(text), buf, cap)
+        assert n <= cap
+        out = buf.raw[:n].decode("latin-1")
+        return out.split("\n")[:-1] if out else []
 
     @staticmethod
     def _pairing(pairing):

@@ -41,6 +41,7 @@
 #include "SeedChain.h"
 #include "Alignment.h"
 #include "ProgEnv.h"
+#include "SeqIO.h"
 #undef private
 #undef protected
 
@@ -702,6 +703,26 @@ int ref_db_save(void* h, const char* mtg_path, const char* mgs_path, const char*
     EGriceLab::saveProgInfo(fmdOut);
     db->fmd.save(fmdOut);
     return (mtgOut && mgsOut && fmdOut) ? 0 : 2;
+}
+
+/* msgseqtk-align's read loop over a FASTQ text (while hasNext: nextSeq,
+ * src/SeqIO.cpp:44-51, 74-87): per read a line "name\tdesc\tSEQ\tQUAL" with
+ * the nt16 codes as hex digits and the quality values as two hex digits
+ * each. Returns the text length; written only when it fits in cap bytes. */
+int64_t ref_fastq_parse(const char* text, int64_t len, char* out, int64_t cap) {
+    std::istringstream in(std::string(text, text + len));
+    SeqIO io(&in, SeqIO::FASTQ);
+    std::string s;
+    char buf[8];
+    while (io.hasNext()) {
+        const PrimarySeq r = io.nextSeq();
+        s += r.getName() + "\t" + r.getDesc() + "\t";
+        for (uint8_t b : r.getSeq()) { std::snprintf(buf, sizeof buf, "%x", (unsigned)b); s += buf; }
+        s += "\t";
+        for (uint8_t q : r.getQual()) { std::snprintf(buf, sizeof buf, "%02x", (unsigned)q); s += buf; }
+        s += "\n";
+    }
+    return put_out(s, out, cap);
 }
 
 int ref_max_threads(void) {

@@ -1,0 +1,137 @@
+"""Reads in, SAM text out (host code of the library, no GPU):
+
+* msg_fastq_parse against the reference's own FASTQ reader (SeqIO +
+  PrimarySeq, compiled from its sources) on records with the inputs the
+  reader meets: descriptions, lowercase and IUPAC bases, digits and other
+  characters its table maps to 0, carriage returns, quality strings shorter or
+  longer than the sequence, quality bytes below '!', names after blank
+  lines, a final record without its last newline or its last lines; and
+  streamed in pieces, the same reads as in one piece.
+* msg_sam_format on the host tail's records: every SAM field against the
+  record and read it comes from (htslib's own float formatting is not
+  available here; %g is checked).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from msgseqtk_b200 import index_build, lib, synth
+from oracle.bind import REF_SO, Oracle, Reference
+
+needs_ref = pytest.mark.skipif(not os.path.exists(REF_SO), reason="oracle/_ref not built")
+
+
+def _ours_lines(res):
+    lines = []
+    names = res["text"].split(b"\n")
+    for i in range(len(res["off"]) - 1):
+        a, b = res["off"][i], res["off"][i + 1]
+        name, desc = names[i].split(b"\t", 1)
+        lines.append("\t".join([name.decode("latin-1"), desc.decode("latin-1"),
+                                "".join(f"{int(x):x}" for x in res["seq"][a:b]),
+                                "".join(f"{int(x):02x}" for x in res["qual"][a:b])]))
+    return lines
+
+
+def _fastq_text(seed):
+    rng = np.random.default_rng(seed)
+    chars = bytes(range(33, 127)).replace(b"@", b"").replace(b"\n", b"")
+    recs = []
+    for i in range(60):
+        L = int(rng.integers(0, 40))
+        seq = rng.choice(list(b"ACGTacgtNnRYKMSWBDHVU0123456.-XZ*"), L).astype(np.uint8).tobytes()
+        ql = L + int(rng.integers(-3, 4)) if i % 7 == 0 else L
+        qual = rng.choice(list(chars), max(ql, 0)).astype(np.uint8).tobytes()
+        desc = [b"", b" len=%d" % L, b"\tx y\tz", b"   "][i % 4]
+        eol = b"\r\n" if i % 11 == 5 else b"\n"
+        recs.append(b"@r%d%s%s%s%s+%s%s%s" % (i, desc, eol, seq, eol, eol, qual, eol))
+    recs.append(b"@\n  spaced name\nACGT\n+\nII\x1f!\n")  # name after a blank line; qualities below '!'
+    recs.append(b"@last desc\nACGTN\n+\nIIIII")              # no final newline
+    return b"".join(recs)
+
+
+@needs_ref
+def test_fastq_parse_matches_reference_reader():
+    ref = Reference([synth.small_genomes(seed=1, n_genomes=1, length=2000)[0]])
+    for seed in (3, 4):
+        text = _fastq_text(seed)
+        exp = ref.fastq_parse(text)
+        got = lib.fastq_parse(text)
+        assert got["consumed"] == len(text)
+        assert _ours_lines(got) == exp
+    # a final record cut short: the reader fills the missing lines with nothing
+    for cut in (b"@a b\nACGT\n+\n", b"@a b\nACGT\n", b"@a b\n"):
+        assert _ours_lines(lib.fastq_parse(cut)) == ref.fastq_parse(cut)
+    # reading stops at a line that does not start with '@'
+    t = b"@a\nAC\n+\nII\n\n@b\nGT\n+\nII\n"
+    assert _ours_lines(lib.fastq_parse(t)) == ref.fastq_parse(t)
+
+
+def test_fastq_parse_streams_in_pieces():
+    text = _fastq_text(5)
+    whole = lib.fastq_parse(text)
+    lines, pos = [], 0
+    while pos < len(text):
+        piece = text[pos:pos + 97]
+        r = lib.fastq_parse(piece, at_eof=pos + 97 >= len(text))
+        if r["consumed"] == 0:  # not one whole record in the piece: take a longer one
+            piece = text[pos:pos + 2000]
+            r = lib.fastq_parse(piece, at_eof=pos + 2000 >= len(text))
+        lines += _ours_lines(r)
+        pos += r["consumed"]
+        assert r["consumed"] > 0
+    assert lines == _ours_lines(whole)
+    # a read cap stops early and reports what was consumed
+    r = lib.fastq_parse(text, max_reads=5)
+    assert len(r["off"]) == 6 and 0 < r["consumed"] < len(text)
+
+
+@needs_ref
+def test_sam_format_fields(oracle_built):
+    g = synth.small_genomes(seed=41, n_genomes=3, length=40_000)
+    view = index_build.build_view(g)
+    orc = Oracle(view)
+    rs = synth.sample_reads(g, 60, seed=42)
+    rng = np.random.default_rng(43)
+    reads = [rs.read(i) for i in range(len(rs))] + [synth._BASES[rng.integers(0, 4, 150)] for _ in range(5)]
+    quals = [rs.qual(i) for i in range(len(rs))] + [rng.integers(20, 41, 150).astype(np.uint8) for _ in range(5)]
+    recs, cig, roff = [], [], [0]
+    for i, r in enumerate(reads):
+        for e in orc.align_read(r):
+            recs.append((i, e["tid"], e["strand"], e["t_start"], e["t_end"], e["aln_from"], e["aln_to"],
+                         e["aln_start"], e["aln_end"], int(e["aln_score"]), e["flags"], len(cig), len(e["cigar"]), 0))
+            cig += e["cigar"]
+        roff.append(len(recs))
+    aln = np.array(recs, dtype=lib.ALN_DTYPE)
+    cig = np.array(cig, dtype=np.uint32)
+    seq = np.concatenate(reads).astype(np.uint8)
+    qual = np.concatenate(quals).astype(np.uint8)
+    off = np.concatenate([[0], np.cumsum([len(x) for x in reads])]).astype(np.int64)
+    out, md = lib.tail(view, seq, off, qual, aln, cig, np.array(roff), lib.tail_params(max_report=0))
+    names = b"".join(b"read%d\tsome description\n" % i for i in range(len(reads)))
+    name_off = np.concatenate([[0], np.cumsum([len(b"read%d\tsome description\n" % i) for i in range(len(reads))])])
+    chrom = [f"chr{t}" for t in range(len(g))]
+    text = lib.sam_format(out, md, seq, off, qual, cig, names, name_off, chrom).decode()
+    lines = text.rstrip("\n").split("\n")
+    assert len(lines) == len(out)
+    comp = np.array([0, 8, 4, 12, 2, 10, 6, 14, 1, 9, 5, 13, 3, 11, 7, 15])
+    for line, r in zip(lines, out):
+        f = line.split("\t")
+        i = int(r["read"])
+        assert f[0] == f"read{i}" and int(f[1]) == r["flag"]
+        q, ql = reads[i], quals[i]
+        if r["flag"] & 0x10:
+            q, ql = comp[q[::-1]], ql[::-1]
+        assert f[9] == "".join("=ACMGRSVTWYHKDBN"[int(x)] for x in q)
+        assert f[10] == "".join(chr(int(x) + 33) for x in ql)
+        assert f[6:9] == ["*", "1", str(int(r["isize"]))]
+        if r["flag"] & 0x4:
+            assert f[2:6] == ["*", "1", "0", "*"] and len(f) == 11
+            continue
+        assert f[2] == chrom[r["tid"]] and int(f[3]) == r["pos"] + 1 and int(f[4]) == r["mapq"]
+        cs = "".join(f"{int(c) >> 4}{'MIDNSHP=XB'[int(c) & 15]}" for c in cig[r["cigar_off"]:r["cigar_off"] + r["n_cigar"]])
+        assert f[5] == cs
+        assert f[11:] == [f"AS:i:{int(r['as'])}", "MD:Z:" + md[r["md_off"]:r["md_off"] + r["md_len"]].decode(),
+                          "XH:f:%g" % float(r["xh"]), f"NH:i:{int(r['nh'])}", f"XN:i:{int(r['xn'])}",
+                          "XP:f:%g" % float(r["xp"])]
