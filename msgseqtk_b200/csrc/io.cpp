@@ -38,14 +38,15 @@ const SymTable& sym() {
 
 inline bool is_space(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r'; }
 
-// One line from p (up to '\n', which is consumed); false at the end of text.
+// One line from p (up to '\n', which is consumed). Returns whether the line
+// ended with a newline (false: it ran to the end of the text).
 inline bool get_line(const char*& p, const char* end, const char*& a, const char*& b) {
     if (p >= end) { a = b = p; return false; }
     a = p;
     const char* nl = static_cast<const char*>(std::memchr(p, '\n', end - p));
     b = nl ? nl : end;
     p = nl ? nl + 1 : end;
-    return true;
+    return nl != nullptr;
 }
 
 }  // namespace
@@ -53,25 +54,19 @@ inline bool get_line(const char*& p, const char* end, const char*& a, const char
 extern "C" int msg_fastq_parse(const char* text, int64_t len, int at_eof, msg_fastq_batch* out, int64_t* consumed) {
     if (!out || !consumed || len < 0 || (len > 0 && !text)) return MSG_EINVAL;
     if (out->cap_reads < 0 || out->cap_bases < 0 || out->cap_text < 0) return MSG_EINVAL;
+    if (!out->off || !out->name_off || (out->cap_bases > 0 && (!out->seq || !out->qual)) ||
+        (out->cap_text > 0 && !out->text))
+        return MSG_EINVAL;
     const uint8_t* code = sym().code;
     const char* p = text;
     const char* end = text + len;
     int64_t n = 0, nb = 0, nt = 0;
-    if (out->off && out->cap_reads >= 0) out->off[0] = 0;
-    if (out->name_off) out->name_off[0] = 0;
+    out->off[0] = 0;
+    out->name_off[0] = 0;
     *consumed = 0;
     // SeqIO::hasNext: the next character is '@'
     while (p < end && *p == '@' && n < out->cap_reads) {
         const char* q = p + 1;
-        // without the whole record in the text and more to come, stop here
-        int lines = 0;
-        for (const char* s = q; s < end && lines < 4;) {
-            const char* nl = static_cast<const char*>(std::memchr(s, '\n', end - s));
-            if (!nl) break;
-            ++lines;
-            s = nl + 1;
-        }
-        if (lines < 4 && !at_eof) break;
         // `in >> name`: skip whitespace (newlines too), then one word
         while (q < end && is_space(*q)) ++q;
         const char* na = q;
@@ -79,10 +74,13 @@ extern "C" int msg_fastq_parse(const char* text, int64_t len, int at_eof, msg_fa
         const char* nz = q;
         while (q < end && is_space(*q) && *q != '\n') ++q;  // blanks before the description
         const char *da, *dz, *sa, *sz, *xa, *xz, *qa, *qz;
-        get_line(q, end, da, dz);  // description: the rest of the line
-        get_line(q, end, sa, sz);  // sequence
-        get_line(q, end, xa, xz);  // '+' line, ignored
-        get_line(q, end, qa, qz);  // quality
+        bool whole = get_line(q, end, da, dz);  // description: the rest of the line
+        whole = get_line(q, end, sa, sz) && whole;  // sequence
+        whole = get_line(q, end, xa, xz) && whole;  // '+' line, ignored
+        whole = get_line(q, end, qa, qz) && whole;  // quality
+        // a record whose lines do not all end in the text waits for more
+        // text, unless this is the end of the stream
+        if (!whole && !at_eof) break;
         const int64_t L = sz - sa;
         const int64_t tl = (nz - na) + 1 + (dz - da) + 1;
         if (nb + L > out->cap_bases || nt + tl > out->cap_text) break;
@@ -136,8 +134,10 @@ extern "C" int msg_sam_format(const msg_sam_rec* recs, int64_t n_recs, const cha
         const int64_t a = reads->off[r.read], L = reads->off[r.read + 1] - a;
         // QNAME: the read's name (its first word)
         const char* nm = names + name_off[r.read];
-        const char* ne = static_cast<const char*>(std::memchr(nm, '\t', name_off[r.read + 1] - name_off[r.read]));
-        s.append(nm, ne ? ne - nm : 0);
+        const int64_t nl = name_off[r.read + 1] - name_off[r.read];
+        const char* ne = static_cast<const char*>(std::memchr(nm, '\t', nl));
+        if (!ne) ne = static_cast<const char*>(std::memchr(nm, '\n', nl));
+        s.append(nm, ne ? ne - nm : nl);
         std::snprintf(buf, sizeof buf, "\t%d\t", r.flag);
         s += buf;
         s += r.tid < 0 ? "*" : chrom_names[r.tid];

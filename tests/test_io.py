@@ -82,6 +82,11 @@ def test_fastq_parse_streams_in_pieces():
         pos += r["consumed"]
         assert r["consumed"] > 0
     assert lines == _ours_lines(whole)
+    # a record whose name follows a line break is not taken before its last line
+    t = b"@\n  n d\nACGT\n+\nIIII\n"
+    assert lib.fastq_parse(t[:-6], at_eof=False)["consumed"] == 0
+    assert _ours_lines(lib.fastq_parse(t[:-1], at_eof=False)) == []
+    assert _ours_lines(lib.fastq_parse(t, at_eof=False)) == _ours_lines(lib.fastq_parse(t))
     # a read cap stops early and reports what was consumed
     r = lib.fastq_parse(text, max_reads=5)
     assert len(r["off"]) == 6 and 0 < r["consumed"] < len(text)
