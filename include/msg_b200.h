@@ -416,6 +416,16 @@ typedef struct msg_fastq_batch {
  * parsed, so a caller streams a file by passing the rest again. */
 int msg_fastq_parse(const char* text, int64_t len, int at_eof, msg_fastq_batch* out, int64_t* consumed);
 
+/* FASTQ text of the reads of a batch (those with keep[i] != 0; every read
+ * when keep is NULL), as msgseqtk-clean writes the reads it keeps
+ * (SeqIO::writeFastqSeq, src/SeqIO.cpp:107-116): "@name", " description"
+ * when there is one, the bases decoded with DNAalphabet's symbols, "+", the
+ * qualities + 33. Names and descriptions come from msg_fastq_parse's
+ * "name\tdescription\n" lines (text, name_off). Writes *text_len bytes into
+ * out (cap bytes; MSG_EINVAL with *text_len set when they do not fit). */
+int msg_fastq_format(const msg_read_batch* reads, const uint8_t* quals, const char* text, const int64_t* name_off,
+                     const uint8_t* keep, char* out, int64_t cap, int64_t* text_len);
+
 /* SAM text lines of msg_tail_batch / msg_tail_pe_batch records, laid out as
  * htslib's sam_format1 prints the BAM records msgseqtk-align writes: QNAME
  * (the read's name from its "name\tdescription" text line), FLAG, RNAME

@@ -175,3 +175,41 @@ extern "C" int msg_sam_format(const msg_sam_rec* recs, int64_t n_recs, const cha
     if (!s.empty()) std::memcpy(out, s.data(), s.size());
     return MSG_OK;
 }
+
+extern "C" int msg_fastq_format(const msg_read_batch* reads, const uint8_t* quals, const char* text,
+                                const int64_t* name_off, const uint8_t* keep, char* out, int64_t cap,
+                                int64_t* text_len) {
+    if (!reads || !text_len || cap < 0) return MSG_EINVAL;
+    const int64_t n = reads->n_reads;
+    if (n < 0 || (n > 0 && (!reads->seq || !reads->off || !text || !name_off))) return MSG_EINVAL;
+    static const char kSym[] = "$ACMGRSVTWYHKDBN";  // DNAalphabet::base2sym (src/DNAalphabet.cpp:36)
+    std::string s;
+    for (int64_t i = 0; i < n; ++i) {
+        if (keep && !keep[i]) continue;
+        // SeqIO::writeFastqSeq (src/SeqIO.cpp:107-116): "@name[ desc]", the
+        // decoded bases, "+", the qualities + 33, each on its own line
+        const char* t = text + name_off[i];
+        const int64_t tl = name_off[i + 1] - name_off[i] - 1;  // without the newline
+        const char* tab = static_cast<const char*>(std::memchr(t, '\t', tl > 0 ? tl : 0));
+        s += '@';
+        if (tab) {
+            s.append(t, tab - t);
+            if (t + tl > tab + 1) {
+                s += ' ';
+                s.append(tab + 1, t + tl - (tab + 1));
+            }
+        } else {
+            s.append(t, tl > 0 ? tl : 0);
+        }
+        s += '\n';
+        const int64_t a = reads->off[i], L = reads->off[i + 1] - a;
+        for (int64_t k = 0; k < L; ++k) s += kSym[reads->seq[a + k] & 15];
+        s += "\n+\n";
+        for (int64_t k = 0; k < L; ++k) s += (char)((quals ? quals[a + k] : 0) + 33);
+        s += '\n';
+    }
+    *text_len = (int64_t)s.size();
+    if ((int64_t)s.size() > cap || (!s.empty() && !out)) return MSG_EINVAL;
+    if (!s.empty()) std::memcpy(out, s.data(), s.size());
+    return MSG_OK;
+}

@@ -31,7 +31,7 @@ EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy"
            "msg_map_params_default", "msg_map_batch", "msg_map_batches", "msg_map_batch_device", "msg_last_stats",
            "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
            "msg_band_train", "msg_band_grad", "msg_tail_params_default", "msg_tail_batch", "msg_pair_params_default", "msg_tail_pe_batch",
-           "msg_fastq_parse", "msg_sam_format",
+           "msg_fastq_parse", "msg_fastq_format", "msg_sam_format",
            "msg_mem_params_default", "msg_mem_batch", "msg_clean_batch",
            "msg_clean_batch_device", "msg_occ_query", "msg_bi_ext_query", "msg_sa_query"]
 
@@ -170,6 +170,7 @@ def load_library(path: str = LIB_PATH):
     L.msg_tail_pe_batch.argtypes = L.msg_tail_batch.argtypes[:7] + [C.POINTER(PairParams)] + \
         L.msg_tail_batch.argtypes[7:]
     L.msg_fastq_parse.argtypes = [C.c_char_p, C.c_int64, C.c_int, C.POINTER(FastqBatch), i64p]
+    L.msg_fastq_format.argtypes = [C.POINTER(ReadBatch), u8p, C.c_char_p, i64p, u8p, C.c_char_p, C.c_int64, i64p]
     L.msg_sam_format.argtypes = [C.c_void_p, C.c_int64, C.c_char_p, C.POINTER(ReadBatch), u8p,
                                  C.POINTER(C.c_uint32), C.c_char_p, i64p, C.POINTER(C.c_char_p), C.c_int64, C.c_char_p,
                                  C.c_int64, i64p]
@@ -287,6 +288,25 @@ def fastq_parse(text: bytes, at_eof: bool = True, max_reads: int | None = None):
     n = b.n_reads
     return dict(seq=seq[:b.n_bases].copy(), qual=qual[:b.n_bases].copy(), off=off[:n + 1].copy(),
                 text=nm[:b.n_text].tobytes(), name_off=noff[:n + 1].copy(), consumed=used.value)
+
+
+def fastq_format(seq, off, qual, text: bytes, name_off, keep=None) -> bytes:
+    """msg_fastq_format: FASTQ text of the kept reads (all when keep is None)."""
+    L = load_library()
+    seq = np.ascontiguousarray(seq, dtype=np.uint8)
+    off = np.ascontiguousarray(off, dtype=np.int64)
+    qual = np.ascontiguousarray(qual, dtype=np.uint8)
+    name_off = np.ascontiguousarray(name_off, dtype=np.int64)
+    kp = None if keep is None else np.ascontiguousarray(keep, dtype=np.uint8)
+    rb = ReadBatch(len(off) - 1, _p(seq, u8p), _p(off, i64p))
+    n = C.c_int64(0)
+    cap = 2 * len(seq) + len(text) + 8 * (len(off) - 1) + 16
+    buf = C.create_string_buffer(cap)
+    rc = L.msg_fastq_format(C.byref(rb), _p(qual, u8p), text, _p(name_off, i64p),
+                            _p(kp, u8p) if kp is not None else None, buf, cap, C.byref(n))
+    if rc != MSG_OK:
+        raise MsgError(rc, "msg_fastq_format")
+    return buf.raw[:n.value]
 
 
 def sam_format(recs, md: bytes, seq, off, qual, cigar, names: bytes, name_off, chrom_names) -> bytes:

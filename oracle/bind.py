@@ -268,6 +268,8 @@ class Reference:
                                               C.POINTER(C.c_uint32), i64p, C.c_double, C.c_int, C.c_double,
                                               C.c_double, C.c_double, C.c_double, ip, C.c_int64, C.c_char_p,
                                               C.c_int64]
+        L.ref_fastq_rewrite.restype = C.c_int64
+        L.ref_fastq_rewrite.argtypes = [C.c_char_p, C.c_int64, u8p, C.c_char_p, C.c_int64]
         L.ref_fastq_parse.restype = C.c_int64
         L.ref_fastq_parse.argtypes = [C.c_char_p, C.c_int64, C.c_char_p, C.c_int64]
         L.ref_sam_from_records.restype = C.c_int64
@@ -448,6 +450,15 @@ class Reference:
         assert n <= cap
         out = buf.raw[:n].decode("latin-1")
         return out.split("\n")[:-1] if out else []
+
+    def fastq_rewrite(self, text: bytes, keep=None) -> bytes:
+        """The reference reading FASTQ text and writing the kept reads back."""
+        cap = 4 * len(text) + 1024
+        buf = C.create_string_buffer(cap)
+        kp = None if keep is None else np.ascontiguousarray(keep, dtype=np.uint8)
+        n = self.lib.ref_fastq_rewrite(text, len(text), _p(kp, u8p) if kp is not None else None, buf, cap)
+        assert n <= cap
+        return buf.raw[:n]
 
     @staticmethod
     def _pairing(pairing):

@@ -725,6 +725,23 @@ int64_t ref_fastq_parse(const char* text, int64_t len, char* out, int64_t cap) {
     return put_out(s, out, cap);
 }
 
+/* The reference reading a FASTQ text and writing back the reads whose
+ * keep[i] is set (every read when keep is NULL), as msgseqtk-clean does
+ * (SeqIO::nextSeq, SeqIO::writeSeq; src/msgseqtk-clean.cpp:420-435). */
+int64_t ref_fastq_rewrite(const char* text, int64_t len, const uint8_t* keep, char* out, int64_t cap) {
+    std::istringstream in(std::string(text, text + len));
+    std::ostringstream os;
+    SeqIO io(&in, SeqIO::FASTQ);
+    SeqIO wo(&os, SeqIO::FASTQ);
+    int64_t i = 0;
+    while (io.hasNext()) {
+        const PrimarySeq r = io.nextSeq();
+        if (!keep || keep[i]) wo.writeSeq(r);
+        ++i;
+    }
+    return put_out(os.str(), out, cap);
+}
+
 int ref_max_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

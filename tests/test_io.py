@@ -68,6 +68,20 @@ def test_fastq_parse_matches_reference_reader():
     assert _ours_lines(lib.fastq_parse(t)) == ref.fastq_parse(t)
 
 
+@needs_ref
+def test_fastq_format_matches_reference_writer():
+    """Reads parsed and written back (all, or a kept subset as msgseqtk-clean
+    writes them) give the reference's SeqIO output byte for byte."""
+    ref = Reference([synth.small_genomes(seed=1, n_genomes=1, length=2000)[0]])
+    for seed in (6, 7):
+        text = _fastq_text(seed)
+        r = lib.fastq_parse(text)
+        assert lib.fastq_format(r["seq"], r["off"], r["qual"], r["text"], r["name_off"]) == ref.fastq_rewrite(text)
+        keep = (np.arange(len(r["off"]) - 1) % 3 != 1).astype(np.uint8)
+        assert lib.fastq_format(r["seq"], r["off"], r["qual"], r["text"], r["name_off"], keep) == \
+            ref.fastq_rewrite(text, keep)
+
+
 def test_fastq_parse_streams_in_pieces():
     text = _fastq_text(5)
     whole = lib.fastq_parse(text)
