@@ -242,6 +242,12 @@ __global__ void k_clean_lod(const double* __restrict__ ll, int64_t n, int n_set,
     keep[i] = d > min_lod;
 }
 
+// off[i] -= base for i < n (host offsets rebased to their set's first read).
+__global__ void k_rebase(int64_t* __restrict__ off, int64_t n, int64_t base) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) off[i] -= base;
+}
+
 // Rows of unit i from its slot to its place in read order.
 __global__ void k_compact_rows(const int64_t* __restrict__ slot, const int64_t* __restrict__ dst,
                                const int32_t* __restrict__ cnt, int64_t n, const int64_t* __restrict__ src,
@@ -286,23 +292,25 @@ int upload_sets(msg_ctx* ctx, const msg_read_batch* const* sets, int n_set, Set*
     cudaError_t e = ctx->reads.ensure(bytes[0] + bytes[1] + 16);
     if (e == cudaSuccess) e = ctx->offs.ensure(n_set * (n + 1) * 8 + 16);
     if (e != cudaSuccess) return ctx->cuda_fail(e);
-    std::vector<int64_t> off0(n_set * (n + 1));
-    int64_t base = 0;
+    // the caller's bytes and offsets are copied as they are (straight from
+    // pinned memory when the caller pinned them) and each set's offsets
+    // rebased on the device; the call returns only after its last copy
     for (int k = 0; k < n_set; ++k) {
         const msg_read_batch* r = sets[k];
-        for (int64_t i = 0; i <= n; ++i) off0[k * (n + 1) + i] = n > 0 ? r->off[i] - r->off[0] : 0;
-        if (bytes[k] > 0) {
-            e = cudaMemcpyAsync(ctx->reads.as<uint8_t>() + base, r->seq + r->off[0], bytes[k], cudaMemcpyHostToDevice,
-                                ctx->stream);
-            if (e != cudaSuccess) return ctx->cuda_fail(e);
+        uint8_t* d_seq = ctx->reads.as<uint8_t>() + (k ? bytes[0] : 0);
+        int64_t* d_off = ctx->offs.as<int64_t>() + k * (n + 1);
+        if (bytes[k] > 0) e = cudaMemcpyAsync(d_seq, r->seq + r->off[0], bytes[k], cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(d_off, r->off, (n + 1) * 8, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess && n > 0 && r->off[0] != 0) {
+            k_rebase<<<nblk(n + 1, 256), 256, 0, ctx->stream>>>(d_off, n + 1, r->off[0]);
+            e = cudaGetLastError();
         }
-        dev[k].seq = ctx->reads.as<uint8_t>() + base;
-        dev[k].off = ctx->offs.as<int64_t>() + k * (n + 1);
-        base += bytes[k];
+        if (e == cudaSuccess && n == 0) e = cudaMemsetAsync(d_off, 0, 8, ctx->stream);
+        if (e != cudaSuccess) return ctx->cuda_fail(e);
+        dev[k].seq = d_seq;
+        dev[k].off = d_off;
     }
-    e = cudaMemcpyAsync(ctx->offs.p, off0.data(), off0.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    return e == cudaSuccess ? MSG_OK : ctx->cuda_fail(e);
+    return MSG_OK;
 }
 
 // Launch the MEM walk of n_set read sets (n reads each) against ctx's index
