@@ -683,6 +683,16 @@ class Database:
                     bd_end=arr(m.bd_end, m.n_chrom), chr_len=arr(m.chr_len, m.n_chrom),
                     chr_off=arr(m.chr_off, m.n_chrom + 1), chr_seq=arr(m.chr_seq, int(m.chr_off[m.n_chrom])))
 
+    def view(self):
+        """The database as an index view (msgseqtk_b200.index_build.FmdView),
+        e.g. for Context.load_index or the oracle."""
+        from .index_build import FmdView as View
+        a = self.arrays()
+        return View(int(self.fmd.n), a["bwt"].astype(np.uint8), a["B"].astype(np.int64),
+                    a["sample_rows"].astype(np.int64), a["sample_vals"].astype(np.int64),
+                    a["bd_start"].astype(np.int64), a["bd_end"].astype(np.int64), a["chr_len"].astype(np.int64),
+                    a["chr_seq"].astype(np.uint8), a["chr_off"].astype(np.int64))
+
     def close(self):
         if self.h:
             self.lib.msg_db_free(self.h)

@@ -289,6 +289,26 @@ class Reference:
                                         _p(k[1], i64p), len(k[2]), _p(k[2], i64p), _p(k[3], i64p), _p(k[4], i64p))
         self.n = L.ref_db_length(self.h)
 
+    @classmethod
+    def merged(cls, chroms_a, chroms_b, so: str = REF_SO):
+        """The DB msgseqtk-mergedb makes from a DB of chroms_a and one of
+        chroms_b (MetaGenome/FMDIndex append, updateIndex, buildSA)."""
+        self = cls.__new__(cls)
+        self.lib = L = cls(chroms_a[:1], so).lib  # declares the signatures
+        L.ref_db_merge.restype = C.c_void_p
+        L.ref_db_merge.argtypes = [C.c_int64, u8p, i64p, C.c_int64, u8p, i64p]
+        keep = []
+        args = []
+        for ch in (chroms_a, chroms_b):
+            seqs = np.ascontiguousarray(np.concatenate(ch).astype(np.uint8))
+            offs = np.zeros(len(ch) + 1, dtype=np.int64)
+            np.cumsum([len(c) for c in ch], out=offs[1:])
+            keep += [seqs, offs]
+            args += [len(ch), _p(seqs, u8p), _p(offs, i64p)]
+        self.h = L.ref_db_merge(*args)
+        self.n = L.ref_db_length(self.h)
+        return self
+
     def __del__(self):
         try:
             self.lib.ref_db_free(self.h)

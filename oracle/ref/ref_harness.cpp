@@ -121,6 +121,34 @@ void* ref_db_from_view(int64_t n_chrom, const uint8_t* seqs, const int64_t* offs
     return db;
 }
 
+/* msgseqtk-mergedb's merge (src/msgseqtk-mergedb.cpp:235-262) of two DBs
+ * built as ref_db_build does (genome names a<k> and b<k>): the MetaGenome and
+ * the FMD-index of the second appended to the first (BWT merge), then
+ * updateIndex and buildSA. */
+void* ref_db_merge(int64_t na, const uint8_t* seqs_a, const int64_t* offs_a, int64_t nb, const uint8_t* seqs_b,
+                   const int64_t* offs_b) {
+    auto build = [](int64_t n, const uint8_t* seqs, const int64_t* offs, const char* tag) {
+        RefDB* db = new RefDB();
+        for (int64_t k = 0; k < n; ++k) {
+            Genome g(tag + std::to_string(k), "genome " + std::string(tag) + std::to_string(k));
+            DNAseq s(seqs + offs[k], seqs + offs[k + 1]);
+            g.addChrom(std::string(tag) + "chr" + std::to_string(k), s);
+            db->mtg.addGenome(g);
+        }
+        db->mtg.updateIndex();
+        db->fmd = FMDIndex(db->mtg.getBDSeq(), true, FMDIndex::SA_SAMPLE_RATE);
+        return db;
+    };
+    RefDB* a = build(na, seqs_a, offs_a, "a");
+    RefDB* b = build(nb, seqs_b, offs_b, "b");
+    a->mtg += b->mtg;
+    a->fmd += b->fmd;
+    delete b;
+    a->mtg.updateIndex();
+    a->fmd.buildSA(FMDIndex::SA_SAMPLE_RATE);
+    return a;
+}
+
 void ref_db_free(void* h) { delete (RefDB*)h; }
 
 int64_t ref_db_length(void* h) { return ((RefDB*)h)->fmd.length(); }

@@ -1,6 +1,8 @@
 """Reading msgseqtk-build's database files (msg_db_read): the reference writes
 a DB with its own save functions; the decoded BWT, base counts, SA samples
-and MetaGenome tables must equal the reference's in-memory index."""
+and MetaGenome tables must equal the reference's in-memory index. Merged DBs
+(msgseqtk-mergedb: BWT merge of two DBs, then buildSA) are read and mapped
+the same way."""
 import os
 
 import numpy as np
@@ -73,6 +75,62 @@ def test_index_from_db_files_maps_like_view(tmp_path):
         for k in ("aln", "cigar", "read_aln_off"):
             assert np.array_equal(a[k], b[k]), k
         assert len(a["aln"]) > 0
+    finally:
+        c.close()
+        db.close()
+
+
+def _merged(tmp_path):
+    ga = synth.small_genomes(seed=31, n_genomes=2, length=25_000)
+    gb = synth.repeat_genomes(seed=32, n_genomes=2, length=20_000)
+    ref = Reference.merged(ga, gb)
+    paths = [tmp_path / "m.mtg", tmp_path / "m.mgs", tmp_path / "m.fmd"]
+    ref.save(*paths)
+    return ga + gb, ref, paths
+
+
+@needs_ref
+def test_merged_db_decodes_and_maps_like_reference(tmp_path, oracle_built):
+    """A merged DB read from its files equals the reference's merged index,
+    and the oracle on it aligns reads exactly as the reference does."""
+    from oracle.bind import Oracle
+    g, ref, paths = _merged(tmp_path)
+    db = lib.Database(*paths, n_threads=4)
+    a = db.arrays()
+    assert np.array_equal(a["bwt"], ref.bwt())
+    rows, vals = ref.sa_samples()
+    assert np.array_equal(a["sample_rows"], rows) and np.array_equal(a["sample_vals"], vals)
+    assert np.array_equal(a["chr_seq"], np.concatenate(g))
+    view = db.view()
+    orc = Oracle(view)
+    rs = synth.sample_reads(g, 80, seed=33, sub_rate=0.02, indel_rate=0.005)
+    for i in range(len(rs)):
+        r = rs.read(i)
+        assert np.array_equal(orc.smems(r), ref.smems(r))
+        exp = ref.align_read(r)
+        got = orc.align_read(r)
+        assert [(e["tid"], e["strand"], e["aln_start"], int(e["aln_score"]), e["cigar"]) for e in got] == \
+            [(e["tid"], e["strand"], e["aln_start"], int(e["aln_score"]), e["cigar"]) for e in exp]
+    db.close()
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_gpu_maps_merged_db_like_oracle(tmp_path, oracle_built):
+    from oracle.bind import Oracle
+    g, ref, paths = _merged(tmp_path)
+    db = lib.Database(*paths)
+    orc = Oracle(db.view())
+    rs = synth.sample_reads(g, 300, seed=34, sub_rate=0.02, indel_rate=0.005)
+    c = lib.Context(0)
+    try:
+        c.load_database(db)
+        res = c.map(rs.seqs, rs.offs)
+        for i in range(len(rs)):
+            got = res["aln"][res["read_aln_off"][i]:res["read_aln_off"][i + 1]]
+            exp = orc.align_read(rs.read(i))
+            assert [(int(x["tid"]), int(x["strand"]), int(x["aln_start"]), int(x["aln_score"])) for x in got] == \
+                [(e["tid"], e["strand"], e["aln_start"], int(e["aln_score"])) for e in exp]
     finally:
         c.close()
         db.close()
