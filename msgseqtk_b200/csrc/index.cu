@@ -98,6 +98,37 @@ __global__ void k_recover_sa(IndexDev ix, const int64_t* __restrict__ rows, cons
     atomicOr(err, kErrInternal);
 }
 
+// FMDIndex::accessSA (FMDIndex.cpp:520-527) for the rows of '$'-suffixes
+// [0, d): LF-walk over base symbols until a sampled row, whose value plus the
+// steps walked is the row's value. Used when those rows are not in the order
+// a whole-text suffix sort gives them (databases merged by the reference's
+// BWT merge, FMDIndex::append); a walk never meets a '$' because rows whose
+// symbol is '$' are samples.
+__global__ void k_dollar_sa(IndexDev ix, const int64_t* __restrict__ srows, const int64_t* __restrict__ svals,
+                            int64_t ns, int64_t d, int64_t* __restrict__ out, uint32_t* __restrict__ err,
+                            int64_t max_walk) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= d) return;
+    int64_t row = r, dist = 0;
+    for (int64_t step = 0; step <= max_walk; ++step) {
+        int64_t lo = 0, hi = ns;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (srows[mid] < row) lo = mid + 1; else hi = mid;
+        }
+        if (lo < ns && srows[lo] == row) {
+            out[r] = svals[lo] + dist;
+            return;
+        }
+        const int b = bwt_at(ix, row);
+        if (b == 0) break;
+        const Occ5 o = occ5(ix, row);
+        row = ix.C[b] + o.c[to_int(b)] - 1;
+        ++dist;
+    }
+    atomicOr(err, kErrInternal);
+}
+
 __global__ void k_occ_query(IndexDev ix, int64_t cnt, const uint8_t* __restrict__ b, const int64_t* __restrict__ i,
                             int64_t* __restrict__ out) {
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -240,18 +271,56 @@ extern "C" int msg_index_load(msg_ctx* ctx, const msg_fmd_view* fmd, const msg_m
             frows.push_back((int64_t)frows.size());
             fvals.push_back(v - 1);
         }
-        if ((int64_t)frows.size() != nd) { rc = ctx->fail(MSG_EINVAL, "SA samples inconsistent with '$' rows"); goto done; }
         std::vector<int64_t> arows, avals;
-        arows.reserve(ns + nd);
-        avals.reserve(ns + nd);
-        size_t a = 0, f = 0;
-        while (a < srows.size() || f < frows.size()) {  // merge, dropping duplicates
-            if (f == frows.size() || (a < srows.size() && srows[a] < frows[f])) { arows.push_back(srows[a]); avals.push_back(svals[a]); ++a; }
-            else if (a == srows.size() || frows[f] < srows[a]) { arows.push_back(frows[f]); avals.push_back(fvals[f]); ++f; }
-            else {
-                if (svals[a] != fvals[f]) { rc = ctx->fail(MSG_EINVAL, "SA sample disagrees with the '$' rows"); goto done; }
-                arows.push_back(srows[a]); avals.push_back(svals[a]); ++a; ++f;
+        // start rows: the samples merged with the '$'-suffix rows, dropping
+        // duplicates; false when a duplicate's values disagree
+        auto merge_starts = [&]() {
+            arows.clear();
+            avals.clear();
+            arows.reserve(ns + nd);
+            avals.reserve(ns + nd);
+            size_t a = 0, f = 0;
+            while (a < srows.size() || f < frows.size()) {
+                if (f == frows.size() || (a < srows.size() && srows[a] < frows[f])) { arows.push_back(srows[a]); avals.push_back(svals[a]); ++a; }
+                else if (a == srows.size() || frows[f] < srows[a]) { arows.push_back(frows[f]); avals.push_back(fvals[f]); ++f; }
+                else {
+                    if (svals[a] != fvals[f]) return false;
+                    arows.push_back(srows[a]); avals.push_back(svals[a]); ++a; ++f;
+                }
             }
+            return true;
+        };
+        if ((int64_t)frows.size() != nd || !merge_starts()) {
+            // the '$'-suffix rows are not in whole-text order (a merged
+            // database): their values by accessSA walks on the device
+            int64_t* d_sr = nullptr;
+            int64_t* d_sv = nullptr;
+            int64_t* d_dv = nullptr;
+            cudaError_t e1 = cudaMalloc(&d_sr, (ns + 1) * sizeof(int64_t));
+            if (e1 == cudaSuccess) e1 = cudaMalloc(&d_sv, (ns + 1) * sizeof(int64_t));
+            if (e1 == cudaSuccess) e1 = cudaMalloc(&d_dv, (nd + 1) * sizeof(int64_t));
+            if (e1 == cudaSuccess) e1 = cudaMemcpyAsync(d_sr, srows.data(), ns * sizeof(int64_t), cudaMemcpyHostToDevice, st);
+            if (e1 == cudaSuccess) e1 = cudaMemcpyAsync(d_sv, svals.data(), ns * sizeof(int64_t), cudaMemcpyHostToDevice, st);
+            if (e1 == cudaSuccess) e1 = cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), st);
+            if (e1 == cudaSuccess && nd > 0) {
+                k_dollar_sa<<<blocks_for(nd, 128), 128, 0, st>>>(ix, d_sr, d_sv, ns, nd, d_dv, d_bad,
+                                                                 std::min<int64_t>(n + 1, (int64_t)1 << 22));
+                e1 = cudaGetLastError();
+            }
+            fvals.assign(nd, 0);
+            if (e1 == cudaSuccess && nd > 0)
+                e1 = cudaMemcpyAsync(fvals.data(), d_dv, nd * sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+            uint32_t bad1 = 0;
+            if (e1 == cudaSuccess) e1 = cudaMemcpyAsync(&bad1, d_bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+            if (e1 == cudaSuccess) e1 = cudaStreamSynchronize(st);
+            cudaFree(d_sr);
+            cudaFree(d_sv);
+            cudaFree(d_dv);
+            if (e1 != cudaSuccess) { rc = ctx->cuda_fail(e1); goto done; }
+            if (bad1) { rc = ctx->fail(MSG_EINVAL, "a '$'-suffix row reaches no SA sample"); goto done; }
+            frows.resize(nd);
+            for (int64_t r = 0; r < nd; ++r) frows[r] = r;
+            if (!merge_starts()) { rc = ctx->fail(MSG_EINVAL, "SA sample disagrees with the '$' rows"); goto done; }
         }
         const int64_t m = (int64_t)arows.size();
         int64_t* d_rows = nullptr;
