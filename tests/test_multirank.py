@@ -45,3 +45,33 @@ def test_two_rank_reduction_and_disjoint_shards():
 def test_single_rank_reduction_is_identity():
     import bench
     assert bench.reduce_over_ranks(3.5, 7.0, "cpu") == (3.5, 7.0)
+
+
+def _clean_worker(rank, world, port, out):
+    import argparse
+    import torch.distributed as dist
+    import bench
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        args = argparse.Namespace(seed=2, genomes=2, median=2e4, pairs=40)
+        g_ref, g_bg, v_ref, v_bg, s1, o1, s2, o2, _ = bench.clean_workload(args, rank, "cpu")
+        ms, n = bench.reduce_over_ranks(1.0 + rank, 2.0 * (len(o1) - 1), "cpu")
+        out[rank] = (v_ref.bwt.tobytes(), v_bg.bwt.tobytes(), s1.tobytes(), s2.tobytes(), len(o1) - 1, ms, n)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_clean_shards():
+    """The clean workload under 2 gloo ranks: both indexes replicated, each
+    rank its own pairs (weak scaling), time max and reads summed."""
+    port = _free_port()
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.start_processes(_clean_worker, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
+    a, b = out[0], out[1]
+    assert a[0] == b[0] and a[1] == b[1]            # replicated indexes
+    assert a[2] != b[2] and a[3] != b[3]            # disjoint read shards
+    assert a[4] == b[4] == 40
+    assert a[5] == b[5] == 2.0 and a[6] == b[6] == 160.0
