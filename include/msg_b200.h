@@ -1,6 +1,8 @@
 /*
  * msg_b200.h -- C ABI of the B200 (sm_100a) read-mapping library that stands
- * in for MSGseqTK's seeding -> locate -> chaining -> DP path.
+ * in for MSGseqTK's seeding -> locate -> chaining -> DP path, with the host
+ * pieces around it (database files, FASTQ in, the likelihood/MAPQ/pairing
+ * tail, SAM text out) and msgseqtk-clean's MEM log-odds path.
  *
  * The reference has no FFI; its "operator API" is a set of C++ classes called
  * from the per-read task bodies of msgseqtk-align (src/msgseqtk-align.cpp:610-628
