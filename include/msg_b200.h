@@ -428,6 +428,15 @@ int msg_fastq_parse(const char* text, int64_t len, int at_eof, msg_fastq_batch* 
 int msg_fastq_format(const msg_read_batch* reads, const uint8_t* quals, const char* text, const int64_t* name_off,
                      const uint8_t* keep, char* out, int64_t cap, int64_t* text_len);
 
+/* msgseqtk-clean's read-assignment lines (--assign; src/msgseqtk-clean.cpp:
+ * 436-437, 473-474): "id\tdescription\trefLoglik\tbgLoglik\tLOD" per read,
+ * the numbers as a C++ ostream prints a double by default, from
+ * msg_fastq_parse's name lines and msg_clean_batch's outputs. The file's
+ * header lines are the caller's. Writes *text_len bytes into out (cap bytes;
+ * MSG_EINVAL with *text_len set when they do not fit). */
+int msg_clean_format(const char* text, const int64_t* name_off, int64_t n, const double* ref_loglik,
+                     const double* bg_loglik, const double* lod, char* out, int64_t cap, int64_t* text_len);
+
 /* SAM text lines of msg_tail_batch / msg_tail_pe_batch records, laid out as
  * htslib's sam_format1 prints the BAM records msgseqtk-align writes: QNAME
  * (the read's name from its "name\tdescription" text line), FLAG, RNAME

@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <sstream>
 #include <string>
 
 #include "../../include/msg_b200.h"
@@ -208,6 +209,29 @@ extern "C" int msg_fastq_format(const msg_read_batch* reads, const uint8_t* qual
         for (int64_t k = 0; k < L; ++k) s += (char)((quals ? quals[a + k] : 0) + 33);
         s += '\n';
     }
+    *text_len = (int64_t)s.size();
+    if ((int64_t)s.size() > cap || (!s.empty() && !out)) return MSG_EINVAL;
+    if (!s.empty()) std::memcpy(out, s.data(), s.size());
+    return MSG_OK;
+}
+
+extern "C" int msg_clean_format(const char* text, const int64_t* name_off, int64_t n, const double* ref_loglik,
+                                const double* bg_loglik, const double* lod, char* out, int64_t cap,
+                                int64_t* text_len) {
+    if (!text_len || n < 0 || cap < 0 || (n > 0 && (!text || !name_off || !ref_loglik || !bg_loglik || !lod)))
+        return MSG_EINVAL;
+    // msgseqtk-clean's assignment line (src/msgseqtk-clean.cpp:436-437):
+    // id, description and the three values through an ostream's defaults
+    std::ostringstream os;
+    for (int64_t i = 0; i < n; ++i) {
+        const char* t = text + name_off[i];
+        const int64_t tl = name_off[i + 1] - name_off[i] - 1;
+        const char* tab = static_cast<const char*>(std::memchr(t, '\t', tl > 0 ? tl : 0));
+        const std::string id = tab ? std::string(t, tab) : std::string(t, tl > 0 ? tl : 0);
+        const std::string desc = tab ? std::string(tab + 1, t + tl) : std::string();
+        os << id << "\t" << desc << "\t" << ref_loglik[i] << "\t" << bg_loglik[i] << "\t" << lod[i] << "\n";
+    }
+    const std::string s = os.str();
     *text_len = (int64_t)s.size();
     if ((int64_t)s.size() > cap || (!s.empty() && !out)) return MSG_EINVAL;
     if (!s.empty()) std::memcpy(out, s.data(), s.size());

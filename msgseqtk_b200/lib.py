@@ -31,7 +31,7 @@ EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy"
            "msg_map_params_default", "msg_map_batch", "msg_map_batches", "msg_map_batch_device", "msg_last_stats",
            "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
            "msg_band_train", "msg_band_grad", "msg_tail_params_default", "msg_tail_batch", "msg_pair_params_default", "msg_tail_pe_batch",
-           "msg_fastq_parse", "msg_fastq_format", "msg_sam_format",
+           "msg_fastq_parse", "msg_fastq_format", "msg_clean_format", "msg_sam_format",
            "msg_mem_params_default", "msg_mem_batch", "msg_clean_batch",
            "msg_clean_batch_device", "msg_occ_query", "msg_bi_ext_query", "msg_sa_query"]
 
@@ -171,6 +171,8 @@ def load_library(path: str = LIB_PATH):
         L.msg_tail_batch.argtypes[7:]
     L.msg_fastq_parse.argtypes = [C.c_char_p, C.c_int64, C.c_int, C.POINTER(FastqBatch), i64p]
     L.msg_fastq_format.argtypes = [C.POINTER(ReadBatch), u8p, C.c_char_p, i64p, u8p, C.c_char_p, C.c_int64, i64p]
+    L.msg_clean_format.argtypes = [C.c_char_p, i64p, C.c_int64] + [C.POINTER(C.c_double)] * 3 + \
+        [C.c_char_p, C.c_int64, i64p]
     L.msg_sam_format.argtypes = [C.c_void_p, C.c_int64, C.c_char_p, C.POINTER(ReadBatch), u8p,
                                  C.POINTER(C.c_uint32), C.c_char_p, i64p, C.POINTER(C.c_char_p), C.c_int64, C.c_char_p,
                                  C.c_int64, i64p]
@@ -306,6 +308,22 @@ def fastq_format(seq, off, qual, text: bytes, name_off, keep=None) -> bytes:
                             _p(kp, u8p) if kp is not None else None, buf, cap, C.byref(n))
     if rc != MSG_OK:
         raise MsgError(rc, "msg_fastq_format")
+    return buf.raw[:n.value]
+
+
+def clean_format(text: bytes, name_off, ref_ll, bg_ll, lod) -> bytes:
+    """msg_clean_format: msgseqtk-clean's assignment lines."""
+    L = load_library()
+    name_off = np.ascontiguousarray(name_off, dtype=np.int64)
+    arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (ref_ll, bg_ll, lod)]
+    dp = C.POINTER(C.c_double)
+    n = C.c_int64(0)
+    cap = len(text) + 96 * (len(name_off) - 1) + 16
+    buf = C.create_string_buffer(cap)
+    rc = L.msg_clean_format(text, _p(name_off, i64p), len(name_off) - 1, *[a.ctypes.data_as(dp) for a in arrs], buf,
+                            cap, C.byref(n))
+    if rc != MSG_OK:
+        raise MsgError(rc, "msg_clean_format")
     return buf.raw[:n.value]
 
 

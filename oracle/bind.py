@@ -268,6 +268,9 @@ class Reference:
                                               C.POINTER(C.c_uint32), i64p, C.c_double, C.c_int, C.c_double,
                                               C.c_double, C.c_double, C.c_double, ip, C.c_int64, C.c_char_p,
                                               C.c_int64]
+        L.ref_clean_assign.restype = C.c_int64
+        L.ref_clean_assign.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p, C.c_int64, C.c_int64, C.c_double,
+                                       C.c_char_p, C.c_int64]
         L.ref_fastq_rewrite.restype = C.c_int64
         L.ref_fastq_rewrite.argtypes = [C.c_char_p, C.c_int64, u8p, C.c_char_p, C.c_int64]
         L.ref_fastq_parse.restype = C.c_int64
@@ -470,6 +473,14 @@ class Reference:
         assert n <= cap
         out = buf.raw[:n].decode("latin-1")
         return out.split("\n")[:-1] if out else []
+
+    def clean_assign(self, bg, text: bytes, min_len=17, max_evalue=0.01) -> bytes:
+        """msgseqtk-clean's assignment lines for the reads of a FASTQ text."""
+        cap = 4 * len(text) + 1024
+        buf = C.create_string_buffer(cap)
+        n = self.lib.ref_clean_assign(self.h, bg.h, text, len(text), min_len, max_evalue, buf, cap)
+        assert n <= cap
+        return buf.raw[:n]
 
     def fastq_rewrite(self, text: bytes, keep=None) -> bytes:
         """The reference reading FASTQ text and writing the kept reads back."""

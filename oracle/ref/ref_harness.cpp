@@ -770,6 +770,29 @@ int64_t ref_fastq_rewrite(const char* text, int64_t len, const uint8_t* keep, ch
     return put_out(os.str(), out, cap);
 }
 
+/* msgseqtk-clean's single-end task with --assign over a FASTQ text
+ * (src/msgseqtk-clean.cpp:423-440, restated: it lives in the program file):
+ * the assignment line of every read. */
+int64_t ref_clean_assign(void* h_ref, void* h_bg, const char* text, int64_t len, int64_t min_len, double max_evalue,
+                         char* out, int64_t cap) {
+    RefDB* rdb = (RefDB*)h_ref;
+    RefDB* bdb = (RefDB*)h_bg;
+    std::istringstream in(std::string(text, text + len));
+    SeqIO io(&in, SeqIO::FASTQ);
+    std::ostringstream assignOut;
+    while (io.hasNext()) {
+        const PrimarySeq read = io.nextSeq();
+        MEM_LIST refMems = SMEM_LIST::findMEMS(&read, &rdb->mtg, &rdb->fmd, min_len, max_evalue);
+        MEM_LIST bgMems = SMEM_LIST::findMEMS(&read, &bdb->mtg, &bdb->fmd, min_len, max_evalue);
+        const double refLoglik = refMems.loglik();
+        const double bgLoglik = bgMems.loglik();
+        const double lod = -refLoglik + bgLoglik;
+        assignOut << read.getName() << "\t" << read.getDesc() << "\t" << refLoglik << "\t" << bgLoglik << "\t" << lod
+                  << std::endl;
+    }
+    return put_out(assignOut.str(), out, cap);
+}
+
 int ref_max_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -82,6 +82,43 @@ def test_fastq_format_matches_reference_writer():
             ref.fastq_rewrite(text, keep)
 
 
+@needs_ref
+def test_clean_assignment_lines_match_reference(oracle_built):
+    """FASTQ in (msg_fastq_parse), the lists' loglik (the oracle, pinned to the
+    reference in test_clean.py) and msg_clean_format give the reference's
+    assignment file lines byte for byte (-inf and nan included)."""
+    g_ref = synth.small_genomes(seed=51, n_genomes=2, length=20_000)
+    g_bg = synth.small_genomes(seed=52, n_genomes=2, length=20_000)
+    ref, bg = Reference(g_ref), Reference(g_bg)
+    o_ref, o_bg = Oracle(index_build.build_view(g_ref)), Oracle(index_build.build_view(g_bg))
+    rng = np.random.default_rng(53)
+    recs = []
+    for k, gs in enumerate((g_ref, g_bg, g_ref)):
+        rs = synth.sample_reads(gs, 20, seed=54 + k)
+        for i in range(len(rs)):
+            s = "".join("$ACMGRSVTWYHKDBN"[x] for x in rs.read(i))
+            if k == 2 and i % 4 == 0:
+                s = s[:30] + "N" + s[31:]  # N inside a kept MEM: loglik -inf
+            recs.append(f"@read{k}_{i} desc {i}\n{s}\n+\n{'I' * len(s)}\n")
+    text = "".join(recs).encode()
+    exp = ref.clean_assign(bg, text)
+    r = lib.fastq_parse(text)
+    n = len(r["off"]) - 1
+    reads = [r["seq"][r["off"][i]:r["off"][i + 1]] for i in range(n)]
+    rl = np.array([o_ref.mems(x)[1] for x in reads])
+    bl = np.array([o_bg.mems(x)[1] for x in reads])
+    with np.errstate(invalid="ignore"):
+        lod = -rl + bl
+    got = lib.clean_format(r["text"], r["name_off"], rl, bl, lod)
+    assert got == exp
+    assert b"-inf" in got
+    # special values as an ostream prints them
+    t = b"a\td\nb\t\nc\t\n"
+    line = lib.clean_format(t, np.array([0, 4, 7, 10]), [float("nan"), -float("inf"), 1e-300],
+                            [123456789.0, 0.1, -0.0], [float("inf"), 2.5, 1e21])
+    assert line == b"a\td\tnan\t1.23457e+08\tinf\nb\t\t-inf\t0.1\t2.5\nc\t\t1e-300\t-0\t1e+21\n"
+
+
 def test_fastq_parse_streams_in_pieces():
     text = _fastq_text(5)
     whole = lib.fastq_parse(text)
