@@ -71,28 +71,33 @@ void md_tag(const uint8_t* q, const uint8_t* t, int64_t i, int64_t j, const uint
     for (int32_t w = 0; w < nc; ++w) {
         const int op = cg[w] & 0xf;
         if (op == kOpS) continue;
-        for (uint32_t r = 0; r < (cg[w] >> 4); ++r) {
-            int o = op;
-            if (op == kOpM) o = (q[i] & t[j]) ? 7 : 8;  // BAM_CEQUAL / BAM_CDIFF
-            switch (o) {
-                case 7: ++i; ++j; ++len; break;
-                case 8:
-                    put_count(md, len);
-                    len = 0;
-                    md.push_back(kDecode[t[j] & 15]);
-                    ++i; ++j;
-                    break;
-                case kOpI:
-                    if (prev != kOpI) put_count(md, len);
-                    len = 0;
-                    if (o != prev) md.push_back('^');
-                    md.push_back(kDecode[q[i] & 15]);
-                    ++i;
-                    break;
-                case kOpD: ++j; break;
-                default: break;
+        const uint32_t run = cg[w] >> 4;
+        if (op == kOpM) {  // '=' runs counted in a tight loop; each 'X' ends one
+            uint32_t r = 0;
+            while (r < run) {
+                while (r < run && (q[i] & t[j])) { ++i; ++j; ++len; ++r; }
+                if (r == run) { prev = 7; break; }  // BAM_CEQUAL
+                put_count(md, len);                 // BAM_CDIFF
+                len = 0;
+                md.push_back(kDecode[t[j] & 15]);
+                ++i; ++j; ++r;
+                prev = 8;
             }
-            prev = o;
+            continue;
+        }
+        for (uint32_t r = 0; r < run; ++r) {
+            if (op == kOpI) {
+                if (prev != kOpI) {
+                    put_count(md, len);
+                    md.push_back('^');
+                }
+                len = 0;
+                md.push_back(kDecode[q[i] & 15]);
+                ++i;
+            } else if (op == kOpD) {
+                ++j;
+            }
+            prev = op;
         }
     }
     put_count(md, len);
@@ -467,6 +472,7 @@ int tail_run(const msg_mtg_view* mtg, const msg_read_batch* reads, const uint8_t
         std::vector<int> mapq;
         const int64_t a = units * w / nt, b = units * (w + 1) / nt;
         parts[w].rec.reserve((size_t)(b - a) * (q ? 2 : 1) * std::max<uint32_t>(1, p->max_report));
+        parts[w].md.reserve((size_t)(b - a) * (q ? 2 : 1) * 16);
         for (int64_t u = a; u < b; ++u) {
             if (q) {
                 if (!valid(2 * u) || !valid(2 * u + 1)) { bad[w] = 1; return; }
