@@ -15,10 +15,10 @@ from oracle.bind import REF_SO, Oracle, Reference
 needs_ref = pytest.mark.skipif(not os.path.exists(REF_SO), reason="oracle/_ref not built")
 
 
-def _records_from_oracle(orc, reads):
+def _records_from_oracle(orc, reads, mode=0):
     recs, cig, roff = [], [], [0]
     for i, r in enumerate(reads):
-        for e in orc.align_read(r):
+        for e in orc.align_read(r, mode=mode):
             recs.append((i, e["tid"], e["strand"], e["t_start"], e["t_end"], e["aln_from"], e["aln_to"],
                          e["aln_start"], e["aln_end"],
                          int(e["aln_score"]) if np.isfinite(e["aln_score"]) else -(2 ** 31), e["flags"], len(cig),
@@ -176,6 +176,11 @@ def test_library_tail_matches_reference_tail_on_oracle_records(oracle_built):
     orc = Oracle(view)
     aln, cig, roff = _records_from_oracle(orc, reads)
     for rate, max_report in ((0.65, 1), (0.65, 0), (0.3, 3), (-1.0, 0)):
+        _check_tail(view, ref, seq, qual, off, aln, cig, roff, rate, max_report)
+    # local (Smith-Waterman) records: soft clips and evaluate's clip penalty
+    aln, cig, roff = _records_from_oracle(orc, reads, mode=1)
+    assert any((c & 0xf) == 4 for c in cig)
+    for rate, max_report in ((0.65, 1), (0.2, 0)):
         _check_tail(view, ref, seq, qual, off, aln, cig, roff, rate, max_report)
 
 
