@@ -146,6 +146,62 @@ double evaluate(const uint8_t* q, const uint8_t* qual, int64_t L, const uint8_t*
     return ll;
 }
 
+// evaluate and getAlnMDTag in one pass over the record's path (the same
+// sums in the same order, the same text): the MD scan runs beside the
+// dependent chain of log10P adds. For reads whose one kept record is also
+// the one reported.
+double evaluate_md(const uint8_t* q, const uint8_t* qual, int64_t L, const uint8_t* t, const msg_aln& a,
+                   const uint32_t* cg, const msg_tail_params& p, std::string& md) {
+    const QualTables& T = tables();
+    double ll = 0;
+    for (int64_t i = 0; i < a.aln_from; ++i) ll += -p.clip;
+    int64_t i = a.aln_from, j = a.aln_start;
+    int prev = -1;       // evaluate's previous op (M, I, D)
+    uint32_t len = 0;    // MD: '=' bases since the last mismatch or insertion
+    for (int32_t w = 0; w < a.n_cigar; ++w) {
+        const int op = cg[w] & 0xf;
+        if (op == kOpS) continue;
+        const uint32_t run = cg[w] >> 4;
+        if (op == kOpM) {
+            for (uint32_t r = 0; r < run; ++r, ++i, ++j) {
+                const bool eq = (q[i] & t[j]) != 0;
+                ll += eq ? T.match[qual[i]] : T.mis[qual[i]];
+                if (eq) {
+                    ++len;
+                } else {
+                    put_count(md, len);
+                    len = 0;
+                    md.push_back(kDecode[t[j] & 15]);
+                }
+            }
+            if (run) prev = kOpM;
+            continue;
+        }
+        for (uint32_t r = 0; r < run; ++r) {
+            const int qv = i < L ? qual[i] : 0;
+            if (op == kOpI) {
+                if (prev != kOpI) {
+                    ll += T.mis[qv] - p.gap_open;
+                    put_count(md, len);
+                    md.push_back('^');
+                }
+                ll += -p.gap_ext;
+                len = 0;
+                md.push_back(kDecode[q[i] & 15]);
+                ++i;
+            } else if (op == kOpD) {
+                if (prev != kOpD) ll += T.mis[qv] - p.gap_open;
+                ll += -p.gap_ext;
+                ++j;
+            }
+            prev = op;
+        }
+    }
+    put_count(md, len);
+    for (int64_t k = a.aln_to; k < L; ++k) ll += -p.clip;
+    return ll;
+}
+
 // One read's alignments after Alignment::filter and evaluate, with the
 // reverse-complemented read (PrimarySeq::revcom: bases reversed and
 // complemented, quality reversed) when a record needs it.
@@ -160,6 +216,8 @@ struct Mate {
     std::vector<double> pr, post;  // calcMapQ work and posterior
     std::vector<int> mapq;
     std::vector<size_t> ord;
+    std::string md1;               // MD text of the only kept record, made with its log10P
+    bool has_md1 = false;
 };
 
 void mate_eval(Mate& m, int64_t r, const uint8_t* seq, const uint8_t* qual, int64_t L, const msg_aln* aln,
@@ -190,12 +248,23 @@ void mate_eval(Mate& m, int64_t r, const uint8_t* seq, const uint8_t* qual, int6
     m.fq = qual ? qual : m.rq.data() + L;
     m.l10.resize(N);
     m.empty.resize(N);
+    m.has_md1 = false;
     for (size_t n = 0; n < N; ++n) {
         const msg_aln& a = aln[m.keep[n]];
         const bool rev = a.strand == 2;
         bool e;
-        m.l10[n] = evaluate(rev ? m.rc.data() : seq, rev ? m.rq.data() : m.fq, L, tg[a.tid].seq, a,
-                            cigar + a.cigar_off, p, &e);
+        if (N == 1) {  // its record is reported: log10P and MD in one pass
+            e = true;
+            for (int32_t w = 0; w < a.n_cigar; ++w)
+                if ((cigar[a.cigar_off + w] & 0xf) != kOpS && (cigar[a.cigar_off + w] >> 4) > 0) e = false;
+            m.md1.clear();
+            m.l10[0] = e ? 0 : evaluate_md(rev ? m.rc.data() : seq, rev ? m.rq.data() : m.fq, L, tg[a.tid].seq, a,
+                                           cigar + a.cigar_off, p, m.md1);
+            m.has_md1 = !e;
+        } else {
+            m.l10[n] = evaluate(rev ? m.rc.data() : seq, rev ? m.rq.data() : m.fq, L, tg[a.tid].seq, a,
+                                cigar + a.cigar_off, p, &e);
+        }
         m.empty[n] = e;
     }
 }
@@ -246,7 +315,9 @@ msg_sam_rec export_rec(const Mate& m, size_t n, const msg_aln* aln, const uint32
     o.cigar_off = a.cigar_off;
     o.n_cigar = a.n_cigar;
     o.md_off = (int64_t)md.size();
-    if (!m.empty[n])
+    if (m.has_md1 && n == 0)
+        md += m.md1;
+    else if (!m.empty[n])
         md_tag(a.strand == 2 ? m.rc.data() : m.seq, tg[a.tid].seq, a.aln_from, a.aln_start, cigar + a.cigar_off,
                a.n_cigar, md);
     o.md_len = (int32_t)((int64_t)md.size() - o.md_off);
