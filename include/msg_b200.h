@@ -347,7 +347,8 @@ typedef struct msg_sam_rec {
  * read's records from msg_map_batch (aln, cigar, read_aln_off as returned),
  * Alignment::filter, evaluate, calcMapQ and sort (src/Alignment.cpp:446-555,
  * src/Alignment.h:629-633), then the reported records in output order. quals
- * holds phred values (not ASCII) at the reads' offsets (NULL: all 0); mtg
+ * holds phred values (not ASCII) at the reads' offsets (NULL: 33 on every
+ * base, as PrimarySeq::fixQual gives reads without qualities); mtg
  * gives the forward chromosome sequences. Records go to out (out_cap), MD
  * texts to md (md_cap bytes); *n_out and *md_len receive the sizes needed,
  * and MSG_EINVAL is returned with nothing written when either exceeds its
@@ -422,7 +423,7 @@ int msg_fastq_parse(const char* text, int64_t len, int at_eof, msg_fastq_batch* 
  * when keep is NULL), as msgseqtk-clean writes the reads it keeps
  * (SeqIO::writeFastqSeq, src/SeqIO.cpp:107-116): "@name", " description"
  * when there is one, the bases decoded with DNAalphabet's symbols, "+", the
- * qualities + 33. Names and descriptions come from msg_fastq_parse's
+ * qualities + 33 (33 + 33 when quals is NULL). Names and descriptions come from msg_fastq_parse's
  * "name\tdescription\n" lines (text, name_off). Writes *text_len bytes into
  * out (cap bytes; MSG_EINVAL with *text_len set when they do not fit). */
 int msg_fastq_format(const msg_read_batch* reads, const uint8_t* quals, const char* text, const int64_t* name_off,
@@ -443,7 +444,8 @@ int msg_clean_format(const char* text, const int64_t* name_off, int64_t n, const
  * (chrom_names[tid], '*' when unmapped), POS (pos + 1), MAPQ, CIGAR ('*'
  * when empty), RNEXT '*' and PNEXT 1 (the records' mate fields are left at
  * -1 and 0, src/SAMtools/BAM.h:61-75), TLEN, SEQ and QUAL (reverse-
- * complemented and reversed when flag has 0x10; phred + 33), then AS:i, MD:Z,
+ * complemented and reversed when flag has 0x10; phred + 33, and 33 + 33 for
+ * every base when quals is NULL, as for reads without qualities), then AS:i, MD:Z,
  * XH:f, NH:i, XN:i, XP:f for mapped records, floats with %g (htslib's
  * exact float formatting is not pinned). Writes *text_len bytes into out
  * (cap bytes; MSG_EINVAL with *text_len set when they do not fit). */

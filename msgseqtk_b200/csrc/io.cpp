@@ -158,9 +158,9 @@ extern "C" int msg_sam_format(const msg_sam_rec* recs, int64_t n_recs, const cha
         if (L == 0) s += "*";
         for (int64_t i = 0; i < L; ++i) s += kSeq[rev ? kComp[reads->seq[a + L - 1 - i] & 15] : reads->seq[a + i] & 15];
         s += '\t';
-        if (L == 0 || !quals) s += "*";
-        else
-            for (int64_t i = 0; i < L; ++i) s += (char)(quals[rev ? a + L - 1 - i : a + i] + 33);
+        if (L == 0) s += "*";
+        else  // a read without qualities has 33 on every base (PrimarySeq::fixQual)
+            for (int64_t i = 0; i < L; ++i) s += (char)((quals ? quals[rev ? a + L - 1 - i : a + i] : 33) + 33);
         if (!(r.flag & 0x4)) {
             std::snprintf(buf, sizeof buf, "\tAS:i:%d\tMD:Z:", r.as);
             s += buf;
@@ -206,7 +206,7 @@ extern "C" int msg_fastq_format(const msg_read_batch* reads, const uint8_t* qual
         const int64_t a = reads->off[i], L = reads->off[i + 1] - a;
         for (int64_t k = 0; k < L; ++k) s += kSym[reads->seq[a + k] & 15];
         s += "\n+\n";
-        for (int64_t k = 0; k < L; ++k) s += (char)((quals ? quals[a + k] : 0) + 33);
+        for (int64_t k = 0; k < L; ++k) s += (char)((quals ? quals[a + k] : 33) + 33);
         s += '\n';
     }
     *text_len = (int64_t)s.size();

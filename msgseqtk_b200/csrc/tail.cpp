@@ -22,6 +22,9 @@ constexpr double kMaxQ = 250;         // quality::MAX_Q_SCORE (src/QualStr.h:35)
 constexpr double kMinLoglikExp = -256;  // MIN_LOGLIK_EXP (src/MSGseqTKConst.h:36)
 constexpr int kOpM = 0, kOpI = 1, kOpD = 2, kOpS = 4;  // SAM CIGAR op codes
 constexpr int kFlagReverse = 0x10, kFlagSecondary = 0x100, kFlagUnmapped = 0x4;
+// quality of every base of a read without one: PrimarySeq::fixQual pads the
+// (empty) quality string to the read's length with 33 (src/PrimarySeq.h:105-109)
+constexpr uint8_t kNoQual = 33;
 const char kDecode[16] = {'$', 'A', 'C', 'M', 'G', 'R', 'S', 'V', 'T', 'W', 'Y', 'H', 'K', 'D', 'B', 'N'};
 
 // Per-quality terms of Alignment::evaluate (src/Alignment.cpp:461-465):
@@ -208,8 +211,8 @@ double evaluate_md(const uint8_t* q, const uint8_t* qual, int64_t L, const uint8
 struct Mate {
     int64_t read = 0, L = 0;
     const uint8_t* seq = nullptr;
-    const uint8_t* fq = nullptr;   // forward quality (zeros without one)
-    std::vector<uint8_t> rc, rq;   // reverse complement; reversed quality then zeros
+    const uint8_t* fq = nullptr;   // forward quality (33s without one)
+    std::vector<uint8_t> rc, rq;   // reverse complement; reversed quality, then 33s for reads without one
     std::vector<int64_t> keep;     // record indices kept by the filter, in record order
     std::vector<double> l10;       // log10P of each kept record
     std::vector<char> empty;       // a record without a path (evaluate skips it)
@@ -237,12 +240,12 @@ void mate_eval(Mate& m, int64_t r, const uint8_t* seq, const uint8_t* qual, int6
     bool any_rev = false;
     for (int64_t k : m.keep) any_rev |= aln[k].strand == 2;
     m.rq.resize(2 * L);
-    if (!qual) std::fill(m.rq.begin() + L, m.rq.end(), 0);
+    if (!qual) std::fill(m.rq.begin() + L, m.rq.end(), kNoQual);
     if (any_rev) {
         m.rc.resize(L);
         for (int64_t i = 0; i < L; ++i) {
             m.rc[i] = kComp[seq[L - 1 - i] & 15];
-            m.rq[i] = qual ? qual[L - 1 - i] : 0;
+            m.rq[i] = qual ? qual[L - 1 - i] : kNoQual;
         }
     }
     m.fq = qual ? qual : m.rq.data() + L;

@@ -177,6 +177,11 @@ def test_library_tail_matches_reference_tail_on_oracle_records(oracle_built):
     aln, cig, roff = _records_from_oracle(orc, reads)
     for rate, max_report in ((0.65, 1), (0.65, 0), (0.3, 3), (-1.0, 0)):
         _check_tail(view, ref, seq, qual, off, aln, cig, roff, rate, max_report)
+    # reads without qualities read 33 on every base (PrimarySeq::fixQual)
+    q33 = np.full_like(qual, 33)
+    a, ma = lib.tail(view, seq, off, None, aln, cig, roff)
+    b, mb = lib.tail(view, seq, off, q33, aln, cig, roff)
+    assert np.array_equal(a, b) and ma == mb
     # local (Smith-Waterman) records: soft clips and evaluate's clip penalty
     aln, cig, roff = _records_from_oracle(orc, reads, mode=1)
     assert any((c & 0xf) == 4 for c in cig)
