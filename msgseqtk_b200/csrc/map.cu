@@ -252,10 +252,14 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     int64_t* d_idx_off = d_chain_off + (n_reads + 1);
     unsigned long long h_maxlen = 0;
     if (n_reads > 0) {
+        uint32_t h_codes = 0;
+        S.n_launch++, k_check_codes<<<ctx->num_sms * 4, 256, 0, st>>>(d_seq, d_off, n_reads, d_status);
         S.n_launch++, k_read_len<<<nblk(n_reads, 256), 256, 0, st>>>(d_off, n_reads, d_rlen, d_ctr + 2);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(&h_maxlen, d_ctr + 2, 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&h_codes, d_status, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        if (h_codes & kErrCodes) return ctx->fail(MSG_EINVAL, "read bytes must be nt16 codes (0..15)");
     }
     const int64_t Lmax = (int64_t)h_maxlen;
 
@@ -1196,12 +1200,16 @@ extern "C" int msg_smem_batch_noalloc(msg_ctx* ctx, int64_t n_reads, const uint8
     e = cudaMemsetAsync(base, 0, kStaticHdr, st);
     if (e != cudaSuccess) return ctx->cuda_fail(e);
     k_maxlen<<<nblk(n_reads, 256), 256, 0, st>>>(d_off, n_reads, hdr + 2);
+    k_check_codes<<<ctx->num_sms * 4, 256, 0, st>>>(d_seq, d_off, n_reads, status);
     unsigned long long maxlen = 0;
+    uint32_t codes = 0;
     e = cudaMemcpyAsync(&maxlen, hdr + 2, sizeof(maxlen), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&codes, status, sizeof(codes), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return ctx->cuda_fail(e);
     if ((int64_t)maxlen > kStaticMaxReadLen)
         return ctx->fail(MSG_EINVAL, "a read is longer than MSG_NOALLOC_MAX_READ_LEN");
+    if (codes & kErrCodes) return ctx->fail(MSG_EINVAL, "read bytes must be nt16 codes (0..15)");
     SmemArgs sa{};
     sa.seq = d_seq; sa.off = d_off; sa.n_reads = n_reads; sa.min_len = params->min_len;
     sa.thr = thr; sa.thr_all = thr_all;

@@ -348,6 +348,18 @@ int mem_launch(msg_ctx* ctx, const msg_ctx* bg, const Set* sets, int n_set, int6
     a.n_ext = reinterpret_cast<unsigned long long*>(ctx->status.p);
     e = cudaMemsetAsync(ctx->status.p, 0, 128, ctx->stream);
     if (e != cudaSuccess) return ctx->cuda_fail(e);
+    if (n > 0) {  // the walks index 16-entry tables with the read bytes: check them first
+        uint32_t* codes = reinterpret_cast<uint32_t*>(ctx->status.p) + 4;
+        for (int k = 0; k < n_set; ++k)
+            k_check_codes<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(sets[k].seq, sets[k].off, n, codes);
+        ctx->stats.n_launch += n_set;
+        uint32_t h_codes = 0;
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&h_codes, codes, 4, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return ctx->cuda_fail(e);
+        if (h_codes & kErrCodes) return ctx->fail(MSG_EINVAL, "read bytes must be nt16 codes (0..15)");
+    }
     if (n_units > 0) {
         cudaStream_t st = ctx->stream;
         const int64_t g = nblk(n * n_set, 256);

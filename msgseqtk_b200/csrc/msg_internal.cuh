@@ -224,6 +224,20 @@ enum : uint32_t {
     kErrInternal = 1u,     // consistency check failed
     kErrOverflow = 2u,     // an output capacity was exceeded (host retries)
     kErrTrace = 4u,        // traceback left the matrix (reference would read out of bounds)
+    kErrCodes = 8u,        // a read byte is not an nt16 code (0..15)
 };
+
+// Every byte of the reads' range [off[0], off[n]) must be an nt16 code
+// (0..15, what DNAalphabet's encoder gives): the kernels index 16-entry
+// tables with them. Sets kErrCodes in *status otherwise. (static: one copy
+// per translation unit that launches it)
+static __global__ void k_check_codes(const uint8_t* __restrict__ seq, const int64_t* __restrict__ off, int64_t n,
+                              uint32_t* __restrict__ status) {
+    const int64_t a = off[0], b = off[n];
+    bool bad = false;
+    for (int64_t i = a + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < b; i += (int64_t)gridDim.x * blockDim.x)
+        bad |= __ldg(seq + i) > 15;
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(status, (uint32_t)kErrCodes);
+}
 
 }  // namespace msg

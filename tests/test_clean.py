@@ -194,6 +194,9 @@ def test_gpu_clean_rejects_bad_arguments(fx):
         assert e.value.code == lib.MSG_EINVAL
         ll, cnt, rows = a.mems(np.zeros(0, np.uint8), np.zeros(1, np.int64))
         assert len(ll) == 0 and len(rows) == 0
+        with pytest.raises(lib.MsgError) as e:  # ASCII instead of nt16 codes
+            a.clean(b, np.frombuffer(b"ACGTACGT", np.uint8), np.array([0, 8], np.int64))
+        assert e.value.code == lib.MSG_EINVAL
     finally:
         for c in (a, b, empty):
             c.close()

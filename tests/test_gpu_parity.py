@@ -277,3 +277,24 @@ def test_map_batches_equals_map_batch(oracle_built):
         assert np.array_equal(ro, expect[2]["read_aln_off"])
     finally:
         c.close()
+
+
+def test_read_bytes_must_be_nt16_codes(oracle_built):
+    """Bytes above 15 (e.g. ASCII letters) are rejected with MSG_EINVAL before
+    any kernel uses them; the context keeps working."""
+    g = synth.small_genomes(seed=91, n_genomes=1, length=20_000)
+    view = index_build.build_view(g)
+    c = lib.Context(0)
+    try:
+        c.load_index(view)
+        good = g[0][1000:1150].copy()
+        bad = np.frombuffer(b"ACGT" * 30, dtype=np.uint8).copy()
+        seq = np.concatenate([good, bad])
+        off = np.array([0, 150, 270], dtype=np.int64)
+        with pytest.raises(lib.MsgError) as e:
+            c.map(seq, off)
+        assert e.value.code == lib.MSG_EINVAL
+        res = c.map(good, np.array([0, 150], dtype=np.int64))
+        assert len(res["aln"]) >= 1
+    finally:
+        c.close()
