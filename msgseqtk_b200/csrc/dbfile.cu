@@ -230,24 +230,46 @@ bool read_fmd(const char* path, int n_threads, msg_db& db) {
     // BWT symbols: the walk of WaveletTreeRRR::access per row
     db.bwt.resize(n);
     bool bad = false;
+    // Rows are decoded in order, so the position a row reaches in a node of
+    // level l + 1 is that node's start plus the rows before it that took
+    // the same path: one cursor per node replaces the per-row rank queries
+    // of the access walk (the 0-child of a node starts where the node does,
+    // the 1-child at occ[symbol prefix]). A thread starting at row lo sets
+    // its cursors with rank queries at the boundary, node by node.
+    const uint64_t nodes = 1ull << height;
+    std::vector<uint64_t> node_start(height * nodes, 0);  // [l * nodes + prefix]
+    for (uint64_t l = 0; l + 1 < height; ++l) {
+        for (uint64_t q = 0; q < (1ull << l); ++q) {
+            // prefixes above the alphabet's largest symbol hold no rows: they
+            // start at n, where any row would be caught as corrupt
+            const uint64_t s1 = ((2 * q + 1) << (height - l - 1));
+            node_start[(l + 1) * nodes + 2 * q] = node_start[l * nodes + q];
+            node_start[(l + 1) * nodes + 2 * q + 1] = s1 < occ.size() ? occ[s1] : n;
+        }
+    }
     auto decode = [&](uint64_t lo, uint64_t hi) {
-        for (uint64_t row = lo; row < hi; ++row) {
-            uint64_t s = 0, start = 0, i = row;
-            for (uint64_t l = 0; l < height; ++l) {
-                const Plain& p = lv[l];
-                const uint64_t before = start > 0 ? p.rank1(start - 1) : 0;
-                const uint64_t r1 = p.rank1(i);
-                if (p.bit(i)) {
-                    s |= 1ull << (height - l - 1);
-                    if (s >= occ.size()) { bad = true; return; }
-                    start = occ[s];
-                    i = r1 - 1 - before + start;
-                } else {
-                    i = (i + 1 - r1) - 1 + before;
-                }
-                if (i >= n) { bad = true; return; }
+        std::vector<uint64_t> cur(height * nodes, 0);  // next position of each node
+        std::vector<uint64_t> cnt(height * nodes, 0);  // rows before lo in each node
+        cnt[0] = lo;
+        for (uint64_t l = 0; l + 1 < height; ++l) {
+            const Plain& p = lv[l];
+            for (uint64_t q = 0; q < (1ull << l); ++q) {
+                const uint64_t st = node_start[l * nodes + q], c = cnt[l * nodes + q];
+                if (st + c > n) { bad = true; return; }
+                const uint64_t ones = c > 0 ? p.rank1(st + c - 1) - (st > 0 ? p.rank1(st - 1) : 0) : 0;
+                cnt[(l + 1) * nodes + 2 * q + 1] = ones;
+                cnt[(l + 1) * nodes + 2 * q] = c - ones;
             }
-            db.bwt[row] = (uint8_t)s;
+        }
+        for (uint64_t k = 0; k < height * nodes; ++k) cur[k] = node_start[k] + cnt[k];
+        for (uint64_t row = lo; row < hi; ++row) {
+            uint64_t q = 0, i = row;
+            for (uint64_t l = 0; l < height; ++l) {
+                if (i >= n) { bad = true; return; }
+                q = 2 * q + (lv[l].bit(i) ? 1 : 0);
+                if (l + 1 < height) i = cur[(l + 1) * nodes + q]++;
+            }
+            db.bwt[row] = (uint8_t)q;
         }
     };
     const int nt = std::max(1, n_threads);
