@@ -158,15 +158,32 @@ struct Plain {
     }
 };
 
-bool read_rrr(Reader& r, const Rrr& tab, Plain& out) {
-    out.n = r.get<uint64_t>();
-    out.ones = r.get<uint64_t>();
-    Bits C, O, Cs, Os;
-    if (!C.read(r, 32) || !O.read(r, 32)) return false;
+// The stored parts of a BitSeqRRR (BitSeqRRR.cpp:308-360): block classes C
+// and offsets O; decoded by decode_rrr.
+struct RawRrr {
+    uint64_t n = 0, ones = 0, nC = 0;
+    Bits C, O;
+};
+
+bool parse_rrr(Reader& r, RawRrr& raw) {
+    raw.n = r.get<uint64_t>();
+    raw.ones = r.get<uint64_t>();
+    Bits Cs, Os;
+    if (!raw.C.read(r, 32) || !raw.O.read(r, 32)) return false;
     const uint64_t nC = r.get<uint64_t>(), wC = r.get<uint64_t>(), nO = r.get<uint64_t>(), wO = r.get<uint64_t>();
     if (!Cs.read(r, 64) || !Os.read(r, 64)) return false;
     for (int k = 0; k < 5; ++k) r.get<uint64_t>();  // nCsampled, wCsampled, nOsampled, wOsampled, sample_rate
-    if (!r.ok || wC != 4 || wO != 1 || nC != (out.n + 14) / 15 || O.nbits < nO) return false;
+    if (!r.ok || wC != 4 || wO != 1 || nC != (raw.n + 14) / 15 || raw.O.nbits < nO) return false;
+    raw.nC = nC;
+    return true;
+}
+
+bool decode_rrr(const RawRrr& raw, const Rrr& tab, Plain& out) {
+    out.n = raw.n;
+    out.ones = raw.ones;
+    const Bits& C = raw.C;
+    const Bits& O = raw.O;
+    const uint64_t nC = raw.nC;
     out.w.assign((out.n + 63) / 64 + 1, 0);
     uint64_t pos = 0, ones = 0;
     for (uint64_t b = 0; b < nC; ++b) {
@@ -219,12 +236,23 @@ bool read_fmd(const char* path, int n_threads, msg_db& db) {
     std::vector<uint64_t> occ(nocc);
     r.bytes(occ.data(), nocc * 8);
     const Rrr tab;
-    std::vector<Plain> lv(height);
+    // the bit sequences are read in file order, then unranked in parallel
+    std::vector<RawRrr> raw(height + 1);
     for (uint64_t l = 0; l < height; ++l)
-        if (!read_rrr(r, tab, lv[l]) || lv[l].n != n) return false;
+        if (!parse_rrr(r, raw[l]) || raw[l].n != n) return false;
     std::vector<int64_t> gap_sa, sa_sampled;
+    if (!read_i64s(r, gap_sa) || !parse_rrr(r, raw[height]) || !read_i64s(r, sa_sampled)) return false;
+    std::vector<Plain> lv(height);
     Plain saidx;
-    if (!read_i64s(r, gap_sa) || !read_rrr(r, tab, saidx) || !read_i64s(r, sa_sampled)) return false;
+    {
+        std::vector<char> ok(height + 1, 0);
+        std::vector<std::thread> th;
+        for (uint64_t l = 0; l <= height; ++l)
+            th.emplace_back([&, l]() { ok[l] = decode_rrr(raw[l], tab, l < height ? lv[l] : saidx); });
+        for (auto& x : th) x.join();
+        for (char x : ok) if (!x) return false;
+        raw.clear();
+    }
     if (saidx.n != n || (saidx.ones != sa_sampled.size() && saidx.ones != sa_sampled.size() + 1)) return false;
     for (int b = 0; b < 16; ++b) db.base_count[b] = B[b];
     // BWT symbols: the walk of WaveletTreeRRR::access per row
