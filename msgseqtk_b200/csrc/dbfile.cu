@@ -30,9 +30,10 @@
 // An RRR block of 15 bits is stored as its class k (popcount) and its offset
 // among the k-subsets of {0..14} listed in lexicographic order of their
 // positions (the table BitSeqRRR::TableOffset builds); the offset takes
-// bits(C(15, k) - 1) bits. Decoding unranks it. The wavelet tree is decoded
-// with the same walk as WaveletTreeRRR::access (WaveletTreeRRR.cpp:58-76)
-// over plain bit vectors with a rank directory, on several host threads.
+// bits(C(15, k) - 1) bits. Decoding unranks it (one thread per bit
+// sequence). The wavelet tree gives the positions WaveletTreeRRR::access
+// (WaveletTreeRRR.cpp:58-76) walks to; rows decoded in order reach them with
+// one cursor per tree node, on several host threads.
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
