@@ -13,6 +13,11 @@
  *
  * Threading: one host thread per msg_ctx (calls on one context are not
  * re-entrant); contexts are independent. Each context owns one CUDA stream.
+ * A call on a context runs on the context's device and gives the calling
+ * thread's current device back before it returns.
+ *
+ * Devices: the library carries sm_100a (B200) code only; msg_ctx_create
+ * returns MSG_EUNSUPPORTED on any other architecture.
  */
 #ifndef MSG_B200_H
 #define MSG_B200_H

@@ -23,10 +23,13 @@ extern "C" int msg_ctx_create(int device, msg_ctx** out) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return MSG_ECUDA;
     if (device < 0 || device >= n) return MSG_EINVAL;
-    if (cudaSetDevice(device) != cudaSuccess) return MSG_ECUDA;
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return MSG_ECUDA;
-    if (prop.major < 10) return MSG_EUNSUPPORTED;  // built for sm_100a only
+    // the library carries sm_100a code only (no PTX): other architectures,
+    // sm_103 and sm_120 included, could not launch its kernels
+    if (prop.major != 10 || prop.minor != 0) return MSG_EUNSUPPORTED;
+    msg::DeviceGuard dg_(device);
+    if (!dg_.ok) return MSG_ECUDA;
     msg_ctx* c = new (std::nothrow) msg_ctx();
     if (!c) return MSG_ENOMEM;
     c->device = device;
@@ -39,7 +42,7 @@ extern "C" int msg_ctx_create(int device, msg_ctx** out) {
 
 extern "C" void msg_ctx_destroy(msg_ctx* c) {
     if (!c) return;
-    cudaSetDevice(c->device);
+    msg::DeviceGuard dg_(c->device);
     cudaStreamSynchronize(c->stream);
     c->index_free();
     c->buffers_free();

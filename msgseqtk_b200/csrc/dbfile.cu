@@ -35,6 +35,7 @@
 // (WaveletTreeRRR.cpp:58-76) walks to; rows decoded in order reach them with
 // one cursor per tree node, on several host threads.
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <fstream>
@@ -246,10 +247,17 @@ bool read_fmd(const char* path, int n_threads, msg_db& db) {
     std::vector<Plain> lv(height);
     Plain saidx;
     {
+        // height + 1 jobs on at most n_threads workers
         std::vector<char> ok(height + 1, 0);
+        std::atomic<uint64_t> next{0};
+        auto worker = [&]() {
+            for (uint64_t l; (l = next.fetch_add(1)) <= height;)
+                ok[l] = decode_rrr(raw[l], tab, l < height ? lv[l] : saidx);
+        };
+        const uint64_t nw = std::min<uint64_t>(height + 1, (uint64_t)std::max(1, n_threads));
         std::vector<std::thread> th;
-        for (uint64_t l = 0; l <= height; ++l)
-            th.emplace_back([&, l]() { ok[l] = decode_rrr(raw[l], tab, l < height ? lv[l] : saidx); });
+        for (uint64_t t = 1; t < nw; ++t) th.emplace_back(worker);
+        worker();
         for (auto& x : th) x.join();
         for (char x : ok) if (!x) return false;
         raw.clear();
@@ -258,7 +266,7 @@ bool read_fmd(const char* path, int n_threads, msg_db& db) {
     for (int b = 0; b < 16; ++b) db.base_count[b] = B[b];
     // BWT symbols: the walk of WaveletTreeRRR::access per row
     db.bwt.resize(n);
-    bool bad = false;
+    std::atomic<bool> bad{false};  // set by any decode thread (relaxed: only read after join)
     // Rows are decoded in order, so the position a row reaches in a node of
     // level l + 1 is that node's start plus the rows before it that took
     // the same path: one cursor per node replaces the per-row rank queries
@@ -276,7 +284,10 @@ bool read_fmd(const char* path, int n_threads, msg_db& db) {
             node_start[(l + 1) * nodes + 2 * q + 1] = s1 < occ.size() ? occ[s1] : n;
         }
     }
-    auto decode = [&](uint64_t lo, uint64_t hi) {
+    const int nt = std::max(1, n_threads);
+    std::vector<std::vector<uint64_t>> hist(nt, std::vector<uint64_t>(nodes, 0));  // decoded symbols per thread
+    auto decode = [&](int t, uint64_t lo, uint64_t hi) {
+        uint64_t* hs = hist[t].data();
         std::vector<uint64_t> cur(height * nodes, 0);  // next position of each node
         std::vector<uint64_t> cnt(height * nodes, 0);  // rows before lo in each node
         cnt[0] = lo;
@@ -284,7 +295,7 @@ bool read_fmd(const char* path, int n_threads, msg_db& db) {
             const Plain& p = lv[l];
             for (uint64_t q = 0; q < (1ull << l); ++q) {
                 const uint64_t st = node_start[l * nodes + q], c = cnt[l * nodes + q];
-                if (st + c > n) { bad = true; return; }
+                if (st + c > n) { bad.store(true, std::memory_order_relaxed); return; }
                 const uint64_t ones = c > 0 ? p.rank1(st + c - 1) - (st > 0 ? p.rank1(st - 1) : 0) : 0;
                 cnt[(l + 1) * nodes + 2 * q + 1] = ones;
                 cnt[(l + 1) * nodes + 2 * q] = c - ones;
@@ -294,22 +305,32 @@ bool read_fmd(const char* path, int n_threads, msg_db& db) {
         for (uint64_t row = lo; row < hi; ++row) {
             uint64_t q = 0, i = row;
             for (uint64_t l = 0; l < height; ++l) {
-                if (i >= n) { bad = true; return; }
+                if (i >= n) { bad.store(true, std::memory_order_relaxed); return; }
                 q = 2 * q + (lv[l].bit(i) ? 1 : 0);
                 if (l + 1 < height) i = cur[(l + 1) * nodes + q]++;
             }
+            // a symbol without an entry in the occurrence table (at most
+            // max symbol + 2 entries, WaveletTreeRRR.h:238) is not one the
+            // index holds
+            if (q + 1 >= occ.size()) { bad.store(true, std::memory_order_relaxed); return; }
             db.bwt[row] = (uint8_t)q;
+            hs[q]++;
         }
     };
-    const int nt = std::max(1, n_threads);
     std::vector<std::thread> th;
     const uint64_t chunk = (n + nt - 1) / nt;
     for (int t = 0; t < nt; ++t) {
         const uint64_t lo = std::min<uint64_t>(n, t * chunk), hi = std::min<uint64_t>(n, lo + chunk);
-        th.emplace_back(decode, lo, hi);
+        th.emplace_back(decode, t, lo, hi);
     }
     for (auto& x : th) x.join();
-    if (bad) return false;
+    if (bad.load()) return false;
+    // the decoded symbols must be the ones the occurrence table counts
+    for (uint64_t q = 0; q + 1 < occ.size() && q < nodes; ++q) {
+        uint64_t c = 0;
+        for (int t = 0; t < nt; ++t) c += hist[t][q];
+        if (c != occ[q + 1] - occ[q]) return false;
+    }
     // FMDIndex::buildSA sizes SAsampled by SAidx.numOnes() (FMDIndex.cpp:495),
     // which can be one short of the marked rows; the last sample's value then
     // lies past the saved array (an index built in memory still holds it; one
@@ -343,7 +364,9 @@ bool read_fmd(const char* path, int n_threads, msg_db& db) {
         for (;;) {
             const uint64_t b = db.bwt[i];
             if (b == 0 || dist > (int64_t)n) return false;  // a '$' row is always sampled and stored
-            i = (uint64_t)C[b] + rank(b, i) - 1;            // LF(b, i) - 1 (FMDIndex.h:130-141)
+            const uint64_t rk = rank(b, i);
+            if (b >= 16 || rk == 0 || (uint64_t)C[b] + rk - 1 >= n) return false;  // inconsistent counts
+            i = (uint64_t)C[b] + rk - 1;                    // LF(b, i) - 1 (FMDIndex.h:130-141)
             ++dist;
             if (saidx.bit(i) && saidx.rank1(i) - 1 < sa_sampled.size()) break;
         }

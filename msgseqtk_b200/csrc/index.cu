@@ -165,6 +165,8 @@ extern "C" int msg_index_load(msg_ctx* ctx, const msg_fmd_view* fmd, const msg_m
     if (!ctx || !fmd || !mtg || !fmd->bwt || !fmd->base_count || !fmd->sample_rows || !fmd->sample_vals ||
         !mtg->bd_start || !mtg->bd_end || !mtg->chr_len || !mtg->chr_seq || !mtg->chr_off)
         return MSG_EINVAL;
+    msg::DeviceGuard dg_(ctx->device);
+    if (!dg_.ok) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
     const int64_t n = fmd->n;
     if (n <= 0 || fmd->n_samples <= 0 || mtg->n_chrom <= 0) return MSG_EINVAL;
     if (n >= (int64_t)0xFFFFFFFFll) return ctx->fail(MSG_EUNSUPPORTED, "BWT length must be below 2^32");
@@ -396,6 +398,8 @@ static int run_query(msg_ctx* ctx, int64_t count, size_t bytes_in, F&& body) {
     if (!ctx) return MSG_EINVAL;
     if (!ctx->idx.loaded) return MSG_ESTATE;
     if (count <= 0) return MSG_OK;
+    msg::DeviceGuard dg_(ctx->device);
+    if (!dg_.ok) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
     void* buf = nullptr;
     cudaError_t e = cudaMalloc(&buf, bytes_in);
     if (e != cudaSuccess) return ctx->cuda_fail(e);

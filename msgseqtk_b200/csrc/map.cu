@@ -804,6 +804,8 @@ extern "C" int msg_map_batch_device(msg_ctx* ctx, const msg_read_batch* reads, c
     if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
     if (reads->n_reads < 0 || (reads->n_reads > 0 && (!reads->seq || !reads->off))) return MSG_EINVAL;
     if (reads->n_reads > INT32_MAX) return MSG_EINVAL;
+    msg::DeviceGuard dg_(ctx->device);
+    if (!dg_.ok) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
     return map_impl(ctx, reads->seq, reads->off, reads->n_reads, params, out, dump);
 }
 
@@ -842,6 +844,8 @@ extern "C" int msg_map_batch(msg_ctx* ctx, const msg_read_batch* reads, const ms
                              msg_aln_out* out, msg_stage_dump* dump) {
     if (!ctx || !reads || !params || !out) return MSG_EINVAL;
     if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
+    msg::DeviceGuard dg_(ctx->device);
+    if (!dg_.ok) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
     const int rc = upload_reads(ctx, reads);
     if (rc != MSG_OK) return rc;
     return map_impl(ctx, ctx->reads.as<uint8_t>(), ctx->offs.as<int64_t>(), reads->n_reads, params, out, dump);
@@ -858,6 +862,8 @@ extern "C" int msg_map_batches(msg_ctx* ctx, int64_t n_batches, const msg_read_b
             if (r.off[i + 1] < r.off[i]) return MSG_EINVAL;
         if (!outs[k].aln || !outs[k].cigar) return ctx->fail(MSG_EINVAL, "null output buffer");
     }
+    msg::DeviceGuard dg_(ctx->device);
+    if (!dg_.ok) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
 #define CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { cudaStreamSynchronize(ctx->cstream); return ctx->cuda_fail(e_); } } while (0)
     if (!ctx->cstream) {
         if (cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking) != cudaSuccess)
@@ -990,6 +996,8 @@ int grad_smem_ready(msg_ctx* ctx) {
 extern "C" int msg_band_model_set(msg_ctx* ctx, const float* params, int64_t n_params) {
     if (!ctx || !params || n_params != kNParams) return MSG_EINVAL;
     if (!params_ok(params)) return ctx->fail(MSG_EINVAL, "non-finite parameter or non-positive feature scale");
+    msg::DeviceGuard dg_(ctx->device);
+    if (!dg_.ok) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
     const int rc = put_model(ctx, params, ctx->band_wts, ctx->band_nrm);
     if (rc == MSG_OK) ctx->band_loaded = true;
     return rc;
@@ -999,6 +1007,8 @@ extern "C" int msg_band_collect(msg_ctx* ctx, const msg_read_batch* reads, const
                                 int32_t* label, int64_t cap, int64_t* n_chain) {
     if (!ctx || !reads || !params || !n_chain || cap < 0 || (cap > 0 && (!feat || !label))) return MSG_EINVAL;
     if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
+    msg::DeviceGuard dg_(ctx->device);
+    if (!dg_.ok) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
     int rc = upload_reads(ctx, reads);
     if (rc != MSG_OK) return rc;
     BandCollect bc{feat, label, cap, n_chain};
@@ -1011,6 +1021,8 @@ extern "C" int msg_band_grad(msg_ctx* ctx, const float* params, const float* fea
     if (!ctx || !params || !feat || !label || n <= 0 || n > INT32_MAX || !grad || !loss) return MSG_EINVAL;
     if (!params_ok(params)) return ctx->fail(MSG_EINVAL, "non-finite parameter or non-positive feature scale");
     for (int64_t k = 0; k < n; ++k) if (label[k] < 0 || label[k] >= kCls) return MSG_EINVAL;
+    msg::DeviceGuard dg_(ctx->device);
+    if (!dg_.ok) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
     int rc = grad_smem_ready(ctx);
     if (rc != MSG_OK) return rc;
     msg::DevBuf& wts = ctx->tr_ord;  // bf16 weights of this call
@@ -1041,6 +1053,8 @@ extern "C" int msg_band_train(msg_ctx* ctx, const float* feat, const int32_t* la
     if (!ctx || !feat || !label || !tp || !params || n <= 0 || n > INT32_MAX) return MSG_EINVAL;
     if (tp->epochs <= 0 || tp->batch <= 0 || !(tp->lr > 0)) return MSG_EINVAL;
     for (int64_t k = 0; k < n; ++k) if (label[k] < 0 || label[k] >= kCls) return MSG_EINVAL;
+    msg::DeviceGuard dg_(ctx->device);
+    if (!dg_.ok) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
     // feature mean and scale from the data
     for (int i = 0; i < kFeat; ++i) {
         double m = 0, v = 0;
@@ -1184,8 +1198,9 @@ extern "C" int msg_smem_batch_noalloc(msg_ctx* ctx, int64_t n_reads, const uint8
     rc = evalue_threshold(ctx->idx.dev.n, params->max_evalue, &thr, &thr_all);
     if (rc != MSG_OK) return ctx->fail(rc, "e-value threshold");
     if (ctx->device < 0 || ctx->device >= 256) return MSG_EINVAL;
-    cudaError_t e = cudaSetDevice(ctx->device);
-    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    msg::DeviceGuard dg_(ctx->device);
+    if (!dg_.ok) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
+    cudaError_t e = cudaSuccess;
     if (!g_noalloc_addr[ctx->device]) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);

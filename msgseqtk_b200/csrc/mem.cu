@@ -456,7 +456,8 @@ extern "C" int msg_mem_batch(msg_ctx* ctx, const msg_read_batch* reads, const ms
     if (rows && (!n_rows || row_cap < 0)) return MSG_EINVAL;
     const int64_t n = reads->n_reads;
     if (n < 0 || n > INT32_MAX) return ctx->fail(MSG_EINVAL, "bad read count");
-    if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
+    msg::DeviceGuard dg_(ctx->device);
+    if (!dg_.ok) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
     const msg_read_batch* sets[1] = {reads};
     Set dev[1];
     int rc = upload_sets(ctx, sets, 1, dev);
@@ -524,7 +525,8 @@ extern "C" int msg_clean_batch(msg_ctx* ref, msg_ctx* bg, const msg_read_batch* 
     int rc = clean_check(ref, bg, fwd, params);
     if (rc != MSG_OK) return rc;
     if (rev && rev->n_reads != fwd->n_reads) return ref->fail(MSG_EINVAL, "mate batches differ in size");
-    if (cudaSetDevice(ref->device) != cudaSuccess) return ref->fail(MSG_ECUDA, "cudaSetDevice");
+    msg::DeviceGuard dg_(ref->device);
+    if (!dg_.ok) return ref->fail(MSG_ECUDA, "cudaSetDevice");
     const msg_read_batch* sets[2] = {fwd, rev};
     Set dev[2];
     const int n_set = rev ? 2 : 1;
@@ -541,7 +543,8 @@ extern "C" int msg_clean_batch_device(msg_ctx* ref, msg_ctx* bg, const msg_read_
     if (dev_rev && dev_rev->n_reads != dev_fwd->n_reads) return ref->fail(MSG_EINVAL, "mate batches differ in size");
     if (dev_fwd->n_reads > 0 && (!dev_fwd->seq || !dev_fwd->off)) return MSG_EINVAL;
     if (dev_rev && dev_rev->n_reads > 0 && (!dev_rev->seq || !dev_rev->off)) return MSG_EINVAL;
-    if (cudaSetDevice(ref->device) != cudaSuccess) return ref->fail(MSG_ECUDA, "cudaSetDevice");
+    msg::DeviceGuard dg_(ref->device);
+    if (!dg_.ok) return ref->fail(MSG_ECUDA, "cudaSetDevice");
     Set dev[2] = {{dev_fwd->seq, dev_fwd->off}, {dev_rev ? dev_rev->seq : nullptr, dev_rev ? dev_rev->off : nullptr}};
     return clean_impl(ref, bg, dev, dev_rev ? 2 : 1, dev_fwd->n_reads, params, min_lod, ref_loglik, bg_loglik, lod,
                       keep);

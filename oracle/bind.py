@@ -18,7 +18,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "build", "libmsgoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmsgref.so")
-REF_SRC = "/root/reference/src"
+# the reference's source tree (read-only); MSG_REFERENCE_SRC overrides it
+REF_SRC = os.environ.get("MSG_REFERENCE_SRC", "/root/reference/src")
 
 i64p = C.POINTER(C.c_int64)
 u8p = C.POINTER(C.c_uint8)
@@ -37,7 +38,7 @@ def build_reference() -> str | None:
     """Compile the reference when its sources are present (this build
     container); elsewhere the prebuilt library is used if it exists."""
     if os.path.isdir(REF_SRC):
-        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "ref")], check=True)
+        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "ref"), f"REF={REF_SRC}"], check=True)
     return REF_SO if os.path.exists(REF_SO) else None
 
 

@@ -22,14 +22,17 @@ def _write(tmp_path, genomes):
 
 
 @needs_ref
-@pytest.mark.parametrize("kind", ["small", "repeats"])
-def test_db_files_decode_to_reference_index(tmp_path, kind):
+@pytest.mark.parametrize("kind,n_threads", [("small", 4), ("repeats", 4), ("small", 1), ("repeats", 3),
+                                            ("small", 7)])
+def test_db_files_decode_to_reference_index(tmp_path, kind, n_threads):
+    """Odd thread counts put the decode's chunk boundaries at uneven node
+    splits; one thread decodes from row 0 with no boundary set-up."""
     if kind == "small":
         g = synth.small_genomes(seed=3, n_genomes=3, length=40_000)
     else:
         g = synth.repeat_genomes(seed=4, n_genomes=3, length=30_000)
     ref, paths = _write(tmp_path, g)
-    db = lib.Database(*paths, n_threads=4)
+    db = lib.Database(*paths, n_threads=n_threads)
     a = db.arrays()
     assert np.array_equal(a["bwt"], ref.bwt())
     B, _ = ref.counts()
@@ -56,6 +59,38 @@ def test_db_read_rejects_bad_files(tmp_path):
     assert e.value.code == lib.MSG_EINVAL
     with pytest.raises(lib.MsgError):
         lib.Database(paths[0], paths[1], tmp_path / "missing.fmd")
+
+
+# .fmd layout up to the wavelet tree's occurrence table: program header
+# (8-byte name, three int32 version fields), B[256] and C[256] as int64, then
+# the tree's n, sigma, height, wid, min, max, sample_rate and the table size
+# (FMDIndex::save, WaveletTreeRRR::save).
+_OCC_AT = 20 + 2 * 256 * 8 + 8 * 8
+
+
+@needs_ref
+@pytest.mark.parametrize("entry,delta", [(8, 1000_000), (8, -1), (4, 3), (2, -2)])
+def test_db_read_rejects_inconsistent_occurrence_table(tmp_path, entry, delta):
+    """A corrupted occurrence-table entry of the BWT's wavelet tree moves a
+    node's rows: the decode then leaves the node, reaches a symbol without an
+    entry in the table, or the suffix-array walk meets counts that do not
+    fit -- the file is rejected, never read out of bounds."""
+    g = synth.small_genomes(seed=5, n_genomes=2, length=6_000)
+    _, paths = _write(tmp_path, g)
+    data = bytearray(open(paths[2], "rb").read())
+    nocc = int(np.frombuffer(bytes(data[_OCC_AT - 8:_OCC_AT]), np.uint64)[0])
+    occ = np.frombuffer(bytes(data[_OCC_AT:_OCC_AT + 8 * nocc]), np.uint64).copy()
+    # the tree is built over nt16 codes 0..15 (FMDIndex.cpp:47): 17 entries,
+    # cumulative, the last one the BWT's length
+    assert nocc == 17 and occ[-1] == 2 * 2 * (6_000 + 1)
+    occ[entry] = np.uint64(int(occ[entry]) + delta)
+    data[_OCC_AT:_OCC_AT + 8 * nocc] = occ.tobytes()
+    bad = tmp_path / "bad.fmd"
+    open(bad, "wb").write(bytes(data))
+    for n_threads in (1, 3):
+        with pytest.raises(lib.MsgError) as e:
+            lib.Database(paths[0], paths[1], bad, n_threads=n_threads)
+        assert e.value.code == lib.MSG_EINVAL
 
 
 @pytest.mark.gpu
