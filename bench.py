@@ -715,13 +715,30 @@ def main():
     # DRAM bytes per extension measured by ncu on the 60-genome workload shape
     # (2.641 GB read + written for 44.86 M extensions), scaled to this launch
     traffic = SMEM_DRAM_BYTES_PER_EXT * agg["n_ext"] / args.steps
-    roofline = {"kernel": "k_smem (SMEM bi-interval extension)", "bound": "hbm", "achieved": achieved, "peak": hbm,
-                "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_smem_thread launch on "
-                                  "the 60-genome shape, per extension, times this launch's extensions",
-                "peak_source": peak_note,
-                "alg_bytes_per_launch": smem_bytes / args.steps, "dominant_stage": dom,
-                "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()}}
+    smem_roof = {"kernel": "k_smem_thread (SMEM bi-interval extension)", "bound": "hbm", "achieved": achieved,
+                 "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_smem_thread launch "
+                                   "on the 60-genome shape, per extension, times this launch's extensions",
+                 "peak_source": peak_note, "alg_bytes_per_launch": smem_bytes / args.steps}
+    # DP: integer-pipe bound; 11 algorithmic integer ops per reference cell
+    # (NW: M 3 adds + 2 max, I 2 adds + 1 max, D 2 adds + 1 max) over the DP
+    # stage's time, against the INT32 issue rate of the GPU: SMs x 128 lanes
+    # x the SM clock sampled under load (no measured integer peak exists)
+    props = torch.cuda.get_device_properties(local)
+    sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
+    int_peak = props.multi_processor_count * 128 * sm_mhz * 1e6 / 1e12
+    dp_ops = 11.0 * agg["dp_cells"]
+    dp_achieved = dp_ops / (agg["dp"] / 1000.0) / 1e12 if agg["dp"] > 0 else 0.0
+    dp_roof = {"kernel": "k_dp_stripe (seed-guided affine DP, register stripes)", "bound": "int32 pipe",
+               "achieved": dp_achieved, "peak": int_peak, "unit": "Tops/s", "frac": dp_achieved / int_peak,
+               "traffic": None,
+               "peak_source": "derived: %d SMs x 128 INT32 lanes x %.0f MHz (median SM clock under load)"
+                              % (props.multi_processor_count, sm_mhz),
+               "ops_per_cell": 11, "reference_cells_per_step": agg["dp_cells"] / args.steps,
+               "cells_evaluated_per_step": agg["dp_cells_done"] / args.steps}
+    roofline = dict(dp_roof if dom == "dp" else smem_roof)
+    roofline.update({"dominant_stage": dom, "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
+                     "stages": {"smem": smem_roof, "dp": dp_roof}})
 
     # validation: a sample of the timed reads through the oracle
     valid = None
@@ -767,7 +784,9 @@ def main():
                 "vs_baseline": None, "dtype": "int32", "data": "synthetic",
                 "config": {"workload": WORKLOADS[args.workload],
                            "reads_per_step": bp, "pairs_per_gpu": args.pairs, "bd_symbols": view.n,
-                           "l2": ("inputs larger than L2 (index %.1f GB, new reads every step)" % setup["index_gb"]
+                           "l2": ("inputs larger than L2 (index %.1f GB; %d batches of %.0f MB of reads cycled, "
+                                  "each larger than L2)" % (setup["index_gb"], n_batches,
+                                                            reads.offs[-1] / n_batches / 1e6)
                                   if n_batches > 1 else "inputs larger than L2 (index %.1f GB, %.0f MB of reads "
                                   "per step)" % (setup["index_gb"], reads.offs[-1] / 1e6)),
                            "parallelism": f"dp{world}" if world > 1 else "single GPU"},

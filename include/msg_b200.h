@@ -245,6 +245,14 @@ int msg_ctx_stream(const msg_ctx* ctx, void** stream);
  * not depend on the limit. */
 int msg_ctx_set_scratch_limit(msg_ctx* ctx, int64_t bytes);
 
+/* Work split of the DP stage. No reference counterpart (the reference fills
+ * every chain's matrices on one CPU thread). Unbanded chains of at most
+ * small_area rectangle cells are filled row by row by one GPU thread; chains
+ * of at most warp_area cells by one thread in register stripes of
+ * stripe_rows rows (8, 16 or 32); larger chains by a warp along
+ * anti-diagonals. Defaults 256, 65536, 16. Results do not depend on it. */
+int msg_ctx_set_dp_shape(msg_ctx* ctx, int32_t stripe_rows, int64_t small_area, int64_t warp_area);
+
 /* ---- Seeding that allocates nothing ----
  * No counterpart in the reference: it exists for callers that cannot call
  * cudaMalloc/cudaFree while mapping -- a host application whose GPU memory is

@@ -152,34 +152,42 @@ __host__ __device__ inline bool bandable(int R, int C, int w) {
     return R > 0 && C > 0 && w < max(R, C) - 1 && 2 * (2 * w + 1) < C;
 }
 
-// List counters: counts[0] thread path, counts[1] warp path (whole cell
-// set), counts[kBandedCount] warp path with a band.
-constexpr int kBandedCount = 8;
-// With small_key, the thread-path list is built by sorting every chain on
-// this key (small chains: their cell count; others last), so that the
-// threads of a warp get chains of similar size and diverge less.
-constexpr int32_t kNotSmallKey = 1023;
-constexpr int kSmallKeyBits = 10;
+// DP classes of a chain. The chains of a range are sorted by (class, area
+// descending); each class runs as one launch over its part of the sorted list,
+// largest chains first, so that the threads of a warp get chains of similar
+// size and the launch ends on small ones.
+enum DpClass : int {
+    kDpSmall = 0,       // unbanded, area <= small_area: k_dp_small (thread, row by row)
+    kDpStripe = 1,      // unbanded, up to warp_area: k_dp_stripe (thread, register stripes)
+    kDpStripeBand = 2,  // banded, up to warp_area: k_dp_stripe with bands
+    kDpWarp = 3,        // unbanded, larger: k_dp (warp wavefront)
+    kDpWarpBand = 4,    // banded, larger: k_dp with bands
+    kDpClasses = 5
+};
+// Counter block of the DP stage (unsigned long long words): class sizes
+// [0, kDpClasses), the fallback lists of the stripe and warp kernels, the
+// traceback list, then the statistics (fallback, exact, dropped, warp cells,
+// thread cells).
+constexpr int kCtrFbStripe = 5, kCtrFbWarp = 6, kCtrTrace = 7, kCtrStat = 8, kCtrWords = 16;
+constexpr int kKeyAreaBits = 21;
+constexpr int kKeyBits = kKeyAreaBits + 3;
 
 __global__ void k_iota(int64_t c0, int64_t n, int64_t* __restrict__ v) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i < n) v[i] = c0 + i;
 }
 
-// Band half-widths per chain and the split into the thread path (chains of
-// at most kSmallArea cells, never banded), the warp path and the banded warp
-// path.
-// mode 0: no band; 1: fixed_w for every larger chain; 2: the classifier's
-// choice for larger chains with a flank that a band of half-width 7 would cut.
-// Each flank is banded only when bandable().
+// Band half-widths per chain, its DP class and sort key.
+// mode 0: no band; 1: fixed_w for every chain above kSmallArea; 2: the
+// classifier's choice for chains above kSmallArea with a flank that a band of
+// half-width 7 would cut. Each flank is banded only when bandable().
 __global__ void __launch_bounds__(128) k_band_assign(int64_t c0, int64_t n_chain, const int4* __restrict__ geo,
                                                      const int64_t* __restrict__ area, const float* __restrict__ feat,
                                                      int mode, int fixed_w, const __nv_bfloat16* __restrict__ wts,
-                                                     const float* __restrict__ nrm, int8_t* __restrict__ band,
-                                                     int64_t* __restrict__ small, int64_t* __restrict__ big,
-                                                     int64_t* __restrict__ banded,
+                                                     const float* __restrict__ nrm, int64_t small_area,
+                                                     int64_t warp_area, int8_t* __restrict__ band,
                                                      unsigned long long* __restrict__ counts,
-                                                     int32_t* __restrict__ small_key) {
+                                                     uint32_t* __restrict__ key) {
     __shared__ float sW[kNTrain];
     __shared__ float sN[2 * kFeat];
     if (mode == 2) {
@@ -188,26 +196,33 @@ __global__ void __launch_bounds__(128) k_band_assign(int64_t c0, int64_t n_chain
         __syncthreads();
     }
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // chains c0 .. c0 + n_chain
-    if (t >= n_chain) return;
-    const int64_t c = c0 + t;
-    const int4 g = geo[c];
-    int w = -1;
-    if (area[c] > kSmallArea) {  // small chains stay on the thread path, whole rectangles
-        if (mode == 1) w = fixed_w;
-        else if (mode == 2 && (bandable(g.x, g.y, band_width(0)) || bandable(g.z, g.w, band_width(0))))
-            w = band_width(mlp_class(feat + c * kFeat, sW, sN));
+    int cls = -1;
+    if (t < n_chain) {
+        const int64_t c = c0 + t;
+        const int4 g = geo[c];
+        const int64_t ar = area[c];
+        int w = -1;
+        if (ar > kSmallArea) {  // small chains are never banded
+            if (mode == 1) w = fixed_w;
+            else if (mode == 2 && (bandable(g.x, g.y, band_width(0)) || bandable(g.z, g.w, band_width(0))))
+                w = band_width(mlp_class(feat + c * kFeat, sW, sN));
+        }
+        const int w5 = (w >= 0 && bandable(g.x, g.y, w)) ? w : -1;
+        const int w3 = (w >= 0 && bandable(g.z, g.w, w)) ? w : -1;
+        band[2 * c] = (int8_t)w5;
+        band[2 * c + 1] = (int8_t)w3;
+        const bool huge = ar > warp_area;
+        if (w5 >= 0 || w3 >= 0) cls = huge ? kDpWarpBand : kDpStripeBand;
+        else if (ar <= small_area) cls = kDpSmall;
+        else cls = huge ? kDpWarp : kDpStripe;
+        const uint32_t amax = (1u << kKeyAreaBits) - 1u;
+        key[t] = ((uint32_t)cls << kKeyAreaBits) | (amax - (uint32_t)min(ar, (int64_t)amax));
     }
-    const int w5 = (w >= 0 && bandable(g.x, g.y, w)) ? w : -1;
-    const int w3 = (w >= 0 && bandable(g.z, g.w, w)) ? w : -1;
-    band[2 * c] = (int8_t)w5;
-    band[2 * c + 1] = (int8_t)w3;
-    const bool is_small = w5 < 0 && w3 < 0 && area[c] <= kSmallArea;
-    if (small_key) small_key[t] = is_small ? (int32_t)area[c] : kNotSmallKey;
-    if (w5 >= 0 || w3 >= 0) banded[atomicAdd(&counts[kBandedCount], 1ull)] = c;
-    else if (is_small) {
-        const unsigned long long k = atomicAdd(&counts[0], 1ull);
-        if (!small_key) small[k] = c;
-    } else big[atomicAdd(&counts[1], 1ull)] = c;
+#pragma unroll
+    for (int q = 0; q < kDpClasses; ++q) {  // one atomic per warp and class
+        const unsigned b = __ballot_sync(0xffffffffu, cls == q);
+        if ((threadIdx.x & 31) == 0 && b) atomicAdd(&counts[q], (unsigned long long)__popc(b));
+    }
 }
 
 // ---------------------------------------------------------------------------

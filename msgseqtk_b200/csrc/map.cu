@@ -170,6 +170,59 @@ struct Timer {
     }
 };
 
+// Band assignment, DP class and sort key of chains c0 .. c0 + n, then the
+// chains sorted by (class, area descending) into `sorted`; class sizes are
+// added to counts[0 .. kDpClasses). keybuf holds 2n uint32 (keys in, out).
+cudaError_t dp_sort(msg_ctx* ctx, int64_t c0, int64_t n, const int4* geo, const int64_t* area, const float* feat,
+                    int mode, int fixed_w, const __nv_bfloat16* wts, const float* nrm, int8_t* band,
+                    unsigned long long* counts, int64_t* keybuf, int64_t* ids, int64_t* sorted, msg_map_stats& S) {
+    cudaStream_t st = ctx->stream;
+    uint32_t* key = reinterpret_cast<uint32_t*>(keybuf);
+    uint32_t* key2 = key + n;
+    S.n_launch++, k_band_assign<<<nblk(n, 128), 128, 0, st>>>(c0, n, geo, area, feat, mode, fixed_w, wts, nrm,
+                                                              ctx->dp_small_area, ctx->dp_warp_area, band, counts,
+                                                              key);
+    S.n_launch++, k_iota<<<nblk(n, 256), 256, 0, st>>>(c0, n, ids);
+    cudaError_t e = cudaGetLastError();
+    size_t tb = 0;
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(nullptr, tb, key, key2, ids, sorted, (int)n, 0, kKeyBits, st);
+    if (e == cudaSuccess) e = ctx->misc.ensure(tb);
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(ctx->misc.p, tb, key, key2, ids, sorted, (int)n, 0, kKeyBits, st);
+    return e;
+}
+
+template <int K>
+void launch_stripe(msg_ctx* ctx, const DpArgs& a, bool band, int64_t n_max) {
+    const int g = (int)std::min<int64_t>(nblk(n_max, kStripeThreads), (int64_t)ctx->num_sms * 16);
+    if (band) k_dp_stripe<K, true><<<g, kStripeThreads, 0, ctx->stream>>>(a);
+    else k_dp_stripe<K, false><<<g, kStripeThreads, 0, ctx->stream>>>(a);
+}
+
+// One DP launch: over class `cls` of the class-sorted list a.list when
+// cls >= 0; with cls < 0 over a.list[0 .. *a.n_list) with the kernel of class
+// -cls - 1 (the fallback recomputations). n_max bounds the chains it may get;
+// the kernels loop over their chains (grid-stride).
+void launch_dp(msg_ctx* ctx, DpArgs a, int cls, int64_t n_max, msg_map_stats& S) {
+    const int kind = cls >= 0 ? cls : -cls - 1;
+    a.cls = cls >= 0 ? cls : -1;
+    cudaStream_t st = ctx->stream;
+    S.n_launch++;
+    if (kind == kDpSmall) {
+        const int g = (int)std::min<int64_t>(nblk(n_max, 128), (int64_t)ctx->num_sms * 16);
+        k_dp_small<<<g, 128, 0, st>>>(a);
+    } else if (kind == kDpStripe || kind == kDpStripeBand) {
+        const bool band = kind == kDpStripeBand;
+        if (ctx->dp_k == 8) launch_stripe<8>(ctx, a, band, n_max);
+        else if (ctx->dp_k == 32) launch_stripe<32>(ctx, a, band, n_max);
+        else launch_stripe<16>(ctx, a, band, n_max);
+    } else {
+        const int g = (int)std::min<int64_t>(nblk(n_max * 32, kDpWarps * 32), (int64_t)ctx->num_sms * 12);
+        if (kind == kDpWarpBand) k_dp<true><<<g, kDpWarps * 32, 0, st>>>(a);
+        else k_dp<false><<<g, kDpWarps * 32, 0, st>>>(a);
+    }
+}
+
 int check_params(const msg_map_params* p, DpParams* dp) {
     if (!p) return MSG_EINVAL;
     if (p->min_len < 1 || p->max_nseed < 1 || (p->mode != 0 && p->mode != 1)) return MSG_EINVAL;
@@ -515,17 +568,15 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     int64_t* d_dpcells = d_path_off + NC;
     int64_t* d_ncig = d_dpcells + NC;
     int64_t* d_area = d_ncig + NC;
-    int64_t* d_small = d_area + NC;
-    int64_t* d_big = d_small + NC;
-    int64_t* d_fb = d_big + NC;
+    int64_t* d_sorted = d_area + NC;    // chains of the range sorted by DP class and area
+    int64_t* d_fbw = d_sorted + NC;     // warp-path chains whose banded result was not certified
+    int64_t* d_fb = d_fbw + NC;         // stripe-path chains whose banded result was not certified (keys first)
     int64_t* d_kidx = d_fb + NC;        // kept-record index per chain (n + 1)
     int64_t* d_map = d_kidx + NC;       // chain of each kept record
-    int64_t* d_bandl = d_map + NC;      // chains with a banded flank
-    int64_t* d_tbl = d_bandl + NC;      // chains traced back by k_traceback
-    // counters: 0 thread list, 1 warp list, 2 fallback list, 3..7 band stats,
-    // kBandedCount banded list, kBandedCount + 1 traceback list
+    int64_t* d_tbl = d_map + 2 * NC;    // chains traced back by k_traceback
+    // counters: class sizes, fallback lists, traceback list, band statistics (kCtr*)
     unsigned long long* d_ctr2 = reinterpret_cast<unsigned long long*>(d_tbl + NC);
-    unsigned long long* d_bstat = d_ctr2 + 3;
+    unsigned long long* d_bstat = d_ctr2 + kCtrStat;
     CK(ctx->geobuf.ensure(NC * sizeof(int4) + NC * kFeat * sizeof(float) + 64));
     int4* d_geo = ctx->geobuf.as<int4>();
     float* d_feat = reinterpret_cast<float*>(d_geo + NC);
@@ -596,7 +647,8 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     da.pp = dpp; da.status = d_status;
     da.band = d_band; da.min_rate = params->min_score_rate; da.keep = d_keep; da.fb_list = d_fb;
     da.fb_n = d_ctr2 + 2; da.bstat = d_bstat;
-    da.tb_list = d_tbl; da.tb_n = d_ctr2 + kBandedCount + 1;
+    da.tb_list = d_tbl; da.tb_n = d_ctr2 + kCtrTrace;
+    da.cls_n = d_ctr2; da.cls = -1;
     const __nv_bfloat16* d_wts = ctx->band_wts.as<__nv_bfloat16>();
     const float* d_nrm = ctx->band_nrm.as<float>();
 
@@ -617,14 +669,14 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         for (int64_t c = 0; c < h_nchain; ++c) best[c] = area[c];
         da.probe = d_probe; da.probe_cells = d_pcells;
         for (int cls = kCls - 2; cls >= 0; --cls) {  // wider classes first: ties keep the wider one
-            CK(cudaMemsetAsync(d_ctr2, 0, 128, st));
+            CK(cudaMemsetAsync(d_ctr2, 0, kCtrWords * 8, st));
             CK(cudaMemsetAsync(d_probe, 3, h_nchain, st));  // 3: not banded at this class
             CK(cudaMemcpyAsync(d_pcells, d_area, h_nchain * 8, cudaMemcpyDeviceToDevice, st));
-            S.n_launch++, k_band_assign<<<nblk(h_nchain, 128), 128, 0, st>>>(0, h_nchain, d_geo, d_area, d_feat, 1, band_width(cls),
-                                                                nullptr, nullptr, d_band, d_small, d_big, d_bandl, d_ctr2,
-                                                                nullptr);
-            da.list = d_bandl; da.n_list = d_ctr2 + kBandedCount;
-            S.n_launch++, k_dp<true><<<nblk(h_nchain * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
+            CK(dp_sort(ctx, 0, h_nchain, d_geo, d_area, d_feat, 1, band_width(cls), nullptr, nullptr, d_band,
+                       d_ctr2, d_fb, d_kidx, d_sorted, S));
+            da.list = d_sorted;
+            launch_dp(ctx, da, kDpStripeBand, h_nchain, S);
+            launch_dp(ctx, da, kDpWarpBand, h_nchain, S);
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(pr.data(), d_probe, h_nchain, cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(pc.data(), d_pcells, h_nchain * 8, cudaMemcpyDeviceToHost, st));
@@ -646,52 +698,41 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     }
 
     const bool filtering = params->min_score_rate >= 0;
-    if (h_nchain > 0) CK(cudaMemsetAsync(d_ctr2, 0, 128, st));
+    if (h_nchain > 0) CK(cudaMemsetAsync(d_ctr2, 0, kCtrWords * 8, st));
     for (size_t ch = 0; ch + 1 < bounds.size(); ++ch) {
         const int64_t c0 = bounds[ch], nch = bounds[ch + 1] - bounds[ch];
         if (nch <= 0) continue;
-        if (ch > 0) {  // list counters start again; the band statistics accumulate
-            CK(cudaMemsetAsync(d_ctr2, 0, 3 * 8, st));
-            CK(cudaMemsetAsync(d_ctr2 + kBandedCount, 0, 2 * 8, st));
-        }
+        if (ch > 0) CK(cudaMemsetAsync(d_ctr2, 0, kCtrStat * 8, st));  // lists start again; statistics accumulate
         da.scr_base = h_rect_off[ch];
         da.band = d_band;
         const int bmode = dpp.mode != 0 ? 0 : params->band_mode;
-        // thread-path list sorted by cell count (keys and values staged in the
-        // fallback and kept-index arrays, which are not in use yet)
-        int32_t* d_key = reinterpret_cast<int32_t*>(d_fb);
-        int32_t* d_key2 = d_key + NC;
-        S.n_launch++, k_band_assign<<<nblk(nch, 128), 128, 0, st>>>(c0, nch, d_geo, d_area, d_feat, bmode,
-                                                                     params->band_w, d_wts, d_nrm, d_band, d_small,
-                                                                     d_big, d_bandl, d_ctr2, d_key);
-        S.n_launch++, k_iota<<<nblk(nch, 256), 256, 0, st>>>(c0, nch, d_kidx);
-        {
-            size_t tb = 0;
-            CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, d_key, d_key2, d_kidx, d_small, (int)nch, 0,
-                                               kSmallKeyBits, st));
-            CK(misc.ensure(tb));
-            CK(cub::DeviceRadixSort::SortPairs(misc.p, tb, d_key, d_key2, d_kidx, d_small, (int)nch, 0,
-                                               kSmallKeyBits, st));
-        }
-        // Every launch is sized for every chain of the range; each reads its
-        // list length on the device, so no host round trip is needed.
-        da.list = d_small; da.n_list = d_ctr2;
-        S.n_launch++, k_dp_small<<<nblk(nch, 128), 128, 0, st>>>(da);
-        da.list = d_big; da.n_list = d_ctr2 + 1;
-        S.n_launch++, k_dp<false><<<nblk(nch * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
+        CK(dp_sort(ctx, c0, nch, d_geo, d_area, d_feat, bmode, params->band_w, d_wts, d_nrm, d_band, d_ctr2, d_fb,
+                   d_kidx, d_sorted, S));
+        da.list = d_sorted;
+        // Every launch is sized for the range; each reads its class's part of
+        // the sorted list on the device, so no host round trip is needed.
+        da.fb_list = d_fb; da.fb_n = d_ctr2 + kCtrFbStripe;
+        launch_dp(ctx, da, kDpSmall, nch, S);
+        launch_dp(ctx, da, kDpStripe, nch, S);
+        launch_dp(ctx, da, kDpWarp, nch, S);
         if (bmode != 0) {
-            da.list = d_bandl; da.n_list = d_ctr2 + kBandedCount;
-            S.n_launch++, k_dp<true><<<nblk(nch * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
+            launch_dp(ctx, da, kDpStripeBand, nch, S);
+            da.fb_list = d_fbw; da.fb_n = d_ctr2 + kCtrFbWarp;
+            launch_dp(ctx, da, kDpWarpBand, nch, S);
             // banded chains without a certificate, on the whole cell set
-            da.list = d_fb; da.n_list = d_ctr2 + 2; da.band = nullptr;
-            S.n_launch++, k_dp<false><<<nblk(nch * 32, kDpWarps * 32), kDpWarps * 32, 0, st>>>(da);
+            DpArgs fb = da;
+            fb.band = nullptr;
+            fb.list = d_fb; fb.n_list = d_ctr2 + kCtrFbStripe;
+            launch_dp(ctx, fb, -kDpStripe - 1, nch, S);
+            fb.list = d_fbw; fb.n_list = d_ctr2 + kCtrFbWarp;
+            launch_dp(ctx, fb, -kDpWarp - 1, nch, S);
         }
         S.n_launch++, k_traceback<<<nblk(nch, 128), 128, 0, st>>>(da);
         CK(cudaGetLastError());
         if (bounds.size() > 2) {  // warp-path chains of this range, for the statistics
-            unsigned long long w[kBandedCount + 1];
+            unsigned long long w[kDpClasses];
             CK(cudaMemcpy(w, d_ctr2, sizeof(w), cudaMemcpyDeviceToHost));
-            S.n_dp_warp += (int64_t)(w[1] + w[kBandedCount]);
+            S.n_dp_warp += (int64_t)(w[kDpWarp] + w[kDpWarpBand]);
         }
     }
     tm.mark();  // 4
@@ -729,8 +770,8 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     }
     tm.mark();  // 5
     uint32_t h_status = 0;
-    unsigned long long h_ctr2[kBandedCount + 1] = {0};
-    const unsigned long long* h_bstat = h_ctr2 + 3;
+    unsigned long long h_ctr2[kCtrWords] = {0};
+    const unsigned long long* h_bstat = h_ctr2 + kCtrStat;
     CK(cudaMemcpyAsync(&h_status, d_status, 4, cudaMemcpyDeviceToHost, st));
     if (h_nchain > 0) CK(cudaMemcpyAsync(h_ctr2, d_ctr2, sizeof(h_ctr2), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -741,7 +782,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     S.n_band_drop = (int64_t)h_bstat[2];
     S.dp_cells_done = (int64_t)(h_bstat[3] + h_bstat[4]);
     S.n_filtered = h_nchain - h_nrec;
-    if (bounds.size() <= 2) S.n_dp_warp = (int64_t)(h_ctr2[1] + h_ctr2[kBandedCount]);
+    if (bounds.size() <= 2) S.n_dp_warp = (int64_t)(h_ctr2[kDpWarp] + h_ctr2[kDpWarpBand]);
     S.ms_smem = tm.ms(0, 1);
     S.ms_locate = tm.ms(1, 2);
     S.ms_chain = tm.ms(2, 3);
@@ -1138,6 +1179,15 @@ extern "C" int msg_result_device(const msg_ctx* ctx, const msg_aln** aln, const 
 extern "C" int msg_ctx_set_scratch_limit(msg_ctx* ctx, int64_t bytes) {
     if (!ctx || bytes <= 0) return MSG_EINVAL;
     ctx->scratch_limit = bytes;
+    return MSG_OK;
+}
+
+extern "C" int msg_ctx_set_dp_shape(msg_ctx* ctx, int32_t stripe_rows, int64_t small_area, int64_t warp_area) {
+    if (!ctx || (stripe_rows != 8 && stripe_rows != 16 && stripe_rows != 32) || small_area < 0 || warp_area < 0)
+        return MSG_EINVAL;
+    ctx->dp_k = stripe_rows;
+    ctx->dp_small_area = small_area;
+    ctx->dp_warp_area = warp_area;
     return MSG_OK;
 }
 

@@ -575,6 +575,7 @@ struct DpParams {
 };
 
 constexpr int kDpWarps = 4;       // warps per block in k_dp
+constexpr int kStripeThreads = 128;  // threads per block in k_dp_stripe (the stride of its score tables)
 constexpr int kSmemSeeds = 64;    // chain seeds cached in shared memory per warp (else global)
 
 __device__ __forceinline__ int match_max(int32_t m, int32_t i, int32_t d) {  // Alignment.h:577-589
@@ -585,10 +586,19 @@ __device__ __forceinline__ int match_max(int32_t m, int32_t i, int32_t d) {  // 
     return s;
 }
 
+// Storage of one rectangle (16-byte aligned, a multiple of 16 bytes):
+// traceback codes, then a row buffer of C + 1 entries of 16 bytes (the
+// bottom row of the previous stripe: M, I, D; the warp and row fills use
+// the first 12 bytes per column of it as 3 int32 per column), then M, I, D
+// of the last row and of the last column. Code layouts: the warp and row
+// fills keep stripes of 32 rows skewed along anti-diagonals (code of row rr,
+// column cc at ((rr / 32) * (C + 31) + cc + rr % 32) * 32 + rr % 32); the
+// register-stripe fill keeps stripes of K rows column by column (code at
+// ((rr / K) * C + cc) * K + rr % K), which fits in the same space for K <= 32.
 struct RectGeo {
     int64_t r0, c0, R, C;
-    uint8_t* code;    // stripes x (C + 31) x 32 codes
-    int32_t* rowbuf;  // (C + 1) x 3: bottom row of the previous stripe
+    uint8_t* code;
+    int32_t* rowbuf;  // (C + 1) x 4
     int32_t* lastrow; // C x 3
     int32_t* lastcol; // R x 3
 };
@@ -597,7 +607,7 @@ __device__ __forceinline__ int64_t rect_bytes(int64_t R, int64_t C) {
     if (R <= 0 || C <= 0) return 0;
     const int64_t stripes = (R + 31) / 32;
     const int64_t code = ((stripes * (C + 31) * 32) + 15) / 16 * 16;
-    return code + ((C + 1) * 3 + C * 3 + R * 3) * 4 + 16;
+    return (code + ((C + 1) * 4 + C * 3 + R * 3) * 4 + 16 + 15) / 16 * 16;
 }
 
 struct ChainCtx {
@@ -615,6 +625,8 @@ struct ChainCtx {
     int32_t* roff;              // per rectangle index (0..n): byte offset in scratch
     DpParams pp;
     uint32_t* status;
+    int kst = 0;                // rows per stripe of the code layout (0: the 32-row skewed layout)
+    uint32_t* stab = nullptr;   // register-stripe fill: this thread's score table, 16 words at stride kStripeThreads
 
     __device__ int64_t qf(int k) const { return sd[k].x; }
     __device__ int64_t qt(int k) const { return sd[k].y; }
@@ -650,12 +662,13 @@ struct ChainCtx {
         g.code = base;
         int32_t* ints = reinterpret_cast<int32_t*>(base + ((stripes * (g.C + 31) * 32) + 15) / 16 * 16);
         g.rowbuf = ints;
-        g.lastrow = ints + (g.C + 1) * 3;
+        g.lastrow = ints + (g.C + 1) * 4;
         g.lastcol = g.lastrow + g.C * 3;
         return g;
     }
     __device__ uint8_t code_at(const RectGeo& g, int64_t i, int64_t j) const {
         const int64_t rr = i - g.r0 - 1, cc = j - g.c0 - 1;
+        if (kst) return g.code[((rr / kst) * g.C + cc) * kst + rr % kst];
         const int64_t stripe = rr >> 5, lane = rr & 31;
         return g.code[(stripe * (g.C + 31) + cc + lane) * 32 + lane];
     }
@@ -798,6 +811,155 @@ struct ChainCtx {
             }
             cells += hi - lo + 1;
             plo = lo; phi = hi;
+        }
+        return cells;
+    }
+
+    // Register-stripe fill of rectangle m by one thread (Alignment::
+    // calculateScoresNW/SW, Alignment.cpp:72-133, cell for cell as
+    // fill_rect_thread): stripes of K rows, column by column. The previous
+    // column's M, I, D of the stripe's rows stay in registers; the row above
+    // the stripe comes from the row buffer (one 16-byte load per column) and
+    // the stripe's bottom row goes back to it; a column's K traceback codes
+    // leave in one store. Cell updates use Blackwell's integer DP
+    // instructions: __vimax3_s32 for M's three-way maximum and
+    // __viaddmax_s32 for the saturating gap terms max(x + g, -inf), which
+    // keep -inf absorbing. The score of a cell is one bit of a per-stripe
+    // table (bit k of stab[t * kStripeThreads]: row k's query base matches
+    // target code t). BANDED: only the cells within w diagonals of the
+    // adjacent seed's diagonal are computed, the others count as -inf
+    // (boundary cells next to band cells are read exactly), as
+    // fill_rect_thread does with w >= 0.
+    // Returns the number of cells evaluated (for a band: its stripes' columns
+    // times their rows).
+    template <int K, bool LOCAL, bool BANDED>
+    __device__ __noinline__ int64_t fill_rect_stripe(int m, int w, int32_t& best, int64_t& bkey) {
+        static_assert(K == 8 || K == 16 || K == 32, "stripe height");
+        const RectGeo g = rect(m);
+        if (g.R <= 0 || g.C <= 0) return 0;
+        const int R = (int)g.R, C = (int)g.C;
+        const int32_t o = -(pp.gap_o + pp.gap_e), e = -pp.gap_e;
+        const int32_t smt = pp.match, smm = -pp.mismatch;
+        int4* rb4 = reinterpret_cast<int4*>(g.rowbuf);
+        const int dg = m == 0 ? C - R : 0;  // column - row of the seed's diagonal in this rectangle
+        if (BANDED) {
+            for (int c = 0; c < 3 * C; ++c) g.lastrow[c] = NEG;
+            for (int c = 0; c < 3 * R; ++c) g.lastcol[c] = NEG;
+        }
+        int plo = 0, phi = C - 1;  // columns of the row buffer that hold the row above
+        if (BANDED) { plo = max(0, dg - w - 1); phi = min(C - 1, dg + w); }
+        for (int c = plo; c <= phi; ++c) {  // the top boundary row
+            const int3 v = MID(g.r0, g.c0 + 1 + c, m);
+            rb4[c] = make_int4(v.x, v.y, v.z, 0);
+        }
+        int64_t cells = 0;
+        const int nsp = (R + K - 1) / K;
+        for (int sp = 0; sp < nsp; ++sp) {
+            const int rr0 = sp * K;
+            const int nrow = min(K, R - rr0);
+            int clo = 0, chi = C - 1;
+            if (BANDED) { clo = max(0, rr0 + dg - w); chi = min(C - 1, rr0 + nrow - 1 + dg + w); }
+            if (clo > chi) { plo = 1; phi = 0; continue; }
+            const int64_t i0 = g.r0 + 1 + rr0;  // matrix row of the stripe's first row
+            {
+                uint32_t tbits[16];
+#pragma unroll
+                for (int t = 0; t < 16; ++t) tbits[t] = 0;
+                for (int k = 0; k < nrow; ++k) {
+                    const int q = qbase(i0 - 1 + k);
+                    if (q == 15) continue;  // N scores a mismatch against everything
+#pragma unroll
+                    for (int t = 1; t < 15; ++t) tbits[t] |= (q & t) ? (1u << k) : 0u;
+                }
+#pragma unroll
+                for (int t = 0; t < 16; ++t) stab[t * kStripeThreads] = tbits[t];
+            }
+            // the previous column's values of the stripe's rows: the left
+            // boundary (column c0) when the stripe starts at column 0
+            int32_t Mp[K], Ip[K], Dp[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                Mp[k] = NEG; Ip[k] = NEG; Dp[k] = NEG;
+                if (clo == 0 && k < nrow) {
+                    const int3 v = MID(i0 + k, g.c0, m);
+                    Mp[k] = v.x; Ip[k] = v.y; Dp[k] = v.z;
+                }
+            }
+            // diagonal neighbour of the stripe's first row at column clo
+            int32_t dM = NEG, dI = NEG, dD = NEG;
+            if (clo == 0) {
+                const int3 v = MID(i0 - 1, g.c0, m);
+                dM = v.x; dI = v.y; dD = v.z;
+            } else if (clo - 1 >= plo && clo - 1 <= phi) {
+                const int4 v = rb4[clo - 1];
+                dM = v.x; dI = v.y; dD = v.z;
+            }
+            uint8_t* code = g.code + (int64_t)sp * C * K;
+            const bool last = sp == nsp - 1;
+            for (int cc = clo; cc <= chi; ++cc) {
+                int4 up = make_int4(NEG, NEG, NEG, 0);
+                if (!BANDED || (cc >= plo && cc <= phi)) up = rb4[cc];
+                const uint32_t tm = stab[(tb(g.c0 + cc) & 15) * kStripeThreads];
+                const int64_t j = g.c0 + 1 + cc;
+                int32_t uM = up.x, uI = up.y;
+                uint32_t wd[K / 4];
+#pragma unroll
+                for (int q = 0; q < K / 4; ++q) wd[q] = 0;
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const int32_t s = ((tm >> k) & 1u) ? smt : smm;
+                    const int32_t mx = __vimax3_s32(dM, dD, dI);
+                    int32_t mv = mx == NEG ? NEG : mx + s;
+                    if (LOCAL) mv = max(mv, 0);
+                    const int32_t a1 = __viaddmax_s32(uM, o, NEG), a2 = __viaddmax_s32(uI, e, NEG);
+                    int32_t iv = max(a1, a2);
+                    const int32_t b1 = __viaddmax_s32(Mp[k], o, NEG), b2 = __viaddmax_s32(Dp[k], e, NEG);
+                    int32_t dv = max(b1, b2);
+                    // matchMax with its quirk (I wins over M, then D only
+                    // when I does not), insMax, delMax, M > 0
+                    uint32_t cd = dI > dM ? (uint32_t)OP_I : (dD > dM ? (uint32_t)OP_D : (uint32_t)OP_M);
+                    cd |= (a1 > a2 ? 4u : 0u) | (b1 > b2 ? 8u : 0u);
+                    if (LOCAL) cd |= mv > 0 ? 16u : 0u;
+                    if (BANDED) {
+                        if ((unsigned)(cc - (rr0 + k) - dg + w) > (unsigned)(2 * w)) { mv = NEG; iv = NEG; dv = NEG; }
+                    }
+                    if (LOCAL && k < nrow) {
+                        const int64_t key = j * (L + 1) + (i0 + k);
+                        if (mv > best || (mv == best && key < bkey)) { best = mv; bkey = key; }
+                    }
+                    wd[k >> 2] |= cd << (8 * (k & 3));
+                    dM = Mp[k]; dI = Ip[k]; dD = Dp[k];
+                    Mp[k] = mv; Ip[k] = iv; Dp[k] = dv;
+                    uM = mv; uI = iv;
+                }
+                if constexpr (K == 8) {
+                    *reinterpret_cast<uint2*>(code + (int64_t)cc * K) = make_uint2(wd[0], wd[1]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < K / 16; ++q)
+                        reinterpret_cast<uint4*>(code + (int64_t)cc * K)[q] =
+                            make_uint4(wd[4 * q], wd[4 * q + 1], wd[4 * q + 2], wd[4 * q + 3]);
+                }
+                dM = up.x; dI = up.y; dD = up.z;  // (stripe row - 1, cc): the next column's diagonal
+                if (nrow == K) rb4[cc] = make_int4(Mp[K - 1], Ip[K - 1], Dp[K - 1], 0);
+                if (last) {
+                    int32_t lm = Mp[0], li = Ip[0], ld = Dp[0];
+#pragma unroll
+                    for (int k = 1; k < K; ++k)
+                        if (k < nrow) { lm = Mp[k]; li = Ip[k]; ld = Dp[k]; }
+                    g.lastrow[cc * 3] = lm; g.lastrow[cc * 3 + 1] = li; g.lastrow[cc * 3 + 2] = ld;
+                }
+            }
+            if (chi == C - 1) {
+#pragma unroll
+                for (int k = 0; k < K; ++k)
+                    if (k < nrow) {
+                        int32_t* lc = g.lastcol + (int64_t)(rr0 + k) * 3;
+                        lc[0] = Mp[k]; lc[1] = Ip[k]; lc[2] = Dp[k];
+                    }
+            }
+            cells += (int64_t)nrow * (chi - clo + 1);  // cells evaluated (a band's stripe is a parallelogram)
+            if (BANDED) { plo = clo; phi = chi; }
         }
         return cells;
     }
@@ -1072,8 +1234,13 @@ struct DpArgs {
     msg_aln* aln;
     DpParams pp;
     uint32_t* status;
-    const int64_t* list;                  // chains handled by this launch
-    const unsigned long long* n_list;     // its length, on the device
+    // Chains handled by this launch: with cls >= 0, the cls-th range of the
+    // class-sorted list `list` (range lengths cls_n[0..], on the device);
+    // otherwise list[0 .. *n_list).
+    const int64_t* list;
+    const unsigned long long* n_list;
+    const unsigned long long* cls_n;
+    int cls;
     int64_t* tb_list;                     // chains whose traceback k_traceback runs
     unsigned long long* tb_n;
     // Banded flanks (GLOBAL mode). band[2c], band[2c+1]: half-width of the 5'
@@ -1229,9 +1396,11 @@ __device__ __forceinline__ void dp_traceback(const DpArgs& a, int64_t c, const C
     if (a.keep) a.keep[c] = (best == NEG || below_filter(best, x.L, a.min_rate)) && a.min_rate >= 0 ? 0 : 1;
 }
 
-template <bool WARP, bool BAND>
+// KST > 0 (thread path): rectangles filled by fill_rect_stripe<KST>, codes
+// in its stripe layout; KST == 0: fill_rect_thread (thread) or the warp fills.
+template <bool WARP, bool BAND, int KST = 0>
 __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, int32_t* rbnd, int32_t* cbnd,
-                                         int4* gsd) {
+                                         int4* gsd, uint32_t* stab = nullptr) {
     const int lane = WARP ? lane_id() : 0;
     const int stride = WARP ? 32 : 1;
     ChainCtx x;
@@ -1251,6 +1420,8 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
     x.roff = aux + x.n;
     x.pp = a.pp;
     x.status = a.status;
+    x.kst = KST;
+    x.stab = stab;
     // geometry in sd/rbnd/cbnd; a warp working in shared memory also leaves a
     // copy in the chain's global slot (gsd) for k_traceback
     int32_t* grb = reinterpret_cast<int32_t*>(gsd + x.n);
@@ -1302,7 +1473,16 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
     int64_t cells = 0;
     int32_t x5 = NEG;       // best state value where the 5' rectangle meets the first seed
     auto fill = [&](int m, int w) {
-        if constexpr (!WARP) {
+        if constexpr (!WARP && KST > 0) {
+            if constexpr (BAND) {
+                if (w >= 0) {
+                    cells += x.template fill_rect_stripe<KST, false, true>(m, w, best, bkey);
+                    return;
+                }
+            }
+            if (x.pp.mode == 1) cells += x.template fill_rect_stripe<KST, true, false>(m, -1, best, bkey);
+            else cells += x.template fill_rect_stripe<KST, false, false>(m, -1, best, bkey);
+        } else if constexpr (!WARP) {
             cells += x.fill_rect_thread(m, w, best, bkey);
         } else {
             if constexpr (BAND) {
@@ -1475,34 +1655,71 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
 }
 
 
-// One warp per chain. BAND: the chains with a banded flank (GLOBAL mode);
-// kept apart so that each kernel holds only the fills it runs.
+// First entry and length of the chains of a launch (DpArgs::list).
+__device__ __forceinline__ void dp_range(const DpArgs& a, int64_t& first, int64_t& n) {
+    first = 0;
+    if (a.cls >= 0) {
+        for (int q = 0; q < a.cls; ++q) first += (int64_t)a.cls_n[q];
+        n = (int64_t)a.cls_n[a.cls];
+    } else {
+        n = (int64_t)*a.n_list;
+    }
+}
+
+// One warp per chain (grid-stride over the launch's chains). BAND: chains
+// with a banded flank (GLOBAL mode); kept apart so that each kernel holds
+// only the fills it runs.
 template <bool BAND>
 __global__ void __launch_bounds__(kDpWarps * 32, BAND ? 4 : 6) k_dp(DpArgs a) {
     __shared__ int4 s_sd[kDpWarps][kSmemSeeds];
     __shared__ int32_t s_bnd[kDpWarps][2][2 * kSmemSeeds + 2];
     const int w = threadIdx.x >> 5;
-    const int64_t wi = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (wi >= (int64_t)*a.n_list) return;
-    const int64_t c = a.list[wi];
-    const int n = a.chain_len[c];
-    int4* gbase = a.sdbuf + 2 * a.chain_idx_off[c] + c;  // 2n+1 int4 per chain when not in shared memory
-    const bool in_smem = n <= kSmemSeeds;
-    int4* sd = in_smem ? s_sd[w] : gbase;
-    int32_t* rbnd = in_smem ? s_bnd[w][0] : reinterpret_cast<int32_t*>(gbase + n);
-    int32_t* cbnd = in_smem ? s_bnd[w][1] : rbnd + 2 * n + 2;
-    dp_chain<true, BAND>(a, c, sd, rbnd, cbnd, gbase);
+    int64_t first, n_items;
+    dp_range(a, first, n_items);
+    const int64_t n_warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t wi = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; wi < n_items; wi += n_warps) {
+        const int64_t c = a.list[first + wi];
+        const int n = a.chain_len[c];
+        int4* gbase = a.sdbuf + 2 * a.chain_idx_off[c] + c;  // 2n+1 int4 per chain when not in shared memory
+        const bool in_smem = n <= kSmemSeeds;
+        int4* sd = in_smem ? s_sd[w] : gbase;
+        int32_t* rbnd = in_smem ? s_bnd[w][0] : reinterpret_cast<int32_t*>(gbase + n);
+        int32_t* cbnd = in_smem ? s_bnd[w][1] : rbnd + 2 * n + 2;
+        dp_chain<true, BAND>(a, c, sd, rbnd, cbnd, gbase);
+        __syncwarp();
+    }
 }
 
-// Chains whose rectangles are all small: one thread each.
+// Chains whose rectangles are all small: one thread each, row by row.
 __global__ void __launch_bounds__(128) k_dp_small(DpArgs a) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= (int64_t)*a.n_list) return;
-    const int64_t c = a.list[t];
-    const int n = a.chain_len[c];
-    int4* gbase = a.sdbuf + 2 * a.chain_idx_off[c] + c;
-    int32_t* rbnd = reinterpret_cast<int32_t*>(gbase + n);
-    dp_chain<false, false>(a, c, gbase, rbnd, rbnd + 2 * n + 2, gbase);
+    int64_t first, n_items;
+    dp_range(a, first, n_items);
+    const int64_t n_thr = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_items; t += n_thr) {
+        const int64_t c = a.list[first + t];
+        const int n = a.chain_len[c];
+        int4* gbase = a.sdbuf + 2 * a.chain_idx_off[c] + c;
+        int32_t* rbnd = reinterpret_cast<int32_t*>(gbase + n);
+        dp_chain<false, false>(a, c, gbase, rbnd, rbnd + 2 * n + 2, gbase);
+    }
+}
+
+// Mid-size chains: one thread each, rectangles in register stripes of K rows
+// (fill_rect_stripe), traceback in the same thread. BAND: chains with a
+// banded flank.
+template <int K, bool BAND>
+__global__ void __launch_bounds__(kStripeThreads, 4) k_dp_stripe(DpArgs a) {
+    __shared__ uint32_t s_tab[16 * kStripeThreads];  // per-thread score tables, word t of thread x at t * 128 + x
+    int64_t first, n_items;
+    dp_range(a, first, n_items);
+    const int64_t n_thr = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_items; t += n_thr) {
+        const int64_t c = a.list[first + t];
+        const int n = a.chain_len[c];
+        int4* gbase = a.sdbuf + 2 * a.chain_idx_off[c] + c;
+        int32_t* rbnd = reinterpret_cast<int32_t*>(gbase + n);
+        dp_chain<false, BAND, K>(a, c, gbase, rbnd, rbnd + 2 * n + 2, gbase, s_tab + threadIdx.x);
+    }
 }
 
 // Tracebacks of the chains filled by the warp kernels, one thread each (a

@@ -85,6 +85,13 @@ struct msg_ctx {
     msg::DevBuf in_seq[2], in_off[2], stage[2];
     bool band_loaded = false;
     int64_t scratch_limit = 16ll << 30;  // DP rectangle storage per pass (msg_ctx_set_scratch_limit)
+    // DP work split (msg_ctx_set_dp_shape): unbanded chains of at most
+    // dp_small_area rectangle cells run row by row on one thread, chains of
+    // at most dp_warp_area in register stripes of dp_k rows on one thread,
+    // larger ones on a warp
+    int dp_k = 16;
+    int64_t dp_small_area = 256;
+    int64_t dp_warp_area = 65536;
     cudaEvent_t ev[8];
     const msg_aln* res_aln = nullptr;
     const uint32_t* res_cigar = nullptr;

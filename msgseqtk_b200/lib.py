@@ -29,7 +29,7 @@ assert ALN_DTYPE.itemsize == 88
 EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy", "msg_index_load", "msg_db_read",
            "msg_db_views", "msg_db_free", "msg_index_bytes",
            "msg_map_params_default", "msg_map_batch", "msg_map_batches", "msg_map_batch_device", "msg_last_stats",
-           "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
+           "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_ctx_set_dp_shape", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
            "msg_band_train", "msg_band_grad", "msg_tail_params_default", "msg_tail_batch", "msg_pair_params_default", "msg_tail_pe_batch",
            "msg_fastq_parse", "msg_fastq_format", "msg_clean_format", "msg_sam_format",
            "msg_mem_params_default", "msg_mem_batch", "msg_clean_batch",
@@ -152,6 +152,7 @@ def load_library(path: str = LIB_PATH):
     L.msg_result_device.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     L.msg_ctx_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     L.msg_ctx_set_scratch_limit.argtypes = [C.c_void_p, C.c_int64]
+    L.msg_ctx_set_dp_shape.argtypes = [C.c_void_p, C.c_int32, C.c_int64, C.c_int64]
     L.msg_smem_batch_noalloc.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(MapParams),
                                          C.c_void_p, C.c_int64, C.c_void_p]
     f32p = C.POINTER(C.c_float)
@@ -629,6 +630,11 @@ class Context:
 
     def set_scratch_limit(self, nbytes: int):
         self._check(self.lib.msg_ctx_set_scratch_limit(self.h, int(nbytes)), "msg_ctx_set_scratch_limit")
+
+    def set_dp_shape(self, stripe_rows: int = 16, small_area: int = 256, warp_area: int = 65536):
+        """DP work split (msg_ctx_set_dp_shape); records do not depend on it."""
+        self._check(self.lib.msg_ctx_set_dp_shape(self.h, int(stripe_rows), int(small_area), int(warp_area)),
+                    "msg_ctx_set_dp_shape")
 
     def stats(self) -> dict:
         s = MapStats()
