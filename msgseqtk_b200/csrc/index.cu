@@ -10,20 +10,20 @@
 
 namespace msg {
 
-// One thread per bucket: pack 64 nt16 BWT symbols into 2-bit codes and count
-// $, A, C, G locally.
+// One thread per bucket: pack 64 nt16 BWT symbols into the two bit planes of
+// their 2-bit codes and count $, A, C, G, N locally ('$' and N are stored as A).
 __global__ void k_pack_buckets(const uint8_t* __restrict__ bwt, int64_t n, int64_t nb, Bucket* __restrict__ bkt,
                                uint32_t* __restrict__ cd, uint32_t* __restrict__ ca, uint32_t* __restrict__ cc,
-                               uint32_t* __restrict__ cg, uint32_t* __restrict__ bad) {
+                               uint32_t* __restrict__ cg, uint32_t* __restrict__ cn, uint32_t* __restrict__ bad) {
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= nb) return;
-    uint32_t words[kBucketWords];
-    uint32_t nd = 0, na = 0, nc = 0, ng = 0;
+    uint32_t plo[2], phi[2];
+    uint32_t nd = 0, na = 0, nc = 0, ng = 0, nn = 0;
     const int64_t base = k * kBucketSyms;
-    for (int w = 0; w < kBucketWords; ++w) {
-        uint32_t x = 0;
-        for (int t = 0; t < 16; ++t) {
-            const int64_t i = base + w * 16 + t;
+    for (int w = 0; w < 2; ++w) {
+        uint32_t xl = 0, xh = 0;
+        for (int t = 0; t < 32; ++t) {
+            const int64_t i = base + w * 32 + t;
             int code = 0;
             if (i < n) {
                 const int b = bwt[i];
@@ -33,32 +33,44 @@ __global__ void k_pack_buckets(const uint8_t* __restrict__ bwt, int64_t n, int64
                     case 2: nc++; code = 1; break;
                     case 4: ng++; code = 2; break;
                     case 8: code = 3; break;
+                    case 15: nn++; code = 0; break;
                     default: atomicOr(bad, 1u); break;
                 }
             }
-            x |= (uint32_t)code << (2 * t);
+            xl |= (uint32_t)(code & 1) << t;
+            xh |= (uint32_t)(code >> 1) << t;
         }
-        words[w] = x;
+        plo[w] = xl;
+        phi[w] = xh;
     }
-    for (int w = 0; w < kBucketWords; ++w) bkt[k].bits[w] = words[w];
-    cd[k] = nd; ca[k] = na; cc[k] = nc; cg[k] = ng;
+    for (int w = 0; w < 2; ++w) { bkt[k].lo[w] = plo[w]; bkt[k].hi[w] = phi[w]; }
+    cd[k] = nd; ca[k] = na; cc[k] = nc; cg[k] = ng; cn[k] = nn;
 }
 
+// Counts before each bucket; bit 31 of the '$' count flags a bucket holding a
+// '$' or an N (exc: '$' and N in the bucket).
 __global__ void k_fill_counts(int64_t nb, Bucket* __restrict__ bkt, const uint32_t* __restrict__ cd,
                               const uint32_t* __restrict__ ca, const uint32_t* __restrict__ cc,
-                              const uint32_t* __restrict__ cg, const uint32_t* __restrict__ ld) {
+                              const uint32_t* __restrict__ cg, const uint32_t* __restrict__ exc) {
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= nb) return;
-    bkt[k].cnt[0] = cd[k] | (ld[k] ? 0x80000000u : 0u);
+    bkt[k].cnt[0] = cd[k] | (exc[k] ? 0x80000000u : 0u);
     bkt[k].cnt[1] = ca[k];
     bkt[k].cnt[2] = cc[k];
     bkt[k].cnt[3] = cg[k];
 }
 
-__global__ void k_collect_dollars(const uint8_t* __restrict__ bwt, int64_t n, int64_t* __restrict__ rows,
-                                  unsigned long long* __restrict__ cnt, int64_t cap) {
+__global__ void k_add_u32(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b, int64_t n,
+                          uint32_t* __restrict__ out) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k < n) out[k] = a[k] + b[k];
+}
+
+// Rows whose BWT symbol is `sym`, in any order.
+__global__ void k_collect_rows(const uint8_t* __restrict__ bwt, int64_t n, int sym, int64_t* __restrict__ rows,
+                               unsigned long long* __restrict__ cnt, int64_t cap) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        if (bwt[i] == 0) {
+        if (bwt[i] == sym) {
             const unsigned long long s = atomicAdd(cnt, 1ull);
             if ((int64_t)s < cap) rows[s] = i;
         }
@@ -89,7 +101,7 @@ __global__ void k_recover_sa(IndexDev ix, const int64_t* __restrict__ rows, cons
         const int b = bwt_at(ix, row);
         if (b == 0) return;
         const Occ5 o = occ5(ix, row);
-        const int64_t nxt = ix.C[b] + o.c[to_int(b)] - 1;
+        const int64_t nxt = ix.C[b] + o.c[occ_slot(b)] - 1;
         if ((start_bits[nxt >> 5] >> (nxt & 31)) & 1u) return;
         val -= 1;
         row = nxt;
@@ -123,7 +135,7 @@ __global__ void k_dollar_sa(IndexDev ix, const int64_t* __restrict__ srows, cons
         const int b = bwt_at(ix, row);
         if (b == 0) break;
         const Occ5 o = occ5(ix, row);
-        row = ix.C[b] + o.c[to_int(b)] - 1;
+        row = ix.C[b] + o.c[occ_slot(b)] - 1;
         ++dist;
     }
     atomicOr(err, kErrInternal);
@@ -137,7 +149,7 @@ __global__ void k_occ_query(IndexDev ix, int64_t cnt, const uint8_t* __restrict_
     if (pos < 0 || pos >= ix.n) { out[k] = -1; return; }
     const Occ5 o = occ5(ix, pos);
     const int s = b[k];
-    out[k] = s == 0 ? o.c[0] : is_basic(s) ? o.c[to_int(s)] : 0;
+    out[k] = (s == 0 || s == 15 || is_basic(s)) ? o.c[occ_slot(s)] : 0;
 }
 
 __global__ void k_ext_query(IndexDev ix, int64_t cnt, int dir, const uint8_t* __restrict__ b, int64_t* __restrict__ p,
@@ -174,8 +186,9 @@ extern "C" int msg_index_load(msg_ctx* ctx, const msg_fmd_view* fmd, const msg_m
     int64_t tot = 0;
     for (int b = 0; b < 16; ++b) {
         if (B[b] < 0) return MSG_EINVAL;
-        if (B[b] > 0 && !(b == 0 || b == 1 || b == 2 || b == 4 || b == 8))
-            return ctx->fail(MSG_EUNSUPPORTED, "BWT symbols other than $,A,C,G,T (N or IUPAC) are not supported");
+        // FMDIndex::buildCounts rejects IUPAC-extended codes (FMDIndex.cpp:130-133)
+        if (B[b] > 0 && !(b == 0 || b == 1 || b == 2 || b == 4 || b == 8 || b == 15))
+            return ctx->fail(MSG_EINVAL, "BWT symbols other than $,A,C,G,T,N (IUPAC-extended codes)");
         tot += B[b];
     }
     if (tot != n) return MSG_EINVAL;
@@ -205,16 +218,18 @@ extern "C" int msg_index_load(msg_ctx* ctx, const msg_fmd_view* fmd, const msg_m
     CK(cudaMalloc(&im.bkt, nb * sizeof(Bucket)));
     CK(cudaMalloc(&d_bwt, n));
     CK(cudaMemcpyAsync(d_bwt, fmd->bwt, n, cudaMemcpyHostToDevice, st));
-    CK(cudaMalloc(&tmp, 9 * nb * sizeof(uint32_t) + 16));
+    CK(cudaMalloc(&tmp, 11 * nb * sizeof(uint32_t) + 16));
     CK(cudaMalloc(&d_bad, sizeof(uint32_t)));
     CK(cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), st));
     {
         uint32_t* cd = tmp; uint32_t* ca = tmp + nb; uint32_t* cc = tmp + 2 * nb; uint32_t* cg = tmp + 3 * nb;
         uint32_t* sd = tmp + 4 * nb; uint32_t* sa_ = tmp + 5 * nb; uint32_t* sc = tmp + 6 * nb; uint32_t* sg = tmp + 7 * nb;
         uint32_t* ld = tmp + 8 * nb;
-        k_pack_buckets<<<blocks_for(nb, 256), 256, 0, st>>>(d_bwt, n, nb, im.bkt, cd, ca, cc, cg, d_bad);
+        uint32_t* cn = tmp + 9 * nb; uint32_t* sn = tmp + 10 * nb;
+        k_pack_buckets<<<blocks_for(nb, 256), 256, 0, st>>>(d_bwt, n, nb, im.bkt, cd, ca, cc, cg, cn, d_bad);
         CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(ld, cd, nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        k_add_u32<<<blocks_for(nb, 256), 256, 0, st>>>(cd, cn, nb, ld);  // '$' and N of each bucket
+        CK(cudaGetLastError());
         size_t tb = 0;
         CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, cd, sd, (int)nb, st));
         void* dt = nullptr;
@@ -225,13 +240,38 @@ extern "C" int msg_index_load(msg_ctx* ctx, const msg_fmd_view* fmd, const msg_m
         CK(cub::DeviceScan::ExclusiveSum(dt, tb, cg, sg, (int)nb, st));
         k_fill_counts<<<blocks_for(nb, 256), 256, 0, st>>>(nb, im.bkt, sd, sa_, sc, sg, ld);
         CK(cudaGetLastError());
+        if (B[15] > 0) {  // N before each bucket
+            CK(cub::DeviceScan::ExclusiveSum(dt, tb, cn, sn, (int)nb, st));
+            CK(cudaMalloc(&im.n_before, nb * sizeof(uint32_t)));
+            CK(cudaMemcpyAsync(im.n_before, sn, nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        }
         CK(cudaStreamSynchronize(st));
         cudaFree(dt);
     }
     {
         uint32_t bad = 0;
         CK(cudaMemcpy(&bad, d_bad, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-        if (bad) { rc = ctx->fail(MSG_EUNSUPPORTED, "BWT holds symbols other than $,A,C,G,T"); goto done; }
+        if (bad) { rc = ctx->fail(MSG_EINVAL, "BWT holds symbols other than $,A,C,G,T,N"); goto done; }
+    }
+    // N rows of the BWT (sorted)
+    if (B[15] > 0) {
+        const int64_t nn = B[15];
+        CK(cudaMalloc(&im.n_rows, nn * sizeof(int64_t)));
+        unsigned long long* ncnt = reinterpret_cast<unsigned long long*>(tmp);
+        CK(cudaMemsetAsync(ncnt, 0, sizeof(unsigned long long), st));
+        k_collect_rows<<<ctx->num_sms * 8, 256, 0, st>>>(d_bwt, n, 15, im.n_rows, ncnt, nn);
+        CK(cudaGetLastError());
+        unsigned long long got = 0;
+        CK(cudaMemcpyAsync(&got, ncnt, sizeof(got), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if ((int64_t)got != nn) { rc = ctx->fail(MSG_EINVAL, "number of N in the BWT differs from B[15]"); goto done; }
+        std::vector<int64_t> nrows(nn);
+        CK(cudaMemcpy(nrows.data(), im.n_rows, nn * sizeof(int64_t), cudaMemcpyDeviceToHost));
+        std::sort(nrows.begin(), nrows.end());
+        CK(cudaMemcpy(im.n_rows, nrows.data(), nn * sizeof(int64_t), cudaMemcpyHostToDevice));
+        ix.n_rows = im.n_rows;
+        ix.n_n = nn;
+        ix.n_before = im.n_before;
     }
     // '$' rows of the BWT
     {
@@ -239,7 +279,7 @@ extern "C" int msg_index_load(msg_ctx* ctx, const msg_fmd_view* fmd, const msg_m
         CK(cudaMalloc(&im.dollar_rows, nd * sizeof(int64_t)));
         unsigned long long* dcnt = reinterpret_cast<unsigned long long*>(tmp);
         CK(cudaMemsetAsync(dcnt, 0, sizeof(unsigned long long), st));
-        k_collect_dollars<<<ctx->num_sms * 8, 256, 0, st>>>(d_bwt, n, im.dollar_rows, dcnt, nd);
+        k_collect_rows<<<ctx->num_sms * 8, 256, 0, st>>>(d_bwt, n, 0, im.dollar_rows, dcnt, nd);
         CK(cudaGetLastError());
         unsigned long long got = 0;
         CK(cudaMemcpyAsync(&got, dcnt, sizeof(got), cudaMemcpyDeviceToHost, st));
@@ -368,7 +408,9 @@ extern "C" int msg_index_load(msg_ctx* ctx, const msg_fmd_view* fmd, const msg_m
         ix.chr_off = im.chr_tab + 3 * nc;
         ix.chr_seq = im.chr_seq;
         ix.n_chrom = nc;
-        im.bytes = nb * sizeof(Bucket) + B[0] * sizeof(int64_t) + n * sizeof(uint32_t) + 4 * nc * 8 + tl;
+        im.chr_len_host.assign(mtg->chr_len, mtg->chr_len + nc);
+        im.bytes = nb * sizeof(Bucket) + B[0] * sizeof(int64_t) + n * sizeof(uint32_t) + 4 * nc * 8 + tl +
+                   (B[15] > 0 ? B[15] * (int64_t)sizeof(int64_t) + nb * (int64_t)sizeof(uint32_t) : 0);
         CK(cudaStreamSynchronize(st));
     }
     // loglik table (FMDIndex::loglik, FMDIndex.h:195-197)

@@ -18,12 +18,15 @@ struct IndexImage {
     bool loaded = false;
     Bucket* bkt = nullptr;
     int64_t* dollar_rows = nullptr;
+    int64_t* n_rows = nullptr;
+    uint32_t* n_before = nullptr;
     uint32_t* sa = nullptr;
     int64_t* chr_tab = nullptr;
     uint8_t* chr_seq = nullptr;
     int64_t B[16] = {0};
     double llk[16] = {0};
     int64_t bytes = 0;
+    std::vector<int64_t> chr_len_host;  // chromosome lengths, for host-side checks of caller arrays
     IndexDev dev{};
 };
 
@@ -121,6 +124,8 @@ struct msg_ctx {
     void index_free() {
         if (idx.bkt) cudaFree(idx.bkt);
         if (idx.dollar_rows) cudaFree(idx.dollar_rows);
+        if (idx.n_rows) cudaFree(idx.n_rows);
+        if (idx.n_before) cudaFree(idx.n_before);
         if (idx.sa) cudaFree(idx.sa);
         if (idx.chr_tab) cudaFree(idx.chr_tab);
         if (idx.chr_seq) cudaFree(idx.chr_seq);

@@ -2,11 +2,17 @@
 //
 // Index image in HBM
 //   * occurrence buckets: 32 B each (one DRAM sector), 64 BWT symbols per bucket.
-//       word 0: count of '$' before the bucket (bit 31 set when the bucket holds a '$')
+//       word 0: count of '$' before the bucket (bit 31 set when the bucket
+//       holds a '$' or an N)
 //       words 1-3: counts of A, C, G before the bucket (T is derived)
-//       words 4-7: 64 symbols x 2 bits (A=0, C=1, G=2, T=3; '$' stored as A)
-//     one 32 B load (2 x 128-bit) gives all five counts at any row.
+//       words 4-5 / 6-7: the low / high bit planes of the 64 symbols' 2-bit
+//       codes (A=00, C=01, G=10, T=11; '$' and N stored as A), symbol k at bit k
+//     one 32 B load (2 x 128-bit) gives all five counts at any row; a count
+//     inside the bucket is one masked 64-bit popcount of a plane expression.
 //   * dollar rows: sorted rows whose BWT symbol is '$' (2 per chromosome).
+//   * N (genomes with N runs; the reference's BWT alphabet is $,A,C,G,T plus
+//     N, FMDIndex.cpp:118-133): sorted rows whose BWT symbol is N, and the
+//     count of N before each bucket (absent when the BWT holds no N).
 //   * full suffix array, uint32 per row (N < 2^32), so locating a row is one
 //     4-byte gather instead of an LF walk.
 //   * chromosome table and forward nt16 target sequences for the DP.
@@ -17,11 +23,11 @@
 namespace msg {
 
 constexpr int kBucketSyms = 64;
-constexpr int kBucketWords = 4;
 
 struct __align__(32) Bucket {
     uint32_t cnt[4];
-    uint32_t bits[kBucketWords];
+    uint32_t lo[2];  // low code bit of symbols 0..31 (lo[0]) and 32..63 (lo[1])
+    uint32_t hi[2];  // high code bit
 };
 static_assert(sizeof(Bucket) == 32, "bucket must be one 32 B sector");
 
@@ -35,11 +41,16 @@ __host__ __device__ inline int comp16(int b) {
     return ((b & 1) << 3) | ((b & 2) << 1) | ((b & 4) >> 1) | ((b & 8) >> 3);
 }
 __host__ __device__ inline int encode_int(int j) { return j == 1 ? 1 : j == 2 ? 2 : j == 3 ? 4 : j == 4 ? 8 : 0; }
+// slot of a BWT symbol in Occ5: $,A,C,G,T -> 0..4, N -> 5
+__host__ __device__ inline int occ_slot(int b) { return b == 15 ? 5 : to_int(b); }
 
 struct IndexDev {
     const Bucket* bkt;
     const int64_t* dollar_rows;
     int64_t n_dollar;
+    const int64_t* n_rows;     // sorted rows whose symbol is N
+    int64_t n_n;
+    const uint32_t* n_before;  // per bucket: N before it (null when n_n == 0)
     const uint32_t* sa;
     int64_t n;
     int64_t C[17];           // FMDIndex::C for nt16 codes 0..16
@@ -52,47 +63,54 @@ struct IndexDev {
 };
 
 struct Occ5 {
-    int64_t c[5];  // $, A, C, G, T in BWT[0 .. i]
+    int64_t c[6];  // $, A, C, G, T, N in BWT[0 .. i]
 };
 
-// Count of '$' rows in [lo, hi) by binary search in the sorted dollar rows.
-__device__ inline int64_t dollar_between(const IndexDev& ix, int64_t lo, int64_t hi) {
-    int64_t a = 0, b = ix.n_dollar;
-    while (a < b) { int64_t m = (a + b) >> 1; if (ix.dollar_rows[m] < lo) a = m + 1; else b = m; }
-    int64_t s = a;
-    a = s; b = ix.n_dollar;
-    while (a < b) { int64_t m = (a + b) >> 1; if (ix.dollar_rows[m] < hi) a = m + 1; else b = m; }
+// Count of rows in [lo, hi) of a sorted row list, by binary search.
+__device__ inline int64_t rows_between(const int64_t* rows, int64_t n, int64_t lo, int64_t hi) {
+    int64_t a = 0, b = n;
+    while (a < b) { int64_t m = (a + b) >> 1; if (rows[m] < lo) a = m + 1; else b = m; }
+    const int64_t s = a;
+    b = n;
+    while (a < b) { int64_t m = (a + b) >> 1; if (rows[m] < hi) a = m + 1; else b = m; }
     return a - s;
 }
+// '$' rows and N rows in [lo, hi)
+__device__ inline int64_t dollar_between(const IndexDev& ix, int64_t lo, int64_t hi) {
+    return rows_between(ix.dollar_rows, ix.n_dollar, lo, hi);
+}
+__device__ inline int64_t nsym_between(const IndexDev& ix, int64_t lo, int64_t hi) {
+    return ix.n_n ? rows_between(ix.n_rows, ix.n_n, lo, hi) : 0;
+}
 
-// Counts of $,A,C,G,T among the first r symbols of a loaded bucket k. With
-// lo/hi the low/high code bits of each symbol: T = lo&hi, C = lo-T, G = hi-T,
-// A (and '$') = r - C - G - T.
+// Bits 0 .. r-1 set (r in [0, 64]): the symbols before row k*64 + r.
+__device__ __forceinline__ uint64_t prefix_mask(uint32_t r) { return r >= 64 ? ~0ull : ((1ull << r) - 1ull); }
+
+__device__ __forceinline__ uint64_t plane_lo(const uint4& w1) { return ((uint64_t)w1.y << 32) | w1.x; }
+__device__ __forceinline__ uint64_t plane_hi(const uint4& w1) { return ((uint64_t)w1.w << 32) | w1.z; }
+
+// Counts of $,A,C,G,T,N among the first r symbols of a loaded bucket k, from
+// the bit planes: T = lo&hi, C = lo&~hi, G = ~lo&hi, A ('$' and N included)
+// the rest; '$' and N inside the bucket from their row lists.
 __device__ inline Occ5 occ5_in(const IndexDev& ix, int64_t k, int r, const uint4& w0, const uint4& w1) {
     Occ5 o;
-    const uint32_t words[kBucketWords] = {w1.x, w1.y, w1.z, w1.w};
-    uint32_t n_lo = 0, n_hi = 0, n_t = 0;
-#pragma unroll
-    for (int w = 0; w < kBucketWords; ++w) {
-        const int nv = min(max(r - 16 * w, 0), 16);
-        const uint32_t m = nv >= 16 ? 0xffffffffu : ((1u << (2 * nv)) - 1u);
-        const uint32_t x = words[w] & m;
-        const uint32_t lo = x & 0x55555555u, hi = (x >> 1) & 0x55555555u;
-        n_lo += __popc(lo);
-        n_hi += __popc(hi);
-        n_t += __popc(lo & hi);
-    }
-    const uint32_t nC = n_lo - n_t, nG = n_hi - n_t;
+    const uint64_t lo = plane_lo(w1), hi = plane_hi(w1), m = prefix_mask((uint32_t)r);
+    const uint32_t n_t = (uint32_t)__popcll(lo & hi & m);
+    const uint32_t nC = (uint32_t)__popcll(lo & ~hi & m), nG = (uint32_t)__popcll(~lo & hi & m);
     const uint32_t nA = (uint32_t)r - nC - nG - n_t;
     const int64_t j = k * kBucketSyms + r;
-    const bool has_dollar = (w0.x >> 31) != 0;
-    int64_t d_in = 0;
-    if (has_dollar && r > 0) d_in = dollar_between(ix, k * kBucketSyms, j);
+    const bool has_exc = (w0.x >> 31) != 0;
+    int64_t d_in = 0, n_in = 0;
+    if (has_exc && r > 0) {
+        d_in = dollar_between(ix, k * kBucketSyms, j);
+        n_in = nsym_between(ix, k * kBucketSyms, j);
+    }
     o.c[0] = (int64_t)(w0.x & 0x7fffffffu) + d_in;
-    o.c[1] = (int64_t)w0.y + (int64_t)nA - d_in;
+    o.c[1] = (int64_t)w0.y + (int64_t)nA - d_in - n_in;
     o.c[2] = (int64_t)w0.z + nC;
     o.c[3] = (int64_t)w0.w + nG;
-    o.c[4] = j - o.c[0] - o.c[1] - o.c[2] - o.c[3];
+    o.c[5] = (ix.n_before ? (int64_t)__ldg(ix.n_before + k) : 0) + n_in;
+    o.c[4] = j - o.c[0] - o.c[1] - o.c[2] - o.c[3] - o.c[5];
     return o;
 }
 
@@ -119,18 +137,21 @@ __device__ inline void occ5_pair(const IndexDev& ix, int64_t i_lo, int64_t i_hi,
     hi = occ5_in(ix, kb, (int)(jb - kb * kBucketSyms), b0, b1);
 }
 
-// BWT symbol (nt16) at row i, with its occurrence count in BWT[0 .. i].
+// BWT symbol (nt16) at row i.
 __device__ inline int bwt_at(const IndexDev& ix, int64_t i) {
     const int64_t k = i / kBucketSyms;
     const int r = (int)(i - k * kBucketSyms);
-    const uint32_t w = __ldg(&ix.bkt[k].bits[r >> 4]);
-    const int code = (w >> (2 * (r & 15))) & 3;
-    if (code == 0 && (__ldg(&ix.bkt[k].cnt[0]) >> 31) && dollar_between(ix, i, i + 1)) return 0;
+    const uint32_t wl = __ldg(&ix.bkt[k].lo[r >> 5]), wh = __ldg(&ix.bkt[k].hi[r >> 5]);
+    const int code = (int)(((wl >> (r & 31)) & 1u) | (((wh >> (r & 31)) & 1u) << 1));
+    if (code == 0 && (__ldg(&ix.bkt[k].cnt[0]) >> 31)) {
+        if (dollar_between(ix, i, i + 1)) return 0;
+        if (nsym_between(ix, i, i + 1)) return 15;
+    }
     return encode_int(code + 1);
 }
 
-// FMDIndex::backExt (FMDIndex.cpp:577-610). Returns the new size.
-// n_ext counts extensions that reached the occurrence lookup.
+// FMDIndex::backExt (FMDIndex.cpp:577-610). Returns the new size. The q
+// update counts '$' and the bases after b, not N, as the reference does.
 __device__ inline int64_t back_ext(const IndexDev& ix, int64_t& p, int64_t& q, int64_t& s, int b) {
     if (!is_basic(b)) return (s = 0);
     const int c = to_int(b);
@@ -160,34 +181,29 @@ __device__ inline int64_t fwd_ext(const IndexDev& ix, int64_t& p, int64_t& q, in
 // of the bases after it (C,G,T after A; G,T after C; T after G), dl =
 // occurrences of '$', all among the rows before k*64 + r. Stored counts give
 // '$', A, C, G before the bucket (T is the rest); within the bucket one masked
-// popcount per word and count: with lo/hi the low/high code bits, the bases
-// after A are lo|hi, after C hi, after G lo&hi. '$' is stored as A and
-// removed from A's count.
+// 64-bit popcount per count over the bit planes: the symbols equal to the
+// code are where both planes match its bits, the bases after A are lo|hi,
+// after C hi, after G lo&hi. '$' and N are stored as A and removed from A's
+// count; the N before the bucket come from their own table.
 __device__ __forceinline__ void occ_counts(const IndexDev& ix, uint32_t k, uint32_t r, uint32_t code, const uint4& w0,
                                            const uint4& w1, uint32_t& eq, uint32_t& gt, uint32_t& dl) {
-    const uint32_t words[kBucketWords] = {w1.x, w1.y, w1.z, w1.w};
-    const uint32_t pat = code * 0x55555555u;  // the code in every 2-bit field
-    uint32_t n_eq = 0, n_gt = 0;
-#pragma unroll
-    for (int w = 0; w < kBucketWords; ++w) {
-        const int nv = min(max((int)r - 16 * w, 0), 16);
-        const uint32_t m = nv >= 16 ? 0x55555555u : (0x55555555u & ((1u << (2 * nv)) - 1u));
-        const uint32_t x = words[w];
-        const uint32_t e = ~(x ^ pat);  // both bits set where the symbol equals the code
-        n_eq += __popc(e & (e >> 1) & m);
-        const uint32_t lo = x & 0x55555555u, hi = (x >> 1) & 0x55555555u;
-        const uint32_t g = code == 0 ? (lo | hi) : code == 1 ? hi : code == 2 ? (lo & hi) : 0u;
-        n_gt += __popc(g & m);
-    }
+    const uint64_t lo = plane_lo(w1), hi = plane_hi(w1), m = prefix_mask(r);
+    const uint64_t cl = (code & 1u) ? ~0ull : 0ull, ch = (code & 2u) ? ~0ull : 0ull;
+    const uint32_t n_eq = (uint32_t)__popcll(~(lo ^ cl) & ~(hi ^ ch) & m);
+    const uint64_t after = code == 0 ? (lo | hi) : code == 1 ? hi : code == 2 ? (lo & hi) : 0ull;
+    const uint32_t n_gt = (uint32_t)__popcll(after & m);
     const uint32_t dollar = w0.x & 0x7fffffffu;
-    uint32_t din = 0;
-    if ((w0.x >> 31) && r > 0)
+    uint32_t din = 0, nin = 0;
+    if ((w0.x >> 31) && r > 0) {
         din = (uint32_t)dollar_between(ix, (int64_t)k * kBucketSyms, (int64_t)k * kBucketSyms + r);
-    const uint32_t all = k * (uint32_t)kBucketSyms - dollar;  // bases before the bucket
+        nin = (uint32_t)nsym_between(ix, (int64_t)k * kBucketSyms, (int64_t)k * kBucketSyms + r);
+    }
+    const uint32_t nbef = ix.n_before ? __ldg(ix.n_before + k) : 0u;
+    const uint32_t all = k * (uint32_t)kBucketSyms - dollar - nbef;  // bases before the bucket
     const uint32_t a = w0.y, c = w0.z, g = w0.w;
     const uint32_t before_eq = code == 0 ? a : code == 1 ? c : code == 2 ? g : all - a - c - g;
     const uint32_t before_gt = code == 0 ? all - a : code == 1 ? all - a - c : code == 2 ? all - a - c - g : 0u;
-    eq = before_eq + n_eq - (code == 0 ? din : 0u);
+    eq = before_eq + n_eq - (code == 0 ? din + nin : 0u);
     gt = before_gt + n_gt;
     dl = dollar + din;
 }
