@@ -222,6 +222,60 @@ int msg_map_batch(msg_ctx* ctx, const msg_read_batch* reads, const msg_map_param
 int msg_map_batches(msg_ctx* ctx, int64_t n_batches, const msg_read_batch* reads, const msg_map_params* params,
                     msg_aln_out* outs);
 
+/* ---- The mapping task one stage at a time ----
+ * msg_map_batch runs these stages fused on the device; each call below stops
+ * at one of the reference's own operator boundaries and takes and returns
+ * host arrays, so a caller can inspect or replace any step (reads in host
+ * memory as for msg_map_batch; results identical to the fused call's).
+ * Caller arrays are checked before any kernel reads them (MSG_EINVAL). */
+
+/* SMEM_LIST::findAllSMEMS (src/SMEM.cpp:186-215), the first step of
+ * SMEM_LIST::findSeeds (src/SMEM.cpp:272): per read its SMEMs in emission
+ * order as rows of 6 int64 (from, to, fwdStart, revStart, size, logP bit
+ * pattern; the SMEM fields of src/SMEM.h:196-200), read i's at rows
+ * smem_off[i] .. smem_off[i+1) (n_reads + 1 offsets). *n_smem receives the
+ * row count; MSG_EINVAL, rows not written, when it exceeds smem_cap. */
+int msg_seed_batch(msg_ctx* ctx, const msg_read_batch* reads, const msg_map_params* params, int64_t* smem,
+                   int64_t smem_cap, int64_t* smem_off, int64_t* n_smem);
+
+/* SMEM::getSeeds (src/SMEM.cpp:244-269, with FMDIndex::accessSA and
+ * MetaGenome::getTid/getLoc/getStrand) of the SMEM rows the caller keeps
+ * after findSeeds' sort and maxNSeed cut (src/SMEM.cpp:275-300; read i's
+ * rows at smem_off[i] .. smem_off[i+1)), then SeedPair::removeRedundant
+ * (src/SeedPair.cpp:71-88): per read its seeds as rows of 6 int64 (from, to,
+ * start, end, tid, strand: SeedPair's fields) in the order removeRedundant
+ * leaves them, read i's at seed_off[i] .. seed_off[i+1). *n_seed receives
+ * the count; MSG_EINVAL, rows not valid, when it exceeds seed_cap. An SMEM
+ * row must lie in its read (0 <= from < to <= length) and address
+ * suffix-array rows of the index (fwdStart, revStart >= 0, + size <= n). */
+int msg_locate_batch(msg_ctx* ctx, const msg_read_batch* reads, const int64_t* smem, const int64_t* smem_off,
+                     int64_t* seed, int64_t seed_cap, int64_t* seed_off, int64_t* n_seed);
+
+/* SeedChain::getChains (src/SeedChain.cpp:40-73; maxMismatch = ceil(L*0.2)
+ * and maxIndel = ceil(L*0.1) as msgseqtk-align sets them,
+ * src/msgseqtk-align.cpp:619-620) on each read's seeds (rows as
+ * msg_locate_batch returns them): chain k of the batch holds the seeds
+ * chain_seed[chain_seed_off[k] .. chain_seed_off[k+1]), indices into its
+ * read's seed rows; read i's chains are read_chain_off[i] ..
+ * read_chain_off[i+1). *n_chain and *n_chain_seed receive the counts;
+ * MSG_EINVAL when they exceed chain_cap (chain_seed_off holds chain_cap + 1
+ * entries) or chain_seed_cap. Seeds must lie in their read and chromosome
+ * (end - start == to - from, tid < chromosomes, strand 1 or 2). */
+int msg_chain_batch(msg_ctx* ctx, const msg_read_batch* reads, const int64_t* seed, const int64_t* seed_off,
+                    int32_t* chain_seed, int64_t chain_seed_cap, int64_t* chain_seed_off, int64_t chain_cap,
+                    int64_t* read_chain_off, int64_t* n_chain, int64_t* n_chain_seed);
+
+/* Alignment::buildAlignments (src/Alignment.cpp:420-427: the window,
+ * calculateScores, backTrace and getAlnCigar of each chain) for chains as
+ * msg_chain_batch returns them: one record per chain in chain order,
+ * exactly as msg_map_batch returns them (params: mode, score scheme,
+ * min_score_rate, band_mode/band_w; the seeding fields are not used). A
+ * chain's seeds must ascend in the read's list, not overlap in the read or
+ * the target, and share tid and strand. */
+int msg_align_batch(msg_ctx* ctx, const msg_read_batch* reads, const int64_t* seed, const int64_t* seed_off,
+                    const int32_t* chain_seed, const int64_t* chain_seed_off, const int64_t* read_chain_off,
+                    const msg_map_params* params, msg_aln_out* out);
+
 /* Same as msg_map_batch with the reads already in device memory (seq and off
  * are device pointers); results still land in the caller's host buffers. */
 int msg_map_batch_device(msg_ctx* ctx, const msg_read_batch* dev_reads, const msg_map_params* params,

@@ -258,6 +258,34 @@ extern "C" void msg_map_params_default(msg_map_params* p) {
 }
 
 namespace {
+// Entry and exit points of map_impl for the per-stage calls: the pipeline
+// starts at stage `first` from the caller's host arrays and stops after stage
+// `last`, returning that stage's results in the caller's host arrays.
+enum MapStage : int { kStSmem = 0, kStLocate = 1, kStChain = 2, kStAlign = 3 };
+struct StageIO {
+    int first = kStSmem, last = kStAlign;
+    // inputs: SMEM rows (first == kStLocate), seeds (first >= kStChain), chains (first == kStAlign)
+    const int64_t* smem = nullptr;
+    const int64_t* smem_off = nullptr;
+    const int64_t* seed = nullptr;
+    const int64_t* seed_off = nullptr;
+    const int32_t* chain_seed = nullptr;
+    const int64_t* chain_seed_off = nullptr;
+    const int64_t* read_chain_off = nullptr;
+    // outputs: rows of 6 int64 (SMEMs or seeds) or chains
+    int64_t* rows = nullptr;
+    int64_t rows_cap = 0;
+    int64_t* rows_off = nullptr;
+    int64_t* n_rows = nullptr;
+    int32_t* o_chain_seed = nullptr;
+    int64_t o_chain_seed_cap = 0;
+    int64_t* o_chain_seed_off = nullptr;
+    int64_t o_chain_cap = 0;
+    int64_t* o_read_chain_off = nullptr;
+    int64_t* o_n_chain = nullptr;
+    int64_t* o_n_chain_seed = nullptr;
+};
+
 struct BandCollect {
     float* feat;
     int32_t* label;
@@ -268,7 +296,7 @@ struct BandCollect {
 
 static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, int64_t n_reads,
                     const msg_map_params* params, msg_aln_out* out, msg_stage_dump* dump,
-                    const BandCollect* collect = nullptr) {
+                    const BandCollect* collect = nullptr, const StageIO* io = nullptr) {
     DpParams dpp;
     int rc = check_params(params, &dpp);
     if (rc != MSG_OK) return ctx->fail(rc, rc == MSG_EUNSUPPORTED ? "score scheme must be non-negative integers" : "bad mapping parameters");
@@ -315,7 +343,26 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         if (h_codes & kErrCodes) return ctx->fail(MSG_EINVAL, "read bytes must be nt16 codes (0..15)");
     }
     const int64_t Lmax = (int64_t)h_maxlen;
-
+    const int first = io ? io->first : (int)kStSmem, last = io ? io->last : (int)kStAlign;
+    int64_t h_nsmem = 0;
+    int64_t* d_smem = nullptr;          // dense SMEM rows
+    int64_t* d_smem_seed_cnt = nullptr; // n_smem + 1
+    int64_t* d_smem_seed_off = nullptr; // n_smem + 1
+    int32_t* d_smem_read = nullptr;
+    int32_t* d_fill = nullptr;
+    uint8_t* d_sel = nullptr;
+    auto setup_sel = [&]() -> cudaError_t {
+        const cudaError_t e = ctx->sel.ensure((h_nsmem + 1) * (48 + 1 + 4 + 8 + 8 + 4) + 64);
+        if (e != cudaSuccess) return e;
+        d_smem = ctx->sel.as<int64_t>();
+        d_smem_seed_cnt = d_smem + 6 * h_nsmem;
+        d_smem_seed_off = d_smem_seed_cnt + (h_nsmem + 1);
+        d_smem_read = reinterpret_cast<int32_t*>(d_smem_seed_off + (h_nsmem + 1));
+        d_fill = d_smem_read + (h_nsmem + 1);
+        d_sel = reinterpret_cast<uint8_t*>(d_fill + (h_nsmem + 1));
+        return cudaSuccess;
+    };
+    if (first == kStSmem) {
     // ---------------- SMEMs ----------------
     // Reads are bucketed by length: up to kThreadMaxLen bp one thread per read
     // (k_smem_thread), longer reads one warp per read with lanes over the
@@ -345,7 +392,6 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     }
     bool thread_path = h_split[0] > 0;
     int64_t cap = 16;
-    int64_t h_nsmem = 0;
     for (int attempt = 0; attempt < 4; ++attempt) {
         int64_t h_rows = 0;
         if (n_reads > 0) S.n_launch++, k_slot_rows<<<nblk(n_reads, 256), 256, 0, st>>>(d_rlen, n_reads, cap, d_slot);
@@ -428,25 +474,42 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     }
     if (n_reads > 0) S.n_launch++, k_i32_to_i64<<<nblk(n_reads, 256), 256, 0, st>>>(ctx->smem_cnt.as<int32_t>(), d_cnt64, n_reads);
     CK(offsets(ctx, d_cnt64, n_reads, d_smem_off, misc, &h_nsmem));
-    S.n_smem = h_nsmem;
-    CK(ctx->sel.ensure((h_nsmem + 1) * (48 + 1 + 4 + 8 + 8 + 4) + 64));
-    int64_t* d_smem = ctx->sel.as<int64_t>();                              // dense SMEM rows
-    int64_t* d_smem_seed_cnt = d_smem + 6 * h_nsmem;                       // n_smem + 1
-    int64_t* d_smem_seed_off = d_smem_seed_cnt + (h_nsmem + 1);            // n_smem + 1
-    int32_t* d_smem_read = reinterpret_cast<int32_t*>(d_smem_seed_off + (h_nsmem + 1));
-    int32_t* d_fill = d_smem_read + (h_nsmem + 1);
-    uint8_t* d_sel = reinterpret_cast<uint8_t*>(d_fill + (h_nsmem + 1));
+    CK(setup_sel());
     if (n_reads > 0) {
         S.n_launch++, k_compact_smem<<<nblk(n_reads * 32, 256), 256, 0, st>>>(ctx->smem.as<int64_t>(), d_slot_off,
                                                                              ctx->smem_cnt.as<int32_t>(), d_smem_off,
                                                                              n_reads, d_smem);
         CK(cudaGetLastError());
     }
+    } else if (first == kStLocate) {  // the caller's SMEM rows (checked by the entry point)
+        const int64_t o0 = io->smem_off[0];
+        h_nsmem = io->smem_off[n_reads] - o0;
+        CK(setup_sel());
+        std::vector<int64_t> so(n_reads + 1);
+        for (int64_t r = 0; r <= n_reads; ++r) so[r] = io->smem_off[r] - o0;
+        if (h_nsmem > 0) CK(cudaMemcpyAsync(d_smem, io->smem + 6 * o0, h_nsmem * 48, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_smem_off, so.data(), (n_reads + 1) * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    } else {
+        CK(setup_sel());
+    }
+    S.n_smem = h_nsmem;
     tm.mark();  // 1
+    if (last == kStSmem) {  // SMEM rows and per-read offsets to the caller
+        *io->n_rows = h_nsmem;
+        if (h_nsmem > io->rows_cap) return ctx->fail(MSG_EINVAL, "output capacity too small");
+        if (h_nsmem > 0) CK(cudaMemcpyAsync(io->rows, d_smem, h_nsmem * 48, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(io->rows_off, d_smem_off, (n_reads + 1) * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        S.ms_smem = tm.ms(0, 1);
+        S.ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host0).count();
+        return MSG_OK;
+    }
 
     // ---------------- selection (maxNSeed) ----------------
     int32_t* d_hflag = reinterpret_cast<int32_t*>(d_cnt64);  // reuse scratch (n int32)
-    if (n_reads > 0) {
+    if (first == kStLocate && h_nsmem > 0) CK(cudaMemsetAsync(d_sel, 1, h_nsmem, st));  // the caller chose them
+    if (first == kStSmem && n_reads > 0) {
         CK(cudaMemsetAsync(d_ctr + 6, 0, 8, st));
         S.n_launch++, k_select<<<nblk(n_reads, 256), 256, 0, st>>>(d_smem, d_smem_off, n_reads, params->max_nseed, d_sel, d_hflag,
                                                                    d_ctr + 6);
@@ -493,11 +556,15 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             S.host_sorted = (int64_t)flagged.size();
         }
     }
+    int64_t h_nseed_raw = 0;
+    Seed* d_seeds = nullptr;
+    Seed* d_seeds2 = nullptr;
+    int32_t* d_ndedup = reinterpret_cast<int32_t*>(d_cnt64);  // n int32 (flags no longer needed)
+    if (first <= kStLocate) {
     if (h_nsmem > 0) {
         S.n_launch++, k_seed_counts<<<nblk(h_nsmem, 256), 256, 0, st>>>(d_smem, d_sel, h_nsmem, d_smem_seed_cnt);
         CK(cudaGetLastError());
     }
-    int64_t h_nseed_raw = 0;
     CK(offsets(ctx, d_smem_seed_cnt, h_nsmem, d_smem_seed_off, misc, &h_nseed_raw));
     if (n_reads > 0) {
         S.n_launch++, k_gather_off<<<nblk(n_reads + 1, 256), 256, 0, st>>>(d_smem_off, d_smem_seed_off, n_reads, d_read_seed_off);
@@ -508,8 +575,8 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     // ---------------- locate ----------------
     CK(ctx->seeds.ensure((h_nseed_raw + 1) * sizeof(Seed)));
     CK(ctx->seeds2.ensure((h_nseed_raw + 1) * sizeof(Seed)));
-    Seed* d_seeds = ctx->seeds.as<Seed>();
-    Seed* d_seeds2 = ctx->seeds2.as<Seed>();
+    d_seeds = ctx->seeds.as<Seed>();
+    d_seeds2 = ctx->seeds2.as<Seed>();
     S.n_sa = 2 * h_nseed_raw;
     if (h_nseed_raw > 0) {
         CK(cudaMemsetAsync(d_fill, 0, (h_nsmem + 1) * 4, st));
@@ -518,21 +585,94 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
                                     d_seeds, d_status);
         CK(cudaGetLastError());
     }
+    } else {  // the caller's seeds (checked by the entry point), already without redundant ones
+        const int64_t o0 = io->seed_off[0];
+        h_nseed_raw = io->seed_off[n_reads] - o0;
+        CK(ctx->seeds.ensure((h_nseed_raw + 1) * sizeof(Seed)));
+        CK(ctx->seeds2.ensure((h_nseed_raw + 1) * sizeof(Seed)));
+        d_seeds = ctx->seeds.as<Seed>();
+        d_seeds2 = ctx->seeds2.as<Seed>();
+        std::vector<Seed> hs(h_nseed_raw);
+        for (int64_t k = 0; k < h_nseed_raw; ++k) {
+            const int64_t* x = io->seed + 6 * (o0 + k);
+            hs[k].from = (int32_t)x[0]; hs[k].to = (int32_t)x[1]; hs[k].start = x[2]; hs[k].end = x[3];
+            hs[k].tid = (int32_t)x[4]; hs[k].strand = (int32_t)x[5];
+        }
+        std::vector<int64_t> so(n_reads + 1);
+        std::vector<int32_t> nd(n_reads + 1, 0);
+        for (int64_t r = 0; r <= n_reads; ++r) so[r] = io->seed_off[r] - o0;
+        for (int64_t r = 0; r < n_reads; ++r) nd[r] = (int32_t)(so[r + 1] - so[r]);
+        if (h_nseed_raw > 0) CK(cudaMemcpyAsync(d_seeds, hs.data(), h_nseed_raw * sizeof(Seed), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_read_seed_off, so.data(), (n_reads + 1) * 8, cudaMemcpyHostToDevice, st));
+        if (n_reads > 0) CK(cudaMemcpyAsync(d_ndedup, nd.data(), n_reads * 4, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
     tm.mark();  // 2
 
     // ---------------- redundant-seed removal ----------------
-    int32_t* d_ndedup = reinterpret_cast<int32_t*>(d_cnt64);  // n int32 (flags no longer needed)
-    if (n_reads > 0) {
+    if (first <= kStLocate && n_reads > 0) {
         S.n_launch++, k_dedup<<<nblk(n_reads * 32, 128), 128, 0, st>>>(d_read_seed_off, n_reads, d_seeds, d_seeds2, d_seeds, d_ndedup);
         CK(cudaGetLastError());
     }
+    // per read, its seeds after removeRedundant as rows of 6 int64 (rows
+    // beyond cap are counted, not written)
+    auto seeds_to_host = [&](int64_t* rows, int64_t cap, int64_t* roff, int64_t* total) -> cudaError_t {
+        std::vector<int64_t> rso(n_reads + 1);
+        std::vector<int32_t> nd(n_reads);
+        std::vector<Seed> hs(h_nseed_raw);
+        cudaError_t e = cudaMemcpyAsync(rso.data(), d_read_seed_off, (n_reads + 1) * 8, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && n_reads > 0) e = cudaMemcpyAsync(nd.data(), d_ndedup, n_reads * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && h_nseed_raw > 0)
+            e = cudaMemcpyAsync(hs.data(), d_seeds, h_nseed_raw * sizeof(Seed), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return e;
+        int64_t k = 0;
+        for (int64_t r = 0; r < n_reads; ++r) {
+            if (roff) roff[r] = k;
+            for (int32_t j = 0; j < nd[r]; ++j, ++k) {
+                if (rows && k < cap) {
+                    const Seed& x = hs[rso[r] + j];
+                    int64_t* o = rows + 6 * k;
+                    o[0] = x.from; o[1] = x.to; o[2] = x.start; o[3] = x.end; o[4] = x.tid; o[5] = x.strand;
+                }
+            }
+        }
+        if (roff) roff[n_reads] = k;
+        *total = k;
+        return cudaSuccess;
+    };
+    if (last == kStLocate) {
+        int64_t tot = 0;
+        CK(seeds_to_host(io->rows, io->rows_cap, io->rows_off, &tot));
+        *io->n_rows = tot;
+        if (tot > io->rows_cap) return ctx->fail(MSG_EINVAL, "output capacity too small");
+        S.n_seed = h_nseed_raw;
+        S.ms_smem = tm.ms(0, 1);
+        S.ms_locate = tm.ms(1, 2);
+        S.ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host0).count();
+        return MSG_OK;
+    }
 
     // ---------------- chains ----------------
+    int64_t h_nchain = 0, h_nidx = 0;
+    int64_t* d_cidx_off = nullptr;
+    int64_t* d_cidx = nullptr;
+    int32_t* d_clen = nullptr;
+    int32_t* d_cread = nullptr;
+    auto setup_chainidx = [&]() -> cudaError_t {
+        const cudaError_t e = ctx->chainidx.ensure((h_nchain + 1) * (8 + 4 + 4) + (h_nidx + 1) * 8 + 64);
+        if (e != cudaSuccess) return e;
+        d_cidx_off = ctx->chainidx.as<int64_t>();
+        d_cidx = d_cidx_off + (h_nchain + 1);
+        d_clen = reinterpret_cast<int32_t*>(d_cidx + (h_nidx + 1));
+        d_cread = d_clen + (h_nchain + 1);
+        return cudaSuccess;
+    };
+    if (first <= kStChain) {
     CK(ctx->chains.ensure((h_nseed_raw + 1) * (1 + 4 + 4) + 64));
     uint8_t* d_vis = ctx->chains.as<uint8_t>();
     int32_t* d_stki = reinterpret_cast<int32_t*>(d_vis + ((h_nseed_raw + 1 + 15) / 16) * 16);
     int32_t* d_stkj = d_stki + (h_nseed_raw + 1);
-    int64_t h_nchain = 0, h_nidx = 0;
     if (n_reads > 0) {
         S.n_launch++, k_chain<<<nblk(n_reads, 128), 128, 0, st>>>(d_read_seed_off, d_ndedup, d_rlen, n_reads, d_seeds, d_vis, d_stki,
                                                    d_stkj, 0, d_nchain, d_nidx, nullptr, nullptr, nullptr, nullptr,
@@ -541,19 +681,72 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     }
     CK(offsets(ctx, d_nchain, n_reads, d_chain_off, misc, &h_nchain));
     CK(offsets(ctx, d_nidx, n_reads, d_idx_off, misc, &h_nidx));
-    S.n_chain = h_nchain;
-    CK(ctx->chainidx.ensure((h_nchain + 1) * (8 + 4 + 4) + (h_nidx + 1) * 8 + 64));
-    int64_t* d_cidx_off = ctx->chainidx.as<int64_t>();
-    int64_t* d_cidx = d_cidx_off + (h_nchain + 1);
-    int32_t* d_clen = reinterpret_cast<int32_t*>(d_cidx + (h_nidx + 1));
-    int32_t* d_cread = d_clen + (h_nchain + 1);
+    CK(setup_chainidx());
     if (n_reads > 0 && h_nchain > 0) {
         S.n_launch++, k_chain<<<nblk(n_reads, 128), 128, 0, st>>>(d_read_seed_off, d_ndedup, d_rlen, n_reads, d_seeds, d_vis, d_stki,
                                                    d_stkj, 1, nullptr, nullptr, d_chain_off, d_idx_off, d_cidx_off,
                                                    d_clen, d_cread, d_cidx);
         CK(cudaGetLastError());
     }
+    } else {  // the caller's chains (checked by the entry point): seed indices local to each read
+        const int64_t c0 = io->read_chain_off[0];
+        h_nchain = io->read_chain_off[n_reads] - c0;
+        const int64_t i0 = io->chain_seed_off[c0];
+        h_nidx = io->chain_seed_off[c0 + h_nchain] - i0;
+        CK(setup_chainidx());
+        std::vector<int64_t> coff(n_reads + 1), cio(h_nchain + 1), cix(h_nidx + 1);
+        std::vector<int32_t> cl(h_nchain + 1), cr(h_nchain + 1);
+        const int64_t so0 = io->seed_off[0];
+        for (int64_t r = 0; r <= n_reads; ++r) coff[r] = io->read_chain_off[r] - c0;
+        for (int64_t r = 0; r < n_reads; ++r) {
+            for (int64_t c = coff[r]; c < coff[r + 1]; ++c) {
+                const int64_t a = io->chain_seed_off[c0 + c] - i0, b = io->chain_seed_off[c0 + c + 1] - i0;
+                cio[c] = a;
+                cl[c] = (int32_t)(b - a);
+                cr[c] = (int32_t)r;
+                for (int64_t k = a; k < b; ++k) cix[k] = (io->seed_off[r] - so0) + io->chain_seed[i0 + k];
+            }
+        }
+        CK(cudaMemcpyAsync(d_chain_off, coff.data(), (n_reads + 1) * 8, cudaMemcpyHostToDevice, st));
+        if (h_nchain > 0) {
+            CK(cudaMemcpyAsync(d_cidx_off, cio.data(), h_nchain * 8, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d_clen, cl.data(), h_nchain * 4, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d_cread, cr.data(), h_nchain * 4, cudaMemcpyHostToDevice, st));
+        }
+        if (h_nidx > 0) CK(cudaMemcpyAsync(d_cidx, cix.data(), h_nidx * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    S.n_chain = h_nchain;
     tm.mark();  // 3
+    if (last == kStChain) {  // chains as seed indices within each read's seed list
+        *io->o_n_chain = h_nchain;
+        *io->o_n_chain_seed = h_nidx;
+        if (h_nchain > io->o_chain_cap || h_nidx > io->o_chain_seed_cap)
+            return ctx->fail(MSG_EINVAL, "output capacity too small");
+        std::vector<int64_t> cio(h_nchain + 1), cix(h_nidx + 1), rso(n_reads + 1);
+        std::vector<int32_t> cl(h_nchain + 1), cr(h_nchain + 1);
+        CK(cudaMemcpyAsync(io->o_read_chain_off, d_chain_off, (n_reads + 1) * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(rso.data(), d_read_seed_off, (n_reads + 1) * 8, cudaMemcpyDeviceToHost, st));
+        if (h_nchain > 0) {
+            CK(cudaMemcpyAsync(cio.data(), d_cidx_off, h_nchain * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(cl.data(), d_clen, h_nchain * 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(cr.data(), d_cread, h_nchain * 4, cudaMemcpyDeviceToHost, st));
+        }
+        if (h_nidx > 0) CK(cudaMemcpyAsync(cix.data(), d_cidx, h_nidx * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        int64_t k = 0;
+        for (int64_t c = 0; c < h_nchain; ++c) {
+            io->o_chain_seed_off[c] = k;
+            for (int32_t j = 0; j < cl[c]; ++j, ++k) io->o_chain_seed[k] = (int32_t)(cix[cio[c] + j] - rso[cr[c]]);
+        }
+        io->o_chain_seed_off[h_nchain] = k;
+        S.n_seed = h_nseed_raw;
+        S.ms_smem = tm.ms(0, 1);
+        S.ms_locate = tm.ms(1, 2);
+        S.ms_chain = tm.ms(2, 3);
+        S.ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host0).count();
+        return MSG_OK;
+    }
 
     // ---------------- DP ----------------
     if (h_nchain >= INT32_MAX) return ctx->fail(MSG_EINVAL, "too many chains in one batch");
@@ -811,25 +1004,8 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             CK(cudaMemcpyAsync(dump->smem, d_smem, h_nsmem * 48, cudaMemcpyDeviceToHost, st));
         if (dump->smem_off) CK(cudaMemcpyAsync(dump->smem_off, d_smem_off, (n_reads + 1) * 8, cudaMemcpyDeviceToHost, st));
         // dense seeds per read after removeRedundant
-        std::vector<int64_t> rso(n_reads + 1);
-        std::vector<int32_t> nd(n_reads);
-        CK(cudaMemcpyAsync(rso.data(), d_read_seed_off, (n_reads + 1) * 8, cudaMemcpyDeviceToHost, st));
-        if (n_reads > 0) CK(cudaMemcpyAsync(nd.data(), d_ndedup, n_reads * 4, cudaMemcpyDeviceToHost, st));
-        std::vector<Seed> hs(h_nseed_raw);
-        if (h_nseed_raw > 0) CK(cudaMemcpyAsync(hs.data(), d_seeds, h_nseed_raw * sizeof(Seed), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
         int64_t k = 0;
-        for (int64_t r = 0; r < n_reads; ++r) {
-            if (dump->seed_off) dump->seed_off[r] = k;
-            for (int32_t j = 0; j < nd[r]; ++j, ++k) {
-                if (dump->seed && k < dump->seed_cap) {
-                    const Seed& s = hs[rso[r] + j];
-                    int64_t* o = dump->seed + 6 * k;
-                    o[0] = s.from; o[1] = s.to; o[2] = s.start; o[3] = s.end; o[4] = s.tid; o[5] = s.strand;
-                }
-            }
-        }
-        if (dump->seed_off) dump->seed_off[n_reads] = k;
+        CK(seeds_to_host(dump->seed, dump->seed_cap, dump->seed_off, &k));
         dump->n_seed = k;
     }
     CK(cudaStreamSynchronize(st));
@@ -975,6 +1151,156 @@ extern "C" int msg_map_batches(msg_ctx* ctx, int64_t n_batches, const msg_read_b
 #undef CK
     if (status != MSG_OK) return ctx->fail(status, "output capacity too small");
     return MSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The mapping task one stage at a time (the reference's operator boundaries).
+// The caller's arrays are checked on the host first so that no kernel indexes
+// memory through them: offsets ascend, SMEM rows address suffix-array rows of
+// the index, seeds lie in their read and chromosome, chains list seeds of
+// their own read in ascending, non-overlapping order.
+// ---------------------------------------------------------------------------
+namespace {
+bool offsets_ok(const int64_t* off, int64_t n) {
+    if (!off || off[0] < 0) return false;
+    for (int64_t i = 0; i < n; ++i)
+        if (off[i + 1] < off[i]) return false;
+    return true;
+}
+
+int64_t read_len_of(const msg_read_batch* reads, int64_t r) { return reads->off[r + 1] - reads->off[r]; }
+
+bool reads_ok(const msg_read_batch* reads) {
+    const int64_t n = reads->n_reads;
+    return n >= 0 && n <= INT32_MAX && (n == 0 || (reads->seq && offsets_ok(reads->off, n)));
+}
+
+bool seeds_ok(const msg_ctx* ctx, const msg_read_batch* reads, const int64_t* seed, const int64_t* seed_off) {
+    const int64_t n = reads->n_reads;
+    if (!offsets_ok(seed_off, n) || (seed_off[n] > seed_off[0] && !seed)) return false;
+    const int64_t* chr_len = ctx->idx.chr_len_host.data();
+    const int64_t nc = (int64_t)ctx->idx.chr_len_host.size();
+    for (int64_t r = 0; r < n; ++r) {
+        const int64_t L = read_len_of(reads, r);
+        for (int64_t k = seed_off[r]; k < seed_off[r + 1]; ++k) {
+            const int64_t* x = seed + 6 * k;  // from, to, start, end, tid, strand
+            if (!(0 <= x[0] && x[0] < x[1] && x[1] <= L && x[4] >= 0 && x[4] < nc && (x[5] == 1 || x[5] == 2)))
+                return false;
+            if (!(0 <= x[2] && x[2] < x[3] && x[3] <= chr_len[x[4]] && x[3] - x[2] == x[1] - x[0])) return false;
+        }
+    }
+    return true;
+}
+
+bool chains_ok(const msg_ctx* ctx, const msg_read_batch* reads, const int64_t* seed, const int64_t* seed_off,
+               const int32_t* chain_seed, const int64_t* chain_seed_off, const int64_t* read_chain_off) {
+    const int64_t n = reads->n_reads;
+    if (!seeds_ok(ctx, reads, seed, seed_off) || !offsets_ok(read_chain_off, n) || !chain_seed_off) return false;
+    const int64_t c0 = read_chain_off[0], nch = read_chain_off[n] - c0;
+    if (nch >= INT32_MAX || !offsets_ok(chain_seed_off + c0, nch)) return false;
+    if (chain_seed_off[c0 + nch] > chain_seed_off[c0] && !chain_seed) return false;
+    for (int64_t r = 0; r < n; ++r) {
+        const int64_t ns = seed_off[r + 1] - seed_off[r];
+        for (int64_t c = read_chain_off[r]; c < read_chain_off[r + 1]; ++c) {
+            const int64_t a = chain_seed_off[c], b = chain_seed_off[c + 1];
+            if (b <= a) return false;  // a chain holds at least one seed
+            for (int64_t k = a; k < b; ++k) {
+                if (chain_seed[k] < 0 || chain_seed[k] >= ns) return false;
+                if (k > a) {
+                    const int64_t* l = seed + 6 * (seed_off[r] + chain_seed[k - 1]);
+                    const int64_t* q = seed + 6 * (seed_off[r] + chain_seed[k]);
+                    if (!(chain_seed[k] > chain_seed[k - 1] && l[1] <= q[0] && l[3] <= q[2] && l[4] == q[4] &&
+                          l[5] == q[5]))
+                        return false;
+                }
+            }
+        }
+    }
+    return true;
+}
+
+int stage_call(msg_ctx* ctx, const msg_read_batch* reads, const msg_map_params* params, StageIO& io,
+               msg_aln_out* out) {
+    msg::DeviceGuard dg_(ctx->device);
+    if (!dg_.ok) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
+    const int rc = upload_reads(ctx, reads);
+    if (rc != MSG_OK) return rc;
+    msg_map_params dflt;
+    msg_map_params_default(&dflt);
+    msg_aln_out none{};
+    return map_impl(ctx, ctx->reads.as<uint8_t>(), ctx->offs.as<int64_t>(), reads->n_reads, params ? params : &dflt,
+                    out ? out : &none, nullptr, nullptr, &io);
+}
+}  // namespace
+
+extern "C" int msg_seed_batch(msg_ctx* ctx, const msg_read_batch* reads, const msg_map_params* params,
+                              int64_t* smem, int64_t smem_cap, int64_t* smem_off, int64_t* n_smem) {
+    if (!ctx || !reads || !params || !smem_off || !n_smem || smem_cap < 0 || (smem_cap > 0 && !smem))
+        return MSG_EINVAL;
+    if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
+    if (!reads_ok(reads)) return MSG_EINVAL;
+    StageIO io;
+    io.first = kStSmem; io.last = kStSmem;
+    io.rows = smem; io.rows_cap = smem_cap; io.rows_off = smem_off; io.n_rows = n_smem;
+    return stage_call(ctx, reads, params, io, nullptr);
+}
+
+extern "C" int msg_locate_batch(msg_ctx* ctx, const msg_read_batch* reads, const int64_t* smem,
+                                const int64_t* smem_off, int64_t* seed, int64_t seed_cap, int64_t* seed_off,
+                                int64_t* n_seed) {
+    if (!ctx || !reads || !seed_off || !n_seed || seed_cap < 0 || (seed_cap > 0 && !seed)) return MSG_EINVAL;
+    if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
+    if (!reads_ok(reads)) return MSG_EINVAL;
+    const int64_t n = reads->n_reads;
+    if (!offsets_ok(smem_off, n) || (smem_off[n] > smem_off[0] && !smem)) return ctx->fail(MSG_EINVAL, "bad SMEM offsets");
+    const int64_t nbwt = ctx->idx.dev.n;
+    for (int64_t r = 0; r < n; ++r) {
+        const int64_t L = read_len_of(reads, r);
+        for (int64_t k = smem_off[r]; k < smem_off[r + 1]; ++k) {
+            const int64_t* x = smem + 6 * k;  // from, to, fwdStart, revStart, size, logP
+            if (!(0 <= x[0] && x[0] < x[1] && x[1] <= L && x[4] >= 0 && x[2] >= 0 && x[3] >= 0 &&
+                  x[4] <= nbwt && x[2] <= nbwt - x[4] && x[3] <= nbwt - x[4]))
+                return ctx->fail(MSG_EINVAL, "an SMEM row lies outside its read or the index");
+        }
+    }
+    StageIO io;
+    io.first = kStLocate; io.last = kStLocate;
+    io.smem = smem; io.smem_off = smem_off;
+    io.rows = seed; io.rows_cap = seed_cap; io.rows_off = seed_off; io.n_rows = n_seed;
+    return stage_call(ctx, reads, nullptr, io, nullptr);
+}
+
+extern "C" int msg_chain_batch(msg_ctx* ctx, const msg_read_batch* reads, const int64_t* seed, const int64_t* seed_off,
+                               int32_t* chain_seed, int64_t chain_seed_cap, int64_t* chain_seed_off,
+                               int64_t chain_cap, int64_t* read_chain_off, int64_t* n_chain, int64_t* n_chain_seed) {
+    if (!ctx || !reads || !read_chain_off || !n_chain || !n_chain_seed || chain_cap < 0 || chain_seed_cap < 0 ||
+        !chain_seed_off || (chain_seed_cap > 0 && !chain_seed))
+        return MSG_EINVAL;
+    if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
+    if (!reads_ok(reads)) return MSG_EINVAL;
+    if (!seeds_ok(ctx, reads, seed, seed_off)) return ctx->fail(MSG_EINVAL, "a seed lies outside its read or chromosome");
+    StageIO io;
+    io.first = kStChain; io.last = kStChain;
+    io.seed = seed; io.seed_off = seed_off;
+    io.o_chain_seed = chain_seed; io.o_chain_seed_cap = chain_seed_cap; io.o_chain_seed_off = chain_seed_off;
+    io.o_chain_cap = chain_cap; io.o_read_chain_off = read_chain_off; io.o_n_chain = n_chain;
+    io.o_n_chain_seed = n_chain_seed;
+    return stage_call(ctx, reads, nullptr, io, nullptr);
+}
+
+extern "C" int msg_align_batch(msg_ctx* ctx, const msg_read_batch* reads, const int64_t* seed, const int64_t* seed_off,
+                               const int32_t* chain_seed, const int64_t* chain_seed_off, const int64_t* read_chain_off,
+                               const msg_map_params* params, msg_aln_out* out) {
+    if (!ctx || !reads || !params || !out) return MSG_EINVAL;
+    if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
+    if (!reads_ok(reads)) return MSG_EINVAL;
+    if (!chains_ok(ctx, reads, seed, seed_off, chain_seed, chain_seed_off, read_chain_off))
+        return ctx->fail(MSG_EINVAL, "a chain or seed does not fit its read, chromosome or seed list");
+    StageIO io;
+    io.first = kStAlign; io.last = kStAlign;
+    io.seed = seed; io.seed_off = seed_off;
+    io.chain_seed = chain_seed; io.chain_seed_off = chain_seed_off; io.read_chain_off = read_chain_off;
+    return stage_call(ctx, reads, params, io, out);
 }
 
 // ---------------------------------------------------------------------------

@@ -28,7 +28,8 @@ assert ALN_DTYPE.itemsize == 88
 # symbols of the C ABI, in include/msg_b200.h order
 EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy", "msg_index_load", "msg_db_read",
            "msg_db_views", "msg_db_free", "msg_index_bytes",
-           "msg_map_params_default", "msg_map_batch", "msg_map_batches", "msg_map_batch_device", "msg_last_stats",
+           "msg_map_params_default", "msg_map_batch", "msg_map_batches", "msg_seed_batch", "msg_locate_batch",
+           "msg_chain_batch", "msg_align_batch", "msg_map_batch_device", "msg_last_stats",
            "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_ctx_set_dp_shape", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
            "msg_band_train", "msg_band_grad", "msg_tail_params_default", "msg_tail_batch", "msg_pair_params_default", "msg_tail_pe_batch",
            "msg_fastq_parse", "msg_fastq_format", "msg_clean_format", "msg_sam_format",
@@ -146,6 +147,13 @@ def load_library(path: str = LIB_PATH):
     L.msg_map_batch.argtypes = [C.c_void_p, C.POINTER(ReadBatch), C.POINTER(MapParams), C.POINTER(AlnOut),
                                 C.POINTER(StageDump)]
     L.msg_map_batch_device.argtypes = L.msg_map_batch.argtypes
+    i32p_ = C.POINTER(C.c_int32)
+    L.msg_seed_batch.argtypes = [C.c_void_p, C.POINTER(ReadBatch), C.POINTER(MapParams), i64p, C.c_int64, i64p, i64p]
+    L.msg_locate_batch.argtypes = [C.c_void_p, C.POINTER(ReadBatch), i64p, i64p, i64p, C.c_int64, i64p, i64p]
+    L.msg_chain_batch.argtypes = [C.c_void_p, C.POINTER(ReadBatch), i64p, i64p, i32p_, C.c_int64, i64p, C.c_int64,
+                                  i64p, i64p, i64p]
+    L.msg_align_batch.argtypes = [C.c_void_p, C.POINTER(ReadBatch), i64p, i64p, i32p_, i64p, i64p,
+                                  C.POINTER(MapParams), C.POINTER(AlnOut)]
     L.msg_map_batches.argtypes = [C.c_void_p, C.c_int64, C.POINTER(ReadBatch), C.POINTER(MapParams),
                                   C.POINTER(AlnOut)]
     L.msg_last_stats.argtypes = [C.c_void_p, C.POINTER(MapStats)]
@@ -469,6 +477,93 @@ class Context:
                     raise MsgError(MSG_EINVAL, "dump capacity")
                 res.update(smem=sm[:d.n_smem].copy(), smem_off=so, seed=sd[:d.n_seed].copy(), seed_off=sdo)
             return res
+
+    # ---- the stages of map() one call each (msg_seed/locate/chain/align_batch) ----
+    @staticmethod
+    def _batch(seq, off):
+        seq = np.ascontiguousarray(seq, dtype=np.uint8)
+        off = np.ascontiguousarray(off, dtype=np.int64)
+        return seq, off, ReadBatch(len(off) - 1, _p(seq, u8p), _p(off, i64p))
+
+    def seed_batch(self, seq, off, params: MapParams | None = None):
+        """SMEM rows (n, 6) in emission order and per-read offsets."""
+        params = params or default_params()
+        seq, off, b = self._batch(seq, off)
+        n = len(off) - 1
+        cap = 8 * n + 16
+        while True:
+            rows = np.zeros((cap, 6), dtype=np.int64)
+            roff = np.zeros(n + 1, dtype=np.int64)
+            cnt = C.c_int64(0)
+            rc = self.lib.msg_seed_batch(self.h, C.byref(b), C.byref(params), _p(rows, i64p), cap, _p(roff, i64p),
+                                         C.byref(cnt))
+            if rc == MSG_EINVAL and cnt.value > cap:
+                cap = cnt.value
+                continue
+            self._check(rc, "msg_seed_batch")
+            return rows[:cnt.value].copy(), roff
+
+    def locate_batch(self, seq, off, smem, smem_off):
+        """Seeds (n, 6) of the given SMEM rows after removeRedundant, per-read offsets."""
+        seq, off, b = self._batch(seq, off)
+        smem = np.ascontiguousarray(smem, dtype=np.int64).reshape(-1, 6)
+        smem_off = np.ascontiguousarray(smem_off, dtype=np.int64)
+        n = len(off) - 1
+        cap = int(smem[:, 4].sum()) + 16 if len(smem) else 16
+        rows = np.zeros((cap, 6), dtype=np.int64)
+        roff = np.zeros(n + 1, dtype=np.int64)
+        cnt = C.c_int64(0)
+        self._check(self.lib.msg_locate_batch(self.h, C.byref(b), _p(smem, i64p), _p(smem_off, i64p), _p(rows, i64p),
+                                              cap, _p(roff, i64p), C.byref(cnt)), "msg_locate_batch")
+        return rows[:cnt.value].copy(), roff
+
+    def chain_batch(self, seq, off, seed, seed_off):
+        """Chains: seed indices within each read's seed rows, per-chain and per-read offsets."""
+        seq, off, b = self._batch(seq, off)
+        seed = np.ascontiguousarray(seed, dtype=np.int64).reshape(-1, 6)
+        seed_off = np.ascontiguousarray(seed_off, dtype=np.int64)
+        n = len(off) - 1
+        ccap, scap = len(seed) + 16, 4 * len(seed) + 16
+        while True:
+            cs = np.zeros(scap, dtype=np.int32)
+            cso = np.zeros(ccap + 1, dtype=np.int64)
+            rco = np.zeros(n + 1, dtype=np.int64)
+            nc, ns = C.c_int64(0), C.c_int64(0)
+            rc = self.lib.msg_chain_batch(self.h, C.byref(b), _p(seed, i64p), _p(seed_off, i64p),
+                                          cs.ctypes.data_as(C.POINTER(C.c_int32)), scap, _p(cso, i64p), ccap,
+                                          _p(rco, i64p), C.byref(nc), C.byref(ns))
+            if rc == MSG_EINVAL and (nc.value > ccap or ns.value > scap):
+                ccap, scap = max(ccap, nc.value), max(scap, ns.value)
+                continue
+            self._check(rc, "msg_chain_batch")
+            return cs[:ns.value].copy(), cso[:nc.value + 1].copy(), rco
+
+    def align_batch(self, seq, off, seed, seed_off, chain_seed, chain_seed_off, read_chain_off,
+                    params: MapParams | None = None):
+        """Records of the given chains, as map() returns them."""
+        params = params or default_params()
+        seq, off, b = self._batch(seq, off)
+        seed = np.ascontiguousarray(seed, dtype=np.int64).reshape(-1, 6)
+        seed_off = np.ascontiguousarray(seed_off, dtype=np.int64)
+        chain_seed = np.ascontiguousarray(chain_seed, dtype=np.int32)
+        chain_seed_off = np.ascontiguousarray(chain_seed_off, dtype=np.int64)
+        read_chain_off = np.ascontiguousarray(read_chain_off, dtype=np.int64)
+        n = len(off) - 1
+        aln_cap = max(16, len(chain_seed_off))
+        cigar_cap = 16 * aln_cap + 64
+        while True:
+            aln = np.zeros(aln_cap, dtype=ALN_DTYPE)
+            cig = np.zeros(cigar_cap, dtype=np.uint32)
+            roff = np.zeros(n + 1, dtype=np.int64)
+            out = AlnOut(aln_cap, aln.ctypes.data, cigar_cap, cig.ctypes.data, 0, 0, _p(roff, i64p))
+            rc = self.lib.msg_align_batch(self.h, C.byref(b), _p(seed, i64p), _p(seed_off, i64p),
+                                          chain_seed.ctypes.data_as(C.POINTER(C.c_int32)), _p(chain_seed_off, i64p),
+                                          _p(read_chain_off, i64p), C.byref(params), C.byref(out))
+            if rc == MSG_EINVAL and (out.n_aln > aln_cap or out.n_cigar > cigar_cap):
+                aln_cap, cigar_cap = max(aln_cap, out.n_aln) * 2, max(cigar_cap, out.n_cigar) * 2
+                continue
+            self._check(rc, "msg_align_batch")
+            return dict(aln=aln[:out.n_aln].copy(), cigar=cig[:out.n_cigar].copy(), read_aln_off=roff)
 
     def stream_handle(self) -> int:
         h = C.c_void_p()
