@@ -247,3 +247,33 @@ def test_gpu_records_through_library_pe_tail_give_reference_pairs():
                 assert got == full
     finally:
         ctx.close()
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_small_config_sam_matches_reference():
+    """The small configuration at its exact shape: 4 genomes of 500 kbp
+    (i.i.d. uniform bases), 10,000 single-end 150 bp reads (1% substitutions,
+    0.1% indels of 1-3 bp, Phred 20-40), default scores, GLOBAL mode, -k 1.
+    The GPU records through the reference's own tail and through the
+    library's tail give the SAM fields of the reference's whole single-end
+    path, read for read."""
+    from msgseqtk_b200 import index_build
+    g = synth.small_genomes(seed=101, n_genomes=4, length=500_000)
+    rs = synth.sample_reads(g, 10_000, seed=102)
+    seq = rs.seqs.astype(np.uint8)
+    off = rs.offs.astype(np.int64)
+    qual = np.concatenate([rs.qual(i) for i in range(len(rs))]).astype(np.uint8)
+    ref = Reference(g)
+    view = index_build.build_view(g)
+    ctx = lib.Context(0)
+    try:
+        ctx.load_index(view)
+        res = ctx.map(seq, off, lib.default_params(min_score_rate=0.65))
+        exp = ref.sam_batch(seq, qual, off, max_report=1)
+        got = ref.sam_from_records(seq, qual, off, res["aln"], res["cigar"], res["read_aln_off"], max_report=1)
+        assert got == exp
+        _check_tail(view, ref, seq, qual, off, res["aln"], res["cigar"], res["read_aln_off"], 0.65, 1)
+        assert len(res["aln"]) > 9_000
+    finally:
+        ctx.close()
