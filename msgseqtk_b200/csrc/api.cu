@@ -35,6 +35,11 @@ extern "C" int msg_ctx_create(int device, msg_ctx** out) {
     c->device = device;
     c->num_sms = prop.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return MSG_ECUDA; }
+    if (cudaHostAlloc(reinterpret_cast<void**>(&c->hpin), 64 * sizeof(int64_t), cudaHostAllocDefault) != cudaSuccess) {
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return MSG_ENOMEM;
+    }
     for (auto& e : c->ev) cudaEventCreate(&e);
     *out = c;
     return MSG_OK;
@@ -48,6 +53,7 @@ extern "C" void msg_ctx_destroy(msg_ctx* c) {
     c->buffers_free();
     for (auto& e : c->ev) cudaEventDestroy(e);
     cudaStreamDestroy(c->stream);
+    if (c->hpin) cudaFreeHost(c->hpin);
     delete c;
 }
 

@@ -87,14 +87,21 @@ cudaError_t scan_excl(msg_ctx* ctx, const T* in, T* out, int64_t n, DevBuf& tmpb
     return cub::DeviceScan::ExclusiveSum(tmpb.p, tb, in, out, n, ctx->stream);
 }
 
-// exclusive scan of n values into n+1 offsets; returns the total
+// exclusive scan of n values into n+1 offsets, the total copied to host
+// memory `total` (pinned: the copy stays asynchronous) without waiting
 template <typename T>
-cudaError_t offsets(msg_ctx* ctx, T* cnt_with_room, int64_t n, T* off, DevBuf& tmpb, T* total) {
+cudaError_t offsets_async(msg_ctx* ctx, T* cnt_with_room, int64_t n, T* off, DevBuf& tmpb, T* total) {
     cudaError_t e = cudaMemsetAsync(cnt_with_room + n, 0, sizeof(T), ctx->stream);
     if (e != cudaSuccess) return e;
     e = scan_excl(ctx, cnt_with_room, off, n + 1, tmpb);
     if (e != cudaSuccess) return e;
-    e = cudaMemcpyAsync(total, off + n, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream);
+    return cudaMemcpyAsync(total, off + n, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream);
+}
+
+// exclusive scan of n values into n+1 offsets; returns the total
+template <typename T>
+cudaError_t offsets(msg_ctx* ctx, T* cnt_with_room, int64_t n, T* off, DevBuf& tmpb, T* total) {
+    cudaError_t e = offsets_async(ctx, cnt_with_room, n, off, tmpb, total);
     if (e != cudaSuccess) return e;
     return cudaStreamSynchronize(ctx->stream);
 }
@@ -466,14 +473,11 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             cap = std::max<int64_t>(cap, ((int64_t)cnt[r] * kSlotBases + per - 1) / per);
         }
     }
-    {
-        unsigned long long e = 0;
-        CK(cudaMemcpyAsync(&e, d_ctr + 1, 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        S.n_ext = (int64_t)e;
-    }
+    // the extension count arrives with the next synchronisation
+    CK(cudaMemcpyAsync(ctx->hpin + 8, d_ctr + 1, 8, cudaMemcpyDeviceToHost, st));
     if (n_reads > 0) S.n_launch++, k_i32_to_i64<<<nblk(n_reads, 256), 256, 0, st>>>(ctx->smem_cnt.as<int32_t>(), d_cnt64, n_reads);
     CK(offsets(ctx, d_cnt64, n_reads, d_smem_off, misc, &h_nsmem));
+    S.n_ext = ctx->hpin[8];
     CK(setup_sel());
     if (n_reads > 0) {
         S.n_launch++, k_compact_smem<<<nblk(n_reads * 32, 256), 256, 0, st>>>(ctx->smem.as<int64_t>(), d_slot_off,
@@ -679,8 +683,11 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
                                                    nullptr, nullptr);
         CK(cudaGetLastError());
     }
-    CK(offsets(ctx, d_nchain, n_reads, d_chain_off, misc, &h_nchain));
-    CK(offsets(ctx, d_nidx, n_reads, d_idx_off, misc, &h_nidx));
+    CK(offsets_async(ctx, d_nchain, n_reads, d_chain_off, misc, ctx->hpin));
+    CK(offsets_async(ctx, d_nidx, n_reads, d_idx_off, misc, ctx->hpin + 1));
+    CK(cudaStreamSynchronize(st));
+    h_nchain = ctx->hpin[0];
+    h_nidx = ctx->hpin[1];
     CK(setup_chainidx());
     if (n_reads > 0 && h_nchain > 0) {
         S.n_launch++, k_chain<<<nblk(n_reads, 128), 128, 0, st>>>(d_read_seed_off, d_ndedup, d_rlen, n_reads, d_seeds, d_vis, d_stki,
@@ -796,8 +803,11 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         CK(cub::DeviceReduce::Sum(misc.p, tb, d_dpcells, d_ncig, h_nchain, st));
         CK(cudaMemcpyAsync(&S.dp_cells, d_ncig, 8, cudaMemcpyDeviceToHost, st));
     }
-    CK(offsets(ctx, d_cells, h_nchain, d_rect_off, misc, &h_cells));  // d_cells holds bytes per chain
-    CK(offsets(ctx, d_pcap, h_nchain, d_path_off, misc, &h_pathtot));
+    CK(offsets_async(ctx, d_cells, h_nchain, d_rect_off, misc, ctx->hpin + 2));  // d_cells holds bytes per chain
+    CK(offsets_async(ctx, d_pcap, h_nchain, d_path_off, misc, ctx->hpin + 3));
+    CK(cudaStreamSynchronize(st));
+    h_cells = ctx->hpin[2];
+    h_pathtot = ctx->hpin[3];
     const int64_t aux_bytes = ((2 * (h_nidx + 1) + h_nchain + 1) * sizeof(int32_t) + 15) / 16 * 16;
     // Rectangle storage of at most scratch_limit bytes at a time: when the
     // batch needs more (long reads with large flanks), the DP runs over
@@ -820,8 +830,8 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         }
     }
     CK(ctx->scratch.ensure(rect_cap + 64 + aux_bytes + (2 * h_nidx + h_nchain + 1) * sizeof(int4)));
-    std::vector<int64_t> h_rect_off(bounds.size());
-    for (size_t b = 0; b < bounds.size(); ++b)
+    std::vector<int64_t> h_rect_off(bounds.size(), 0);  // bounds[0] = 0 starts at offset 0
+    for (size_t b = 1; b < bounds.size(); ++b)
         CK(cudaMemcpy(&h_rect_off[b], d_rect_off + bounds[b], 8, cudaMemcpyDeviceToHost));
     const int64_t P16 = ((h_pathtot + 1 + 15) / 16) * 16;
     CK(ctx->path.ensure(P16 + (h_nchain + 1) * 4 + 64));

@@ -846,10 +846,21 @@ struct ChainCtx {
             for (int c = 0; c < 3 * C; ++c) g.lastrow[c] = NEG;
             for (int c = 0; c < 3 * R; ++c) g.lastcol[c] = NEG;
         }
+        // Boundary cells. The 5' rectangle's (m == 0) are those of the
+        // initialised matrices, no region having been written before it
+        // (initNW/initSW, Alignment.h:599-613): row 0 holds M = 0; column 0
+        // holds I = -gapPenalty(i) in NW and M = 0 in SW; the rest is -inf.
+        const int32_t go = pp.gap_o, ge = pp.gap_e;
+        const bool nw = pp.mode == 0;
+        auto bnd = [&](int64_t i, int64_t j) -> int3 {
+            if (m != 0) return MID(i, j, m);
+            if (i == 0) return make_int3(0, (nw && j == 0) ? 0 : NEG, NEG);
+            return make_int3(nw ? NEG : 0, nw ? -(go + ge * (int32_t)i) : NEG, NEG);  // j == 0
+        };
         int plo = 0, phi = C - 1;  // columns of the row buffer that hold the row above
         if (BANDED) { plo = max(0, dg - w - 1); phi = min(C - 1, dg + w); }
         for (int c = plo; c <= phi; ++c) {  // the top boundary row
-            const int3 v = MID(g.r0, g.c0 + 1 + c, m);
+            const int3 v = bnd(g.r0, g.c0 + 1 + c);
             rb4[c] = make_int4(v.x, v.y, v.z, 0);
         }
         int64_t cells = 0;
@@ -881,14 +892,14 @@ struct ChainCtx {
             for (int k = 0; k < K; ++k) {
                 Mp[k] = NEG; Ip[k] = NEG; Dp[k] = NEG;
                 if (clo == 0 && k < nrow) {
-                    const int3 v = MID(i0 + k, g.c0, m);
+                    const int3 v = bnd(i0 + k, g.c0);
                     Mp[k] = v.x; Ip[k] = v.y; Dp[k] = v.z;
                 }
             }
             // diagonal neighbour of the stripe's first row at column clo
             int32_t dM = NEG, dI = NEG, dD = NEG;
             if (clo == 0) {
-                const int3 v = MID(i0 - 1, g.c0, m);
+                const int3 v = bnd(i0 - 1, g.c0);
                 dM = v.x; dI = v.y; dD = v.z;
             } else if (clo - 1 >= plo && clo - 1 <= phi) {
                 const int4 v = rb4[clo - 1];

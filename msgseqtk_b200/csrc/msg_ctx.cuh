@@ -96,6 +96,7 @@ struct msg_ctx {
     int64_t dp_small_area = 256;
     int64_t dp_warp_area = 65536;
     cudaEvent_t ev[8];
+    int64_t* hpin = nullptr;  // pinned host words for counts copied back without extra waits
     const msg_aln* res_aln = nullptr;
     const uint32_t* res_cigar = nullptr;
     const int64_t* res_off = nullptr;
