@@ -90,7 +90,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--validate", type=int, default=2000, help="reads checked against the oracle after timing")
-    ap.add_argument("--train-pairs", type=int, default=600_000,
+    ap.add_argument("--train-pairs", type=int, default=2_200_000,
                     help="read pairs (fresh seed) whose chains train the band classifier")
     ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--min-score", type=float, default=0.65, help="Alignment::filter rate (msgseqtk-align -s)")
