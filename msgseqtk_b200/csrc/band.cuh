@@ -152,10 +152,12 @@ __host__ __device__ inline bool bandable(int R, int C, int w) {
     return R > 0 && C > 0 && w < max(R, C) - 1 && 2 * (2 * w + 1) < C;
 }
 
-// DP classes of a chain. The chains of a range are sorted by (class, area
-// descending); each class runs as one launch over its part of the sorted list,
-// largest chains first, so that the threads of a warp get chains of similar
-// size and the launch ends on small ones.
+// DP classes of a chain. The chains of a range are sorted by class, then by
+// the sizes of their 5' and 3' flank rectangles (powers of two, larger
+// first), then by area (larger first); each class runs as one launch over its
+// part of the sorted list. The threads of a warp then hold chains of similar
+// shape -- their flank fills run side by side rather than one after the
+// other -- and the launch ends on small chains.
 enum DpClass : int {
     kDpSmall = 0,       // unbanded, area <= small_area: k_dp_small (thread, row by row)
     kDpStripe = 1,      // unbanded, up to warp_area: k_dp_stripe (thread, register stripes)
@@ -169,8 +171,13 @@ enum DpClass : int {
 // traceback list, then the statistics (fallback, exact, dropped, warp cells,
 // thread cells).
 constexpr int kCtrFbStripe = 5, kCtrFbWarp = 6, kCtrTrace = 7, kCtrStat = 8, kCtrWords = 16;
-constexpr int kKeyAreaBits = 21;
-constexpr int kKeyBits = kKeyAreaBits + 3;
+constexpr int kKeyAreaBits = 13;
+constexpr int kKeyBits = kKeyAreaBits + 4 + 4 + 3;
+
+// log2 class (0..15) of a flank area
+__device__ __forceinline__ uint32_t area_class(int64_t a) {
+    return a <= 0 ? 0u : (uint32_t)min(15, 64 - __clzll((unsigned long long)a));
+}
 
 __global__ void k_iota(int64_t c0, int64_t n, int64_t* __restrict__ v) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -216,7 +223,10 @@ __global__ void __launch_bounds__(128) k_band_assign(int64_t c0, int64_t n_chain
         else if (ar <= small_area) cls = kDpSmall;
         else cls = huge ? kDpWarp : kDpStripe;
         const uint32_t amax = (1u << kKeyAreaBits) - 1u;
-        key[t] = ((uint32_t)cls << kKeyAreaBits) | (amax - (uint32_t)min(ar, (int64_t)amax));
+        const uint32_t q5 = 15u - area_class((int64_t)max(g.x, 0) * max(g.y, 0));
+        const uint32_t q3 = 15u - area_class((int64_t)max(g.z, 0) * max(g.w, 0));
+        key[t] = ((uint32_t)cls << (kKeyAreaBits + 8)) | (q5 << (kKeyAreaBits + 4)) | (q3 << kKeyAreaBits) |
+                 (amax - (uint32_t)min(ar >> 3, (int64_t)amax));
     }
 #pragma unroll
     for (int q = 0; q < kDpClasses; ++q) {  // one atomic per warp and class
