@@ -153,7 +153,7 @@ __host__ __device__ inline bool bandable(int R, int C, int w) {
 }
 
 // DP classes of a chain. The chains of a range are sorted by class, then by
-// the sizes of their 5' and 3' flank rectangles (powers of two, larger
+// the sizes of their 5' and 3' flank rectangles (half powers of two, larger
 // first), then by area (larger first); each class runs as one launch over its
 // part of the sorted list. The threads of a warp then hold chains of similar
 // shape -- their flank fills run side by side rather than one after the
@@ -171,12 +171,15 @@ enum DpClass : int {
 // traceback list, then the statistics (fallback, exact, dropped, warp cells,
 // thread cells).
 constexpr int kCtrFbStripe = 5, kCtrFbWarp = 6, kCtrTrace = 7, kCtrStat = 8, kCtrWords = 16;
-constexpr int kKeyAreaBits = 13;
-constexpr int kKeyBits = kKeyAreaBits + 4 + 4 + 3;
+constexpr int kKeyAreaBits = 11;
+constexpr int kKeyBits = kKeyAreaBits + 5 + 5 + 3;
 
-// log2 class (0..15) of a flank area
+// size class (0..31) of a flank area: half powers of two
 __device__ __forceinline__ uint32_t area_class(int64_t a) {
-    return a <= 0 ? 0u : (uint32_t)min(15, 64 - __clzll((unsigned long long)a));
+    if (a <= 0) return 0u;
+    const int b = 63 - __clzll((unsigned long long)a);                  // floor(log2 a)
+    const int half = b >= 1 && ((unsigned long long)a >> (b - 1)) >= 3;  // a >= 1.5 * 2^b
+    return (uint32_t)min(31, 1 + 2 * b + half);
 }
 
 __global__ void k_iota(int64_t c0, int64_t n, int64_t* __restrict__ v) {
@@ -223,10 +226,10 @@ __global__ void __launch_bounds__(128) k_band_assign(int64_t c0, int64_t n_chain
         else if (ar <= small_area) cls = kDpSmall;
         else cls = huge ? kDpWarp : kDpStripe;
         const uint32_t amax = (1u << kKeyAreaBits) - 1u;
-        const uint32_t q5 = 15u - area_class((int64_t)max(g.x, 0) * max(g.y, 0));
-        const uint32_t q3 = 15u - area_class((int64_t)max(g.z, 0) * max(g.w, 0));
-        key[t] = ((uint32_t)cls << (kKeyAreaBits + 8)) | (q5 << (kKeyAreaBits + 4)) | (q3 << kKeyAreaBits) |
-                 (amax - (uint32_t)min(ar >> 3, (int64_t)amax));
+        const uint32_t q5 = 31u - area_class((int64_t)max(g.x, 0) * max(g.y, 0));
+        const uint32_t q3 = 31u - area_class((int64_t)max(g.z, 0) * max(g.w, 0));
+        key[t] = ((uint32_t)cls << (kKeyAreaBits + 10)) | (q5 << (kKeyAreaBits + 5)) | (q3 << kKeyAreaBits) |
+                 (amax - (uint32_t)min(ar >> 5, (int64_t)amax));
     }
 #pragma unroll
     for (int q = 0; q < kDpClasses; ++q) {  // one atomic per warp and class

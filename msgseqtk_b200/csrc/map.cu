@@ -922,11 +922,13 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             launch_dp(ctx, da, kDpStripeBand, nch, S);
             da.fb_list = d_fbw; da.fb_n = d_ctr2 + kCtrFbWarp;
             launch_dp(ctx, da, kDpWarpBand, nch, S);
-            // banded chains without a certificate, on the whole cell set
+            // banded chains without a certificate, on the whole cell set: few
+            // chains, mostly large, so a warp each (a thread each would leave
+            // the launch waiting on its largest chain)
             DpArgs fb = da;
             fb.band = nullptr;
             fb.list = d_fb; fb.n_list = d_ctr2 + kCtrFbStripe;
-            launch_dp(ctx, fb, -kDpStripe - 1, nch, S);
+            launch_dp(ctx, fb, -kDpWarp - 1, nch, S);
             fb.list = d_fbw; fb.n_list = d_ctr2 + kCtrFbWarp;
             launch_dp(ctx, fb, -kDpWarp - 1, nch, S);
         }
@@ -1524,6 +1526,65 @@ extern "C" int msg_ctx_set_dp_shape(msg_ctx* ctx, int32_t stripe_rows, int64_t s
     ctx->dp_k = stripe_rows;
     ctx->dp_small_area = small_area;
     ctx->dp_warp_area = warp_area;
+    return MSG_OK;
+}
+
+extern "C" int msg_dp_autotune(msg_ctx* ctx, const msg_read_batch* sample, const msg_map_params* params,
+                               msg_dp_tune* result) {
+    if (!ctx || !sample || !params || !result) return MSG_EINVAL;
+    if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
+    msg::DeviceGuard dg_(ctx->device);
+    if (!dg_.ok) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
+    int rc = upload_reads(ctx, sample);
+    if (rc != MSG_OK) return rc;
+    int n_tried = 0;
+    // DP stage time of one shape: an untimed run, then the timed one
+    auto time_shape = [&](int k, int64_t small, int64_t warp, double* ms) -> int {
+        ctx->dp_k = k;
+        ctx->dp_small_area = small;
+        ctx->dp_warp_area = warp;
+        double t = 0;
+        for (int rep = 0; rep < 2; ++rep) {
+            msg_aln_out dev{};  // results stay on the device
+            const int r = map_impl(ctx, ctx->reads.as<uint8_t>(), ctx->offs.as<int64_t>(), sample->n_reads, params,
+                                   &dev, nullptr);
+            if (r != MSG_OK) return r;
+            t = ctx->stats.ms_dp;
+        }
+        ++n_tried;
+        *ms = t;
+        return MSG_OK;
+    };
+    int best_k = 16;
+    int64_t best_small = 256, best_warp = 65536;
+    double best = 0;
+    rc = time_shape(best_k, best_small, best_warp, &best);
+    if (rc != MSG_OK) return rc;
+    const double t_default = best;
+    for (int64_t warp : {4096ll, 16384ll, 262144ll}) {
+        double t = 0;
+        if ((rc = time_shape(best_k, best_small, warp, &t)) != MSG_OK) return rc;
+        if (t < best) { best = t; best_warp = warp; }
+    }
+    for (int k : {8, 32}) {
+        double t = 0;
+        if ((rc = time_shape(k, best_small, best_warp, &t)) != MSG_OK) return rc;
+        if (t < best) { best = t; best_k = k; }
+    }
+    for (int64_t small : {0ll, 64ll, 1024ll}) {
+        double t = 0;
+        if ((rc = time_shape(best_k, small, best_warp, &t)) != MSG_OK) return rc;
+        if (t < best) { best = t; best_small = small; }
+    }
+    ctx->dp_k = best_k;
+    ctx->dp_small_area = best_small;
+    ctx->dp_warp_area = best_warp;
+    result->stripe_rows = best_k;
+    result->small_area = best_small;
+    result->warp_area = best_warp;
+    result->ms_dp = best;
+    result->ms_dp_default = t_default;
+    result->n_tried = n_tried;
     return MSG_OK;
 }
 

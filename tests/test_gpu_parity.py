@@ -272,6 +272,16 @@ def test_dp_shape_gives_same_records(oracle_built):
             assert len(base["aln"]) > 0
         with pytest.raises(lib.MsgError):
             c.set_dp_shape(12, 256, 65536)
+        # the autotuner picks one of its candidates and changes no record
+        params = plist[2]
+        c.set_dp_shape(*DP_SHAPES[0])
+        before = c.map(seq, off, params)
+        tune = c.dp_autotune(seq, off, params)
+        assert tune["stripe_rows"] in (8, 16, 32) and tune["n_tried"] == 9
+        assert tune["warp_area"] in (4096, 16384, 65536, 262144) and tune["small_area"] in (0, 64, 256, 1024)
+        after = c.map(seq, off, params)
+        for k in ("aln", "cigar", "read_aln_off"):
+            assert np.array_equal(before[k], after[k]), k
     finally:
         c.close()
 
