@@ -566,10 +566,10 @@ def main():
               for k in range(n_batches)]
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
 
-    # the library's autotuner picks the DP work split on a sample of the
-    # first batch (untimed; records do not depend on the split)
+    # the library's autotuner picks the SMEM and DP kernel shapes on a sample
+    # of the first batch (untimed; records do not depend on the shapes)
     ns = min(200_000, bp, len(reads))
-    dp_shape = ctx.dp_autotune(reads.seqs[:reads.offs[ns]], reads.offs[:ns + 1], params)
+    dp_shape = ctx.autotune(reads.seqs[:reads.offs[ns]], reads.offs[:ns + 1], params)
     dp_shape["sample_reads"] = ns
 
     def run_device(k, prm):
@@ -798,7 +798,7 @@ def main():
                            "parallelism": f"dp{world}" if world > 1 else "single GPU"},
                 "gcups": gcups(agg), "plain_gpu": plain, "learned_band": band_info,
                 "e2e": e2e, "e2e_sam": e2e_sam, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
-                "gpu_launches": agg["n_launch"], "validation": valid, "setup": setup, "dp_shape": dp_shape,
+                "gpu_launches": agg["n_launch"], "validation": valid, "setup": setup, "tuned_shapes": dp_shape,
                 "stats": {k: agg[k] for k in counters}}
         print(json.dumps(line), flush=True)
     ctx.close()

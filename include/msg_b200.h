@@ -307,23 +307,34 @@ int msg_ctx_set_scratch_limit(msg_ctx* ctx, int64_t bytes);
  * anti-diagonals. Defaults 256, 65536, 16. Results do not depend on it. */
 int msg_ctx_set_dp_shape(msg_ctx* ctx, int32_t stripe_rows, int64_t small_area, int64_t warp_area);
 
-/* The DP work split chosen by msg_dp_autotune, with the DP stage times that
- * chose it. */
-typedef struct msg_dp_tune {
+/* Kernel shape of the SMEM stage for reads up to 254 bp (no reference
+ * counterpart): 0 = one read per thread (default); 1 and 2 = two reads per
+ * thread, each thread keeping two extensions' bucket loads in flight (1:
+ * registers sized for 4 blocks of 128 threads per SM, 2: for 3). Results do
+ * not depend on it. */
+int msg_ctx_set_smem_shape(msg_ctx* ctx, int32_t variant);
+
+/* The shapes chosen by msg_autotune, with the stage times that chose them. */
+typedef struct msg_tune {
     int32_t stripe_rows;
     int32_t n_tried;        /* shapes timed */
     int64_t small_area, warp_area;
-    double ms_dp;           /* DP stage time of the chosen shape on the sample */
+    double ms_dp;           /* DP stage time of the chosen split on the sample */
     double ms_dp_default;   /* the same with the defaults (16, 256, 65536) */
-} msg_dp_tune;
+    int32_t smem_variant;
+    int32_t pad;
+    double ms_smem;         /* SMEM stage time of the chosen variant */
+    double ms_smem_default; /* the same with variant 0 */
+} msg_tune;
 
-/* Autotuner of the DP work split (no reference counterpart): maps the
- * sample batch (host memory) with `params` under candidate shapes -- the
- * warp threshold, then the stripe height, then the row-by-row threshold, each
- * chosen with the others fixed -- timing the DP stage of each (a second run
- * of every shape, after one untimed), and sets the fastest on the context.
- * Records never depend on the shape, so the choice only changes speed. */
-int msg_dp_autotune(msg_ctx* ctx, const msg_read_batch* sample, const msg_map_params* params, msg_dp_tune* result);
+/* Autotuner of the kernel shapes (no reference counterpart): maps the sample
+ * batch (host memory) with `params` under candidate shapes -- the SMEM
+ * variant, then the DP warp threshold, stripe height and row-by-row
+ * threshold, each chosen with the others fixed -- timing the stage it
+ * affects (a second run of every shape, after one untimed), and sets the
+ * fastest on the context. Records never depend on the shapes, so the choice
+ * only changes speed. */
+int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const msg_map_params* params, msg_tune* result);
 
 /* ---- Seeding that allocates nothing ----
  * No counterpart in the reference: it exists for callers that cannot call

@@ -409,11 +409,17 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         CK(cudaMemsetAsync(d_status, 0, 4, st));
         // short reads on the thread kernel
         if (thread_path) {
+            // one read per thread, or two per thread (ctx->smem_variant 1
+            // and 2: each thread keeps two extensions' loads in flight)
+            const int var = ctx->smem_variant;
+            const bool pair = var != 0;
             int bps = 0;
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread, 128, 0));
+            if (var == 1) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread2<4>, 128, 0));
+            else if (var == 2) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread2<3>, 128, 0));
+            else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread, 128, 0));
             const int64_t n_thr = (int64_t)ctx->num_sms * std::max(1, bps) * 128;
             const int64_t pv_cap = kThreadPrev;
-            CK(ctx->prev.ensure(n_thr * pv_cap * sizeof(PrevEntry) + 64));
+            CK(ctx->prev.ensure((pair ? 2 : 1) * n_thr * pv_cap * sizeof(PrevEntry) + 64));
             SmemThreadArgs ta{};
             for (int b = 0; b < 16; ++b) ta.llk[b] = im.llk[b];
             ta.seq = d_seq; ta.off = d_off; ta.n_reads = (int64_t)h_split[0]; ta.min_len = params->min_len;
@@ -424,7 +430,9 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             ta.count = ctx->smem_cnt.as<int32_t>();
             ta.prev = ctx->prev.as<PrevEntry>(); ta.pv_cap = pv_cap;
             ta.work = d_ctr; ta.n_ext = d_ctr + 1; ta.status = d_status;
-            S.n_launch++, k_smem_thread<<<n_thr / 128, 128, 0, st>>>(ta, ix);
+            if (var == 1) S.n_launch++, k_smem_thread2<4><<<n_thr / 128, 128, 0, st>>>(ta, ix);
+            else if (var == 2) S.n_launch++, k_smem_thread2<3><<<n_thr / 128, 128, 0, st>>>(ta, ix);
+            else S.n_launch++, k_smem_thread<<<n_thr / 128, 128, 0, st>>>(ta, ix);
             CK(cudaGetLastError());
         }
         // long reads (all reads once the thread kernel has given up) on the warp kernel
@@ -1529,8 +1537,14 @@ extern "C" int msg_ctx_set_dp_shape(msg_ctx* ctx, int32_t stripe_rows, int64_t s
     return MSG_OK;
 }
 
-extern "C" int msg_dp_autotune(msg_ctx* ctx, const msg_read_batch* sample, const msg_map_params* params,
-                               msg_dp_tune* result) {
+extern "C" int msg_ctx_set_smem_shape(msg_ctx* ctx, int32_t variant) {
+    if (!ctx || variant < 0 || variant > 2) return MSG_EINVAL;
+    ctx->smem_variant = variant;
+    return MSG_OK;
+}
+
+extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const msg_map_params* params,
+                            msg_tune* result) {
     if (!ctx || !sample || !params || !result) return MSG_EINVAL;
     if (!ctx->idx.loaded) return ctx->fail(MSG_ESTATE, "no index loaded");
     msg::DeviceGuard dg_(ctx->device);
@@ -1538,52 +1552,57 @@ extern "C" int msg_dp_autotune(msg_ctx* ctx, const msg_read_batch* sample, const
     int rc = upload_reads(ctx, sample);
     if (rc != MSG_OK) return rc;
     int n_tried = 0;
-    // DP stage time of one shape: an untimed run, then the timed one
-    auto time_shape = [&](int k, int64_t small, int64_t warp, double* ms) -> int {
+    // stage times of one shape: an untimed run, then the timed one
+    auto time_shape = [&](int var, int k, int64_t small, int64_t warp, double* ms_smem, double* ms_dp) -> int {
+        ctx->smem_variant = var;
         ctx->dp_k = k;
         ctx->dp_small_area = small;
         ctx->dp_warp_area = warp;
-        double t = 0;
         for (int rep = 0; rep < 2; ++rep) {
             msg_aln_out dev{};  // results stay on the device
             const int r = map_impl(ctx, ctx->reads.as<uint8_t>(), ctx->offs.as<int64_t>(), sample->n_reads, params,
                                    &dev, nullptr);
             if (r != MSG_OK) return r;
-            t = ctx->stats.ms_dp;
         }
         ++n_tried;
-        *ms = t;
+        *ms_smem = ctx->stats.ms_smem;
+        *ms_dp = ctx->stats.ms_dp;
         return MSG_OK;
     };
-    int best_k = 16;
+    int best_var = 0, best_k = 16;
     int64_t best_small = 256, best_warp = 65536;
-    double best = 0;
-    rc = time_shape(best_k, best_small, best_warp, &best);
-    if (rc != MSG_OK) return rc;
-    const double t_default = best;
+    double best_smem = 0, best_dp = 0, ts = 0, td = 0;
+    if ((rc = time_shape(best_var, best_k, best_small, best_warp, &best_smem, &best_dp)) != MSG_OK) return rc;
+    const double smem_default = best_smem, dp_default = best_dp;
+    for (int var : {1, 2}) {
+        if ((rc = time_shape(var, best_k, best_small, best_warp, &ts, &td)) != MSG_OK) return rc;
+        if (ts < best_smem) { best_smem = ts; best_var = var; }
+    }
     for (int64_t warp : {4096ll, 16384ll, 262144ll}) {
-        double t = 0;
-        if ((rc = time_shape(best_k, best_small, warp, &t)) != MSG_OK) return rc;
-        if (t < best) { best = t; best_warp = warp; }
+        if ((rc = time_shape(best_var, best_k, best_small, warp, &ts, &td)) != MSG_OK) return rc;
+        if (td < best_dp) { best_dp = td; best_warp = warp; }
     }
     for (int k : {8, 32}) {
-        double t = 0;
-        if ((rc = time_shape(k, best_small, best_warp, &t)) != MSG_OK) return rc;
-        if (t < best) { best = t; best_k = k; }
+        if ((rc = time_shape(best_var, k, best_small, best_warp, &ts, &td)) != MSG_OK) return rc;
+        if (td < best_dp) { best_dp = td; best_k = k; }
     }
     for (int64_t small : {0ll, 64ll, 1024ll}) {
-        double t = 0;
-        if ((rc = time_shape(best_k, small, best_warp, &t)) != MSG_OK) return rc;
-        if (t < best) { best = t; best_small = small; }
+        if ((rc = time_shape(best_var, best_k, small, best_warp, &ts, &td)) != MSG_OK) return rc;
+        if (td < best_dp) { best_dp = td; best_small = small; }
     }
+    ctx->smem_variant = best_var;
     ctx->dp_k = best_k;
     ctx->dp_small_area = best_small;
     ctx->dp_warp_area = best_warp;
     result->stripe_rows = best_k;
     result->small_area = best_small;
     result->warp_area = best_warp;
-    result->ms_dp = best;
-    result->ms_dp_default = t_default;
+    result->ms_dp = best_dp;
+    result->ms_dp_default = dp_default;
+    result->smem_variant = best_var;
+    result->pad = 0;
+    result->ms_smem = best_smem;
+    result->ms_smem_default = smem_default;
     result->n_tried = n_tried;
     return MSG_OK;
 }

@@ -208,31 +208,50 @@ __device__ __forceinline__ void occ_counts(const IndexDev& ix, uint32_t k, uint3
     dl = dollar + din;
 }
 
-// FMDIndex::backExt (FMDIndex.cpp:577-610) on 32-bit bi-intervals: the size
-// from the base's counts at the two rows, and q, when the size changes, from
-// the counts of '$' and of the bases after it (FMDIndex.cpp:592-604).
-__device__ inline int64_t back_ext32(const IndexDev& ix, uint32_t& p, uint32_t& q, uint32_t& s, int b) {
-    if (!is_basic(b)) { s = 0; return 0; }
-    const int c = to_int(b);
-    const uint32_t code = (uint32_t)(c - 1);
-    const uint32_t ja = p, jb = p + s;  // exclusive ends of rows p-1 and p+s-1
-    const uint32_t ka = ja >> 6, kb = jb >> 6;
+// The two occurrence buckets a 32-bit backward extension of (p, s) reads: the
+// buckets of rows p-1 and p+s-1 (one when both fall in the same bucket).
+struct ExtLoad {
+    uint4 a0, a1, b0, b1;
+};
+
+__device__ __forceinline__ void back_ext32_load(const IndexDev& ix, uint32_t p, uint32_t s, ExtLoad& l) {
+    const uint32_t ka = p >> 6, kb = (p + s) >> 6;  // exclusive ends of rows p-1 and p+s-1
     const uint4* pa = reinterpret_cast<const uint4*>(ix.bkt + ka);
-    const uint4 a0 = __ldg(pa), a1 = __ldg(pa + 1);
-    uint4 b0 = a0, b1 = a1;
+    l.a0 = __ldg(pa);
+    l.a1 = __ldg(pa + 1);
+    l.b0 = l.a0;
+    l.b1 = l.a1;
     if (kb != ka) {
         const uint4* pb = reinterpret_cast<const uint4*>(ix.bkt + kb);
-        b0 = __ldg(pb); b1 = __ldg(pb + 1);
+        l.b0 = __ldg(pb);
+        l.b1 = __ldg(pb + 1);
     }
+}
+
+// FMDIndex::backExt (FMDIndex.cpp:577-610) on 32-bit bi-intervals from loaded
+// buckets (b a basic base): the size from the base's counts at the two rows,
+// and q, when the size changes, from the counts of '$' and of the bases after
+// it (FMDIndex.cpp:592-604).
+__device__ __forceinline__ uint32_t back_ext32_apply(const IndexDev& ix, uint32_t& p, uint32_t& q, uint32_t& s, int b,
+                                                     const ExtLoad& l) {
+    const uint32_t code = (uint32_t)(to_int(b) - 1);
+    const uint32_t ja = p, jb = p + s;
     uint32_t oa, ga, da, ob, gb, db;
-    occ_counts(ix, ka, ja & 63u, code, a0, a1, oa, ga, da);
-    occ_counts(ix, kb, jb & 63u, code, b0, b1, ob, gb, db);
+    occ_counts(ix, ja >> 6, ja & 63u, code, l.a0, l.a1, oa, ga, da);
+    occ_counts(ix, jb >> 6, jb & 63u, code, l.b0, l.b1, ob, gb, db);
     const uint32_t ns = ob - oa;
     if (ns == 0) { s = 0; return 0; }
     if (ns != s) q = q + (db - da) + (gb - ga);
     p = (uint32_t)ix.C[b] + oa;
     s = ns;
     return ns;
+}
+
+__device__ inline int64_t back_ext32(const IndexDev& ix, uint32_t& p, uint32_t& q, uint32_t& s, int b) {
+    if (!is_basic(b)) { s = 0; return 0; }
+    ExtLoad l;
+    back_ext32_load(ix, p, s, l);
+    return back_ext32_apply(ix, p, q, s, b, l);
 }
 
 // Error bits of the device status word.

@@ -274,6 +274,32 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
     }
 }
 
+// Finish the read in progress (its count) and start the next one from the
+// batch's work counter; false when the batch has no read left.
+__device__ __forceinline__ bool smem_next_read(ThreadSmem& t, const SmemThreadArgs& a, const IndexDev& ix) {
+    if (t.phase == PH_DONE) {
+        a.count[t.r] = t.n_out;
+        if (t.n_out > t.cap_r) atomicOr(a.status, kErrOverflow);
+    }
+    unsigned long long r = atomicAdd(a.work, 1ull);
+    if ((int64_t)r >= a.n_reads) return false;
+    if (a.list) r = (unsigned long long)a.list[r];
+    t.r = (int32_t)r;
+    const int64_t o0 = a.off[r];
+    t.rd = a.seq + o0;
+    t.L = (int32_t)(a.off[r + 1] - o0);
+    const int64_t slot = a.out_off ? a.out_off[r] : (int64_t)r * a.cap;
+    t.cap_r = (int32_t)(a.out_off ? a.out_off[r + 1] - slot : a.cap);
+    t.out = a.out + 6 * slot;
+    t.n_out = 0;
+    t.ovf = 0;
+    if (t.L <= 0) { t.phase = PH_DONE; return true; }
+    t.from = t.L / 2;  // SMEM.cpp:189-191
+    t.to = t.from + 1;
+    smem_call(t, ix, 0, 1, t.from);
+    return true;
+}
+
 __global__ void __launch_bounds__(128, 5) k_smem_thread(SmemThreadArgs a, IndexDev ix) {
     if (threadIdx.x < 16) s_llk[threadIdx.x] = a.llk[threadIdx.x];
     __syncthreads();
@@ -291,26 +317,7 @@ __global__ void __launch_bounds__(128, 5) k_smem_thread(SmemThreadArgs a, IndexD
         bool have = false;
         while (alive && !have) {
             if (t.phase == PH_NEXT_READ || t.phase == PH_DONE) {
-                if (t.phase == PH_DONE) {
-                    a.count[t.r] = t.n_out;
-                    if (t.n_out > t.cap_r) atomicOr(a.status, kErrOverflow);
-                }
-                unsigned long long r = atomicAdd(a.work, 1ull);
-                if ((int64_t)r >= a.n_reads) { alive = false; break; }
-                if (a.list) r = (unsigned long long)a.list[r];
-                t.r = (int32_t)r;
-                const int64_t o0 = a.off[r];
-                t.rd = a.seq + o0;
-                t.L = (int32_t)(a.off[r + 1] - o0);
-                const int64_t slot = a.out_off ? a.out_off[r] : (int64_t)r * a.cap;
-                t.cap_r = (int32_t)(a.out_off ? a.out_off[r + 1] - slot : a.cap);
-                t.out = a.out + 6 * slot;
-                t.n_out = 0;
-                t.ovf = 0;
-                if (t.L <= 0) { t.phase = PH_DONE; continue; }
-                t.from = t.L / 2;  // SMEM.cpp:189-191
-                t.to = t.from + 1;
-                smem_call(t, ix, 0, 1, t.from);
+                alive = smem_next_read(t, a, ix);
                 continue;
             }
             have = smem_advance(t, a, ix, pv, P, Q, S, B);
@@ -327,6 +334,66 @@ __global__ void __launch_bounds__(128, 5) k_smem_thread(SmemThreadArgs a, IndexD
         if (have) smem_apply(t, a, pv, P, Q, S);
     }
     if (t.ext) atomicAdd(a.n_ext, t.ext);
+}
+
+// Two reads per thread, each with its own state machine and candidate list:
+// an iteration advances both to their next extension, issues the bucket loads
+// of both, then finishes both, so that a thread has two extensions' loads in
+// flight instead of one. Same per-read results as k_smem_thread. MINB: blocks
+// of 128 threads per SM the registers are sized for (4: spills a little; 3:
+// fewer resident threads).
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_smem_thread2(SmemThreadArgs a, IndexDev ix) {
+    if (threadIdx.x < 16) s_llk[threadIdx.x] = a.llk[threadIdx.x];
+    __syncthreads();
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    PrevEntry* pv[2] = {a.prev + (2 * tid) * a.pv_cap, a.prev + (2 * tid + 1) * a.pv_cap};
+    ThreadSmem t[2];
+    bool alive[2] = {true, true};
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        t[u].phase = PH_NEXT_READ;
+        t[u].ext = 0;
+        t[u].n_out = 0;
+        t[u].r = -1;
+    }
+    for (;;) {
+        uint32_t P[2] = {0, 0}, Q[2] = {0, 0}, S[2] = {0, 0};
+        int B[2] = {0, 0};
+        bool have[2] = {false, false};
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            while (alive[u] && !have[u]) {
+                if (t[u].phase == PH_NEXT_READ || t[u].phase == PH_DONE) {
+                    alive[u] = smem_next_read(t[u], a, ix);
+                    continue;
+                }
+                have[u] = smem_advance(t[u], a, ix, pv[u], P[u], Q[u], S[u], B[u]);
+            }
+        }
+        __syncwarp();
+        if (!__any_sync(0xffffffffu, alive[0] || alive[1])) break;
+        ExtLoad l[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+            if (have[u] && is_basic(B[u])) back_ext32_load(ix, P[u], S[u], l[u]);
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            if (!have[u]) continue;
+            if (is_basic(B[u])) {
+                t[u].ext++;
+                back_ext32_apply(ix, P[u], Q[u], S[u], B[u], l[u]);
+            } else {
+                S[u] = 0;
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+            if (have[u]) smem_apply(t[u], a, pv[u], P[u], Q[u], S[u]);
+    }
+    const unsigned long long e = t[0].ext + t[1].ext;
+    if (e) atomicAdd(a.n_ext, e);
 }
 
 }  // namespace msg

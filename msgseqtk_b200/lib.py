@@ -30,7 +30,7 @@ EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy"
            "msg_db_views", "msg_db_free", "msg_index_bytes",
            "msg_map_params_default", "msg_map_batch", "msg_map_batches", "msg_seed_batch", "msg_locate_batch",
            "msg_chain_batch", "msg_align_batch", "msg_map_batch_device", "msg_last_stats",
-           "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_ctx_set_dp_shape", "msg_dp_autotune", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
+           "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_ctx_set_dp_shape", "msg_ctx_set_smem_shape", "msg_autotune", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
            "msg_band_train", "msg_band_grad", "msg_tail_params_default", "msg_tail_batch", "msg_pair_params_default", "msg_tail_pe_batch",
            "msg_fastq_parse", "msg_fastq_format", "msg_clean_format", "msg_sam_format",
            "msg_mem_params_default", "msg_mem_batch", "msg_clean_batch",
@@ -102,9 +102,11 @@ class StageDump(C.Structure):
                 ("seed", i64p), ("seed_off", i64p), ("n_smem", C.c_int64), ("n_seed", C.c_int64)]
 
 
-class DpTune(C.Structure):
+class Tune(C.Structure):
     _fields_ = [("stripe_rows", C.c_int32), ("n_tried", C.c_int32), ("small_area", C.c_int64),
-                ("warp_area", C.c_int64), ("ms_dp", C.c_double), ("ms_dp_default", C.c_double)]
+                ("warp_area", C.c_int64), ("ms_dp", C.c_double), ("ms_dp_default", C.c_double),
+                ("smem_variant", C.c_int32), ("pad", C.c_int32), ("ms_smem", C.c_double),
+                ("ms_smem_default", C.c_double)]
 
 
 class MapStats(C.Structure):
@@ -166,7 +168,8 @@ def load_library(path: str = LIB_PATH):
     L.msg_ctx_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     L.msg_ctx_set_scratch_limit.argtypes = [C.c_void_p, C.c_int64]
     L.msg_ctx_set_dp_shape.argtypes = [C.c_void_p, C.c_int32, C.c_int64, C.c_int64]
-    L.msg_dp_autotune.argtypes = [C.c_void_p, C.POINTER(ReadBatch), C.POINTER(MapParams), C.POINTER(DpTune)]
+    L.msg_ctx_set_smem_shape.argtypes = [C.c_void_p, C.c_int32]
+    L.msg_autotune.argtypes = [C.c_void_p, C.POINTER(ReadBatch), C.POINTER(MapParams), C.POINTER(Tune)]
     L.msg_smem_batch_noalloc.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(MapParams),
                                          C.c_void_p, C.c_int64, C.c_void_p]
     f32p = C.POINTER(C.c_float)
@@ -732,14 +735,19 @@ class Context:
     def set_scratch_limit(self, nbytes: int):
         self._check(self.lib.msg_ctx_set_scratch_limit(self.h, int(nbytes)), "msg_ctx_set_scratch_limit")
 
-    def dp_autotune(self, seq, off, params: MapParams | None = None) -> dict:
-        """msg_dp_autotune on a sample batch: sets the fastest DP work split."""
+    def autotune(self, seq, off, params: MapParams | None = None) -> dict:
+        """msg_autotune on a sample batch: sets the fastest SMEM and DP shapes."""
         params = params or default_params()
         seq, off, b = self._batch(seq, off)
-        r = DpTune()
-        self._check(self.lib.msg_dp_autotune(self.h, C.byref(b), C.byref(params), C.byref(r)), "msg_dp_autotune")
-        return dict(stripe_rows=r.stripe_rows, small_area=r.small_area, warp_area=r.warp_area, ms_dp=r.ms_dp,
+        r = Tune()
+        self._check(self.lib.msg_autotune(self.h, C.byref(b), C.byref(params), C.byref(r)), "msg_autotune")
+        return dict(smem_variant=r.smem_variant, stripe_rows=r.stripe_rows, small_area=r.small_area,
+                    warp_area=r.warp_area, ms_smem=r.ms_smem, ms_smem_default=r.ms_smem_default, ms_dp=r.ms_dp,
                     ms_dp_default=r.ms_dp_default, n_tried=r.n_tried)
+
+    def set_smem_shape(self, variant: int = 0):
+        """SMEM thread-path variant (msg_ctx_set_smem_shape); records do not depend on it."""
+        self._check(self.lib.msg_ctx_set_smem_shape(self.h, int(variant)), "msg_ctx_set_smem_shape")
 
     def set_dp_shape(self, stripe_rows: int = 16, small_area: int = 256, warp_area: int = 65536):
         """DP work split (msg_ctx_set_dp_shape); records do not depend on it."""

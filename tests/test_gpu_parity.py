@@ -226,6 +226,34 @@ def test_scratch_limit_gives_same_records(oracle_built):
         c.close()
 
 
+@pytest.mark.parametrize("variant", [1, 2])
+def test_smem_two_reads_per_thread_match_reference_fixtures(cases, variant):
+    """The SMEM kernel that advances two reads per thread emits every read's
+    SMEMs exactly as the reference does (committed fixtures, all parameter
+    sets), and maps to the same records."""
+    c = lib.Context(0)
+    try:
+        for name in ("uniform", "repeats"):
+            cs = cases[name]
+            c.load_index(cs.view)
+            for k in range(cs.n_params):
+                ps = cs.params(k)
+                ex = cs.expected(k)
+                params = lib.default_params(min_len=ps["min_len"], max_evalue=ps["max_evalue"],
+                                            max_nseed=ps["max_nseed"], mode=ps["mode"])
+                c.set_smem_shape(0)
+                one = c.map(cs.reads, cs.read_off, params, dump=True)
+                c.set_smem_shape(variant)
+                two = c.map(cs.reads, cs.read_off, params, dump=True)
+                assert np.array_equal(two["smem_off"], ex["smem_off"]) and np.array_equal(two["smem"], ex["smem"])
+                for key in ("seed", "seed_off", "aln", "cigar", "read_aln_off"):
+                    assert np.array_equal(one[key], two[key]), (name, k, key)
+        with pytest.raises(lib.MsgError):
+            c.set_smem_shape(3)
+    finally:
+        c.close()
+
+
 DP_SHAPES = [(16, 256, 65536), (8, 0, 1 << 40), (32, 0, 1 << 40), (16, 1 << 40, 1 << 40), (16, 0, 0),
              (8, 64, 4096), (32, 256, 20000)]
 
@@ -276,8 +304,8 @@ def test_dp_shape_gives_same_records(oracle_built):
         params = plist[2]
         c.set_dp_shape(*DP_SHAPES[0])
         before = c.map(seq, off, params)
-        tune = c.dp_autotune(seq, off, params)
-        assert tune["stripe_rows"] in (8, 16, 32) and tune["n_tried"] == 9
+        tune = c.autotune(seq, off, params)
+        assert tune["stripe_rows"] in (8, 16, 32) and tune["n_tried"] == 11 and tune["smem_variant"] in (0, 1, 2)
         assert tune["warp_area"] in (4096, 16384, 65536, 262144) and tune["small_area"] in (0, 64, 256, 1024)
         after = c.map(seq, off, params)
         for k in ("aln", "cigar", "read_aln_off"):
