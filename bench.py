@@ -63,6 +63,9 @@ WORKLOADS = {
              "0.1% indel, 5% random pairs; mates mapped as single reads (findSeedsPE)",
     "uneven": "uneven: 200 genomes ~600 Mbp; single-end reads 60% 75-150 bp, 30% 250-300 bp, 10% 1-10 kbp, "
               "5% errors (70% substitutions, 30% indels); one batch",
+    "repeats": "repeats: two ~750 Mbp metagenomes (log-normal lengths, GC 30-70%, 10% repeat families: 500-5000 bp "
+               "units x 10-200 copies at 2-5% divergence) indexed together (~3.0 G BD symbols), 2x150 bp pairs, "
+               "insert N(400,50), 1% sub, 0.1% indel, 5% random pairs",
     "clean": "clean: reference index = 200 genomes ~600 Mbp, background index = 100 genomes ~300 Mbp (other "
              "seed); 2x150 bp pairs, half from each set, insert N(400,50), 1% sub, 0.1% indel, 5% random pairs; "
              "findMEMS (min seed 17, e-value 0.01) on both indexes, log-odds > 0 keeps the pair",
@@ -82,7 +85,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--pairs", type=int, default=2_000_000, help="read pairs per GPU")
+    ap.add_argument("--pairs", type=int, default=None, help="read pairs per GPU (2 M; 10 M for repeats)")
     ap.add_argument("--batch-pairs", type=int, default=500_000)
     ap.add_argument("--genomes", type=int, default=200)
     ap.add_argument("--median", type=float, default=3e6)
@@ -94,11 +97,15 @@ def parse():
                     help="read pairs (fresh seed) whose chains train the band classifier")
     ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--min-score", type=float, default=0.65, help="Alignment::filter rate (msgseqtk-align -s)")
-    ap.add_argument("--workload", default="scale", choices=["scale", "uneven", "clean"],
+    ap.add_argument("--repeat-mbp", type=float, default=750.0, help="size of each repeats metagenome (Mbp)")
+    ap.add_argument("--workload", default="scale", choices=["scale", "uneven", "clean", "repeats"],
                     help="scale: 2x150 bp pairs; uneven: single-end reads of mixed lengths (one batch); "
                          "clean: msgseqtk-clean's MEM log-odds path on two indexes")
     ap.add_argument("--uneven-reads", type=int, default=500_000)
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.pairs is None:
+        args.pairs = 10_000_000 if args.workload == "repeats" else 2_000_000
+    return args
 
 
 class Clocks:
@@ -200,7 +207,11 @@ def uneven_reads(genomes, n, seed):
 def make_workload(args, rank, device):
     from msgseqtk_b200 import index_build, synth
     t0 = time.time()
-    genomes = synth.scale_genomes(seed=args.seed, n_genomes=args.genomes, median=args.median)
+    if args.workload == "repeats":
+        genomes = (synth.repeat_metagenome(seed=args.seed + 300, total_bp=args.repeat_mbp * 1e6, median=args.median) +
+                   synth.repeat_metagenome(seed=args.seed + 400, total_bp=args.repeat_mbp * 1e6, median=args.median))
+    else:
+        genomes = synth.scale_genomes(seed=args.seed, n_genomes=args.genomes, median=args.median)
     t1 = time.time()
     view = index_build.build_view(genomes, device=device)
     t2 = time.time()
@@ -268,8 +279,7 @@ def run_reference(args, world, rank):
             "warmup": args.warmup, "ms_per_step": 1000 * total / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "scale: 200 genomes ~600 Mbp (log-normal, GC 30-70%), 2x150 bp pairs, "
-                                   "insert N(400,50), 1% sub, 0.1% indel, 5% random pairs",
+            "config": {"workload": WORKLOADS[args.workload],
                        "reads_per_step": per_step, "bd_symbols": view.n, "parallelism": f"omp{threads}"},
             "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads, "kind": "reference",
                              "sample": f"{per_step} reads per step from the workload"},
@@ -554,7 +564,7 @@ def main():
     del treads, tm1, tm2
 
     # batches: reads resident on the device, and pinned host copies for e2e
-    bp = 2 * args.batch_pairs if args.workload == "scale" else len(reads)
+    bp = 2 * args.batch_pairs if args.workload in ("scale", "repeats") else len(reads)
     n_batches = max(1, len(reads) // bp)
     d_seq = torch.from_numpy(reads.seqs).cuda()
     offs_d = []
@@ -672,7 +682,7 @@ def main():
     from concurrent.futures import ThreadPoolExecutor
     tail_threads = max(1, (os.cpu_count() or 2) - 1)
     tprm = lib.tail_params(min_score_rate=args.min_score, max_report=1, n_threads=tail_threads)
-    pairing = lib.pair_params(mean=400.0, sd=50.0, min_ins=-100.0, max_ins=900.0) if args.workload == "scale" \
+    pairing = lib.pair_params(mean=400.0, sd=50.0, min_ins=-100.0, max_ins=900.0) if args.workload in ("scale", "repeats") \
         else None
     bufs = [(aln_buf, cig_buf, roff_buf), (pinned(8 * bp, lib.ALN_DTYPE), pinned(64 * bp, np.uint32),
                                             pinned(bp + 1, np.int64))]
@@ -780,7 +790,7 @@ def main():
                  "compared": "records after Alignment::filter (alnScore >= L * %g)" % args.min_score}
 
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline and args.workload == "scale":
+    if rank == 0 and not args.no_cpu_baseline and args.workload in ("scale", "repeats"):
         r = cpu_baseline(genomes, view, reads, args.cpu_seconds)
         cpu = r[0] if r else None
 

@@ -47,45 +47,64 @@ def bd_text(chroms) -> np.ndarray:
     return np.concatenate(parts)
 
 
-def suffix_array(text: np.ndarray, device: str | torch.device = "cpu") -> torch.Tensor:
+def suffix_array(text: np.ndarray, device: str | torch.device = "cpu", chunk: int = 1 << 28) -> torch.Tensor:
     """Suffix array of a byte string by prefix doubling (standard order: a
     suffix that is a proper prefix of another sorts first). Returns int64 on
-    `device`."""
+    `device`. Elementwise work runs in chunks of `chunk` elements and in
+    place, so that at most a few n-element int64 arrays are alive at once
+    (texts of 3 G symbols on one GPU)."""
     n = int(text.shape[0])
     dev = torch.device(device)
-    sym = torch.from_numpy(text.astype(np.int64)).to(dev)
     # 0 = past the end, 1 + distinct symbol index otherwise
-    uniq = torch.unique(sym)
-    bits = max(1, int(uniq.numel()).bit_length())
+    uniq = np.unique(text)
+    lut = np.zeros(256, dtype=np.uint8)
+    lut[uniq] = np.arange(1, len(uniq) + 1, dtype=np.uint8)
+    bits = max(1, int(len(uniq)).bit_length())
     k = 63 // bits
-    code = torch.zeros(n + k, dtype=torch.int64, device=dev)
-    code[:n] = torch.searchsorted(uniq, sym) + 1
+    code = torch.zeros(n + k, dtype=torch.uint8, device=dev)
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        code[a:b] = torch.from_numpy(lut[text[a:b]]).to(dev)
     key = torch.zeros(n, dtype=torch.int64, device=dev)
-    for j in range(k):
-        key = (key << bits) | code[j:j + n]
-    del code, sym
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        kk = key[a:b]
+        for j in range(k):
+            kk <<= bits
+            kk |= code[a + j:b + j].to(torch.int64)
+    del code
     h = k
     sorted_key, sa = torch.sort(key)
     del key
     rank = torch.empty(n, dtype=torch.int64, device=dev)
     while True:
-        flag = torch.ones(n, dtype=torch.int64, device=dev)
-        flag[1:] = (sorted_key[1:] != sorted_key[:-1]).to(torch.int64)
-        grp = torch.cumsum(flag, 0)
-        del flag
+        # group number of each sorted position: 1 + count of key changes before it
+        grp = torch.empty(n, dtype=torch.int64, device=dev)
+        grp[0] = 1
+        for a in range(1, n, chunk):
+            b = min(n, a + chunk)
+            grp[a:b] = (sorted_key[a:b] != sorted_key[a - 1:b - 1]).to(torch.int64)
+        del sorted_key
+        torch.cumsum(grp, 0, out=grp)
         rank[sa] = grp
         ngroups = int(grp[-1].item())
-        del grp, sorted_key
+        del grp
         if ngroups == n:
             break
-        nxt = torch.zeros(n, dtype=torch.int64, device=dev)
-        if h < n:
-            nxt[: n - h] = rank[h:]
-        key = rank * (n + 1) + nxt
-        del nxt
+        # key = rank * (n + 1) + rank of the suffix h further (0 past the end)
+        key = torch.empty(n, dtype=torch.int64, device=dev)
+        for a in range(0, n, chunk):
+            b = min(n, a + chunk)
+            kk = key[a:b]
+            torch.mul(rank[a:b], n + 1, out=kk)
+            lo, hi = a + h, min(n, b + h)
+            if lo < hi:
+                kk[:hi - lo] += rank[lo:hi]
+        del sa
         sorted_key, sa = torch.sort(key)
         del key
         h *= 2
+    del rank
     return sa
 
 
@@ -93,17 +112,26 @@ def build_view(chroms, device: str | torch.device = "cpu") -> FmdView:
     text = bd_text(chroms)
     n = int(text.shape[0])
     sa_t = suffix_array(text, device)
-    text_t = torch.from_numpy(text).to(sa_t.device)
-    prev = (sa_t - 1).clamp_min(0)
-    bwt_t = torch.where(sa_t == 0, torch.zeros_like(prev, dtype=torch.uint8), text_t[prev])
-    del prev
-    rows_t = torch.nonzero((torch.arange(n, device=sa_t.device) % SA_SAMPLE_RATE == 0) | (bwt_t == 0)).flatten()
-    vals_t = sa_t[rows_t]
+    dev = sa_t.device
+    text_t = torch.from_numpy(text).to(dev)
+    chunk = 1 << 28
+    bwt = np.empty(n, dtype=np.uint8)
+    rows_l, vals_l = [], []
+    for a in range(0, n, chunk):  # BWT and the SA sample set, chunk by chunk
+        b = min(n, a + chunk)
+        s_c = sa_t[a:b]
+        bw = torch.where(s_c == 0, torch.zeros((), dtype=torch.uint8, device=dev), text_t[(s_c - 1).clamp_min(0)])
+        r = torch.nonzero((torch.arange(a, b, device=dev) % SA_SAMPLE_RATE == 0) | (bw == 0)).flatten()
+        rows_l.append((r + a).cpu().numpy().astype(np.int64))
+        vals_l.append(s_c[r].cpu().numpy().astype(np.int64))
+        bwt[a:b] = bw.cpu().numpy()
+        del s_c, bw, r
     gap_sa = sa_t[: 2 * len(chroms)].cpu().numpy().astype(np.int64)
-    bwt = bwt_t.cpu().numpy()
-    rows = rows_t.cpu().numpy().astype(np.int64)
-    vals = vals_t.cpu().numpy().astype(np.int64)
-    del sa_t, bwt_t, rows_t, vals_t, text_t
+    rows = np.concatenate(rows_l)
+    vals = np.concatenate(vals_l)
+    del sa_t, text_t
+    if torch.cuda.is_available():
+        torch.cuda.empty_cache()
     B = np.bincount(text, minlength=16).astype(np.int64)[:16]
     lens = np.array([len(s) for s in chroms], dtype=np.int64)
     span = 2 * (lens + 1)

@@ -12,6 +12,8 @@ Workloads:
   * scale: 200 genomes with log-normal lengths (median 3 Mbp, sigma 0.5,
     ~600 Mbp total), per-genome GC uniform in 30-70%; paired 2x150 bp reads,
     fragment ~ Normal(400, 50), same error model, plus 5% random pairs.
+  * repeats: two metagenomes of ~750 Mbp each (repeat_metagenome: 10% of
+    the sequence in repeat families), indexed together; reads as for scale.
 """
 from __future__ import annotations
 
@@ -56,6 +58,46 @@ def scale_genomes(seed: int = 2, n_genomes: int = 200, median: float = 3e6, sigm
     lens = np.maximum(1000, np.round(median * np.exp(sigma * rng.standard_normal(n_genomes)))).astype(np.int64)
     gcs = rng.uniform(0.3, 0.7, size=n_genomes)
     return [random_genome(rng, int(l), float(g)) for l, g in zip(lens, gcs)]
+
+
+def repeat_metagenome(seed: int, total_bp: float = 750e6, median: float = 3e6, sigma: float = 0.5,
+                      repeat_frac: float = 0.10, unit_range=(500, 5001), copies_range=(10, 201),
+                      divergence_range=(0.02, 0.05)):
+    """A metagenome for the repeat-rich workload: genomes with log-normal
+    lengths (median, sigma) adding up to about total_bp, per-genome GC
+    uniform in 30-70%, of which repeat_frac of the sequence is overwritten by
+    repeat families -- units of U{500..5000} bp, each copied U{10..200} times
+    to uniformly chosen places of the metagenome, on either strand, every
+    copy with its own substitution divergence U(2%, 5%). Copies of one
+    family land in different genomes, so SMEMs in repeats have many
+    occurrences."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    mean_len = median * np.exp(sigma * sigma / 2.0)
+    n_genomes = max(1, int(round(total_bp / mean_len)))
+    lens = np.maximum(10_000, np.round(median * np.exp(sigma * rng.standard_normal(n_genomes)))).astype(np.int64)
+    gcs = rng.uniform(0.3, 0.7, size=n_genomes)
+    genomes = [random_genome(rng, int(l), float(g)) for l, g in zip(lens, gcs)]
+    ends = np.cumsum(lens)
+    budget = int(repeat_frac * ends[-1])
+    while budget > 0:
+        ul = int(rng.integers(*unit_range))
+        unit = _BASES[rng.integers(0, 4, size=ul)]
+        for _ in range(int(rng.integers(*copies_range))):
+            if budget <= 0:
+                break
+            gi = int(np.searchsorted(ends, rng.integers(0, ends[-1]), side="right"))
+            g = genomes[gi]
+            if len(g) <= ul:
+                continue
+            cp = unit.copy()
+            m = rng.random(ul) < rng.uniform(*divergence_range)
+            cp[m] = _BASES[(np.searchsorted(_BASES, cp[m]) + rng.integers(1, 4, size=int(m.sum()))) % 4]
+            if rng.random() < 0.5:
+                cp = revcom(cp)
+            at = int(rng.integers(0, len(g) - ul))
+            g[at:at + ul] = cp
+            budget -= ul
+    return genomes
 
 
 def _indel_read(rng, win: np.ndarray, L: int, n_ev: int) -> np.ndarray:
