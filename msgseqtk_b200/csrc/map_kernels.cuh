@@ -907,10 +907,20 @@ struct ChainCtx {
             }
             uint8_t* code = g.code + (int64_t)sp * C * K;
             const bool last = sp == nsp - 1;
+            // the row above and the target base of a column are loaded one
+            // column ahead, so that their latency overlaps a column's cells
+            auto up_of = [&](int c) -> int4 {
+                return (!BANDED || (c >= plo && c <= phi)) ? rb4[c] : make_int4(NEG, NEG, NEG, 0);
+            };
+            int4 up_next = up_of(clo);
+            int tb_next = tb(g.c0 + clo);
             for (int cc = clo; cc <= chi; ++cc) {
-                int4 up = make_int4(NEG, NEG, NEG, 0);
-                if (!BANDED || (cc >= plo && cc <= phi)) up = rb4[cc];
-                const uint32_t tm = stab[(tb(g.c0 + cc) & 15) * kStripeThreads];
+                const int4 up = up_next;
+                const uint32_t tm = stab[(tb_next & 15) * kStripeThreads];
+                if (cc < chi) {
+                    up_next = up_of(cc + 1);
+                    tb_next = tb(g.c0 + cc + 1);
+                }
                 const int64_t j = g.c0 + 1 + cc;
                 int32_t uM = up.x, uI = up.y;
                 uint32_t wd[K / 4];
