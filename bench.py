@@ -582,6 +582,11 @@ def main():
     dp_shape = ctx.autotune(reads.seqs[:reads.offs[ns]], reads.offs[:ns + 1], params)
     dp_shape["sample_reads"] = ns
 
+    def offs_sb(first, count):
+        """Device offsets of reads first .. first + count, rebased to 0."""
+        o = reads.offs[first:first + count + 1]
+        return torch.from_numpy(o - o[0]).cuda()
+
     def run_device(k, prm):
         base = int(reads.offs[k * bp])
         return ctx.map_device(d_seq.data_ptr() + base, offs_d[k].data_ptr(), len(offs_d[k]) - 1, prm)
@@ -620,6 +625,27 @@ def main():
     ms_p, reads_p, agg_p, _ = timed(plain_params)
     ms, total_reads, agg, clk = timed(params, Clocks(local))
     value = total_reads / (ms / 1000.0)
+
+    # the same path in batches of 50 k reads (an interactive caller's batch
+    # size): fixed per-batch costs show against the 1 M-read batches above
+    small_batch = None
+    if args.workload in ("scale", "repeats"):
+        sb = 50_000
+        n_sb = min(40, max(1, bp // sb))
+        for s in range(3):
+            ctx.map_device(d_seq.data_ptr() + int(reads.offs[s * sb]), offs_sb(s * sb, sb).data_ptr(), sb, params)
+        torch.cuda.synchronize()
+        sb_offs = [offs_sb((3 + s) * sb, sb) for s in range(n_sb)]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for s in range(n_sb):
+            ctx.map_device(d_seq.data_ptr() + int(reads.offs[(3 + s) * sb]), sb_offs[s].data_ptr(), sb, params)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sb_value = n_sb * sb / (e0.elapsed_time(e1) / 1000.0)
+        small_batch = {"value": sb_value, "unit": "reads/s", "batch_reads": sb, "batches": n_sb,
+                       "fraction_of_value": sb_value / value}
     banded = agg["n_band_exact"] + agg["n_band_drop"] + agg["n_band_fallback"]
 
     def gcups(a):
@@ -808,7 +834,7 @@ def main():
                            "parallelism": f"dp{world}" if world > 1 else "single GPU"},
                 "gcups": gcups(agg), "plain_gpu": plain, "learned_band": band_info,
                 "e2e": e2e, "e2e_sam": e2e_sam, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
-                "gpu_launches": agg["n_launch"], "validation": valid, "setup": setup, "tuned_shapes": dp_shape,
+                "gpu_launches": agg["n_launch"], "validation": valid, "setup": setup, "tuned_shapes": dp_shape, "small_batch": small_batch,
                 "stats": {k: agg[k] for k in counters}}
         print(json.dumps(line), flush=True)
     ctx.close()
