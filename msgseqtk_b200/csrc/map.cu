@@ -200,29 +200,29 @@ cudaError_t dp_sort(msg_ctx* ctx, int64_t c0, int64_t n, const int4* geo, const 
 }
 
 template <int K>
-void launch_stripe(msg_ctx* ctx, const DpArgs& a, bool band, int64_t n_max) {
+void launch_stripe(msg_ctx* ctx, const DpArgs& a, bool band, int64_t n_max, cudaStream_t st) {
     const int g = (int)std::min<int64_t>(nblk(n_max, kStripeThreads), (int64_t)ctx->num_sms * 16);
-    if (band) k_dp_stripe<K, true><<<g, kStripeThreads, 0, ctx->stream>>>(a);
-    else k_dp_stripe<K, false><<<g, kStripeThreads, 0, ctx->stream>>>(a);
+    if (band) k_dp_stripe<K, true><<<g, kStripeThreads, 0, st>>>(a);
+    else k_dp_stripe<K, false><<<g, kStripeThreads, 0, st>>>(a);
 }
 
 // One DP launch: over class `cls` of the class-sorted list a.list when
 // cls >= 0; with cls < 0 over a.list[0 .. *a.n_list) with the kernel of class
 // -cls - 1 (the fallback recomputations). n_max bounds the chains it may get;
 // the kernels loop over their chains (grid-stride).
-void launch_dp(msg_ctx* ctx, DpArgs a, int cls, int64_t n_max, msg_map_stats& S) {
+void launch_dp(msg_ctx* ctx, DpArgs a, int cls, int64_t n_max, msg_map_stats& S, cudaStream_t st = nullptr) {
     const int kind = cls >= 0 ? cls : -cls - 1;
     a.cls = cls >= 0 ? cls : -1;
-    cudaStream_t st = ctx->stream;
+    if (!st) st = ctx->stream;
     S.n_launch++;
     if (kind == kDpSmall) {
         const int g = (int)std::min<int64_t>(nblk(n_max, 128), (int64_t)ctx->num_sms * 16);
         k_dp_small<<<g, 128, 0, st>>>(a);
     } else if (kind == kDpStripe || kind == kDpStripeBand) {
         const bool band = kind == kDpStripeBand;
-        if (ctx->dp_k == 8) launch_stripe<8>(ctx, a, band, n_max);
-        else if (ctx->dp_k == 32) launch_stripe<32>(ctx, a, band, n_max);
-        else launch_stripe<16>(ctx, a, band, n_max);
+        if (ctx->dp_k == 8) launch_stripe<8>(ctx, a, band, n_max, st);
+        else if (ctx->dp_k == 32) launch_stripe<32>(ctx, a, band, n_max, st);
+        else launch_stripe<16>(ctx, a, band, n_max, st);
     } else {
         const int g = (int)std::min<int64_t>(nblk(n_max * 32, kDpWarps * 32), (int64_t)ctx->num_sms * 12);
         if (kind == kDpWarpBand) k_dp<true><<<g, kDpWarps * 32, 0, st>>>(a);
@@ -922,23 +922,37 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         da.list = d_sorted;
         // Every launch is sized for the range; each reads its class's part of
         // the sorted list on the device, so no host round trip is needed.
+        // The classes run side by side: row-by-row, stripe and banded-stripe
+        // launches on three streams forked from the context's, the warp
+        // launches on the context's own; a launch's last blocks (its largest
+        // chains) then overlap the other launches' work. Chains of different
+        // classes touch disjoint storage.
+        CK(ctx->dp_streams_ready());
+        CK(cudaEventRecord(ctx->dp_ev[0], st));
+        for (int q = 0; q < 3; ++q) CK(cudaStreamWaitEvent(ctx->dp_side[q], ctx->dp_ev[0], 0));
         da.fb_list = d_fb; da.fb_n = d_ctr2 + kCtrFbStripe;
-        launch_dp(ctx, da, kDpSmall, nch, S);
-        launch_dp(ctx, da, kDpStripe, nch, S);
+        launch_dp(ctx, da, kDpSmall, nch, S, ctx->dp_side[0]);
+        launch_dp(ctx, da, kDpStripe, nch, S, ctx->dp_side[1]);
         launch_dp(ctx, da, kDpWarp, nch, S);
         if (bmode != 0) {
-            launch_dp(ctx, da, kDpStripeBand, nch, S);
+            launch_dp(ctx, da, kDpStripeBand, nch, S, ctx->dp_side[2]);
             da.fb_list = d_fbw; da.fb_n = d_ctr2 + kCtrFbWarp;
             launch_dp(ctx, da, kDpWarpBand, nch, S);
             // banded chains without a certificate, on the whole cell set: few
             // chains, mostly large, so a warp each (a thread each would leave
-            // the launch waiting on its largest chain)
+            // the launch waiting on its largest chain); each after the launch
+            // that lists them, on its stream
             DpArgs fb = da;
             fb.band = nullptr;
             fb.list = d_fb; fb.n_list = d_ctr2 + kCtrFbStripe;
-            launch_dp(ctx, fb, -kDpWarp - 1, nch, S);
+            launch_dp(ctx, fb, -kDpWarp - 1, nch, S, ctx->dp_side[2]);
             fb.list = d_fbw; fb.n_list = d_ctr2 + kCtrFbWarp;
             launch_dp(ctx, fb, -kDpWarp - 1, nch, S);
+        }
+        CK(cudaGetLastError());
+        for (int q = 0; q < 3; ++q) {
+            CK(cudaEventRecord(ctx->dp_ev[1 + q], ctx->dp_side[q]));
+            CK(cudaStreamWaitEvent(st, ctx->dp_ev[1 + q], 0));
         }
         S.n_launch++, k_traceback<<<nblk(nch, 128), 128, 0, st>>>(da);
         CK(cudaGetLastError());

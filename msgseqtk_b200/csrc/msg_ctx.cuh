@@ -98,6 +98,21 @@ struct msg_ctx {
     int64_t dp_warp_area = 65536;
     cudaEvent_t ev[8];
     int64_t* hpin = nullptr;  // pinned host words for counts copied back without extra waits
+    // DP class launches side by side: three streams forked from `stream`
+    cudaStream_t dp_side[3] = {};
+    cudaEvent_t dp_ev[4] = {};
+    cudaError_t dp_streams_ready() {
+        if (dp_side[0]) return cudaSuccess;
+        for (auto& s : dp_side) {
+            const cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+            if (e != cudaSuccess) return e;
+        }
+        for (auto& e : dp_ev) {
+            const cudaError_t r = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+            if (r != cudaSuccess) return r;
+        }
+        return cudaSuccess;
+    }
     const msg_aln* res_aln = nullptr;
     const uint32_t* res_cigar = nullptr;
     const int64_t* res_off = nullptr;
@@ -122,6 +137,8 @@ struct msg_ctx {
             cudaStreamDestroy(cstream);
             cstream = nullptr;
         }
+        for (auto& s : dp_side) if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); s = nullptr; }
+        for (auto& e : dp_ev) if (e) { cudaEventDestroy(e); e = nullptr; }
     }
     void index_free() {
         if (idx.bkt) cudaFree(idx.bkt);
