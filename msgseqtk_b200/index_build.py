@@ -76,7 +76,6 @@ def suffix_array(text: np.ndarray, device: str | torch.device = "cpu", chunk: in
     h = k
     sorted_key, sa = torch.sort(key)
     del key
-    rank = torch.empty(n, dtype=torch.int64, device=dev)
     while True:
         # group number of each sorted position: 1 + count of key changes before it
         grp = torch.empty(n, dtype=torch.int64, device=dev)
@@ -86,12 +85,14 @@ def suffix_array(text: np.ndarray, device: str | torch.device = "cpu", chunk: in
             grp[a:b] = (sorted_key[a:b] != sorted_key[a - 1:b - 1]).to(torch.int64)
         del sorted_key
         torch.cumsum(grp, 0, out=grp)
+        rank = torch.empty(n, dtype=torch.int64, device=dev)
         rank[sa] = grp
         ngroups = int(grp[-1].item())
         del grp
         if ngroups == n:
             break
         # key = rank * (n + 1) + rank of the suffix h further (0 past the end)
+        del sa
         key = torch.empty(n, dtype=torch.int64, device=dev)
         for a in range(0, n, chunk):
             b = min(n, a + chunk)
@@ -100,7 +101,9 @@ def suffix_array(text: np.ndarray, device: str | torch.device = "cpu", chunk: in
             lo, hi = a + h, min(n, b + h)
             if lo < hi:
                 kk[:hi - lo] += rank[lo:hi]
-        del sa
+        del rank  # rebuilt from the sorted keys; only key and the sort's buffers live during the sort
+        if dev.type == "cuda":
+            torch.cuda.empty_cache()
         sorted_key, sa = torch.sort(key)
         del key
         h *= 2
