@@ -42,6 +42,7 @@
 #include "Alignment.h"
 #include "ProgEnv.h"
 #include "SeqIO.h"
+#include "from_device.h"
 #undef private
 #undef protected
 
@@ -630,43 +631,17 @@ int64_t ref_sam_batch(void* h, int64_t n_reads, const uint8_t* reads, const uint
     return put_out(text, out, cap);
 }
 
-struct RecAln {  // msg_aln (include/msg_b200.h), 88 bytes
-    int64_t read; int32_t tid, strand; int64_t t_start, t_end, aln_from, aln_to, aln_start, aln_end;
-    int32_t aln_score, flags; int64_t cigar_off; int32_t n_cigar, pad;
-};
-static_assert(sizeof(RecAln) == 88, "msg_aln layout");
+static_assert(sizeof(msg_aln) == 88, "msg_aln layout");
 
-/* The alignments of records k0..k1 of the CUDA library: each record sets the
- * fields buildAlignments would set (Alignment.h:357-375), the path is the
- * CIGAR's M/I/D runs (soft clips are alnFrom/alnTo). */
+/* The alignments of records k0..k1 of the CUDA library, through the adapter
+ * a maintainer adds to the reference (from_device.h). */
 static ALIGN_LIST records_to_alignments(RefDB* db, const PrimarySeq* r, const PrimarySeq* rc, int64_t L,
                                         const void* records, const uint32_t* cigar, int64_t k0, int64_t k1) {
-    const RecAln* rec = (const RecAln*)records;
+    const msg_aln* rec = (const msg_aln*)records;
     ALIGN_LIST alns;
-    for (int64_t k = k0; k < k1; ++k) {
-        const RecAln& g = rec[k];
-        Alignment a(r);
-        a.rcRead = rc;
-        a.tid = g.tid;
-        a.target = &db->mtg.getSeq(g.tid);
-        a.qStrand = (GLoc::STRAND)g.strand;
-        a.qFrom = 0;
-        a.qTo = L;
-        a.tStart = g.t_start;
-        a.tEnd = g.t_end;
-        a.alnMode = Alignment::GLOBAL;
-        a.alnFrom = g.aln_from;
-        a.alnTo = g.aln_to;
-        a.alnStart = g.aln_start;
-        a.alnEnd = g.aln_end;
-        a.alnScore = g.aln_score == INT32_MIN ? -std::numeric_limits<double>::infinity() : (double)g.aln_score;
-        for (int32_t w = 0; w < g.n_cigar; ++w) {
-            const uint32_t c = cigar[g.cigar_off + w];
-            if ((c & 0xf) == BAM_CSOFT_CLIP) continue;
-            a.alnPath.append(c >> 4, c & 0xf);
-        }
-        alns.push_back(a);
-    }
+    (void)L;
+    for (int64_t k = k0; k < k1; ++k)
+        alns.push_back(msg_adapter::fromDevice(r, rc, db->mtg, rec[k], cigar, Alignment::GLOBAL));
     return alns;
 }
 
