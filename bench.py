@@ -576,9 +576,11 @@ def main():
               for k in range(n_batches)]
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
 
-    # the library's autotuner picks the SMEM and DP kernel shapes on a sample
-    # of the first batch (untimed; records do not depend on the shapes)
-    ns = min(200_000, bp, len(reads))
+    # the library's autotuner picks the SMEM and DP kernel shapes on the
+    # first batch, whole (untimed; records do not depend on the shapes; a
+    # smaller sample leaves the DP launches too short to rank the shapes as
+    # the full batch does)
+    ns = min(bp, len(reads))
     dp_shape = ctx.autotune(reads.seqs[:reads.offs[ns]], reads.offs[:ns + 1], params)
     dp_shape["sample_reads"] = ns
 

@@ -740,6 +740,40 @@ struct ChainCtx {
         return make_int2(M(i, j, stage), D(i, j, stage));
     }
 
+    // M, I, D of a boundary cell (top row or left column) of rectangle m,
+    // with closed forms for the two common cases and the region rule for the
+    // rest:
+    //  * the 5' rectangle (m == 0): no region is written before it, so its
+    //    boundary holds the initialised matrices (initNW/initSW,
+    //    Alignment.h:599-613): row 0 M = 0 (I(0,0) = 0 in NW); column 0
+    //    I = -gapPenalty(i) in NW, M = 0 in SW; the rest -inf;
+    //  * the 3' rectangle of a one-seed chain (m == 2): its top row is the
+    //    seed's last row qt and its left column the seed's last column te;
+    //    every cell there is -inf but the seed's last diagonal cell (qt, te)
+    //    with M = E (the seed's final diagonal value), D(qt, te + 1) =
+    //    E + o from the whole-column overwrite and I(qt + 1, te) = E + o
+    //    from the whole-row overwrite (Alignment.cpp:161-169).
+    // OUTLINE: the region rule through the out-of-line MID (else inlined).
+    template <bool OUTLINE = true>
+    __device__ __forceinline__ int3 boundary(int m, int64_t i, int64_t j) const {
+        if (m == 0) {
+            const bool nw = pp.mode == 0;
+            if (i == 0) return make_int3(0, (nw && j == 0) ? 0 : NEG, NEG);
+            return make_int3(nw ? NEG : 0, nw ? -(pp.gap_o + pp.gap_e * (int32_t)i) : NEG, NEG);  // j == 0
+        }
+        if (m == 2 && n == 1) {
+            const int64_t q1 = qt(0), t1 = te(0);
+            const int32_t E = diag[0] + (int32_t)(q1 - qf(0) - 1) * pp.match;
+            const int32_t Eo = sat_add(E, -(pp.gap_o + pp.gap_e));
+            if (i == q1 && j == t1) return make_int3(E, NEG, NEG);
+            if (i == q1 && j == t1 + 1) return make_int3(NEG, NEG, Eo);
+            if (j == t1 && i == q1 + 1) return make_int3(NEG, Eo, NEG);
+            return make_int3(NEG, NEG, NEG);
+        }
+        if constexpr (OUTLINE) return MID(i, j, m);
+        else return make_int3(M(i, j, m), I(i, j, m), D(i, j, m));
+    }
+
     // Single-thread fill of rectangle m, row by row, into the same code layout
     // (rowbuf holds the row above). With w >= 0 only the cells within w
     // diagonals of the adjacent seed's diagonal are computed (the 5' rectangle
@@ -759,10 +793,10 @@ struct ChainCtx {
         int64_t plo = 0, phi = g.C - 1;  // columns of the row above held in rowbuf
         if (banded) { plo = max((int64_t)0, dg - w - 1); phi = min(g.C - 1, dg + w); }
         for (int64_t c = plo; c <= phi; ++c) {  // the top boundary row
-            const int64_t j = g.c0 + 1 + c;
-            g.rowbuf[c * 3] = M(g.r0, j, m);
-            g.rowbuf[c * 3 + 1] = I(g.r0, j, m);
-            g.rowbuf[c * 3 + 2] = D(g.r0, j, m);
+            const int3 v = boundary<false>(m, g.r0, g.c0 + 1 + c);
+            g.rowbuf[c * 3] = v.x;
+            g.rowbuf[c * 3 + 1] = v.y;
+            g.rowbuf[c * 3 + 2] = v.z;
         }
         int64_t cells = 0;
         int64_t lrow = -1;         // matrix row whose left boundary cell (lrow, c0) is cached
@@ -775,8 +809,9 @@ struct ChainCtx {
             int32_t ml = NEG, dl = NEG, dm = NEG, di = NEG, dd = NEG;
             if (lo == 0) {
                 if (lrow == i - 1) { dm = lm; di = li; dd = ld; }
-                else { dm = M(i - 1, g.c0, m); di = I(i - 1, g.c0, m); dd = D(i - 1, g.c0, m); }
-                lm = M(i, g.c0, m); li = I(i, g.c0, m); ld = D(i, g.c0, m);
+                else { const int3 v = boundary<false>(m, i - 1, g.c0); dm = v.x; di = v.y; dd = v.z; }
+                const int3 v = boundary<false>(m, i, g.c0);
+                lm = v.x; li = v.y; ld = v.z;
                 lrow = i;
                 ml = lm; dl = ld;
             } else if (lo - 1 >= plo && lo - 1 <= phi) {
@@ -846,17 +881,13 @@ struct ChainCtx {
             for (int c = 0; c < 3 * C; ++c) g.lastrow[c] = NEG;
             for (int c = 0; c < 3 * R; ++c) g.lastcol[c] = NEG;
         }
-        // Boundary cells. The 5' rectangle's (m == 0) are those of the
-        // initialised matrices, no region having been written before it
-        // (initNW/initSW, Alignment.h:599-613): row 0 holds M = 0; column 0
-        // holds I = -gapPenalty(i) in NW and M = 0 in SW; the rest is -inf.
-        const int32_t go = pp.gap_o, ge = pp.gap_e;
-        const bool nw = pp.mode == 0;
-        auto bnd = [&](int64_t i, int64_t j) -> int3 {
-            if (m != 0) return MID(i, j, m);
-            if (i == 0) return make_int3(0, (nw && j == 0) ? 0 : NEG, NEG);
-            return make_int3(nw ? NEG : 0, nw ? -(go + ge * (int32_t)i) : NEG, NEG);  // j == 0
-        };
+        auto bnd = [&](int64_t i, int64_t j) -> int3 { return boundary(m, i, j); };
+        // the context's fields the column loop reads, in registers (the
+        // context itself lives in local memory)
+        const uint8_t* const tgt = target + g.c0;
+        const int64_t tgt_n = target_avail - g.c0;
+        uint32_t* const tab = stab;
+        const int64_t Lq = L;
         int plo = 0, phi = C - 1;  // columns of the row buffer that hold the row above
         if (BANDED) { plo = max(0, dg - w - 1); phi = min(C - 1, dg + w); }
         for (int c = plo; c <= phi; ++c) {  // the top boundary row
@@ -883,7 +914,7 @@ struct ChainCtx {
                     for (int t = 1; t < 15; ++t) tbits[t] |= (q & t) ? (1u << k) : 0u;
                 }
 #pragma unroll
-                for (int t = 0; t < 16; ++t) stab[t * kStripeThreads] = tbits[t];
+                for (int t = 0; t < 16; ++t) tab[t * kStripeThreads] = tbits[t];
             }
             // the previous column's values of the stripe's rows: the left
             // boundary (column c0) when the stripe starts at column 0
@@ -912,14 +943,15 @@ struct ChainCtx {
             auto up_of = [&](int c) -> int4 {
                 return (!BANDED || (c >= plo && c <= phi)) ? rb4[c] : make_int4(NEG, NEG, NEG, 0);
             };
+            auto tbase = [&](int c) -> int { return c < tgt_n ? (int)__ldg(tgt + c) : 0; };
             int4 up_next = up_of(clo);
-            int tb_next = tb(g.c0 + clo);
+            int tb_next = tbase(clo);
             for (int cc = clo; cc <= chi; ++cc) {
                 const int4 up = up_next;
-                const uint32_t tm = stab[(tb_next & 15) * kStripeThreads];
+                const uint32_t tm = tab[(tb_next & 15) * kStripeThreads];
                 if (cc < chi) {
                     up_next = up_of(cc + 1);
-                    tb_next = tb(g.c0 + cc + 1);
+                    tb_next = tbase(cc + 1);
                 }
                 const int64_t j = g.c0 + 1 + cc;
                 int32_t uM = up.x, uI = up.y;
@@ -945,7 +977,7 @@ struct ChainCtx {
                         if ((unsigned)(cc - (rr0 + k) - dg + w) > (unsigned)(2 * w)) { mv = NEG; iv = NEG; dv = NEG; }
                     }
                     if (LOCAL && k < nrow) {
-                        const int64_t key = j * (L + 1) + (i0 + k);
+                        const int64_t key = j * (Lq + 1) + (i0 + k);
                         if (mv > best || (mv == best && key < bkey)) { best = mv; bkey = key; }
                     }
                     wd[k >> 2] |= cd << (8 * (k & 3));
@@ -1337,9 +1369,10 @@ __global__ void k_dp_prep(IndexDev ix, const Seed* __restrict__ seeds, const int
 // Traceback of one chain (Alignment::backTraceNW/SW, Alignment.cpp:173-276)
 // from the end cell (aln_to, aln_end) in state s0, writing the reversed path
 // and the alignment record.
-__device__ __forceinline__ void dp_traceback(const DpArgs& a, int64_t c, const ChainCtx& x, int64_t r, const Seed& f,
+__device__ __forceinline__ void dp_traceback(const DpArgs& a, int64_t c, const ChainCtx& xc, int64_t r, const Seed& f,
                                              int64_t t_start, int64_t aln_to, int64_t aln_end, int s0, int32_t best,
                                              int32_t flags) {
+    const ChainCtx x = xc;  // a copy of its own, which registers can hold (the caller's lives in memory)
     const int stage = 2 * x.n + 2;
     uint8_t* path = a.path + a.path_off[c];
     const int32_t go = a.pp.gap_o, ge = a.pp.gap_e;
@@ -1657,17 +1690,20 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
         aln_end = bkey / (x.L + 1);
         s0 = OP_M;
     }
-    if constexpr (WARP) {
+    if constexpr (WARP || KST > 0) {
         // Hand the start of the traceback to k_traceback (one thread per
         // chain): the record carries the end cell, the score and flags, and
-        // `pad` the starting state.
+        // `pad` the starting state (bits 0-7) and the stripe height of the
+        // code layout (bits 8-15). A stripe chain's thread leaves the serial
+        // walk to that launch too: the fill kernel then holds no traceback
+        // code, and its next chain starts at once.
         if (lane == 0) {
             msg_aln& o = a.aln[c];
             o.aln_to = aln_to;
             o.aln_end = aln_end;
             o.aln_score = best;
             o.flags = flags;
-            o.pad = s0;
+            o.pad = s0 | (KST << 8);
             a.tb_list[atomicAdd(a.tb_n, 1ull)] = c;
         }
     } else {
@@ -1726,7 +1762,7 @@ __global__ void __launch_bounds__(128) k_dp_small(DpArgs a) {
 }
 
 // Mid-size chains: one thread each, rectangles in register stripes of K rows
-// (fill_rect_stripe), traceback in the same thread. BAND: chains with a
+// (fill_rect_stripe); k_traceback walks them back. BAND: chains with a
 // banded flank.
 template <int K, bool BAND>
 __global__ void __launch_bounds__(kStripeThreads, 4) k_dp_stripe(DpArgs a) {
@@ -1743,8 +1779,9 @@ __global__ void __launch_bounds__(kStripeThreads, 4) k_dp_stripe(DpArgs a) {
     }
 }
 
-// Tracebacks of the chains filled by the warp kernels, one thread each (a
-// traceback is a serial walk; a warp per chain would leave 31 lanes idle).
+// Tracebacks of the chains filled by the warp and stripe kernels, one thread
+// each (a traceback is a serial walk; a warp per chain would leave 31 lanes
+// idle).
 __global__ void __launch_bounds__(128, 6) k_traceback(DpArgs a) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t >= (int64_t)*a.tb_n) return;
@@ -1772,7 +1809,8 @@ __global__ void __launch_bounds__(128, 6) k_traceback(DpArgs a) {
     x.rd = a.rseq + a.roff[r];
     x.rev = f.strand != FWD;
     const msg_aln h = a.aln[c];
-    dp_traceback(a, c, x, r, f, t_start, h.aln_to, h.aln_end, h.pad, h.aln_score, h.flags);
+    x.kst = h.pad >> 8;
+    dp_traceback(a, c, x, r, f, t_start, h.aln_to, h.aln_end, h.pad & 0xff, h.aln_score, h.flags);
 }
 
 // CIGAR runs (Alignment::getAlnCigar): 5' clip, the reversed path in runs, 3' clip.
