@@ -631,23 +631,27 @@ def main():
     # the same path in batches of 50 k reads (an interactive caller's batch
     # size): fixed per-batch costs show against the 1 M-read batches above
     small_batch = None
-    if args.workload in ("scale", "repeats"):
-        sb = 50_000
-        n_sb = min(40, max(1, bp // sb))
+    sb = 50_000
+    n_sb = min(40, bp // sb, len(reads) // sb - 3)  # 3 untimed batches first
+    if args.workload in ("scale", "repeats") and n_sb >= 1:
         for s in range(3):
             ctx.map_device(d_seq.data_ptr() + int(reads.offs[s * sb]), offs_sb(s * sb, sb).data_ptr(), sb, params)
         torch.cuda.synchronize()
         sb_offs = [offs_sb((3 + s) * sb, sb) for s in range(n_sb)]
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
+        sb_stage = {"smem": 0.0, "locate": 0.0, "chain": 0.0, "dp": 0.0, "total": 0.0}
         e0.record(stream)
         for s in range(n_sb):
             ctx.map_device(d_seq.data_ptr() + int(reads.offs[(3 + s) * sb]), sb_offs[s].data_ptr(), sb, params)
+            st = ctx.stats()
+            for k in ("smem", "locate", "chain", "dp", "total"):
+                sb_stage[k] += st["ms_" + k] / n_sb
         e1.record(stream)
         torch.cuda.synchronize()
         sb_value = n_sb * sb / (e0.elapsed_time(e1) / 1000.0)
         small_batch = {"value": sb_value, "unit": "reads/s", "batch_reads": sb, "batches": n_sb,
-                       "fraction_of_value": sb_value / value}
+                       "fraction_of_value": sb_value / value, "stage_ms_per_batch": sb_stage}
     banded = agg["n_band_exact"] + agg["n_band_drop"] + agg["n_band_fallback"]
 
     def gcups(a):

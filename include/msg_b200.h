@@ -310,8 +310,11 @@ int msg_ctx_set_dp_shape(msg_ctx* ctx, int32_t stripe_rows, int64_t small_area, 
 /* Kernel shape of the SMEM stage for reads up to 254 bp (no reference
  * counterpart): 0 = one read per thread (default); 1 and 2 = two reads per
  * thread, each thread keeping two extensions' bucket loads in flight (1:
- * registers sized for 4 blocks of 128 threads per SM, 2: for 3). Results do
- * not depend on it. */
+ * registers sized for 4 blocks of 128 threads per SM, 2: for 3); 3 and 4 =
+ * one read per thread, the candidates of one pass of findFwdBackSMEMS /
+ * findBackFwdSMEMS (SMEM.cpp:93-116, 148-171) extended up to 4 (3) or 2 (4)
+ * at a time, their bucket loads in flight together. Results do not depend
+ * on it. */
 int msg_ctx_set_smem_shape(msg_ctx* ctx, int32_t variant);
 
 /* The shapes chosen by msg_autotune, with the stage times that chose them. */

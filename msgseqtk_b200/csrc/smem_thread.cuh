@@ -236,6 +236,27 @@ __device__ __forceinline__ void smem_push(ThreadSmem& t, const SmemThreadArgs& a
     }
 }
 
+// One entry of a pass over prev (SMEM.cpp:97-112 (fb) / 152-167 (bf)): e0 is
+// the entry before its extension, (P, Q, S) the extension's result.
+__device__ __forceinline__ void smem_apply_entry(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv,
+                                                 const PrevEntry& e0, uint32_t P, uint32_t Q, uint32_t S) {
+    const bool fb = t.fb;
+    PrevEntry e = e0;
+    e.p = P; e.q = Q; e.s = S;
+    const bool add = fb ? (t.cf > 0) : (t.ct < t.L);
+    if (add) e.lp = __dadd_rn(e.lp, s_llk[t.b2]);
+    const int32_t e_from = fb ? t.cf : e0.pos;
+    const int32_t e_to = fb ? e0.pos : t.ct;
+    if (e.s != e0.s && e0.s >= 1 && t.n_valid == 0 && e_to - e_from >= a.min_len && (a.thr_all || e0.lp <= a.thr))
+        smem_emit(t, a, e_from, e_to, fb ? e0.p : e0.q, fb ? e0.q : e0.p, e0.s, e0.lp);
+    if (e.s >= 1 && e.s != t.s0) {
+        t.s0 = e.s;
+        t.n_valid++;
+        pv[t.pv_base + t.n_keep++] = e;
+    }
+    t.k++;
+}
+
 // Apply the result of the extension requested by smem_advance.
 __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, uint32_t P, uint32_t Q,
                                            uint32_t S) {
@@ -254,23 +275,8 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
                 smem_push(t, a, pv, fb ? t0 : f0);
         }
         t.wp0 = t.wp; t.wq0 = t.wq; t.s0w = t.s; t.lp0 = t.lp;
-    } else if (t.phase == PH_ENTRY) {  // SMEM.cpp:97-112 (fb) / 152-167 (bf)
-        const bool fb = t.fb;
-        PrevEntry e = t.e0;
-        e.p = P; e.q = Q; e.s = S;
-        const bool add = fb ? (t.cf > 0) : (t.ct < t.L);
-        if (add) e.lp = __dadd_rn(e.lp, s_llk[t.b2]);
-        const int32_t e_from = fb ? t.cf : t.e0.pos;
-        const int32_t e_to = fb ? t.e0.pos : t.ct;
-        if (e.s != t.e0.s && t.e0.s >= 1 && t.n_valid == 0 && e_to - e_from >= a.min_len &&
-            (a.thr_all || t.e0.lp <= a.thr))
-            smem_emit(t, a, e_from, e_to, fb ? t.e0.p : t.e0.q, fb ? t.e0.q : t.e0.p, t.e0.s, t.e0.lp);
-        if (e.s >= 1 && e.s != t.s0) {
-            t.s0 = e.s;
-            t.n_valid++;
-            pv[t.pv_base + t.n_keep++] = e;
-        }
-        t.k++;
+    } else if (t.phase == PH_ENTRY) {
+        smem_apply_entry(t, a, pv, t.e0, P, Q, S);
     }
 }
 
@@ -394,6 +400,126 @@ __global__ void __launch_bounds__(128, MINB) k_smem_thread2(SmemThreadArgs a, In
     }
     const unsigned long long e = t[0].ext + t[1].ext;
     if (e) atomicAdd(a.n_ext, e);
+}
+
+// 16 bytes from global to shared memory without passing through registers
+// (cp.async: the copy is in flight until cp_async_wait_all).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// One read per thread, like k_smem_thread, but a step of a pass over the
+// candidate list extends up to NB entries at once: the entries of one pass
+// are independent (each is extended by the same base; only the bookkeeping
+// after each extension -- running size, emission, compaction -- is ordered),
+// so their bucket loads are issued together and their results applied in
+// list order afterwards. The buckets land in shared memory (cp.async), four
+// 16-byte words per extension at [4 j + w][thread], so a thread holds no
+// registers for the loads in flight. The walks stay one extension per step
+// (each depends on the previous). Same per-read results as k_smem_thread.
+// MINB: resident blocks of 128 threads per SM the registers are sized for.
+template <int NB, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_smem_pass(SmemThreadArgs a, IndexDev ix) {
+    __shared__ uint4 s_bk[NB * 4][128];
+    if (threadIdx.x < 16) s_llk[threadIdx.x] = a.llk[threadIdx.x];
+    __syncthreads();
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int x = threadIdx.x;
+    PrevEntry* pv = a.prev + tid * a.pv_cap;
+    ThreadSmem t;
+    t.phase = PH_NEXT_READ;
+    t.ext = 0;
+    t.n_out = 0;
+    t.r = -1;
+    bool alive = true;
+    for (;;) {
+        uint32_t P = 0, Q = 0, S = 0;
+        int B = 0;
+        bool have = false;
+        while (alive && !have) {
+            if (t.phase == PH_NEXT_READ || t.phase == PH_DONE) {
+                alive = smem_next_read(t, a, ix);
+                continue;
+            }
+            have = smem_advance(t, a, ix, pv, P, Q, S, B);
+        }
+        __syncwarp();
+        if (!__any_sync(0xffffffffu, alive)) break;
+        // this step's extensions: the walk's one, or entries k .. k+nb-1 of a pass
+        // (entries 1.. keep only p and s in registers; they are read whole
+        // again when applied: the batch writes only positions below them)
+        int nb = 0;
+        uint32_t Ep[NB], Es[NB];
+        Ep[0] = P; Es[0] = S;
+        if (have) {
+            nb = 1;
+            if (t.phase == PH_ENTRY) {
+                nb = min(NB, t.n_prev - t.k);
+#pragma unroll
+                for (int j = 1; j < NB; ++j) {
+                    if (j < nb) {
+                        const PrevEntry& e = j == 1 ? t.e_next : pv[t.pv_base + t.k + j];
+                        Ep[j] = e.p;
+                        Es[j] = e.s;
+                    }
+                }
+            }
+        }
+        const bool basic = is_basic(B);
+        if (basic) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                if (j < nb) {
+                    const uint32_t p = Ep[j], sz = Es[j];
+                    const uint32_t ka = p >> 6, kb = (p + sz) >> 6;
+                    const uint4* ga = reinterpret_cast<const uint4*>(ix.bkt + ka);
+                    cp_async16(&s_bk[4 * j][x], ga);
+                    cp_async16(&s_bk[4 * j + 1][x], ga + 1);
+                    if (kb != ka) {
+                        const uint4* gb = reinterpret_cast<const uint4*>(ix.bkt + kb);
+                        cp_async16(&s_bk[4 * j + 2][x], gb);
+                        cp_async16(&s_bk[4 * j + 3][x], gb + 1);
+                    }
+                }
+            }
+        }
+        cp_async_wait_all();
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            if (j < nb) {
+                const bool entry = t.phase == PH_ENTRY;
+                const PrevEntry e0 = !entry ? PrevEntry{} : j == 0 ? t.e0 : pv[t.pv_base + t.k];
+                uint32_t p = Ep[j], q = j == 0 ? Q : e0.q, sz = Es[j];
+                if (basic) {
+                    t.ext++;
+                    ExtLoad l;
+                    l.a0 = s_bk[4 * j][x];
+                    l.a1 = s_bk[4 * j + 1][x];
+                    if (((p + sz) >> 6) != (p >> 6)) {
+                        l.b0 = s_bk[4 * j + 2][x];
+                        l.b1 = s_bk[4 * j + 3][x];
+                    } else {
+                        l.b0 = l.a0;
+                        l.b1 = l.a1;
+                    }
+                    back_ext32_apply(ix, p, q, sz, B, l);
+                } else {
+                    sz = 0;
+                }
+                if (entry) smem_apply_entry(t, a, pv, e0, p, q, sz);
+                else smem_apply(t, a, pv, p, q, sz);
+            }
+        }
+        // the entry after the batch, for the next step (the batch wrote only
+        // positions below it)
+        if (have && t.phase == PH_ENTRY && nb > 1 && t.k < t.n_prev) t.e_next = pv[t.pv_base + t.k];
+    }
+    if (t.ext) atomicAdd(a.n_ext, t.ext);
 }
 
 }  // namespace msg
