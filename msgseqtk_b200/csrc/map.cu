@@ -199,25 +199,36 @@ cudaError_t dp_sort(msg_ctx* ctx, int64_t c0, int64_t n, const int4* geo, const 
     return e;
 }
 
+// Blocks of a thread-per-chain DP launch: as many as are resident at once
+// (the warps take chains from the launch's work counter until none is left),
+// and no more than the chains need.
+template <typename F>
+int resident_blocks(msg_ctx* ctx, F kernel, int threads, int64_t n_max) {
+    int bps = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, threads, 0) != cudaSuccess || bps < 1) bps = 1;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(nblk(n_max, threads), (int64_t)ctx->num_sms * bps));
+}
+
 template <int K>
 void launch_stripe(msg_ctx* ctx, const DpArgs& a, bool band, int64_t n_max, cudaStream_t st) {
-    const int g = (int)std::min<int64_t>(nblk(n_max, kStripeThreads), (int64_t)ctx->num_sms * 16);
-    if (band) k_dp_stripe<K, true><<<g, kStripeThreads, 0, st>>>(a);
-    else k_dp_stripe<K, false><<<g, kStripeThreads, 0, st>>>(a);
+    if (band) k_dp_stripe<K, true><<<resident_blocks(ctx, k_dp_stripe<K, true>, kStripeThreads, n_max), kStripeThreads, 0, st>>>(a);
+    else k_dp_stripe<K, false><<<resident_blocks(ctx, k_dp_stripe<K, false>, kStripeThreads, n_max), kStripeThreads, 0, st>>>(a);
 }
 
 // One DP launch: over class `cls` of the class-sorted list a.list when
 // cls >= 0; with cls < 0 over a.list[0 .. *a.n_list) with the kernel of class
-// -cls - 1 (the fallback recomputations). n_max bounds the chains it may get;
-// the kernels loop over their chains (grid-stride).
+// -cls - 1 (the fallback recomputations). n_max bounds the chains it may get.
+// The thread kernels (row by row, stripes) take their chains 32 at a time
+// from the class's work counter (class order: the largest first), the warp
+// kernels loop over theirs (grid-stride).
 void launch_dp(msg_ctx* ctx, DpArgs a, int cls, int64_t n_max, msg_map_stats& S, cudaStream_t st = nullptr) {
     const int kind = cls >= 0 ? cls : -cls - 1;
     a.cls = cls >= 0 ? cls : -1;
+    a.queue = const_cast<unsigned long long*>(a.cls_n) + kCtrQueue + kind;  // the counter block is the stage's own
     if (!st) st = ctx->stream;
     S.n_launch++;
     if (kind == kDpSmall) {
-        const int g = (int)std::min<int64_t>(nblk(n_max, 128), (int64_t)ctx->num_sms * 16);
-        k_dp_small<<<g, 128, 0, st>>>(a);
+        k_dp_small<<<resident_blocks(ctx, k_dp_small, 128, n_max), 128, 0, st>>>(a);
     } else if (kind == kDpStripe || kind == kDpStripeBand) {
         const bool band = kind == kDpStripeBand;
         if (ctx->dp_k == 8) launch_stripe<8>(ctx, a, band, n_max, st);
@@ -919,7 +930,10 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     for (size_t ch = 0; ch + 1 < bounds.size(); ++ch) {
         const int64_t c0 = bounds[ch], nch = bounds[ch + 1] - bounds[ch];
         if (nch <= 0) continue;
-        if (ch > 0) CK(cudaMemsetAsync(d_ctr2, 0, kCtrStat * 8, st));  // lists start again; statistics accumulate
+        if (ch > 0) {  // lists and work counters start again; statistics accumulate
+            CK(cudaMemsetAsync(d_ctr2, 0, kCtrStat * 8, st));
+            CK(cudaMemsetAsync(d_ctr2 + kCtrQueue, 0, (kCtrWords - kCtrQueue) * 8, st));
+        }
         da.scr_base = h_rect_off[ch];
         da.band = d_band;
         const int bmode = dpp.mode != 0 ? 0 : params->band_mode;

@@ -1294,6 +1294,7 @@ struct DpArgs {
     const unsigned long long* n_list;
     const unsigned long long* cls_n;
     int cls;
+    unsigned long long* queue;            // thread kernels: chains of the launch handed out so far
     int64_t* tb_list;                     // chains whose traceback k_traceback runs
     unsigned long long* tb_n;
     // Banded flanks (GLOBAL mode). band[2c], band[2c+1]: half-width of the 5'
@@ -1712,6 +1713,15 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
 }
 
 
+// The next 32 items of a launch's list for the calling warp, from its work
+// counter (one atomic per warp); a value >= n when none is left. Every lane
+// of the warp calls it.
+__device__ __forceinline__ int64_t dp_take32(const DpArgs& a) {
+    unsigned long long b = 0;
+    if ((threadIdx.x & 31) == 0) b = atomicAdd(a.queue, 32ull);
+    return (int64_t)__shfl_sync(0xffffffffu, b, 0);
+}
+
 // First entry and length of the chains of a launch (DpArgs::list).
 __device__ __forceinline__ void dp_range(const DpArgs& a, int64_t& first, int64_t& n) {
     first = 0;
@@ -1751,8 +1761,9 @@ __global__ void __launch_bounds__(kDpWarps * 32, BAND ? 4 : 6) k_dp(DpArgs a) {
 __global__ void __launch_bounds__(128) k_dp_small(DpArgs a) {
     int64_t first, n_items;
     dp_range(a, first, n_items);
-    const int64_t n_thr = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_items; t += n_thr) {
+    for (int64_t b = dp_take32(a); b < n_items; b = dp_take32(a)) {
+        const int64_t t = b + (threadIdx.x & 31);
+        if (t >= n_items) continue;
         const int64_t c = a.list[first + t];
         const int n = a.chain_len[c];
         int4* gbase = a.sdbuf + 2 * a.chain_idx_off[c] + c;
@@ -1769,8 +1780,9 @@ __global__ void __launch_bounds__(kStripeThreads, 4) k_dp_stripe(DpArgs a) {
     __shared__ uint32_t s_tab[16 * kStripeThreads];  // per-thread score tables, word t of thread x at t * 128 + x
     int64_t first, n_items;
     dp_range(a, first, n_items);
-    const int64_t n_thr = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_items; t += n_thr) {
+    for (int64_t b = dp_take32(a); b < n_items; b = dp_take32(a)) {
+        const int64_t t = b + (threadIdx.x & 31);
+        if (t >= n_items) continue;
         const int64_t c = a.list[first + t];
         const int n = a.chain_len[c];
         int4* gbase = a.sdbuf + 2 * a.chain_idx_off[c] + c;
