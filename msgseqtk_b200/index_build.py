@@ -47,7 +47,66 @@ def bd_text(chroms) -> np.ndarray:
     return np.concatenate(parts)
 
 
-def suffix_array(text: np.ndarray, device: str | torch.device = "cpu", chunk: int = 1 << 28) -> torch.Tensor:
+# Largest array torch.sort and the scans below take in one call (index
+# arithmetic in 32 bits); longer arrays go through _sort_keys' partitions.
+SORT_LIMIT = 1 << 30
+
+
+def _sort_keys(key: torch.Tensor, chunk: int, limit: int = SORT_LIMIT):
+    """torch.sort(key) (values and source positions) for arrays of any
+    length: keys are partitioned by their top bits into ranges of at most
+    `limit` elements, each range gathered, sorted and written at its place.
+    Equal keys may come out in any order (the callers only need the order of
+    distinct keys)."""
+    n = key.numel()
+    if n <= limit:
+        return torch.sort(key)
+    dev = key.device
+    mx = int(key.max().item())
+    shift = max(0, mx.bit_length() - 16)
+    nb = (mx >> shift) + 1
+    hist = torch.zeros(nb, dtype=torch.int64, device=dev)
+    for a in range(0, n, chunk):
+        hist += torch.bincount(key[a:a + chunk] >> shift, minlength=nb)
+    counts = hist.cpu().numpy()
+    # consecutive buckets grouped into ranges of at most `limit` keys
+    groups, lo, size = [], 0, 0
+    for b in range(nb):
+        c = int(counts[b])
+        if c > limit:
+            raise ValueError("suffix array: one key bucket exceeds the sort limit")
+        if size + c > limit:
+            groups.append((lo, b, size))
+            lo, size = b, 0
+        size += c
+    groups.append((lo, nb, size))
+    out_key = torch.empty_like(key)
+    out_idx = torch.empty(n, dtype=torch.int64, device=dev)
+    off = 0
+    for blo, bhi, size in groups:
+        if size == 0:
+            continue
+        ks, ix = [], []
+        for a in range(0, n, chunk):
+            kk = key[a:a + chunk]
+            bk = kk >> shift
+            sel = torch.nonzero((bk >= blo) & (bk < bhi)).flatten()
+            ks.append(kk[sel])
+            ix.append(sel + a)
+            del bk, sel
+        kg = torch.cat(ks)
+        ig = torch.cat(ix)
+        del ks, ix
+        sk, perm = torch.sort(kg)
+        out_key[off:off + size] = sk
+        out_idx[off:off + size] = ig[perm]
+        off += size
+        del kg, ig, sk, perm
+    return out_key, out_idx
+
+
+def suffix_array(text: np.ndarray, device: str | torch.device = "cpu", chunk: int = 1 << 28,
+                 sort_limit: int = SORT_LIMIT) -> torch.Tensor:
     """Suffix array of a byte string by prefix doubling (standard order: a
     suffix that is a proper prefix of another sorts first). Returns int64 on
     `device`. Elementwise work runs in chunks of `chunk` elements and in
@@ -74,7 +133,7 @@ def suffix_array(text: np.ndarray, device: str | torch.device = "cpu", chunk: in
             kk |= code[a + j:b + j].to(torch.int64)
     del code
     h = k
-    sorted_key, sa = torch.sort(key)
+    sorted_key, sa = _sort_keys(key, chunk, sort_limit)
     del key
     while True:
         # group number of each sorted position: 1 + count of key changes before it
@@ -84,9 +143,15 @@ def suffix_array(text: np.ndarray, device: str | torch.device = "cpu", chunk: in
             b = min(n, a + chunk)
             grp[a:b] = (sorted_key[a:b] != sorted_key[a - 1:b - 1]).to(torch.int64)
         del sorted_key
-        torch.cumsum(grp, 0, out=grp)
+        carry = 0
+        for a in range(0, n, chunk):  # running sum, chunk by chunk
+            g = grp[a:a + chunk]
+            torch.cumsum(g, 0, out=g)
+            g += carry
+            carry = int(g[-1].item())
         rank = torch.empty(n, dtype=torch.int64, device=dev)
-        rank[sa] = grp
+        for a in range(0, n, chunk):
+            rank[sa[a:a + chunk]] = grp[a:a + chunk]
         ngroups = int(grp[-1].item())
         del grp
         if ngroups == n:
@@ -104,7 +169,7 @@ def suffix_array(text: np.ndarray, device: str | torch.device = "cpu", chunk: in
         del rank  # rebuilt from the sorted keys; only key and the sort's buffers live during the sort
         if dev.type == "cuda":
             torch.cuda.empty_cache()
-        sorted_key, sa = torch.sort(key)
+        sorted_key, sa = _sort_keys(key, chunk, sort_limit)
         del key
         h *= 2
     del rank
