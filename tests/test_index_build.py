@@ -25,6 +25,19 @@ def test_suffix_array_repetitive():
     assert np.array_equal(index_build.suffix_array(text).numpy(), naive_sa(text))
 
 
+def test_suffix_array_partitioned_sort():
+    """Texts longer than one sort call takes (3 G symbols in the repeat-rich
+    workload) sort their keys in partitions; forced here with tiny limits,
+    on repetitive and random texts alike."""
+    rng = np.random.default_rng(11)
+    for trial in range(4):
+        chroms = [synth._BASES[rng.integers(0, 4, size=int(rng.integers(200, 900)))] for _ in range(3)]
+        chroms.append(np.tile(chroms[0][:37], 9))  # a repeat family
+        text = index_build.bd_text(chroms)
+        sa = index_build.suffix_array(text, chunk=97, sort_limit=701).numpy()
+        assert np.array_equal(sa, naive_sa(text)), trial
+
+
 def test_view_equals_reference_fixture(cases):
     for c in cases.values():
         v = index_build.build_view(c.genomes)
