@@ -609,6 +609,8 @@ def main():
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         agg = {"smem": 0.0, "locate": 0.0, "chain": 0.0, "dp": 0.0}
         agg.update({k: 0 for k in counters})
+        agg["n_dp_class"] = [0] * 5
+        agg["dp_class_cells"] = [0] * 5
         torch.cuda.synchronize()
         ev0.record(stream)
         for s in range(args.steps):
@@ -618,6 +620,8 @@ def main():
             agg["dp"] += st["ms_dp"]
             for k in counters:
                 agg[k] += st[k]
+            for k in ("n_dp_class", "dp_class_cells"):
+                agg[k] = [x + y for x, y in zip(agg[k], st[k])]
         ev1.record(stream)
         torch.cuda.synchronize()
         clk = clocks.stop() if clocks else None
@@ -841,7 +845,9 @@ def main():
                 "gcups": gcups(agg), "plain_gpu": plain, "learned_band": band_info,
                 "e2e": e2e, "e2e_sam": e2e_sam, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
                 "gpu_launches": agg["n_launch"], "validation": valid, "setup": setup, "tuned_shapes": dp_shape, "small_batch": small_batch,
-                "stats": {k: agg[k] for k in counters}}
+                "stats": dict({k: agg[k] for k in counters},
+                              dp_classes={"names": ["row-by-row", "stripes", "banded stripes", "warp", "banded warp"],
+                                          "chains": agg["n_dp_class"], "cells": agg["dp_class_cells"]})}
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

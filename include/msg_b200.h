@@ -200,6 +200,8 @@ typedef struct msg_map_stats {
     int64_t n_band_fallback;/* banded chains recomputed on the whole cell set */
     int64_t n_filtered;     /* records removed by min_score_rate (drops included) */
     int64_t n_dp_warp;      /* chains whose DP ran one warp each (the rest: one thread each) */
+    int64_t n_dp_class[5];  /* chains per DP class: row by row, stripes, banded stripes, warp, banded warp */
+    int64_t dp_class_cells[5]; /* cells computed per class (recomputations count with the warp class) */
 } msg_map_stats;
 
 /* Map a batch of reads held in HOST memory: the per-read SE task body

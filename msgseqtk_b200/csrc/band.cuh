@@ -168,9 +168,10 @@ enum DpClass : int {
 };
 // Counter block of the DP stage (unsigned long long words): class sizes
 // [0, kDpClasses), the fallback lists of the stripe and warp kernels, the
-// traceback list, then the statistics (fallback, exact, dropped, warp cells,
-// thread cells), then per class the work counter of its launch (chains
+// traceback list, then the statistics (fallback, exact, dropped, then cells
+// computed per class), then per class the work counter of its launch (chains
 // handed out so far).
+static_assert(kDpWarp == kDpClassWarp, "DP class numbering");
 constexpr int kCtrFbStripe = 5, kCtrFbWarp = 6, kCtrTrace = 7, kCtrStat = 8, kCtrQueue = 16, kCtrWords = 24;
 constexpr int kKeyAreaBits = 11;
 constexpr int kKeyBits = kKeyAreaBits + 5 + 5 + 3;

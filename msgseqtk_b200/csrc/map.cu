@@ -976,10 +976,11 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         }
         S.n_launch++, k_traceback<<<nblk(nch, 128), 128, 0, st>>>(da);
         CK(cudaGetLastError());
-        if (bounds.size() > 2) {  // warp-path chains of this range, for the statistics
+        if (bounds.size() > 2) {  // chains per class of this range, for the statistics
             unsigned long long w[kDpClasses];
             CK(cudaMemcpy(w, d_ctr2, sizeof(w), cudaMemcpyDeviceToHost));
             S.n_dp_warp += (int64_t)(w[kDpWarp] + w[kDpWarpBand]);
+            for (int q = 0; q < kDpClasses; ++q) S.n_dp_class[q] += (int64_t)w[q];
         }
     }
     tm.mark();  // 4
@@ -1027,9 +1028,16 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     S.n_band_fallback = (int64_t)h_bstat[0];
     S.n_band_exact = (int64_t)h_bstat[1];
     S.n_band_drop = (int64_t)h_bstat[2];
-    S.dp_cells_done = (int64_t)(h_bstat[3] + h_bstat[4]);
+    S.dp_cells_done = 0;
+    for (int q = 0; q < kDpClasses; ++q) {
+        S.dp_class_cells[q] = (int64_t)h_bstat[3 + q];
+        S.dp_cells_done += S.dp_class_cells[q];
+    }
     S.n_filtered = h_nchain - h_nrec;
-    if (bounds.size() <= 2) S.n_dp_warp = (int64_t)(h_ctr2[kDpWarp] + h_ctr2[kDpWarpBand]);
+    if (bounds.size() <= 2) {
+        S.n_dp_warp = (int64_t)(h_ctr2[kDpWarp] + h_ctr2[kDpWarpBand]);
+        for (int q = 0; q < kDpClasses; ++q) S.n_dp_class[q] = (int64_t)h_ctr2[q];
+    }
     S.ms_smem = tm.ms(0, 1);
     S.ms_locate = tm.ms(1, 2);
     S.ms_chain = tm.ms(2, 3);

@@ -575,6 +575,7 @@ struct DpParams {
 };
 
 constexpr int kDpWarps = 4;       // warps per block in k_dp
+constexpr int kDpClassWarp = 3;   // DP class of the unbanded warp launch (DpClass::kDpWarp)
 constexpr int kStripeThreads = 128;  // threads per block in k_dp_stripe (the stride of its score tables)
 constexpr int kSmemSeeds = 64;    // chain seeds cached in shared memory per warp (else global)
 
@@ -1566,7 +1567,8 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
         fill(2 * q, q == 0 ? w5 : q == x.n ? w3 : -1);
     }
     if (WARP) __syncwarp();
-    if (a.bstat && cells && lane == 0) atomicAdd(a.bstat + (WARP ? 3 : 4), (unsigned long long)cells);
+    // cells per DP class (the fallback recomputations count with the warp class)
+    if (a.bstat && cells && lane == 0) atomicAdd(a.bstat + 3 + (a.cls >= 0 ? a.cls : kDpClassWarp), (unsigned long long)cells);
     const int stage = 2 * x.n + 2;
     auto reduce = [&]() {
         if (WARP) {

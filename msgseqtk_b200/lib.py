@@ -114,7 +114,8 @@ class MapStats(C.Structure):
                                          "dp_cells", "host_sorted", "n_launch")] + \
                [(n, C.c_double) for n in ("ms_total", "ms_smem", "ms_locate", "ms_chain", "ms_dp")] + \
                [(n, C.c_int64) for n in ("dp_cells_done", "n_band_exact", "n_band_drop", "n_band_fallback",
-                                         "n_filtered", "n_dp_warp")]
+                                         "n_filtered", "n_dp_warp")] + \
+               [("n_dp_class", C.c_int64 * 5), ("dp_class_cells", C.c_int64 * 5)]
 
 
 def build(force: bool = False) -> str:
@@ -757,7 +758,10 @@ class Context:
     def stats(self) -> dict:
         s = MapStats()
         self._check(self.lib.msg_last_stats(self.h, C.byref(s)), "msg_last_stats")
-        return {k: getattr(s, k) for k, _ in MapStats._fields_}
+        d = {k: getattr(s, k) for k, _ in MapStats._fields_}
+        d["n_dp_class"] = list(s.n_dp_class)
+        d["dp_class_cells"] = list(s.dp_class_cells)
+        return d
 
 
 _ASCII = np.frombuffer(b"$ACMGRSVTWYHKDBN", dtype=np.uint8)
