@@ -539,12 +539,24 @@ def main():
     t1 = time.time()
     feats, labels = [], []
     tb = 2 * args.batch_pairs
-    for a in range(0, len(treads), tb):
-        b = min(len(treads), a + tb)
-        f, l = ctx.band_collect(treads.seqs[treads.offs[a]:treads.offs[b]], treads.offs[a:b + 1] - treads.offs[a],
-                                plain_params)
+
+    def collect(a, b):
+        """Certificates of reads a..b, in halves when the batch's rectangles
+        exceed the context's DP storage (one collection fills them all)."""
+        try:
+            f, l = ctx.band_collect(treads.seqs[treads.offs[a]:treads.offs[b]],
+                                    treads.offs[a:b + 1] - treads.offs[a], plain_params)
+        except lib.MsgError as e:
+            if b - a < 2 or "too large" not in str(e):
+                raise
+            collect(a, (a + b) // 2)
+            collect((a + b) // 2, b)
+            return
         feats.append(f)
         labels.append(l)
+
+    for a in range(0, len(treads), tb):
+        collect(a, min(len(treads), a + tb))
     feats = np.concatenate(feats)
     labels = np.concatenate(labels)
     n_all = len(labels)
