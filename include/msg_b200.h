@@ -309,6 +309,14 @@ int msg_ctx_set_scratch_limit(msg_ctx* ctx, int64_t bytes);
  * anti-diagonals. Defaults 256, 65536, 16. Results do not depend on it. */
 int msg_ctx_set_dp_shape(msg_ctx* ctx, int32_t stripe_rows, int64_t small_area, int64_t warp_area);
 
+/* Lane width of the register-stripe DP fill (no reference counterpart):
+ * 16 (default) = unbanded chains in GLOBAL mode whose every finite value lies
+ * within +-8191 by a score bound ((L + T + 1) * max(match, mismatch,
+ * gap_open + gap_ext) < 8192) run two 16-row stripes per thread in 16-bit
+ * halves of each register, two cells per DP instruction; 32 = every chain
+ * in 32-bit values. Results do not depend on it. */
+int msg_ctx_set_dp_lanes(msg_ctx* ctx, int32_t bits);
+
 /* Kernel shape of the SMEM stage for reads up to 254 bp (no reference
  * counterpart): 0 = one read per thread (default); 1 and 2 = two reads per
  * thread, each thread keeping two extensions' bucket loads in flight (1:
@@ -327,15 +335,15 @@ typedef struct msg_tune {
     double ms_dp;           /* DP stage time of the chosen split on the sample */
     double ms_dp_default;   /* the same with the defaults (16, 256, 65536) */
     int32_t smem_variant;
-    int32_t pad;
+    int32_t dp_lanes;       /* 16 or 32 (msg_ctx_set_dp_lanes) */
     double ms_smem;         /* SMEM stage time of the chosen variant */
     double ms_smem_default; /* the same with variant 0 */
 } msg_tune;
 
 /* Autotuner of the kernel shapes (no reference counterpart): maps the sample
  * batch (host memory) with `params` under candidate shapes -- the SMEM
- * variant, then the DP warp threshold, stripe height and row-by-row
- * threshold, each chosen with the others fixed -- timing the stage it
+ * variant, then the DP warp threshold, stripe height, row-by-row threshold
+ * and lane width, each chosen with the others fixed -- timing the stage it
  * affects (a second run of every shape, after one untimed), and sets the
  * fastest on the context. Records never depend on the shapes, so the choice
  * only changes speed. */

@@ -876,6 +876,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     da.band = d_band; da.min_rate = params->min_score_rate; da.keep = d_keep; da.fb_list = d_fb;
     da.fb_n = d_ctr2 + 2; da.bstat = d_bstat;
     da.tb_list = d_tbl; da.tb_n = d_ctr2 + kCtrTrace;
+    da.lanes16 = ctx->dp_lanes == 16;
     da.cls_n = d_ctr2; da.cls = -1;
     const __nv_bfloat16* d_wts = ctx->band_wts.as<__nv_bfloat16>();
     const float* d_nrm = ctx->band_nrm.as<float>();
@@ -1579,6 +1580,12 @@ extern "C" int msg_ctx_set_dp_shape(msg_ctx* ctx, int32_t stripe_rows, int64_t s
     return MSG_OK;
 }
 
+extern "C" int msg_ctx_set_dp_lanes(msg_ctx* ctx, int32_t bits) {
+    if (!ctx || (bits != 16 && bits != 32)) return MSG_EINVAL;
+    ctx->dp_lanes = bits;
+    return MSG_OK;
+}
+
 extern "C" int msg_ctx_set_smem_shape(msg_ctx* ctx, int32_t variant) {
     if (!ctx || variant < 0 || variant > 4) return MSG_EINVAL;
     ctx->smem_variant = variant;
@@ -1595,7 +1602,9 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
     if (rc != MSG_OK) return rc;
     int n_tried = 0;
     // stage times of one shape: an untimed run, then the timed one
+    int best_lanes = 16;
     auto time_shape = [&](int var, int k, int64_t small, int64_t warp, double* ms_smem, double* ms_dp) -> int {
+        ctx->dp_lanes = best_lanes;
         ctx->smem_variant = var;
         ctx->dp_k = k;
         ctx->dp_small_area = small;
@@ -1632,6 +1641,11 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
         if ((rc = time_shape(best_var, best_k, small, best_warp, &ts, &td)) != MSG_OK) return rc;
         if (td < best_dp) { best_dp = td; best_small = small; }
     }
+    best_lanes = 32;  // the 32-bit fill for every stripe chain
+    if ((rc = time_shape(best_var, best_k, best_small, best_warp, &ts, &td)) != MSG_OK) return rc;
+    if (td < best_dp) best_dp = td;
+    else best_lanes = 16;
+    ctx->dp_lanes = best_lanes;
     ctx->smem_variant = best_var;
     ctx->dp_k = best_k;
     ctx->dp_small_area = best_small;
@@ -1642,7 +1656,7 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
     result->ms_dp = best_dp;
     result->ms_dp_default = dp_default;
     result->smem_variant = best_var;
-    result->pad = 0;
+    result->dp_lanes = best_lanes;
     result->ms_smem = best_smem;
     result->ms_smem_default = smem_default;
     result->n_tried = n_tried;

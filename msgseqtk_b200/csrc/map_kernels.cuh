@@ -569,6 +569,27 @@ __device__ __forceinline__ int32_t sat_add(int32_t a, int32_t b) {  // a + b for
 }
 __device__ __forceinline__ int32_t add_s(int32_t a, int32_t s) { return a == NEG ? NEG : a + s; }
 
+// 16-bit lanes of the two-stripe fill (fill_rect_stripe16): a finite value v
+// is held as v + kBias16 (> 0) and -inf as 0, two per 32-bit register. Then
+// max(x + g, 0) keeps -inf exact for a gap term (g < 0), and
+// min(x + x, max(x + s, 0)) for M's score s: x = 0 stays 0, while a finite
+// x (> |s|) gives x + s, as 2x >= x + s. Exact when every finite value of the
+// chain lies within (-kBias16 + W, kBias16), W the largest one-step change of
+// a score: any finite value is a path's score of at most L + T steps, so
+// (L + T + 1) * W < kBias16 suffices (fits16).
+constexpr int32_t kBias16 = 8192;
+__device__ __forceinline__ uint32_t to16(int32_t v) { return v == NEG ? 0u : (uint32_t)(v + kBias16); }
+__device__ __forceinline__ int32_t from16(uint32_t u) { return u == 0u ? NEG : (int32_t)u - kBias16; }
+__device__ __forceinline__ uint32_t pack16(int32_t x) { return ((uint32_t)x & 0xFFFFu) * 0x10001u; }
+__device__ __forceinline__ uint32_t pk16(uint32_t lo, uint32_t hi) { return __byte_perm(lo, hi, 0x5410); }
+// 0xFFFF in each 16-bit half of x whose top bit (bit 15, bit 31) is set, else
+// 0: prmt's sign-replicating byte selects (nibble 8 + byte index).
+__device__ __forceinline__ uint32_t halfmask16(uint32_t x) {
+    uint32_t r;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(0u), "r"(0xBB99u));
+    return r;
+}
+
 struct DpParams {
     int32_t match, mismatch, gap_o, gap_e;
     int32_t mode;  // 0 NW, 1 SW
@@ -1018,6 +1039,186 @@ struct ChainCtx {
         return cells;
     }
 
+    // Two-stripe fill in 16-bit lanes (GLOBAL mode, whole rectangle; the
+    // chain fits16): one thread fills 32 rows at a time as two 16-row
+    // stripes held in the two halves of 16 registers per matrix, the lower
+    // stripe one column behind the upper, so that within an iteration the
+    // halves are independent (the lower stripe's row above is the upper
+    // stripe's last row, finished one iteration earlier; an extra iteration
+    // ends the lower stripe, a first dummy one starts it from the left
+    // boundary). Each instruction updates two cells: __vibmax_s16x2 gives a
+    // maximum with its comparison outcomes (the traceback code bits),
+    // __viaddmax_s16x2 / __viaddmin_s16x2 the gap and score terms. A cell's
+    // score comes from its row's bit in the stripe table word of its
+    // column's target code (bits 0-15 upper rows, 16-31 lower rows), moved
+    // to a byte's top bit and widened to a 16-bit mask by a byte permute.
+    // Codes and last row/column go where fill_rect_stripe<16> puts them (the
+    // last row/column in 32-bit values), so the traceback reads both alike.
+    // The row buffer holds 16-bit values here. Returns the cells evaluated.
+    __device__ __noinline__ int64_t fill_rect_stripe16(int m) {
+        constexpr int K = 16;
+        const RectGeo g = rect(m);
+        if (g.R <= 0 || g.C <= 0) return 0;
+        const int R = (int)g.R, C = (int)g.C;
+        const uint32_t O2 = pack16(-(pp.gap_o + pp.gap_e)), E2 = pack16(-pp.gap_e);
+        const uint32_t SMM2 = pack16(-pp.mismatch), SX2 = SMM2 ^ pack16(pp.match);
+        int4* rb4 = reinterpret_cast<int4*>(g.rowbuf);
+        const uint8_t* const tgt = target + g.c0;
+        const int64_t tgt_n = target_avail - g.c0;
+        uint32_t* const tab = stab;
+        auto tbase = [&](int c) -> int { return c < tgt_n ? (int)__ldg(tgt + c) : 0; };
+        for (int c = 0; c < C; ++c) {  // the top boundary row
+            const int3 v = boundary(m, g.r0, g.c0 + 1 + c);
+            rb4[c] = make_int4((int)to16(v.x), (int)to16(v.y), (int)to16(v.z), 0);
+        }
+        const int nds = (R + 2 * K - 1) / (2 * K);
+        for (int ds = 0; ds < nds; ++ds) {
+            const int rr0 = ds * 2 * K;
+            const int nlo = min(K, R - rr0), nhi = max(0, min(K, R - rr0 - K));
+            const int64_t i0 = g.r0 + 1 + rr0;  // matrix row of the upper stripe's first row
+            {
+                uint32_t tbits[16];
+#pragma unroll
+                for (int t = 0; t < 16; ++t) tbits[t] = 0;
+                for (int k = 0; k < nlo + nhi; ++k) {
+                    const int q = qbase(i0 - 1 + k);
+                    if (q == 15) continue;  // N scores a mismatch against everything
+#pragma unroll
+                    for (int t = 1; t < 15; ++t) tbits[t] |= (q & t) ? (1u << k) : 0u;
+                }
+#pragma unroll
+                for (int t = 0; t < 16; ++t) tab[t * kStripeThreads] = tbits[t];
+            }
+            // diagonal inputs of row 0 of each half at the next iteration:
+            // upper (row above the stripe, previous column), lower (upper
+            // stripe's last row two columns back)
+            const int3 cv = boundary(m, i0 - 1, g.c0);
+            uint32_t dlM = to16(cv.x), dlI = to16(cv.y), dlD = to16(cv.z);
+            // the left boundary (column c0) of the pair's rows, parked in the
+            // rectangle's last-column slots until the loop reads it (those
+            // slots get their final values at the last column)
+            for (int k = 0; k < nlo + nhi; ++k) {
+                const int3 v = boundary(m, i0 + k, g.c0);
+                int32_t* lc = g.lastcol + (int64_t)(rr0 + k) * 3;
+                lc[0] = v.x; lc[1] = v.y; lc[2] = v.z;
+            }
+            // the previous column's values: the upper rows' left boundary (the
+            // lower halves are set after the first iteration)
+            uint32_t Mp[K], Ip[K], Dp[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                Mp[k] = 0u; Ip[k] = 0u; Dp[k] = 0u;
+                if (k < nlo) {
+                    const int32_t* lc = g.lastcol + (int64_t)(rr0 + k) * 3;
+                    Mp[k] = to16(lc[0]); Ip[k] = to16(lc[1]); Dp[k] = to16(lc[2]);
+                }
+            }
+            uint32_t dhM = 0u, dhI = 0u, dhD = 0u;
+            uint8_t* const code_lo = g.code + (int64_t)(2 * ds) * C * K;
+            uint8_t* const code_hi = code_lo + (int64_t)C * K;
+            const bool last = ds == nds - 1;
+            const int lr = R - 1 - rr0;  // the rectangle's last row within this pair (last pair)
+            const int iters = nhi > 0 ? C + 1 : C;
+            int4 up_next = rb4[0];
+            int tb_next = tbase(0);
+            uint32_t tprev = 0u;
+            for (int cc = 0; cc < iters; ++cc) {
+                const int4 up = up_next;  // upper stripe: the row above at column cc
+                const uint32_t tw = tab[(tb_next & 15) * kStripeThreads];
+                if (cc + 1 < C) {
+                    up_next = rb4[cc + 1];
+                    tb_next = tbase(cc + 1);
+                }
+                const uint32_t cw = (tw & 0xFFFFu) | (tprev & 0xFFFF0000u);
+                tprev = tw;
+                uint32_t uM = pk16((uint32_t)up.x, Mp[K - 1]), uI = pk16((uint32_t)up.y, Ip[K - 1]);
+                uint32_t dM = pk16(dlM, dhM), dI = pk16(dlI, dhI), dD = pk16(dlD, dhD);
+                dlM = (uint32_t)up.x; dlI = (uint32_t)up.y; dlD = (uint32_t)up.z;
+                dhM = Mp[K - 1]; dhI = Ip[K - 1]; dhD = Dp[K - 1];
+                uint32_t wl[K / 4], wh[K / 4];
+#pragma unroll
+                for (int q = 0; q < K / 4; ++q) { wl[q] = 0u; wh[q] = 0u; }
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const uint32_t msk = halfmask16(cw << (15 - k));
+                    const uint32_t s2 = (msk & SX2) ^ SMM2;
+                    bool aIh, aIl, aDh, aDl, bIh, bIl, bDh, bDl;
+                    const uint32_t t1 = __vibmax_s16x2(dM, dI, &aIh, &aIl);
+                    const uint32_t mx = __vibmax_s16x2(t1, dD, &aDh, &aDl);
+                    const uint32_t mv = __viaddmin_s16x2(mx, mx, __viaddmax_s16x2(mx, s2, 0u));
+                    const uint32_t a1 = __viaddmax_s16x2(uM, O2, 0u);
+                    const uint32_t iv = __vibmax_s16x2(__viaddmax_s16x2(uI, E2, 0u), a1, &bIh, &bIl);
+                    const uint32_t b1 = __viaddmax_s16x2(Mp[k], O2, 0u);
+                    const uint32_t dv = __vibmax_s16x2(__viaddmax_s16x2(Dp[k], E2, 0u), b1, &bDh, &bDl);
+                    // matchMax (I over M, then D only when I does not win), insMax, delMax
+                    const uint32_t cl = (aIl ? (aDl ? 0u : 2u) : 1u) | (bIl ? 0u : 4u) | (bDl ? 0u : 8u);
+                    const uint32_t ch = (aIh ? (aDh ? 0u : 2u) : 1u) | (bIh ? 0u : 4u) | (bDh ? 0u : 8u);
+                    wl[k >> 2] |= cl << (8 * (k & 3));
+                    wh[k >> 2] |= ch << (8 * (k & 3));
+                    dM = Mp[k]; dI = Ip[k]; dD = Dp[k];
+                    Mp[k] = mv; Ip[k] = iv; Dp[k] = dv;
+                    uM = mv; uI = iv;
+                }
+                if (cc < C) {  // upper stripe: column cc
+                    reinterpret_cast<uint4*>(code_lo + (int64_t)cc * K)[0] = make_uint4(wl[0], wl[1], wl[2], wl[3]);
+                    if (last && lr < K) {
+                        uint32_t lm = Mp[0], li = Ip[0], ld = Dp[0];
+#pragma unroll
+                        for (int k = 1; k < K; ++k)
+                            if (k == lr) { lm = Mp[k]; li = Ip[k]; ld = Dp[k]; }
+                        g.lastrow[cc * 3] = from16(lm & 0xFFFFu);
+                        g.lastrow[cc * 3 + 1] = from16(li & 0xFFFFu);
+                        g.lastrow[cc * 3 + 2] = from16(ld & 0xFFFFu);
+                    }
+                    if (cc == C - 1) {
+#pragma unroll
+                        for (int k = 0; k < K; ++k)
+                            if (k < nlo) {
+                                int32_t* lc = g.lastcol + (int64_t)(rr0 + k) * 3;
+                                lc[0] = from16(Mp[k] & 0xFFFFu); lc[1] = from16(Ip[k] & 0xFFFFu); lc[2] = from16(Dp[k] & 0xFFFFu);
+                            }
+                    }
+                }
+                if (nhi > 0) {
+                    if (cc == 0) {  // the lower stripe starts from its left boundary
+#pragma unroll
+                        for (int k = 0; k < K; ++k) {
+                            uint32_t hm = 0u, hi = 0u, hd = 0u;
+                            if (k < nhi) {
+                                const int32_t* lc = g.lastcol + (int64_t)(rr0 + K + k) * 3;
+                                hm = to16(lc[0]); hi = to16(lc[1]); hd = to16(lc[2]);
+                            }
+                            Mp[k] = pk16(Mp[k], hm); Ip[k] = pk16(Ip[k], hi); Dp[k] = pk16(Dp[k], hd);
+                        }
+                    } else {  // lower stripe: column cc - 1
+                        const int c1 = cc - 1;
+                        reinterpret_cast<uint4*>(code_hi + (int64_t)c1 * K)[0] = make_uint4(wh[0], wh[1], wh[2], wh[3]);
+                        if (nhi == K)
+                            rb4[c1] = make_int4((int)(Mp[K - 1] >> 16), (int)(Ip[K - 1] >> 16), (int)(Dp[K - 1] >> 16), 0);
+                        if (last && lr >= K) {
+                            uint32_t lm = Mp[0], li = Ip[0], ld = Dp[0];
+#pragma unroll
+                            for (int k = 1; k < K; ++k)
+                                if (k == lr - K) { lm = Mp[k]; li = Ip[k]; ld = Dp[k]; }
+                            g.lastrow[c1 * 3] = from16(lm >> 16);
+                            g.lastrow[c1 * 3 + 1] = from16(li >> 16);
+                            g.lastrow[c1 * 3 + 2] = from16(ld >> 16);
+                        }
+                        if (c1 == C - 1) {
+#pragma unroll
+                            for (int k = 0; k < K; ++k)
+                                if (k < nhi) {
+                                    int32_t* lc = g.lastcol + (int64_t)(rr0 + K + k) * 3;
+                                    lc[0] = from16(Mp[k] >> 16); lc[1] = from16(Ip[k] >> 16); lc[2] = from16(Dp[k] >> 16);
+                                }
+                        }
+                    }
+                }
+            }
+        }
+        return (int64_t)R * C;
+    }
+
     // Warp fill of the band of rectangle m (m = 0 or 2n; GLOBAL mode): the
     // 2w+1 diagonals within w of the adjacent seed's diagonal. Position
     // p = lane + 32 h (h < NP) of row rr is column rr + dg - w + p; one row is
@@ -1296,6 +1497,7 @@ struct DpArgs {
     const unsigned long long* cls_n;
     int cls;
     unsigned long long* queue;            // thread kernels: chains of the launch handed out so far
+    int lanes16;                          // stripe chains may use the 16-bit two-stripe fill
     int64_t* tb_list;                     // chains whose traceback k_traceback runs
     unsigned long long* tb_n;
     // Banded flanks (GLOBAL mode). band[2c], band[2c+1]: half-width of the 5'
@@ -1476,7 +1678,11 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
     x.roff = aux + x.n;
     x.pp = a.pp;
     x.status = a.status;
-    x.kst = KST;
+    // unbanded stripe chains in GLOBAL mode whose values fit 16-bit lanes
+    // run the two-stripe 16-bit fill (codes in 16-row stripes)
+    const int64_t w1 = max(max(a.pp.match, a.pp.mismatch), a.pp.gap_o + a.pp.gap_e);
+    const bool use16 = !WARP && KST > 0 && !BAND && a.lanes16 && a.pp.mode == 0 && (x.L + x.T + 1) * w1 < kBias16;
+    x.kst = use16 ? 16 : KST;
     x.stab = stab;
     // geometry in sd/rbnd/cbnd; a warp working in shared memory also leaves a
     // copy in the chain's global slot (gsd) for k_traceback
@@ -1536,7 +1742,8 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
                     return;
                 }
             }
-            if (x.pp.mode == 1) cells += x.template fill_rect_stripe<KST, true, false>(m, -1, best, bkey);
+            if (use16) cells += x.fill_rect_stripe16(m);
+            else if (x.pp.mode == 1) cells += x.template fill_rect_stripe<KST, true, false>(m, -1, best, bkey);
             else cells += x.template fill_rect_stripe<KST, false, false>(m, -1, best, bkey);
         } else if constexpr (!WARP) {
             cells += x.fill_rect_thread(m, w, best, bkey);
@@ -1706,7 +1913,7 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
             o.aln_end = aln_end;
             o.aln_score = best;
             o.flags = flags;
-            o.pad = s0 | (KST << 8);
+            o.pad = s0 | (x.kst << 8);
             a.tb_list[atomicAdd(a.tb_n, 1ull)] = c;
         }
     } else {

@@ -93,7 +93,9 @@ struct msg_ctx {
     // at most dp_warp_area in register stripes of dp_k rows on one thread,
     // larger ones on a warp
     int dp_k = 16;
-    int smem_variant = 0;  // SMEM thread path (msg_ctx_set_smem_shape): 0 one read per thread, 1/2 two
+    int dp_lanes = 16;     // 16: unbanded GLOBAL stripe chains that fit use 16-bit lanes (msg_ctx_set_dp_lanes)
+    int smem_variant = 0;  // SMEM thread path (msg_ctx_set_smem_shape): 0 one read per thread, 1/2 two,
+                           // 3/4 a pass's candidates extended several at a time
     int64_t dp_small_area = 256;
     int64_t dp_warp_area = 65536;
     cudaEvent_t ev[8];

@@ -261,10 +261,13 @@ DP_SHAPES = [(16, 256, 65536), (8, 0, 1 << 40), (32, 0, 1 << 40), (16, 1 << 40, 
 
 def test_dp_shape_gives_same_records(oracle_built):
     """The DP's work split (row-by-row threads, register stripes of 8/16/32
-    rows, warps) never changes a record: every split maps the same reads --
-    with errors, random, and long (1 kbp) ones whose chains are large -- to
-    the same records, plain, banded (fixed widths, certified or recomputed)
-    and local; the default split also equals the oracle."""
+    rows, warps) and lane width (16-bit two-stripe fill where the score
+    bound allows it, or 32-bit everywhere) never change a record: every
+    split maps the same reads -- with errors, random, and long (1 kbp) ones
+    whose chains are large -- to the same records, plain, banded (fixed
+    widths, certified or recomputed), local, and under a scoring scheme whose
+    bound leaves only the shorter chains in 16 bits; the default split also
+    equals the oracle."""
     g = synth.small_genomes(seed=75, n_genomes=3, length=120_000)
     view = index_build.build_view(g)
     orc = Oracle(view)
@@ -282,23 +285,32 @@ def test_dp_shape_gives_same_records(oracle_built):
         plist = [lib.default_params(min_len=13), lib.default_params(min_len=13, mode=1),
                  lib.default_params(min_len=13, min_score_rate=0.65, band_mode=1, band_w=7),
                  lib.default_params(min_len=13, min_score_rate=0.5, band_mode=1, band_w=31),
-                 lib.default_params(min_len=13, band_mode=1, band_w=15)]
+                 lib.default_params(min_len=13, band_mode=1, band_w=15),
+                 lib.default_params(min_len=13, mismatch=4, gap_open=10, gap_ext=10)]
         for pi, params in enumerate(plist):
             c.set_dp_shape(*DP_SHAPES[0])
+            c.set_dp_lanes(16)
             base = c.map(seq, off, params)
             st0 = c.stats()
-            if pi < 2:
-                compare_with_oracle(base, orc, lambda i: reads[i], len(reads), g, min_len=13, mode=params.mode)
-            for shape in DP_SHAPES[1:]:
-                c.set_dp_shape(*shape)
-                got = c.map(seq, off, params)
-                for k in ("aln", "cigar", "read_aln_off"):
-                    assert np.array_equal(base[k], got[k]), (pi, shape, k)
-                st = c.stats()
-                assert st["dp_cells"] == st0["dp_cells"], (pi, shape)
-                assert (st["n_band_exact"], st["n_band_drop"], st["n_band_fallback"]) == \
-                    (st0["n_band_exact"], st0["n_band_drop"], st0["n_band_fallback"]), (pi, shape)
+            if pi < 2 or pi == 5:
+                compare_with_oracle(base, orc, lambda i: reads[i], len(reads), g, min_len=13, mode=params.mode,
+                                    score=tuple(int(v) for v in (params.match, params.mismatch, params.gap_open,
+                                                                   params.gap_ext)))
+            for lanes in (16, 32):
+                c.set_dp_lanes(lanes)
+                for shape in DP_SHAPES[1:] if lanes == 16 else DP_SHAPES:
+                    c.set_dp_shape(*shape)
+                    got = c.map(seq, off, params)
+                    for k in ("aln", "cigar", "read_aln_off"):
+                        assert np.array_equal(base[k], got[k]), (pi, lanes, shape, k)
+                    st = c.stats()
+                    assert st["dp_cells"] == st0["dp_cells"], (pi, shape)
+                    assert (st["n_band_exact"], st["n_band_drop"], st["n_band_fallback"]) == \
+                        (st0["n_band_exact"], st0["n_band_drop"], st0["n_band_fallback"]), (pi, shape)
+            c.set_dp_lanes(16)
             assert len(base["aln"]) > 0
+        with pytest.raises(lib.MsgError):
+            c.set_dp_lanes(8)
         with pytest.raises(lib.MsgError):
             c.set_dp_shape(12, 256, 65536)
         # the autotuner picks one of its candidates and changes no record
@@ -306,7 +318,8 @@ def test_dp_shape_gives_same_records(oracle_built):
         c.set_dp_shape(*DP_SHAPES[0])
         before = c.map(seq, off, params)
         tune = c.autotune(seq, off, params)
-        assert tune["stripe_rows"] in (8, 16, 32) and tune["n_tried"] == 13 and tune["smem_variant"] in (0, 1, 2, 3, 4)
+        assert tune["stripe_rows"] in (8, 16, 32) and tune["n_tried"] == 14 and tune["smem_variant"] in (0, 1, 2, 3, 4)
+        assert tune["dp_lanes"] in (16, 32)
         assert tune["warp_area"] in (4096, 16384, 65536, 262144) and tune["small_area"] in (0, 64, 256, 1024)
         after = c.map(seq, off, params)
         for k in ("aln", "cigar", "read_aln_off"):
