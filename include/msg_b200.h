@@ -202,6 +202,8 @@ typedef struct msg_map_stats {
     int64_t n_dp_warp;      /* chains whose DP ran one warp each (the rest: one thread each) */
     int64_t n_dp_class[5];  /* chains per DP class: row by row, stripes, banded stripes, warp, banded warp */
     int64_t dp_class_cells[5]; /* cells computed per class (recomputations count with the warp class) */
+    int64_t n_smem_rerun;   /* reads the one-thread SMEM kernel gave to the warp kernel (candidate list too long) */
+    int64_t smem_retries;   /* SMEM stage reruns with larger output slots */
 } msg_map_stats;
 
 /* Map a batch of reads held in HOST memory: the per-read SE task body

@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <thread>
 #include <vector>
 
 #include <cub/cub.cuh>
@@ -129,6 +130,30 @@ __global__ void k_smem_read(const int64_t* __restrict__ smem_off, int64_t n_read
     const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (r >= n_reads) return;
     for (int64_t k = smem_off[r] + (threadIdx.x & 31); k < smem_off[r + 1]; k += 32) smem_read[k] = (int32_t)r;
+}
+
+// (logP bits, size) of the SMEM rows of the reads in `list`, packed read by
+// read at pack_off (one warp per listed read).
+__global__ void k_gather_rank_keys(const int64_t* __restrict__ list, int64_t n, const int64_t* __restrict__ smem_off,
+                                   const int64_t* __restrict__ pack_off, const int64_t* __restrict__ smem,
+                                   int64_t* __restrict__ out) {
+    const int64_t f = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (f >= n) return;
+    const int64_t r = list[f], a = smem_off[r], b = smem_off[r + 1], o = pack_off[f];
+    for (int64_t k = a + (threadIdx.x & 31); k < b; k += 32) {
+        out[2 * (o + k - a)] = smem[6 * k + 5];
+        out[2 * (o + k - a) + 1] = smem[6 * k + 4];
+    }
+}
+
+// The selection flags of the listed reads' rows back to their places.
+__global__ void k_scatter_sel(const int64_t* __restrict__ list, int64_t n, const int64_t* __restrict__ smem_off,
+                              const int64_t* __restrict__ pack_off, const uint8_t* __restrict__ psel,
+                              uint8_t* __restrict__ sel) {
+    const int64_t f = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (f >= n) return;
+    const int64_t r = list[f], a = smem_off[r], b = smem_off[r + 1], o = pack_off[f];
+    for (int64_t k = a + (threadIdx.x & 31); k < b; k += 32) sel[k] = psel[o + k - a];
 }
 
 __global__ void k_gather_off(const int64_t* __restrict__ smem_off, const int64_t* __restrict__ smem_seed_off,
@@ -386,19 +411,22 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     // (k_smem_thread), longer reads one warp per read with lanes over the
     // candidate list (k_smem); both launches share the batch. Each read's SMEM
     // rows go to its own slot, cap rows per 150 bases (at least cap), so long
-    // reads get room in proportion. The thread kernel keeps at most
-    // kThreadPrev candidates per read so that all candidate lists stay in L2;
-    // when a list outgrows it, the short reads rerun on the warp kernel too.
+    // reads get room in proportion (cap starts from the largest a batch of
+    // this context needed). The thread kernel keeps at most kThreadPrev
+    // candidates per read so that all candidate lists stay in L2; a read
+    // whose list outgrows it is abandoned and mapped again by the warp
+    // kernel.
     constexpr int64_t kThreadPrev = 48;
     constexpr int64_t kThreadMaxLen = 254;
     const int threads = 256;
     const int blocks = ctx->num_sms * 8;
     const int64_t n_warps = (int64_t)blocks * threads / 32;
-    CK(ctx->rlist.ensure((n_reads + 1) * 8 * 4 + 64));
+    CK(ctx->rlist.ensure((n_reads + 1) * 8 * 5 + 64));
     int64_t* d_short = ctx->rlist.as<int64_t>();
     int64_t* d_long = d_short + (n_reads + 1);
     int64_t* d_slot = d_long + (n_reads + 1);        // slot rows per read (n + 1)
     int64_t* d_slot_off = d_slot + (n_reads + 1);    // slot offsets (n + 1)
+    int64_t* d_ovf = d_slot_off + (n_reads + 1);     // reads the thread kernel abandoned
     unsigned long long h_split[2] = {0, 0};
     if (n_reads > 0) {
         CK(cudaMemsetAsync(d_ctr + 4, 0, 16, st));
@@ -409,7 +437,34 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         CK(cudaStreamSynchronize(st));
     }
     bool thread_path = h_split[0] > 0;
-    int64_t cap = 16;
+    int64_t cap = std::max<int64_t>(16, ctx->smem_cap);
+    // the warp kernel over `n` reads of `list` (all reads when null)
+    auto run_warp = [&](const int64_t* list, int64_t n) -> cudaError_t {
+        const int64_t pv_cap = Lmax + 2;
+        cudaError_t e = ctx->prevw.ensure(n_warps * pv_cap * (4 + 8 + 8 + 8 + 8) + 64);
+        if (e != cudaSuccess) return e;
+        SmemArgs sa{};
+        sa.seq = d_seq; sa.off = d_off; sa.n_reads = n; sa.min_len = params->min_len;
+        sa.thr = thr; sa.thr_all = thr_all;
+        for (int b = 0; b < 16; ++b) sa.llk[b] = im.llk[b];
+        sa.out = ctx->smem.as<int64_t>(); sa.cap = cap; sa.out_off = d_slot_off;
+        sa.list = list;
+        sa.count = ctx->smem_cnt.as<int32_t>();
+        char* pv = ctx->prevw.as<char>();
+        sa.pv_p = reinterpret_cast<int64_t*>(pv);
+        sa.pv_q = sa.pv_p + n_warps * pv_cap;
+        sa.pv_s = sa.pv_q + n_warps * pv_cap;
+        sa.pv_lp = reinterpret_cast<double*>(sa.pv_s + n_warps * pv_cap);
+        sa.pv_pos = reinterpret_cast<int32_t*>(sa.pv_lp + n_warps * pv_cap);
+        sa.pv_cap = pv_cap;
+        sa.work = d_ctr + 3;
+        sa.n_ext = d_ctr + 1;
+        sa.status = d_status;
+        e = cudaMemsetAsync(d_ctr + 3, 0, 8, st);
+        if (e != cudaSuccess) return e;
+        S.n_launch++, k_smem<<<blocks, threads, 0, st>>>(sa, ix);
+        return cudaGetLastError();
+    };
     for (int attempt = 0; attempt < 4; ++attempt) {
         int64_t h_rows = 0;
         if (n_reads > 0) S.n_launch++, k_slot_rows<<<nblk(n_reads, 256), 256, 0, st>>>(d_rlen, n_reads, cap, d_slot);
@@ -417,6 +472,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         CK(ctx->smem.ensure((size_t)std::max<int64_t>(1, h_rows) * 48));
         CK(ctx->smem_cnt.ensure((n_reads + 1) * sizeof(int32_t)));
         CK(cudaMemsetAsync(d_ctr, 0, 8 * 4, st));
+        CK(cudaMemsetAsync(d_ctr + 7, 0, 8, st));
         CK(cudaMemsetAsync(d_status, 0, 4, st));
         // short reads on the thread kernel
         if (thread_path) {
@@ -445,6 +501,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             ta.count = ctx->smem_cnt.as<int32_t>();
             ta.prev = ctx->prev.as<PrevEntry>(); ta.pv_cap = pv_cap;
             ta.work = d_ctr; ta.n_ext = d_ctr + 1; ta.status = d_status;
+            ta.ovf_list = d_ovf; ta.ovf_n = d_ctr + 7;
             if (var == 1) S.n_launch++, k_smem_thread2<4><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else if (var == 2) S.n_launch++, k_smem_thread2<3><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else if (var == 3) S.n_launch++, k_smem_pass<4, 4><<<n_thr / 128, 128, 0, st>>>(ta, ix);
@@ -452,39 +509,25 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             else S.n_launch++, k_smem_thread<<<n_thr / 128, 128, 0, st>>>(ta, ix);
             CK(cudaGetLastError());
         }
-        // long reads (all reads once the thread kernel has given up) on the warp kernel
+        // long reads (all reads when no read is short) on the warp kernel
         const int64_t n_warp_reads = thread_path ? (int64_t)h_split[1] : n_reads;
-        if (n_warp_reads > 0) {
-            const int64_t pv_cap = Lmax + 2;
-            CK(ctx->prevw.ensure(n_warps * pv_cap * (4 + 8 + 8 + 8 + 8) + 64));
-            SmemArgs sa{};
-            sa.seq = d_seq; sa.off = d_off; sa.n_reads = n_warp_reads; sa.min_len = params->min_len;
-            sa.thr = thr; sa.thr_all = thr_all;
-            for (int b = 0; b < 16; ++b) sa.llk[b] = im.llk[b];
-            sa.out = ctx->smem.as<int64_t>(); sa.cap = cap; sa.out_off = d_slot_off;
-            sa.list = thread_path ? d_long : nullptr;
-            sa.count = ctx->smem_cnt.as<int32_t>();
-            char* pv = ctx->prevw.as<char>();
-            sa.pv_p = reinterpret_cast<int64_t*>(pv);
-            sa.pv_q = sa.pv_p + n_warps * pv_cap;
-            sa.pv_s = sa.pv_q + n_warps * pv_cap;
-            sa.pv_lp = reinterpret_cast<double*>(sa.pv_s + n_warps * pv_cap);
-            sa.pv_pos = reinterpret_cast<int32_t*>(sa.pv_lp + n_warps * pv_cap);
-            sa.pv_cap = pv_cap;
-            sa.work = d_ctr + 3;
-            sa.n_ext = d_ctr + 1;
-            sa.status = d_status;
-            S.n_launch++, k_smem<<<blocks, threads, 0, st>>>(sa, ix);
-            CK(cudaGetLastError());
-        }
+        if (n_warp_reads > 0) CK(run_warp(thread_path ? d_long : nullptr, n_warp_reads));
         uint32_t h_status = 0;
         CK(cudaMemcpyAsync(&h_status, d_status, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(ctx->hpin + 9, d_ctr + 7, 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         if (h_status & kErrInternal) return ctx->fail(MSG_EINTERNAL, "SMEM stage consistency check failed");
-        if (h_status & 0x100u) {  // a candidate list outgrew the thread kernel's cap
-            if (!thread_path) return ctx->fail(MSG_EINTERNAL, "SMEM candidate list overflow");
-            thread_path = false;
-            continue;
+        if (h_status & 0x100u) {  // reads whose candidate list outgrew the thread kernel's cap
+            const int64_t n_ovf = ctx->hpin[9];
+            if (!thread_path || n_ovf <= 0) return ctx->fail(MSG_EINTERNAL, "SMEM candidate list overflow");
+            S.n_smem_rerun += n_ovf;
+            CK(cudaMemsetAsync(d_status, 0, 4, st));
+            CK(run_warp(d_ovf, n_ovf));
+            uint32_t h2 = 0;
+            CK(cudaMemcpyAsync(&h2, d_status, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (h2 & (kErrInternal | 0x100u)) return ctx->fail(MSG_EINTERNAL, "SMEM stage consistency check failed");
+            h_status = (h_status & ~0x100u) | h2;
         }
         if (!(h_status & kErrOverflow)) break;
         if (attempt == 3) return ctx->fail(MSG_EINTERNAL, "SMEM output overflow after resizing");
@@ -497,7 +540,11 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             const int64_t per = std::max<int64_t>(len[r], kSlotBases);
             cap = std::max<int64_t>(cap, ((int64_t)cnt[r] * kSlotBases + per - 1) / per);
         }
+        S.smem_retries++;
     }
+    // later batches start from this batch's capacity (bounded: rarer reads
+    // that need more still get their rerun)
+    ctx->smem_cap = std::min<int64_t>(std::max(ctx->smem_cap, cap), 256);
     // the extension count arrives with the next synchronisation
     CK(cudaMemcpyAsync(ctx->hpin + 8, d_ctr + 1, 8, cudaMemcpyDeviceToHost, st));
     if (n_reads > 0) S.n_launch++, k_i32_to_i64<<<nblk(n_reads, 256), 256, 0, st>>>(ctx->smem_cnt.as<int32_t>(), d_cnt64, n_reads);
@@ -556,33 +603,63 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         if (!flagged.empty()) {
             // SMEM_LIST::findSeeds (SMEM.cpp:275-291): std::sort by loglik (not
             // stable; same libstdc++ algorithm on the same emission order), then
-            // locate until at least maxNSeed seeds.
-            std::vector<int64_t> soff(n_reads + 1);
+            // locate until at least maxNSeed seeds. The flagged reads' (logP,
+            // size) pairs come to the host in one copy, are sorted read by read
+            // on host threads, and their selections go back in one copy.
+            const int64_t nf = (int64_t)flagged.size();
+            std::vector<int64_t> soff(n_reads + 1), poff(nf + 1, 0);
             CK(cudaMemcpy(soff.data(), d_smem_off, (n_reads + 1) * 8, cudaMemcpyDeviceToHost));
+            for (int64_t f = 0; f < nf; ++f) poff[f + 1] = poff[f] + soff[flagged[f] + 1] - soff[flagged[f]];
+            const int64_t F = poff[nf];
+            CK(ctx->hsort.ensure((2 * nf + 1 + 2 * F) * 8 + F + 64));
+            int64_t* d_flist = ctx->hsort.as<int64_t>();
+            int64_t* d_poff = d_flist + nf;
+            int64_t* d_pairs = d_poff + (nf + 1);
+            uint8_t* d_psel = reinterpret_cast<uint8_t*>(d_pairs + 2 * F);
+            std::vector<int64_t> pairs(2 * F);
+            std::vector<uint8_t> psel(F, 0);
+            CK(cudaMemcpyAsync(d_flist, flagged.data(), nf * 8, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d_poff, poff.data(), (nf + 1) * 8, cudaMemcpyHostToDevice, st));
+            S.n_launch++, k_gather_rank_keys<<<nblk(nf * 32, 256), 256, 0, st>>>(d_flist, nf, d_smem_off, d_poff, d_smem,
+                                                                                 d_pairs);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(pairs.data(), d_pairs, 2 * F * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
             struct HS { double lp; int64_t size; int64_t k; };
-            for (int64_t r : flagged) {
-                const int64_t a = soff[r], b = soff[r + 1];
-                std::vector<int64_t> rows((b - a) * 6);
-                CK(cudaMemcpy(rows.data(), d_smem + 6 * a, (b - a) * 48, cudaMemcpyDeviceToHost));
+            auto sort_range = [&](int64_t f0, int64_t f1) {
                 std::vector<HS> v;
-                for (int64_t k = 0; k < b - a; ++k) {
-                    HS h;
-                    std::memcpy(&h.lp, &rows[6 * k + 5], 8);
-                    h.size = rows[6 * k + 4];
-                    h.k = k;
-                    v.push_back(h);
+                for (int64_t f = f0; f < f1; ++f) {
+                    const int64_t o = poff[f], m = poff[f + 1] - o;
+                    v.clear();
+                    for (int64_t k = 0; k < m; ++k) {
+                        HS h;
+                        std::memcpy(&h.lp, &pairs[2 * (o + k)], 8);
+                        h.size = pairs[2 * (o + k) + 1];
+                        h.k = k;
+                        v.push_back(h);
+                    }
+                    std::sort(v.begin(), v.end(), [](const HS& x, const HS& y) -> bool { return x.lp < y.lp; });
+                    int64_t got = 0;
+                    for (const HS& h : v) {
+                        psel[o + h.k] = 1;
+                        got += h.size;
+                        if (got >= params->max_nseed) break;
+                    }
                 }
-                std::sort(v.begin(), v.end(), [](const HS& x, const HS& y) -> bool { return x.lp < y.lp; });
-                std::vector<uint8_t> sel(b - a, 0);
-                int64_t got = 0;
-                for (const HS& h : v) {
-                    sel[h.k] = 1;
-                    got += h.size;
-                    if (got >= params->max_nseed) break;
-                }
-                CK(cudaMemcpy(d_sel + a, sel.data(), b - a, cudaMemcpyHostToDevice));
+            };
+            const int64_t nth = std::min<int64_t>(std::max(1u, std::thread::hardware_concurrency()), 16);
+            if (nf < 256 || nth < 2) {
+                sort_range(0, nf);
+            } else {
+                std::vector<std::thread> pool;
+                for (int64_t t = 0; t < nth; ++t) pool.emplace_back(sort_range, nf * t / nth, nf * (t + 1) / nth);
+                for (auto& th : pool) th.join();
             }
-            S.host_sorted = (int64_t)flagged.size();
+            CK(cudaMemcpyAsync(d_psel, psel.data(), F, cudaMemcpyHostToDevice, st));
+            S.n_launch++, k_scatter_sel<<<nblk(nf * 32, 256), 256, 0, st>>>(d_flist, nf, d_smem_off, d_poff, d_psel, d_sel);
+            CK(cudaGetLastError());
+            CK(cudaStreamSynchronize(st));  // psel and the lists leave scope
+            S.host_sorted = nf;
         }
     }
     int64_t h_nseed_raw = 0;

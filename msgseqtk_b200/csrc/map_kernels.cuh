@@ -648,6 +648,7 @@ struct ChainCtx {
     DpParams pp;
     uint32_t* status;
     int kst = 0;                // rows per stripe of the code layout (0: the 32-row skewed layout)
+    int sep = 0;                // seeds in order without overlap, each of 2 or more bases (see boundary)
     uint32_t* stab = nullptr;   // register-stripe fill: this thread's score table, 16 words at stride kStripeThreads
 
     __device__ int64_t qf(int k) const { return sd[k].x; }
@@ -769,12 +770,18 @@ struct ChainCtx {
     //    boundary holds the initialised matrices (initNW/initSW,
     //    Alignment.h:599-613): row 0 M = 0 (I(0,0) = 0 in NW); column 0
     //    I = -gapPenalty(i) in NW, M = 0 in SW; the rest -inf;
-    //  * the 3' rectangle of a one-seed chain (m == 2): its top row is the
-    //    seed's last row qt and its left column the seed's last column te;
-    //    every cell there is -inf but the seed's last diagonal cell (qt, te)
-    //    with M = E (the seed's final diagonal value), D(qt, te + 1) =
-    //    E + o from the whole-column overwrite and I(qt + 1, te) = E + o
-    //    from the whole-row overwrite (Alignment.cpp:161-169).
+    //  * the rectangle after seed p (m == 2p + 2: a gap or the 3'
+    //    rectangle) of a one-seed chain, or of a chain whose seeds are in
+    //    order without overlap (qf_k >= qt_k-1, ts_k >= te_k-1) and at least
+    //    2 bases long (sep): its top row is the seed's last row qt and its
+    //    left column the seed's last column te; every cell there is -inf but
+    //    the seed's last diagonal cell (qt, te) with M = E (the seed's final
+    //    diagonal value), D(qt, te + 1) = E + o from the whole-column
+    //    overwrite and I(qt + 1, te) = E + o from the whole-row overwrite
+    //    (Alignment.cpp:161-169). No other region reaches those cells: the
+    //    earlier seeds' blocks, cells past them, row and column overwrites
+    //    and rectangles all lie in rows before qt and columns before te, as
+    //    the region rule confirms cell by cell.
     // OUTLINE: the region rule through the out-of-line MID (else inlined).
     template <bool OUTLINE = true>
     __device__ __forceinline__ int3 boundary(int m, int64_t i, int64_t j) const {
@@ -783,9 +790,10 @@ struct ChainCtx {
             if (i == 0) return make_int3(0, (nw && j == 0) ? 0 : NEG, NEG);
             return make_int3(nw ? NEG : 0, nw ? -(pp.gap_o + pp.gap_e * (int32_t)i) : NEG, NEG);  // j == 0
         }
-        if (m == 2 && n == 1) {
-            const int64_t q1 = qt(0), t1 = te(0);
-            const int32_t E = diag[0] + (int32_t)(q1 - qf(0) - 1) * pp.match;
+        if (m >= 2 && !(m & 1) && (n == 1 || sep)) {
+            const int p = (m >> 1) - 1;
+            const int64_t q1 = qt(p), t1 = te(p);
+            const int32_t E = diag[p] + (int32_t)(q1 - qf(p) - 1) * pp.match;
             const int32_t Eo = sat_add(E, -(pp.gap_o + pp.gap_e));
             if (i == q1 && j == t1) return make_int3(E, NEG, NEG);
             if (i == q1 && j == t1 + 1) return make_int3(NEG, NEG, Eo);
@@ -1712,6 +1720,15 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
     x.sd = sd;
     x.rbnd = rbnd;
     x.cbnd = cbnd;
+    if (WARP) __syncwarp();
+    {
+        bool sep = true;
+        for (int k = 0; k < x.n && sep; ++k) {
+            const int4 g = sd[k];
+            sep = g.y - g.x >= 2 && (k == 0 || (g.x >= sd[k - 1].y && g.z >= sd[k - 1].w));
+        }
+        x.sep = sep;
+    }
     x.rd = a.rseq + a.roff[r];
     x.rev = f.strand != FWD;
     if (WARP) __syncwarp();
@@ -1765,7 +1782,16 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
             const int k = q - 1, m = 2 * k + 1;
             if (lane == 0) {  // first diagonal cell (Alignment.cpp:146-153): max(M,D,I + s, 0)
                 const int64_t i = x.qf(k), j = x.ts(k);
-                const int32_t mx = max(max(x.M(i, j, m), x.D(i, j, m)), x.I(i, j, m));
+                // (i, j) is the last cell of the rectangle before the seed when
+                // it has cells: its stored last row holds the values
+                const RectGeo gp = x.rect(2 * k);
+                int32_t mx;
+                if (gp.R > 0 && gp.C > 0) {
+                    const int32_t* v = gp.lastrow + (gp.C - 1) * 3;
+                    mx = max(max(v[0], v[2]), v[1]);
+                } else {
+                    mx = max(max(x.M(i, j, m), x.D(i, j, m)), x.I(i, j, m));
+                }
                 x.diag[k] = max(add_s(mx, a.pp.match), 0);
                 if (k == 0) x5 = mx;
             }

@@ -77,7 +77,7 @@ struct msg_ctx {
     msg_map_stats stats{};
     // batch buffers
     msg::DevBuf reads, offs, smem, smem_cnt, prev, sel, seedoff, seeds, seeds2, rcount, chains, chainidx, dpinfo,
-        scratch, path, alnbuf, cigbuf, misc, status, geobuf, bandbuf, alnbuf2, recoff, rlist, prevw;
+        scratch, path, alnbuf, cigbuf, misc, status, geobuf, bandbuf, alnbuf2, recoff, rlist, prevw, hsort;
     // band model (bf16 weights, fp32 feature mean/scale) and training buffers
     msg::DevBuf band_wts, band_nrm, tr_x, tr_y, tr_ord, tr_w, tr_m, tr_v, tr_g, tr_loss;
     // MEM search / read cleaning: per-unit loglik and counts, clean outputs, MEM rows, row slots
@@ -96,6 +96,7 @@ struct msg_ctx {
     int dp_lanes = 16;     // 16: unbanded GLOBAL stripe chains that fit use 16-bit lanes (msg_ctx_set_dp_lanes)
     int smem_variant = 0;  // SMEM thread path (msg_ctx_set_smem_shape): 0 one read per thread, 1/2 two,
                            // 3/4 a pass's candidates extended several at a time
+    int64_t smem_cap = 16;  // SMEM rows per 150 read bases the slots start with (grows after an overflow)
     int64_t dp_small_area = 256;
     int64_t dp_warp_area = 65536;
     cudaEvent_t ev[8];
@@ -130,7 +131,7 @@ struct msg_ctx {
     void buffers_free() {
         for (msg::DevBuf* b : {&reads, &offs, &smem, &smem_cnt, &prev, &sel, &seedoff, &seeds, &seeds2, &rcount,
                                &chains, &chainidx, &dpinfo, &scratch, &path, &alnbuf, &cigbuf, &misc, &status, &geobuf,
-                               &bandbuf, &alnbuf2, &recoff, &rlist, &prevw, &band_wts, &band_nrm, &tr_x, &tr_y,
+                               &bandbuf, &alnbuf2, &recoff, &rlist, &prevw, &hsort, &band_wts, &band_nrm, &tr_x, &tr_y,
                                &tr_ord, &tr_w, &tr_m, &tr_v, &tr_g, &tr_loss, &memo, &memo2, &memrows, &memslot,
                                &in_seq[0], &in_seq[1], &in_off[0], &in_off[1], &stage[0], &stage[1]})
             b->release();

@@ -50,6 +50,8 @@ struct SmemThreadArgs {
     unsigned long long* work;
     unsigned long long* n_ext;
     uint32_t* status;
+    int64_t* ovf_list;      // reads abandoned because their candidate list outgrew pv_cap (rerun on k_smem)
+    unsigned long long* ovf_n;
 };
 
 // per-block copy of the argument table: lanes index it by their own bases,
@@ -231,7 +233,7 @@ __device__ __forceinline__ void smem_push(ThreadSmem& t, const SmemThreadArgs& a
         pv[a.pv_cap - 1 - t.n_prev] = e;
         t.n_prev++;
     } else {
-        atomicOr(a.status, 0x100u);  // list longer than the cap: the batch reruns on the warp kernel
+        atomicOr(a.status, 0x100u);  // list longer than the cap: this read reruns on the warp kernel
         t.ovf = 1;
     }
 }
@@ -284,8 +286,12 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
 // batch's work counter; false when the batch has no read left.
 __device__ __forceinline__ bool smem_next_read(ThreadSmem& t, const SmemThreadArgs& a, const IndexDev& ix) {
     if (t.phase == PH_DONE) {
-        a.count[t.r] = t.n_out;
-        if (t.n_out > t.cap_r) atomicOr(a.status, kErrOverflow);
+        if (t.ovf) {  // abandoned: the warp kernel maps it again
+            a.ovf_list[atomicAdd(a.ovf_n, 1ull)] = t.r;
+        } else {
+            a.count[t.r] = t.n_out;
+            if (t.n_out > t.cap_r) atomicOr(a.status, kErrOverflow);
+        }
     }
     unsigned long long r = atomicAdd(a.work, 1ull);
     if ((int64_t)r >= a.n_reads) return false;

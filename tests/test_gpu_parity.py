@@ -159,6 +159,36 @@ def test_edge_cases_match_oracle(ctx, oracle_built):
     assert len(res["aln"]) == 0
 
 
+def test_tandem_repeats_long_candidate_lists_match_oracle(ctx, oracle_built):
+    """A genome of 200 diverged copies of one 600 bp unit: a walk's interval
+    shrinks a few copies per base, so candidate lists outgrow the one-thread
+    SMEM kernel's cap (those reads are abandoned and mapped again on the warp
+    kernel), and with a small maxNSeed many reads need the host sort of
+    their SMEMs (done for the whole batch in one round trip). Records equal
+    the oracle's either way, and both paths are taken."""
+    rng = np.random.default_rng(91)
+    unit = synth._BASES[rng.integers(0, 4, 600)]
+    parts = []
+    for _ in range(200):
+        u = unit.copy()
+        mut = rng.random(600) < 0.015
+        u[mut] = synth._BASES[rng.integers(0, 4, int(mut.sum()))]
+        parts.append(u)
+    g = [np.concatenate(parts), synth._BASES[rng.integers(0, 4, 50_000)]]
+    view = index_build.build_view(g)
+    ctx.load_index(view)
+    orc = Oracle(view)
+    rs = synth.sample_reads(g, 600, seed=92)
+    for ps in (dict(min_len=13, max_evalue=0.01, max_nseed=500, mode=0),
+               dict(min_len=13, max_evalue=0.01, max_nseed=30, mode=0)):
+        res = ctx.map(rs.seqs, rs.offs, lib.default_params(**ps))
+        st = ctx.stats()
+        compare_with_oracle(res, orc, rs.read, len(rs), g, **ps)
+        assert st["n_smem_rerun"] > 0
+        if ps["max_nseed"] == 30:
+            assert st["host_sorted"] > 0
+
+
 def test_unsupported_inputs_fail_loudly(ctx):
     g = synth.small_genomes(seed=41, n_genomes=1, length=5000)
     view = index_build.build_view(g)
