@@ -325,8 +325,9 @@ int msg_ctx_set_dp_lanes(msg_ctx* ctx, int32_t bits);
  * registers sized for 4 blocks of 128 threads per SM, 2: for 3); 3 and 4 =
  * one read per thread, the candidates of one pass of findFwdBackSMEMS /
  * findBackFwdSMEMS (SMEM.cpp:93-116, 148-171) extended up to 4 (3) or 2 (4)
- * at a time, their bucket loads in flight together. Results do not depend
- * on it. */
+ * at a time, their bucket loads in flight together; 5 and 6 = variant 0 with
+ * registers sized for 6 and 8 resident blocks of 128 threads per SM (more
+ * warps, some spilling) instead of 5. Results do not depend on it. */
 int msg_ctx_set_smem_shape(msg_ctx* ctx, int32_t variant);
 
 /* The shapes chosen by msg_autotune, with the stage times that chose them. */

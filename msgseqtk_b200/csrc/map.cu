@@ -476,10 +476,11 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         CK(cudaMemsetAsync(d_status, 0, 4, st));
         // short reads on the thread kernel
         if (thread_path) {
-            // one read per thread (ctx->smem_variant 0), two per thread (1
-            // and 2: each thread keeps two extensions' loads in flight), or
-            // one per thread with a pass's entries extended up to 4 (3) or 2
-            // (4) at a time
+            // one read per thread (ctx->smem_variant 0; 5 and 6: registers
+            // sized for 6 and 8 resident blocks), two per thread (1 and 2:
+            // each thread keeps two extensions' loads in flight), or one per
+            // thread with a pass's entries extended up to 4 (3) or 2 (4) at a
+            // time
             const int var = ctx->smem_variant;
             const bool pair = var == 1 || var == 2;
             int bps = 0;
@@ -487,7 +488,9 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             else if (var == 2) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread2<3>, 128, 0));
             else if (var == 3) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_pass<4, 4>, 128, 0));
             else if (var == 4) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_pass<2, 5>, 128, 0));
-            else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread, 128, 0));
+            else if (var == 5) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<6>, 128, 0));
+            else if (var == 6) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<8>, 128, 0));
+            else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<5>, 128, 0));
             const int64_t n_thr = (int64_t)ctx->num_sms * std::max(1, bps) * 128;
             const int64_t pv_cap = kThreadPrev;
             CK(ctx->prev.ensure((pair ? 2 : 1) * n_thr * pv_cap * sizeof(PrevEntry) + 64));
@@ -506,7 +509,9 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             else if (var == 2) S.n_launch++, k_smem_thread2<3><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else if (var == 3) S.n_launch++, k_smem_pass<4, 4><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else if (var == 4) S.n_launch++, k_smem_pass<2, 5><<<n_thr / 128, 128, 0, st>>>(ta, ix);
-            else S.n_launch++, k_smem_thread<<<n_thr / 128, 128, 0, st>>>(ta, ix);
+            else if (var == 5) S.n_launch++, k_smem_thread<6><<<n_thr / 128, 128, 0, st>>>(ta, ix);
+            else if (var == 6) S.n_launch++, k_smem_thread<8><<<n_thr / 128, 128, 0, st>>>(ta, ix);
+            else S.n_launch++, k_smem_thread<5><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             CK(cudaGetLastError());
         }
         // long reads (all reads when no read is short) on the warp kernel
@@ -1664,7 +1669,7 @@ extern "C" int msg_ctx_set_dp_lanes(msg_ctx* ctx, int32_t bits) {
 }
 
 extern "C" int msg_ctx_set_smem_shape(msg_ctx* ctx, int32_t variant) {
-    if (!ctx || variant < 0 || variant > 4) return MSG_EINVAL;
+    if (!ctx || variant < 0 || variant > 6) return MSG_EINVAL;
     ctx->smem_variant = variant;
     return MSG_OK;
 }
@@ -1702,7 +1707,7 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
     double best_smem = 0, best_dp = 0, ts = 0, td = 0;
     if ((rc = time_shape(best_var, best_k, best_small, best_warp, &best_smem, &best_dp)) != MSG_OK) return rc;
     const double smem_default = best_smem, dp_default = best_dp;
-    for (int var : {1, 2, 3, 4}) {
+    for (int var : {1, 2, 3, 4, 5, 6}) {
         if ((rc = time_shape(var, best_k, best_small, best_warp, &ts, &td)) != MSG_OK) return rc;
         if (ts < best_smem) { best_smem = ts; best_var = var; }
     }

@@ -312,7 +312,9 @@ __device__ __forceinline__ bool smem_next_read(ThreadSmem& t, const SmemThreadAr
     return true;
 }
 
-__global__ void __launch_bounds__(128, 5) k_smem_thread(SmemThreadArgs a, IndexDev ix) {
+// MINB: resident blocks of 128 threads per SM the registers are sized for.
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_smem_thread(SmemThreadArgs a, IndexDev ix) {
     if (threadIdx.x < 16) s_llk[threadIdx.x] = a.llk[threadIdx.x];
     __syncthreads();
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
