@@ -1047,23 +1047,27 @@ struct ChainCtx {
         return cells;
     }
 
-    // Two-stripe fill in 16-bit lanes (GLOBAL mode, whole rectangle; the
-    // chain fits16): one thread fills 32 rows at a time as two 16-row
-    // stripes held in the two halves of 16 registers per matrix, the lower
-    // stripe one column behind the upper, so that within an iteration the
-    // halves are independent (the lower stripe's row above is the upper
-    // stripe's last row, finished one iteration earlier; an extra iteration
-    // ends the lower stripe, a first dummy one starts it from the left
-    // boundary). Each instruction updates two cells: __vibmax_s16x2 gives a
-    // maximum with its comparison outcomes (the traceback code bits),
-    // __viaddmax_s16x2 / __viaddmin_s16x2 the gap and score terms. A cell's
-    // score comes from its row's bit in the stripe table word of its
-    // column's target code (bits 0-15 upper rows, 16-31 lower rows), moved
-    // to a byte's top bit and widened to a 16-bit mask by a byte permute.
-    // Codes and last row/column go where fill_rect_stripe<16> puts them (the
-    // last row/column in 32-bit values), so the traceback reads both alike.
-    // The row buffer holds 16-bit values here. Returns the cells evaluated.
-    __device__ __noinline__ int64_t fill_rect_stripe16(int m) {
+    // Two-stripe fill in 16-bit lanes (GLOBAL mode; the chain fits16): one
+    // thread fills 32 rows at a time as two 16-row stripes held in the two
+    // halves of 16 registers per matrix, the lower stripe one column behind
+    // the upper, so that within an iteration the halves are independent (the
+    // lower stripe's row above is the upper stripe's last row, finished one
+    // iteration earlier; an extra iteration ends the lower stripe, the first
+    // one starts it from the left boundary). Each instruction updates two
+    // cells: __vibmax_s16x2 gives a maximum with its comparison outcomes (the
+    // traceback code bits), __viaddmax_s16x2 / __viaddmin_s16x2 the gap and
+    // score terms. A cell's score comes from its row's bit in the stripe
+    // table word of its column's target code (bits 0-15 upper rows, 16-31
+    // lower rows), moved to a byte's top bit and widened to a 16-bit mask by
+    // a byte permute. BANDED (w >= 0): only the cells within w diagonals of
+    // the adjacent seed's diagonal count, the others are -inf (masked to 0
+    // through a per-column bitmap of the rows in band), as fill_rect_stripe
+    // does; each half runs over its own band's columns. Codes and last
+    // row/column go where fill_rect_stripe<16> puts them (the last row and
+    // column in 32-bit values), so the traceback reads both alike. The row
+    // buffer holds 16-bit values here. Returns the cells evaluated.
+    template <bool BANDED>
+    __device__ __noinline__ int64_t fill_rect_stripe16(int m, int w) {
         constexpr int K = 16;
         const RectGeo g = rect(m);
         if (g.R <= 0 || g.C <= 0) return 0;
@@ -1075,15 +1079,30 @@ struct ChainCtx {
         const int64_t tgt_n = target_avail - g.c0;
         uint32_t* const tab = stab;
         auto tbase = [&](int c) -> int { return c < tgt_n ? (int)__ldg(tgt + c) : 0; };
-        for (int c = 0; c < C; ++c) {  // the top boundary row
+        const int dg = m == 0 ? C - R : 0;  // column - row of the seed's diagonal in this rectangle
+        if (BANDED) {
+            for (int c = 0; c < 3 * C; ++c) g.lastrow[c] = NEG;
+            for (int c = 0; c < 3 * R; ++c) g.lastcol[c] = NEG;
+        }
+        int plo = 0, phi = C - 1;  // columns of the row buffer that hold the row above
+        if (BANDED) { plo = max(0, dg - w - 1); phi = min(C - 1, dg + w); }
+        for (int c = plo; c <= phi; ++c) {  // the top boundary row
             const int3 v = boundary(m, g.r0, g.c0 + 1 + c);
             rb4[c] = make_int4((int)to16(v.x), (int)to16(v.y), (int)to16(v.z), 0);
         }
+        int64_t cells = 0;
         const int nds = (R + 2 * K - 1) / (2 * K);
         for (int ds = 0; ds < nds; ++ds) {
             const int rr0 = ds * 2 * K;
             const int nlo = min(K, R - rr0), nhi = max(0, min(K, R - rr0 - K));
             const int64_t i0 = g.r0 + 1 + rr0;  // matrix row of the upper stripe's first row
+            // columns of each half: all, or its rows' band
+            int clo = 0, chi = C - 1, hlo = 0, hhi = nhi > 0 ? C - 1 : -1;
+            if (BANDED) {
+                clo = max(0, rr0 + dg - w); chi = min(C - 1, rr0 + nlo - 1 + dg + w);
+                if (nhi > 0) { hlo = max(0, rr0 + K + dg - w); hhi = min(C - 1, rr0 + K + nhi - 1 + dg + w); }
+                if (clo > chi) { plo = 1; phi = 0; continue; }  // no band cell left in this rectangle
+            }
             {
                 uint32_t tbits[16];
 #pragma unroll
@@ -1097,48 +1116,76 @@ struct ChainCtx {
 #pragma unroll
                 for (int t = 0; t < 16; ++t) tab[t * kStripeThreads] = tbits[t];
             }
-            // diagonal inputs of row 0 of each half at the next iteration:
-            // upper (row above the stripe, previous column), lower (upper
-            // stripe's last row two columns back)
-            const int3 cv = boundary(m, i0 - 1, g.c0);
-            uint32_t dlM = to16(cv.x), dlI = to16(cv.y), dlD = to16(cv.z);
-            // the left boundary (column c0) of the pair's rows, parked in the
-            // rectangle's last-column slots until the loop reads it (those
-            // slots get their final values at the last column)
-            for (int k = 0; k < nlo + nhi; ++k) {
-                const int3 v = boundary(m, i0 + k, g.c0);
-                int32_t* lc = g.lastcol + (int64_t)(rr0 + k) * 3;
-                lc[0] = v.x; lc[1] = v.y; lc[2] = v.z;
+            // the left boundary (column c0) of the pair's rows when the band
+            // reaches it, parked in the rectangle's last-column slots until
+            // the loop reads it (those slots get their final values at the
+            // last column); -inf (0) left of a band
+            const bool left = clo == 0;
+            if (left) {
+                for (int k = 0; k < nlo + nhi; ++k) {
+                    const int3 v = boundary(m, i0 + k, g.c0);
+                    int32_t* lc = g.lastcol + (int64_t)(rr0 + k) * 3;
+                    lc[0] = v.x; lc[1] = v.y; lc[2] = v.z;
+                }
             }
-            // the previous column's values: the upper rows' left boundary (the
-            // lower halves are set after the first iteration)
             uint32_t Mp[K], Ip[K], Dp[K];
 #pragma unroll
             for (int k = 0; k < K; ++k) {
                 Mp[k] = 0u; Ip[k] = 0u; Dp[k] = 0u;
-                if (k < nlo) {
-                    const int32_t* lc = g.lastcol + (int64_t)(rr0 + k) * 3;
+                if (left && k < nlo) {
+                    int32_t* lc = g.lastcol + (int64_t)(rr0 + k) * 3;
                     Mp[k] = to16(lc[0]); Ip[k] = to16(lc[1]); Dp[k] = to16(lc[2]);
+                    if (BANDED) { lc[0] = NEG; lc[1] = NEG; lc[2] = NEG; }  // a band may not reach the last column
                 }
+            }
+            // diagonal inputs of row 0 of each half at the next iteration:
+            // upper (row above the pair, previous column), lower (upper
+            // stripe's last row two columns back)
+            uint32_t dlM = 0u, dlI = 0u, dlD = 0u;
+            if (left) {
+                const int3 cv = boundary(m, i0 - 1, g.c0);
+                dlM = to16(cv.x); dlI = to16(cv.y); dlD = to16(cv.z);
+            } else if (clo - 1 >= plo && clo - 1 <= phi) {
+                const int4 v = rb4[clo - 1];
+                dlM = (uint32_t)v.x; dlI = (uint32_t)v.y; dlD = (uint32_t)v.z;
             }
             uint32_t dhM = 0u, dhI = 0u, dhD = 0u;
             uint8_t* const code_lo = g.code + (int64_t)(2 * ds) * C * K;
             uint8_t* const code_hi = code_lo + (int64_t)C * K;
             const bool last = ds == nds - 1;
             const int lr = R - 1 - rr0;  // the rectangle's last row within this pair (last pair)
-            const int iters = nhi > 0 ? C + 1 : C;
-            int4 up_next = rb4[0];
-            int tb_next = tbase(0);
-            uint32_t tprev = 0u;
-            for (int cc = 0; cc < iters; ++cc) {
-                const int4 up = up_next;  // upper stripe: the row above at column cc
+            const int cend = nhi > 0 ? max(chi, hhi + 1) : chi;  // last iteration
+            auto up_of = [&](int c) -> int4 {
+                return (!BANDED || (c >= plo && c <= phi)) ? rb4[c] : make_int4(0, 0, 0, 0);
+            };
+            int4 up_next = up_of(clo);
+            int tb_next = tbase(clo);
+            uint32_t tprev = clo > 0 ? tab[(tbase(clo - 1) & 15) * kStripeThreads] : 0u;
+            for (int cc = clo; cc <= cend; ++cc) {
+                const int4 up = up_next;  // upper stripe: the row above at column cc (cc <= chi)
                 const uint32_t tw = tab[(tb_next & 15) * kStripeThreads];
-                if (cc + 1 < C) {
-                    up_next = rb4[cc + 1];
+                if (cc + 1 <= min(chi, C - 1)) {
+                    up_next = up_of(cc + 1);
                     tb_next = tbase(cc + 1);
+                } else {
+                    up_next = make_int4(0, 0, 0, 0);
+                    tb_next = cc + 1 < C ? tbase(cc + 1) : 0;
                 }
                 const uint32_t cw = (tw & 0xFFFFu) | (tprev & 0xFFFF0000u);
                 tprev = tw;
+                // rows in band at this iteration: upper rows at column cc,
+                // lower rows at column cc - 1 (bits 0-15, 16-31)
+                uint32_t band = 0xFFFFFFFFu;
+                if (BANDED) {
+                    // row k of a half is in band when its column minus its row
+                    // minus dg lies in [-w, w]
+                    const int bl = cc - rr0 - dg + w, bh = cc - 1 - rr0 - K - dg + w;
+                    const int l0 = max(0, bl - 2 * w), l1 = min(K - 1, bl);
+                    const int h0 = max(0, bh - 2 * w), h1 = min(K - 1, bh);
+                    const uint32_t ml = (l0 <= l1 && cc <= chi) ? ((0xFFFFu >> (15 - l1 + l0)) << l0) : 0u;
+                    const uint32_t mh = (h0 <= h1 && cc - 1 >= hlo && cc - 1 <= hhi) ? ((0xFFFFu >> (15 - h1 + h0)) << h0) : 0u;
+                    band = ml | (mh << 16);
+                }
                 uint32_t uM = pk16((uint32_t)up.x, Mp[K - 1]), uI = pk16((uint32_t)up.y, Ip[K - 1]);
                 uint32_t dM = pk16(dlM, dhM), dI = pk16(dlI, dhI), dD = pk16(dlD, dhD);
                 dlM = (uint32_t)up.x; dlI = (uint32_t)up.y; dlD = (uint32_t)up.z;
@@ -1153,11 +1200,15 @@ struct ChainCtx {
                     bool aIh, aIl, aDh, aDl, bIh, bIl, bDh, bDl;
                     const uint32_t t1 = __vibmax_s16x2(dM, dI, &aIh, &aIl);
                     const uint32_t mx = __vibmax_s16x2(t1, dD, &aDh, &aDl);
-                    const uint32_t mv = __viaddmin_s16x2(mx, mx, __viaddmax_s16x2(mx, s2, 0u));
+                    uint32_t mv = __viaddmin_s16x2(mx, mx, __viaddmax_s16x2(mx, s2, 0u));
                     const uint32_t a1 = __viaddmax_s16x2(uM, O2, 0u);
-                    const uint32_t iv = __vibmax_s16x2(__viaddmax_s16x2(uI, E2, 0u), a1, &bIh, &bIl);
+                    uint32_t iv = __vibmax_s16x2(__viaddmax_s16x2(uI, E2, 0u), a1, &bIh, &bIl);
                     const uint32_t b1 = __viaddmax_s16x2(Mp[k], O2, 0u);
-                    const uint32_t dv = __vibmax_s16x2(__viaddmax_s16x2(Dp[k], E2, 0u), b1, &bDh, &bDl);
+                    uint32_t dv = __vibmax_s16x2(__viaddmax_s16x2(Dp[k], E2, 0u), b1, &bDh, &bDl);
+                    if (BANDED) {  // cells outside the band are -inf
+                        const uint32_t in = halfmask16(band << (15 - k));
+                        mv &= in; iv &= in; dv &= in;
+                    }
                     // matchMax (I over M, then D only when I does not win), insMax, delMax
                     const uint32_t cl = (aIl ? (aDl ? 0u : 2u) : 1u) | (bIl ? 0u : 4u) | (bDl ? 0u : 8u);
                     const uint32_t ch = (aIh ? (aDh ? 0u : 2u) : 1u) | (bIh ? 0u : 4u) | (bDh ? 0u : 8u);
@@ -1167,7 +1218,7 @@ struct ChainCtx {
                     Mp[k] = mv; Ip[k] = iv; Dp[k] = dv;
                     uM = mv; uI = iv;
                 }
-                if (cc < C) {  // upper stripe: column cc
+                if (cc <= chi) {  // upper stripe: column cc
                     reinterpret_cast<uint4*>(code_lo + (int64_t)cc * K)[0] = make_uint4(wl[0], wl[1], wl[2], wl[3]);
                     if (last && lr < K) {
                         uint32_t lm = Mp[0], li = Ip[0], ld = Dp[0];
@@ -1188,17 +1239,18 @@ struct ChainCtx {
                     }
                 }
                 if (nhi > 0) {
-                    if (cc == 0) {  // the lower stripe starts from its left boundary
+                    if (cc == clo) {  // the lower stripe starts from its left boundary (-inf left of a band)
 #pragma unroll
                         for (int k = 0; k < K; ++k) {
                             uint32_t hm = 0u, hi = 0u, hd = 0u;
-                            if (k < nhi) {
-                                const int32_t* lc = g.lastcol + (int64_t)(rr0 + K + k) * 3;
+                            if (left && k < nhi) {
+                                int32_t* lc = g.lastcol + (int64_t)(rr0 + K + k) * 3;
                                 hm = to16(lc[0]); hi = to16(lc[1]); hd = to16(lc[2]);
+                                if (BANDED) { lc[0] = NEG; lc[1] = NEG; lc[2] = NEG; }
                             }
                             Mp[k] = pk16(Mp[k], hm); Ip[k] = pk16(Ip[k], hi); Dp[k] = pk16(Dp[k], hd);
                         }
-                    } else {  // lower stripe: column cc - 1
+                    } else if (cc - 1 >= hlo && cc - 1 <= hhi) {  // lower stripe: column cc - 1
                         const int c1 = cc - 1;
                         reinterpret_cast<uint4*>(code_hi + (int64_t)c1 * K)[0] = make_uint4(wh[0], wh[1], wh[2], wh[3]);
                         if (nhi == K)
@@ -1223,8 +1275,10 @@ struct ChainCtx {
                     }
                 }
             }
+            cells += (int64_t)nlo * (chi - clo + 1) + (nhi > 0 ? (int64_t)nhi * (hhi - hlo + 1) : 0);
+            if (BANDED) { plo = hhi >= 0 && nhi > 0 ? hlo : clo; phi = nhi > 0 ? hhi : chi; }
         }
-        return (int64_t)R * C;
+        return cells;
     }
 
     // Warp fill of the band of rectangle m (m = 0 or 2n; GLOBAL mode): the
@@ -1689,7 +1743,7 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
     // unbanded stripe chains in GLOBAL mode whose values fit 16-bit lanes
     // run the two-stripe 16-bit fill (codes in 16-row stripes)
     const int64_t w1 = max(max(a.pp.match, a.pp.mismatch), a.pp.gap_o + a.pp.gap_e);
-    const bool use16 = !WARP && KST > 0 && !BAND && a.lanes16 && a.pp.mode == 0 && (x.L + x.T + 1) * w1 < kBias16;
+    const bool use16 = !WARP && KST > 0 && a.lanes16 && a.pp.mode == 0 && (x.L + x.T + 1) * w1 < kBias16;
     x.kst = use16 ? 16 : KST;
     x.stab = stab;
     // geometry in sd/rbnd/cbnd; a warp working in shared memory also leaves a
@@ -1755,11 +1809,12 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
         if constexpr (!WARP && KST > 0) {
             if constexpr (BAND) {
                 if (w >= 0) {
-                    cells += x.template fill_rect_stripe<KST, false, true>(m, w, best, bkey);
+                    if (use16) cells += x.template fill_rect_stripe16<true>(m, w);
+                    else cells += x.template fill_rect_stripe<KST, false, true>(m, w, best, bkey);
                     return;
                 }
             }
-            if (use16) cells += x.fill_rect_stripe16(m);
+            if (use16) cells += x.template fill_rect_stripe16<false>(m, -1);
             else if (x.pp.mode == 1) cells += x.template fill_rect_stripe<KST, true, false>(m, -1, best, bkey);
             else cells += x.template fill_rect_stripe<KST, false, false>(m, -1, best, bkey);
         } else if constexpr (!WARP) {
