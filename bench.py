@@ -607,7 +607,7 @@ def main():
 
     counters = ("n_ext", "dp_cells", "dp_cells_done", "n_reads", "n_launch", "n_aln", "host_sorted", "n_sa",
                 "n_chain", "n_band_exact", "n_band_drop", "n_band_fallback", "n_filtered", "n_dp_warp",
-                "n_smem_rerun", "smem_retries")
+                "n_smem_rerun", "smem_retries", "n_ext_ff")
 
     def timed(prm, clocks=None):
         """W warm-up steps, then K timed steps on new batches (inputs larger

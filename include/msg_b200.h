@@ -204,6 +204,7 @@ typedef struct msg_map_stats {
     int64_t dp_class_cells[5]; /* cells computed per class (recomputations count with the warp class) */
     int64_t n_smem_rerun;   /* reads the one-thread SMEM kernel gave to the warp kernel (candidate list too long) */
     int64_t smem_retries;   /* SMEM stage reruns with larger output slots */
+    int64_t n_ext_ff;       /* bi-interval extensions of unique matches done by text comparison instead */
 } msg_map_stats;
 
 /* Map a batch of reads held in HOST memory: the per-read SE task body
@@ -327,7 +328,12 @@ int msg_ctx_set_dp_lanes(msg_ctx* ctx, int32_t bits);
  * findBackFwdSMEMS (SMEM.cpp:93-116, 148-171) extended up to 4 (3) or 2 (4)
  * at a time, their bucket loads in flight together; 5 and 6 = variant 0 with
  * registers sized for 6 and 8 resident blocks of 128 threads per SM (more
- * warps, some spilling) instead of 5. Results do not depend on it. */
+ * warps, some spilling) instead of 5; 7 = variant 0 without the
+ * fast-forward over unique matches (0, 5 and 6 replace a run of
+ * extensions of a size-1 interval -- a walk's, or a pass's single
+ * candidate's -- by comparing the read with the BD text before the match's
+ * suffix-array position and one inverse-suffix-array lookup). Results do
+ * not depend on it. */
 int msg_ctx_set_smem_shape(msg_ctx* ctx, int32_t variant);
 
 /* The shapes chosen by msg_autotune, with the stage times that chose them. */

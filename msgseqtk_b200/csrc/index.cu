@@ -89,6 +89,17 @@ __global__ void k_mark_starts(const int64_t* __restrict__ rows, int64_t m, uint3
 // rows of the preceding text positions until the next start row. LF never
 // crosses a '$' because rows whose BWT symbol is '$' are SA samples
 // (FMDIndex.cpp:465-480) and end every walk.
+// The BD text from the BWT and the suffix array (text[sa[i] - 1] = bwt[i],
+// cyclically), and the inverse suffix array.
+__global__ void k_text_isa(const uint8_t* __restrict__ bwt, const uint32_t* __restrict__ sa, int64_t n,
+                           uint8_t* __restrict__ text, uint32_t* __restrict__ isa) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = sa[i];
+        isa[p] = (uint32_t)i;
+        text[p == 0 ? n - 1 : p - 1] = bwt[i];
+    }
+}
+
 __global__ void k_recover_sa(IndexDev ix, const int64_t* __restrict__ rows, const int64_t* __restrict__ vals,
                              int64_t m, const uint32_t* __restrict__ start_bits, uint32_t* __restrict__ sa,
                              uint32_t* __restrict__ err, int64_t max_walk) {
@@ -390,6 +401,15 @@ extern "C" int msg_index_load(msg_ctx* ctx, const msg_fmd_view* fmd, const msg_m
         CK(cudaMemcpy(&bad, d_bad, sizeof(uint32_t), cudaMemcpyDeviceToHost));
         if (bad) { rc = ctx->fail(MSG_EINTERNAL, "suffix-array recovery did not terminate"); goto done; }
         ix.sa = im.sa;
+        // the text and inverse suffix array the SMEM kernel's fast-forward
+        // over unique matches reads
+        CK(cudaMalloc(&im.text, n + 32));
+        CK(cudaMalloc(&im.isa, n * sizeof(uint32_t)));
+        CK(cudaMemsetAsync(im.text + n, 0, 32, st));
+        k_text_isa<<<ctx->num_sms * 16, 256, 0, st>>>(d_bwt, im.sa, n, im.text, im.isa);
+        CK(cudaGetLastError());
+        ix.text = im.text;
+        ix.isa = im.isa;
     }
     // chromosome table and targets
     {
@@ -409,7 +429,7 @@ extern "C" int msg_index_load(msg_ctx* ctx, const msg_fmd_view* fmd, const msg_m
         ix.chr_seq = im.chr_seq;
         ix.n_chrom = nc;
         im.chr_len_host.assign(mtg->chr_len, mtg->chr_len + nc);
-        im.bytes = nb * sizeof(Bucket) + B[0] * sizeof(int64_t) + n * sizeof(uint32_t) + 4 * nc * 8 + tl +
+        im.bytes = nb * sizeof(Bucket) + B[0] * sizeof(int64_t) + 2 * n * sizeof(uint32_t) + n + 4 * nc * 8 + tl +
                    (B[15] > 0 ? B[15] * (int64_t)sizeof(int64_t) + nb * (int64_t)sizeof(uint32_t) : 0);
         CK(cudaStreamSynchronize(st));
     }

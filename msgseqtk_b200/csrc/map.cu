@@ -472,7 +472,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         CK(ctx->smem.ensure((size_t)std::max<int64_t>(1, h_rows) * 48));
         CK(ctx->smem_cnt.ensure((n_reads + 1) * sizeof(int32_t)));
         CK(cudaMemsetAsync(d_ctr, 0, 8 * 4, st));
-        CK(cudaMemsetAsync(d_ctr + 7, 0, 8, st));
+        CK(cudaMemsetAsync(d_ctr + 7, 0, 16, st));
         CK(cudaMemsetAsync(d_status, 0, 4, st));
         // short reads on the thread kernel
         if (thread_path) {
@@ -488,9 +488,10 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             else if (var == 2) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread2<3>, 128, 0));
             else if (var == 3) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_pass<4, 4>, 128, 0));
             else if (var == 4) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_pass<2, 5>, 128, 0));
-            else if (var == 5) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<6>, 128, 0));
-            else if (var == 6) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<8>, 128, 0));
-            else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<5>, 128, 0));
+            else if (var == 5) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<6, true>, 128, 0));
+            else if (var == 6) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<8, true>, 128, 0));
+            // variant 7: variant 0 without the fast-forward over unique matches
+            else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<5, true>, 128, 0));
             const int64_t n_thr = (int64_t)ctx->num_sms * std::max(1, bps) * 128;
             const int64_t pv_cap = kThreadPrev;
             CK(ctx->prev.ensure((pair ? 2 : 1) * n_thr * pv_cap * sizeof(PrevEntry) + 64));
@@ -505,13 +506,18 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             ta.prev = ctx->prev.as<PrevEntry>(); ta.pv_cap = pv_cap;
             ta.work = d_ctr; ta.n_ext = d_ctr + 1; ta.status = d_status;
             ta.ovf_list = d_ovf; ta.ovf_n = d_ctr + 7;
+            ta.n_ffx = d_ctr + 8;
+            const bool ff = ctx->smem_ff && ix.text && ix.isa;
             if (var == 1) S.n_launch++, k_smem_thread2<4><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else if (var == 2) S.n_launch++, k_smem_thread2<3><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else if (var == 3) S.n_launch++, k_smem_pass<4, 4><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else if (var == 4) S.n_launch++, k_smem_pass<2, 5><<<n_thr / 128, 128, 0, st>>>(ta, ix);
-            else if (var == 5) S.n_launch++, k_smem_thread<6><<<n_thr / 128, 128, 0, st>>>(ta, ix);
-            else if (var == 6) S.n_launch++, k_smem_thread<8><<<n_thr / 128, 128, 0, st>>>(ta, ix);
-            else S.n_launch++, k_smem_thread<5><<<n_thr / 128, 128, 0, st>>>(ta, ix);
+            else if (var == 5 && ff) S.n_launch++, k_smem_thread<6, true><<<n_thr / 128, 128, 0, st>>>(ta, ix);
+            else if (var == 5) S.n_launch++, k_smem_thread<6, false><<<n_thr / 128, 128, 0, st>>>(ta, ix);
+            else if (var == 6 && ff) S.n_launch++, k_smem_thread<8, true><<<n_thr / 128, 128, 0, st>>>(ta, ix);
+            else if (var == 6) S.n_launch++, k_smem_thread<8, false><<<n_thr / 128, 128, 0, st>>>(ta, ix);
+            else if (ff) S.n_launch++, k_smem_thread<5, true><<<n_thr / 128, 128, 0, st>>>(ta, ix);
+            else S.n_launch++, k_smem_thread<5, false><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             CK(cudaGetLastError());
         }
         // long reads (all reads when no read is short) on the warp kernel
@@ -550,11 +556,13 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     // later batches start from this batch's capacity (bounded: rarer reads
     // that need more still get their rerun)
     ctx->smem_cap = std::min<int64_t>(std::max(ctx->smem_cap, cap), 256);
-    // the extension count arrives with the next synchronisation
+    // the extension counts arrive with the next synchronisation
     CK(cudaMemcpyAsync(ctx->hpin + 8, d_ctr + 1, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(ctx->hpin + 10, d_ctr + 8, 8, cudaMemcpyDeviceToHost, st));
     if (n_reads > 0) S.n_launch++, k_i32_to_i64<<<nblk(n_reads, 256), 256, 0, st>>>(ctx->smem_cnt.as<int32_t>(), d_cnt64, n_reads);
     CK(offsets(ctx, d_cnt64, n_reads, d_smem_off, misc, &h_nsmem));
     S.n_ext = ctx->hpin[8];
+    S.n_ext_ff = ctx->hpin[10];
     CK(setup_sel());
     if (n_reads > 0) {
         S.n_launch++, k_compact_smem<<<nblk(n_reads * 32, 256), 256, 0, st>>>(ctx->smem.as<int64_t>(), d_slot_off,
@@ -1669,8 +1677,9 @@ extern "C" int msg_ctx_set_dp_lanes(msg_ctx* ctx, int32_t bits) {
 }
 
 extern "C" int msg_ctx_set_smem_shape(msg_ctx* ctx, int32_t variant) {
-    if (!ctx || variant < 0 || variant > 6) return MSG_EINVAL;
-    ctx->smem_variant = variant;
+    if (!ctx || variant < 0 || variant > 7) return MSG_EINVAL;
+    ctx->smem_ff = variant != 7;
+    ctx->smem_variant = variant == 7 ? 0 : variant;
     return MSG_OK;
 }
 
@@ -1687,7 +1696,8 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
     int best_lanes = 16;
     auto time_shape = [&](int var, int k, int64_t small, int64_t warp, double* ms_smem, double* ms_dp) -> int {
         ctx->dp_lanes = best_lanes;
-        ctx->smem_variant = var;
+        ctx->smem_ff = var != 7;
+        ctx->smem_variant = var == 7 ? 0 : var;
         ctx->dp_k = k;
         ctx->dp_small_area = small;
         ctx->dp_warp_area = warp;
@@ -1707,7 +1717,7 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
     double best_smem = 0, best_dp = 0, ts = 0, td = 0;
     if ((rc = time_shape(best_var, best_k, best_small, best_warp, &best_smem, &best_dp)) != MSG_OK) return rc;
     const double smem_default = best_smem, dp_default = best_dp;
-    for (int var : {1, 2, 3, 4, 5, 6}) {
+    for (int var : {1, 2, 3, 4, 5, 6, 7}) {
         if ((rc = time_shape(var, best_k, best_small, best_warp, &ts, &td)) != MSG_OK) return rc;
         if (ts < best_smem) { best_smem = ts; best_var = var; }
     }
@@ -1728,7 +1738,8 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
     if (td < best_dp) best_dp = td;
     else best_lanes = 16;
     ctx->dp_lanes = best_lanes;
-    ctx->smem_variant = best_var;
+    ctx->smem_ff = best_var != 7;
+    ctx->smem_variant = best_var == 7 ? 0 : best_var;
     ctx->dp_k = best_k;
     ctx->dp_small_area = best_small;
     ctx->dp_warp_area = best_warp;

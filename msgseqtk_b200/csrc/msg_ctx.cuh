@@ -21,6 +21,8 @@ struct IndexImage {
     int64_t* n_rows = nullptr;
     uint32_t* n_before = nullptr;
     uint32_t* sa = nullptr;
+    uint8_t* text = nullptr;
+    uint32_t* isa = nullptr;
     int64_t* chr_tab = nullptr;
     uint8_t* chr_seq = nullptr;
     int64_t B[16] = {0};
@@ -94,6 +96,7 @@ struct msg_ctx {
     // larger ones on a warp
     int dp_k = 16;
     int dp_lanes = 16;     // 16: unbanded GLOBAL stripe chains that fit use 16-bit lanes (msg_ctx_set_dp_lanes)
+    int smem_ff = 1;       // SMEM walks and single-entry passes skip unique matches by text comparison (variant 7: off)
     int smem_variant = 0;  // SMEM thread path (msg_ctx_set_smem_shape): 0 one read per thread, 1/2 two,
                            // 3/4 a pass's candidates extended several at a time
     int64_t smem_cap = 16;  // SMEM rows per 150 read bases the slots start with (grows after an overflow)
@@ -149,6 +152,8 @@ struct msg_ctx {
         if (idx.n_rows) cudaFree(idx.n_rows);
         if (idx.n_before) cudaFree(idx.n_before);
         if (idx.sa) cudaFree(idx.sa);
+        if (idx.text) cudaFree(idx.text);
+        if (idx.isa) cudaFree(idx.isa);
         if (idx.chr_tab) cudaFree(idx.chr_tab);
         if (idx.chr_seq) cudaFree(idx.chr_seq);
         idx = msg::IndexImage();

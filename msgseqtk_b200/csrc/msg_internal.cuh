@@ -52,6 +52,8 @@ struct IndexDev {
     int64_t n_n;
     const uint32_t* n_before;  // per bucket: N before it (null when n_n == 0)
     const uint32_t* sa;
+    const uint8_t* text;       // the BD text (nt16 codes, '$' = 0) that the suffix array indexes, 16 bytes of slack
+    const uint32_t* isa;       // inverse suffix array: isa[sa[i]] = i
     int64_t n;
     int64_t C[17];           // FMDIndex::C for nt16 codes 0..16
     const int64_t* bd_start; // per chromosome

@@ -49,6 +49,7 @@ struct SmemThreadArgs {
     int64_t pv_cap;
     unsigned long long* work;
     unsigned long long* n_ext;
+    unsigned long long* n_ffx;   // extensions replaced by the fast-forward over unique matches
     uint32_t* status;
     int64_t* ovf_list;      // reads abandoned because their candidate list outgrew pv_cap (rerun on k_smem)
     unsigned long long* ovf_n;
@@ -90,7 +91,7 @@ struct ThreadSmem {
     uint32_t wp0, wq0, s0w;
     int32_t n_prev;
     int32_t pv_base;        // the list is pv[pv_base .. pv_base + n_prev), longest first
-    int32_t ovf;            // a push found the list full: this read is abandoned (the batch reruns)
+    int32_t ovf;            // a push found the list full: this read is abandoned (the warp kernel reruns it)
     // pass over prev
     int32_t k, n_keep, n_valid;
     uint32_t s0;            // running size; 0 stands for the reference's -1 (sizes compared are >= 1)
@@ -98,9 +99,56 @@ struct ThreadSmem {
     PrevEntry e0, e_next;   // entry being extended, and the next one (loaded early)
     int32_t phase;
     unsigned long long ext;
+    // fast-forward over a unique match (interval size 1): 0 none, 1 suffix
+    // array word of the row, 2 text chunks, 3 inverse-suffix-array word
+    int32_t ffst;
+    int32_t ffent;          // the fast-forward extends the pass's single entry (else the walk)
+    int32_t ffm;            // bases matched so far
+    int32_t ffdone;         // a fast-forward just ended: the next extension is an ordinary one
+    uint32_t ffp;           // the row at the start
+    uint32_t ffpos;         // text position of its string (sa[ffp])
+    unsigned long long ffx;
 
     __device__ int base(int32_t i) const { return (i >= 0 && i < L) ? (int)__ldg(rd + i) : 0; }
 };
+
+// Fast-forward over a unique match. While a walk's interval (or a pass's
+// single candidate) has size 1, its string occurs once in the BD text, at
+// sa[P], and extending it backward by base B keeps size 1 exactly when the
+// text has B just before that occurrence (the row's BWT symbol); the new row
+// is then the inverse suffix array at that position and q does not change
+// (backExt only moves q when the size changes, FMDIndex.cpp:592-604). So a
+// run of such extensions is the common prefix of the read's next bases and
+// the text read backward from sa[P] - 1, and one inverse-suffix-array lookup
+// gives the final row. Only basic read bases inside the read are taken; the
+// extension that ends the run is an ordinary one. The run's steps (the
+// suffix-array word, 16-byte text chunks, the inverse word) are steps of the
+// state machine, so that their loads issue with the other lanes' bucket
+// loads.
+//
+// Read position of the i-th base of a run (walk: at `to` going forward for
+// findFwdBackSMEMS, before `from` going backward otherwise; pass: before cf
+// or at ct), -1 past the read.
+__device__ __forceinline__ int32_t ff_read_pos(const ThreadSmem& t, int32_t i) {
+    int32_t pos;
+    if (!t.ffent) pos = t.fb ? t.mto + i : t.mfrom - 1 - i;
+    else pos = t.fb ? t.cf - 1 - i : t.ct + i;
+    return (pos >= 0 && pos < t.L) ? pos : -1;
+}
+// The oriented base the i-th extension of the run prepends (-1: not a basic
+// base inside the read): complemented when it extends the reverse strand.
+__device__ __forceinline__ int ff_base(const ThreadSmem& t, int32_t i) {
+    const int32_t pos = ff_read_pos(t, i);
+    if (pos < 0) return -1;
+    const int b = t.base(pos);
+    if (!is_basic(b)) return -1;
+    return (t.ffent ? !t.fb : t.fb) ? comp16(b) : b;
+}
+
+__device__ __forceinline__ uint32_t byte_of16(const uint4& v, int j) {
+    const uint32_t w = j < 8 ? (j < 4 ? v.x : v.y) : (j < 12 ? v.z : v.w);
+    return (w >> ((j & 3) * 8)) & 0xFFu;
+}
 
 __device__ __forceinline__ void smem_emit(ThreadSmem& t, const SmemThreadArgs& a, int32_t from, int32_t to,
                                           uint32_t p, uint32_t q, uint32_t s, double lp) {
@@ -141,6 +189,8 @@ __device__ __forceinline__ void smem_call(ThreadSmem& t, const IndexDev& ix, int
 
 // Advance the state machine until an extension is needed. On return with
 // true, (P,Q,S,B) is the backward extension to perform.
+// FF: runs over unique matches become fast-forward steps (k_smem_thread).
+template <bool FF = false>
 __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const IndexDev& ix, PrevEntry* pv,
                              uint32_t& P, uint32_t& Q, uint32_t& S, int& B) {
     for (;;) {
@@ -157,6 +207,13 @@ __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const Index
                 continue;
             case PH_WALK:
                 if (t.s >= 1) {  // extend at `to` (fb, the base past the read is 0) or before `from`
+                    if (FF && t.s == 1 && !t.ffdone) {
+                        t.ffent = 0;
+                        if (ff_base(t, 0) >= 0) {  // a run over a unique match starts
+                            t.ffst = 1; t.ffm = 0; t.ffp = t.wp;
+                            return true;
+                        }
+                    }
                     const int nb = t.fb ? t.base(t.mto) : t.base(t.mfrom - 1);
                     P = t.wp; Q = t.wq; S = t.s; B = t.fb ? comp16(nb) : nb;
                     return true;
@@ -175,6 +232,15 @@ __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const Index
                 // passes extend the other end: before cf (fb) or at ct (bf)
                 const bool more = t.fb ? t.cf >= 0 : t.ct <= t.L;
                 if (!(more && t.n_prev > 0)) { smem_return(t); continue; }
+                if (FF && t.n_prev == 1 && !t.ffdone) {
+                    const PrevEntry e = pv[t.pv_base];
+                    t.ffent = 1;
+                    if (e.s == 1 && ff_base(t, 0) >= 0) {  // the single candidate's run over a unique match
+                        t.e0 = e;
+                        t.ffst = 1; t.ffm = 0; t.ffp = e.p;
+                        return true;
+                    }
+                }
                 t.k = 0; t.n_keep = 0; t.s0 = 0; t.n_valid = 0;
                 t.b2 = t.fb ? (t.cf > 0 ? t.base(t.cf - 1) : 0) : t.base(t.ct);
                 t.e_next = pv[t.pv_base];
@@ -262,6 +328,7 @@ __device__ __forceinline__ void smem_apply_entry(ThreadSmem& t, const SmemThread
 // Apply the result of the extension requested by smem_advance.
 __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, uint32_t P, uint32_t Q,
                                            uint32_t S) {
+    t.ffdone = 0;
     if (t.phase == PH_WALK) {  // SMEM.cpp:79-86 (fb) / 134-141 (bf)
         const bool fb = t.fb;
         t.wp = P; t.wq = Q; t.s = S;
@@ -279,6 +346,43 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
         t.wp0 = t.wp; t.wq0 = t.wq; t.s0w = t.s; t.lp0 = t.lp;
     } else if (t.phase == PH_ENTRY) {
         smem_apply_entry(t, a, pv, t.e0, P, Q, S);
+    }
+}
+
+// One step of a fast-forward run with its loaded word (w.x for the
+// suffix-array and inverse words, all of w for a text chunk).
+__device__ __forceinline__ void smem_ff_apply(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, const uint4& w) {
+    if (t.ffst == 1) {  // the string's text position
+        t.ffpos = w.x;
+        t.ffst = 2;
+    } else if (t.ffst == 2) {  // compare the chunk holding text position ffpos - 1 - ffm, downward
+        const uint32_t cb = (t.ffpos - 1u - (uint32_t)t.ffm) & ~15u;  // where this step's chunk starts
+        for (;;) {
+            if ((int64_t)t.ffpos - 1 - t.ffm < 0) { t.ffst = 3; break; }  // the text starts here
+            const uint32_t x = t.ffpos - 1u - (uint32_t)t.ffm;
+            if (x < cb) return;  // chunk done: the next step loads the one below
+            const int b = ff_base(t, t.ffm);
+            if (b < 0 || b != (int)byte_of16(w, (int)(x - cb))) { t.ffst = 3; break; }
+            t.ffm++;
+        }
+        if (t.ffm == 0) { t.ffst = 0; t.ffdone = 1; }  // nothing to skip: the ordinary extension follows
+    } else {  // the final row: commit the run's ffm extensions
+        const int32_t m = t.ffm;
+        if (!t.ffent) {  // SMEM.cpp:79-86 (fb) / 134-141 (bf), m times with the size staying 1
+            for (int32_t i = 0; i < m; ++i) t.lp = __dadd_rn(t.lp, s_llk[t.base(ff_read_pos(t, i))]);
+            t.wp = w.x;
+            if (t.fb) t.mto += m; else t.mfrom -= m;
+            t.wp0 = t.wp; t.wq0 = t.wq; t.s0w = t.s; t.lp0 = t.lp;
+        } else {  // SMEM.cpp:97-112 (fb) / 152-167 (bf), m passes keeping the single entry
+            PrevEntry e = t.e0;
+            for (int32_t i = 0; i < m; ++i) e.lp = __dadd_rn(e.lp, s_llk[t.base(ff_read_pos(t, i))]);
+            e.p = w.x;
+            pv[t.pv_base] = e;
+            if (t.fb) t.cf -= m; else t.ct += m;
+        }
+        t.ffx += (unsigned long long)m;
+        t.ffst = 0;
+        t.ffdone = 1;
     }
 }
 
@@ -305,6 +409,8 @@ __device__ __forceinline__ bool smem_next_read(ThreadSmem& t, const SmemThreadAr
     t.out = a.out + 6 * slot;
     t.n_out = 0;
     t.ovf = 0;
+    t.ffst = 0;
+    t.ffdone = 0;
     if (t.L <= 0) { t.phase = PH_DONE; return true; }
     t.from = t.L / 2;  // SMEM.cpp:189-191
     t.to = t.from + 1;
@@ -312,8 +418,10 @@ __device__ __forceinline__ bool smem_next_read(ThreadSmem& t, const SmemThreadAr
     return true;
 }
 
-// MINB: resident blocks of 128 threads per SM the registers are sized for.
-template <int MINB>
+// MINB: resident blocks of 128 threads per SM the registers are sized for;
+// FF: with the fast-forward over unique matches (the index's text and
+// inverse suffix array).
+template <int MINB, bool FF>
 __global__ void __launch_bounds__(128, MINB) k_smem_thread(SmemThreadArgs a, IndexDev ix) {
     if (threadIdx.x < 16) s_llk[threadIdx.x] = a.llk[threadIdx.x];
     __syncthreads();
@@ -322,6 +430,8 @@ __global__ void __launch_bounds__(128, MINB) k_smem_thread(SmemThreadArgs a, Ind
     ThreadSmem t;
     t.phase = PH_NEXT_READ;
     t.ext = 0;
+    t.ffx = 0;
+    t.ffst = 0;
     t.n_out = 0;
     t.r = -1;
     bool alive = true;  // this lane still has reads to take
@@ -334,20 +444,36 @@ __global__ void __launch_bounds__(128, MINB) k_smem_thread(SmemThreadArgs a, Ind
                 alive = smem_next_read(t, a, ix);
                 continue;
             }
-            have = smem_advance(t, a, ix, pv, P, Q, S, B);
+            have = smem_advance<FF>(t, a, ix, pv, P, Q, S, B);
         }
         // Reconverge the warp so that every lane with a pending extension
         // issues its bucket loads in the same instructions.
         __syncwarp();
         if (!__any_sync(0xffffffffu, alive)) break;
-        if (have) {
+        // a fast-forward step's word is requested first, so that its load is
+        // in flight while the other lanes' extensions wait on theirs
+        const bool ff = FF && have && t.ffst != 0;
+        uint4 w = make_uint4(0u, 0u, 0u, 0u);
+        if (ff) {
+            if (t.ffst == 1) {
+                w.x = __ldg(ix.sa + t.ffp);
+            } else if (t.ffst == 2) {
+                const int64_t x = (int64_t)t.ffpos - 1 - t.ffm;
+                if (x >= 0) w = __ldg(reinterpret_cast<const uint4*>(ix.text + (x & ~(int64_t)15)));
+            } else {
+                w.x = __ldg(ix.isa + (t.ffpos - (uint32_t)t.ffm));
+            }
+        }
+        if (have && !ff) {
             if (is_basic(B)) t.ext++;
             back_ext32(ix, P, Q, S, B);
         }
         __syncwarp();
-        if (have) smem_apply(t, a, pv, P, Q, S);
+        if (ff) smem_ff_apply(t, a, pv, w);
+        else if (have) smem_apply(t, a, pv, P, Q, S);
     }
     if (t.ext) atomicAdd(a.n_ext, t.ext);
+    if (FF && t.ffx) atomicAdd(a.n_ffx, t.ffx);
 }
 
 // Two reads per thread, each with its own state machine and candidate list:

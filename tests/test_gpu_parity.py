@@ -256,11 +256,12 @@ def test_scratch_limit_gives_same_records(oracle_built):
         c.close()
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6, 7])
 def test_smem_variants_match_reference_fixtures(cases, variant):
     """The SMEM kernel variants -- two reads per thread (1, 2), a pass's
     candidates extended four (3) or two (4) at a time, one read per thread
-    with smaller register budgets (5, 6) -- emit every read's
+    with smaller register budgets (5, 6), one read per thread without the
+    fast-forward over unique matches (7) -- emit every read's
     SMEMs exactly as the reference does (committed fixtures, all parameter
     sets), and map to the same records."""
     c = lib.Context(0)
@@ -281,7 +282,7 @@ def test_smem_variants_match_reference_fixtures(cases, variant):
                 for key in ("seed", "seed_off", "aln", "cigar", "read_aln_off"):
                     assert np.array_equal(one[key], two[key]), (name, k, key)
         with pytest.raises(lib.MsgError):
-            c.set_smem_shape(7)
+            c.set_smem_shape(8)
     finally:
         c.close()
 
@@ -349,7 +350,7 @@ def test_dp_shape_gives_same_records(oracle_built):
         c.set_dp_shape(*DP_SHAPES[0])
         before = c.map(seq, off, params)
         tune = c.autotune(seq, off, params)
-        assert tune["stripe_rows"] in (8, 16, 32) and tune["n_tried"] == 16 and tune["smem_variant"] in range(7)
+        assert tune["stripe_rows"] in (8, 16, 32) and tune["n_tried"] == 17 and tune["smem_variant"] in range(8)
         assert tune["dp_lanes"] in (16, 32)
         assert tune["warp_area"] in (4096, 16384, 65536, 262144) and tune["small_area"] in (0, 64, 256, 1024)
         after = c.map(seq, off, params)
