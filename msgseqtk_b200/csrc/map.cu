@@ -796,6 +796,9 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         S.n_launch++, k_chain<<<nblk(n_reads, 128), 128, 0, st>>>(d_read_seed_off, d_ndedup, d_rlen, n_reads, d_seeds, d_vis, d_stki,
                                                    d_stkj, 0, d_nchain, d_nidx, nullptr, nullptr, nullptr, nullptr,
                                                    nullptr, nullptr);
+        S.n_launch++, k_chain_warp<<<ctx->num_sms * 8, 128, 0, st>>>(d_read_seed_off, d_ndedup, d_rlen, n_reads, d_seeds, d_vis,
+                                                   d_stki, d_stkj, 0, d_nchain, d_nidx, nullptr, nullptr, nullptr,
+                                                   nullptr, nullptr, nullptr);
         CK(cudaGetLastError());
     }
     CK(offsets_async(ctx, d_nchain, n_reads, d_chain_off, misc, ctx->hpin));
@@ -808,6 +811,9 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         S.n_launch++, k_chain<<<nblk(n_reads, 128), 128, 0, st>>>(d_read_seed_off, d_ndedup, d_rlen, n_reads, d_seeds, d_vis, d_stki,
                                                    d_stkj, 1, nullptr, nullptr, d_chain_off, d_idx_off, d_cidx_off,
                                                    d_clen, d_cread, d_cidx);
+        S.n_launch++, k_chain_warp<<<ctx->num_sms * 8, 128, 0, st>>>(d_read_seed_off, d_ndedup, d_rlen, n_reads, d_seeds, d_vis,
+                                                   d_stki, d_stkj, 1, nullptr, nullptr, d_chain_off, d_idx_off,
+                                                   d_cidx_off, d_clen, d_cread, d_cidx);
         CK(cudaGetLastError());
     }
     } else {  // the caller's chains (checked by the entry point): seed indices local to each read

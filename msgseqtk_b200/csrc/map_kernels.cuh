@@ -485,6 +485,10 @@ __device__ __forceinline__ bool chain_ok(const Seed& l, const Seed& r, int64_t m
     return ind <= max_indel;
 }
 
+// Reads with more seeds than this chain on a warp each (k_chain_warp), the
+// others on a thread each (k_chain).
+constexpr int64_t kChainThreadSeeds = 32;
+
 __global__ void k_chain(const int64_t* __restrict__ read_seed_off, const int32_t* __restrict__ n_seed,
                         const int64_t* __restrict__ read_len, int64_t n_reads, const Seed* __restrict__ seeds,
                         uint8_t* __restrict__ visited, int32_t* __restrict__ stk_i, int32_t* __restrict__ stk_j,
@@ -496,6 +500,7 @@ __global__ void k_chain(const int64_t* __restrict__ read_seed_off, const int32_t
     if (r >= n_reads) return;
     const int64_t a = read_seed_off[r];
     const int64_t N = n_seed[r];
+    if (N > kChainThreadSeeds) return;  // k_chain_warp's
     const int64_t L = read_len[r];
     // msgseqtk-align.cpp:619-620
     const int64_t max_mm = (int64_t)ceil(__dmul_rn((double)L, 0.2));
@@ -546,6 +551,95 @@ __global__ void k_chain(const int64_t* __restrict__ read_seed_off, const int32_t
         }
     }
     if (!pass) { n_chain[r] = nc; n_idx[r] = ni; }
+}
+
+// SeedChain::getChains / dfsSeeds (SeedChain.cpp:40-73) for reads with more
+// than kChainThreadSeeds seeds, one warp per read: the DFS is k_chain's
+// (same order, same chains), but each search for the next unvisited
+// compatible seed tests 32 candidates at once and takes the first by ballot,
+// which turns the serial O(N^2) scans of seed-rich reads (repeats) into
+// N^2 / 32 steps. Lane 0 keeps the stack and visited flags in memory; the
+// warp keeps depth and the resume point in registers.
+__global__ void k_chain_warp(const int64_t* __restrict__ read_seed_off, const int32_t* __restrict__ n_seed,
+                             const int64_t* __restrict__ read_len, int64_t n_reads, const Seed* __restrict__ seeds,
+                             uint8_t* __restrict__ visited, int32_t* __restrict__ stk_i, int32_t* __restrict__ stk_j,
+                             int pass, int64_t* __restrict__ n_chain, int64_t* __restrict__ n_idx,
+                             const int64_t* __restrict__ chain_off, const int64_t* __restrict__ idx_off,
+                             int64_t* __restrict__ chain_idx_off, int32_t* __restrict__ chain_len,
+                             int32_t* __restrict__ chain_read, int64_t* __restrict__ chain_idx) {
+    const int lane = threadIdx.x & 31;
+    const int64_t n_warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < n_reads; r += n_warps) {
+        const int64_t N = n_seed[r];
+        if (N <= kChainThreadSeeds) continue;
+        const int64_t a = read_seed_off[r];
+        const int64_t L = read_len[r];
+        const int64_t max_mm = (int64_t)ceil(__dmul_rn((double)L, 0.2));  // msgseqtk-align.cpp:619-620
+        const int64_t max_indel = (int64_t)ceil(__dmul_rn((double)L, 0.1));
+        uint8_t* vis = visited + a;
+        int32_t* si = stk_i + a;
+        const Seed* sd = seeds + a;
+        for (int64_t i = lane; i < N; i += 32) vis[i] = 0;
+        __syncwarp();
+        int64_t nc = 0, ni = 0;
+        const int64_t c_base = pass ? chain_off[r] : 0;
+        const int64_t i_base = pass ? idx_off[r] : 0;
+        for (int64_t root = 0; root < N; ++root) {
+            if (vis[root]) continue;  // every lane reads the same flag
+            __syncwarp();
+            if (lane == 0) { vis[root] = 1; si[0] = (int32_t)root; }
+            int depth = 0;
+            int64_t j = root + 1;   // resume point of the top frame
+            bool had_child = false; // the top frame has descended once
+            // resume points and child flags of the frames below, on the stack
+            int32_t* sj = stk_j + a;
+            __syncwarp();
+            while (depth >= 0) {
+                const int64_t i = si[depth];
+                const Seed s_i = sd[i];
+                int64_t found = -1;
+                for (int64_t base = j; base < N; base += 32) {
+                    const int64_t jj = base + lane;
+                    const bool ok = jj < N && !vis[jj] && chain_ok(s_i, sd[jj], max_mm, max_indel);
+                    const unsigned m = __ballot_sync(0xffffffffu, ok);
+                    if (m) { found = base + __ffs(m) - 1; break; }
+                }
+                if (found >= 0) {  // descend
+                    if (lane == 0) {
+                        sj[depth] = (int32_t)(-(found + 1) - 1);  // resume after it, child taken
+                        vis[found] = 1;
+                        si[depth + 1] = (int32_t)found;
+                    }
+                    __syncwarp();
+                    ++depth;
+                    j = found + 1;
+                    had_child = false;
+                    continue;
+                }
+                if (!had_child) {  // leaf: emit the current stack as a chain
+                    if (pass) {
+                        if (lane == 0) {
+                            chain_idx_off[c_base + nc] = i_base + ni;
+                            chain_len[c_base + nc] = depth + 1;
+                            chain_read[c_base + nc] = (int32_t)r;
+                        }
+                        for (int d = lane; d <= depth; d += 32) chain_idx[i_base + ni + d] = a + si[d];
+                    }
+                    nc++;
+                    ni += depth + 1;
+                }
+                --depth;
+                if (depth >= 0) {  // back to the frame below: its resume point and child flag
+                    const int32_t v = sj[depth];
+                    had_child = v < 0;
+                    j = v < 0 ? -(int64_t)v - 1 : v;
+                }
+                __syncwarp();
+            }
+        }
+        if (!pass && lane == 0) { n_chain[r] = nc; n_idx[r] = ni; }
+        __syncwarp();
+    }
 }
 
 // ======================================================================
