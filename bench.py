@@ -607,7 +607,7 @@ def main():
 
     counters = ("n_ext", "dp_cells", "dp_cells_done", "n_reads", "n_launch", "n_aln", "host_sorted", "n_sa",
                 "n_chain", "n_band_exact", "n_band_drop", "n_band_fallback", "n_filtered", "n_dp_warp",
-                "n_smem_rerun", "smem_retries", "n_ext_ff")
+                "n_smem_rerun", "smem_retries", "n_ext_ff", "n_ff_steps")
 
     def timed(prm, clocks=None):
         """W warm-up steps, then K timed steps on new batches (inputs larger
@@ -774,8 +774,10 @@ def main():
     stage_ms = {k: agg[k] for k in ("smem", "locate", "chain", "dp")}
     dom = max(stage_ms, key=stage_ms.get)
     read_bytes = float(reads.offs[min(len(reads), n_batches * bp)]) / n_batches * args.steps
-    # two 32 B occurrence buckets per bi-interval extension, plus the read bytes
-    smem_bytes = 64.0 * agg["n_ext"] + read_bytes
+    # two 32 B occurrence buckets per bi-interval extension, one 32 B sector
+    # per fast-forward step (a suffix-array word, a 16-byte text chunk or an
+    # inverse-suffix-array word), plus the read bytes
+    smem_bytes = 64.0 * agg["n_ext"] + 32.0 * agg["n_ff_steps"] + read_bytes
     achieved = smem_bytes / (agg["smem"] / 1000.0) / 1e9 if agg["smem"] > 0 else 0.0
     # DRAM bytes per extension measured by ncu on the 60-genome workload shape
     # (2.641 GB read + written for 44.86 M extensions), scaled to this launch

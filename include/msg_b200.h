@@ -205,6 +205,8 @@ typedef struct msg_map_stats {
     int64_t n_smem_rerun;   /* reads the one-thread SMEM kernel gave to the warp kernel (candidate list too long) */
     int64_t smem_retries;   /* SMEM stage reruns with larger output slots */
     int64_t n_ext_ff;       /* bi-interval extensions of unique matches done by text comparison instead */
+    int64_t n_ff_steps;     /* steps of those comparisons (a suffix-array word, a 16-byte text chunk or an
+                               inverse-suffix-array word loaded each) */
 } msg_map_stats;
 
 /* Map a batch of reads held in HOST memory: the per-read SE task body

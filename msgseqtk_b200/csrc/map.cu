@@ -472,7 +472,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         CK(ctx->smem.ensure((size_t)std::max<int64_t>(1, h_rows) * 48));
         CK(ctx->smem_cnt.ensure((n_reads + 1) * sizeof(int32_t)));
         CK(cudaMemsetAsync(d_ctr, 0, 8 * 4, st));
-        CK(cudaMemsetAsync(d_ctr + 7, 0, 16, st));
+        CK(cudaMemsetAsync(d_ctr + 7, 0, 24, st));
         CK(cudaMemsetAsync(d_status, 0, 4, st));
         // short reads on the thread kernel
         if (thread_path) {
@@ -507,6 +507,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             ta.work = d_ctr; ta.n_ext = d_ctr + 1; ta.status = d_status;
             ta.ovf_list = d_ovf; ta.ovf_n = d_ctr + 7;
             ta.n_ffx = d_ctr + 8;
+            ta.n_ffs = d_ctr + 9;
             const bool ff = ctx->smem_ff && ix.text && ix.isa;
             if (var == 1) S.n_launch++, k_smem_thread2<4><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else if (var == 2) S.n_launch++, k_smem_thread2<3><<<n_thr / 128, 128, 0, st>>>(ta, ix);
@@ -558,11 +559,12 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     ctx->smem_cap = std::min<int64_t>(std::max(ctx->smem_cap, cap), 256);
     // the extension counts arrive with the next synchronisation
     CK(cudaMemcpyAsync(ctx->hpin + 8, d_ctr + 1, 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(ctx->hpin + 10, d_ctr + 8, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(ctx->hpin + 10, d_ctr + 8, 16, cudaMemcpyDeviceToHost, st));
     if (n_reads > 0) S.n_launch++, k_i32_to_i64<<<nblk(n_reads, 256), 256, 0, st>>>(ctx->smem_cnt.as<int32_t>(), d_cnt64, n_reads);
     CK(offsets(ctx, d_cnt64, n_reads, d_smem_off, misc, &h_nsmem));
     S.n_ext = ctx->hpin[8];
     S.n_ext_ff = ctx->hpin[10];
+    S.n_ff_steps = ctx->hpin[11];
     CK(setup_sel());
     if (n_reads > 0) {
         S.n_launch++, k_compact_smem<<<nblk(n_reads * 32, 256), 256, 0, st>>>(ctx->smem.as<int64_t>(), d_slot_off,

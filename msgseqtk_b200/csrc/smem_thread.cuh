@@ -50,6 +50,7 @@ struct SmemThreadArgs {
     unsigned long long* work;
     unsigned long long* n_ext;
     unsigned long long* n_ffx;   // extensions replaced by the fast-forward over unique matches
+    unsigned long long* n_ffs;   // fast-forward steps (one word or 16-byte text chunk loaded each)
     uint32_t* status;
     int64_t* ovf_list;      // reads abandoned because their candidate list outgrew pv_cap (rerun on k_smem)
     unsigned long long* ovf_n;
@@ -107,7 +108,7 @@ struct ThreadSmem {
     int32_t ffdone;         // a fast-forward just ended: the next extension is an ordinary one
     uint32_t ffp;           // the row at the start
     uint32_t ffpos;         // text position of its string (sa[ffp])
-    unsigned long long ffx;
+    unsigned long long ffx, ffs;
 
     __device__ int base(int32_t i) const { return (i >= 0 && i < L) ? (int)__ldg(rd + i) : 0; }
 };
@@ -352,6 +353,7 @@ __device__ __forceinline__ void smem_apply(ThreadSmem& t, const SmemThreadArgs& 
 // One step of a fast-forward run with its loaded word (w.x for the
 // suffix-array and inverse words, all of w for a text chunk).
 __device__ __forceinline__ void smem_ff_apply(ThreadSmem& t, const SmemThreadArgs& a, PrevEntry* pv, const uint4& w) {
+    t.ffs++;
     if (t.ffst == 1) {  // the string's text position
         t.ffpos = w.x;
         t.ffst = 2;
@@ -431,6 +433,7 @@ __global__ void __launch_bounds__(128, MINB) k_smem_thread(SmemThreadArgs a, Ind
     t.phase = PH_NEXT_READ;
     t.ext = 0;
     t.ffx = 0;
+    t.ffs = 0;
     t.ffst = 0;
     t.n_out = 0;
     t.r = -1;
@@ -474,6 +477,7 @@ __global__ void __launch_bounds__(128, MINB) k_smem_thread(SmemThreadArgs a, Ind
     }
     if (t.ext) atomicAdd(a.n_ext, t.ext);
     if (FF && t.ffx) atomicAdd(a.n_ffx, t.ffx);
+    if (FF && t.ffs) atomicAdd(a.n_ffs, t.ffs);
 }
 
 // Two reads per thread, each with its own state machine and candidate list:

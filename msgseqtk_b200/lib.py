@@ -116,7 +116,7 @@ class MapStats(C.Structure):
                [(n, C.c_int64) for n in ("dp_cells_done", "n_band_exact", "n_band_drop", "n_band_fallback",
                                          "n_filtered", "n_dp_warp")] + \
                [("n_dp_class", C.c_int64 * 5), ("dp_class_cells", C.c_int64 * 5), ("n_smem_rerun", C.c_int64),
-                ("smem_retries", C.c_int64), ("n_ext_ff", C.c_int64)]
+                ("smem_retries", C.c_int64), ("n_ext_ff", C.c_int64), ("n_ff_steps", C.c_int64)]
 
 
 def build(force: bool = False) -> str:
