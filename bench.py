@@ -102,6 +102,7 @@ def parse():
                     help="scale: 2x150 bp pairs; uneven: single-end reads of mixed lengths (one batch); "
                          "clean: msgseqtk-clean's MEM log-odds path on two indexes")
     ap.add_argument("--uneven-reads", type=int, default=500_000)
+    ap.add_argument("--no-tune", action="store_true", help="keep the library's default kernel shapes (no autotuner)")
     args = ap.parse_args()
     if args.pairs is None:
         args.pairs = 10_000_000 if args.workload == "repeats" else 2_000_000
@@ -593,8 +594,11 @@ def main():
     # smaller sample leaves the DP launches too short to rank the shapes as
     # the full batch does)
     ns = min(bp, len(reads))
-    dp_shape = ctx.autotune(reads.seqs[:reads.offs[ns]], reads.offs[:ns + 1], params)
-    dp_shape["sample_reads"] = ns
+    if args.no_tune:
+        dp_shape = {"tuned": False, "note": "library default shapes"}
+    else:
+        dp_shape = ctx.autotune(reads.seqs[:reads.offs[ns]], reads.offs[:ns + 1], params)
+        dp_shape["sample_reads"] = ns
 
     def offs_sb(first, count):
         """Device offsets of reads first .. first + count, rebased to 0."""

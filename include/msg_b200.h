@@ -311,7 +311,7 @@ int msg_ctx_set_scratch_limit(msg_ctx* ctx, int64_t bytes);
  * small_area rectangle cells are filled row by row by one GPU thread; chains
  * of at most warp_area cells by one thread in register stripes of
  * stripe_rows rows (8, 16 or 32); larger chains by a warp along
- * anti-diagonals. Defaults 256, 65536, 16. Results do not depend on it. */
+ * anti-diagonals. Defaults 64, 262144, 16. Results do not depend on it. */
 int msg_ctx_set_dp_shape(msg_ctx* ctx, int32_t stripe_rows, int64_t small_area, int64_t warp_area);
 
 /* Lane width of the register-stripe DP fill (no reference counterpart):
@@ -344,7 +344,7 @@ typedef struct msg_tune {
     int32_t n_tried;        /* shapes timed */
     int64_t small_area, warp_area;
     double ms_dp;           /* DP stage time of the chosen split on the sample */
-    double ms_dp_default;   /* the same with the defaults (16, 256, 65536) */
+    double ms_dp_default;   /* the same with the defaults (16, 64, 262144) */
     int32_t smem_variant;
     int32_t dp_lanes;       /* 16 or 32 (msg_ctx_set_dp_lanes) */
     double ms_smem;         /* SMEM stage time of the chosen variant */

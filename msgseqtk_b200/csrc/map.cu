@@ -1721,7 +1721,7 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
         return MSG_OK;
     };
     int best_var = 0, best_k = 16;
-    int64_t best_small = 256, best_warp = 65536;
+    int64_t best_small = 64, best_warp = 262144;
     double best_smem = 0, best_dp = 0, ts = 0, td = 0;
     if ((rc = time_shape(best_var, best_k, best_small, best_warp, &best_smem, &best_dp)) != MSG_OK) return rc;
     const double smem_default = best_smem, dp_default = best_dp;
@@ -1729,7 +1729,7 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
         if ((rc = time_shape(var, best_k, best_small, best_warp, &ts, &td)) != MSG_OK) return rc;
         if (ts < best_smem) { best_smem = ts; best_var = var; }
     }
-    for (int64_t warp : {4096ll, 16384ll, 262144ll}) {
+    for (int64_t warp : {4096ll, 16384ll, 65536ll}) {
         if ((rc = time_shape(best_var, best_k, best_small, warp, &ts, &td)) != MSG_OK) return rc;
         if (td < best_dp) { best_dp = td; best_warp = warp; }
     }
@@ -1737,7 +1737,7 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
         if ((rc = time_shape(best_var, k, best_small, best_warp, &ts, &td)) != MSG_OK) return rc;
         if (td < best_dp) { best_dp = td; best_k = k; }
     }
-    for (int64_t small : {0ll, 64ll, 1024ll}) {
+    for (int64_t small : {0ll, 256ll, 1024ll}) {
         if ((rc = time_shape(best_var, best_k, small, best_warp, &ts, &td)) != MSG_OK) return rc;
         if (td < best_dp) { best_dp = td; best_small = small; }
     }

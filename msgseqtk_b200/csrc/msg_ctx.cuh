@@ -100,8 +100,8 @@ struct msg_ctx {
     int smem_variant = 0;  // SMEM thread path (msg_ctx_set_smem_shape): 0 one read per thread, 1/2 two,
                            // 3/4 a pass's candidates extended several at a time
     int64_t smem_cap = 16;  // SMEM rows per 150 read bases the slots start with (grows after an overflow)
-    int64_t dp_small_area = 256;
-    int64_t dp_warp_area = 65536;
+    int64_t dp_small_area = 64;
+    int64_t dp_warp_area = 262144;
     cudaEvent_t ev[8];
     int64_t* hpin = nullptr;  // pinned host words for counts copied back without extra waits
     // DP class launches side by side: three streams forked from `stream`
