@@ -726,6 +726,18 @@ __device__ __forceinline__ int64_t rect_bytes(int64_t R, int64_t C) {
     return (code + ((C + 1) * 4 + C * 3 + R * 3) * 4 + 16 + 15) / 16 * 16;
 }
 
+// Boundary cells of one rectangle, with the closed forms' constants taken
+// once (ChainCtx::bnd_info) and held in registers: the per-cell queries then
+// read nothing from the chain context.
+struct RectBnd {
+    int kind;            // 0: the 5' rectangle, 1: the rectangle after seed p (closed form), 2: region rule
+    int m;
+    int nw;
+    int32_t go, ge;      // gap open and extension
+    int32_t E, Eo;       // kind 1: the seed's final diagonal value, and E + o
+    int64_t q1, t1;      // kind 1: the seed's last row and column
+};
+
 struct ChainCtx {
     const int4* sd;             // per seed: qf, qt, ts, te (window-relative)
     const int32_t* rbnd;        // row boundaries b[0..2n+1]: 0, qf_0, qt_0, ..., qf_n-1, qt_n-1, L
@@ -877,25 +889,47 @@ struct ChainCtx {
     //    and rectangles all lie in rows before qt and columns before te, as
     //    the region rule confirms cell by cell.
     // OUTLINE: the region rule through the out-of-line MID (else inlined).
+    // (bnd_info takes the constants of a rectangle once, bnd_at answers a
+    // cell from them)
     template <bool OUTLINE = true>
     __device__ __forceinline__ int3 boundary(int m, int64_t i, int64_t j) const {
+        return bnd_at<OUTLINE>(bnd_info(m), i, j);
+    }
+
+    __device__ __forceinline__ RectBnd bnd_info(int m) const {
+        RectBnd b;
+        b.m = m;
+        b.nw = pp.mode == 0;
+        b.go = pp.gap_o; b.ge = pp.gap_e;
+        b.E = 0; b.Eo = 0; b.q1 = 0; b.t1 = 0;
         if (m == 0) {
-            const bool nw = pp.mode == 0;
-            if (i == 0) return make_int3(0, (nw && j == 0) ? 0 : NEG, NEG);
-            return make_int3(nw ? NEG : 0, nw ? -(pp.gap_o + pp.gap_e * (int32_t)i) : NEG, NEG);  // j == 0
-        }
-        if (m >= 2 && !(m & 1) && (n == 1 || sep)) {
+            b.kind = 0;
+        } else if (!(m & 1) && (n == 1 || sep)) {
             const int p = (m >> 1) - 1;
-            const int64_t q1 = qt(p), t1 = te(p);
-            const int32_t E = diag[p] + (int32_t)(q1 - qf(p) - 1) * pp.match;
-            const int32_t Eo = sat_add(E, -(pp.gap_o + pp.gap_e));
-            if (i == q1 && j == t1) return make_int3(E, NEG, NEG);
-            if (i == q1 && j == t1 + 1) return make_int3(NEG, NEG, Eo);
-            if (j == t1 && i == q1 + 1) return make_int3(NEG, Eo, NEG);
+            b.kind = 1;
+            b.q1 = qt(p); b.t1 = te(p);
+            b.E = diag[p] + (int32_t)(b.q1 - qf(p) - 1) * pp.match;
+            b.Eo = sat_add(b.E, -(pp.gap_o + pp.gap_e));
+        } else {
+            b.kind = 2;
+        }
+        return b;
+    }
+    // boundary(m, i, j) from the constants of bnd_info(m)
+    template <bool OUTLINE = true>
+    __device__ __forceinline__ int3 bnd_at(const RectBnd& b, int64_t i, int64_t j) const {
+        if (b.kind == 0) {
+            if (i == 0) return make_int3(0, (b.nw && j == 0) ? 0 : NEG, NEG);
+            return make_int3(b.nw ? NEG : 0, b.nw ? -(b.go + b.ge * (int32_t)i) : NEG, NEG);  // j == 0
+        }
+        if (b.kind == 1) {
+            if (i == b.q1 && j == b.t1) return make_int3(b.E, NEG, NEG);
+            if (i == b.q1 && j == b.t1 + 1) return make_int3(NEG, NEG, b.Eo);
+            if (j == b.t1 && i == b.q1 + 1) return make_int3(NEG, b.Eo, NEG);
             return make_int3(NEG, NEG, NEG);
         }
-        if constexpr (OUTLINE) return MID(i, j, m);
-        else return make_int3(M(i, j, m), I(i, j, m), D(i, j, m));
+        if constexpr (OUTLINE) return MID(i, j, b.m);
+        else return make_int3(M(i, j, b.m), I(i, j, b.m), D(i, j, b.m));
     }
 
     // Single-thread fill of rectangle m, row by row, into the same code layout
@@ -906,6 +940,7 @@ struct ChainCtx {
     // number of cells computed.
     __device__ __forceinline__ int64_t fill_rect_thread(int m, int w, int32_t& best, int64_t& bkey) {
         const RectGeo g = rect(m);
+        const RectBnd bi = bnd_info(m);
         if (g.R <= 0 || g.C <= 0) return 0;
         const int32_t o = -(pp.gap_o + pp.gap_e), e = -pp.gap_e;
         const bool banded = w >= 0;
@@ -917,7 +952,7 @@ struct ChainCtx {
         int64_t plo = 0, phi = g.C - 1;  // columns of the row above held in rowbuf
         if (banded) { plo = max((int64_t)0, dg - w - 1); phi = min(g.C - 1, dg + w); }
         for (int64_t c = plo; c <= phi; ++c) {  // the top boundary row
-            const int3 v = boundary<false>(m, g.r0, g.c0 + 1 + c);
+            const int3 v = bnd_at<false>(bi, g.r0, g.c0 + 1 + c);
             g.rowbuf[c * 3] = v.x;
             g.rowbuf[c * 3 + 1] = v.y;
             g.rowbuf[c * 3 + 2] = v.z;
@@ -933,8 +968,8 @@ struct ChainCtx {
             int32_t ml = NEG, dl = NEG, dm = NEG, di = NEG, dd = NEG;
             if (lo == 0) {
                 if (lrow == i - 1) { dm = lm; di = li; dd = ld; }
-                else { const int3 v = boundary<false>(m, i - 1, g.c0); dm = v.x; di = v.y; dd = v.z; }
-                const int3 v = boundary<false>(m, i, g.c0);
+                else { const int3 v = bnd_at<false>(bi, i - 1, g.c0); dm = v.x; di = v.y; dd = v.z; }
+                const int3 v = bnd_at<false>(bi, i, g.c0);
                 lm = v.x; li = v.y; ld = v.z;
                 lrow = i;
                 ml = lm; dl = ld;
@@ -1005,7 +1040,8 @@ struct ChainCtx {
             for (int c = 0; c < 3 * C; ++c) g.lastrow[c] = NEG;
             for (int c = 0; c < 3 * R; ++c) g.lastcol[c] = NEG;
         }
-        auto bnd = [&](int64_t i, int64_t j) -> int3 { return boundary(m, i, j); };
+        const RectBnd bi = bnd_info(m);
+        auto bnd = [&](int64_t i, int64_t j) -> int3 { return bnd_at(bi, i, j); };
         // the context's fields the column loop reads, in registers (the
         // context itself lives in local memory)
         const uint8_t* const tgt = target + g.c0;
@@ -1164,6 +1200,7 @@ struct ChainCtx {
     __device__ __noinline__ int64_t fill_rect_stripe16(int m, int w) {
         constexpr int K = 16;
         const RectGeo g = rect(m);
+        const RectBnd bi = bnd_info(m);
         if (g.R <= 0 || g.C <= 0) return 0;
         const int R = (int)g.R, C = (int)g.C;
         const uint32_t O2 = pack16(-(pp.gap_o + pp.gap_e)), E2 = pack16(-pp.gap_e);
@@ -1181,7 +1218,7 @@ struct ChainCtx {
         int plo = 0, phi = C - 1;  // columns of the row buffer that hold the row above
         if (BANDED) { plo = max(0, dg - w - 1); phi = min(C - 1, dg + w); }
         for (int c = plo; c <= phi; ++c) {  // the top boundary row
-            const int3 v = boundary(m, g.r0, g.c0 + 1 + c);
+            const int3 v = bnd_at(bi, g.r0, g.c0 + 1 + c);
             rb4[c] = make_int4((int)to16(v.x), (int)to16(v.y), (int)to16(v.z), 0);
         }
         int64_t cells = 0;
@@ -1217,7 +1254,7 @@ struct ChainCtx {
             const bool left = clo == 0;
             if (left) {
                 for (int k = 0; k < nlo + nhi; ++k) {
-                    const int3 v = boundary(m, i0 + k, g.c0);
+                    const int3 v = bnd_at(bi, i0 + k, g.c0);
                     int32_t* lc = g.lastcol + (int64_t)(rr0 + k) * 3;
                     lc[0] = v.x; lc[1] = v.y; lc[2] = v.z;
                 }
@@ -1237,7 +1274,7 @@ struct ChainCtx {
             // stripe's last row two columns back)
             uint32_t dlM = 0u, dlI = 0u, dlD = 0u;
             if (left) {
-                const int3 cv = boundary(m, i0 - 1, g.c0);
+                const int3 cv = bnd_at(bi, i0 - 1, g.c0);
                 dlM = to16(cv.x); dlI = to16(cv.y); dlD = to16(cv.z);
             } else if (clo - 1 >= plo && clo - 1 <= phi) {
                 const int4 v = rb4[clo - 1];
