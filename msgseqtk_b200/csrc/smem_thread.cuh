@@ -61,6 +61,13 @@ struct SmemThreadArgs {
 // would serialise
 __shared__ double s_llk[16];
 
+// Steps one read's state machine may take: at most 2L calls, each a walk of
+// at most L extensions and at most L passes over at most pv_cap (48)
+// candidates -- under 6.4 M for a 254-base read (about 500 on average); a
+// read that exceeds the bound sets kErrInternal and ends, so a defect fails
+// the batch loudly instead of running without end.
+constexpr int32_t kSmemMaxSteps = 1 << 25;
+
 enum SmemPhase : int {
     PH_NEXT_READ = 0,
     PH_OUTER_LOOP,      // while (from > 0 || to < L)
@@ -100,6 +107,7 @@ struct ThreadSmem {
     PrevEntry e0, e_next;   // entry being extended, and the next one (loaded early)
     int32_t phase;
     unsigned long long ext;
+    int32_t steps;          // state-machine steps of the read in progress (bounded by kSmemMaxSteps)
     // fast-forward over a unique match (interval size 1): 0 none, 1 suffix
     // array word of the row, 2 text chunks, 3 inverse-suffix-array word
     int32_t ffst;
@@ -194,6 +202,12 @@ __device__ __forceinline__ void smem_call(ThreadSmem& t, const IndexDev& ix, int
 template <bool FF = false>
 __device__ bool smem_advance(ThreadSmem& t, const SmemThreadArgs& a, const IndexDev& ix, PrevEntry* pv,
                              uint32_t& P, uint32_t& Q, uint32_t& S, int& B) {
+    if (FF && t.ffst != 0) return true;  // a fast-forward run in progress takes its next step
+    if (++t.steps > kSmemMaxSteps) {  // no read needs this many: a broken state machine ends the read
+        atomicOr(a.status, kErrInternal);
+        t.phase = PH_DONE;
+        return false;
+    }
     for (;;) {
         switch (t.phase) {
             case PH_OUTER_LOOP:
@@ -413,6 +427,7 @@ __device__ __forceinline__ bool smem_next_read(ThreadSmem& t, const SmemThreadAr
     t.ovf = 0;
     t.ffst = 0;
     t.ffdone = 0;
+    t.steps = 0;
     if (t.L <= 0) { t.phase = PH_DONE; return true; }
     t.from = t.L / 2;  // SMEM.cpp:189-191
     t.to = t.from + 1;
