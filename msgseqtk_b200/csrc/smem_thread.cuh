@@ -66,7 +66,7 @@ __shared__ double s_llk[16];
 // candidates -- under 6.4 M for a 254-base read (about 500 on average); a
 // read that exceeds the bound sets kErrInternal and ends, so a defect fails
 // the batch loudly instead of running without end.
-constexpr int32_t kSmemMaxSteps = 1 << 25;
+constexpr int32_t kSmemMaxSteps = 1 << 23;
 
 enum SmemPhase : int {
     PH_NEXT_READ = 0,
