@@ -330,12 +330,11 @@ int msg_ctx_set_dp_lanes(msg_ctx* ctx, int32_t bits);
  * findBackFwdSMEMS (SMEM.cpp:93-116, 148-171) extended up to 4 (3) or 2 (4)
  * at a time, their bucket loads in flight together; 5 and 6 = variant 0 with
  * registers sized for 6 and 8 resident blocks of 128 threads per SM (more
- * warps, some spilling) instead of 5; 7 = variant 0 without the
- * fast-forward over unique matches (0, 5 and 6 replace a run of
- * extensions of a size-1 interval -- a walk's, or a pass's single
- * candidate's -- by comparing the read with the BD text before the match's
- * suffix-array position and one inverse-suffix-array lookup). Results do
- * not depend on it. */
+ * warps, some spilling) instead of 5; 7 = variant 0 with the fast-forward
+ * over unique matches (a run of extensions of a size-1 interval -- a
+ * walk's, or a pass's single candidate's -- replaced by comparing the read
+ * with the BD text before the match's suffix-array position and one
+ * inverse-suffix-array lookup). Results do not depend on it. */
 int msg_ctx_set_smem_shape(msg_ctx* ctx, int32_t variant);
 
 /* The shapes chosen by msg_autotune, with the stage times that chose them. */

@@ -488,10 +488,11 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             else if (var == 2) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread2<3>, 128, 0));
             else if (var == 3) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_pass<4, 4>, 128, 0));
             else if (var == 4) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_pass<2, 5>, 128, 0));
-            else if (var == 5) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<6, true>, 128, 0));
-            else if (var == 6) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<8, true>, 128, 0));
-            // variant 7: variant 0 without the fast-forward over unique matches
-            else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<5, true>, 128, 0));
+            else if (var == 5) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<6, false>, 128, 0));
+            else if (var == 6) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<8, false>, 128, 0));
+            // variant 7: variant 0 with the fast-forward over unique matches
+            else if (ctx->smem_ff) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<5, true>, 128, 0));
+            else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_smem_thread<5, false>, 128, 0));
             const int64_t n_thr = (int64_t)ctx->num_sms * std::max(1, bps) * 128;
             const int64_t pv_cap = kThreadPrev;
             CK(ctx->prev.ensure((pair ? 2 : 1) * n_thr * pv_cap * sizeof(PrevEntry) + 64));
@@ -508,14 +509,12 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
             ta.ovf_list = d_ovf; ta.ovf_n = d_ctr + 7;
             ta.n_ffx = d_ctr + 8;
             ta.n_ffs = d_ctr + 9;
-            const bool ff = ctx->smem_ff && ix.text && ix.isa;
+            const bool ff = var == 0 && ctx->smem_ff && ix.text && ix.isa;
             if (var == 1) S.n_launch++, k_smem_thread2<4><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else if (var == 2) S.n_launch++, k_smem_thread2<3><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else if (var == 3) S.n_launch++, k_smem_pass<4, 4><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else if (var == 4) S.n_launch++, k_smem_pass<2, 5><<<n_thr / 128, 128, 0, st>>>(ta, ix);
-            else if (var == 5 && ff) S.n_launch++, k_smem_thread<6, true><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else if (var == 5) S.n_launch++, k_smem_thread<6, false><<<n_thr / 128, 128, 0, st>>>(ta, ix);
-            else if (var == 6 && ff) S.n_launch++, k_smem_thread<8, true><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else if (var == 6) S.n_launch++, k_smem_thread<8, false><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else if (ff) S.n_launch++, k_smem_thread<5, true><<<n_thr / 128, 128, 0, st>>>(ta, ix);
             else S.n_launch++, k_smem_thread<5, false><<<n_thr / 128, 128, 0, st>>>(ta, ix);
@@ -1686,7 +1685,7 @@ extern "C" int msg_ctx_set_dp_lanes(msg_ctx* ctx, int32_t bits) {
 
 extern "C" int msg_ctx_set_smem_shape(msg_ctx* ctx, int32_t variant) {
     if (!ctx || variant < 0 || variant > 7) return MSG_EINVAL;
-    ctx->smem_ff = variant != 7;
+    ctx->smem_ff = variant == 7;
     ctx->smem_variant = variant == 7 ? 0 : variant;
     return MSG_OK;
 }
@@ -1704,7 +1703,7 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
     int best_lanes = 16;
     auto time_shape = [&](int var, int k, int64_t small, int64_t warp, double* ms_smem, double* ms_dp) -> int {
         ctx->dp_lanes = best_lanes;
-        ctx->smem_ff = var != 7;
+        ctx->smem_ff = var == 7;
         ctx->smem_variant = var == 7 ? 0 : var;
         ctx->dp_k = k;
         ctx->dp_small_area = small;
@@ -1746,7 +1745,7 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
     if (td < best_dp) best_dp = td;
     else best_lanes = 16;
     ctx->dp_lanes = best_lanes;
-    ctx->smem_ff = best_var != 7;
+    ctx->smem_ff = best_var == 7;
     ctx->smem_variant = best_var == 7 ? 0 : best_var;
     ctx->dp_k = best_k;
     ctx->dp_small_area = best_small;

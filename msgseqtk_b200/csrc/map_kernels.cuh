@@ -1192,7 +1192,11 @@ struct ChainCtx {
     // a byte permute. BANDED (w >= 0): only the cells within w diagonals of
     // the adjacent seed's diagonal count, the others are -inf (masked to 0
     // through a per-column bitmap of the rows in band), as fill_rect_stripe
-    // does; each half runs over its own band's columns. Codes and last
+    // does; each half runs over its own band's columns. (The dispatcher
+    // keeps banded flanks on the 32-bit fill: a band of 2w+1 diagonals
+    // leaves each lagged half idle for 17 of the pair's 2w+33 columns, and
+    // measured on the 1 M-read workload the 16-bit banded form made the DP
+    // stage slower, 19.5 against 18.3 ms.) Codes and last
     // row/column go where fill_rect_stripe<16> puts them (the last row and
     // column in 32-bit values), so the traceback reads both alike. The row
     // buffer holds 16-bit values here. Returns the cells evaluated.
@@ -1874,7 +1878,10 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
     // unbanded stripe chains in GLOBAL mode whose values fit 16-bit lanes
     // run the two-stripe 16-bit fill (codes in 16-row stripes)
     const int64_t w1 = max(max(a.pp.match, a.pp.mismatch), a.pp.gap_o + a.pp.gap_e);
-    const bool use16 = !WARP && KST > 0 && a.lanes16 && a.pp.mode == 0 && (x.L + x.T + 1) * w1 < kBias16;
+    // (a banded chain keeps its banded flank in 32-bit stripes of KST rows,
+    // so its other rectangles share the 16-row code layout only when KST is 16)
+    const bool use16 = !WARP && KST > 0 && a.lanes16 && a.pp.mode == 0 && (x.L + x.T + 1) * w1 < kBias16 &&
+                       (!BAND || KST == 16);
     x.kst = use16 ? 16 : KST;
     x.stab = stab;
     // geometry in sd/rbnd/cbnd; a warp working in shared memory also leaves a
@@ -1939,9 +1946,8 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
     auto fill = [&](int m, int w) {
         if constexpr (!WARP && KST > 0) {
             if constexpr (BAND) {
-                if (w >= 0) {
-                    if (use16) cells += x.template fill_rect_stripe16<true>(m, w);
-                    else cells += x.template fill_rect_stripe<KST, false, true>(m, w, best, bkey);
+                if (w >= 0) {  // banded flanks in 32-bit stripes (see fill_rect_stripe16)
+                    cells += x.template fill_rect_stripe<KST, false, true>(m, w, best, bkey);
                     return;
                 }
             }

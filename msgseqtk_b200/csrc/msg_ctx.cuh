@@ -96,7 +96,7 @@ struct msg_ctx {
     // larger ones on a warp
     int dp_k = 16;
     int dp_lanes = 16;     // 16: unbanded GLOBAL stripe chains that fit use 16-bit lanes (msg_ctx_set_dp_lanes)
-    int smem_ff = 1;       // SMEM walks and single-entry passes skip unique matches by text comparison (variant 7: off)
+    int smem_ff = 0;       // SMEM walks and single-entry passes skip unique matches by text comparison (variant 7)
     int smem_variant = 0;  // SMEM thread path (msg_ctx_set_smem_shape): 0 one read per thread, 1/2 two,
                            // 3/4 a pass's candidates extended several at a time
     int64_t smem_cap = 16;  // SMEM rows per 150 read bases the slots start with (grows after an overflow)

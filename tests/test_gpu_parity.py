@@ -260,7 +260,7 @@ def test_scratch_limit_gives_same_records(oracle_built):
 def test_smem_variants_match_reference_fixtures(cases, variant):
     """The SMEM kernel variants -- two reads per thread (1, 2), a pass's
     candidates extended four (3) or two (4) at a time, one read per thread
-    with smaller register budgets (5, 6), one read per thread without the
+    with smaller register budgets (5, 6), one read per thread with the
     fast-forward over unique matches (7) -- emit every read's
     SMEMs exactly as the reference does (committed fixtures, all parameter
     sets), and map to the same records."""
