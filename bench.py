@@ -628,6 +628,7 @@ def main():
         agg.update({k: 0 for k in counters})
         agg["n_dp_class"] = [0] * 5
         agg["dp_class_cells"] = [0] * 5
+        agg["ms_dp_part"] = [0.0] * 4
         torch.cuda.synchronize()
         ev0.record(stream)
         for s in range(args.steps):
@@ -637,7 +638,7 @@ def main():
             agg["dp"] += st["ms_dp"]
             for k in counters:
                 agg[k] += st[k]
-            for k in ("n_dp_class", "dp_class_cells"):
+            for k in ("n_dp_class", "dp_class_cells", "ms_dp_part"):
                 agg[k] = [x + y for x, y in zip(agg[k], st[k])]
         ev1.record(stream)
         torch.cuda.synchronize()
@@ -866,7 +867,11 @@ def main():
                 "gpu_launches": agg["n_launch"], "validation": valid, "setup": setup, "tuned_shapes": dp_shape, "small_batch": small_batch,
                 "stats": dict({k: agg[k] for k in counters},
                               dp_classes={"names": ["row-by-row", "stripes", "banded stripes", "warp", "banded warp"],
-                                          "chains": agg["n_dp_class"], "cells": agg["dp_class_cells"]})}
+                                          "chains": agg["n_dp_class"], "cells": agg["dp_class_cells"]},
+                              dp_ms_per_step_by_part={"prepare_and_size": agg["ms_dp_part"][0] / args.steps,
+                                                      "classes_and_sort": agg["ms_dp_part"][1] / args.steps,
+                                                      "fills_and_tracebacks": agg["ms_dp_part"][2] / args.steps,
+                                                      "filter_and_cigars": agg["ms_dp_part"][3] / args.steps})}
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

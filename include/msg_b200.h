@@ -207,6 +207,8 @@ typedef struct msg_map_stats {
     int64_t n_ext_ff;       /* bi-interval extensions of unique matches done by text comparison instead */
     int64_t n_ff_steps;     /* steps of those comparisons (a suffix-array word, a 16-byte text chunk or an
                                inverse-suffix-array word loaded each) */
+    double ms_dp_part[4];   /* ms_dp by part: chain preparation and storage sizing, band classes and sort,
+                               fills and tracebacks, filter and CIGARs */
 } msg_map_stats;
 
 /* Map a batch of reads held in HOST memory: the per-read SE task body

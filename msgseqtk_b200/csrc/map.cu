@@ -195,6 +195,7 @@ struct Timer {
     msg_ctx* ctx;
     int k = 0;
     void mark() { cudaEventRecord(ctx->ev[k++], ctx->stream); }
+    void mark_at(int i) { cudaEventRecord(ctx->ev[i], ctx->stream); }  // the DP stage's inner marks (6, 7)
     float ms(int a, int b) {
         float t = 0;
         cudaEventElapsedTime(&t, ctx->ev[a], ctx->ev[b]);
@@ -930,6 +931,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     CK(cudaStreamSynchronize(st));
     h_cells = ctx->hpin[2];
     h_pathtot = ctx->hpin[3];
+    tm.mark_at(6);  // chains prepared and storage sized
     const int64_t aux_bytes = ((2 * (h_nidx + 1) + h_nchain + 1) * sizeof(int32_t) + 15) / 16 * 16;
     // Rectangle storage of at most scratch_limit bytes at a time: when the
     // batch needs more (long reads with large flanks), the DP runs over
@@ -1038,6 +1040,7 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
         CK(dp_sort(ctx, c0, nch, d_geo, d_area, d_feat, bmode, params->band_w, d_wts, d_nrm, d_band, d_ctr2, d_fb,
                    d_kidx, d_sorted, S));
         da.list = d_sorted;
+        if (ch == 0) tm.mark_at(7);  // first range's classes assigned and sorted
         // Every launch is sized for the range; each reads its class's part of
         // the sorted list on the device, so no host round trip is needed.
         // The classes run side by side: row-by-row, stripe and banded-stripe
@@ -1140,6 +1143,12 @@ static int map_impl(msg_ctx* ctx, const uint8_t* d_seq, const int64_t* d_off, in
     S.ms_locate = tm.ms(1, 2);
     S.ms_chain = tm.ms(2, 3);
     S.ms_dp = tm.ms(3, 5);
+    if (h_nchain > 0) {  // the DP stage by part (one range: exact; several: the first range's sort ends part 1)
+        S.ms_dp_part[0] = tm.ms(3, 6);  // prep, features, sizes
+        S.ms_dp_part[1] = tm.ms(6, 7);  // band classes and the class sort
+        S.ms_dp_part[2] = tm.ms(7, 4);  // fills and tracebacks
+        S.ms_dp_part[3] = tm.ms(4, 5);  // filter and CIGARs
+    }
 
     // ---------------- results ----------------
     out->n_aln = h_nrec;

@@ -116,7 +116,8 @@ class MapStats(C.Structure):
                [(n, C.c_int64) for n in ("dp_cells_done", "n_band_exact", "n_band_drop", "n_band_fallback",
                                          "n_filtered", "n_dp_warp")] + \
                [("n_dp_class", C.c_int64 * 5), ("dp_class_cells", C.c_int64 * 5), ("n_smem_rerun", C.c_int64),
-                ("smem_retries", C.c_int64), ("n_ext_ff", C.c_int64), ("n_ff_steps", C.c_int64)]
+                ("smem_retries", C.c_int64), ("n_ext_ff", C.c_int64), ("n_ff_steps", C.c_int64),
+                ("ms_dp_part", C.c_double * 4)]
 
 
 def build(force: bool = False) -> str:
@@ -767,6 +768,7 @@ class Context:
         d = {k: getattr(s, k) for k, _ in MapStats._fields_}
         d["n_dp_class"] = list(s.n_dp_class)
         d["dp_class_cells"] = list(s.dp_class_cells)
+        d["ms_dp_part"] = list(s.ms_dp_part)
         return d
 
 
