@@ -324,6 +324,12 @@ int msg_ctx_set_dp_shape(msg_ctx* ctx, int32_t stripe_rows, int64_t small_area, 
  * in 32-bit values. Results do not depend on it. */
 int msg_ctx_set_dp_lanes(msg_ctx* ctx, int32_t bits);
 
+/* Register budget of the register-stripe DP kernel (no reference
+ * counterpart): sized for 3 (default; 168 registers, no spills in the
+ * 16-bit fill) or 4 (128 registers, more warps) resident blocks of 128
+ * threads per SM. Results do not depend on it. */
+int msg_ctx_set_dp_occupancy(msg_ctx* ctx, int32_t blocks);
+
 /* Kernel shape of the SMEM stage for reads up to 254 bp (no reference
  * counterpart): 0 = one read per thread (default); 1 and 2 = two reads per
  * thread, each thread keeping two extensions' bucket loads in flight (1:
@@ -350,12 +356,15 @@ typedef struct msg_tune {
     int32_t dp_lanes;       /* 16 or 32 (msg_ctx_set_dp_lanes) */
     double ms_smem;         /* SMEM stage time of the chosen variant */
     double ms_smem_default; /* the same with variant 0 */
+    int32_t dp_stripe_blocks; /* 3 or 4 (msg_ctx_set_dp_occupancy) */
+    int32_t pad2;
 } msg_tune;
 
 /* Autotuner of the kernel shapes (no reference counterpart): maps the sample
  * batch (host memory) with `params` under candidate shapes -- the SMEM
- * variant, then the DP warp threshold, stripe height, row-by-row threshold
- * and lane width, each chosen with the others fixed -- timing the stage it
+ * variant, then the DP warp threshold, stripe height, row-by-row threshold,
+ * lane width and stripe-kernel register budget, each chosen with the others
+ * fixed -- timing the stage it
  * affects (a second run of every shape, after one untimed), and sets the
  * fastest on the context. Records never depend on the shapes, so the choice
  * only changes speed. */

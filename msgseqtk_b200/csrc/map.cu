@@ -237,8 +237,13 @@ int resident_blocks(msg_ctx* ctx, F kernel, int threads, int64_t n_max) {
 
 template <int K>
 void launch_stripe(msg_ctx* ctx, const DpArgs& a, bool band, int64_t n_max, cudaStream_t st) {
-    if (band) k_dp_stripe<K, true><<<resident_blocks(ctx, k_dp_stripe<K, true>, kStripeThreads, n_max), kStripeThreads, 0, st>>>(a);
-    else k_dp_stripe<K, false><<<resident_blocks(ctx, k_dp_stripe<K, false>, kStripeThreads, n_max), kStripeThreads, 0, st>>>(a);
+    if (ctx->dp_stripe_blocks == 3) {
+        if (band) k_dp_stripe<K, true, 3><<<resident_blocks(ctx, k_dp_stripe<K, true, 3>, kStripeThreads, n_max), kStripeThreads, 0, st>>>(a);
+        else k_dp_stripe<K, false, 3><<<resident_blocks(ctx, k_dp_stripe<K, false, 3>, kStripeThreads, n_max), kStripeThreads, 0, st>>>(a);
+    } else {
+        if (band) k_dp_stripe<K, true, 4><<<resident_blocks(ctx, k_dp_stripe<K, true, 4>, kStripeThreads, n_max), kStripeThreads, 0, st>>>(a);
+        else k_dp_stripe<K, false, 4><<<resident_blocks(ctx, k_dp_stripe<K, false, 4>, kStripeThreads, n_max), kStripeThreads, 0, st>>>(a);
+    }
 }
 
 // One DP launch: over class `cls` of the class-sorted list a.list when
@@ -1686,6 +1691,12 @@ extern "C" int msg_ctx_set_dp_shape(msg_ctx* ctx, int32_t stripe_rows, int64_t s
     return MSG_OK;
 }
 
+extern "C" int msg_ctx_set_dp_occupancy(msg_ctx* ctx, int32_t blocks) {
+    if (!ctx || (blocks != 3 && blocks != 4)) return MSG_EINVAL;
+    ctx->dp_stripe_blocks = blocks;
+    return MSG_OK;
+}
+
 extern "C" int msg_ctx_set_dp_lanes(msg_ctx* ctx, int32_t bits) {
     if (!ctx || (bits != 16 && bits != 32)) return MSG_EINVAL;
     ctx->dp_lanes = bits;
@@ -1709,9 +1720,10 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
     if (rc != MSG_OK) return rc;
     int n_tried = 0;
     // stage times of one shape: an untimed run, then the timed one
-    int best_lanes = 16;
+    int best_lanes = 16, best_blocks = 3;
     auto time_shape = [&](int var, int k, int64_t small, int64_t warp, double* ms_smem, double* ms_dp) -> int {
         ctx->dp_lanes = best_lanes;
+        ctx->dp_stripe_blocks = best_blocks;
         ctx->smem_ff = var == 7;
         ctx->smem_variant = var == 7 ? 0 : var;
         ctx->dp_k = k;
@@ -1753,7 +1765,12 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
     if ((rc = time_shape(best_var, best_k, best_small, best_warp, &ts, &td)) != MSG_OK) return rc;
     if (td < best_dp) best_dp = td;
     else best_lanes = 16;
+    best_blocks = best_blocks == 3 ? 4 : 3;  // the other register budget of the stripe kernel
+    if ((rc = time_shape(best_var, best_k, best_small, best_warp, &ts, &td)) != MSG_OK) return rc;
+    if (td < best_dp) best_dp = td;
+    else best_blocks = best_blocks == 3 ? 4 : 3;
     ctx->dp_lanes = best_lanes;
+    ctx->dp_stripe_blocks = best_blocks;
     ctx->smem_ff = best_var == 7;
     ctx->smem_variant = best_var == 7 ? 0 : best_var;
     ctx->dp_k = best_k;
@@ -1766,6 +1783,7 @@ extern "C" int msg_autotune(msg_ctx* ctx, const msg_read_batch* sample, const ms
     result->ms_dp_default = dp_default;
     result->smem_variant = best_var;
     result->dp_lanes = best_lanes;
+    result->dp_stripe_blocks = best_blocks;
     result->ms_smem = best_smem;
     result->ms_smem_default = smem_default;
     result->n_tried = n_tried;

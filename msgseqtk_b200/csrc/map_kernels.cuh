@@ -2201,9 +2201,10 @@ __global__ void __launch_bounds__(128) k_dp_small(DpArgs a) {
 
 // Mid-size chains: one thread each, rectangles in register stripes of K rows
 // (fill_rect_stripe); k_traceback walks them back. BAND: chains with a
-// banded flank.
-template <int K, bool BAND>
-__global__ void __launch_bounds__(kStripeThreads, 4) k_dp_stripe(DpArgs a) {
+// banded flank. MINB: resident blocks per SM the registers are sized for (4:
+// 128 registers, the 16-bit fill spills; 3: 168, none spills).
+template <int K, bool BAND, int MINB>
+__global__ void __launch_bounds__(kStripeThreads, MINB) k_dp_stripe(DpArgs a) {
     __shared__ uint32_t s_tab[16 * kStripeThreads];  // per-thread score tables, word t of thread x at t * 128 + x
     int64_t first, n_items;
     dp_range(a, first, n_items);

@@ -96,6 +96,7 @@ struct msg_ctx {
     // larger ones on a warp
     int dp_k = 16;
     int dp_lanes = 16;     // 16: unbanded GLOBAL stripe chains that fit use 16-bit lanes (msg_ctx_set_dp_lanes)
+    int dp_stripe_blocks = 3;  // register budget of the stripe kernel: 3 or 4 resident blocks (msg_ctx_set_dp_occupancy)
     int smem_ff = 0;       // SMEM walks and single-entry passes skip unique matches by text comparison (variant 7)
     int smem_variant = 0;  // SMEM thread path (msg_ctx_set_smem_shape): 0 one read per thread, 1/2 two,
                            // 3/4 a pass's candidates extended several at a time

@@ -30,7 +30,7 @@ EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy"
            "msg_db_views", "msg_db_free", "msg_index_bytes",
            "msg_map_params_default", "msg_map_batch", "msg_map_batches", "msg_seed_batch", "msg_locate_batch",
            "msg_chain_batch", "msg_align_batch", "msg_map_batch_device", "msg_last_stats",
-           "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_ctx_set_dp_shape", "msg_ctx_set_dp_lanes", "msg_ctx_set_smem_shape", "msg_autotune", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
+           "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_ctx_set_dp_shape", "msg_ctx_set_dp_lanes", "msg_ctx_set_dp_occupancy", "msg_ctx_set_smem_shape", "msg_autotune", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
            "msg_band_train", "msg_band_grad", "msg_tail_params_default", "msg_tail_batch", "msg_pair_params_default", "msg_tail_pe_batch",
            "msg_fastq_parse", "msg_fastq_format", "msg_clean_format", "msg_sam_format",
            "msg_mem_params_default", "msg_mem_batch", "msg_clean_batch",
@@ -106,7 +106,7 @@ class Tune(C.Structure):
     _fields_ = [("stripe_rows", C.c_int32), ("n_tried", C.c_int32), ("small_area", C.c_int64),
                 ("warp_area", C.c_int64), ("ms_dp", C.c_double), ("ms_dp_default", C.c_double),
                 ("smem_variant", C.c_int32), ("dp_lanes", C.c_int32), ("ms_smem", C.c_double),
-                ("ms_smem_default", C.c_double)]
+                ("ms_smem_default", C.c_double), ("dp_stripe_blocks", C.c_int32), ("pad2", C.c_int32)]
 
 
 class MapStats(C.Structure):
@@ -173,6 +173,7 @@ def load_library(path: str = LIB_PATH):
     L.msg_ctx_set_dp_shape.argtypes = [C.c_void_p, C.c_int32, C.c_int64, C.c_int64]
     L.msg_ctx_set_smem_shape.argtypes = [C.c_void_p, C.c_int32]
     L.msg_ctx_set_dp_lanes.argtypes = [C.c_void_p, C.c_int32]
+    L.msg_ctx_set_dp_occupancy.argtypes = [C.c_void_p, C.c_int32]
     L.msg_autotune.argtypes = [C.c_void_p, C.POINTER(ReadBatch), C.POINTER(MapParams), C.POINTER(Tune)]
     L.msg_smem_batch_noalloc.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(MapParams),
                                          C.c_void_p, C.c_int64, C.c_void_p]
@@ -747,7 +748,12 @@ class Context:
         self._check(self.lib.msg_autotune(self.h, C.byref(b), C.byref(params), C.byref(r)), "msg_autotune")
         return dict(smem_variant=r.smem_variant, stripe_rows=r.stripe_rows, small_area=r.small_area,
                     warp_area=r.warp_area, ms_smem=r.ms_smem, ms_smem_default=r.ms_smem_default, ms_dp=r.ms_dp,
-                    ms_dp_default=r.ms_dp_default, n_tried=r.n_tried, dp_lanes=r.dp_lanes)
+                    ms_dp_default=r.ms_dp_default, n_tried=r.n_tried, dp_lanes=r.dp_lanes,
+                    dp_stripe_blocks=r.dp_stripe_blocks)
+
+    def set_dp_occupancy(self, blocks: int = 3):
+        """Register budget of the stripe DP kernel (msg_ctx_set_dp_occupancy); records do not depend on it."""
+        self._check(self.lib.msg_ctx_set_dp_occupancy(self.h, int(blocks)), "msg_ctx_set_dp_occupancy")
 
     def set_dp_lanes(self, bits: int = 16):
         """Lane width of the stripe DP fill (msg_ctx_set_dp_lanes); records do not depend on it."""

@@ -328,9 +328,10 @@ def test_dp_shape_gives_same_records(oracle_built):
                 compare_with_oracle(base, orc, lambda i: reads[i], len(reads), g, min_len=13, mode=params.mode,
                                     score=tuple(int(v) for v in (params.match, params.mismatch, params.gap_open,
                                                                    params.gap_ext)))
-            for lanes in (16, 32):
+            for lanes, blocks in ((16, 3), (32, 3), (16, 4)):
                 c.set_dp_lanes(lanes)
-                for shape in DP_SHAPES[1:] if lanes == 16 else DP_SHAPES:
+                c.set_dp_occupancy(blocks)
+                for shape in DP_SHAPES[1:] if (lanes, blocks) == (16, 3) else DP_SHAPES[:4]:
                     c.set_dp_shape(*shape)
                     got = c.map(seq, off, params)
                     for k in ("aln", "cigar", "read_aln_off"):
@@ -340,6 +341,7 @@ def test_dp_shape_gives_same_records(oracle_built):
                     assert (st["n_band_exact"], st["n_band_drop"], st["n_band_fallback"]) == \
                         (st0["n_band_exact"], st0["n_band_drop"], st0["n_band_fallback"]), (pi, shape)
             c.set_dp_lanes(16)
+            c.set_dp_occupancy(3)
             assert len(base["aln"]) > 0
         with pytest.raises(lib.MsgError):
             c.set_dp_lanes(8)
@@ -350,8 +352,8 @@ def test_dp_shape_gives_same_records(oracle_built):
         c.set_dp_shape(*DP_SHAPES[0])
         before = c.map(seq, off, params)
         tune = c.autotune(seq, off, params)
-        assert tune["stripe_rows"] in (8, 16, 32) and tune["n_tried"] == 17 and tune["smem_variant"] in range(8)
-        assert tune["dp_lanes"] in (16, 32)
+        assert tune["stripe_rows"] in (8, 16, 32) and tune["n_tried"] == 18 and tune["smem_variant"] in range(8)
+        assert tune["dp_lanes"] in (16, 32) and tune["dp_stripe_blocks"] in (3, 4)
         assert tune["warp_area"] in (4096, 16384, 65536, 262144) and tune["small_area"] in (0, 64, 256, 1024)
         after = c.map(seq, off, params)
         for k in ("aln", "cigar", "read_aln_off"):
