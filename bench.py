@@ -72,7 +72,9 @@ WORKLOADS = {
 }
 CLEAN_METRIC = "cleaned reads/sec/GPU (2x150bp pairs, findMEMS on reference + background index, log-odds decision)"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-SMEM_DRAM_BYTES_PER_EXT = 2.641e9 / 44.86e6
+# DRAM bytes per SMEM extension, ncu on the 60-genome shape with 1 M-read
+# batches (29.55 GB read + written for 449.5 M extensions)
+SMEM_DRAM_BYTES_PER_EXT = 29.552e9 / 449.48e6
 # DRAM bytes per MEM extension, ncu on the 60 + 30 genome clean shape
 # (4.437 GB read + written for 57.32 M extensions)
 MEM_DRAM_BYTES_PER_EXT = 4.437e9 / 57.32e6
@@ -785,7 +787,7 @@ def main():
     smem_bytes = 64.0 * agg["n_ext"] + 32.0 * agg["n_ff_steps"] + read_bytes
     achieved = smem_bytes / (agg["smem"] / 1000.0) / 1e9 if agg["smem"] > 0 else 0.0
     # DRAM bytes per extension measured by ncu on the 60-genome workload shape
-    # (2.641 GB read + written for 44.86 M extensions), scaled to this launch
+    # with 1 M-read batches, scaled to this launch
     traffic = SMEM_DRAM_BYTES_PER_EXT * agg["n_ext"] / args.steps
     smem_roof = {"kernel": "k_smem_thread (SMEM bi-interval extension)", "bound": "hbm", "achieved": achieved,
                  "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
