@@ -1200,9 +1200,10 @@ struct ChainCtx {
     // row/column go where fill_rect_stripe<16> puts them (the last row and
     // column in 32-bit values), so the traceback reads both alike. The row
     // buffer holds 16-bit values here. Returns the cells evaluated.
-    template <bool BANDED>
+    template <bool BANDED, int KH>
     __device__ __noinline__ int64_t fill_rect_stripe16(int m, int w) {
-        constexpr int K = 16;
+        static_assert(KH == 4 || KH == 8 || KH == 16, "rows per half");
+        constexpr int K = KH;
         const RectGeo g = rect(m);
         const RectBnd bi = bnd_info(m);
         if (g.R <= 0 || g.C <= 0) return 0;
@@ -1245,8 +1246,9 @@ struct ChainCtx {
                 for (int k = 0; k < nlo + nhi; ++k) {
                     const int q = qbase(i0 - 1 + k);
                     if (q == 15) continue;  // N scores a mismatch against everything
+                    const uint32_t bit = 1u << (k < K ? k : 16 + k - K);  // upper rows from bit 0, lower from bit 16
 #pragma unroll
-                    for (int t = 1; t < 15; ++t) tbits[t] |= (q & t) ? (1u << k) : 0u;
+                    for (int t = 1; t < 15; ++t) tbits[t] |= (q & t) ? bit : 0u;
                 }
 #pragma unroll
                 for (int t = 0; t < 16; ++t) tab[t * kStripeThreads] = tbits[t];
@@ -1285,8 +1287,17 @@ struct ChainCtx {
                 dlM = (uint32_t)v.x; dlI = (uint32_t)v.y; dlD = (uint32_t)v.z;
             }
             uint32_t dhM = 0u, dhI = 0u, dhD = 0u;
-            uint8_t* const code_lo = g.code + (int64_t)(2 * ds) * C * K;
-            uint8_t* const code_hi = code_lo + (int64_t)C * K;
+            // codes in 16-row stripes: a pair of 16-row halves fills stripes
+            // 2ds and 2ds+1; smaller halves share one stripe, the upper at
+            // byte b0 of each column, the lower right after it
+            uint8_t* const code_lo = K == 16 ? g.code + (int64_t)(2 * ds) * C * 16
+                                             : g.code + (int64_t)(rr0 / 16) * C * 16 + (rr0 % 16);
+            uint8_t* const code_hi = K == 16 ? code_lo + (int64_t)C * 16 : code_lo + K;
+            auto store_codes = [&](uint8_t* p, const uint32_t* wv) {
+                if constexpr (K == 16) *reinterpret_cast<uint4*>(p) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+                else if constexpr (K == 8) *reinterpret_cast<uint2*>(p) = make_uint2(wv[0], wv[1]);
+                else *reinterpret_cast<uint32_t*>(p) = wv[0];
+            };
             const bool last = ds == nds - 1;
             const int lr = R - 1 - rr0;  // the rectangle's last row within this pair (last pair)
             const int cend = nhi > 0 ? max(chi, hhi + 1) : chi;  // last iteration
@@ -1354,7 +1365,7 @@ struct ChainCtx {
                     uM = mv; uI = iv;
                 }
                 if (cc <= chi) {  // upper stripe: column cc
-                    reinterpret_cast<uint4*>(code_lo + (int64_t)cc * K)[0] = make_uint4(wl[0], wl[1], wl[2], wl[3]);
+                    store_codes(code_lo + (int64_t)cc * 16, wl);
                     if (last && lr < K) {
                         uint32_t lm = Mp[0], li = Ip[0], ld = Dp[0];
 #pragma unroll
@@ -1387,7 +1398,7 @@ struct ChainCtx {
                         }
                     } else if (cc - 1 >= hlo && cc - 1 <= hhi) {  // lower stripe: column cc - 1
                         const int c1 = cc - 1;
-                        reinterpret_cast<uint4*>(code_hi + (int64_t)c1 * K)[0] = make_uint4(wh[0], wh[1], wh[2], wh[3]);
+                        store_codes(code_hi + (int64_t)c1 * 16, wh);
                         if (nhi == K)
                             rb4[c1] = make_int4((int)(Mp[K - 1] >> 16), (int)(Ip[K - 1] >> 16), (int)(Dp[K - 1] >> 16), 0);
                         if (last && lr >= K) {
@@ -1951,7 +1962,12 @@ __device__ __forceinline__ void dp_chain(const DpArgs& a, int64_t c, int4* sd, i
                     return;
                 }
             }
-            if (use16) cells += x.template fill_rect_stripe16<false>(m, -1);
+            if (use16) {  // halves of 4, 8 or 16 rows, the fewest that cover the rectangle's rows in one pair
+                const int64_t R = x.rb(m + 1) - x.rb(m);
+                if (R <= 8) cells += x.template fill_rect_stripe16<false, 4>(m, -1);
+                else if (R <= 16) cells += x.template fill_rect_stripe16<false, 8>(m, -1);
+                else cells += x.template fill_rect_stripe16<false, 16>(m, -1);
+            }
             else if (x.pp.mode == 1) cells += x.template fill_rect_stripe<KST, true, false>(m, -1, best, bkey);
             else cells += x.template fill_rect_stripe<KST, false, false>(m, -1, best, bkey);
         } else if constexpr (!WARP) {
