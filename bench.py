@@ -105,6 +105,8 @@ def parse():
                          "clean: msgseqtk-clean's MEM log-odds path on two indexes")
     ap.add_argument("--uneven-reads", type=int, default=500_000)
     ap.add_argument("--no-tune", action="store_true", help="keep the library's default kernel shapes (no autotuner)")
+    ap.add_argument("--sb-contexts", type=int, default=4,
+                    help="contexts mapping the 50 k-read batches side by side (1: one context only)")
     args = ap.parse_args()
     if args.pairs is None:
         args.pairs = 10_000_000 if args.workload == "repeats" else 2_000_000
@@ -445,7 +447,9 @@ def main_clean(args, world, rank, local):
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": WORKLOADS["clean"], "pairs_per_step": bp, "reads_per_step": 2 * bp,
                            "bd_symbols": [v_ref.n, v_bg.n],
-                           "l2": "inputs larger than L2 (indexes %.1f GB, new reads every step)" % setup["index_gb"],
+                           "l2": ("inputs larger than L2 (indexes %.1f GB; %d batches of %.0f MB of mates cycled, "
+                                  "each larger than L2)" % (setup["index_gb"], n_batches,
+                                                            (o1[bp] + o2[bp]) / 1e6)),
                            "parallelism": f"dp{world}" if world > 1 else "single GPU"},
                 "kept_fraction": agg["kept"] / (bp * args.steps),
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
@@ -676,6 +680,61 @@ def main():
         sb_value = n_sb * sb / (e0.elapsed_time(e1) / 1000.0)
         small_batch = {"value": sb_value, "unit": "reads/s", "batch_reads": sb, "batches": n_sb,
                        "fraction_of_value": sb_value / value, "stage_ms_per_batch": sb_stage}
+        # the same batches on several contexts that share the index
+        # (msg_ctx_share_index), one host thread each: a batch's slowest
+        # reads and chains overlap the other batches' work on their streams
+        P = args.sb_contexts
+        if P > 1:
+            side = []
+            for _ in range(P - 1):
+                c2 = lib.Context(local)
+                c2.share_index(ctx)
+                if not args.no_tune:
+                    c2.apply_shapes(dp_shape)
+                c2.band_model_set(bparams)
+                side.append(c2)
+            cs = [ctx] + side
+            sts = [stream] + [torch.cuda.ExternalStream(c.stream_handle()) for c in side]
+
+            def sb_map(c, s):
+                c.map_device(d_seq.data_ptr() + int(reads.offs[(3 + s) * sb]), sb_offs[s].data_ptr(), sb, params)
+
+            for c in side:  # each context sizes its buffers untimed
+                for s in range(3):
+                    sb_map(c, s)
+            torch.cuda.synchronize()
+            errs = []
+
+            def sb_worker(j):
+                try:
+                    for s in range(j, n_sb, P):
+                        sb_map(cs[j], s)
+                except Exception as exc:  # re-raised below
+                    errs.append(exc)
+
+            e0.record(stream)
+            for st_ in sts[1:]:
+                st_.wait_event(e0)
+            workers = [threading.Thread(target=sb_worker, args=(j,)) for j in range(P)]
+            for w in workers:
+                w.start()
+            for w in workers:
+                w.join()
+            if errs:
+                raise errs[0]
+            for st_ in sts[1:]:
+                ev = torch.cuda.Event()
+                ev.record(st_)
+                stream.wait_event(ev)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            cv = n_sb * sb / (e0.elapsed_time(e1) / 1000.0)
+            small_batch["contexts"] = {"value": cv, "unit": "reads/s", "contexts": P, "batches": n_sb,
+                                       "fraction_of_value": cv / value,
+                                       "note": "one host thread per context, index shared (msg_ctx_share_index); "
+                                               "device time from the first launch to the last stream's end"}
+            for c in side:
+                c.close()
     banded = agg["n_band_exact"] + agg["n_band_drop"] + agg["n_band_fallback"]
 
     def gcups(a):

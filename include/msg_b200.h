@@ -97,8 +97,32 @@ int msg_db_read(const char* mtg_path, const char* mgs_path, const char* fmd_path
 int msg_db_views(const msg_db* db, msg_fmd_view* fmd, msg_mtg_view* mtg);
 void msg_db_free(msg_db* db);
 
+/* msg_db_read with a decoded image of the database kept at image_path (e.g.
+ * "<db>.fmd.b200"), the load step of the same call sites. The image holds the
+ * decoded arrays and is keyed by the sizes and 64-bit content hashes of the
+ * three files: when the key and the image's own body hash match, the database
+ * is read from it (no wavelet-tree decode; *from_image = 1); otherwise the
+ * files are decoded and the image is written anew next to its path and
+ * renamed into place (*from_image = 0, or -1 when it could not be written,
+ * which is not an error). from_image may be NULL. */
+int msg_db_read_cached(const char* mtg_path, const char* mgs_path, const char* fmd_path, const char* image_path,
+                       int n_threads, msg_db** db, int* from_image);
+
 /* Device bytes held by the loaded index. */
 int msg_index_bytes(const msg_ctx* ctx, int64_t* bytes);
+
+/* Let `ctx` map against the index `owner` loaded, without a second copy in
+ * device memory (both contexts on the same device). The reference's mapping
+ * tasks share one read-only FMDIndex and MetaGenome across OpenMP threads
+ * (src/msgseqtk-align.cpp:600-607, the const pointers held at SMEM.h:192-194
+ * and Alignment.h:352-355); this is the same sharing across contexts, so that
+ * several host threads, one context each, can map batches side by side on
+ * their own streams. The index memory lives until the last context holding
+ * it is destroyed or loads another index; reloading `owner` afterwards does
+ * not change what `ctx` maps against. Kernel shapes and the band model are
+ * per context and are not copied. Waits for `ctx`'s own stream first.
+ * MSG_ESTATE if `owner` has no index. */
+int msg_ctx_share_index(msg_ctx* ctx, const msg_ctx* owner);
 
 /* Mapping parameters (src/msgseqtk-align.cpp:183-397 defaults). */
 typedef struct msg_map_params {

@@ -34,9 +34,12 @@
 // sequence). The wavelet tree gives the positions WaveletTreeRRR::access
 // (WaveletTreeRRR.cpp:58-76) walks to; rows decoded in order reach them with
 // one cursor per tree node, on several host threads.
+#include <unistd.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <string>
@@ -461,5 +464,269 @@ extern "C" int msg_db_views(const msg_db* db, msg_fmd_view* fmd, msg_mtg_view* m
     mtg->chr_len = db->chr_len.data();
     mtg->chr_seq = db->chr_seq.data();
     mtg->chr_off = db->chr_off.data();
+    return MSG_OK;
+}
+
+// ---- Decoded image of a database (msg_db_read_cached) ----
+//
+// The wavelet-tree decode above costs seconds per G symbols; the image holds
+// its result -- the arrays msg_db_views hands out and the chromosome names --
+// so that a later run reads them back in one pass. The image is keyed by the
+// three source files' sizes and 64-bit content hashes, and carries a hash of
+// its own body; an image whose key or body does not match is ignored and
+// written anew.
+//
+// Layout (little-endian): "MSGB200I", uint32 version, uint32 0; key: three
+// (uint64 size, uint64 hash) for .mtg, .mgs, .fmd; int64 n, base_count[16],
+// n_samples, n_chrom, total chromosome bases, name bytes; then bwt[n],
+// sample_rows, sample_vals, bd_start, bd_end, chr_len, chr_off[n_chrom + 1],
+// chr_seq, the names (each a uint64 length + bytes); last, the body hash.
+namespace {
+
+constexpr char kImageMagic[8] = {'M', 'S', 'G', 'B', '2', '0', '0', 'I'};
+constexpr uint32_t kImageVersion = 1;
+
+uint64_t fold64(uint64_t x) {  // splitmix64's finaliser
+    x ^= x >> 30;
+    x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27;
+    x *= 0x94d049bb133111ebull;
+    return x ^ (x >> 31);
+}
+
+// Hash of a byte range: four lanes over consecutive 8-byte words (xor, odd
+// multiply, xor-shift: a bijection of the lane per word), folded with the
+// tail bytes and the length. It tells files apart; it is not meant to
+// resist a deliberate collision.
+uint64_t hash_range(const uint8_t* p, size_t n, uint64_t seed) {
+    uint64_t l[4] = {seed ^ 0x243f6a8885a308d3ull, seed ^ 0x13198a2e03707344ull, seed ^ 0xa4093822299f31d0ull,
+                     seed ^ 0x082efa98ec4e6c89ull};
+    size_t i = 0;
+    for (; i + 32 <= n; i += 32) {
+        uint64_t w[4];
+        std::memcpy(w, p + i, 32);
+        for (int j = 0; j < 4; ++j) {
+            l[j] = (l[j] ^ w[j]) * 0x9e3779b97f4a7c15ull;
+            l[j] ^= l[j] >> 32;
+        }
+    }
+    uint64_t h = fold64(seed ^ (uint64_t)n);
+    for (; i < n; ++i) h = fold64(h ^ p[i]);
+    for (int j = 0; j < 4; ++j) h = fold64(h ^ l[j]);
+    return h;
+}
+
+constexpr size_t kHashChunk = 16u << 20;
+
+// hash_range over chunks of kHashChunk bytes on up to nt threads, the chunk
+// hashes folded in order (the result does not depend on nt)
+uint64_t hash_par(const uint8_t* p, size_t n, int nt) {
+    const size_t nc = (n + kHashChunk - 1) / kHashChunk;
+    std::vector<uint64_t> ch(nc);
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t k; (k = next.fetch_add(1)) < nc;)
+            ch[k] = hash_range(p + k * kHashChunk, std::min(kHashChunk, n - k * kHashChunk), k);
+    };
+    const int w = (int)std::min<size_t>(nc, (size_t)std::max(1, nt));
+    std::vector<std::thread> th;
+    for (int t = 1; t < w; ++t) th.emplace_back(work);
+    work();
+    for (auto& x : th) x.join();
+    uint64_t h = fold64(n);
+    for (uint64_t x : ch) h = fold64(h ^ x);
+    return h;
+}
+
+// Size and hash of a file's contents, read in chunks of kHashChunk bytes by
+// up to nt threads (each with its own stream); same value as hash_par over
+// the whole file.
+bool hash_file(const char* path, int nt, uint64_t* size, uint64_t* hash) {
+    std::ifstream f(path, std::ios::binary | std::ios::ate);
+    if (!f) return false;
+    const std::streamoff end = f.tellg();
+    if (end < 0) return false;
+    const size_t n = (size_t)end;
+    const size_t nc = (n + kHashChunk - 1) / kHashChunk;
+    std::vector<uint64_t> ch(nc);
+    std::atomic<size_t> next{0};
+    std::atomic<bool> bad{false};
+    auto work = [&]() {
+        std::ifstream in(path, std::ios::binary);
+        std::vector<uint8_t> buf(std::min(kHashChunk, n));
+        if (!in) { bad = true; return; }
+        for (size_t k; (k = next.fetch_add(1)) < nc;) {
+            const size_t len = std::min(kHashChunk, n - k * kHashChunk);
+            in.seekg((std::streamoff)(k * kHashChunk));
+            in.read(reinterpret_cast<char*>(buf.data()), (std::streamsize)len);
+            if (!in) { bad = true; return; }
+            ch[k] = hash_range(buf.data(), len, k);
+        }
+    };
+    const int w = (int)std::min<size_t>(nc, (size_t)std::max(1, nt));
+    std::vector<std::thread> th;
+    for (int t = 1; t < w; ++t) th.emplace_back(work);
+    work();
+    for (auto& x : th) x.join();
+    if (bad) return false;
+    uint64_t h = fold64(n);
+    for (uint64_t x : ch) h = fold64(h ^ x);
+    *size = n;
+    *hash = h;
+    return true;
+}
+
+struct ImageKey {
+    uint64_t v[6] = {};
+    bool operator==(const ImageKey& o) const { return std::memcmp(v, o.v, sizeof(v)) == 0; }
+};
+
+template <typename T> uint64_t vec_hash(const std::vector<T>& x, int nt) {
+    return hash_par(reinterpret_cast<const uint8_t*>(x.data()), x.size() * sizeof(T), nt);
+}
+
+uint64_t body_hash(const msg_db& d, int nt) {
+    uint64_t h = fold64(0x6d7367ull);
+    for (uint64_t x : {vec_hash(d.bwt, nt), vec_hash(d.sample_rows, nt), vec_hash(d.sample_vals, nt),
+                       vec_hash(d.bd_start, nt), vec_hash(d.bd_end, nt), vec_hash(d.chr_len, nt),
+                       vec_hash(d.chr_off, nt), vec_hash(d.chr_seq, nt),
+                       hash_range(reinterpret_cast<const uint8_t*>(d.base_count), sizeof(d.base_count), 16)})
+        h = fold64(h ^ x);
+    for (const std::string& s : d.chr_names)
+        h = fold64(h ^ hash_range(reinterpret_cast<const uint8_t*>(s.data()), s.size(), 17));
+    return h;
+}
+
+template <typename T> bool put(std::ofstream& o, const T* p, size_t n) {
+    if (n) o.write(reinterpret_cast<const char*>(p), (std::streamsize)(n * sizeof(T)));
+    return (bool)o;
+}
+
+bool write_image(const char* path, const ImageKey& key, const msg_db& d, int nt) {
+    // written beside the target and renamed over it, so a reader never
+    // sees a partial image
+    const std::string tmp = std::string(path) + ".tmp." + std::to_string((long)getpid());
+    {
+        std::ofstream o(tmp, std::ios::binary | std::ios::trunc);
+        if (!o) return false;
+        int64_t names = 0;
+        for (const std::string& s : d.chr_names) names += 8 + (int64_t)s.size();
+        const uint32_t ver[2] = {kImageVersion, 0};
+        const int64_t head[4] = {(int64_t)d.sample_rows.size(), (int64_t)d.chr_len.size(),
+                                 (int64_t)d.chr_seq.size(), names};
+        const int64_t n = (int64_t)d.bwt.size();
+        bool ok = put(o, kImageMagic, 8) && put(o, ver, 2) && put(o, key.v, 6) && put(o, &n, 1) &&
+                  put(o, d.base_count, 16) && put(o, head, 4) && put(o, d.bwt.data(), d.bwt.size()) &&
+                  put(o, d.sample_rows.data(), d.sample_rows.size()) &&
+                  put(o, d.sample_vals.data(), d.sample_vals.size()) && put(o, d.bd_start.data(), d.bd_start.size()) &&
+                  put(o, d.bd_end.data(), d.bd_end.size()) && put(o, d.chr_len.data(), d.chr_len.size()) &&
+                  put(o, d.chr_off.data(), d.chr_off.size()) && put(o, d.chr_seq.data(), d.chr_seq.size());
+        for (const std::string& s : d.chr_names) {
+            const uint64_t len = s.size();
+            ok = ok && put(o, &len, 1) && put(o, s.data(), s.size());
+        }
+        const uint64_t bh = body_hash(d, nt);
+        ok = ok && put(o, &bh, 1);
+        o.close();
+        if (!ok || !o) { std::remove(tmp.c_str()); return false; }
+    }
+    if (std::rename(tmp.c_str(), path) != 0) { std::remove(tmp.c_str()); return false; }
+    return true;
+}
+
+// Reads an image whose key equals `key` and whose body hash and tables are
+// consistent; false (and `d` left partly filled) for anything else.
+bool read_image(const char* path, const ImageKey& key, msg_db& d, int nt) {
+    std::ifstream in(path, std::ios::binary | std::ios::ate);
+    if (!in) return false;
+    const std::streamoff fsize = in.tellg();
+    in.seekg(0);
+    auto get = [&](void* p, size_t bytes) {
+        if (bytes) in.read(reinterpret_cast<char*>(p), (std::streamsize)bytes);
+        return (bool)in;
+    };
+    char magic[8];
+    uint32_t ver[2];
+    ImageKey k;
+    int64_t n = 0, head[4];
+    if (!get(magic, 8) || std::memcmp(magic, kImageMagic, 8) != 0 || !get(ver, 8) || ver[0] != kImageVersion ||
+        !get(k.v, sizeof(k.v)) || !(k == key) || !get(&n, 8) || !get(d.base_count, sizeof(d.base_count)) ||
+        !get(head, sizeof(head)))
+        return false;
+    const int64_t ns = head[0], nc = head[1], nseq = head[2], names = head[3];
+    if (n <= 0 || ns < 0 || nc <= 0 || nseq < 0 || names < 8 * nc) return false;
+    // the sizes must account for the file exactly
+    const int64_t fixed = 8 + 8 + (int64_t)sizeof(k.v) + 8 + (int64_t)sizeof(d.base_count) + (int64_t)sizeof(head);
+    const double body = (double)n + 16.0 * ns + 8.0 * (4 * nc + 1) + (double)nseq + (double)names + 8.0;
+    if ((double)fixed + body != (double)fsize) return false;
+    d.bwt.resize(n);
+    d.sample_rows.resize(ns);
+    d.sample_vals.resize(ns);
+    d.bd_start.resize(nc);
+    d.bd_end.resize(nc);
+    d.chr_len.resize(nc);
+    d.chr_off.resize(nc + 1);
+    d.chr_seq.resize(nseq);
+    if (!get(d.bwt.data(), n) || !get(d.sample_rows.data(), 8 * ns) || !get(d.sample_vals.data(), 8 * ns) ||
+        !get(d.bd_start.data(), 8 * nc) || !get(d.bd_end.data(), 8 * nc) || !get(d.chr_len.data(), 8 * nc) ||
+        !get(d.chr_off.data(), 8 * (nc + 1)) || !get(d.chr_seq.data(), nseq))
+        return false;
+    d.chr_names.resize(nc);
+    int64_t left = names;
+    for (int64_t c = 0; c < nc; ++c) {
+        uint64_t len = 0;
+        if (!get(&len, 8) || (int64_t)len > left - 8) return false;
+        d.chr_names[c].resize(len);
+        if (!get(&d.chr_names[c][0], len)) return false;
+        left -= 8 + (int64_t)len;
+    }
+    uint64_t bh = 0;
+    if (left != 0 || !get(&bh, 8) || bh != body_hash(d, nt)) return false;
+    // the tables msg_db_read checks on a decode
+    int64_t tot = 0;
+    for (int b = 0; b < 16; ++b) {
+        if (d.base_count[b] < 0) return false;
+        tot += d.base_count[b];
+    }
+    if (tot != n || d.chr_off[0] != 0 || d.chr_off[nc] != nseq || d.bd_end[nc - 1] != n) return false;
+    for (int64_t c = 0; c < nc; ++c)
+        if (d.chr_off[c + 1] - d.chr_off[c] != d.chr_len[c] || d.bd_end[c] - d.bd_start[c] != 2 * (d.chr_len[c] + 1))
+            return false;
+    return true;
+}
+
+}  // namespace
+
+extern "C" int msg_db_read_cached(const char* mtg_path, const char* mgs_path, const char* fmd_path,
+                                  const char* image_path, int n_threads, msg_db** db, int* from_image) {
+    if (!mtg_path || !mgs_path || !fmd_path || !image_path || !db) return MSG_EINVAL;
+    *db = nullptr;
+    if (from_image) *from_image = 0;
+    const int nt = std::max(1, n_threads);
+    ImageKey key;
+    const char* src[3] = {mtg_path, mgs_path, fmd_path};
+    try {
+        for (int f = 0; f < 3; ++f)
+            if (!hash_file(src[f], nt, &key.v[2 * f], &key.v[2 * f + 1])) return MSG_EINVAL;
+        msg_db* d = new (std::nothrow) msg_db();
+        if (!d) return MSG_ENOMEM;
+        if (read_image(image_path, key, *d, nt)) {
+            *db = d;
+            if (from_image) *from_image = 1;
+            return MSG_OK;
+        }
+        delete d;
+    } catch (const std::bad_alloc&) {
+        return MSG_ENOMEM;
+    }
+    const int rc = msg_db_read(mtg_path, mgs_path, fmd_path, n_threads, db);
+    if (rc != MSG_OK) return rc;
+    bool written = false;
+    try {
+        written = write_image(image_path, key, **db, nt);
+    } catch (const std::bad_alloc&) {
+        written = false;
+    }
+    if (from_image) *from_image = written ? 0 : -1;
     return MSG_OK;
 }

@@ -438,6 +438,10 @@ extern "C" int msg_index_load(msg_ctx* ctx, const msg_fmd_view* fmd, const msg_m
         static const int to_basic[16] = {0, 1, 2, 2, 4, 4, 4, 4, 8, 8, 8, 8, 8, 8, 8, 15};
         for (int b = 0; b < 16; ++b) im.llk[b] = std::log((double)B[to_basic[b]]) - std::log((double)n);
     }
+    if (!ctx->index_own()) {
+        rc = ctx->fail(MSG_ENOMEM, "index ownership record");
+        goto done;
+    }
     im.loaded = true;
 done:
 #undef CK
@@ -452,6 +456,25 @@ extern "C" int msg_index_bytes(const msg_ctx* ctx, int64_t* bytes) {
     if (!ctx || !bytes) return MSG_EINVAL;
     if (!ctx->idx.loaded) return MSG_ESTATE;
     *bytes = ctx->idx.bytes;
+    return MSG_OK;
+}
+
+extern "C" int msg_ctx_share_index(msg_ctx* ctx, const msg_ctx* owner) {
+    if (!ctx || !owner || ctx == owner) return MSG_EINVAL;
+    if (ctx->device != owner->device) return ctx->fail(MSG_EINVAL, "contexts on different devices");
+    if (!owner->idx.loaded || !owner->idx.mem) return ctx->fail(MSG_ESTATE, "the owner has no index loaded");
+    msg::DeviceGuard dg_(ctx->device);
+    if (!dg_.ok) return ctx->fail(MSG_ECUDA, "cudaSetDevice");
+    // work this context still has in flight may read its current index
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return ctx->cuda_fail(e);
+    try {
+        msg::IndexImage im = owner->idx;  // copies the chromosome lengths: may throw
+        ctx->index_free();
+        ctx->idx = std::move(im);
+    } catch (const std::bad_alloc&) {
+        return ctx->fail(MSG_ENOMEM, "chromosome table");
+    }
     return MSG_OK;
 }
 

@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -14,8 +15,18 @@
 
 namespace msg {
 
+// The device allocations of one loaded index. Held through a shared_ptr by
+// the context that loaded it and by every context that shares it
+// (msg_ctx_share_index); the last holder to let go frees them.
+struct IndexMem {
+    int device = 0;
+    void* p[9] = {};
+    ~IndexMem();
+};
+
 struct IndexImage {
     bool loaded = false;
+    std::shared_ptr<IndexMem> mem;  // set once a load has succeeded
     Bucket* bkt = nullptr;
     int64_t* dollar_rows = nullptr;
     int64_t* n_rows = nullptr;
@@ -67,6 +78,12 @@ struct DeviceGuard {
     DeviceGuard(const DeviceGuard&) = delete;
     DeviceGuard& operator=(const DeviceGuard&) = delete;
 };
+
+inline IndexMem::~IndexMem() {
+    DeviceGuard g(device);
+    for (void* q : p)
+        if (q) cudaFree(q);
+}
 
 }  // namespace msg
 
@@ -147,7 +164,26 @@ struct msg_ctx {
         for (auto& s : dp_side) if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); s = nullptr; }
         for (auto& e : dp_ev) if (e) { cudaEventDestroy(e); e = nullptr; }
     }
+    // After a successful load the image's allocations move into a shared
+    // IndexMem; index_free then only drops this context's hold on them.
+    bool index_own() {
+        try {
+            auto m = std::make_shared<msg::IndexMem>();
+            m->device = device;
+            void* ps[9] = {idx.bkt, idx.dollar_rows, idx.n_rows, idx.n_before, idx.sa, idx.text, idx.isa,
+                           idx.chr_tab, idx.chr_seq};
+            for (int k = 0; k < 9; ++k) m->p[k] = ps[k];
+            idx.mem = std::move(m);
+        } catch (const std::bad_alloc&) {
+            return false;
+        }
+        return true;
+    }
     void index_free() {
+        if (idx.mem) {
+            idx = msg::IndexImage();  // frees the allocations if no other context holds them
+            return;
+        }
         if (idx.bkt) cudaFree(idx.bkt);
         if (idx.dollar_rows) cudaFree(idx.dollar_rows);
         if (idx.n_rows) cudaFree(idx.n_rows);

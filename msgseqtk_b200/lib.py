@@ -27,7 +27,7 @@ assert ALN_DTYPE.itemsize == 88
 
 # symbols of the C ABI, in include/msg_b200.h order
 EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy", "msg_index_load", "msg_db_read",
-           "msg_db_views", "msg_db_free", "msg_index_bytes",
+           "msg_db_views", "msg_db_free", "msg_db_read_cached", "msg_index_bytes", "msg_ctx_share_index",
            "msg_map_params_default", "msg_map_batch", "msg_map_batches", "msg_seed_batch", "msg_locate_batch",
            "msg_chain_batch", "msg_align_batch", "msg_map_batch_device", "msg_last_stats",
            "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_ctx_set_dp_shape", "msg_ctx_set_dp_lanes", "msg_ctx_set_dp_occupancy", "msg_ctx_set_smem_shape", "msg_autotune", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
@@ -148,9 +148,12 @@ def load_library(path: str = LIB_PATH):
     L.msg_ctx_destroy.argtypes = [C.c_void_p]
     L.msg_index_load.argtypes = [C.c_void_p, C.POINTER(FmdView), C.POINTER(MtgView)]
     L.msg_index_bytes.argtypes = [C.c_void_p, i64p]
+    L.msg_ctx_share_index.argtypes = [C.c_void_p, C.c_void_p]
     L.msg_db_read.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]
     L.msg_db_views.argtypes = [C.c_void_p, C.POINTER(FmdView), C.POINTER(MtgView)]
     L.msg_db_free.argtypes = [C.c_void_p]
+    L.msg_db_read_cached.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.POINTER(C.c_void_p),
+                                     C.POINTER(C.c_int)]
     L.msg_db_free.restype = None
     L.msg_map_params_default.argtypes = [C.POINTER(MapParams)]
     L.msg_map_params_default.restype = None
@@ -421,6 +424,18 @@ class Context:
     def load_database(self, db: "Database"):
         """msg_index_load from a database read with msg_db_read."""
         self._check(self.lib.msg_index_load(self.h, C.byref(db.fmd), C.byref(db.mtg)), "msg_index_load")
+
+    def share_index(self, owner: "Context"):
+        """Map against the index `owner` loaded, without a second device
+        copy (msg_ctx_share_index); the memory lives while any holder does."""
+        self._check(self.lib.msg_ctx_share_index(self.h, owner.h), "msg_ctx_share_index")
+
+    def apply_shapes(self, shapes: dict):
+        """Set the kernel shapes an autotune() result names on this context."""
+        self.set_smem_shape(shapes["smem_variant"])
+        self.set_dp_shape(shapes["stripe_rows"], shapes["small_area"], shapes["warp_area"])
+        self.set_dp_lanes(shapes["dp_lanes"])
+        self.set_dp_occupancy(shapes["dp_stripe_blocks"])
 
     def index_bytes(self) -> int:
         b = C.c_int64(0)
@@ -824,13 +839,22 @@ class Database:
     """A database read from msgseqtk-build files (msg_db_read): host arrays of
     the FMD-index and the MetaGenome, as numpy views."""
 
-    def __init__(self, mtg_path, mgs_path, fmd_path, n_threads: int = 8):
+    def __init__(self, mtg_path, mgs_path, fmd_path, n_threads: int = 8, image=None):
+        """With `image` (a path), msg_db_read_cached: read the decoded image
+        there when it matches the files, else decode and write it;
+        `from_image` tells which (1 read, 0 written, -1 not writable)."""
         self.lib = load_library()
         self.h = C.c_void_p()
-        rc = self.lib.msg_db_read(str(mtg_path).encode(), str(mgs_path).encode(), str(fmd_path).encode(),
-                                  n_threads, C.byref(self.h))
+        self.from_image = None
+        paths = [str(x).encode() for x in (mtg_path, mgs_path, fmd_path)]
+        if image is None:
+            rc = self.lib.msg_db_read(*paths, n_threads, C.byref(self.h))
+        else:
+            hit = C.c_int(0)
+            rc = self.lib.msg_db_read_cached(*paths, str(image).encode(), n_threads, C.byref(self.h), C.byref(hit))
+            self.from_image = hit.value
         if rc != MSG_OK:
-            raise MsgError(rc, "msg_db_read")
+            raise MsgError(rc, "msg_db_read" if image is None else "msg_db_read_cached")
         self.fmd = FmdView()
         self.mtg = MtgView()
         self.lib.msg_db_views(self.h, C.byref(self.fmd), C.byref(self.mtg))

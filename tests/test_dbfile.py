@@ -93,6 +93,71 @@ def test_db_read_rejects_inconsistent_occurrence_table(tmp_path, entry, delta):
         assert e.value.code == lib.MSG_EINVAL
 
 
+def _same_arrays(a, b):
+    assert a.keys() == b.keys()
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+
+
+@needs_ref
+def test_decoded_image_is_reused_and_rebuilt(tmp_path):
+    """msg_db_read_cached: the first read decodes and writes the image, the
+    next reads it back (same arrays as a plain decode, for any thread
+    count); an image whose source files changed, whose body was altered or
+    cut short, or of another format is ignored and written anew."""
+    g = synth.repeat_genomes(seed=6, n_genomes=3, length=20_000)
+    _, paths = _write(tmp_path, g)
+    img = tmp_path / "db.fmd.b200"
+    plain = lib.Database(*paths, n_threads=2)
+    want = plain.arrays()
+    plain.close()
+    first = lib.Database(*paths, n_threads=3, image=img)
+    assert first.from_image == 0 and img.exists()
+    _same_arrays(first.arrays(), want)
+    first.close()
+    for nt in (1, 5):
+        again = lib.Database(*paths, n_threads=nt, image=img)
+        assert again.from_image == 1
+        _same_arrays(again.arrays(), want)
+        again.close()
+
+    good = img.read_bytes()
+    for damaged in (good[:-1], good[:len(good) // 2], good[:9] + bytes([good[9] ^ 1]) + good[10:],
+                    good[:-200] + bytes([good[-200] ^ 0x40]) + good[-199:]):
+        img.write_bytes(damaged)
+        db = lib.Database(*paths, n_threads=2, image=img)
+        assert db.from_image == 0
+        _same_arrays(db.arrays(), want)
+        db.close()
+        assert img.read_bytes() == good
+
+    # other source files at the same paths: a new key, the new database
+    g2 = synth.small_genomes(seed=7, n_genomes=2, length=15_000)
+    _, paths2 = _write(tmp_path, g2)
+    assert paths2 == paths
+    db = lib.Database(*paths, n_threads=2, image=img)
+    assert db.from_image == 0
+    a = db.arrays()
+    assert np.array_equal(a["chr_seq"], np.concatenate(g2))
+    db.close()
+    db = lib.Database(*paths, n_threads=2, image=img)
+    assert db.from_image == 1
+    _same_arrays(db.arrays(), a)
+    db.close()
+
+    # an image path that cannot be written: decoded all the same
+    db = lib.Database(*paths, n_threads=2, image=tmp_path / "missing_dir" / "x.b200")
+    assert db.from_image == -1
+    _same_arrays(db.arrays(), a)
+    db.close()
+    # unreadable source files are an error, as for msg_db_read
+    with pytest.raises(lib.MsgError) as e:
+        lib.Database(paths[0], paths[1], tmp_path / "missing.fmd", image=img)
+    assert e.value.code == lib.MSG_EINVAL
+    L = lib.load_library()
+    assert L.msg_db_read_cached(None, None, None, None, 1, None, None) == lib.MSG_EINVAL
+
+
 @pytest.mark.gpu
 @needs_ref
 def test_index_from_db_files_maps_like_view(tmp_path):
