@@ -253,6 +253,35 @@ def cpu_baseline(genomes, view, reads, target_s, impl_line=False):
             "seconds": round(sec, 2), "mapped_reads": int(mapped), "index_build_s": round(build_s, 1)}, ref
 
 
+def sam_validation(ref, view, ctx, reads, n, params, min_score):
+    """SAM fields of the first n reads (whole pairs), mapped on the GPU and
+    passed through the library's paired-end tail, against the reference's
+    whole paired-end path (findSeedsPE -> ... -> AlignmentPE -> output) with
+    -m 400 -d 50, compiled from its sources."""
+    from msgseqtk_b200 import lib
+    from oracle.sam_fields import ours_as_fields, ref_as_fields
+    n = min(n, len(reads))
+    n -= n % 2
+    if n <= 0:
+        return None
+    try:
+        seq, qual, off = reads.seqs[:reads.offs[n]], reads.quals[:reads.offs[n]], reads.offs[:n + 1]
+        exp = ref_as_fields(ref.sam_pe_batch(seq, qual, off, min_score_rate=min_score, max_report=1,
+                                             pairing=dict(mean=400.0, sd=50.0, min=-100.0, max=900.0)))
+        res = ctx.map(seq, off, params)
+        recs, md = lib.tail(view, seq, off, qual, res["aln"], res["cigar"], res["read_aln_off"],
+                            lib.tail_params(min_score_rate=min_score, max_report=1),
+                            pairing=lib.pair_params(mean=400.0, sd=50.0, min_ins=-100.0, max_ins=900.0))
+        got = ours_as_fields(recs, md, seq, qual, off, res["cigar"], pairs=True)
+        bad = sum(1 for g, e in zip(got, exp) if g != e) + abs(len(got) - len(exp))
+        return {"pairs": n // 2, "records": len(exp), "mismatching_records": bad,
+                "compared": "SAM fields (flag, tid, pos, MAPQ, CIGAR, SEQ, QUAL, TLEN, AS, MD, XH, NH, XN, XP; "
+                            "float tags to the bit) of the learned-band path + msg_tail_pe_batch against the "
+                            "reference's paired-end path, -m 400 -d 50 -s %g" % min_score}
+    except Exception as exc:  # reported in the line, not fatal to the measurement
+        return {"error": f"{type(exc).__name__}: {exc}"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -910,6 +939,8 @@ def main():
     if rank == 0 and not args.no_cpu_baseline and args.workload in ("scale", "repeats"):
         r = cpu_baseline(genomes, view, reads, args.cpu_seconds)
         cpu = r[0] if r else None
+        if r and valid is not None:
+            valid["sam"] = sam_validation(r[1], view, ctx, reads, args.validate, params, args.min_score)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,

@@ -11,6 +11,7 @@ import pytest
 
 from msgseqtk_b200 import lib, synth
 from oracle.bind import REF_SO, Oracle, Reference
+from oracle.sam_fields import ours_as_fields as _ours_as_fields, ref_as_fields as _ref_as_fields
 
 needs_ref = pytest.mark.skipif(not os.path.exists(REF_SO), reason="oracle/_ref not built")
 
@@ -41,46 +42,6 @@ def _workload(seed):
     qual = np.concatenate(quals).astype(np.uint8)
     off = np.concatenate([[0], np.cumsum([len(x) for x in reads])]).astype(np.int64)
     return g, reads, seq, qual, off
-
-
-_COMP = np.array([0, 8, 4, 12, 2, 10, 6, 14, 1, 9, 5, 13, 3, 11, 7, 15], dtype=np.uint8)
-
-
-def _ours_as_fields(recs, md, seq, qual, off, cigar, pairs=False):
-    """The library's tail records as the fields of the reference harness's
-    lines: QNAME FLAG TID POS MAPQ CIGAR L_SEQ SEQ QUAL ISIZE then aux (floats
-    as float values, compared exactly)."""
-    rows = []
-    for r in recs:
-        i = int(r["read"])
-        name = f"p{i // 2}" if pairs else f"r{i}"
-        q = seq[off[i]:off[i + 1]]
-        ql = qual[off[i]:off[i + 1]]
-        if r["flag"] & 0x10:
-            q, ql = _COMP[q[::-1]], ql[::-1]
-        cg = cigar[r["cigar_off"]:r["cigar_off"] + r["n_cigar"]] if r["n_cigar"] else []
-        cs = "".join(f"{int(c) >> 4}{'MIDNSHP=XB'[int(c) & 15]}" for c in cg) or "*"
-        f = [name, str(int(r["flag"])), str(int(r["tid"])), str(int(r["pos"])), str(int(r["mapq"])), cs,
-             str(len(q)), "".join(f"{int(x):x}" for x in q), "".join(f"{int(x):02x}" for x in ql),
-             str(int(r["isize"]))]
-        if not r["flag"] & 0x4:
-            m = md[r["md_off"]:r["md_off"] + r["md_len"]].decode()
-            f += [f"AS:i:{int(r['as'])}", f"MD:Z:{m}", ("XH", float(r["xh"])), f"NH:i:{int(r['nh'])}",
-                  f"XN:i:{int(r['xn'])}", ("XP", float(r["xp"]))]
-        rows.append(f)
-    return rows
-
-
-def _ref_as_fields(lines):
-    rows = []
-    for line in lines:
-        f = line.split("\t")
-        out = f[:10]
-        for a in f[10:]:
-            tag, typ, val = a.split(":", 2)
-            out.append((tag, float.fromhex(val)) if typ == "f" else a)
-        rows.append(out)
-    return rows
 
 
 def _check_tail(view, ref, seq, qual, off, aln, cig, roff, rate, max_report):
