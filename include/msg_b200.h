@@ -97,6 +97,14 @@ int msg_db_read(const char* mtg_path, const char* mgs_path, const char* fmd_path
 int msg_db_views(const msg_db* db, msg_fmd_view* fmd, msg_mtg_view* mtg);
 void msg_db_free(msg_db* db);
 
+/* msg_db_read with the BWT decoded on the GPU `device`: the same database,
+ * the same checks (MSG_EINVAL for files msg_db_read rejects), the RRR bit
+ * sequences unranked, the wavelet tree walked (WaveletTreeRRR::access,
+ * src/libsds/src/WaveletTreeRRR.cpp:58-76) and the sampled rows listed by
+ * device kernels instead of host threads. Device memory is held only during
+ * the call (about 2.5 bytes per BD symbol); the result lives on the host. */
+int msg_db_read_device(int device, const char* mtg_path, const char* mgs_path, const char* fmd_path, msg_db** db);
+
 /* msg_db_read with a decoded image of the database kept at image_path (e.g.
  * "<db>.fmd.b200"), the load step of the same call sites. The image holds the
  * decoded arrays and is keyed by the sizes and 64-bit content hashes of the

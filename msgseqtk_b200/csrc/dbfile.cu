@@ -222,31 +222,67 @@ bool read_i64s(Reader& r, std::vector<int64_t>& v) {
     return r.ok;
 }
 
-bool read_fmd(const char* path, int n_threads, msg_db& db) {
+// The stored parts of an .fmd file, parsed but not decoded.
+struct FmdRaw {
+    int64_t B[256], C[256];
+    uint64_t n = 0, height = 0;
+    std::vector<uint64_t> occ;          // the wavelet tree's occurrence table
+    std::vector<RawRrr> raw;            // its `height` levels, then SAidx
+    std::vector<int64_t> sa_sampled;
+};
+
+bool parse_fmd(const char* path, FmdRaw& f) {
     Reader r(path);
     if (!r.ok || !r.header()) return false;
-    int64_t B[256], C[256];
-    r.bytes(B, sizeof(B));
-    r.bytes(C, sizeof(C));
+    r.bytes(f.B, sizeof(f.B));
+    r.bytes(f.C, sizeof(f.C));
     // wavelet tree
-    const uint64_t n = r.get<uint64_t>();
+    f.n = r.get<uint64_t>();
     r.get<uint64_t>();  // sigma
-    const uint64_t height = r.get<uint64_t>();
+    f.height = r.get<uint64_t>();
     r.get<uint64_t>();  // wid
     r.get<uint64_t>();  // min
     r.get<uint64_t>();  // max
     r.get<uint64_t>();  // sample_rate
     const uint64_t nocc = r.get<uint64_t>();
-    if (!r.ok || height == 0 || height > 8 || nocc > 1024) return false;
-    std::vector<uint64_t> occ(nocc);
-    r.bytes(occ.data(), nocc * 8);
+    if (!r.ok || f.height == 0 || f.height > 8 || nocc > 1024) return false;
+    f.occ.resize(nocc);
+    r.bytes(f.occ.data(), nocc * 8);
+    f.raw.resize(f.height + 1);
+    for (uint64_t l = 0; l < f.height; ++l)
+        if (!parse_rrr(r, f.raw[l]) || f.raw[l].n != f.n) return false;
+    std::vector<int64_t> gap_sa;
+    return read_i64s(r, gap_sa) && parse_rrr(r, f.raw[f.height]) && read_i64s(r, f.sa_sampled);
+}
+
+// The first rows' positions in each wavelet-tree node, [l * 2^height +
+// prefix]: the 0-child of a node starts where the node does, the 1-child
+// at occ[symbol prefix]; prefixes above the alphabet's largest symbol hold
+// no rows and start at n, where any row would be caught as corrupt.
+std::vector<uint64_t> node_starts(const FmdRaw& f) {
+    const uint64_t height = f.height, nodes = 1ull << height;
+    std::vector<uint64_t> node_start(height * nodes, 0);
+    for (uint64_t l = 0; l + 1 < height; ++l) {
+        for (uint64_t q = 0; q < (1ull << l); ++q) {
+            const uint64_t s1 = ((2 * q + 1) << (height - l - 1));
+            node_start[(l + 1) * nodes + 2 * q] = node_start[l * nodes + q];
+            node_start[(l + 1) * nodes + 2 * q + 1] = s1 < f.occ.size() ? f.occ[s1] : f.n;
+        }
+    }
+    return node_start;
+}
+
+bool read_fmd(const char* path, int n_threads, msg_db& db) {
+    FmdRaw f;
+    if (!parse_fmd(path, f)) return false;
+    const int64_t* B = f.B;
+    const int64_t* C = f.C;
+    const uint64_t n = f.n, height = f.height;
+    const std::vector<uint64_t>& occ = f.occ;
+    std::vector<RawRrr>& raw = f.raw;
+    std::vector<int64_t>& sa_sampled = f.sa_sampled;
     const Rrr tab;
-    // the bit sequences are read in file order, then unranked in parallel
-    std::vector<RawRrr> raw(height + 1);
-    for (uint64_t l = 0; l < height; ++l)
-        if (!parse_rrr(r, raw[l]) || raw[l].n != n) return false;
-    std::vector<int64_t> gap_sa, sa_sampled;
-    if (!read_i64s(r, gap_sa) || !parse_rrr(r, raw[height]) || !read_i64s(r, sa_sampled)) return false;
+    // the bit sequences were read in file order; they are unranked in parallel
     std::vector<Plain> lv(height);
     Plain saidx;
     {
@@ -277,16 +313,7 @@ bool read_fmd(const char* path, int n_threads, msg_db& db) {
     // the 1-child at occ[symbol prefix]). A thread starting at row lo sets
     // its cursors with rank queries at the boundary, node by node.
     const uint64_t nodes = 1ull << height;
-    std::vector<uint64_t> node_start(height * nodes, 0);  // [l * nodes + prefix]
-    for (uint64_t l = 0; l + 1 < height; ++l) {
-        for (uint64_t q = 0; q < (1ull << l); ++q) {
-            // prefixes above the alphabet's largest symbol hold no rows: they
-            // start at n, where any row would be caught as corrupt
-            const uint64_t s1 = ((2 * q + 1) << (height - l - 1));
-            node_start[(l + 1) * nodes + 2 * q] = node_start[l * nodes + q];
-            node_start[(l + 1) * nodes + 2 * q + 1] = s1 < occ.size() ? occ[s1] : n;
-        }
-    }
+    const std::vector<uint64_t> node_start = node_starts(f);  // [l * nodes + prefix]
     const int nt = std::max(1, n_threads);
     std::vector<std::vector<uint64_t>> hist(nt, std::vector<uint64_t>(nodes, 0));  // decoded symbols per thread
     auto decode = [&](int t, uint64_t lo, uint64_t hi) {
@@ -728,5 +755,485 @@ extern "C" int msg_db_read_cached(const char* mtg_path, const char* mgs_path, co
         written = false;
     }
     if (from_image) *from_image = written ? 0 : -1;
+    return MSG_OK;
+}
+
+// ---- Decoding the BWT on the GPU (msg_db_read_device) ----
+//
+// The same decode as read_fmd, with its per-symbol work on the device:
+//   1. each RRR bit sequence (the tree's levels and SAidx) is unranked by one
+//      thread per superblock of 64 blocks (64 x 15 bits = 15 whole words, so
+//      no two threads write one word); the superblock's first offset bit is
+//      an exclusive sum of its blocks' offset widths;
+//   2. a rank directory per sequence (ones before each word: a scan of the
+//      words' popcounts);
+//   3. one thread per BWT row walks the tree as WaveletTreeRRR::access does
+//      (WaveletTreeRRR.cpp:58-76): the row's position in a child node is the
+//      child's first row plus the rows before it in its node that took the
+//      same branch -- a rank difference -- which is where the host decode's
+//      per-node cursors put it;
+//   4. SAidx's set bits become the sampled rows, and the last sample's value
+//      (missing from files written by FMDIndex::buildSA, FMDIndex.cpp:495)
+//      is recomputed by the same LF walk as on the host.
+// Every index a kernel forms from file contents is checked before use; a
+// file the host decode rejects is rejected here too (MSG_EINVAL).
+#include <cub/cub.cuh>
+
+namespace {
+
+constexpr int kSbBlocks = 64;  // RRR blocks per superblock
+constexpr int kSbWords = 15;   // 64-bit words of plain bits per superblock
+constexpr uint32_t kDecBad = 1u;
+constexpr int kFixupMaxSteps = 1 << 16;  // LF steps of the last-sample walk (about 32 expected)
+
+// C(15, k) and the width of a class-k offset (bits of C(15, k) - 1)
+__device__ __host__ inline uint32_t binom15(int k) {
+    uint32_t c = 1;
+    for (int i = 0; i < k; ++i) c = c * (15 - i) / (i + 1);
+    return c;
+}
+__device__ __host__ inline int offset_bits(int k) {
+    uint32_t x = binom15(k) - 1;
+    int b = 0;
+    for (; x; x >>= 1) ++b;
+    return b;
+}
+
+// Shared tables of a block: binomial coefficients C(i, j), i, j < 16, and
+// the offset widths.
+struct RrrShared {
+    uint32_t binom[16][16];
+    int offbits[16];
+};
+
+__device__ void rrr_shared_init(RrrShared& t) {
+    for (int e = threadIdx.x; e < 256; e += blockDim.x) {
+        const int i = e >> 4, j = e & 15;
+        uint32_t c = 0;
+        if (j <= i) {
+            c = 1;
+            for (int k = 0; k < j; ++k) c = c * (i - k) / (k + 1);
+        }
+        t.binom[i][j] = c;
+    }
+    if (threadIdx.x < 16) t.offbits[threadIdx.x] = offset_bits(threadIdx.x);
+    __syncthreads();
+}
+
+__device__ __forceinline__ int rrr_class(const uint64_t* __restrict__ cw, int64_t ncw, int64_t b) {
+    const int64_t i = b >> 4;  // 16 four-bit classes per word
+    return i < ncw ? (int)((cw[i] >> (4 * (b & 15))) & 15) : 0;
+}
+
+__global__ void k_rrr_sb_bits(const uint64_t* __restrict__ cw, int64_t ncw, int64_t nC, int64_t nsb,
+                              uint64_t* __restrict__ sb_bits) {
+    __shared__ RrrShared t;
+    rrr_shared_init(t);
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < nsb; g += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t s = 0;
+        const int64_t b0 = g * kSbBlocks, b1 = min(nC, b0 + kSbBlocks);
+        for (int64_t b = b0; b < b1; ++b) s += (uint64_t)t.offbits[rrr_class(cw, ncw, b)];
+        sb_bits[g] = s;
+    }
+}
+
+// bits [pos, pos + len) of the offset stream, len <= 13
+__device__ __forceinline__ uint64_t o_bits(const uint64_t* __restrict__ ow, int64_t now, uint64_t pos, int len) {
+    if (len == 0) return 0;
+    const uint64_t i = pos >> 6;
+    const int j = (int)(pos & 63);
+    uint64_t v = (int64_t)i < now ? ow[i] >> j : 0;
+    if (j + len > 64 && (int64_t)(i + 1) < now) v |= ow[i + 1] << (64 - j);
+    return v & ((1ull << len) - 1);
+}
+
+// The offset-th k-subset of {0..14} in lexicographic order, as a bitmap
+// (BitSeqRRR's block encoding, as Rrr::unrank on the host).
+__device__ __forceinline__ uint32_t rrr_unrank(const RrrShared& t, int k, uint64_t off) {
+    if (k == 0) return 0;
+    if (k == 15) return 0x7fff;
+    uint32_t v = 0;
+    int r = k;
+    for (int i = 0; i < 15 && r > 0; ++i) {
+        const uint32_t cnt = t.binom[14 - i][r - 1];
+        if (off < cnt) { v |= 1u << i; --r; }
+        else off -= cnt;
+    }
+    return v;
+}
+
+// One thread per superblock: its 64 blocks unranked into its 15 words
+// (bits past n cleared), the class sum and the popcount counted.
+__global__ void k_rrr_unrank(const uint64_t* __restrict__ cw, int64_t ncw, const uint64_t* __restrict__ ow, int64_t now,
+                             uint64_t o_nbits, int64_t nC, int64_t nsb, const uint64_t* __restrict__ sb_pos,
+                             uint64_t n_bits, uint64_t* __restrict__ out, unsigned long long* __restrict__ sums,
+                             uint32_t* __restrict__ err) {
+    __shared__ RrrShared t;
+    rrr_shared_init(t);
+    unsigned long long cls = 0, pop = 0;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < nsb; g += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t wb[kSbWords];
+#pragma unroll
+        for (int j = 0; j < kSbWords; ++j) wb[j] = 0;
+        uint64_t pos = sb_pos[g];
+        const int64_t b0 = g * kSbBlocks, b1 = min(nC, b0 + kSbBlocks);
+        for (int64_t b = b0; b < b1; ++b) {
+            const int k = rrr_class(cw, ncw, b);
+            const int len = t.offbits[k];
+            if (pos + len > o_nbits) { atomicOr(err, kDecBad); break; }
+            const uint32_t v = rrr_unrank(t, k, o_bits(ow, now, pos, len));
+            pos += len;
+            cls += (unsigned long long)k;
+            const int lb = (int)(b - b0) * 15;
+            const int lw = lb >> 6, sh = lb & 63;
+            wb[lw] |= (uint64_t)v << sh;
+            if (sh > 49) wb[lw + 1] |= (uint64_t)v >> (64 - sh);  // lw + 1 < 15: the last block ends at bit 960
+        }
+#pragma unroll
+        for (int j = 0; j < kSbWords; ++j) {
+            const uint64_t gb = (uint64_t)(g * kSbWords + j) * 64;  // first bit of the word
+            uint64_t x = wb[j];
+            if (gb >= n_bits) x = 0;
+            else if (n_bits - gb < 64) x &= (1ull << (n_bits - gb)) - 1;
+            out[g * kSbWords + j] = x;
+            pop += (unsigned long long)__popcll(x);
+        }
+    }
+    if (cls) atomicAdd(&sums[0], cls);
+    if (pop) atomicAdd(&sums[1], pop);
+}
+
+__global__ void k_word_popc(const uint64_t* __restrict__ w, int64_t nw, uint64_t* __restrict__ cnt) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= nw; i += (int64_t)gridDim.x * blockDim.x)
+        cnt[i] = i < nw ? (uint64_t)__popcll(w[i]) : 0;
+}
+
+struct WtLevels {
+    const uint64_t* w[9];
+    const uint64_t* dir[9];  // ones before each word; one entry past the last word
+};
+
+// ones in [0, x), x <= n (the directory has an entry for every word and one past)
+__device__ __forceinline__ uint64_t rank_excl(const uint64_t* __restrict__ w, const uint64_t* __restrict__ dir,
+                                              uint64_t x) {
+    const uint64_t k = x >> 6;
+    const int r = (int)(x & 63);
+    return dir[k] + (r ? (uint64_t)__popcll(w[k] & ((1ull << r) - 1)) : 0);
+}
+
+__global__ void k_wt_access(WtLevels L, int height, int64_t n, const uint64_t* __restrict__ node_start, int nodes,
+                            int64_t nocc, uint8_t* __restrict__ bwt, unsigned long long* __restrict__ hist,
+                            uint32_t* __restrict__ err) {
+    __shared__ unsigned long long s_hist[256];
+    for (int e = threadIdx.x; e < 256; e += blockDim.x) s_hist[e] = 0;
+    __syncthreads();
+    bool any_bad = false;
+    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n; row += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t i = (uint64_t)row;
+        uint32_t q = 0;
+        bool bad = false;
+        for (int l = 0; l < height; ++l) {
+            if (i >= (uint64_t)n) { bad = true; break; }
+            const uint64_t* w = L.w[l];
+            const uint32_t bit = (uint32_t)((w[i >> 6] >> (i & 63)) & 1);
+            if (l + 1 < height) {
+                const uint64_t st = node_start[l * nodes + q];
+                if (st > i) { bad = true; break; }
+                const uint64_t ob = rank_excl(w, L.dir[l], i) - rank_excl(w, L.dir[l], st);
+                const uint32_t child = 2 * q + bit;
+                const uint64_t cst = node_start[(l + 1) * nodes + child];
+                i = bit ? cst + ob : cst + (i - st - ob);
+                q = child;
+            } else {
+                q = 2 * q + bit;
+            }
+        }
+        // a symbol without an entry in the occurrence table is not one the
+        // index holds (WaveletTreeRRR.h:238)
+        if (!bad && (int64_t)q + 1 >= nocc) bad = true;
+        if (bad) { any_bad = true; continue; }
+        bwt[row] = (uint8_t)q;
+        atomicAdd(&s_hist[q], 1ull);
+    }
+    if (any_bad) atomicOr(err, kDecBad);
+    __syncthreads();
+    for (int e = threadIdx.x; e < 256; e += blockDim.x)
+        if (s_hist[e]) atomicAdd(&hist[e], s_hist[e]);
+}
+
+__global__ void k_set_bit_rows(const uint64_t* __restrict__ w, const uint64_t* __restrict__ dir, int64_t nw,
+                               uint64_t cap, int64_t* __restrict__ rows) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nw; k += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t x = w[k], at = dir[k];
+        while (x) {
+            const int b = __ffsll((long long)x) - 1;
+            if (at < cap) rows[at] = k * 64 + b;
+            ++at;
+            x &= x - 1;
+        }
+    }
+}
+
+// WaveletTreeRRR::rank (occurrences of sym in [0, i]) over the decoded
+// levels; 0 for positions outside the sequence.
+__device__ uint64_t wt_rank(const WtLevels& L, int height, uint64_t n, const uint64_t* __restrict__ occ, int64_t nocc,
+                            uint64_t sym, uint64_t i) {
+    uint64_t start = 0, r = ~0ull;
+    for (int l = 0; r != 0 && l < height; ++l) {
+        if (i >= n || start > n) return 0;
+        const uint64_t* w = L.w[l];
+        const uint64_t* dir = L.dir[l];
+        const uint64_t before = rank_excl(w, dir, start);
+        const uint64_t upto = rank_excl(w, dir, i + 1);
+        if ((sym >> (height - l - 1)) & 1) {
+            const uint64_t masked = (sym >> (height - l - 1)) << (height - l - 1);
+            r = upto - before;
+            if (masked >= (uint64_t)nocc) return 0;
+            start = occ[masked];
+        } else {
+            r = i - start + before - upto + 1;
+        }
+        if (r == 0) return 0;
+        i = r + start - 1;
+    }
+    return r;
+}
+
+// The last sampled row's SA value: LF-walk from it to the next sampled row
+// with a stored value (out[0] = that sample's index, out[1] = the distance).
+__global__ void k_sample_fixup(WtLevels L, int height, int64_t n, const uint64_t* __restrict__ occ, int64_t nocc,
+                               const int64_t* __restrict__ C, const uint8_t* __restrict__ bwt,
+                               const uint64_t* __restrict__ sw, const uint64_t* __restrict__ sdir, int64_t n_stored,
+                               int64_t j, int64_t* __restrict__ out, uint32_t* __restrict__ err) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    uint64_t i = (uint64_t)j;
+    int64_t dist = 0;
+    for (;;) {
+        if (i >= (uint64_t)n || dist >= kFixupMaxSteps) { atomicOr(err, kDecBad); return; }
+        const uint64_t b = bwt[i];
+        if (b == 0 || b >= 16) { atomicOr(err, kDecBad); return; }  // a '$' row is always sampled and stored
+        const uint64_t rk = wt_rank(L, height, (uint64_t)n, occ, nocc, b, i);
+        if (rk == 0 || C[b] < 0 || (uint64_t)C[b] + rk - 1 >= (uint64_t)n) { atomicOr(err, kDecBad); return; }
+        i = (uint64_t)C[b] + rk - 1;  // LF(b, i) - 1 (FMDIndex.h:130-141)
+        ++dist;
+        if ((sw[i >> 6] >> (i & 63)) & 1) {
+            const uint64_t idx = rank_excl(sw, sdir, i + 1) - 1;
+            if (idx < (uint64_t)n_stored) {
+                out[0] = (int64_t)idx;
+                out[1] = dist;
+                return;
+            }
+        }
+    }
+}
+
+// Device allocations of one decode, freed together.
+struct DevPool {
+    std::vector<void*> ptrs;
+    cudaError_t err = cudaSuccess;
+    template <typename T> T* get(size_t count) {
+        void* p = nullptr;
+        if (err == cudaSuccess) err = cudaMalloc(&p, std::max<size_t>(count * sizeof(T), 16));
+        if (err != cudaSuccess) return nullptr;
+        ptrs.push_back(p);
+        return static_cast<T*>(p);
+    }
+    void release(void* p) {
+        for (auto& q : ptrs)
+            if (q == p) { cudaFree(q); q = nullptr; }
+    }
+    ~DevPool() {
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
+    }
+};
+
+int grid_for(int64_t n, int threads, int num_sms) {
+    const int64_t b = (n + threads - 1) / threads;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)num_sms * 16));
+}
+
+// One decoded bit sequence on the device: plain words and rank directory.
+struct DevBits {
+    uint64_t* w = nullptr;
+    uint64_t* dir = nullptr;
+    int64_t nw = 0;
+};
+
+// Unranks `raw` into `out`; MSG_EINVAL when its classes, offsets or ones
+// disagree with its header.
+int unrank_device(const RawRrr& raw, DevPool& pool, int num_sms, cudaStream_t st, DevBits& out) {
+    const int64_t nC = (int64_t)raw.nC, nsb = (nC + kSbBlocks - 1) / kSbBlocks;
+    const int64_t ncw = (int64_t)raw.C.w.size(), now = (int64_t)raw.O.w.size();
+    if ((uint64_t)ncw * 64 < 4 * raw.nC || (uint64_t)now * 64 < raw.O.nbits || nsb <= 0) return MSG_EINVAL;
+    uint64_t* d_cw = pool.get<uint64_t>(ncw);
+    uint64_t* d_ow = pool.get<uint64_t>(now);
+    uint64_t* d_sb = pool.get<uint64_t>(nsb);
+    uint64_t* d_pos = pool.get<uint64_t>(nsb);
+    out.nw = nsb * kSbWords;
+    out.w = pool.get<uint64_t>(out.nw);
+    uint64_t* d_cnt = pool.get<uint64_t>(out.nw + 1);
+    out.dir = pool.get<uint64_t>(out.nw + 1);
+    unsigned long long* d_sums = pool.get<unsigned long long>(2);
+    uint32_t* d_err = pool.get<uint32_t>(1);
+    if (pool.err != cudaSuccess) return pool.err == cudaErrorMemoryAllocation ? MSG_ENOMEM : MSG_ECUDA;
+    cudaError_t e = cudaMemcpyAsync(d_cw, raw.C.w.data(), ncw * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && now > 0) e = cudaMemcpyAsync(d_ow, raw.O.w.data(), now * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_sums, 0, 16, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_err, 0, 4, st);
+    if (e != cudaSuccess) return MSG_ECUDA;
+    k_rrr_sb_bits<<<grid_for(nsb, 256, num_sms), 256, 0, st>>>(d_cw, ncw, nC, nsb, d_sb);
+    size_t tb = 0;
+    if (cub::DeviceScan::ExclusiveSum(nullptr, tb, d_sb, d_pos, (int)nsb, st) != cudaSuccess) return MSG_ECUDA;
+    size_t tb2 = 0;
+    if (cub::DeviceScan::ExclusiveSum(nullptr, tb2, d_cnt, out.dir, (int)(out.nw + 1), st) != cudaSuccess)
+        return MSG_ECUDA;
+    void* d_tmp = pool.get<uint8_t>(std::max(tb, tb2));
+    if (pool.err != cudaSuccess) return pool.err == cudaErrorMemoryAllocation ? MSG_ENOMEM : MSG_ECUDA;
+    if (cub::DeviceScan::ExclusiveSum(d_tmp, tb, d_sb, d_pos, (int)nsb, st) != cudaSuccess) return MSG_ECUDA;
+    k_rrr_unrank<<<grid_for(nsb, 128, num_sms), 128, 0, st>>>(d_cw, ncw, d_ow, now, raw.O.nbits, nC, nsb, d_pos,
+                                                              raw.n, out.w, d_sums, d_err);
+    k_word_popc<<<grid_for(out.nw + 1, 256, num_sms), 256, 0, st>>>(out.w, out.nw, d_cnt);
+    if (cub::DeviceScan::ExclusiveSum(d_tmp, tb2, d_cnt, out.dir, (int)(out.nw + 1), st) != cudaSuccess)
+        return MSG_ECUDA;
+    unsigned long long sums[2] = {0, 0};
+    uint32_t bad = 0;
+    uint64_t total = 0;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sums, d_sums, 16, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_err, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&total, out.dir + out.nw, 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return MSG_ECUDA;
+    pool.release(d_cw);
+    pool.release(d_ow);
+    pool.release(d_sb);
+    pool.release(d_pos);
+    pool.release(d_cnt);
+    pool.release(d_tmp);
+    if (bad || sums[0] != raw.ones || sums[1] != raw.ones || total != raw.ones) return MSG_EINVAL;
+    return MSG_OK;
+}
+
+int read_fmd_device(const char* path, int num_sms, cudaStream_t st, msg_db& db) {
+    FmdRaw f;
+    // (below 2^36 symbols the scans' item counts fit their int arguments)
+    if (!parse_fmd(path, f) || f.n == 0 || f.n >= (1ull << 36)) return MSG_EINVAL;
+    const uint64_t n = f.n;
+    const int height = (int)f.height, nodes = 1 << height;
+    DevPool pool;
+    WtLevels L{};
+    DevBits sa_bits;
+    for (int l = 0; l <= height; ++l) {
+        DevBits b;
+        const int rc = unrank_device(f.raw[l], pool, num_sms, st, b);
+        if (rc != MSG_OK) return rc;
+        if (l < height) { L.w[l] = b.w; L.dir[l] = b.dir; }
+        else sa_bits = b;
+        f.raw[l] = RawRrr();  // the host copy is no longer needed
+    }
+    const std::vector<uint64_t> ns = node_starts(f);
+    uint64_t* d_ns = pool.get<uint64_t>(ns.size());
+    uint64_t* d_occ = pool.get<uint64_t>(f.occ.size() + 1);
+    int64_t* d_C = pool.get<int64_t>(256);
+    uint8_t* d_bwt = pool.get<uint8_t>(n);
+    unsigned long long* d_hist = pool.get<unsigned long long>(256);
+    uint32_t* d_err = pool.get<uint32_t>(1);
+    int64_t* d_fix = pool.get<int64_t>(2);
+    if (pool.err != cudaSuccess) return pool.err == cudaErrorMemoryAllocation ? MSG_ENOMEM : MSG_ECUDA;
+    cudaError_t e = cudaMemcpyAsync(d_ns, ns.data(), ns.size() * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !f.occ.empty())
+        e = cudaMemcpyAsync(d_occ, f.occ.data(), f.occ.size() * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_C, f.C, sizeof(f.C), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_hist, 0, 256 * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_err, 0, 4, st);
+    if (e != cudaSuccess) return MSG_ECUDA;
+    k_wt_access<<<grid_for((int64_t)n, 256, num_sms), 256, 0, st>>>(L, height, (int64_t)n, d_ns, nodes,
+                                                                    (int64_t)f.occ.size(), d_bwt, d_hist, d_err);
+    unsigned long long hist[256];
+    uint32_t bad = 0;
+    uint64_t marked = 0;  // SAidx's set bits
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hist, d_hist, sizeof(hist), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_err, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&marked, sa_bits.dir + sa_bits.nw, 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return MSG_ECUDA;
+    if (bad) return MSG_EINVAL;
+    // the decoded symbols must be the ones the occurrence table counts
+    for (uint64_t q = 0; q + 1 < f.occ.size() && q < (uint64_t)nodes; ++q)
+        if (hist[q] != f.occ[q + 1] - f.occ[q]) return MSG_EINVAL;
+    if (marked != f.sa_sampled.size() && marked != f.sa_sampled.size() + 1) return MSG_EINVAL;
+    // sampled rows: SAidx's set bits, in order
+    int64_t* d_rows = pool.get<int64_t>(marked);
+    if (pool.err != cudaSuccess) return pool.err == cudaErrorMemoryAllocation ? MSG_ENOMEM : MSG_ECUDA;
+    k_set_bit_rows<<<grid_for(sa_bits.nw, 256, num_sms), 256, 0, st>>>(sa_bits.w, sa_bits.dir, sa_bits.nw, marked,
+                                                                      d_rows);
+    db.sample_rows.resize(marked);
+    db.bwt.resize(n);
+    e = cudaGetLastError();
+    if (e == cudaSuccess && marked > 0)
+        e = cudaMemcpyAsync(db.sample_rows.data(), d_rows, marked * 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(db.bwt.data(), d_bwt, n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return MSG_ECUDA;
+    if (marked == f.sa_sampled.size() + 1) {
+        // FMDIndex::buildSA left the last sample's value out of the file: walk
+        // LF from that row to the next sampled row with a stored value
+        const int64_t j = db.sample_rows[marked - 1];
+        int64_t fix[2] = {-1, 0};
+        uint32_t fb = 0;
+        e = cudaMemsetAsync(d_err, 0, 4, st);
+        if (e == cudaSuccess) {
+            k_sample_fixup<<<1, 32, 0, st>>>(L, height, (int64_t)n, d_occ, (int64_t)f.occ.size(), d_C, d_bwt,
+                                             sa_bits.w, sa_bits.dir, (int64_t)f.sa_sampled.size(), j, d_fix, d_err);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(fix, d_fix, 16, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&fb, d_err, 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return MSG_ECUDA;
+        if (fb || fix[0] < 0 || fix[0] >= (int64_t)f.sa_sampled.size()) return MSG_EINVAL;
+        f.sa_sampled.push_back(f.sa_sampled[fix[0]] + fix[1]);
+    }
+    for (int b = 0; b < 16; ++b) db.base_count[b] = f.B[b];
+    db.sample_vals = std::move(f.sa_sampled);
+    return db.sample_rows.size() == db.sample_vals.size() ? MSG_OK : MSG_EINVAL;
+}
+
+}  // namespace
+
+extern "C" int msg_db_read_device(int device, const char* mtg_path, const char* mgs_path, const char* fmd_path,
+                                  msg_db** db) {
+    if (!mtg_path || !mgs_path || !fmd_path || !db) return MSG_EINVAL;
+    *db = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return MSG_ECUDA;
+    if (device < 0 || device >= count) return MSG_EINVAL;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return MSG_ECUDA;
+    if (prop.major != 10 || prop.minor != 0) return MSG_EUNSUPPORTED;
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) return MSG_ECUDA;
+    if (prev != device && cudaSetDevice(device) != cudaSuccess) return MSG_ECUDA;
+    int rc = MSG_OK;
+    msg_db* d = new (std::nothrow) msg_db();
+    cudaStream_t st = nullptr;
+    if (!d) rc = MSG_ENOMEM;
+    else if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) rc = MSG_ECUDA;
+    try {
+        if (rc == MSG_OK) rc = read_mtg(mtg_path, mgs_path, *d) ? MSG_OK : MSG_EINVAL;
+        if (rc == MSG_OK) rc = read_fmd_device(fmd_path, prop.multiProcessorCount, st, *d);
+    } catch (const std::bad_alloc&) {
+        rc = MSG_ENOMEM;
+    }
+    if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    if (rc == MSG_OK && (d->bd_end.empty() || d->bd_end.back() != (int64_t)d->bwt.size())) rc = MSG_EINVAL;
+    if (prev >= 0 && prev != device) cudaSetDevice(prev);
+    if (rc != MSG_OK) { delete d; return rc; }
+    *db = d;
     return MSG_OK;
 }

@@ -27,7 +27,7 @@ assert ALN_DTYPE.itemsize == 88
 
 # symbols of the C ABI, in include/msg_b200.h order
 EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy", "msg_index_load", "msg_db_read",
-           "msg_db_views", "msg_db_free", "msg_db_read_cached", "msg_index_bytes", "msg_ctx_share_index",
+           "msg_db_views", "msg_db_free", "msg_db_read_device", "msg_db_read_cached", "msg_index_bytes", "msg_ctx_share_index",
            "msg_map_params_default", "msg_map_batch", "msg_map_batches", "msg_seed_batch", "msg_locate_batch",
            "msg_chain_batch", "msg_align_batch", "msg_map_batch_device", "msg_last_stats",
            "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_ctx_set_dp_shape", "msg_ctx_set_dp_lanes", "msg_ctx_set_dp_occupancy", "msg_ctx_set_smem_shape", "msg_autotune", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
@@ -152,6 +152,7 @@ def load_library(path: str = LIB_PATH):
     L.msg_db_read.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]
     L.msg_db_views.argtypes = [C.c_void_p, C.POINTER(FmdView), C.POINTER(MtgView)]
     L.msg_db_free.argtypes = [C.c_void_p]
+    L.msg_db_read_device.argtypes = [C.c_int, C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_void_p)]
     L.msg_db_read_cached.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.POINTER(C.c_void_p),
                                      C.POINTER(C.c_int)]
     L.msg_db_free.restype = None
@@ -839,15 +840,20 @@ class Database:
     """A database read from msgseqtk-build files (msg_db_read): host arrays of
     the FMD-index and the MetaGenome, as numpy views."""
 
-    def __init__(self, mtg_path, mgs_path, fmd_path, n_threads: int = 8, image=None):
+    def __init__(self, mtg_path, mgs_path, fmd_path, n_threads: int = 8, image=None, device=None):
         """With `image` (a path), msg_db_read_cached: read the decoded image
         there when it matches the files, else decode and write it;
-        `from_image` tells which (1 read, 0 written, -1 not writable)."""
+        `from_image` tells which (1 read, 0 written, -1 not writable). With
+        `device`, msg_db_read_device: the BWT decoded on that GPU."""
         self.lib = load_library()
         self.h = C.c_void_p()
         self.from_image = None
         paths = [str(x).encode() for x in (mtg_path, mgs_path, fmd_path)]
-        if image is None:
+        if device is not None:
+            rc = self.lib.msg_db_read_device(int(device), *paths, C.byref(self.h))
+            if rc != MSG_OK:
+                raise MsgError(rc, "msg_db_read_device")
+        elif image is None:
             rc = self.lib.msg_db_read(*paths, n_threads, C.byref(self.h))
         else:
             hit = C.c_int(0)

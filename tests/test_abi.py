@@ -40,6 +40,7 @@ def test_null_arguments_rejected_without_device():
     assert L.msg_ctx_create(0, None) == lib.MSG_EINVAL
     assert L.msg_index_load(None, None, None) == lib.MSG_EINVAL
     assert L.msg_ctx_share_index(None, None) == lib.MSG_EINVAL
+    assert L.msg_db_read_device(0, None, None, None, None) == lib.MSG_EINVAL
     assert L.msg_map_batch(None, None, None, None, None) == lib.MSG_EINVAL
     assert L.msg_last_stats(None, None) == lib.MSG_EINVAL
     assert L.msg_mem_batch(None, None, None, None, None, None, 0, None) == lib.MSG_EINVAL

@@ -160,6 +160,52 @@ def test_decoded_image_is_reused_and_rebuilt(tmp_path):
 
 @pytest.mark.gpu
 @needs_ref
+@pytest.mark.parametrize("kind", ["small", "repeats", "merged"])
+def test_device_decode_equals_host_decode(tmp_path, kind):
+    """msg_db_read_device (BWT unranked, walked and listed by device
+    kernels) gives msg_db_read's database: BWT, counts, sampled rows and
+    values -- the last sample recomputed where the file lacks it -- and the
+    MetaGenome tables."""
+    if kind == "merged":
+        _, _, paths = _merged(tmp_path)
+    else:
+        g = (synth.small_genomes(seed=3, n_genomes=3, length=40_000) if kind == "small"
+             else synth.repeat_genomes(seed=4, n_genomes=3, length=30_000))
+        _, paths = _write(tmp_path, g)
+    host = lib.Database(*paths, n_threads=3)
+    dev = lib.Database(*paths, device=0)
+    _same_arrays(dev.arrays(), host.arrays())
+    host.close()
+    dev.close()
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_device_decode_rejects_what_host_rejects(tmp_path):
+    g = synth.small_genomes(seed=5, n_genomes=2, length=6_000)
+    _, paths = _write(tmp_path, g)
+    data = open(paths[2], "rb").read()
+    nocc = int(np.frombuffer(data[_OCC_AT - 8:_OCC_AT], np.uint64)[0])
+    for entry, delta in [(8, 1000_000), (8, -1), (4, 3), (2, -2)]:
+        occ = np.frombuffer(data[_OCC_AT:_OCC_AT + 8 * nocc], np.uint64).copy()
+        occ[entry] = np.uint64(int(occ[entry]) + delta)
+        bad = tmp_path / "bad.fmd"
+        bad.write_bytes(data[:_OCC_AT] + occ.tobytes() + data[_OCC_AT + 8 * nocc:])
+        with pytest.raises(lib.MsgError) as e:
+            lib.Database(paths[0], paths[1], bad, device=0)
+        assert e.value.code == lib.MSG_EINVAL, (entry, delta)
+    (tmp_path / "cut.fmd").write_bytes(data[: len(data) // 2])
+    with pytest.raises(lib.MsgError) as e:
+        lib.Database(paths[0], paths[1], tmp_path / "cut.fmd", device=0)
+    assert e.value.code == lib.MSG_EINVAL
+    # a good file still decodes after the rejected ones
+    dev = lib.Database(*paths, device=0)
+    _same_arrays(dev.arrays(), lib.Database(*paths, n_threads=1).arrays())
+    dev.close()
+
+
+@pytest.mark.gpu
+@needs_ref
 def test_index_from_db_files_maps_like_view(tmp_path):
     from msgseqtk_b200 import index_build
     g = synth.repeat_genomes(seed=4, n_genomes=3, length=30_000)
