@@ -615,6 +615,38 @@ int msg_sam_format(const msg_sam_rec* recs, int64_t n_recs, const char* md, cons
                    const uint8_t* quals, const uint32_t* cigar, const char* names, const int64_t* name_off,
                    const char* const* chrom_names, int64_t n_chrom, char* out, int64_t cap, int64_t* text_len);
 
+/* BAM output (msgseqtk-align's `-o out.bam`, written through htslib in the
+ * reference: src/msgseqtk-align.cpp:473-519, src/SAMtools/SAMfile.cpp), for
+ * callers without htslib. A file is
+ *   msg_bgzf_compress(header) + msg_bgzf_compress(records)... + the EOF member.
+ *
+ * msg_bam_header: the binary header of the SAM/BAM specification -- "BAM",
+ * the header text as given (the caller's @HD/@SQ/@PG lines), and one
+ * reference per chromosome (name, length) in tid order. */
+int msg_bam_header(const char* text, int64_t text_len, const char* const* chrom_names, const int64_t* chrom_len,
+                   int64_t n_chrom, uint8_t* out, int64_t cap, int64_t* len);
+
+/* msg_bam_format: the binary records of msg_sam_format's lines, from the same
+ * inputs -- the fields msgseqtk-align's BAM records carry (src/SAMtools/
+ * BAM.cpp:20-56: bin from [pos, pos + reference length of the CIGAR), next
+ * refID -1 and next pos 0, read name without padding, SEQ as nt16 codes two
+ * per byte, QUAL as phred values) and the aux fields in the order the
+ * reference sets them (AS, MD, XH, NH, XN, XP; integers in the smallest type
+ * that holds them, as htslib's bam_aux_update_int stores them). Writes *len
+ * bytes (uncompressed) into out (cap bytes; MSG_EINVAL with *len set when
+ * they do not fit). */
+int msg_bam_format(const msg_sam_rec* recs, int64_t n_recs, const char* md, const msg_read_batch* reads,
+                   const uint8_t* quals, const uint32_t* cigar, const char* names, const int64_t* name_off,
+                   int64_t n_chrom, uint8_t* out, int64_t cap, int64_t* len);
+
+/* msg_bgzf_compress: data[0..n) as BGZF members of at most 0xff00 input bytes
+ * each (raw deflate at `level` 0-9, CRC32 and size; the members are
+ * compressed on up to n_threads host threads and written in order), followed
+ * by the 28-byte end-of-file member when add_eof is set. Writes *len bytes
+ * into out (cap bytes; MSG_EINVAL with *len set when they do not fit). */
+int msg_bgzf_compress(const uint8_t* data, int64_t n, int level, int n_threads, int add_eof, uint8_t* out,
+                      int64_t cap, int64_t* len);
+
 /* ---- MEM search and read cleaning (msgseqtk-clean) ---- */
 
 typedef struct msg_mem_params {

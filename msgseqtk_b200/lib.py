@@ -32,7 +32,8 @@ EXPORTS = ["msg_strerror", "msg_last_error", "msg_ctx_create", "msg_ctx_destroy"
            "msg_chain_batch", "msg_align_batch", "msg_map_batch_device", "msg_last_stats",
            "msg_result_device", "msg_ctx_stream", "msg_ctx_set_scratch_limit", "msg_ctx_set_dp_shape", "msg_ctx_set_dp_lanes", "msg_ctx_set_dp_occupancy", "msg_ctx_set_smem_shape", "msg_autotune", "msg_smem_batch_noalloc", "msg_band_model_set", "msg_band_collect",
            "msg_band_train", "msg_band_grad", "msg_tail_params_default", "msg_tail_batch", "msg_pair_params_default", "msg_tail_pe_batch",
-           "msg_fastq_parse", "msg_fastq_format", "msg_clean_format", "msg_sam_format",
+           "msg_fastq_parse", "msg_fastq_format", "msg_clean_format", "msg_sam_format", "msg_bam_header",
+           "msg_bam_format", "msg_bgzf_compress",
            "msg_mem_params_default", "msg_mem_batch", "msg_clean_batch",
            "msg_clean_batch_device", "msg_occ_query", "msg_bi_ext_query", "msg_sa_query"]
 
@@ -203,6 +204,10 @@ def load_library(path: str = LIB_PATH):
     L.msg_sam_format.argtypes = [C.c_void_p, C.c_int64, C.c_char_p, C.POINTER(ReadBatch), u8p,
                                  C.POINTER(C.c_uint32), C.c_char_p, i64p, C.POINTER(C.c_char_p), C.c_int64, C.c_char_p,
                                  C.c_int64, i64p]
+    L.msg_bam_header.argtypes = [C.c_char_p, C.c_int64, C.POINTER(C.c_char_p), i64p, C.c_int64, u8p, C.c_int64, i64p]
+    L.msg_bam_format.argtypes = [C.c_void_p, C.c_int64, C.c_char_p, C.POINTER(ReadBatch), u8p,
+                                 C.POINTER(C.c_uint32), C.c_char_p, i64p, C.c_int64, u8p, C.c_int64, i64p]
+    L.msg_bgzf_compress.argtypes = [u8p, C.c_int64, C.c_int, C.c_int, C.c_int, u8p, C.c_int64, i64p]
     f64p = C.POINTER(C.c_double)
     L.msg_mem_params_default.argtypes = [C.POINTER(MemParams)]
     L.msg_mem_params_default.restype = None
@@ -378,6 +383,55 @@ def sam_format(recs, md: bytes, seq, off, qual, cigar, names: bytes, name_off, c
         if rc != MSG_OK:
             raise MsgError(rc, "msg_sam_format")
         return buf.raw[:n.value]
+
+
+def _grow(call, cap, what):
+    """Runs call(buf, cap, n) with a buffer that grows to the size it asks for."""
+    n = C.c_int64(0)
+    while True:
+        buf = np.empty(max(cap, 1), dtype=np.uint8)
+        rc = call(_p(buf, u8p), cap, C.byref(n))
+        if rc == MSG_EINVAL and n.value > cap:
+            cap = n.value
+            continue
+        if rc != MSG_OK:
+            raise MsgError(rc, what)
+        return buf[:n.value].tobytes()
+
+
+def bam_header(text: bytes, chrom_names, chrom_len) -> bytes:
+    """msg_bam_header: the uncompressed binary BAM header."""
+    L = load_library()
+    cn = (C.c_char_p * max(1, len(chrom_names)))(*[c.encode() for c in chrom_names])
+    cl = np.ascontiguousarray(chrom_len, dtype=np.int64)
+    return _grow(lambda b, cap, n: L.msg_bam_header(text, len(text), cn, _p(cl, i64p), len(chrom_names), b, cap, n),
+                 len(text) + 64 * len(chrom_names) + 64, "msg_bam_header")
+
+
+def bam_format(recs, md: bytes, seq, off, qual, cigar, names: bytes, name_off, n_chrom: int) -> bytes:
+    """msg_bam_format: uncompressed binary BAM records of tail records."""
+    L = load_library()
+    recs = np.ascontiguousarray(recs, dtype=SAM_DTYPE)
+    seq = np.ascontiguousarray(seq, dtype=np.uint8)
+    off = np.ascontiguousarray(off, dtype=np.int64)
+    qual = None if qual is None else np.ascontiguousarray(qual, dtype=np.uint8)
+    cigar = np.ascontiguousarray(cigar, dtype=np.uint32)
+    name_off = np.ascontiguousarray(name_off, dtype=np.int64)
+    rb = ReadBatch(len(off) - 1, _p(seq, u8p), _p(off, i64p))
+    return _grow(lambda b, cap, n: L.msg_bam_format(recs.ctypes.data, len(recs), md, C.byref(rb),
+                                                    _p(qual, u8p) if qual is not None else None,
+                                                    cigar.ctypes.data_as(C.POINTER(C.c_uint32)), names,
+                                                    _p(name_off, i64p), int(n_chrom), b, cap, n),
+                 1 << 16, "msg_bam_format")
+
+
+def bgzf_compress(data: bytes, level: int = 6, n_threads: int = 1, eof: bool = True) -> bytes:
+    """msg_bgzf_compress: BGZF members of data (and the EOF member)."""
+    L = load_library()
+    a = np.frombuffer(data, dtype=np.uint8) if len(data) else np.zeros(1, np.uint8)
+    a = np.ascontiguousarray(a)
+    return _grow(lambda b, cap, n: L.msg_bgzf_compress(_p(a, u8p), len(data), level, n_threads, int(eof), b, cap, n),
+                 len(data) + len(data) // 8 + 1024, "msg_bgzf_compress")
 
 
 def mem_params(**kw) -> MemParams:
